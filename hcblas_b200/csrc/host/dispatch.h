@@ -1,0 +1,46 @@
+/*
+ * dispatch.h -- internal interface between the API layer (gemm.cpp) and the
+ * path selection (dispatch.cpp).  Internal header.
+ */
+#ifndef HCBLAS_B200_DISPATCH_H_
+#define HCBLAS_B200_DISPATCH_H_
+
+#include <stdint.h>
+
+#include "../../../include/hcblas.h"
+#include "../../../include/hcblaslib.h"
+#include "../kernels/hcbk.h"
+#include "state.h"
+
+namespace hcblas_b200 {
+
+/* One GEMM call as the API layer sees it (before canonicalisation). */
+struct GemmCall {
+  int dtype;            /* HCBK_S .. HCBK_H */
+  hcblasOrder order;
+  int op_a, op_b;       /* HCBK_OP_* */
+  int64_t m, n, k;
+  double alpha_re, alpha_im, beta_re, beta_im;
+  const void *a;
+  int64_t lda, a_off, stride_a;
+  const void *const *a_arr;
+  const void *b;
+  int64_t ldb, b_off, stride_b;
+  const void *const *b_arr;
+  void *c;
+  int64_t ldc, c_off, stride_c;
+  void *const *c_arr;
+  int64_t batch;
+};
+
+int op_from_char(hcblasTranspose t);
+hcblasTranspose char_from_op(hcblasOperation_t op);
+hcblasStatus run_gemm(Hcblaslibrary *h, const hc::accelerator_view &view, GemmCall g);
+
+/* Choose and launch the kernel path for a canonical (column-major, alpha != 0)
+ * problem.  Returns an HCBK_* code; *path names the path taken. */
+int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path);
+
+}  // namespace hcblas_b200
+
+#endif /* HCBLAS_B200_DISPATCH_H_ */

@@ -1,0 +1,375 @@
+/*
+ * runtime.cpp -- handle lifecycle, accelerator views (streams), device memory
+ * and host<->device copies: the parts of hcBLAS's C API around GEMM
+ * (lib/src/hcblas.cpp:39-312) and of its HCC runtime usage (hc::am_alloc,
+ * accelerator_view::copy) re-expressed on the CUDA runtime.
+ */
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+
+#include "../../../include/hcblas.h"
+#include "../../../include/hcblaslib.h"
+#include "state.h"
+
+namespace hcblas_b200 {
+
+DeviceGuard::DeviceGuard(int dev) {
+  if (cudaGetDevice(&prev_) != cudaSuccess) {
+    prev_ = -1;
+    ok_ = false;
+    return;
+  }
+  if (dev == prev_) {
+    ok_ = true;
+    return;
+  }
+  ok_ = cudaSetDevice(dev) == cudaSuccess;
+}
+
+DeviceGuard::~DeviceGuard() {
+  int cur = -1;
+  if (prev_ >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev_) cudaSetDevice(prev_);
+}
+
+void *ensure_workspace(HcblasB200State *st, size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (st->workspace && st->workspace_bytes >= bytes && st->workspace_device == dev)
+    return st->workspace;
+  if (st->workspace) {
+    /* the previous workspace may still be read by queued kernels */
+    cudaDeviceSynchronize();
+    DeviceGuard g(st->workspace_device);
+    cudaFree(st->workspace);
+    st->workspace = nullptr;
+    st->workspace_bytes = 0;
+  }
+  size_t want = bytes < (size_t)(64u << 20) ? (size_t)(64u << 20) : bytes;
+  void *p = nullptr;
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  st->workspace = p;
+  st->workspace_bytes = want;
+  st->workspace_device = dev;
+  return p;
+}
+
+static std::atomic<long long> g_launches{0};
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+void *prof_event(HcblasB200State *st) {
+  if (!st->event_pool.empty()) {
+    void *e = st->event_pool.back();
+    st->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_record(void *ev, void *stream) {
+  cudaEventRecord(static_cast<cudaEvent_t>(ev), static_cast<cudaStream_t>(stream));
+}
+
+bool log_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HCBLAS_LOG");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
+}  // namespace hcblas_b200
+
+using hcblas_b200::DeviceGuard;
+
+/* ---------------------------------------------------- hc_compat services -- */
+
+extern "C" void *hcblas_am_alloc(size_t bytes, int device_id, unsigned flags) {
+  (void)flags;
+  DeviceGuard g(device_id);
+  if (!g.ok()) return nullptr;
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+extern "C" int hcblas_am_free(void *ptr) {
+  if (!ptr) return 0;
+  return cudaFree(ptr) == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int hcblas_am_copy(hcblas_accl_view_t view, const void *src, void *dst,
+                              size_t bytes) {
+  DeviceGuard g(view.device_id);
+  cudaStream_t s = static_cast<cudaStream_t>(view.stream);
+  if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s) != cudaSuccess) return -1;
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int hcblas_view_wait(hcblas_accl_view_t view) {
+  DeviceGuard g(view.device_id);
+  return cudaStreamSynchronize(static_cast<cudaStream_t>(view.stream)) == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int hcblas_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+extern "C" int hcblas_current_device(void) {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return d;
+}
+
+/* ------------------------------------------------------- Hcblaslibrary -- */
+
+Hcblaslibrary::Hcblaslibrary(hc::accelerator_view *av)
+    : currentAccl(av ? av->device_id : hcblas_current_device()),
+      currentAcclView(av ? *av : hc::accelerator_view()) {
+  const int n = hcblas_device_count();
+  const int dev = currentAccl.get_device_id();
+  initialized = (dev >= 0 && dev < n);
+  currentStream = currentAcclView.stream;
+  Order = ColMajor;
+  impl = new (std::nothrow) HcblasB200State();
+  if (!impl) initialized = false;
+}
+
+Hcblaslibrary::~Hcblaslibrary() {
+  initialized = false;
+  if (impl) {
+    if (impl->workspace) {
+      DeviceGuard g(impl->workspace_device);
+      cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
+      cudaFree(impl->workspace);
+    }
+    for (auto &r : impl->prof) {
+      cudaEventDestroy(static_cast<cudaEvent_t>(r.ev0));
+      cudaEventDestroy(static_cast<cudaEvent_t>(r.ev1));
+    }
+    for (void *e : impl->event_pool) cudaEventDestroy(static_cast<cudaEvent_t>(e));
+    delete impl;
+    impl = nullptr;
+  }
+}
+
+/* ------------------------------------------------------------- C API -- */
+
+extern "C" hcblasStatus_t hcblasCreate(hcblasHandle_t *handle, hcblas_accl_view_t *av) {
+  if (handle == nullptr) return HCBLAS_STATUS_INVALID_VALUE;
+  hc::accelerator_view view;
+  if (av) {
+    view.device_id = av->device_id;
+    view.stream = av->stream;
+  }
+  Hcblaslibrary *h = new (std::nothrow) Hcblaslibrary(&view);
+  if (h == nullptr) return HCBLAS_STATUS_ALLOC_FAILED;
+  if (!h->initialized) {
+    delete h;
+    *handle = nullptr;
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  }
+  *handle = h;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" hcblasStatus_t hcblasDestroy(hcblasHandle_t *handle) {
+  if (handle == nullptr || *handle == nullptr || !(*handle)->initialized)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  delete *handle;
+  *handle = nullptr;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" hcblasStatus_t hcblasSetAcclView(hcblasHandle_t handle, hcblas_accl_view_t *accl_view,
+                                            void *stream) {
+  if (handle == nullptr || !handle->initialized) return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (accl_view) {
+    handle->currentAcclView.device_id = accl_view->device_id;
+    handle->currentAcclView.stream = accl_view->stream;
+    handle->currentAccl = hc::accelerator(accl_view->device_id);
+  }
+  if (stream) handle->currentAcclView.stream = stream;
+  handle->currentStream = handle->currentAcclView.stream;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" hcblasStatus_t hcblasGetAcclView(hcblasHandle_t handle, hcblas_accl_view_t **accl_view,
+                                            void **stream) {
+  if (handle == nullptr) return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (accl_view) *accl_view = &handle->currentAcclView;
+  if (stream) *stream = handle->currentStream;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" hcblasStatus_t hcblasSetStream(hcblasHandle_t handle, void *stream) {
+  if (handle == nullptr || !handle->initialized) return HCBLAS_STATUS_NOT_INITIALIZED;
+  handle->currentAcclView.stream = stream;
+  handle->currentStream = stream;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+namespace {
+
+/* 2-D copy of `cols` columns of `rows` elements, then wait on the stream. */
+hcblasStatus_t copy2d(hcblasHandle_t h, const void *src, size_t spitch, void *dst,
+                      size_t dpitch, size_t width, size_t height) {
+  DeviceGuard g(h->currentAcclView.device_id);
+  cudaStream_t s = static_cast<cudaStream_t>(h->currentAcclView.stream);
+  cudaError_t e;
+  if (spitch == width && dpitch == width)
+    e = cudaMemcpyAsync(dst, src, width * height, cudaMemcpyDefault, s);
+  else
+    e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDefault, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return HCBLAS_STATUS_MAPPING_ERROR;
+  }
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+hcblasStatus_t copy_matrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                           const void *A, int lda, void *B, int ldb) {
+  if (handle == nullptr || !handle->initialized) return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (rows < 0 || cols < 0 || lda <= 0 || ldb <= 0 || elemSize <= 0)
+    return HCBLAS_STATUS_INVALID_VALUE;
+  if (rows == 0 || cols == 0) return HCBLAS_STATUS_SUCCESS;
+  if (A == nullptr || B == nullptr) return HCBLAS_STATUS_MAPPING_ERROR;
+  const size_t es = (size_t)elemSize;
+  if (lda >= rows && ldb >= rows)
+    return copy2d(handle, A, (size_t)lda * es, B, (size_t)ldb * es, (size_t)rows * es,
+                  (size_t)cols);
+  /* the reference's behaviour: rows*cols contiguous elements */
+  const size_t w = (size_t)rows * (size_t)cols * es;
+  return copy2d(handle, A, w, B, w, w, 1);
+}
+
+hcblasStatus_t copy_vector(hcblasHandle_t handle, int n, int elemSize, const void *x, int incx,
+                           void *y, int incy) {
+  if (handle == nullptr || !handle->initialized) return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (n < 0 || elemSize <= 0 || incx <= 0 || incy <= 0) return HCBLAS_STATUS_INVALID_VALUE;
+  if (n == 0) return HCBLAS_STATUS_SUCCESS;
+  if (x == nullptr || y == nullptr) return HCBLAS_STATUS_MAPPING_ERROR;
+  const size_t es = (size_t)elemSize;
+  return copy2d(handle, x, (size_t)incx * es, y, (size_t)incy * es, es, (size_t)n);
+}
+
+}  // namespace
+
+extern "C" hcblasStatus_t hcblasSetVector(hcblasHandle_t handle, int n, int elemSize,
+                                          const void *x, int incx, void *y, int incy) {
+  return copy_vector(handle, n, elemSize, x, incx, y, incy);
+}
+
+extern "C" hcblasStatus_t hcblasGetVector(hcblasHandle_t handle, int n, int elemSize,
+                                          const void *x, int incx, void *y, int incy) {
+  return copy_vector(handle, n, elemSize, x, incx, y, incy);
+}
+
+extern "C" hcblasStatus_t hcblasSetMatrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                                          const void *A, int lda, void *B, int ldb) {
+  return copy_matrix(handle, rows, cols, elemSize, A, lda, B, ldb);
+}
+
+extern "C" hcblasStatus_t hcblasGetMatrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                                          const void *A, int lda, void *B, int ldb) {
+  return copy_matrix(handle, rows, cols, elemSize, A, lda, B, ldb);
+}
+
+extern "C" hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param) {
+  if (handle == nullptr || !handle->initialized || !handle->impl)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (mode < HCBLAS_MATH_NATIVE || mode > HCBLAS_MATH_OZAKI_INT8)
+    return HCBLAS_STATUS_INVALID_VALUE;
+  if (mode == HCBLAS_MATH_SPLIT_BF16 && !(param == 0 || param == 3 || param == 6))
+    return HCBLAS_STATUS_INVALID_VALUE;
+  if (mode == HCBLAS_MATH_OZAKI_INT8 && (param < 0 || param > 8))
+    return HCBLAS_STATUS_INVALID_VALUE;
+  handle->impl->math_mode = mode;
+  handle->impl->math_param = param;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param) {
+  if (handle == nullptr || !handle->initialized || !handle->impl)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (mode) *mode = handle->impl->math_mode;
+  if (param) *param = handle->impl->math_param;
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" const char *hcblasGetLastPath(hcblasHandle_t handle) {
+  if (handle == nullptr || !handle->impl) return "none";
+  return handle->impl->last_path;
+}
+
+extern "C" const char *hcblasGetVersionString(void) { return "hcblas-b200 0.1.0 (sm_100a)"; }
+
+extern "C" long long hcblasGetKernelLaunchCount(void) { return hcblas_b200::launch_count(); }
+
+extern "C" hcblasStatus_t hcblasSetProfiling(hcblasHandle_t handle, int on) {
+  if (handle == nullptr || !handle->initialized || !handle->impl)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  HcblasB200State *st = handle->impl;
+  st->profiling = on != 0;
+  for (auto &r : st->prof) {
+    st->event_pool.push_back(r.ev0);
+    st->event_pool.push_back(r.ev1);
+  }
+  st->prof.clear();
+  return HCBLAS_STATUS_SUCCESS;
+}
+
+extern "C" int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap) {
+  if (handle == nullptr || !handle->initialized || !handle->impl) return -1;
+  HcblasB200State *st = handle->impl;
+  DeviceGuard g(handle->currentAcclView.device_id);
+  std::map<std::string, std::pair<long long, double>> agg;
+  for (auto &r : st->prof) {
+    cudaEventSynchronize(static_cast<cudaEvent_t>(r.ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(r.ev0), static_cast<cudaEvent_t>(r.ev1));
+    auto &a = agg[r.name];
+    a.first += 1;
+    a.second += ms;
+  }
+  std::string out;
+  char line[256];
+  for (auto &kv : agg) {
+    std::snprintf(line, sizeof(line), "%s %lld %.6f\n", kv.first.c_str(), kv.second.first,
+                  kv.second.second);
+    out += line;
+  }
+  if (buf && cap > 0) {
+    std::strncpy(buf, out.c_str(), (size_t)cap - 1);
+    buf[cap - 1] = '\0';
+  }
+  return (int)out.size();
+}

@@ -1,0 +1,87 @@
+/*
+ * state.h -- per-handle state that the B200 library adds behind
+ * Hcblaslibrary::impl (math mode, device workspace, tuned configurations,
+ * diagnostics).  Internal header.
+ */
+#ifndef HCBLAS_B200_STATE_H_
+#define HCBLAS_B200_STATE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+/* one timed kernel launch (events recorded on the launch stream) */
+struct HcblasProfRec {
+  const char *name;
+  void *ev0; /* cudaEvent_t */
+  void *ev1;
+};
+
+struct HcblasB200State {
+  int math_mode = 0;   /* HCBLAS_MATH_* */
+  int math_param = 0;  /* terms (split-BF16) or slices (Ozaki) */
+  const char *last_path = "none";
+  /* device workspace owned by the handle (grown on demand, freed at destroy) */
+  void *workspace = nullptr;
+  size_t workspace_bytes = 0;
+  int workspace_device = -1;
+  /* per-kernel CUDA-event timing (hcblasSetProfiling) */
+  bool profiling = false;
+  std::vector<HcblasProfRec> prof;
+  std::vector<void *> event_pool;
+};
+
+namespace hcblas_b200 {
+
+/* Launch one kernel through `fn` (returns an HCBK_* code); when profiling is
+ * on, bracket it with CUDA events on `stream`.  Counts every launch. */
+template <typename F>
+int timed_launch(HcblasB200State *st, void *stream, const char *name, F &&fn);
+
+/* cumulative number of kernels launched by this library in this process */
+void count_launch(int n = 1);
+long long launch_count();
+void *prof_event(HcblasB200State *st);
+void prof_record(void *ev, void *stream);
+
+template <typename F>
+int timed_launch(HcblasB200State *st, void *stream, const char *name, F &&fn) {
+  if (st && st->profiling) {
+    void *e0 = prof_event(st);
+    void *e1 = prof_event(st);
+    prof_record(e0, stream);
+    int rc = fn();
+    prof_record(e1, stream);
+    st->prof.push_back(HcblasProfRec{name, e0, e1});
+    if (rc == 0) count_launch();
+    return rc;
+  }
+  int rc = fn();
+  if (rc == 0) count_launch();
+  return rc;
+}
+
+/* Make `dev` current for the lifetime of the guard, restoring the previous
+ * device afterwards. */
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+  bool ok() const { return ok_; }
+
+ private:
+  int prev_ = -1;
+  bool ok_ = false;
+};
+
+/* Grow the handle's workspace to at least `bytes` on the current device. */
+void *ensure_workspace(HcblasB200State *st, size_t bytes);
+
+/* HCBLAS_LOG=1 prints one line per GEMM call with the path taken. */
+bool log_enabled();
+
+}  // namespace hcblas_b200
+
+#endif /* HCBLAS_B200_STATE_H_ */

@@ -1,0 +1,83 @@
+/*
+ * hcbk.h -- the thin C-ABI shim between the C++ host library (handle,
+ * argument checks, dispatch, autotuner) and the sm_100a CUDA kernels.
+ *
+ * Everything crossing this boundary is plain C: POD structs, raw device
+ * pointers, int64 sizes and a cudaStream_t passed as void*.  The host side is
+ * compiled by g++, the kernel side by nvcc; neither includes the other's
+ * headers.  All problems arrive here already in column-major canonical form
+ * (the host rewrites row-major C = op(A) op(B) as column-major
+ * C^T = op(B)^T op(A)^T), so every kernel implements column-major only.
+ */
+#ifndef HCBLAS_B200_HCBK_H_
+#define HCBLAS_B200_HCBK_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* storage types */
+enum hcbk_dtype { HCBK_S = 0, HCBK_D = 1, HCBK_C = 2, HCBK_Z = 3, HCBK_H = 4 };
+/* operand transforms: op(X) = X, X^T, X^H */
+enum hcbk_op { HCBK_OP_N = 0, HCBK_OP_T = 1, HCBK_OP_C = 2 };
+
+/* return codes of every hcbk_* launcher */
+enum hcbk_status {
+  HCBK_OK = 0,
+  HCBK_ERR_ARGS = 1,      /* unsupported argument combination */
+  HCBK_ERR_LAUNCH = 2,    /* cudaGetLastError() reported a failure */
+  HCBK_ERR_ALIGN = 3,     /* operands not aligned for the requested path */
+  HCBK_ERR_NOMEM = 4,     /* workspace too small */
+  HCBK_ERR_DRIVER = 5     /* driver entry point (tensor maps) unavailable */
+};
+
+/*
+ * One GEMM problem (or a batch of identically-shaped ones), column-major:
+ *   C_b := alpha * op(A_b) * op(B_b) + beta * C_b,   b = 0 .. batch-1
+ * with
+ *   X_b = (x_array ? x_array[b] : x) + x_off + b * stride_x   (elements).
+ * op(A) is m x k, op(B) is k x n, C is m x n.  alpha/beta are given in
+ * binary64 {re, im}; the kernels cast them to the compute type.
+ */
+typedef struct hcbk_gemm_args {
+  int dtype;
+  int op_a, op_b;
+  int64_t m, n, k;
+  const void *a;
+  int64_t lda, stride_a, a_off;
+  const void *b;
+  int64_t ldb, stride_b, b_off;
+  void *c;
+  int64_t ldc, stride_c, c_off;
+  const void *const *a_array; /* device-resident pointer arrays or NULL */
+  const void *const *b_array;
+  void *const *c_array;
+  int64_t batch;
+  double alpha_re, alpha_im;
+  double beta_re, beta_im;
+} hcbk_gemm_args;
+
+/* SIMT tile-shape choice (index into the per-dtype config table). */
+typedef struct hcbk_simt_cfg {
+  int variant; /* 0 = large tile, 1 = small tile */
+} hcbk_simt_cfg;
+
+/* Plain paths on CUDA cores: FP32 / FP64 / complex FMA, FP16 with FP32
+ * accumulation.  Any op, ld, offset, alignment, batch. */
+int hcbk_gemm_simt(const hcbk_gemm_args *args, hcbk_simt_cfg cfg, void *stream);
+
+/* C := beta * C (beta == 0 writes zeros without reading C): the alpha == 0
+ * path.  Any dtype, ld, offset, batch. */
+int hcbk_scale_c(const hcbk_gemm_args *args, void *stream);
+
+/* Number of SMs of the current device (cached per device). */
+int hcbk_sm_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HCBLAS_B200_HCBK_H_ */

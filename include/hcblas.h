@@ -1,0 +1,331 @@
+/*
+ * hcblas.h -- C ABI of hcblas-b200, a B200 (sm_100a) drop-in for the GEMM
+ * hot path of hcBLAS.
+ *
+ * Every entry point below keeps the name, parameter list, argument meaning
+ * and status codes of the hcBLAS C API it replaces (lib/include/hcblas.h of
+ * the reference; file:line given per function).  The functions are exported
+ * with C linkage (plain pointers and sizes), so the same symbols serve C++
+ * callers that include this header, C callers, and FFI bindings (ctypes,
+ * cffi, JNI, cgo) alike.  Entries marked "extension" have no counterpart in
+ * the reference's C API.
+ *
+ * Semantics.  hcblas{S,D,C,Z,H}gemm compute C := alpha*op(A)*op(B) + beta*C
+ * in column-major order (the reference's handle order, hcblaslib.h:82) with
+ * CBLAS numerics: HCBLAS_OP_C is a true conjugate transpose, beta == 0 means
+ * C is not read.  Status codes follow the reference exactly
+ * (lib/src/hcblas.cpp:1304-1327): NULL/destroyed handle -> NOT_INITIALIZED;
+ * m, n, k (or batchCount) < 0 -> INVALID_VALUE; m, n or k == 0, or a NULL
+ * matrix -> EXECUTION_FAILED (the class layer's HCBLAS_INVALID quick return,
+ * sgemm_array_wrapper.cpp:307-309); launch failure -> EXECUTION_FAILED.
+ * Calls are asynchronous on the handle's stream.
+ */
+#ifndef HCBLAS_B200_HCBLAS_H_
+#define HCBLAS_B200_HCBLAS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "hc_compat.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque library context (reference: lib/include/hcblas.h:46). */
+typedef struct Hcblaslibrary *hcblasHandle_t;
+
+/* Status and operation codes (reference: lib/include/hcblas.h:56-78).  The
+ * reference declares them as C++ enums with unsigned short storage; the C
+ * view uses the same storage type so both sides share one ABI. */
+#ifdef __cplusplus
+enum hcblasStatus_t : unsigned short {
+#else
+typedef unsigned short hcblasStatus_t;
+enum {
+#endif
+  HCBLAS_STATUS_SUCCESS = 0,
+  HCBLAS_STATUS_NOT_INITIALIZED = 1,
+  HCBLAS_STATUS_ALLOC_FAILED = 2,
+  HCBLAS_STATUS_INVALID_VALUE = 3,
+  HCBLAS_STATUS_MAPPING_ERROR = 4,
+  HCBLAS_STATUS_EXECUTION_FAILED = 5,
+  HCBLAS_STATUS_INTERNAL_ERROR = 6
+};
+
+#ifdef __cplusplus
+enum hcblasOperation_t : unsigned short {
+#else
+typedef unsigned short hcblasOperation_t;
+enum {
+#endif
+  HCBLAS_OP_N = 0,
+  HCBLAS_OP_T = 1,
+  HCBLAS_OP_C = 2
+};
+
+/* Complex scalars, interleaved {re, im} (reference: lib/include/hcblas.h:80-97). */
+typedef struct float_2_ {
+  float x;
+  float y;
+} float_2_;
+typedef struct double_2_ {
+  double x;
+  double y;
+} double_2_;
+typedef float_2_ hcFloatComplex;
+typedef hcFloatComplex hcComplex;
+typedef double_2_ hcDoubleComplex;
+
+#ifdef __cplusplus
+typedef hc::half hcblasHalf;
+#else
+typedef hcblas_half_t hcblasHalf;
+#endif
+
+/* ---------------------------------------------------------------- handle -- */
+
+/* Reference: hcblasCreate, lib/include/hcblas.h:112.  `av` selects the device
+ * and stream; NULL means the current device's default stream (extension: the
+ * reference requires a view).  Allocates the handle only: no device memory is
+ * touched until the first call that needs workspace. */
+hcblasStatus_t hcblasCreate(hcblasHandle_t *handle, hcblas_accl_view_t *av);
+
+/* Reference: hcblasDestroy, lib/include/hcblas.h:125. */
+hcblasStatus_t hcblasDestroy(hcblasHandle_t *handle);
+
+/* Reference: hcblasSetAcclView, lib/include/hcblas.h:140 (C++ callers pass an
+ * hc::accelerator_view& through the overload below).  A non-NULL `stream`
+ * (a cudaStream_t) overrides the view's own stream. */
+hcblasStatus_t hcblasSetAcclView(hcblasHandle_t handle, hcblas_accl_view_t *accl_view,
+                                 void *stream);
+
+/* Reference: hcblasGetAcclView, lib/include/hcblas.h:155. */
+hcblasStatus_t hcblasGetAcclView(hcblasHandle_t handle, hcblas_accl_view_t **accl_view,
+                                 void **stream);
+
+/* Extension: bind a raw cudaStream_t (cuBLAS-style). */
+hcblasStatus_t hcblasSetStream(hcblasHandle_t handle, void *stream);
+
+/* ------------------------------------------------------- host <-> device -- */
+
+/* Reference: lib/include/hcblas.h:174-233.  The reference copies
+ * rows*cols*elemSize contiguous bytes and ignores lda/ldb
+ * (lib/src/hcblas.cpp:260,309); its own tests pass lda = ldb = 1.  Here a
+ * leading dimension >= rows (incx/incy == 1 for vectors) is honoured as a
+ * strided copy, while a smaller one reproduces the reference's contiguous
+ * copy.  Copies are synchronous with respect to the host, like the
+ * reference's accelerator_view::copy. */
+hcblasStatus_t hcblasSetVector(hcblasHandle_t handle, int n, int elemSize, const void *x,
+                               int incx, void *y, int incy);
+hcblasStatus_t hcblasGetVector(hcblasHandle_t handle, int n, int elemSize, const void *x,
+                               int incx, void *y, int incy);
+hcblasStatus_t hcblasSetMatrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                               const void *A, int lda, void *B, int ldb);
+hcblasStatus_t hcblasGetMatrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                               const void *A, int lda, void *B, int ldb);
+
+/* ------------------------------------------------------------------ GEMM -- */
+
+/* Reference: lib/include/hcblas.h:662-665, lib/src/hcblas.cpp:1304-1327. */
+hcblasStatus_t hcblasSgemm(hcblasHandle_t handle, hcblasOperation_t transa,
+                           hcblasOperation_t transb, int m, int n, int k, const float *alpha,
+                           float *A, int lda, float *B, int ldb, const float *beta, float *C,
+                           int ldc);
+
+/* Reference: lib/include/hcblas.h:667-670, lib/src/hcblas.cpp:1363-1386. */
+hcblasStatus_t hcblasDgemm(hcblasHandle_t handle, hcblasOperation_t transa,
+                           hcblasOperation_t transb, int m, int n, int k, const double *alpha,
+                           double *A, int lda, double *B, int ldb, const double *beta,
+                           double *C, int ldc);
+
+/* Reference: lib/include/hcblas.h:672-676, lib/src/hcblas.cpp:1329-1361. */
+hcblasStatus_t hcblasCgemm(hcblasHandle_t handle, hcblasOperation_t transa,
+                           hcblasOperation_t transb, int m, int n, int k,
+                           const hcComplex *alpha, hcComplex *A, int lda, hcComplex *B,
+                           int ldb, const hcComplex *beta, hcComplex *C, int ldc);
+
+/* Reference: lib/include/hcblas.h:678-683, lib/src/hcblas.cpp:1388-1421. */
+hcblasStatus_t hcblasZgemm(hcblasHandle_t handle, hcblasOperation_t transa,
+                           hcblasOperation_t transb, int m, int n, int k,
+                           const hcDoubleComplex *alpha, hcDoubleComplex *A, int lda,
+                           hcDoubleComplex *B, int ldb, const hcDoubleComplex *beta,
+                           hcDoubleComplex *C, int ldc);
+
+/* Reference: lib/include/hcblas.h:685-689, lib/src/hcblas.cpp:1423-1450.
+ * FP16 storage; accumulation is FP32 (the reference accumulates in half). */
+hcblasStatus_t hcblasHgemm(hcblasHandle_t handle, hcblasOperation_t transa,
+                           hcblasOperation_t transb, int m, int n, int k,
+                           const hcblasHalf *alpha, hcblasHalf *A, int lda, hcblasHalf *B,
+                           int ldb, const hcblasHalf *beta, hcblasHalf *C, int ldc);
+
+/* Pointer-array batched GEMM: C[i] := alpha*op(A[i])*op(B[i]) + beta*C[i].
+ * Aarray/Barray/Carray are DEVICE-resident arrays of device pointers, as in
+ * the reference tests (test/unit-api/test-blas.cpp:1969-1971).
+ * Reference: lib/include/hcblas.h:762-790, lib/src/hcblas.cpp:1523-1675. */
+hcblasStatus_t hcblasSgemmBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                  hcblasOperation_t transb, int m, int n, int k,
+                                  const float *alpha, float *Aarray[], int lda, float *Barray[],
+                                  int ldb, const float *beta, float *Carray[], int ldc,
+                                  int batchCount);
+hcblasStatus_t hcblasCgemmBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                  hcblasOperation_t transb, int m, int n, int k,
+                                  const hcComplex *alpha, hcComplex *Aarray[], int lda,
+                                  hcComplex *Barray[], int ldb, const hcComplex *beta,
+                                  hcComplex *Carray[], int ldc, int batchCount);
+hcblasStatus_t hcblasDgemmBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                  hcblasOperation_t transb, int m, int n, int k,
+                                  const double *alpha, double *Aarray[], int lda,
+                                  double *Barray[], int ldb, const double *beta,
+                                  double *Carray[], int ldc, int batchCount);
+hcblasStatus_t hcblasZgemmBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                  hcblasOperation_t transb, int m, int n, int k,
+                                  const hcDoubleComplex *alpha, hcDoubleComplex *Aarray[],
+                                  int lda, hcDoubleComplex *Barray[], int ldb,
+                                  const hcDoubleComplex *beta, hcDoubleComplex *Carray[],
+                                  int ldc, int batchCount);
+
+/* Extension: HGEMM pointer-array batch (the reference compiles an HGEMM batch
+ * path but leaves it unreachable, hgemm_array_wrapper.cpp:315-370). */
+hcblasStatus_t hcblasHgemmBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                  hcblasOperation_t transb, int m, int n, int k,
+                                  const hcblasHalf *alpha, hcblasHalf *Aarray[], int lda,
+                                  hcblasHalf *Barray[], int ldb, const hcblasHalf *beta,
+                                  hcblasHalf *Carray[], int ldc, int batchCount);
+
+/* Extension: strided batched GEMM, X_i = X + i * strideX (elements).  The
+ * reference's closest form is its row-major batch kernel addressing
+ * `A_batchOffset * elt` (sgemm_array_kernels_rMajor_batch.cpp:67), which its
+ * wrapper never reaches (sgemm_array_wrapper.cpp:113-151). */
+hcblasStatus_t hcblasSgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                         hcblasOperation_t transb, int m, int n, int k,
+                                         const float *alpha, const float *A, int lda,
+                                         long long strideA, const float *B, int ldb,
+                                         long long strideB, const float *beta, float *C,
+                                         int ldc, long long strideC, int batchCount);
+hcblasStatus_t hcblasDgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                         hcblasOperation_t transb, int m, int n, int k,
+                                         const double *alpha, const double *A, int lda,
+                                         long long strideA, const double *B, int ldb,
+                                         long long strideB, const double *beta, double *C,
+                                         int ldc, long long strideC, int batchCount);
+hcblasStatus_t hcblasCgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                         hcblasOperation_t transb, int m, int n, int k,
+                                         const hcComplex *alpha, const hcComplex *A, int lda,
+                                         long long strideA, const hcComplex *B, int ldb,
+                                         long long strideB, const hcComplex *beta,
+                                         hcComplex *C, int ldc, long long strideC,
+                                         int batchCount);
+hcblasStatus_t hcblasZgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                         hcblasOperation_t transb, int m, int n, int k,
+                                         const hcDoubleComplex *alpha, const hcDoubleComplex *A,
+                                         int lda, long long strideA, const hcDoubleComplex *B,
+                                         int ldb, long long strideB,
+                                         const hcDoubleComplex *beta, hcDoubleComplex *C,
+                                         int ldc, long long strideC, int batchCount);
+hcblasStatus_t hcblasHgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_t transa,
+                                         hcblasOperation_t transb, int m, int n, int k,
+                                         const hcblasHalf *alpha, const hcblasHalf *A, int lda,
+                                         long long strideA, const hcblasHalf *B, int ldb,
+                                         long long strideB, const hcblasHalf *beta,
+                                         hcblasHalf *C, int ldc, long long strideC,
+                                         int batchCount);
+
+/* ------------------------------------------------ class-API C shims -- */
+
+/* C-ABI forms of the Hcblaslibrary::hcblas_Xgemm methods (include/hcblaslib.h;
+ * reference lib/include/hcblaslib.h:215-315) for FFI callers that cannot call
+ * C++ member functions.  Same arguments in the same order: `order` is
+ * RowMajor = 0 / ColMajor = 1, typeA/typeB are 'n', 't' or 'c', offsets are
+ * in elements; scalars are passed by pointer; the handle's current view (its
+ * stream) is used.  Return HCBLAS_SUCCEEDS (0) or HCBLAS_INVALID (-1) as the
+ * methods do.  Batched forms take device-resident pointer arrays; matrix i
+ * is X[i] + xOffset + i * X_batchOffset. */
+int hcblasLibSgemm(hcblasHandle_t h, int order, char typeA, char typeB, int M, int N, int K,
+                   const float *alpha, float *A, int64_t lda, float *B, int64_t ldb,
+                   const float *beta, float *C, int64_t ldc, int64_t aOffset, int64_t bOffset,
+                   int64_t cOffset);
+int hcblasLibDgemm(hcblasHandle_t h, int order, char typeA, char typeB, int M, int N, int K,
+                   const double *alpha, double *A, int64_t lda, double *B, int64_t ldb,
+                   const double *beta, double *C, int64_t ldc, int64_t aOffset, int64_t bOffset,
+                   int64_t cOffset);
+int hcblasLibHgemm(hcblasHandle_t h, int order, char typeA, char typeB, int M, int N, int K,
+                   const hcblasHalf *alpha, hcblasHalf *A, int64_t lda, hcblasHalf *B,
+                   int64_t ldb, const hcblasHalf *beta, hcblasHalf *C, int64_t ldc,
+                   int64_t aOffset, int64_t bOffset, int64_t cOffset);
+int hcblasLibCgemm(hcblasHandle_t h, int order, char typeA, char typeB, int M, int N, int K,
+                   const hcComplex *alpha, hcComplex *A, int64_t aOffset, int64_t lda,
+                   hcComplex *B, int64_t bOffset, int64_t ldb, const hcComplex *beta,
+                   hcComplex *C, int64_t cOffset, int64_t ldc);
+int hcblasLibZgemm(hcblasHandle_t h, int order, char typeA, char typeB, int M, int N, int K,
+                   const hcDoubleComplex *alpha, hcDoubleComplex *A, int64_t aOffset,
+                   int64_t lda, hcDoubleComplex *B, int64_t bOffset, int64_t ldb,
+                   const hcDoubleComplex *beta, hcDoubleComplex *C, int64_t cOffset,
+                   int64_t ldc);
+/* batched: (A[], lda, A_batchOffset, B[], ldb, B_batchOffset, beta, C[], ldc,
+ * C_batchOffset, aOffset, bOffset, cOffset, batchSize) as
+ * hcblaslib.h:244-266; dtype: 0 = S, 1 = D, 2 = C, 3 = Z, 4 = H. */
+int hcblasLibGemmBatched(hcblasHandle_t h, int dtype, int order, char typeA, char typeB, int M,
+                         int N, int K, const void *alpha, void **A, int64_t lda,
+                         int64_t A_batchOffset, void **B, int64_t ldb, int64_t B_batchOffset,
+                         const void *beta, void **C, int64_t ldc, int64_t C_batchOffset,
+                         int64_t aOffset, int64_t bOffset, int64_t cOffset, int batchSize);
+
+/* ----------------------------------------------------------- math modes -- */
+
+/* Extension: how the S/C and D/Z entry points compute.
+ *   HCBLAS_MATH_NATIVE     plain FP32 / FP64 arithmetic (default)
+ *   HCBLAS_MATH_SPLIT_BF16 S/C: FP32 operands split into bf16 hi/lo terms,
+ *                          products on tcgen05 tensor cores, FP32 accumulate
+ *                          (`param` = number of terms: 3, or 6 for a 3-way split)
+ *   HCBLAS_MATH_OZAKI_INT8 D/Z: Ozaki scheme, FP64 operands scaled per row/col
+ *                          and sliced into `param` INT8 slices, slice products
+ *                          exact in INT32 on tcgen05 tensor cores
+ *                          (`param` = 0 picks the slice count from the
+ *                          accuracy set by hcblasSetEmulationAccuracy). */
+enum {
+  HCBLAS_MATH_NATIVE = 0,
+  HCBLAS_MATH_SPLIT_BF16 = 1,
+  HCBLAS_MATH_OZAKI_INT8 = 2
+};
+hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param);
+hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
+
+/* Extension: the path the last GEMM call on this handle took (a short static
+ * string such as "simt.d.128x128" or "tc.f16.128x256"). */
+const char *hcblasGetLastPath(hcblasHandle_t handle);
+
+/* Extension: library version string. */
+const char *hcblasGetVersionString(void);
+
+/* Extension: diagnostics.
+ *   hcblasGetKernelLaunchCount: kernels this library has launched in this
+ *     process (all handles).
+ *   hcblasSetProfiling: on != 0 brackets every kernel the handle launches
+ *     with CUDA events on its stream; any value clears the records.
+ *   hcblasGetProfile: writes "name launches total_ms\n" lines (synchronising
+ *     on the recorded events) into buf; returns the full text length. */
+long long hcblasGetKernelLaunchCount(void);
+hcblasStatus_t hcblasSetProfiling(hcblasHandle_t handle, int on);
+int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap);
+
+#ifdef __cplusplus
+} /* extern "C" */
+
+/* C++ conveniences with the reference's exact parameter types.
+ * (hcblasCreate needs none: hc::accelerator_view* converts to
+ * hcblas_accl_view_t*.) */
+inline hcblasStatus_t hcblasSetAcclView(hcblasHandle_t handle, hc::accelerator_view &accl_view,
+                                        void *stream = nullptr) {
+  return hcblasSetAcclView(handle, static_cast<hcblas_accl_view_t *>(&accl_view), stream);
+}
+inline hcblasStatus_t hcblasGetAcclView(hcblasHandle_t handle,
+                                        hc::accelerator_view *(&accl_view), void **stream) {
+  hcblas_accl_view_t *v = nullptr;
+  hcblasStatus_t s = hcblasGetAcclView(handle, &v, stream);
+  accl_view = static_cast<hc::accelerator_view *>(v);
+  return s;
+}
+#endif
+
+#endif /* HCBLAS_B200_HCBLAS_H_ */
