@@ -52,6 +52,7 @@ EXPORTED = (
     "hcblasLibCgemm", "hcblasLibZgemm", "hcblasLibGemmBatched",
     "hcblasSetMathMode", "hcblasGetMathMode",
     "hcblasGetLastPath", "hcblasGetVersionString", "hcblasGetKernelLaunchCount",
+    "hcblasGetDeviceError", "hcblasSetTuningParam",
     "hcblasSetProfiling", "hcblasGetProfile", "hcblas_am_alloc", "hcblas_am_free",
     "hcblas_am_copy", "hcblas_view_wait", "hcblas_device_count", "hcblas_current_device",
 )
@@ -143,6 +144,10 @@ def lib():
         L.hcblasGetVersionString.restype = ctypes.c_char_p
         L.hcblasGetKernelLaunchCount.argtypes = []
         L.hcblasGetKernelLaunchCount.restype = ctypes.c_longlong
+        L.hcblasSetTuningParam.argtypes = [vp, ctypes.c_char_p, ci]
+        L.hcblasSetTuningParam.restype = st
+        L.hcblasGetDeviceError.argtypes = [vp]
+        L.hcblasGetDeviceError.restype = ci
         L.hcblasSetProfiling.argtypes = [vp, ci]
         L.hcblasSetProfiling.restype = st
         L.hcblasGetProfile.argtypes = [vp, ctypes.c_char_p, ci]
@@ -188,6 +193,15 @@ def hcblasSetMathMode(handle, mode, param=0):
 
 def hcblasGetLastPath(handle) -> str:
     return lib().hcblasGetLastPath(handle).decode()
+
+
+def set_tuning(handle, name: str, value: int):
+    return lib().hcblasSetTuningParam(handle, name.encode(), int(value))
+
+
+def device_error(handle) -> int:
+    """Sync the handle's stream; return and clear a tensor-core timeout code."""
+    return int(lib().hcblasGetDeviceError(handle))
 
 
 def kernel_launch_count() -> int:

@@ -3,30 +3,137 @@
  *
  * Replaces the reference's hand-written size-bucket dispatchers
  * (e.g. lib/src/blas/sgemm/sgemm_array_kernels.cpp:3291-3490, thresholds such
- * as `M % 128 == 0 && ... && M <= 6700`) with: math mode (native / emulated)
- * -> storage type -> alignment -> tile shape from the SM count and the
- * problem's tile count.
+ * as `M % 128 == 0 && ... && M <= 6700`) with:
+ *   math mode (native / emulated) -> storage type -> alignment -> tile shape
+ *   from the SM count and the problem's tile count.
+ * Tensor-core paths fall back to the SIMT kernels when an operand is not
+ * TMA-addressable (16-byte base and stride alignment).
  */
 #include "dispatch.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
 
 #include "../kernels/hcbk.h"
 
 namespace hcblas_b200 {
 
-int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+namespace {
+
+int64_t tiles_of(int64_t m, int64_t n, int64_t bm, int64_t bn) {
+  return ((m + bm - 1) / bm) * ((n + bn - 1) / bn);
+}
+
+bool aligned16(const void *p, int64_t off, int esz) {
+  return ((reinterpret_cast<uintptr_t>(p) + (uintptr_t)(off * esz)) & 15) == 0;
+}
+
+int simt(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
   const int sms = hcbk_sm_count();
-  /* large tiles when they fill the machine at least once; else small tiles */
-  int64_t big_tile = (a->dtype == HCBK_C || a->dtype == HCBK_Z) ? 64 : 128;
-  const int64_t tiles = ((a->m + big_tile - 1) / big_tile) * ((a->n + big_tile - 1) / big_tile) *
-                        a->batch;
+  const int64_t big = (a->dtype == HCBK_C || a->dtype == HCBK_Z) ? 64 : 128;
   hcbk_simt_cfg cfg;
-  cfg.variant = (tiles >= sms) ? 0 : 1;
+  cfg.variant = (tiles_of(a->m, a->n, big, big) * a->batch >= sms) ? 0 : 1;
   static const char *names[5][2] = {
-      {"simt.s.128x128", "simt.s.64x64"},   {"simt.d.128x128", "simt.d.64x64"},
-      {"simt.c.64x64", "simt.c.64x64"},     {"simt.z.64x64", "simt.z.64x64"},
+      {"simt.s.128x128", "simt.s.64x64"}, {"simt.d.128x128", "simt.d.64x64"},
+      {"simt.c.64x64", "simt.c.64x64"},   {"simt.z.64x64", "simt.z.64x64"},
       {"simt.h.128x128", "simt.h.64x64"}};
   *path = names[a->dtype][cfg.variant];
   return timed_launch(st, stream, *path, [&] { return hcbk_gemm_simt(a, cfg, stream); });
+}
+
+/* HGEMM on tcgen05 with operands read in place by TMA. */
+int hgemm_tc(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  if (!aligned16(a->a, a->a_off, 2) || !aligned16(a->b, a->b_off, 2) || (a->lda & 7) ||
+      (a->ldb & 7))
+    return HCBK_ERR_ALIGN;
+  int *err = device_error_flag(st);
+  if (!err) return HCBK_ERR_NOMEM;
+  const int bn = tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  *path = bn == 256 ? "tc.h.128x256" : "tc.h.128x128";
+  return timed_launch(st, stream, *path, [&] { return hcbk_hgemm_tc(a, bn, err, stream); });
+}
+
+/* Split-BF16 SGEMM: split both operands into bf16 planes (K-major), then one
+ * tensor-core GEMM over the 3 or 6 plane products. */
+int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *stream,
+                const char **path) {
+  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  const int nplanes = terms == 6 ? 3 : 2;
+  const int64_t kp = (a->k + 7) & ~int64_t(7); /* 16-byte row pitch */
+  const size_t a_plane = (size_t)a->m * kp * 2, b_plane = (size_t)a->n * kp * 2;
+  const size_t a_bytes = (a_plane + 1023) & ~size_t(1023);
+  const size_t b_bytes = (b_plane + 1023) & ~size_t(1023);
+  char *ws = static_cast<char *>(ensure_workspace(st, nplanes * (a_bytes + b_bytes)));
+  int *err = device_error_flag(st);
+  if (!ws || !err) return HCBK_ERR_NOMEM;
+
+  hcbk_pack_args pa;
+  pa.src = static_cast<const float *>(a->a) + a->a_off;
+  pa.ld = a->lda;
+  pa.k_contig = a->op_a != HCBK_OP_N; /* op(A) = A^T: element (m, k) at A[k + m*lda] */
+  pa.rows = a->m;
+  pa.kdim = a->k;
+  pa.nplanes = nplanes;
+  pa.ld_dst = kp;
+  for (int i = 0; i < 3; ++i) pa.planes[i] = i < nplanes ? ws + i * a_bytes : nullptr;
+  hcbk_pack_args pb;
+  pb.src = static_cast<const float *>(a->b) + a->b_off;
+  pb.ld = a->ldb;
+  pb.k_contig = a->op_b == HCBK_OP_N; /* op(B) = B: element (k, n) at B[k + n*ldb] */
+  pb.rows = a->n;
+  pb.kdim = a->k;
+  pb.nplanes = nplanes;
+  pb.ld_dst = kp;
+  char *bws = ws + nplanes * a_bytes;
+  for (int i = 0; i < 3; ++i) pb.planes[i] = i < nplanes ? bws + i * b_bytes : nullptr;
+
+  int rc = timed_launch(st, stream, "pack.split_bf16",
+                        [&] { return hcbk_pack_split_bf16(&pa, stream); });
+  if (rc) return rc;
+  rc = timed_launch(st, stream, "pack.split_bf16",
+                    [&] { return hcbk_pack_split_bf16(&pb, stream); });
+  if (rc) return rc;
+
+  hcbk_split_gemm g;
+  g.m = a->m;
+  g.n = a->n;
+  g.k = a->k;
+  g.terms = terms;
+  g.bn = 128;
+  g.promote_kb = st->split_promote_kb;
+  for (int i = 0; i < 3; ++i) {
+    g.a_planes[i] = pa.planes[i];
+    g.b_planes[i] = pb.planes[i];
+  }
+  g.ld_a = kp;
+  g.ld_b = kp;
+  g.c = static_cast<float *>(a->c) + a->c_off;
+  g.ldc = a->ldc;
+  g.alpha = a->alpha_re;
+  g.beta = a->beta_re;
+  if (terms == 6) *path = g.promote_kb == 4 ? "tc.split_bf16x6.128x128.p4" : "tc.split_bf16x6.128x128.p1";
+  else *path = g.promote_kb == 4 ? "tc.split_bf16x3.128x128.p4" : "tc.split_bf16x3.128x128.p1";
+  return timed_launch(st, stream, *path, [&] { return hcbk_sgemm_split_tc(&g, err, stream); });
+}
+
+}  // namespace
+
+int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+  if (a->dtype == HCBK_H && a->batch == 1 && !a->a_array) {
+    int rc = hgemm_tc(st, a, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] hgemm tensor-core path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_S && st->math_mode == 1 /* HCBLAS_MATH_SPLIT_BF16 */ && a->batch == 1 &&
+      !a->a_array) {
+    const int terms = st->math_param == 6 ? 6 : 3;
+    int rc = sgemm_split(st, a, terms, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] split-bf16 path declined (%d)\n", rc);
+  }
+  return simt(st, a, stream, path);
 }
 
 }  // namespace hcblas_b200

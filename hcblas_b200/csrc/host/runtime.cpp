@@ -63,6 +63,26 @@ void *ensure_workspace(HcblasB200State *st, size_t bytes) {
   return p;
 }
 
+int *device_error_flag(HcblasB200State *st) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (st->dev_err && st->dev_err_device == dev) return st->dev_err;
+  if (st->dev_err) {
+    DeviceGuard g(st->dev_err_device);
+    cudaFree(st->dev_err);
+    st->dev_err = nullptr;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  cudaMemset(p, 0, sizeof(int));
+  st->dev_err = static_cast<int *>(p);
+  st->dev_err_device = dev;
+  return st->dev_err;
+}
+
 static std::atomic<long long> g_launches{0};
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -174,6 +194,10 @@ Hcblaslibrary::~Hcblaslibrary() {
       cudaEventDestroy(static_cast<cudaEvent_t>(r.ev1));
     }
     for (void *e : impl->event_pool) cudaEventDestroy(static_cast<cudaEvent_t>(e));
+    if (impl->dev_err) {
+      DeviceGuard g(impl->dev_err_device);
+      cudaFree(impl->dev_err);
+    }
     delete impl;
     impl = nullptr;
   }
@@ -325,6 +349,19 @@ extern "C" hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, in
   return HCBLAS_STATUS_SUCCESS;
 }
 
+extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char *name,
+                                               int value) {
+  if (handle == nullptr || !handle->initialized || !handle->impl)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (name == nullptr) return HCBLAS_STATUS_INVALID_VALUE;
+  if (std::strcmp(name, "split_promote_kb") == 0) {
+    if (value != 1 && value != 4) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->split_promote_kb = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
+  return HCBLAS_STATUS_INVALID_VALUE;
+}
+
 extern "C" const char *hcblasGetLastPath(hcblasHandle_t handle) {
   if (handle == nullptr || !handle->impl) return "none";
   return handle->impl->last_path;
@@ -333,6 +370,21 @@ extern "C" const char *hcblasGetLastPath(hcblasHandle_t handle) {
 extern "C" const char *hcblasGetVersionString(void) { return "hcblas-b200 0.1.0 (sm_100a)"; }
 
 extern "C" long long hcblasGetKernelLaunchCount(void) { return hcblas_b200::launch_count(); }
+
+extern "C" int hcblasGetDeviceError(hcblasHandle_t handle) {
+  if (handle == nullptr || !handle->initialized || !handle->impl) return -1;
+  HcblasB200State *st = handle->impl;
+  if (!st->dev_err) return 0;
+  DeviceGuard g(st->dev_err_device);
+  int v = 0;
+  cudaStreamSynchronize(static_cast<cudaStream_t>(handle->currentAcclView.stream));
+  if (cudaMemcpy(&v, st->dev_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return -2;
+  }
+  if (v) cudaMemset(st->dev_err, 0, sizeof(int));
+  return v;
+}
 
 extern "C" hcblasStatus_t hcblasSetProfiling(hcblasHandle_t handle, int on) {
   if (handle == nullptr || !handle->initialized || !handle->impl)

@@ -22,11 +22,15 @@ struct HcblasProfRec {
 struct HcblasB200State {
   int math_mode = 0;   /* HCBLAS_MATH_* */
   int math_param = 0;  /* terms (split-BF16) or slices (Ozaki) */
+  int split_promote_kb = 1; /* split-BF16: K-slabs per TMEM chunk (tuning knob) */
   const char *last_path = "none";
   /* device workspace owned by the handle (grown on demand, freed at destroy) */
   void *workspace = nullptr;
   size_t workspace_bytes = 0;
   int workspace_device = -1;
+  /* device int that tensor-core kernels set when a pipeline wait times out */
+  int *dev_err = nullptr;
+  int dev_err_device = -1;
   /* per-kernel CUDA-event timing (hcblasSetProfiling) */
   bool profiling = false;
   std::vector<HcblasProfRec> prof;
@@ -78,6 +82,10 @@ class DeviceGuard {
 
 /* Grow the handle's workspace to at least `bytes` on the current device. */
 void *ensure_workspace(HcblasB200State *st, size_t bytes);
+
+/* The handle's device error flag on the current device (allocated and
+ * zeroed on first use); nullptr if it cannot be allocated. */
+int *device_error_flag(HcblasB200State *st);
 
 /* HCBLAS_LOG=1 prints one line per GEMM call with the path taken. */
 bool log_enabled();

@@ -76,6 +76,50 @@ int hcbk_scale_c(const hcbk_gemm_args *args, void *stream);
 /* Number of SMs of the current device (cached per device). */
 int hcbk_sm_count(void);
 
+/* ------------------------------------------------ tensor-core paths -- */
+
+/* HGEMM on tcgen05: f16 operands read by TMA directly from the caller's
+ * matrices (any N/T combination), f32 accumulation in TMEM, f16 C.
+ * Requirements (else HCBK_ERR_ALIGN / HCBK_ERR_ARGS and the caller falls
+ * back to hcbk_gemm_simt): batch == 1, base pointers (after offsets) 16-byte
+ * aligned, lda/ldb multiples of 8 elements.  `bn` = 128 or 256.
+ * `err` is a device int that receives a nonzero code if a pipeline wait
+ * times out (the kernel then exits instead of hanging). */
+int hcbk_hgemm_tc(const hcbk_gemm_args *args, int bn, int *err, void *stream);
+
+/* Split-BF16 SGEMM: operands already split into bf16 planes, K-major:
+ * a_planes[t] is M rows x ld_a elements (row m holds op(A)(m, 0..K-1)),
+ * b_planes[t] is N rows x ld_b elements (row n holds op(B)(0..K-1, n)).
+ * terms = 3 (planes hi, lo) or 6 (planes hi, mid, lo). */
+typedef struct hcbk_split_gemm {
+  int64_t m, n, k;
+  int terms;
+  int bn;         /* 128 */
+  int promote_kb; /* K-slabs (64 elements) per TMEM chunk: 1 or 4 */
+  const void *a_planes[3];
+  const void *b_planes[3];
+  int64_t ld_a, ld_b;
+  float *c;
+  int64_t ldc;
+  double alpha, beta;
+} hcbk_split_gemm;
+int hcbk_sgemm_split_tc(const hcbk_split_gemm *g, int *err, void *stream);
+
+/* Split an f32 operand into bf16 planes in K-major layout.
+ *   src element (r, k) = src[k + r*ld] if k_contig else src[r + k*ld]
+ *   planes[t][r*ld_dst + k], t < nplanes (2: hi/lo, 3: hi/mid/lo)
+ * r < rows, k < kdim. */
+typedef struct hcbk_pack_args {
+  const float *src;
+  int64_t ld;
+  int k_contig;
+  int64_t rows, kdim;
+  void *planes[3];
+  int nplanes;
+  int64_t ld_dst;
+} hcbk_pack_args;
+int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,119 @@
+/*
+ * pack.cu -- operand preparation for the emulated tensor-core paths.
+ *
+ * Split-BF16 (Henry, Tang & Heinecke, "Leveraging the bfloat16 artificial
+ * intelligence datatype for higher-precision computations", ARITH 2019):
+ * each f32 value x is written as an unevaluated sum of bf16 terms
+ *     hi  = rn_bf16(x)
+ *     mid = rn_bf16(x - hi)            (exact subtraction in f32)
+ *     lo  = rn_bf16(x - hi - mid)
+ * Two planes (hi, lo := mid) carry ~16 significant bits and feed the 3-product
+ * scheme hi*hi + hi*lo + lo*hi; three planes carry the full 24 bits and feed
+ * the 6-product scheme.  Non-finite hi keeps the special value in hi and
+ * zeroes the lower terms.
+ *
+ * The planes are written K-major ([rows][ld_dst], K contiguous) whatever the
+ * source layout, so the tensor-core kernel always reads 128-byte K rows; a
+ * source whose rows are contiguous along M/N is transposed through a 32x32
+ * shared-memory tile (coalesced on both sides).
+ */
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hcbk.h"
+
+namespace {
+
+__device__ __forceinline__ void split_terms(float x, __nv_bfloat16 (&t)[3]) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const float hf = __bfloat162float(h);
+  t[0] = h;
+  if (!isfinite(hf)) {
+    t[1] = __float2bfloat16_rn(0.f);
+    t[2] = t[1];
+    return;
+  }
+  const float r1 = x - hf;
+  const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+  t[1] = m;
+  t[2] = __float2bfloat16_rn(r1 - __bfloat162float(m));
+}
+
+/* source K-contiguous: element (r, k) at src[k + r*ld]; 4 k per thread */
+__global__ void pack_kcontig(hcbk_pack_args a) {
+  const int64_t kq = (a.kdim + 3) / 4;
+  const int64_t total = a.rows * kq;
+  const bool vec = ((reinterpret_cast<uintptr_t>(a.src) & 15) == 0) && ((a.ld & 3) == 0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / kq;
+    const int64_t k0 = (i % kq) * 4;
+    const float *s = a.src + r * a.ld + k0;
+    float v[4];
+    if (vec && k0 + 4 <= a.kdim) {
+      const float4 f = *reinterpret_cast<const float4 *>(s);
+      v[0] = f.x;
+      v[1] = f.y;
+      v[2] = f.z;
+      v[3] = f.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[e] = (k0 + e < a.kdim) ? s[e] : 0.f;
+    }
+    __nv_bfloat16 t[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split_terms(v[e], t[e]);
+    for (int p = 0; p < a.nplanes; ++p) {
+      __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(a.planes[p]) + r * a.ld_dst + k0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (k0 + e < a.kdim) d[e] = t[e][p];
+    }
+  }
+}
+
+/* source MN-contiguous: element (r, k) at src[r + k*ld]; 32x32 tiles */
+__global__ void pack_rcontig(hcbk_pack_args a) {
+  __shared__ float tile[32][33];
+  const int64_t r0 = (int64_t)blockIdx.x * 32;
+  const int64_t k0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int kl = ty + 8 * i;
+    const int64_t r = r0 + tx, k = k0 + kl;
+    tile[kl][tx] = (r < a.rows && k < a.kdim) ? a.src[r + k * a.ld] : 0.f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int rl = ty + 8 * i;
+    const int64_t r = r0 + rl, k = k0 + tx;
+    if (r < a.rows && k < a.kdim) {
+      __nv_bfloat16 t[3];
+      split_terms(tile[tx][rl], t);
+      for (int p = 0; p < a.nplanes; ++p)
+        static_cast<__nv_bfloat16 *>(a.planes[p])[r * a.ld_dst + k] = t[p];
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream) {
+  if (a->rows <= 0 || a->kdim <= 0 || a->nplanes < 1 || a->nplanes > 3) return HCBK_ERR_ARGS;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (a->k_contig) {
+    const int64_t total = a->rows * ((a->kdim + 3) / 4);
+    int64_t blocks = (total + 255) / 256;
+    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    pack_kcontig<<<(unsigned)blocks, 256, 0, st>>>(*a);
+  } else {
+    const int64_t gx = (a->rows + 31) / 32, gy = (a->kdim + 31) / 32;
+    if (gy > 65535) return HCBK_ERR_ARGS;
+    pack_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(*a);
+  }
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}

@@ -1,0 +1,228 @@
+/*
+ * tc_common.cuh -- sm_100a building blocks written directly in PTX:
+ * mbarriers with bounded waits, TMA tile loads (no cluster multicast),
+ * tcgen05 MMA / TMEM allocation / TMEM loads, and the shared-memory matrix
+ * and instruction descriptors of the 5th-generation tensor cores.
+ *
+ * Descriptor bit layouts follow the PTX ISA ("tcgen05 matrix descriptors",
+ * "instruction descriptor"): they were cross-checked against the field
+ * definitions in CUTLASS's cute/arch/mma_sm100_desc.hpp.
+ *
+ * Every wait on an mbarrier is bounded: after HCBK_WAIT_TIMEOUT_NS of
+ * %globaltimer time the wait records an error code in a device flag and
+ * returns false, and the kernel unwinds (frees TMEM, exits) instead of
+ * hanging the GPU.
+ */
+#ifndef HCBLAS_B200_TC_COMMON_CUH_
+#define HCBLAS_B200_TC_COMMON_CUH_
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#ifndef HCBK_WAIT_TIMEOUT_NS
+#define HCBK_WAIT_TIMEOUT_NS 2000000000ull /* 2 s */
+#endif
+
+namespace hcbk {
+namespace tc {
+
+/* error codes written to the device error flag */
+enum : int {
+  ERR_NONE = 0,
+  ERR_TIMEOUT_PRODUCER = 1,
+  ERR_TIMEOUT_MMA_FULL = 2,
+  ERR_TIMEOUT_MMA_TMEM = 3,
+  ERR_TIMEOUT_EPILOGUE = 4,
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+/* ------------------------------------------------------------ mbarrier -- */
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+/* Wait for the phase with the given parity to complete.  Bounded: returns
+ * false (after recording `code` in *err) on timeout, or when another thread
+ * has already recorded an error. */
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  uint32_t n = 0;
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((++n & 1023u) == 0) {
+      if (*reinterpret_cast<volatile int *>(err) != 0) return false;
+      if (globaltimer() - t0 > HCBK_WAIT_TIMEOUT_NS) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+    }
+  }
+}
+
+/* ---------------------------------------------------------------- TMA -- */
+
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+/* 2-D tiled bulk tensor load into this CTA's shared memory; completion is
+ * signalled on `bar` (complete_tx).  No multicast. */
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int32_t c0, int32_t c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
+
+/* ------------------------------------------------------------ tcgen05 -- */
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+/* D[tmem] (+)= A[smem] * B[smem]; kind::f16 covers f16 and bf16 operands
+ * with an f32 accumulator. */
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+/* D[tmem] (+)= A[smem] * B[smem]; 8-bit integer operands, s32 accumulator. */
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+/* Arrive on `bar` once all previously issued tcgen05.mma of this thread
+ * have completed. */
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+/* 32 lanes x 32 consecutive 32-bit columns: thread i of the warp receives
+ * lane (base + i), columns [col, col + 32). */
+__device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld_wait() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+/* ------------------------------------------------------- descriptors -- */
+
+/* Shared-memory matrix descriptor, SWIZZLE_128B (layout type 2), sm_100
+ * version bits (46-47 = 1).  Offsets in bytes.
+ *   K-major:  LBO unused (16), SBO = 1024 (8 rows x 128 B)
+ *   MN-major: LBO = byte distance between 64-element MN blocks,
+ *             SBO = 1024 (8 K-rows x 128 B) */
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(2) << 61;
+  return d;
+}
+
+/* Instruction descriptor (kind::f16 / kind::i8, dense).
+ *   c_fmt: 1 = f32, 2 = s32 accumulator;  ab_fmt: f16 = 0, bf16 = 1 (kind::f16),
+ *   u8 = 0, s8 = 1 (kind::i8);  a_mn/b_mn: operand is MN-major;
+ *   neg_a: negate A (f16 kinds only). */
+__host__ __device__ constexpr uint32_t make_idesc(uint32_t c_fmt, uint32_t ab_fmt, bool a_mn,
+                                                  bool b_mn, uint32_t M, uint32_t N,
+                                                  bool neg_a = false) {
+  return (c_fmt << 4) | (ab_fmt << 7) | (ab_fmt << 10) | ((neg_a ? 1u : 0u) << 13) |
+         ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) | ((N >> 3) << 17) |
+         ((M >> 4) << 24);
+}
+
+}  // namespace tc
+}  // namespace hcbk
+
+#endif /* HCBLAS_B200_TC_COMMON_CUH_ */

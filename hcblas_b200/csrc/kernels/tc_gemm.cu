@@ -1,0 +1,573 @@
+/*
+ * tc_gemm.cu -- persistent tensor-core GEMM for sm_100a (tcgen05 + TMA + TMEM).
+ *
+ * One kernel family serves every tensor-core path of the library:
+ *   HGEMM            f16 x f16 -> f32 accumulate in TMEM -> f16 C, operands
+ *                    read straight from the caller's matrices by TMA (K-major
+ *                    or MN-major: transposes live in the tensor maps and in
+ *                    the descriptors' major bits, not in copy kernels);
+ *   split-BF16 SGEMM f32 operands pre-split into bf16 planes (hi, lo[, lo2]);
+ *                    3 (or 6) products per K-step into one f32 accumulator;
+ *   (the "recipe" template describes which operand planes are multiplied
+ *    into which accumulator, so emulated schemes reuse the same pipeline).
+ *
+ * CTA organisation (192 threads, 1 CTA per SM, persistent over output tiles):
+ *   warp 0      TMA producer: one elected lane streams A/B K-slabs into a
+ *               STAGES-deep shared-memory ring (full/empty mbarriers)
+ *   warp 1      allocates TMEM; one lane issues tcgen05.mma for each K-slab
+ *               and commits the slab back to the producer; accumulators are
+ *               double-buffered in TMEM so the next tile's MMAs overlap the
+ *               previous tile's epilogue
+ *   warps 2..5  epilogue: tcgen05.ld (32 lanes x 32 columns per load) ->
+ *               alpha*acc + beta*C in registers -> column-major C; each warp
+ *               owns one 32-lane TMEM quadrant, so every store instruction
+ *               writes 32 consecutive rows of one column (coalesced)
+ * Tile: 128 x BN output, K-slab = 128 bytes of K per row (64 f16/bf16 or
+ * 128 int8 elements), SWIZZLE_128B shared-memory layout shared by TMA and the
+ * MMA descriptors.  No cluster multicast is used anywhere.
+ */
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "hcbk.h"
+#include "tc_common.cuh"
+
+namespace hcbk {
+namespace tc {
+
+constexpr int MAX_PLANES = 6;
+constexpr int BM = 128;
+constexpr int ROWB = 128; /* bytes of K per tile row (one swizzle atom) */
+
+struct TcParams {
+  CUtensorMap ta[MAX_PLANES];
+  CUtensorMap tb[MAX_PLANES];
+  int m, n, k;
+  int tiles_m, tiles_n;
+  int a_mn, b_mn; /* operand is MN-major in global memory */
+  void *c;
+  long long ldc;
+  float alpha, beta;
+  int beta_nonzero;
+  int *err;
+};
+
+/* ---------------------------------------------------------- recipes -- */
+
+/* one plane pair per product: A plane PA[i] x B plane PB[i] -> accumulator
+ * PACC[i]; FIRST[i] marks the first product written to its accumulator */
+struct RecipeSingle {
+  static constexpr int NA = 1, NB = 1, NP = 1, NACC = 1;
+  __host__ __device__ static constexpr int pa(int) { return 0; }
+  __host__ __device__ static constexpr int pb(int) { return 0; }
+  __host__ __device__ static constexpr int pacc(int) { return 0; }
+  __host__ __device__ static constexpr bool first(int i) { return i == 0; }
+};
+/* bf16x3: lo*hi + hi*lo into accumulator 1, hi*hi into accumulator 0
+ * (lo*lo dropped).  Keeping the correction terms (2^-8 smaller) apart from
+ * the leading term keeps them from being truncated against it. */
+struct RecipeBf16x3 {
+  static constexpr int NA = 2, NB = 2, NP = 3, NACC = 2;
+  __host__ __device__ static constexpr int pa(int i) { return i == 0 ? 1 : 0; }
+  __host__ __device__ static constexpr int pb(int i) { return i == 1 ? 1 : 0; }
+  __host__ __device__ static constexpr int pacc(int i) { return i == 2 ? 0 : 1; }
+  __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 2; }
+};
+/* bf16x6: three-way split, every product of total order <= 2; hi*hi into
+ * accumulator 0, the five correction products into accumulator 1 */
+struct RecipeBf16x6 {
+  static constexpr int NA = 3, NB = 3, NP = 6, NACC = 2;
+  __host__ __device__ static constexpr int pa(int i) {
+    return i == 0 ? 2 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 1 : 0;
+  }
+  __host__ __device__ static constexpr int pb(int i) {
+    return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 2 : i == 3 ? 0 : i == 4 ? 1 : 0;
+  }
+  __host__ __device__ static constexpr int pacc(int i) { return i == 5 ? 0 : 1; }
+  __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 5; }
+};
+
+/* ---------------------------------------------------------- epilogues -- */
+
+__device__ __forceinline__ void store_out(float *p, float v) { *p = v; }
+__device__ __forceinline__ void store_out(__half *p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ float load_out(const float *p) { return *p; }
+__device__ __forceinline__ float load_out(const __half *p) { return __half2float(*p); }
+
+/* f32 accumulator -> alpha*acc + beta*C in OutT (float or half) */
+template <typename OutT> struct EpiAlphaBeta {
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
+    const bool row_ok = m < p.m;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32) {
+      uint32_t r[32];
+      tmem_ld_32x32b_x32(tbase + c, r);
+      tmem_ld_wait();
+      if (row_ok) {
+        float v[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+        store32(p, v, m, n0 + c);
+      }
+    }
+  }
+
+  /* C[m, n0 .. n0+31] = alpha * v + beta * C: all C loads are issued before
+   * the first store, so they overlap instead of serialising behind stores
+   * that might alias them. */
+  static __device__ __forceinline__ void store32(const TcParams &p, const float (&v)[32], int m,
+                                                 int n0) {
+    OutT *C = static_cast<OutT *>(p.c) + (long long)m + (long long)n0 * p.ldc;
+    const int nvalid = p.n - n0;
+    float cv[32];
+    if (p.beta_nonzero) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        cv[j] = (j < nvalid) ? load_out(C + (long long)j * p.ldc) : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (j < nvalid) {
+        float o = p.alpha * v[j];
+        if (p.beta_nonzero) o = fmaf(p.beta, cv[j], o);
+        store_out(C + (long long)j * p.ldc, o);
+      }
+    }
+  }
+
+  /* acc[j] += sum over accumulators a (highest index first) of TMEM column
+   * a*BN + j of this thread's lane, with IEEE round-to-nearest adds: the
+   * promotion step of the chunked accumulation */
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void accumulate(uint32_t tbase, float (&acc)[BN]) {
+#pragma unroll
+    for (int c = 0; c < BN; c += 32) {
+      float part[32];
+#pragma unroll
+      for (int a = NACC - 1; a >= 0; --a) {
+        uint32_t r[32];
+        tmem_ld_32x32b_x32(tbase + a * BN + c, r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          part[j] = (a == NACC - 1) ? __uint_as_float(r[j]) : part[j] + __uint_as_float(r[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[c + j] += part[j];
+    }
+  }
+
+  template <int BN>
+  static __device__ __forceinline__ void store_acc(const TcParams &p, const float (&acc)[BN],
+                                                   int m, int n0) {
+    if (m >= p.m) return;
+#pragma unroll
+    for (int c = 0; c < BN; c += 32) {
+      if (n0 + c >= p.n) break;
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = acc[c + j];
+      store32(p, v, m, n0 + c);
+    }
+  }
+};
+
+/* ------------------------------------------------------------- kernel -- */
+
+template <int KIND> struct KindTraits;
+template <> struct KindTraits<0> { /* f16 */
+  static constexpr int BKE = 64, UK = 16, ESZ = 2;
+  static constexpr uint32_t CFMT = 1, ABFMT = 0;
+};
+template <> struct KindTraits<1> { /* bf16 */
+  static constexpr int BKE = 64, UK = 16, ESZ = 2;
+  static constexpr uint32_t CFMT = 1, ABFMT = 1;
+};
+
+__host__ __device__ constexpr uint32_t tmem_cols_for(uint32_t c) {
+  return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512;
+}
+
+template <int BN, int STAGES, class R, int KIND>
+struct TcCfg {
+  using KT = KindTraits<KIND>;
+  static constexpr uint32_t A_PLANE = BM * ROWB;
+  static constexpr uint32_t B_PLANE = BN * ROWB;
+  static constexpr uint32_t STAGE_BYTES = R::NA * A_PLANE + R::NB * B_PLANE;
+  static constexpr uint32_t ACC_COLS = R::NACC * BN;
+  static constexpr uint32_t TMEM_COLS = tmem_cols_for(2 * ACC_COLS);
+  static constexpr uint32_t BAR_BYTES = 256;
+  static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+  static_assert(2 * ACC_COLS <= 512, "accumulators exceed TMEM");
+  static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "BN");
+  static_assert(SMEM_BYTES <= 232448, "shared memory");
+};
+
+/*
+ * PROMOTE_KB = 0: each tile accumulates over all of K in TMEM (double-
+ *   buffered per tile) and the epilogue converts once.
+ * PROMOTE_KB = n > 0: the tile's K range is cut into chunks of n K-slabs;
+ *   every chunk starts a fresh TMEM accumulator (double-buffered per chunk)
+ *   and the epilogue warps add it into an f32 register accumulator with
+ *   IEEE round-to-nearest.  The tensor core's own f32 accumulation then
+ *   spans only n*128 bytes of K, which bounds the error it adds; used by the
+ *   split-BF16 paths, whose contract is "error no worse than FP32".
+ */
+template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0>
+__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
+  using Cfg = TcCfg<BN, STAGES, R, KIND>;
+  using KT = typename Cfg::KT;
+  constexpr int BKE = KT::BKE;
+  constexpr int KSTEPS = BKE / KT::UK;
+  static_assert(PROMOTE_KB > 0 || R::NACC == 1, "several accumulators need promotion");
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * Cfg::STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_fence_init();
+  }
+  if (warp == 0 && lane == 0) {
+    for (int i = 0; i < R::NA; ++i) tma_prefetch_desc(&p.ta[i]);
+    for (int i = 0; i < R::NB; ++i) tma_prefetch_desc(&p.tb[i]);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int num_tiles = p.tiles_m * p.tiles_n;
+  const int kblocks = (p.k + BKE - 1) / BKE;
+  const int chunk_kb = PROMOTE_KB > 0 ? PROMOTE_KB : kblocks;
+
+  if (warp == 0) {
+    /* ------------------------------------------------ TMA producer -- */
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
+        const int tm = t % p.tiles_m, tn = t / p.tiles_m;
+        for (int kb = 0; kb < kblocks; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
+          uint8_t *st = smem + s * Cfg::STAGE_BYTES;
+          const int k0 = kb * BKE;
+#pragma unroll
+          for (int a = 0; a < R::NA; ++a) {
+            uint8_t *dst = st + a * Cfg::A_PLANE;
+            if (!p.a_mn) {
+              tma_load_2d(dst, &p.ta[a], &full[s], k0, tm * BM);
+            } else {
+#pragma unroll
+              for (int j = 0; j < BM / 64; ++j)
+                tma_load_2d(dst + j * (BKE * ROWB), &p.ta[a], &full[s], tm * BM + j * 64, k0);
+            }
+          }
+#pragma unroll
+          for (int b = 0; b < R::NB; ++b) {
+            uint8_t *dst = st + R::NA * Cfg::A_PLANE + b * Cfg::B_PLANE;
+            if (!p.b_mn) {
+              tma_load_2d(dst, &p.tb[b], &full[s], k0, tn * BN);
+            } else {
+#pragma unroll
+              for (int j = 0; j < BN / 64; ++j)
+                tma_load_2d(dst + j * (BKE * ROWB), &p.tb[b], &full[s], tn * BN + j * 64, k0);
+            }
+          }
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    /* ------------------------------------------------ MMA issuer -- */
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc(KT::CFMT, KT::ABFMT, p.a_mn != 0, p.b_mn != 0, BM, BN);
+      const uint32_t a_lbo = p.a_mn ? BKE * ROWB : 16, b_lbo = p.b_mn ? BKE * ROWB : 16;
+      const uint32_t a_kstep = p.a_mn ? KT::UK * ROWB : KT::UK * KT::ESZ;
+      const uint32_t b_kstep = p.b_mn ? KT::UK * ROWB : KT::UK * KT::ESZ;
+      int s = 0;
+      uint32_t ph = 0;
+      int ci = 0; /* chunk counter (all tiles): selects the TMEM buffer */
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
+        for (int kc = 0; ok && kc < kblocks; kc += chunk_kb, ++ci) {
+          const int b = ci & 1;
+          const uint32_t tph = (ci >> 1) & 1;
+          if (!mbar_wait(&tempty[b], tph ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dbase = tmem_base + b * Cfg::ACC_COLS;
+          const int kend = (kc + chunk_kb < kblocks) ? kc + chunk_kb : kblocks;
+          for (int kb = kc; kb < kend; ++kb) {
+            if (!mbar_wait(&full[s], ph, p.err, ERR_TIMEOUT_MMA_FULL)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sbase = smem_u32(smem + s * Cfg::STAGE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < KSTEPS; ++kk) {
+#pragma unroll
+              for (int pi = 0; pi < R::NP; ++pi) {
+                const uint32_t aa = sbase + R::pa(pi) * Cfg::A_PLANE + kk * a_kstep;
+                const uint32_t ba =
+                    sbase + R::NA * Cfg::A_PLANE + R::pb(pi) * Cfg::B_PLANE + kk * b_kstep;
+                const uint64_t ad = sw128_desc(aa, a_lbo, 1024);
+                const uint64_t bd = sw128_desc(ba, b_lbo, 1024);
+                const uint32_t acc = (kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
+                mma_f16(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
+              }
+            }
+            mma_commit(&empty[s]);
+            if (++s == STAGES) {
+              s = 0;
+              ph ^= 1u;
+            }
+          }
+          if (ok) mma_commit(&tfull[b]);
+        }
+      }
+    }
+  } else {
+    /* ------------------------------------------------ epilogue -- */
+    const int q = warp & 3; /* TMEM lane quadrant of this warp */
+    int ci = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
+      const int tm = t % p.tiles_m, tn = t / p.tiles_m;
+      const int m = tm * BM + q * 32 + lane;
+      if constexpr (PROMOTE_KB == 0) {
+        const int b = ci & 1;
+        const uint32_t tph = (ci >> 1) & 1;
+        ++ci;
+        if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) break;
+        tc_fence_after();
+        const uint32_t tbase =
+            tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS;
+        EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[b]);
+      } else {
+        float acc[BN];
+#pragma unroll
+        for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+        for (int kc = 0; kc < kblocks; kc += chunk_kb, ++ci) {
+          const int b = ci & 1;
+          const uint32_t tph = (ci >> 1) & 1;
+          if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          EPI::template accumulate<BN, R::NACC>(
+              tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS, acc);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[b]);
+        }
+        if (ok) EPI::template store_acc<BN>(p, acc, m, tn * BN);
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+  }
+}
+
+/* ------------------------------------------------------------- host -- */
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q);
+    if (e == cudaSuccess && q == cudaDriverEntryPointSuccess && ptr) {
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    } else {
+      cudaGetLastError();
+      const char *env = getenv("HCBLAS_LOG");
+      if (env && env[0] == '1')
+        fprintf(stderr, "[hcblas] cuTensorMapEncodeTiled entry point unavailable (%d, %d)\n",
+                (int)e, (int)q);
+    }
+  }
+  return fn;
+}
+
+/* Tensor map over a 2-D operand with `inner` contiguous elements per line,
+ * `outer` lines `ld` elements apart; box = {box_inner, box_outer}, 128-byte
+ * swizzle, zero fill out of bounds. */
+static int make_map(CUtensorMap *map, CUtensorMapDataType dt, int esz, const void *base,
+                    uint64_t inner, uint64_t outer, uint64_t ld, uint32_t box_inner,
+                    uint32_t box_outer) {
+  auto fn = encode_fn();
+  if (!fn) return HCBK_ERR_DRIVER;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * esz) & 15)) return HCBK_ERR_ALIGN;
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {ld * esz};
+  cuuint32_t box[2] = {box_inner, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, dt, 2, const_cast<void *>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    const char *e = getenv("HCBLAS_LOG");
+    if (e && e[0] == '1')
+      fprintf(stderr,
+              "[hcblas] cuTensorMapEncodeTiled failed (%d): base=%p dims={%llu,%llu} "
+              "stride=%llu box={%u,%u}\n",
+              (int)r, base, (unsigned long long)inner, (unsigned long long)outer,
+              (unsigned long long)(ld * esz), box_inner, box_outer);
+    return HCBK_ERR_ALIGN;
+  }
+  return HCBK_OK;
+}
+
+template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0>
+static int launch_tc(TcParams &p, void *stream) {
+  using Cfg = TcCfg<BN, STAGES, R, KIND>;
+  auto kern = tc_gemm_kernel<BN, STAGES, R, KIND, EPI, PROMOTE_KB>;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Cfg::SMEM_BYTES) != cudaSuccess)
+      return HCBK_ERR_LAUNCH;
+    attr_set[dev] = true;
+  }
+  p.tiles_m = (p.m + BM - 1) / BM;
+  p.tiles_n = (p.n + BN - 1) / BN;
+  const int tiles = p.tiles_m * p.tiles_n;
+  int grid = hcbk_sm_count();
+  if (tiles < grid) grid = tiles;
+  kern<<<grid, 192, Cfg::SMEM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+}  // namespace tc
+}  // namespace hcbk
+
+using namespace hcbk::tc;
+
+/* f16 operands straight from the caller's matrices (column-major canonical). */
+extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int *err, void *stream) {
+  if (a->dtype != HCBK_H || a->batch != 1 || a->a_array || a->op_a == HCBK_OP_C ||
+      a->op_b == HCBK_OP_C)
+    return HCBK_ERR_ARGS;
+  if (a->m > 0x7fffffff || a->n > 0x7fffffff || a->k > 0x7fffffff) return HCBK_ERR_ARGS;
+  TcParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = (int)a->m;
+  p.n = (int)a->n;
+  p.k = (int)a->k;
+  const __half *A = static_cast<const __half *>(a->a) + a->a_off;
+  const __half *B = static_cast<const __half *>(a->b) + a->b_off;
+  /* op(A) = A: column-major M x K, M contiguous (MN-major);  op(A) = A^T: K contiguous */
+  p.a_mn = (a->op_a == HCBK_OP_N);
+  /* op(B) = B: K x N, K contiguous (K-major);  op(B) = B^T: N contiguous */
+  p.b_mn = (a->op_b != HCBK_OP_N);
+  const auto F16 = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  int rc;
+  if (p.a_mn)
+    rc = make_map(&p.ta[0], F16, 2, A, a->m, a->k, a->lda, 64, 64);
+  else
+    rc = make_map(&p.ta[0], F16, 2, A, a->k, a->m, a->lda, 64, BM);
+  if (rc) return rc;
+  const uint32_t bn_box = (uint32_t)bn;
+  if (p.b_mn)
+    rc = make_map(&p.tb[0], F16, 2, B, a->n, a->k, a->ldb, 64, 64);
+  else
+    rc = make_map(&p.tb[0], F16, 2, B, a->k, a->n, a->ldb, 64, bn_box);
+  if (rc) return rc;
+  p.c = static_cast<__half *>(a->c) + a->c_off;
+  p.ldc = a->ldc;
+  p.alpha = (float)a->alpha_re;
+  p.beta = (float)a->beta_re;
+  p.beta_nonzero = a->beta_re != 0.0;
+  p.err = err;
+  if (bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EpiAlphaBeta<__half>>(p, stream);
+  if (bn == 128) return launch_tc<128, 6, RecipeSingle, 0, EpiAlphaBeta<__half>>(p, stream);
+  return HCBK_ERR_ARGS;
+}
+
+/* split-BF16 SGEMM on pre-split K-major planes:
+ *   A planes: [M][lda_p] bf16 (K contiguous), B planes: [N][ldb_p] bf16. */
+extern "C" int hcbk_sgemm_split_tc(const hcbk_split_gemm *g, int *err, void *stream) {
+  TcParams p;
+  memset(&p, 0, sizeof(p));
+  if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > 0x7fffffff) return HCBK_ERR_ARGS;
+  p.m = (int)g->m;
+  p.n = (int)g->n;
+  p.k = (int)g->k;
+  p.a_mn = 0;
+  p.b_mn = 0;
+  const auto BF16 = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  const int planes = g->terms == 6 ? 3 : 2;
+  const uint32_t bn = (uint32_t)g->bn;
+  for (int i = 0; i < planes; ++i) {
+    int rc = make_map(&p.ta[i], BF16, 2, g->a_planes[i], g->k, g->m, g->ld_a, 64, BM);
+    if (rc) return rc;
+    rc = make_map(&p.tb[i], BF16, 2, g->b_planes[i], g->k, g->n, g->ld_b, 64, bn);
+    if (rc) return rc;
+  }
+  p.c = g->c;
+  p.ldc = g->ldc;
+  p.alpha = (float)g->alpha;
+  p.beta = (float)g->beta;
+  p.beta_nonzero = g->beta != 0.0;
+  p.err = err;
+  /* two accumulators per chunk, double-buffered: 2 x 2 x 128 TMEM columns */
+  if (g->bn != 128) return HCBK_ERR_ARGS;
+  using EF = EpiAlphaBeta<float>;
+  if (g->terms == 6) {
+    if (g->promote_kb == 4) return launch_tc<128, 2, RecipeBf16x6, 1, EF, 4>(p, stream);
+    return launch_tc<128, 2, RecipeBf16x6, 1, EF, 1>(p, stream);
+  }
+  if (g->promote_kb == 4) return launch_tc<128, 3, RecipeBf16x3, 1, EF, 4>(p, stream);
+  return launch_tc<128, 3, RecipeBf16x3, 1, EF, 1>(p, stream);
+}

@@ -291,6 +291,12 @@ enum {
 hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param);
 hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
 
+/* Extension: set a named tuning knob on the handle.
+ *   "split_promote_kb"  split-BF16 paths: 64-element K-slabs accumulated in
+ *                       TMEM before each promotion to the IEEE f32
+ *                       accumulator (1 or 4; default 1). */
+hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char *name, int value);
+
 /* Extension: the path the last GEMM call on this handle took (a short static
  * string such as "simt.d.128x128" or "tc.f16.128x256"). */
 const char *hcblasGetLastPath(hcblasHandle_t handle);
@@ -306,6 +312,10 @@ const char *hcblasGetVersionString(void);
  *   hcblasGetProfile: writes "name launches total_ms\n" lines (synchronising
  *     on the recorded events) into buf; returns the full text length. */
 long long hcblasGetKernelLaunchCount(void);
+/* Extension: waits for the handle's stream, then returns and clears the
+ * device error code set by a tensor-core kernel whose pipeline wait timed out
+ * (0 = none; such a kernel exits early and leaves C incomplete). */
+int hcblasGetDeviceError(hcblasHandle_t handle);
 hcblasStatus_t hcblasSetProfiling(hcblasHandle_t handle, int on);
 int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap);
 

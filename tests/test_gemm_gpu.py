@@ -62,12 +62,14 @@ def rand_op(rng, kind, n):
     return v.astype(NP[kind])
 
 
-def make_case(rng, kind, order, ta, tb, M, N, K, pad=0, offs=(0, 0, 0)):
+def make_case(rng, kind, order, ta, tb, M, N, K, pad=0, offs=(0, 0, 0), ld_align=1):
+    """Random operands for one GEMM; ld = rows (+pad), rounded up to ld_align."""
     ar, ac = (M, K) if ta == 0 else (K, M)
     br, bc = (K, N) if tb == 0 else (N, K)
-    lda = (ar if order == O.COL else ac) + pad
-    ldb = (br if order == O.COL else bc) + pad
-    ldc = (M if order == O.COL else N) + pad
+    up = lambda v: -(-v // ld_align) * ld_align
+    lda = up((ar if order == O.COL else ac) + pad)
+    ldb = up((br if order == O.COL else bc) + pad)
+    ldc = up((M if order == O.COL else N) + pad)
     na = offs[0] + lda * (ac if order == O.COL else ar)
     nb = offs[1] + ldb * (bc if order == O.COL else br)
     nc = offs[2] + ldc * (N if order == O.COL else M)
