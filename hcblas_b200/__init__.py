@@ -20,7 +20,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libhcblas.so")
+LIB_PATH = os.environ.get("HCBLAS_B200_LIB") or os.path.join(_HERE, "libhcblas.so")
 
 # hcblasStatus_t (lib/include/hcblas.h:56-64 of the reference)
 HCBLAS_STATUS_SUCCESS = 0

@@ -118,6 +118,84 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   return timed_launch(st, stream, *path, [&] { return hcbk_sgemm_split_tc(&g, err, stream); });
 }
 
+/* Ozaki-scheme DGEMM on INT8 tensor cores: per-row / per-column exponents,
+ * `s` int8 slices per operand, slice products exact in INT32, FP64 epilogue.
+ * K is split so that every INT32 group sum stays exact. */
+int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, void *stream,
+                const char **path) {
+  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  if (s < 3 || s > 8) return HCBK_ERR_ARGS;
+  const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch */
+  auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
+  const size_t a_pl = up1k((size_t)a->m * kp), b_pl = up1k((size_t)a->n * kp);
+  const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
+  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl);
+  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  int *err = device_error_flag(st);
+  if (!ws || !err) return HCBK_ERR_NOMEM;
+  int *exp_a = reinterpret_cast<int *>(ws);
+  int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
+  char *pa_base = ws + ea_bytes + eb_bytes;
+  char *pb_base = pa_base + s * a_pl;
+
+  hcbk_ozaki_prep pa;
+  pa.src = static_cast<const double *>(a->a) + a->a_off;
+  pa.ld = a->lda;
+  pa.k_contig = a->op_a != HCBK_OP_N;
+  pa.rows = a->m;
+  pa.kdim = a->k;
+  pa.exps = exp_a;
+  pa.slices = s;
+  pa.planes = pa_base;
+  pa.plane_stride = (int64_t)a_pl;
+  pa.ld_dst = kp;
+  hcbk_ozaki_prep pb;
+  pb.src = static_cast<const double *>(a->b) + a->b_off;
+  pb.ld = a->ldb;
+  pb.k_contig = a->op_b == HCBK_OP_N;
+  pb.rows = a->n;
+  pb.kdim = a->k;
+  pb.exps = exp_b;
+  pb.slices = s;
+  pb.planes = pb_base;
+  pb.plane_stride = (int64_t)b_pl;
+  pb.ld_dst = kp;
+
+  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pa, stream); });
+  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pb, stream); });
+  if (!rc) rc = timed_launch(st, stream, "ozaki.slice", [&] { return hcbk_ozaki_slice(&pa, stream); });
+  if (!rc) rc = timed_launch(st, stream, "ozaki.slice", [&] { return hcbk_ozaki_slice(&pb, stream); });
+  if (rc) return rc;
+
+  static const char *names[9] = {"", "", "", "tc.ozaki_s3", "tc.ozaki_s4", "tc.ozaki_s5",
+                                  "tc.ozaki_s6", "tc.ozaki_s7", "tc.ozaki_s8"};
+  *path = names[s];
+  const int64_t kmax = hcbk_ozaki_max_k(s);
+  hcbk_ozaki_gemm g;
+  g.m = a->m;
+  g.n = a->n;
+  g.slices = s;
+  g.a_planes = pa_base;
+  g.b_planes = pb_base;
+  g.ld_a = kp;
+  g.ld_b = kp;
+  g.a_plane_stride = (int64_t)a_pl;
+  g.b_plane_stride = (int64_t)b_pl;
+  g.exp_a = exp_a;
+  g.exp_b = exp_b;
+  g.c = static_cast<double *>(a->c) + a->c_off;
+  g.ldc = a->ldc;
+  g.alpha = a->alpha_re;
+  for (int64_t k0 = 0; k0 < a->k; k0 += kmax) {
+    g.k0 = k0;
+    g.k = (a->k - k0 < kmax) ? a->k - k0 : kmax;
+    g.beta = (k0 == 0) ? a->beta_re : 1.0;
+    rc = timed_launch(st, stream, *path, [&] { return hcbk_ozaki_gemm_tc(&g, err, stream); });
+    if (rc) return rc;
+  }
+  return HCBK_OK;
+}
+
 }  // namespace
 
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
@@ -132,6 +210,13 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     int rc = sgemm_split(st, a, terms, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] split-bf16 path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_D && st->math_mode == 2 /* HCBLAS_MATH_OZAKI_INT8 */ && a->batch == 1 &&
+      !a->a_array) {
+    const int s = st->math_param > 0 ? st->math_param : st->ozaki_default_slices;
+    int rc = dgemm_ozaki(st, a, s, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] ozaki path declined (%d)\n", rc);
   }
   return simt(st, a, stream, path);
 }

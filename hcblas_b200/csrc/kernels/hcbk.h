@@ -120,6 +120,53 @@ typedef struct hcbk_pack_args {
 } hcbk_pack_args;
 int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream);
 
+/* ------------------------------------------------------- Ozaki DGEMM -- */
+
+/* exponent markers of the Ozaki scaling */
+#define HCBK_OZ_ZERO (-2000000)     /* all-zero row / column */
+#define HCBK_OZ_NONFINITE 2000000   /* row / column holds Inf or NaN */
+
+/* One operand of the Ozaki scheme, viewed as `rows` x `kdim`:
+ *   element (r, k) = src[k + r*ld] if k_contig else src[r + k*ld].
+ * hcbk_ozaki_exponents writes exps[r] (frexp exponent of max_k |x(r,k)|);
+ * hcbk_ozaki_slice then writes `slices` int8 planes, plane i at
+ * planes + i*plane_stride, element (r, k) at [r*ld_dst + k]. */
+typedef struct hcbk_ozaki_prep {
+  const double *src;
+  int64_t ld;
+  int k_contig;
+  int64_t rows, kdim;
+  int *exps;
+  int slices;
+  void *planes;
+  int64_t plane_stride; /* bytes between planes */
+  int64_t ld_dst;       /* bytes (= int8 elements) between rows */
+} hcbk_ozaki_prep;
+int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
+int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream);
+
+/* The slice-product GEMM and FP64 epilogue over K range [k0, k0 + k):
+ *   C := alpha * 2^(ea_m + eb_n) * sum_{i+j<s} 2^(-7(i+j+2)) a_i . b_j + beta * C
+ * a_planes: M rows, b_planes: N rows, both K-major int8 with row pitch ld
+ * (bytes) and plane pitch plane_stride; C column-major FP64.  k must keep the
+ * INT32 group sums exact: s * k * 127^2 < 2^31. */
+typedef struct hcbk_ozaki_gemm {
+  int64_t m, n, k, k0;
+  int slices;
+  const void *a_planes;
+  const void *b_planes;
+  int64_t ld_a, ld_b;
+  int64_t a_plane_stride, b_plane_stride;
+  const int *exp_a;
+  const int *exp_b;
+  double *c;
+  int64_t ldc;
+  double alpha, beta;
+} hcbk_ozaki_gemm;
+int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream);
+/* largest K per launch for s slices (INT32 exactness), multiple of 64 */
+int64_t hcbk_ozaki_max_k(int slices);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,6 +115,16 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+/* 3-D tiled bulk tensor load (coordinates innermost first).  No multicast. */
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int32_t c0, int32_t c1, int32_t c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
 /* ------------------------------------------------------------ tcgen05 -- */
 
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
@@ -195,19 +205,27 @@ __device__ __forceinline__ void tmem_ld_wait() {
 
 /* ------------------------------------------------------- descriptors -- */
 
-/* Shared-memory matrix descriptor, SWIZZLE_128B (layout type 2), sm_100
- * version bits (46-47 = 1).  Offsets in bytes.
- *   K-major:  LBO unused (16), SBO = 1024 (8 rows x 128 B)
- *   MN-major: LBO = byte distance between 64-element MN blocks,
+/* Shared-memory matrix descriptor with sm_100 version bits (46-47 = 1) and a
+ * swizzle layout (bits 61-63: 2 = 128B, 4 = 64B).  Offsets in bytes.
+ *   K-major:  LBO unused (16), SBO = 8 rows x row bytes (1024 for 128B,
+ *             512 for 64B swizzle)
+ *   MN-major (128B): LBO = byte distance between 64-element MN blocks,
  *             SBO = 1024 (8 K-rows x 128 B) */
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                              uint32_t layout) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
   d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
   d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
   d |= static_cast<uint64_t>(1) << 46;
-  d |= static_cast<uint64_t>(2) << 61;
+  d |= static_cast<uint64_t>(layout & 7u) << 61;
   return d;
+}
+
+/* SWIZZLE_128B (layout 2) form used by the 16-bit paths.  (The int8 path
+ * uses SWIZZLE_64B, layout 4: K-major rows of 64 bytes, SBO = 512.) */
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return smem_desc(saddr, lbo, sbo, 2);
 }
 
 /* Instruction descriptor (kind::f16 / kind::i8, dense).

@@ -42,14 +42,14 @@
 namespace hcbk {
 namespace tc {
 
-constexpr int MAX_PLANES = 6;
+constexpr int MAX_PLANES = 3;
 constexpr int BM = 128;
-constexpr int ROWB = 128; /* bytes of K per tile row (one swizzle atom) */
 
 struct TcParams {
   CUtensorMap ta[MAX_PLANES];
   CUtensorMap tb[MAX_PLANES];
   int m, n, k;
+  int k0; /* first K coordinate (K split across launches) */
   int tiles_m, tiles_n;
   int a_mn, b_mn; /* operand is MN-major in global memory */
   void *c;
@@ -57,6 +57,10 @@ struct TcParams {
   float alpha, beta;
   int beta_nonzero;
   int *err;
+  /* Ozaki epilogue */
+  double alpha_d, beta_d;
+  const int *exp_a;
+  const int *exp_b;
 };
 
 /* ---------------------------------------------------------- recipes -- */
@@ -65,6 +69,7 @@ struct TcParams {
  * PACC[i]; FIRST[i] marks the first product written to its accumulator */
 struct RecipeSingle {
   static constexpr int NA = 1, NB = 1, NP = 1, NACC = 1;
+  static constexpr bool P3D = false; /* planes are separate 2-D tensor maps */
   __host__ __device__ static constexpr int pa(int) { return 0; }
   __host__ __device__ static constexpr int pb(int) { return 0; }
   __host__ __device__ static constexpr int pacc(int) { return 0; }
@@ -75,6 +80,7 @@ struct RecipeSingle {
  * the leading term keeps them from being truncated against it. */
 struct RecipeBf16x3 {
   static constexpr int NA = 2, NB = 2, NP = 3, NACC = 2;
+  static constexpr bool P3D = false;
   __host__ __device__ static constexpr int pa(int i) { return i == 0 ? 1 : 0; }
   __host__ __device__ static constexpr int pb(int i) { return i == 1 ? 1 : 0; }
   __host__ __device__ static constexpr int pacc(int i) { return i == 2 ? 0 : 1; }
@@ -84,6 +90,7 @@ struct RecipeBf16x3 {
  * accumulator 0, the five correction products into accumulator 1 */
 struct RecipeBf16x6 {
   static constexpr int NA = 3, NB = 3, NP = 6, NACC = 2;
+  static constexpr bool P3D = false;
   __host__ __device__ static constexpr int pa(int i) {
     return i == 0 ? 2 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 1 : 0;
   }
@@ -92,6 +99,33 @@ struct RecipeBf16x6 {
   }
   __host__ __device__ static constexpr int pacc(int i) { return i == 5 ? 0 : 1; }
   __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 5; }
+};
+/* Ozaki, S int8 slices per operand: every pair (i, j) with i + j < S,
+ * enumerated by weight d = i + j, accumulated exactly into INT32
+ * accumulator d.  All planes of an operand share one 3-D tensor map
+ * {K, rows, plane}. */
+template <int S> struct RecipeOzaki {
+  static constexpr int NA = S, NB = S, NP = S * (S + 1) / 2, NACC = S;
+  static constexpr bool P3D = true;
+  __host__ __device__ static constexpr int pd(int pi) {
+    int d = 0;
+    while (pi > d) {
+      pi -= d + 1;
+      ++d;
+    }
+    return d;
+  }
+  __host__ __device__ static constexpr int pa(int pi) {
+    int d = 0;
+    while (pi > d) {
+      pi -= d + 1;
+      ++d;
+    }
+    return pi;
+  }
+  __host__ __device__ static constexpr int pb(int pi) { return pd(pi) - pa(pi); }
+  __host__ __device__ static constexpr int pacc(int pi) { return pd(pi); }
+  __host__ __device__ static constexpr bool first(int pi) { return pa(pi) == 0; }
 };
 
 /* ---------------------------------------------------------- epilogues -- */
@@ -105,6 +139,7 @@ __device__ __forceinline__ float load_out(const __half *p) { return __half2float
 template <typename OutT> struct EpiAlphaBeta {
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
+    static_assert(NACC == 1, "several accumulators need the promoting epilogue");
     const bool row_ok = m < p.m;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
@@ -180,33 +215,110 @@ template <typename OutT> struct EpiAlphaBeta {
   }
 };
 
+/* Ozaki epilogue: NACC exact INT32 group sums acc_d (d = i + j) ->
+ *   C = alpha * 2^(ea_m + eb_n) * sum_d 2^(-7(d+2)) acc_d + beta * C   (FP64)
+ * The group terms are exact in binary64 (|acc_d| < 2^31, power-of-two
+ * weights) and are added smallest weight first. */
+__host__ __device__ constexpr double pow2(int e) {
+  /* exact 2^e for -1022 <= e <= 1023 */
+  return e >= 0 ? (e == 0 ? 1.0 : 2.0 * pow2(e - 1)) : 0.5 * pow2(e + 1);
+}
+
+/* 2^e as a binary64 bit pattern (normal range only) */
+__device__ __forceinline__ double pow2_bits(int e) {
+  return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+}
+
+struct EpiOzaki {
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
+    const bool row_ok = m < p.m;
+    const int ea = row_ok ? p.exp_a[m] : 0;
+    double *C = static_cast<double *>(p.c) + (long long)m;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32) {
+      double v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = 0.0;
+#pragma unroll
+      for (int d = NACC - 1; d >= 0; --d) {
+        uint32_t r[32];
+        tmem_ld_32x32b_x32(tbase + d * BN + c, r);
+        tmem_ld_wait();
+        constexpr double w0 = pow2(-14);
+        const double w = w0 * pow2(-7 * d); /* 2^(-7(d+2)), exact */
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          v[j] = fma(static_cast<double>(static_cast<int>(r[j])), w, v[j]);
+      }
+      if (!row_ok) continue;
+      const int nvalid = p.n - (n0 + c);
+      double cv[32];
+      int eb[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) eb[j] = (j < nvalid) ? p.exp_b[n0 + c + j] : 0;
+      if (p.beta_nonzero) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          cv[j] = (j < nvalid) ? C[(long long)(n0 + c + j) * p.ldc] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        if (j < nvalid) {
+          const int e = ea + eb[j];
+          double o;
+          if (ea == HCBK_OZ_NONFINITE || eb[j] == HCBK_OZ_NONFINITE)
+            o = __longlong_as_double(0x7ff8000000000000ll);
+          else if (ea == HCBK_OZ_ZERO || eb[j] == HCBK_OZ_ZERO)
+            o = 0.0;
+          else if (e >= -1022 && e <= 1023)
+            o = v[j] * pow2_bits(e); /* exact scaling */
+          else
+            o = ldexp(v[j], e);
+          o *= p.alpha_d;
+          if (p.beta_nonzero) o = fma(p.beta_d, cv[j], o);
+          C[(long long)(n0 + c + j) * p.ldc] = o;
+        }
+      }
+    }
+  }
+};
+
 /* ------------------------------------------------------------- kernel -- */
 
+/* per operand kind: K bytes per tile row (one swizzle atom), elements per
+ * K-slab, K per MMA instruction, accumulator / operand formats, swizzle */
 template <int KIND> struct KindTraits;
-template <> struct KindTraits<0> { /* f16 */
-  static constexpr int BKE = 64, UK = 16, ESZ = 2;
-  static constexpr uint32_t CFMT = 1, ABFMT = 0;
+template <> struct KindTraits<0> { /* f16, 128-byte swizzle */
+  static constexpr int ROWB = 128, BKE = 64, UK = 16, ESZ = 2;
+  static constexpr uint32_t CFMT = 1, ABFMT = 0, LAYOUT = 2, SBO = 1024;
 };
-template <> struct KindTraits<1> { /* bf16 */
-  static constexpr int BKE = 64, UK = 16, ESZ = 2;
-  static constexpr uint32_t CFMT = 1, ABFMT = 1;
+template <> struct KindTraits<1> { /* bf16, 128-byte swizzle */
+  static constexpr int ROWB = 128, BKE = 64, UK = 16, ESZ = 2;
+  static constexpr uint32_t CFMT = 1, ABFMT = 1, LAYOUT = 2, SBO = 1024;
+};
+template <> struct KindTraits<2> { /* s8 -> s32, 64-byte swizzle */
+  static constexpr int ROWB = 64, BKE = 64, UK = 32, ESZ = 1;
+  static constexpr uint32_t CFMT = 2, ABFMT = 1, LAYOUT = 4, SBO = 512;
 };
 
 __host__ __device__ constexpr uint32_t tmem_cols_for(uint32_t c) {
   return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512;
 }
 
-template <int BN, int STAGES, class R, int KIND>
+/* NBUF: TMEM accumulator sets (2 = the epilogue of one tile/chunk overlaps
+ * the MMAs of the next; 1 when the accumulators fill TMEM) */
+template <int BN, int STAGES, class R, int KIND, int NBUF = 2>
 struct TcCfg {
   using KT = KindTraits<KIND>;
-  static constexpr uint32_t A_PLANE = BM * ROWB;
-  static constexpr uint32_t B_PLANE = BN * ROWB;
+  static constexpr uint32_t A_PLANE = BM * KT::ROWB;
+  static constexpr uint32_t B_PLANE = BN * KT::ROWB;
   static constexpr uint32_t STAGE_BYTES = R::NA * A_PLANE + R::NB * B_PLANE;
   static constexpr uint32_t ACC_COLS = R::NACC * BN;
-  static constexpr uint32_t TMEM_COLS = tmem_cols_for(2 * ACC_COLS);
+  static constexpr uint32_t TMEM_COLS = tmem_cols_for(NBUF * ACC_COLS);
   static constexpr uint32_t BAR_BYTES = 256;
   static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
-  static_assert(2 * ACC_COLS <= 512, "accumulators exceed TMEM");
+  static_assert(NBUF * ACC_COLS <= 512, "accumulators exceed TMEM");
   static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "BN");
   static_assert(SMEM_BYTES <= 232448, "shared memory");
 };
@@ -221,13 +333,13 @@ struct TcCfg {
  *   spans only n*128 bytes of K, which bounds the error it adds; used by the
  *   split-BF16 paths, whose contract is "error no worse than FP32".
  */
-template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0>
+template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
-  using Cfg = TcCfg<BN, STAGES, R, KIND>;
+  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF>;
   using KT = typename Cfg::KT;
   constexpr int BKE = KT::BKE;
+  constexpr int ROWB = KT::ROWB;
   constexpr int KSTEPS = BKE / KT::UK;
-  static_assert(PROMOTE_KB > 0 || R::NACC == 1, "several accumulators need promotion");
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -253,8 +365,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     mbar_fence_init();
   }
   if (warp == 0 && lane == 0) {
-    for (int i = 0; i < R::NA; ++i) tma_prefetch_desc(&p.ta[i]);
-    for (int i = 0; i < R::NB; ++i) tma_prefetch_desc(&p.tb[i]);
+    constexpr int NMA = R::P3D ? 1 : R::NA, NMB = R::P3D ? 1 : R::NB;
+    for (int i = 0; i < NMA; ++i) tma_prefetch_desc(&p.ta[i]);
+    for (int i = 0; i < NMB; ++i) tma_prefetch_desc(&p.tb[i]);
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
@@ -284,11 +397,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           }
           mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
           uint8_t *st = smem + s * Cfg::STAGE_BYTES;
-          const int k0 = kb * BKE;
+          const int k0 = p.k0 + kb * BKE;
 #pragma unroll
           for (int a = 0; a < R::NA; ++a) {
             uint8_t *dst = st + a * Cfg::A_PLANE;
-            if (!p.a_mn) {
+            if constexpr (R::P3D) {
+              tma_load_3d(dst, &p.ta[0], &full[s], k0, tm * BM, a);
+            } else if (!p.a_mn) {
               tma_load_2d(dst, &p.ta[a], &full[s], k0, tm * BM);
             } else {
 #pragma unroll
@@ -299,7 +414,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
 #pragma unroll
           for (int b = 0; b < R::NB; ++b) {
             uint8_t *dst = st + R::NA * Cfg::A_PLANE + b * Cfg::B_PLANE;
-            if (!p.b_mn) {
+            if constexpr (R::P3D) {
+              tma_load_3d(dst, &p.tb[0], &full[s], k0, tn * BN, b);
+            } else if (!p.b_mn) {
               tma_load_2d(dst, &p.tb[b], &full[s], k0, tn * BN);
             } else {
 #pragma unroll
@@ -327,8 +444,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       bool ok = true;
       for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
         for (int kc = 0; ok && kc < kblocks; kc += chunk_kb, ++ci) {
-          const int b = ci & 1;
-          const uint32_t tph = (ci >> 1) & 1;
+          const int b = ci % NBUF;
+          const uint32_t tph = (ci / NBUF) & 1;
           if (!mbar_wait(&tempty[b], tph ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
             ok = false;
             break;
@@ -350,10 +467,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
                 const uint32_t aa = sbase + R::pa(pi) * Cfg::A_PLANE + kk * a_kstep;
                 const uint32_t ba =
                     sbase + R::NA * Cfg::A_PLANE + R::pb(pi) * Cfg::B_PLANE + kk * b_kstep;
-                const uint64_t ad = sw128_desc(aa, a_lbo, 1024);
-                const uint64_t bd = sw128_desc(ba, b_lbo, 1024);
+                const uint64_t ad = smem_desc(aa, a_lbo, KT::SBO, KT::LAYOUT);
+                const uint64_t bd = smem_desc(ba, b_lbo, KT::SBO, KT::LAYOUT);
                 const uint32_t acc = (kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
-                mma_f16(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
+                if constexpr (KIND == 2)
+                  mma_i8(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
+                else
+                  mma_f16(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
               }
             }
             mma_commit(&empty[s]);
@@ -375,8 +495,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       const int tm = t % p.tiles_m, tn = t / p.tiles_m;
       const int m = tm * BM + q * 32 + lane;
       if constexpr (PROMOTE_KB == 0) {
-        const int b = ci & 1;
-        const uint32_t tph = (ci >> 1) & 1;
+        const int b = ci % NBUF;
+        const uint32_t tph = (ci / NBUF) & 1;
         ++ci;
         if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) break;
         tc_fence_after();
@@ -391,8 +511,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
 #pragma unroll
         for (int j = 0; j < BN; ++j) acc[j] = 0.f;
         for (int kc = 0; kc < kblocks; kc += chunk_kb, ++ci) {
-          const int b = ci & 1;
-          const uint32_t tph = (ci >> 1) & 1;
+          const int b = ci % NBUF;
+          const uint32_t tph = (ci / NBUF) & 1;
           if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) {
             ok = false;
             break;
@@ -467,10 +587,33 @@ static int make_map(CUtensorMap *map, CUtensorMapDataType dt, int esz, const voi
   return HCBK_OK;
 }
 
-template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0>
+/* 3-D map over `planes` int8 slices: {K, rows, plane}, row pitch ld bytes,
+ * plane pitch `pstride` bytes; box = {64, box_rows, 1}, 64-byte swizzle. */
+static int make_map_planes(CUtensorMap *map, const void *base, uint64_t kdim, uint64_t rows,
+                           uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return HCBK_ERR_DRIVER;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld & 15) || (pstride & 15)) return HCBK_ERR_ALIGN;
+  cuuint64_t dims[3] = {kdim, rows, planes};
+  cuuint64_t strides[2] = {ld, pstride};
+  cuuint32_t box[3] = {64, box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    const char *e = getenv("HCBLAS_LOG");
+    if (e && e[0] == '1')
+      fprintf(stderr, "[hcblas] cuTensorMapEncodeTiled(3d) failed (%d)\n", (int)r);
+    return HCBK_ERR_ALIGN;
+  }
+  return HCBK_OK;
+}
+
+template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2>
 static int launch_tc(TcParams &p, void *stream) {
-  using Cfg = TcCfg<BN, STAGES, R, KIND>;
-  auto kern = tc_gemm_kernel<BN, STAGES, R, KIND, EPI, PROMOTE_KB>;
+  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF>;
+  auto kern = tc_gemm_kernel<BN, STAGES, R, KIND, EPI, PROMOTE_KB, NBUF>;
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -570,4 +713,48 @@ extern "C" int hcbk_sgemm_split_tc(const hcbk_split_gemm *g, int *err, void *str
   }
   if (g->promote_kb == 4) return launch_tc<128, 3, RecipeBf16x3, 1, EF, 4>(p, stream);
   return launch_tc<128, 3, RecipeBf16x3, 1, EF, 1>(p, stream);
+}
+
+extern "C" int64_t hcbk_ozaki_max_k(int slices) {
+  if (slices < 1) return 0;
+  /* |acc_d| <= slices * K * 127^2 must stay below 2^31 */
+  const int64_t k = (int64_t)0x7fffffff / ((int64_t)slices * 127 * 127);
+  return k & ~int64_t(63);
+}
+
+/* Ozaki slice-product GEMM with the FP64 epilogue (one K range). */
+extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream) {
+  if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > hcbk_ozaki_max_k(g->slices) ||
+      g->k0 + g->k > 0x7fffffff || g->k <= 0)
+    return HCBK_ERR_ARGS;
+  TcParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = (int)g->m;
+  p.n = (int)g->n;
+  p.k = (int)g->k;
+  p.k0 = (int)g->k0;
+  const int s = g->slices;
+  const uint32_t bn = s <= 4 ? 128 : 64;
+  const uint64_t kdim = (uint64_t)(g->k0 + g->k);
+  int rc = make_map_planes(&p.ta[0], g->a_planes, kdim, g->m, s, g->ld_a, g->a_plane_stride, BM);
+  if (rc) return rc;
+  rc = make_map_planes(&p.tb[0], g->b_planes, kdim, g->n, s, g->ld_b, g->b_plane_stride, bn);
+  if (rc) return rc;
+  p.c = g->c;
+  p.ldc = g->ldc;
+  p.alpha_d = g->alpha;
+  p.beta_d = g->beta;
+  p.beta_nonzero = g->beta != 0.0;
+  p.exp_a = g->exp_a;
+  p.exp_b = g->exp_b;
+  p.err = err;
+  switch (s) {
+    case 3: return launch_tc<128, 4, RecipeOzaki<3>, 2, EpiOzaki, 0, 1>(p, stream);
+    case 4: return launch_tc<128, 3, RecipeOzaki<4>, 2, EpiOzaki, 0, 1>(p, stream);
+    case 5: return launch_tc<64, 3, RecipeOzaki<5>, 2, EpiOzaki, 0, 1>(p, stream);
+    case 6: return launch_tc<64, 3, RecipeOzaki<6>, 2, EpiOzaki, 0, 1>(p, stream);
+    case 7: return launch_tc<64, 2, RecipeOzaki<7>, 2, EpiOzaki, 0, 1>(p, stream);
+    case 8: return launch_tc<64, 2, RecipeOzaki<8>, 2, EpiOzaki, 0, 1>(p, stream);
+    default: return HCBK_ERR_ARGS;
+  }
 }
