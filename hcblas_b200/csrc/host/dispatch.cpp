@@ -121,13 +121,14 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
 /* Ozaki-scheme DGEMM on INT8 tensor cores: per-row / per-column exponents,
  * `s` int8 slices per operand, slice products exact in INT32, FP64 epilogue.
  * K is split so that every INT32 group sum stays exact. */
-int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, void *stream,
+int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, void *stream,
                 const char **path) {
   if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
-  if (s < 3 || s > 8) return HCBK_ERR_ARGS;
-  const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch */
+  if (s < 3 || s > (f16 ? 7 : 8)) return HCBK_ERR_ARGS;
+  const int esz = f16 ? 2 : 1;
+  const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for either slice type */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
-  const size_t a_pl = up1k((size_t)a->m * kp), b_pl = up1k((size_t)a->n * kp);
+  const size_t a_pl = up1k((size_t)a->m * kp * esz), b_pl = up1k((size_t)a->n * kp * esz);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
   const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl);
   char *ws = static_cast<char *>(ensure_workspace(st, total));
@@ -149,6 +150,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, void *strea
   pa.planes = pa_base;
   pa.plane_stride = (int64_t)a_pl;
   pa.ld_dst = kp;
+  pa.f16 = f16 ? 1 : 0;
   hcbk_ozaki_prep pb;
   pb.src = static_cast<const double *>(a->b) + a->b_off;
   pb.ld = a->ldb;
@@ -160,6 +162,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, void *strea
   pb.planes = pb_base;
   pb.plane_stride = (int64_t)b_pl;
   pb.ld_dst = kp;
+  pb.f16 = f16 ? 1 : 0;
 
   int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pa, stream); });
   if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pb, stream); });
@@ -167,10 +170,14 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, void *strea
   if (!rc) rc = timed_launch(st, stream, "ozaki.slice", [&] { return hcbk_ozaki_slice(&pb, stream); });
   if (rc) return rc;
 
-  static const char *names[9] = {"", "", "", "tc.ozaki_s3", "tc.ozaki_s4", "tc.ozaki_s5",
-                                  "tc.ozaki_s6", "tc.ozaki_s7", "tc.ozaki_s8"};
-  *path = names[s];
-  const int64_t kmax = hcbk_ozaki_max_k(s);
+  static const char *names[9] = {"", "", "", "tc.ozaki_i8_s3", "tc.ozaki_i8_s4", "tc.ozaki_i8_s5",
+                                  "tc.ozaki_i8_s6", "tc.ozaki_i8_s7", "tc.ozaki_i8_s8"};
+  static const char *names16[8] = {"", "", "", "tc.ozaki_f16_s3", "tc.ozaki_f16_s4",
+                                    "tc.ozaki_f16_s5", "tc.ozaki_f16_s6", "tc.ozaki_f16_s7"};
+  *path = f16 ? names16[s] : names[s];
+  /* INT32 exactness bounds one INT8 launch's K; the f16 kernel promotes per
+   * K-slab and takes any K */
+  const int64_t kmax = f16 ? a->k : hcbk_ozaki_max_k(s);
   hcbk_ozaki_gemm g;
   g.m = a->m;
   g.n = a->n;
@@ -190,7 +197,9 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, void *strea
     g.k0 = k0;
     g.k = (a->k - k0 < kmax) ? a->k - k0 : kmax;
     g.beta = (k0 == 0) ? a->beta_re : 1.0;
-    rc = timed_launch(st, stream, *path, [&] { return hcbk_ozaki_gemm_tc(&g, err, stream); });
+    rc = timed_launch(st, stream, *path, [&] {
+      return f16 ? hcbk_ozaki16_gemm_tc(&g, err, stream) : hcbk_ozaki_gemm_tc(&g, err, stream);
+    });
     if (rc) return rc;
   }
   return HCBK_OK;
@@ -211,10 +220,12 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] split-bf16 path declined (%d)\n", rc);
   }
-  if (a->dtype == HCBK_D && st->math_mode == 2 /* HCBLAS_MATH_OZAKI_INT8 */ && a->batch == 1 &&
+  if (a->dtype == HCBK_D && (st->math_mode == 2 || st->math_mode == 3) && a->batch == 1 &&
       !a->a_array) {
-    const int s = st->math_param > 0 ? st->math_param : st->ozaki_default_slices;
-    int rc = dgemm_ozaki(st, a, s, stream, path);
+    /* 2: HCBLAS_MATH_OZAKI_INT8, 3: HCBLAS_MATH_OZAKI_F16 */
+    const bool f16 = st->math_mode == 3;
+    const int s = st->math_param > 0 ? st->math_param : (f16 ? 7 : st->ozaki_default_slices);
+    int rc = dgemm_ozaki(st, a, s, f16, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] ozaki path declined (%d)\n", rc);
   }

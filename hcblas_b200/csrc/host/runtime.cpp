@@ -330,11 +330,13 @@ extern "C" hcblasStatus_t hcblasGetMatrix(hcblasHandle_t handle, int rows, int c
 extern "C" hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param) {
   if (handle == nullptr || !handle->initialized || !handle->impl)
     return HCBLAS_STATUS_NOT_INITIALIZED;
-  if (mode < HCBLAS_MATH_NATIVE || mode > HCBLAS_MATH_OZAKI_INT8)
+  if (mode < HCBLAS_MATH_NATIVE || mode > HCBLAS_MATH_OZAKI_F16)
     return HCBLAS_STATUS_INVALID_VALUE;
   if (mode == HCBLAS_MATH_SPLIT_BF16 && !(param == 0 || param == 3 || param == 6))
     return HCBLAS_STATUS_INVALID_VALUE;
-  if (mode == HCBLAS_MATH_OZAKI_INT8 && (param < 0 || param > 8))
+  if (mode == HCBLAS_MATH_OZAKI_INT8 && (param < 0 || param > 8 || (param > 0 && param < 3)))
+    return HCBLAS_STATUS_INVALID_VALUE;
+  if (mode == HCBLAS_MATH_OZAKI_F16 && (param < 0 || param > 7 || (param > 0 && param < 3)))
     return HCBLAS_STATUS_INVALID_VALUE;
   handle->impl->math_mode = mode;
   handle->impl->math_param = param;

@@ -140,7 +140,8 @@ typedef struct hcbk_ozaki_prep {
   int slices;
   void *planes;
   int64_t plane_stride; /* bytes between planes */
-  int64_t ld_dst;       /* bytes (= int8 elements) between rows */
+  int64_t ld_dst;       /* elements between rows */
+  int f16;              /* 0: int8 slices of 7 bits; 1: binary16 slices of 8 bits */
 } hcbk_ozaki_prep;
 int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
 int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream);
@@ -164,6 +165,10 @@ typedef struct hcbk_ozaki_gemm {
   double alpha, beta;
 } hcbk_ozaki_gemm;
 int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream);
+/* The same product on the f16 tensor path: binary16 planes holding 8-bit
+ * integer slices (ld_a / ld_b in elements), weights 2^(-8(i+j+2)); any K
+ * (k0 must be 0), slices 3..7. */
+int hcbk_ozaki16_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream);
 /* largest K per launch for s slices (INT32 exactness), multiple of 64 */
 int64_t hcbk_ozaki_max_k(int slices);
 

@@ -22,6 +22,7 @@
  * HCBK_OZ_NONFINITE, its slices are zero and the epilogue returns NaN for
  * the outputs it touches.  An all-zero row gets exponent 0 and zero slices.
  */
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -81,28 +82,42 @@ __global__ void oz_fill(int *exps, int64_t n, int v) {
     exps[i] = v;
 }
 
-template <int S>
-__device__ __forceinline__ void slice_value(double x, int e, int8_t (&a)[S]) {
+/* slice storage: int8 with 7-bit slices (radix 128) or binary16 with 8-bit
+ * slices (radix 256, integers <= 255 are exact in binary16) */
+template <typename ST> struct SliceT;
+template <> struct SliceT<int8_t> {
+  static constexpr double RADIX = 128.0;
+  static __device__ __forceinline__ int8_t make(int v) { return static_cast<int8_t>(v); }
+};
+template <> struct SliceT<__half> {
+  static constexpr double RADIX = 256.0;
+  static __device__ __forceinline__ __half make(int v) { return __int2half_rn(v); }
+};
+
+template <int S, typename ST>
+__device__ __forceinline__ void slice_value(double x, int e, ST (&a)[S]) {
   if (e == HCBK_OZ_NONFINITE || e == HCBK_OZ_ZERO) {
 #pragma unroll
-    for (int i = 0; i < S; ++i) a[i] = 0;
+    for (int i = 0; i < S; ++i) a[i] = SliceT<ST>::make(0);
     return;
   }
   double y = ldexp(x, -e); /* |y| < 1, exact */
 #pragma unroll
   for (int i = 0; i < S; ++i) {
-    y *= 128.0;
+    y *= SliceT<ST>::RADIX;
     const double t = trunc(y);
-    a[i] = static_cast<int8_t>(static_cast<int>(t));
+    a[i] = SliceT<ST>::make(static_cast<int>(t));
     y -= t;
   }
 }
 
-/* K-contiguous source: 8 consecutive k per thread, 8-byte plane stores */
-template <int S>
+/* K-contiguous source: 8 consecutive k per thread, one vector store of the
+ * 8 slices per plane (8 bytes for int8, 16 bytes for binary16) */
+template <int S, typename ST>
 __global__ void oz_slice_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
-                                 const int *exps, int8_t *planes, int64_t plane_stride,
+                                 const int *exps, char *planes, int64_t plane_stride,
                                  int64_t ld_dst) {
+  struct alignas(8 * sizeof(ST)) Vec8 { ST v[8]; };
   const int64_t kq = (kdim + 7) / 8;
   const int64_t total = rows * kq;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -110,34 +125,31 @@ __global__ void oz_slice_kcontig(const double *src, int64_t ld, int64_t rows, in
     const int64_t r = idx / kq;
     const int64_t k0 = (idx % kq) * 8;
     const int e = exps[r];
-    int8_t out[S][8];
+    Vec8 out[S];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      int8_t a[S];
+      ST a[S];
       const double x = (k0 + j < kdim) ? src[r * ld + k0 + j] : 0.0;
-      slice_value<S>(x, e, a);
+      slice_value<S, ST>(x, e, a);
 #pragma unroll
-      for (int i = 0; i < S; ++i) out[i][j] = a[i];
+      for (int i = 0; i < S; ++i) out[i].v[j] = a[i];
     }
     for (int i = 0; i < S; ++i) {
-      int8_t *d = planes + i * plane_stride + r * ld_dst + k0;
-      if (k0 + 8 <= kdim && ((reinterpret_cast<uintptr_t>(d) & 7) == 0)) {
-        uint64_t w = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) w |= static_cast<uint64_t>(static_cast<uint8_t>(out[i][j])) << (8 * j);
-        *reinterpret_cast<uint64_t *>(d) = w;
+      ST *d = reinterpret_cast<ST *>(planes + i * plane_stride) + r * ld_dst + k0;
+      if (k0 + 8 <= kdim && ((reinterpret_cast<uintptr_t>(d) & (sizeof(Vec8) - 1)) == 0)) {
+        *reinterpret_cast<Vec8 *>(d) = out[i];
       } else {
         for (int j = 0; j < 8; ++j)
-          if (k0 + j < kdim) d[j] = out[i][j];
+          if (k0 + j < kdim) d[j] = out[i].v[j];
       }
     }
   }
 }
 
 /* MN-contiguous source: 32x32 tile through shared memory */
-template <int S>
+template <int S, typename ST>
 __global__ void oz_slice_rcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
-                                 const int *exps, int8_t *planes, int64_t plane_stride,
+                                 const int *exps, char *planes, int64_t plane_stride,
                                  int64_t ld_dst) {
   __shared__ double tile[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
@@ -155,32 +167,37 @@ __global__ void oz_slice_rcontig(const double *src, int64_t ld, int64_t rows, in
     const int rl = ty + 8 * i;
     const int64_t r = r0 + rl, k = k0 + tx;
     if (r < rows && k < kdim) {
-      int8_t a[S];
-      slice_value<S>(tile[tx][rl], exps[r], a);
+      ST a[S];
+      slice_value<S, ST>(tile[tx][rl], exps[r], a);
 #pragma unroll
-      for (int p = 0; p < S; ++p) planes[p * plane_stride + r * ld_dst + k] = a[p];
+      for (int p = 0; p < S; ++p)
+        reinterpret_cast<ST *>(planes + p * plane_stride)[r * ld_dst + k] = a[p];
     }
   }
 }
 
-template <int S>
+template <int S, typename ST>
 int launch_slice(const hcbk_ozaki_prep *a, cudaStream_t st) {
-  int8_t *planes = static_cast<int8_t *>(a->planes);
+  char *planes = static_cast<char *>(a->planes);
   if (a->k_contig) {
     const int64_t total = a->rows * ((a->kdim + 7) / 8);
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    oz_slice_kcontig<S><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim,
-                                                          a->exps, planes, a->plane_stride,
-                                                          a->ld_dst);
+    oz_slice_kcontig<S, ST><<<(unsigned)blocks, 256, 0, st>>>(
+        a->src, a->ld, a->rows, a->kdim, a->exps, planes, a->plane_stride, a->ld_dst);
   } else {
     const int64_t gx = (a->rows + 31) / 32, gy = (a->kdim + 31) / 32;
     if (gy > 65535) return HCBK_ERR_ARGS;
-    oz_slice_rcontig<S><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(
+    oz_slice_rcontig<S, ST><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(
         a->src, a->ld, a->rows, a->kdim, a->exps, planes, a->plane_stride, a->ld_dst);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+template <int S>
+int launch_slice_any(const hcbk_ozaki_prep *a, cudaStream_t st) {
+  return a->f16 ? launch_slice<S, __half>(a, st) : launch_slice<S, int8_t>(a, st);
 }
 
 }  // namespace
@@ -212,12 +229,12 @@ extern "C" int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a->rows <= 0 || a->kdim <= 0) return HCBK_ERR_ARGS;
   switch (a->slices) {
-    case 3: return launch_slice<3>(a, st);
-    case 4: return launch_slice<4>(a, st);
-    case 5: return launch_slice<5>(a, st);
-    case 6: return launch_slice<6>(a, st);
-    case 7: return launch_slice<7>(a, st);
-    case 8: return launch_slice<8>(a, st);
+    case 3: return launch_slice_any<3>(a, st);
+    case 4: return launch_slice_any<4>(a, st);
+    case 5: return launch_slice_any<5>(a, st);
+    case 6: return launch_slice_any<6>(a, st);
+    case 7: return launch_slice_any<7>(a, st);
+    case 8: return launch_slice_any<8>(a, st);
     default: return HCBK_ERR_ARGS;
   }
 }

@@ -219,12 +219,9 @@ template <typename OutT> struct EpiAlphaBeta {
  *   C = alpha * 2^(ea_m + eb_n) * sum_d 2^(-7(d+2)) acc_d + beta * C   (FP64)
  * The group terms are exact in binary64 (|acc_d| < 2^31, power-of-two
  * weights) and are added smallest weight first. */
-__host__ __device__ constexpr double pow2(int e) {
-  /* exact 2^e for -1022 <= e <= 1023 */
-  return e >= 0 ? (e == 0 ? 1.0 : 2.0 * pow2(e - 1)) : 0.5 * pow2(e + 1);
-}
-
-/* 2^e as a binary64 bit pattern (normal range only) */
+/* 2^e built from its binary64 bit pattern (exact; normal range
+ * -1022 <= e <= 1023 only).  Deliberately not recursive: device recursion
+ * consumes the (1 KB default) call stack. */
 __device__ __forceinline__ double pow2_bits(int e) {
   return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
 }
@@ -245,39 +242,42 @@ struct EpiOzaki {
         uint32_t r[32];
         tmem_ld_32x32b_x32(tbase + d * BN + c, r);
         tmem_ld_wait();
-        constexpr double w0 = pow2(-14);
-        const double w = w0 * pow2(-7 * d); /* 2^(-7(d+2)), exact */
+        const double w = pow2_bits(-7 * (d + 2)); /* exact group weight */
 #pragma unroll
         for (int j = 0; j < 32; ++j)
           v[j] = fma(static_cast<double>(static_cast<int>(r[j])), w, v[j]);
       }
       if (!row_ok) continue;
-      const int nvalid = p.n - (n0 + c);
-      double cv[32];
-      int eb[32];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) eb[j] = (j < nvalid) ? p.exp_b[n0 + c + j] : 0;
-      if (p.beta_nonzero) {
+      for (int c8 = 0; c8 < 32; c8 += 8) {
+        const int nvalid = p.n - (n0 + c + c8);
+        if (nvalid <= 0) break;
+        double cv[8];
+        int eb[8];
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-          cv[j] = (j < nvalid) ? C[(long long)(n0 + c + j) * p.ldc] : 0.0;
-      }
+        for (int j = 0; j < 8; ++j) eb[j] = (j < nvalid) ? p.exp_b[n0 + c + c8 + j] : 0;
+        if (p.beta_nonzero) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        if (j < nvalid) {
-          const int e = ea + eb[j];
-          double o;
-          if (ea == HCBK_OZ_NONFINITE || eb[j] == HCBK_OZ_NONFINITE)
-            o = __longlong_as_double(0x7ff8000000000000ll);
-          else if (ea == HCBK_OZ_ZERO || eb[j] == HCBK_OZ_ZERO)
-            o = 0.0;
-          else if (e >= -1022 && e <= 1023)
-            o = v[j] * pow2_bits(e); /* exact scaling */
-          else
-            o = ldexp(v[j], e);
-          o *= p.alpha_d;
-          if (p.beta_nonzero) o = fma(p.beta_d, cv[j], o);
-          C[(long long)(n0 + c + j) * p.ldc] = o;
+          for (int j = 0; j < 8; ++j)
+            cv[j] = (j < nvalid) ? C[(long long)(n0 + c + c8 + j) * p.ldc] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (j < nvalid) {
+            const int e = ea + eb[j];
+            double o;
+            if (ea == HCBK_OZ_NONFINITE || eb[j] == HCBK_OZ_NONFINITE)
+              o = __longlong_as_double(0x7ff8000000000000ll);
+            else if (ea == HCBK_OZ_ZERO || eb[j] == HCBK_OZ_ZERO)
+              o = 0.0;
+            else if (e >= -1022 && e <= 1023)
+              o = v[c8 + j] * pow2_bits(e); /* exact scaling */
+            else
+              o = ldexp(v[c8 + j], e);
+            o *= p.alpha_d;
+            if (p.beta_nonzero) o = fma(p.beta_d, cv[j], o);
+            C[(long long)(n0 + c + c8 + j) * p.ldc] = o;
+          }
         }
       }
     }

@@ -281,12 +281,17 @@ int hcblasLibGemmBatched(hcblasHandle_t h, int dtype, int order, char typeA, cha
  *   HCBLAS_MATH_OZAKI_INT8 D/Z: Ozaki scheme, FP64 operands scaled per row/col
  *                          and sliced into `param` INT8 slices, slice products
  *                          exact in INT32 on tcgen05 tensor cores
- *                          (`param` = 0 picks the slice count from the
- *                          accuracy set by hcblasSetEmulationAccuracy). */
+ *                          (`param` = 3..8 slices of 7 bits; 0 = 7 slices)
+ *   HCBLAS_MATH_OZAKI_F16  D: the same scheme with 8-bit integer slices held
+ *                          in binary16, products on the tcgen05 f16 path with
+ *                          FP32 sums kept exact (integers < 2^24) and promoted
+ *                          to FP64 per 32-element K slab (`param` = 3..7
+ *                          slices of 8 bits; 0 = 7 slices, 56 bits). */
 enum {
   HCBLAS_MATH_NATIVE = 0,
   HCBLAS_MATH_SPLIT_BF16 = 1,
-  HCBLAS_MATH_OZAKI_INT8 = 2
+  HCBLAS_MATH_OZAKI_INT8 = 2,
+  HCBLAS_MATH_OZAKI_F16 = 3
 };
 hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param);
 hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);

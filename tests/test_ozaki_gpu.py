@@ -1,11 +1,15 @@
-"""GPU parity of the Ozaki-scheme DGEMM (INT8 slices on tcgen05) against the
-double-double oracle.
+"""GPU parity of the Ozaki-scheme DGEMM (INT8 slices on tcgen05 kind::i8, and
+8-bit slices in binary16 on tcgen05 kind::f16) against the double-double
+oracle.
 
 Bound (a-priori, per element).  With e_m, f_n the row/column exponents
-(|A(m,k)| < 2^e_m, |B(k,n)| < 2^f_n) and s slices of 7 bits:
-  representation: |A - A_s| < 2^(e_m - 7s), same for B      -> 2 * 2^-7s
-  dropped products a_i b_j with i + j >= s                 -> (s+1) * 2^-7s
-so |C - C_s| <= |alpha| * K * (s+3) * 2^(e_m + f_n - 7s) + (s+2) u |C_s|.
+(|A(m,k)| < 2^e_m, |B(k,n)| < 2^f_n), s slices of b bits (b = 7 for INT8,
+b = 8 for f16):
+  representation: |A - A_s| < 2^(e_m - b s), same for B     -> 2 * 2^(-b s)
+  dropped products a_i b_j with i + j >= s                  -> (s+1) * 2^(-b s)
+  binary64 additions of the group sums (n_add of them, each
+  on a partial sum below K 2^(e_m + f_n))                   -> n_add * u
+so |C - C_s| <= |alpha| K 2^(e_m + f_n) ((s+3) 2^(-b s) + n_add u) + 2u|beta C|.
 The test uses the Frobenius norm of that elementwise bound.
 """
 import numpy as np
@@ -13,29 +17,32 @@ import pytest
 
 import hcblas_b200 as hb
 from oracle import oracle as O
-from tests.test_gemm_gpu import make_case, TCH
+from tests.test_gemm_gpu import make_case, op_dense, TCH
 
 pytestmark = pytest.mark.gpu
 
-
-def frexp_exp(x):
-    _, e = np.frexp(np.max(np.abs(x)) if np.size(x) else 0.0)
-    return e
+MODES = {"i8": (hb.HCBLAS_MATH_OZAKI_INT8, 7), "f16": (hb.HCBLAS_MATH_OZAKI_F16, 8)}
+U = 2.0 ** -53
 
 
-def ozaki_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, s, ref):
-    from tests.test_gemm_gpu import op_dense
+def ozaki_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, s, ref, kind="i8", beta=0.0, C=None,
+                ldc=None):
+    bits = MODES[kind][1]
     Ad = op_dense(A, order, ta, M, K, lda, 0)
     Bd = op_dense(B, order, tb, K, N, ldb, 0)
     ea = np.frexp(np.max(np.abs(Ad), axis=1))[1].astype(np.float64)
     eb = np.frexp(np.max(np.abs(Bd), axis=0))[1].astype(np.float64)
-    scale = np.exp2(ea[:, None] + eb[None, :] - 7 * s)
-    elem = abs(alpha) * K * (s + 3) * scale
-    return np.linalg.norm(elem) + (s + 2) * 2.0 ** -53 * np.linalg.norm(ref)
+    scale = np.exp2(ea[:, None] + eb[None, :])
+    n_add = (-(-K // 32)) * s + 2 if kind == "f16" else s + 2
+    elem = abs(alpha) * K * scale * ((s + 3) * 2.0 ** (-bits * s) + n_add * U)
+    out = np.linalg.norm(elem) + 4 * U * np.linalg.norm(ref)
+    if beta and C is not None:
+        out += 2 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
+    return out
 
 
-def run_ozaki(handle, s, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C, ldc):
-    assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_INT8, s) == 0
+def run_ozaki(handle, kind, s, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C, ldc):
+    assert hb.hcblasSetMathMode(handle, MODES[kind][0], s) == 0
     try:
         dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
         rc = hb.lib_gemm(handle, order, TCH[ta], TCH[tb], M, N, K, alpha, dA, lda, dB, ldb, beta,
@@ -48,24 +55,30 @@ def run_ozaki(handle, s, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C,
         hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
 
 
-@pytest.mark.parametrize("s", [3, 4, 5, 6, 7, 8])
-def test_ozaki_slices_vs_dd_oracle(handle, s):
+CASES = [(O.COL, 0, 1, 300, 200, 500), (O.COL, 1, 0, 129, 77, 64), (O.ROW, 0, 0, 256, 256, 1000),
+         (O.COL, 1, 1, 1000, 130, 257)]
+
+
+@pytest.mark.parametrize("kind,s", [("i8", 3), ("i8", 5), ("i8", 7), ("i8", 8), ("f16", 3),
+                                    ("f16", 4), ("f16", 5), ("f16", 6), ("f16", 7)])
+def test_ozaki_slices_vs_dd_oracle(handle, kind, s):
     rng = np.random.default_rng(500 + s)
-    cases = [(O.COL, 0, 1, 300, 200, 500), (O.COL, 1, 0, 129, 77, 64), (O.ROW, 0, 0, 256, 256, 1000),
-             (O.COL, 1, 1, 1000, 130, 257)]
-    for order, ta, tb, M, N, K in cases:
+    for order, ta, tb, M, N, K in CASES:
         A, lda, B, ldb, C, ldc = make_case(rng, "d", order, ta, tb, M, N, K)
         alpha, beta = 1.5, -0.25
-        got, path = run_ozaki(handle, s, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C, ldc)
-        assert path == f"tc.ozaki_s{s}", path
+        got, path = run_ozaki(handle, kind, s, order, ta, tb, M, N, K, alpha, beta, A, lda, B,
+                              ldb, C, ldc)
+        assert path == f"tc.ozaki_{kind}_s{s}", path
         _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
         gv = O.view_c(got, order, M, N, ldc)
         err = np.linalg.norm(gv - ref)
-        bound = ozaki_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, s, ref)
-        assert err <= bound, (s, order, ta, tb, M, N, K, err, bound)
+        bound = ozaki_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, s, ref, kind, beta, C,
+                            ldc)
+        assert err <= bound, (kind, s, order, ta, tb, M, N, K, err, bound)
 
 
-def test_ozaki_hard_exponent_range(handle):
+@pytest.mark.parametrize("kind", ["i8", "f16"])
+def test_ozaki_hard_exponent_range(handle, kind):
     """Entries N(0,1) * 2^e, e ~ U{-20..20} per row of A and per column of B."""
     rng = np.random.default_rng(1)
     M = N = K = 512
@@ -76,16 +89,18 @@ def test_ozaki_hard_exponent_range(handle):
     C = np.zeros(M * N)
     _, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, Af, M, Bf, K, 0.0, C, M)
     errs = {}
-    for s in (5, 6, 7, 8):
-        got, _ = run_ozaki(handle, s, O.COL, 0, 0, M, N, K, 1.0, 0.0, Af, M, Bf, K, C, M)
-        errs[s] = O.normwise_rel_error(O.view_c(got, O.COL, M, N, M), ref)
-        bound = ozaki_bound(O.COL, 0, 0, M, N, K, 1.0, Af, M, Bf, K, s, ref)
-        assert np.linalg.norm(O.view_c(got, O.COL, M, N, M) - ref) <= bound
-    print("ozaki hard-range normwise errors:", errs)
-    assert errs[8] < errs[6] < errs[5]
+    for s in (5, 6, 7):
+        got, _ = run_ozaki(handle, kind, s, O.COL, 0, 0, M, N, K, 1.0, 0.0, Af, M, Bf, K, C, M)
+        gv = O.view_c(got, O.COL, M, N, M)
+        errs[s] = O.normwise_rel_error(gv, ref)
+        bound = ozaki_bound(O.COL, 0, 0, M, N, K, 1.0, Af, M, Bf, K, s, ref, kind)
+        assert np.linalg.norm(gv - ref) <= bound
+    print(f"ozaki {kind} hard-range normwise errors:", errs)
+    assert errs[7] < errs[6] < errs[5]
 
 
-def test_ozaki_special_rows(handle):
+@pytest.mark.parametrize("kind", ["i8", "f16"])
+def test_ozaki_special_rows(handle, kind):
     rng = np.random.default_rng(4)
     M, N, K = 64, 48, 80
     A = rng.standard_normal(M * K)
@@ -93,7 +108,7 @@ def test_ozaki_special_rows(handle):
     A[3 + np.arange(K) * M] = 0.0       # row 3 of A all zero
     A[5 + 7 * M] = np.nan               # row 5 holds a NaN
     C = np.ones(M * N)
-    got, _ = run_ozaki(handle, 7, O.COL, 0, 0, M, N, K, 1.0, 0.5, A, M, B, K, C, M)
+    got, _ = run_ozaki(handle, kind, 7, O.COL, 0, 0, M, N, K, 1.0, 0.5, A, M, B, K, C, M)
     gv = O.view_c(got, O.COL, M, N, M)
     assert np.all(np.isnan(gv[5, :]))
     assert np.all(gv[3, :] == 0.5)
@@ -101,25 +116,27 @@ def test_ozaki_special_rows(handle):
     ok[5] = False
     A0 = np.nan_to_num(A)
     _, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, 0.5, C, M)
-    ref_ok = ref[ok]
-    bound = ozaki_bound(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, 7, ref)
-    assert np.linalg.norm(gv[ok] - ref_ok) <= bound
+    bound = ozaki_bound(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, 7, ref, kind, 0.5, C, M)
+    assert np.linalg.norm(gv[ok] - ref[ok]) <= bound
 
 
-def test_ozaki_k_split(handle):
-    """K beyond one launch's INT32-exact range (~16.6k for s = 8) is split."""
+@pytest.mark.parametrize("kind", ["i8", "f16"])
+def test_ozaki_long_k(handle, kind):
+    """K beyond one INT8 launch's INT32-exact range (~16.6k for s = 8) is split
+    into launches; the f16 kernel promotes per slab and runs it in one."""
     rng = np.random.default_rng(6)
     M, N, K = 40, 36, 17000
+    s = 8 if kind == "i8" else 7
     A, lda, B, ldb, C, ldc = make_case(rng, "d", O.COL, 1, 0, M, N, K)
-    got, path = run_ozaki(handle, 8, O.COL, 1, 0, M, N, K, 1.0, 1.0, A, lda, B, ldb, C, ldc)
+    got, path = run_ozaki(handle, kind, s, O.COL, 1, 0, M, N, K, 1.0, 1.0, A, lda, B, ldb, C, ldc)
     _, ref = O.gemm(O.COL, 1, 0, M, N, K, 1.0, A, lda, B, ldb, 1.0, C, ldc)
     err = np.linalg.norm(O.view_c(got, O.COL, M, N, ldc) - ref)
-    assert err <= ozaki_bound(O.COL, 1, 0, M, N, K, 1.0, A, lda, B, ldb, 8, ref)
+    assert err <= ozaki_bound(O.COL, 1, 0, M, N, K, 1.0, A, lda, B, ldb, s, ref, kind, 1.0, C, ldc)
 
 
 def test_ozaki_vs_native_accuracy(handle):
-    """Config of the headline: col-major N/T, N(0,1); report errors of native
-    FP64 and Ozaki s = 6, 7, 8 against the double-double oracle."""
+    """Config of the headline: col-major N/T, N(0,1); errors of native FP64
+    and of the Ozaki paths against the double-double oracle."""
     rng = np.random.default_rng(1)
     M = N = K = 1024
     A = rng.standard_normal(M * K)
@@ -129,8 +146,9 @@ def test_ozaki_vs_native_accuracy(handle):
     dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
     assert hb.lib_gemm(handle, O.COL, "n", "t", M, N, K, 1.0, dA, M, dB, N, 0.0, dC, M) == 0
     errs = {"native": O.normwise_rel_error(O.view_c(dC.download(), O.COL, M, N, M), ref)}
-    for s in (6, 7, 8):
-        got, _ = run_ozaki(handle, s, O.COL, 0, 1, M, N, K, 1.0, 0.0, A, M, B, N, C, M)
-        errs[s] = O.normwise_rel_error(O.view_c(got, O.COL, M, N, M), ref)
+    for kind, s in (("i8", 6), ("i8", 7), ("i8", 8), ("f16", 6), ("f16", 7)):
+        got, _ = run_ozaki(handle, kind, s, O.COL, 0, 1, M, N, K, 1.0, 0.0, A, M, B, N, C, M)
+        errs[f"{kind}_s{s}"] = O.normwise_rel_error(O.view_c(got, O.COL, M, N, M), ref)
     print("native vs ozaki normwise errors:", errs)
-    assert errs[8] <= errs["native"] * 4
+    assert errs["i8_s8"] <= errs["native"] * 4
+    assert errs["f16_s7"] <= errs["native"] * 4
