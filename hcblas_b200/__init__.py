@@ -40,6 +40,7 @@ RowMajor, ColMajor = 0, 1
 # math modes (extension)
 HCBLAS_MATH_NATIVE, HCBLAS_MATH_SPLIT_BF16, HCBLAS_MATH_OZAKI_INT8 = 0, 1, 2
 HCBLAS_MATH_OZAKI_F16 = 3
+HCBLAS_MATH_OZAKI_CRT = 4
 
 # every C-ABI entry point include/hcblas.h declares (checked by the tests)
 EXPORTED = (

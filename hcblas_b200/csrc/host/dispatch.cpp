@@ -13,7 +13,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "../kernels/hcbk.h"
 
@@ -205,6 +207,140 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   return HCBK_OK;
 }
 
+/* Choose the number of moduli and the integer width beta for K so that the
+ * exact product fits the CRT range: prod(p_i) > 2 K 2^(2 beta).  `want` = 0
+ * asks for full binary64 width (beta = 53) with the fewest moduli. */
+bool crt_plan(int64_t k, int want, int *nmod, int *beta) {
+  int count = 0;
+  const int *mods = hcbk_crt_moduli(&count);
+  const double lk = std::ceil(std::log2((double)(k > 1 ? k : 2)));
+  double cum = 0.0;
+  for (int i = 0; i < count; ++i) {
+    cum += std::log2((double)mods[i]);
+    const int n = i + 1;
+    int b = (int)std::floor((cum - 1.0 - lk - 0.01) / 2.0);
+    if (b > 53) b = 53;
+    if ((want == 0 && b >= 53) || (want == n)) {
+      if (b < 8) return false;
+      *nmod = n;
+      *beta = b;
+      return true;
+    }
+  }
+  if (want == 0) { /* K too large for 53 bits: use every modulus */
+    const int b = (int)std::floor((cum - 1.0 - lk - 0.01) / 2.0);
+    if (b < 8) return false;
+    *nmod = count;
+    *beta = b > 53 ? 53 : b;
+    return true;
+  }
+  return false;
+}
+
+/* CRT (Ozaki scheme II) DGEMM: exponents, residue planes of the scaled
+ * integer operands, one modular tensor-core GEMM per modulus, Garner
+ * reconstruction with the alpha/beta epilogue. */
+int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
+              const char **path) {
+  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  int nmod = 0, beta_bits = 0;
+  if (!crt_plan(a->k, want, &nmod, &beta_bits)) return HCBK_ERR_ARGS;
+  const int *mods = hcbk_crt_moduli(nullptr);
+  const int64_t kp = (a->k + 7) & ~int64_t(7); /* 16-byte f16 row pitch */
+  auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
+  const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
+  const size_t t_pl = up1k((size_t)a->m * a->n * 2);
+  const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
+  const size_t total = ea_bytes + eb_bytes + nmod * (a_pl + b_pl + t_pl);
+  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  int *err = device_error_flag(st);
+  if (!ws || !err) return HCBK_ERR_NOMEM;
+  int *exp_a = reinterpret_cast<int *>(ws);
+  int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
+  char *pa_base = ws + ea_bytes + eb_bytes;
+  char *pb_base = pa_base + nmod * a_pl;
+  char *t_base = pb_base + nmod * b_pl;
+
+  hcbk_ozaki_prep ea;
+  std::memset(&ea, 0, sizeof(ea));
+  ea.src = static_cast<const double *>(a->a) + a->a_off;
+  ea.ld = a->lda;
+  ea.k_contig = a->op_a != HCBK_OP_N;
+  ea.rows = a->m;
+  ea.kdim = a->k;
+  ea.exps = exp_a;
+  hcbk_ozaki_prep eb = ea;
+  eb.src = static_cast<const double *>(a->b) + a->b_off;
+  eb.ld = a->ldb;
+  eb.k_contig = a->op_b == HCBK_OP_N;
+  eb.rows = a->n;
+  eb.exps = exp_b;
+  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); });
+  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); });
+  if (rc) return rc;
+
+  hcbk_crt_prep ra;
+  ra.src = ea.src;
+  ra.ld = ea.ld;
+  ra.k_contig = ea.k_contig;
+  ra.rows = a->m;
+  ra.kdim = a->k;
+  ra.exps = exp_a;
+  ra.beta_bits = beta_bits;
+  ra.nmod = nmod;
+  ra.planes = pa_base;
+  ra.plane_stride = (int64_t)a_pl;
+  ra.ld_dst = kp;
+  hcbk_crt_prep rb = ra;
+  rb.src = eb.src;
+  rb.ld = eb.ld;
+  rb.k_contig = eb.k_contig;
+  rb.rows = a->n;
+  rb.exps = exp_b;
+  rb.planes = pb_base;
+  rb.plane_stride = (int64_t)b_pl;
+  rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&ra, stream); });
+  if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
+  if (rc) return rc;
+
+  for (int i = 0; i < nmod && !rc; ++i) {
+    hcbk_crt_gemm g;
+    g.m = a->m;
+    g.n = a->n;
+    g.k = a->k;
+    g.a_plane = pa_base + i * a_pl;
+    g.b_plane = pb_base + i * b_pl;
+    g.ld_a = kp;
+    g.ld_b = kp;
+    g.modulus = mods[i];
+    g.t = reinterpret_cast<int16_t *>(t_base + i * t_pl);
+    g.ldt = a->m;
+    rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
+  }
+  if (rc) return rc;
+
+  hcbk_crt_combine_args cb;
+  cb.m = a->m;
+  cb.n = a->n;
+  cb.nmod = nmod;
+  cb.res = reinterpret_cast<const int16_t *>(t_base);
+  cb.res_plane = (int64_t)(t_pl / 2);
+  cb.ldr = a->m;
+  cb.exp_a = exp_a;
+  cb.exp_b = exp_b;
+  cb.shift = 2 * beta_bits;
+  cb.c = static_cast<double *>(a->c) + a->c_off;
+  cb.ldc = a->ldc;
+  cb.alpha = a->alpha_re;
+  cb.beta = a->beta_re;
+  static const char *names[HCBK_CRT_MAX_MODULI + 1] = {
+      "", "", "", "", "", "", "", "", "tc.crt_m8", "tc.crt_m9", "tc.crt_m10", "tc.crt_m11",
+      "tc.crt_m12", "tc.crt_m13", "tc.crt_m14", "tc.crt_m15", "tc.crt_m16", "tc.crt_m17",
+      "tc.crt_m18", "tc.crt_m19", "tc.crt_m20"};
+  *path = names[nmod];
+  return timed_launch(st, stream, "crt.combine", [&] { return hcbk_crt_combine(&cb, stream); });
+}
+
 }  // namespace
 
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
@@ -228,6 +364,12 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     int rc = dgemm_ozaki(st, a, s, f16, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] ozaki path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_D && st->math_mode == 4 /* HCBLAS_MATH_OZAKI_CRT */ && a->batch == 1 &&
+      !a->a_array) {
+    int rc = dgemm_crt(st, a, st->math_param, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] crt path declined (%d)\n", rc);
   }
   return simt(st, a, stream, path);
 }

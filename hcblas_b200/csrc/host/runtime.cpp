@@ -16,6 +16,7 @@
 
 #include "../../../include/hcblas.h"
 #include "../../../include/hcblaslib.h"
+#include "../kernels/hcbk.h"
 #include "state.h"
 
 namespace hcblas_b200 {
@@ -330,7 +331,9 @@ extern "C" hcblasStatus_t hcblasGetMatrix(hcblasHandle_t handle, int rows, int c
 extern "C" hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param) {
   if (handle == nullptr || !handle->initialized || !handle->impl)
     return HCBLAS_STATUS_NOT_INITIALIZED;
-  if (mode < HCBLAS_MATH_NATIVE || mode > HCBLAS_MATH_OZAKI_F16)
+  if (mode < HCBLAS_MATH_NATIVE || mode > HCBLAS_MATH_OZAKI_CRT)
+    return HCBLAS_STATUS_INVALID_VALUE;
+  if (mode == HCBLAS_MATH_OZAKI_CRT && (param < 0 || param > HCBK_CRT_MAX_MODULI || (param > 0 && param < 8)))
     return HCBLAS_STATUS_INVALID_VALUE;
   if (mode == HCBLAS_MATH_SPLIT_BF16 && !(param == 0 || param == 3 || param == 6))
     return HCBLAS_STATUS_INVALID_VALUE;

@@ -172,6 +172,61 @@ int hcbk_ozaki16_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream);
 /* largest K per launch for s slices (INT32 exactness), multiple of 64 */
 int64_t hcbk_ozaki_max_k(int slices);
 
+/* ----------------------------------------- CRT (Ozaki scheme II) DGEMM -- */
+
+#define HCBK_CRT_MAX_MODULI 20
+
+/* The library's moduli (pairwise coprime, odd, <= 255), largest first. */
+const int *hcbk_crt_moduli(int *count);
+
+/* Residues of the scaled integer operand: for row r (exponent exps[r], from
+ * hcbk_ozaki_exponents) A'(r,k) = rint(x(r,k) * 2^(beta_bits - exps[r])) and
+ * plane i holds the symmetric residue A' mod moduli[i] as binary16 at
+ * [r*ld_dst + k] (planes plane_stride bytes apart). */
+typedef struct hcbk_crt_prep {
+  const double *src;
+  int64_t ld;
+  int k_contig;
+  int64_t rows, kdim;
+  const int *exps;
+  int beta_bits;
+  int nmod;
+  void *planes;
+  int64_t plane_stride; /* bytes */
+  int64_t ld_dst;       /* elements */
+} hcbk_crt_prep;
+int hcbk_crt_residues(const hcbk_crt_prep *a, void *stream);
+
+/* One modulus: T = A_res * B_res mod p on the f16 tensor path, written as
+ * symmetric int16 residues, column-major M x N with leading dimension ldt. */
+typedef struct hcbk_crt_gemm {
+  int64_t m, n, k;
+  const void *a_plane; /* M rows x ld_a f16, K contiguous */
+  const void *b_plane; /* N rows x ld_b f16, K contiguous */
+  int64_t ld_a, ld_b;
+  int modulus;
+  int16_t *t;
+  int64_t ldt;
+} hcbk_crt_gemm;
+int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
+
+/* Garner reconstruction of P' from the residue planes and the epilogue
+ * C = alpha * P' * 2^(exp_a[m] + exp_b[n] - shift) + beta * C. */
+typedef struct hcbk_crt_combine_args {
+  int64_t m, n;
+  int nmod;
+  const int16_t *res;
+  int64_t res_plane; /* elements between planes */
+  int64_t ldr;
+  const int *exp_a;
+  const int *exp_b;
+  int shift; /* 2 * beta_bits */
+  double *c;
+  int64_t ldc;
+  double alpha, beta;
+} hcbk_crt_combine_args;
+int hcbk_crt_combine(const hcbk_crt_combine_args *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

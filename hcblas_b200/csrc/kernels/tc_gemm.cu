@@ -61,6 +61,9 @@ struct TcParams {
   double alpha_d, beta_d;
   const int *exp_a;
   const int *exp_b;
+  /* modular (CRT) epilogue */
+  int modulus;
+  float inv_modulus;
 };
 
 /* ---------------------------------------------------------- recipes -- */
@@ -137,6 +140,7 @@ __device__ __forceinline__ float load_out(const __half *p) { return __half2float
 
 /* f32 accumulator -> alpha*acc + beta*C in OutT (float or half) */
 template <typename OutT> struct EpiAlphaBeta {
+  using AccT = float; /* register accumulator of the promoting path */
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
     static_assert(NACC == 1, "several accumulators need the promoting epilogue");
@@ -182,7 +186,8 @@ template <typename OutT> struct EpiAlphaBeta {
    * a*BN + j of this thread's lane, with IEEE round-to-nearest adds: the
    * promotion step of the chunked accumulation */
   template <int BN, int NACC>
-  static __device__ __forceinline__ void accumulate(uint32_t tbase, float (&acc)[BN]) {
+  static __device__ __forceinline__ void accumulate(const TcParams &, uint32_t tbase,
+                                                    float (&acc)[BN], int /* chunk */) {
 #pragma unroll
     for (int c = 0; c < BN; c += 32) {
       float part[32];
@@ -219,6 +224,65 @@ template <typename OutT> struct EpiAlphaBeta {
  *   C = alpha * 2^(ea_m + eb_n) * sum_d 2^(-7(d+2)) acc_d + beta * C   (FP64)
  * The group terms are exact in binary64 (|acc_d| < 2^31, power-of-two
  * weights) and are added smallest weight first. */
+/* Modular epilogue of the CRT scheme.  With f16 residues |r| <= 127
+ * (moduli <= 255) every f32 chunk sum over 1024 K elements is an exact
+ * integer below 2^24.  It is reduced modulo p on the FP32 pipe -- q =
+ * rint(s / p) by the 1.5 * 2^23 rounding constant, r = fma(-q, p, s), exact
+ * because r is a small integer -- and added to an f32 register accumulator
+ * that stays a small exact integer.  The final residues are stored as
+ * symmetric int16 values (C viewed as the column-major int16 residue plane).
+ * No float->int conversion runs per chunk. */
+struct EpiModP {
+  using AccT = float;
+  static constexpr float RND = 12582912.0f; /* 1.5 * 2^23 */
+
+  /* exact x mod p into (-p, p) for integral |x| < 2^24 */
+  static __device__ __forceinline__ float mod_f(float x, float p, float inv_p) {
+    const float q = fmaf(x, inv_p, RND) - RND;
+    return fmaf(-q, p, x);
+  }
+
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void run(const TcParams &, uint32_t, int, int) {
+    static_assert(NACC == 0, "the modular epilogue only runs on the promoting path");
+  }
+
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void accumulate(const TcParams &p, uint32_t tbase,
+                                                    float (&acc)[BN], int /* chunk */) {
+    const float pf = static_cast<float>(p.modulus);
+#pragma unroll
+    for (int c = 0; c < BN; c += 32) {
+      uint32_t r[32];
+      tmem_ld_32x32b_x32(tbase + c, r);
+      tmem_ld_wait();
+      /* each reduced chunk lies in (-p, p): the f32 sum stays an exact
+       * integer for up to 2^16 chunks (K < 2^26) */
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[c + j] += mod_f(__uint_as_float(r[j]), pf, p.inv_modulus);
+    }
+  }
+
+  template <int BN>
+  static __device__ __forceinline__ void store_acc(const TcParams &p, const float (&acc)[BN],
+                                                   int m, int n0) {
+    if (m >= p.m) return;
+    int16_t *T = static_cast<int16_t *>(p.c) + (long long)m + (long long)n0 * p.ldc;
+    const int nvalid = p.n - n0;
+    const int hp = (p.modulus - 1) >> 1;
+    const float pf = static_cast<float>(p.modulus);
+#pragma unroll
+    for (int j = 0; j < BN; ++j) {
+      if (j < nvalid) {
+        int v = static_cast<int>(mod_f(acc[j], pf, p.inv_modulus)); /* exact, |v| < p */
+        if (v > hp) v -= p.modulus;
+        else if (v < -hp) v += p.modulus;
+        T[(long long)j * p.ldc] = static_cast<int16_t>(v);
+      }
+    }
+  }
+};
+
 /* 2^e built from its binary64 bit pattern (exact; normal range
  * -1022 <= e <= 1023 only).  Deliberately not recursive: device recursion
  * consumes the (1 KB default) call stack. */
@@ -507,9 +571,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         __syncwarp();
         if (lane == 0) mbar_arrive(&tempty[b]);
       } else {
-        float acc[BN];
+        typename EPI::AccT acc[BN];
 #pragma unroll
-        for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+        for (int j = 0; j < BN; ++j) acc[j] = 0;
         for (int kc = 0; kc < kblocks; kc += chunk_kb, ++ci) {
           const int b = ci % NBUF;
           const uint32_t tph = (ci / NBUF) & 1;
@@ -519,7 +583,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           }
           tc_fence_after();
           EPI::template accumulate<BN, R::NACC>(
-              tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS, acc);
+              p, tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS, acc,
+              kc / chunk_kb);
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&tempty[b]);
@@ -757,4 +822,30 @@ extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stre
     case 8: return launch_tc<64, 2, RecipeOzaki<8>, 2, EpiOzaki, 0, 1>(p, stream);
     default: return HCBK_ERR_ARGS;
   }
+}
+
+/* One modulus of the CRT scheme: f16 residue planes (K-major, |r| <= 127),
+ * FP32 chunk sums exact over 1024-element K chunks (PROMOTE_KB = 16 slabs of
+ * 64: 1024 * 127^2 < 2^24), reduced mod p in registers, int16 residues out.
+ * K below 2^25 keeps the register sums (|chunk residue| < 1.5 p) exact. */
+extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) {
+  if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k >= (1LL << 25) || g->k <= 0 ||
+      g->modulus < 3 || g->modulus > 255 || (g->modulus & 1) == 0)
+    return HCBK_ERR_ARGS;
+  TcParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = (int)g->m;
+  p.n = (int)g->n;
+  p.k = (int)g->k;
+  const auto F16 = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  int rc = make_map(&p.ta[0], F16, 2, g->a_plane, g->k, g->m, g->ld_a, 64, BM);
+  if (rc) return rc;
+  rc = make_map(&p.tb[0], F16, 2, g->b_plane, g->k, g->n, g->ld_b, 64, 128);
+  if (rc) return rc;
+  p.c = g->t;
+  p.ldc = g->ldt;
+  p.modulus = g->modulus;
+  p.inv_modulus = 1.0f / (float)g->modulus;
+  p.err = err;
+  return launch_tc<128, 6, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);
 }

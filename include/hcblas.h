@@ -286,12 +286,20 @@ int hcblasLibGemmBatched(hcblasHandle_t h, int dtype, int order, char typeA, cha
  *                          in binary16, products on the tcgen05 f16 path with
  *                          FP32 sums kept exact (integers < 2^24) and promoted
  *                          to FP64 per 32-element K slab (`param` = 3..7
- *                          slices of 8 bits; 0 = 7 slices, 56 bits). */
+ *                          slices of 8 bits; 0 = 7 slices, 56 bits)
+ *   HCBLAS_MATH_OZAKI_CRT  D: integer-modular (CRT) scheme: operands scaled
+ *                          to beta-bit integers per row/column, residues
+ *                          modulo pairwise-coprime odd moduli <= 255 in
+ *                          binary16, one exact tensor-core GEMM per modulus,
+ *                          Garner reconstruction in double-double
+ *                          (`param` = number of moduli 8..20; 0 = the fewest
+ *                          giving beta = 53 bits for the call's K). */
 enum {
   HCBLAS_MATH_NATIVE = 0,
   HCBLAS_MATH_SPLIT_BF16 = 1,
   HCBLAS_MATH_OZAKI_INT8 = 2,
-  HCBLAS_MATH_OZAKI_F16 = 3
+  HCBLAS_MATH_OZAKI_F16 = 3,
+  HCBLAS_MATH_OZAKI_CRT = 4
 };
 hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param);
 hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);

@@ -134,6 +134,88 @@ def test_ozaki_long_k(handle, kind):
     assert err <= ozaki_bound(O.COL, 1, 0, M, N, K, 1.0, A, lda, B, ldb, s, ref, kind, 1.0, C, ldc)
 
 
+CRT_MODULI = [255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193, 191, 181,
+              179, 173, 167]
+CRT_CASES = CASES + [(O.COL, 0, 1, 160, 96, 2500)]  # K over two 1024-element chunks
+
+
+def crt_plan(K, want=0):
+    """Moduli count and integer width beta, as the library chooses them."""
+    lk = np.ceil(np.log2(max(K, 2)))
+    cum = 0.0
+    for i, p in enumerate(CRT_MODULI):
+        cum += np.log2(p)
+        b = min(53, int(np.floor((cum - 1.0 - lk - 0.01) / 2.0)))
+        if (want == 0 and b >= 53) or want == i + 1:
+            return i + 1, b
+    return len(CRT_MODULI), min(53, int(np.floor((cum - 1.0 - lk - 0.01) / 2.0)))
+
+
+def crt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta_bits, ref, beta=0.0, C=None,
+              ldc=None):
+    """|alpha| K 2^(e_m + f_n) (2^-beta + 2^-2beta) + 4u|C| (+ 2u|beta C|)."""
+    Ad = op_dense(A, order, ta, M, K, lda, 0)
+    Bd = op_dense(B, order, tb, K, N, ldb, 0)
+    ea = np.frexp(np.max(np.abs(Ad), axis=1))[1].astype(np.float64)
+    eb = np.frexp(np.max(np.abs(Bd), axis=0))[1].astype(np.float64)
+    scale = np.exp2(ea[:, None] + eb[None, :])
+    elem = abs(alpha) * K * scale * (2.0 ** -beta_bits + 2.0 ** (-2 * beta_bits))
+    out = np.linalg.norm(elem) + 4 * U * np.linalg.norm(ref)
+    if beta and C is not None:
+        out += 2 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
+    return out
+
+
+def run_crt(handle, want, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C, ldc):
+    assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, want) == 0
+    try:
+        dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+        rc = hb.lib_gemm(handle, order, TCH[ta], TCH[tb], M, N, K, alpha, dA, lda, dB, ldb, beta,
+                         dC, ldc)
+        assert rc == 0
+        assert hb.device_error(handle) == 0
+        return dC.download(), hb.hcblasGetLastPath(handle)
+    finally:
+        hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+
+
+@pytest.mark.parametrize("want", [0, 10, 12, 14, 16, 18, 20])
+def test_crt_vs_dd_oracle(handle, want):
+    rng = np.random.default_rng(900 + want)
+    for order, ta, tb, M, N, K in CRT_CASES:
+        A, lda, B, ldb, C, ldc = make_case(rng, "d", order, ta, tb, M, N, K)
+        alpha, beta = 1.5, -0.25
+        nmod, bb = crt_plan(K, want)
+        got, path = run_crt(handle, want, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C,
+                            ldc)
+        assert path == f"tc.crt_m{nmod}", path
+        _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+        err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
+        bound = crt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, bb, ref, beta, C, ldc)
+        assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
+
+
+def test_crt_special_and_hard_range(handle):
+    rng = np.random.default_rng(12)
+    M, N, K = 96, 80, 700
+    A = rng.standard_normal(M * K) * np.exp2(rng.integers(-20, 21, M))[np.arange(M * K) % M]
+    B = rng.standard_normal(K * N) * np.exp2(rng.integers(-20, 21, N))[np.arange(K * N) // K]
+    A[4 + np.arange(K) * M] = 0.0  # zero row
+    A[9 + 3 * M] = np.inf          # non-finite row
+    C = np.ones(M * N)
+    got, _ = run_crt(handle, 0, O.COL, 0, 0, M, N, K, 1.0, 0.5, A, M, B, K, C, M)
+    gv = O.view_c(got, O.COL, M, N, M)
+    assert np.all(np.isnan(gv[9, :]))
+    assert np.all(gv[4, :] == 0.5)
+    ok = np.ones(M, bool)
+    ok[9] = False
+    A0 = np.where(np.isfinite(A), A, 0.0)
+    _, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, 0.5, C, M)
+    _, bb = crt_plan(K)
+    bound = crt_bound(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, bb, ref, 0.5, C, M)
+    assert np.linalg.norm(gv[ok] - ref[ok]) <= bound
+
+
 def test_ozaki_vs_native_accuracy(handle):
     """Config of the headline: col-major N/T, N(0,1); errors of native FP64
     and of the Ozaki paths against the double-double oracle."""
@@ -149,6 +231,11 @@ def test_ozaki_vs_native_accuracy(handle):
     for kind, s in (("i8", 6), ("i8", 7), ("i8", 8), ("f16", 6), ("f16", 7)):
         got, _ = run_ozaki(handle, kind, s, O.COL, 0, 1, M, N, K, 1.0, 0.0, A, M, B, N, C, M)
         errs[f"{kind}_s{s}"] = O.normwise_rel_error(O.view_c(got, O.COL, M, N, M), ref)
+    for want in (0, 14, 15):
+        got, path = run_crt(handle, want, O.COL, 0, 1, M, N, K, 1.0, 0.0, A, M, B, N, C, M)
+        errs[path] = O.normwise_rel_error(O.view_c(got, O.COL, M, N, M), ref)
     print("native vs ozaki normwise errors:", errs)
     assert errs["i8_s8"] <= errs["native"] * 4
     assert errs["f16_s7"] <= errs["native"] * 4
+    nmod, _ = crt_plan(K)
+    assert errs[f"tc.crt_m{nmod}"] <= errs["native"]
