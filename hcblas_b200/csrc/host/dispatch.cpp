@@ -44,6 +44,14 @@ int simt(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char 
   return timed_launch(st, stream, *path, [&] { return hcbk_gemm_simt(a, cfg, stream); });
 }
 
+/* CTA pairs (256-row tiles) once the problem has enough of them to fill
+ * every SM pair; tc_pair = 2 forces them, 0 disables them. */
+bool use_pair(const HcblasB200State *st, int64_t m, int64_t n, int64_t bn) {
+  if (st->tc_pair == 0) return false;
+  if (st->tc_pair == 2) return true;
+  return tiles_of(m, n, 256, bn) >= hcbk_sm_count() / 2;
+}
+
 /* HGEMM on tcgen05 with operands read in place by TMA. */
 int hgemm_tc(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
   if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
@@ -52,9 +60,11 @@ int hgemm_tc(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const c
     return HCBK_ERR_ALIGN;
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;
-  const int bn = tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
-  *path = bn == 256 ? "tc.h.128x256" : "tc.h.128x128";
-  return timed_launch(st, stream, *path, [&] { return hcbk_hgemm_tc(a, bn, err, stream); });
+  const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
+  const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  *path = pair ? "tc.h.256x256.pair" : bn == 256 ? "tc.h.128x256" : "tc.h.128x128";
+  return timed_launch(st, stream, *path,
+                      [&] { return hcbk_hgemm_tc(a, bn, pair, err, stream); });
 }
 
 /* Split-BF16 SGEMM: split both operands into bf16 planes (K-major), then one
@@ -105,6 +115,7 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   g.terms = terms;
   g.bn = 128;
   g.promote_kb = st->split_promote_kb;
+  g.pair = use_pair(st, a->m, a->n, 128) ? 1 : 0;
   for (int i = 0; i < 3; ++i) {
     g.a_planes[i] = pa.planes[i];
     g.b_planes[i] = pb.planes[i];
@@ -115,8 +126,12 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   g.ldc = a->ldc;
   g.alpha = a->alpha_re;
   g.beta = a->beta_re;
-  if (terms == 6) *path = g.promote_kb == 4 ? "tc.split_bf16x6.128x128.p4" : "tc.split_bf16x6.128x128.p1";
-  else *path = g.promote_kb == 4 ? "tc.split_bf16x3.128x128.p4" : "tc.split_bf16x3.128x128.p1";
+  static const char *names[2][2][2] = {
+      {{"tc.split_bf16x3.128x128.p1", "tc.split_bf16x3.128x128.p4"},
+       {"tc.split_bf16x3.256x128.pair.p1", "tc.split_bf16x3.256x128.pair.p4"}},
+      {{"tc.split_bf16x6.128x128.p1", "tc.split_bf16x6.128x128.p4"},
+       {"tc.split_bf16x6.256x128.pair.p1", "tc.split_bf16x6.256x128.pair.p4"}}};
+  *path = names[terms == 6][g.pair][g.promote_kb == 4];
   return timed_launch(st, stream, *path, [&] { return hcbk_sgemm_split_tc(&g, err, stream); });
 }
 
@@ -303,6 +318,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
   if (rc) return rc;
 
+  const int pair = use_pair(st, a->m, a->n, 128) ? 1 : 0;
   for (int i = 0; i < nmod && !rc; ++i) {
     hcbk_crt_gemm g;
     g.m = a->m;
@@ -315,6 +331,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
     g.modulus = mods[i];
     g.t = reinterpret_cast<int16_t *>(t_base + i * t_pl);
     g.ldt = a->m;
+    g.pair = pair;
     rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   }
   if (rc) return rc;

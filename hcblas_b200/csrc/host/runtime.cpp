@@ -364,6 +364,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->split_promote_kb = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "tc_pair") == 0) {
+    if (value < 0 || value > 2) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->tc_pair = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   return HCBLAS_STATUS_INVALID_VALUE;
 }
 

@@ -83,9 +83,11 @@ int hcbk_sm_count(void);
  * Requirements (else HCBK_ERR_ALIGN / HCBK_ERR_ARGS and the caller falls
  * back to hcbk_gemm_simt): batch == 1, base pointers (after offsets) 16-byte
  * aligned, lda/ldb multiples of 8 elements.  `bn` = 128 or 256.
+ * `pair` = 1 runs CTA pairs (tcgen05 cta_group::2, 256 x bn tiles, bn = 256
+ * only), 0 single CTAs (128 x bn tiles).
  * `err` is a device int that receives a nonzero code if a pipeline wait
  * times out (the kernel then exits instead of hanging). */
-int hcbk_hgemm_tc(const hcbk_gemm_args *args, int bn, int *err, void *stream);
+int hcbk_hgemm_tc(const hcbk_gemm_args *args, int bn, int pair, int *err, void *stream);
 
 /* Split-BF16 SGEMM: operands already split into bf16 planes, K-major:
  * a_planes[t] is M rows x ld_a elements (row m holds op(A)(m, 0..K-1)),
@@ -96,6 +98,7 @@ typedef struct hcbk_split_gemm {
   int terms;
   int bn;         /* 128 */
   int promote_kb; /* K-slabs (64 elements) per TMEM chunk: 1 or 4 */
+  int pair;       /* 1: CTA pairs, 256 x bn tiles */
   const void *a_planes[3];
   const void *b_planes[3];
   int64_t ld_a, ld_b;
@@ -207,6 +210,7 @@ typedef struct hcbk_crt_gemm {
   int modulus;
   int16_t *t;
   int64_t ldt;
+  int pair; /* 1: CTA pairs, 256 x 128 tiles */
 } hcbk_crt_gemm;
 int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
 

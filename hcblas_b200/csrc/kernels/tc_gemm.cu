@@ -371,12 +371,15 @@ __host__ __device__ constexpr uint32_t tmem_cols_for(uint32_t c) {
 }
 
 /* NBUF: TMEM accumulator sets (2 = the epilogue of one tile/chunk overlaps
- * the MMAs of the next; 1 when the accumulators fill TMEM) */
-template <int BN, int STAGES, class R, int KIND, int NBUF = 2>
+ * the MMAs of the next; 1 when the accumulators fill TMEM).
+ * CG: CTAs per MMA (1, or 2 for a CTA pair computing a 256 x BN tile; each
+ * CTA of a pair holds 128 rows of A and BN/2 rows of B per stage). */
+template <int BN, int STAGES, class R, int KIND, int NBUF = 2, int CG = 1>
 struct TcCfg {
   using KT = KindTraits<KIND>;
   static constexpr uint32_t A_PLANE = BM * KT::ROWB;
-  static constexpr uint32_t B_PLANE = BN * KT::ROWB;
+  static constexpr uint32_t B_ROWS = BN / CG;
+  static constexpr uint32_t B_PLANE = B_ROWS * KT::ROWB;
   static constexpr uint32_t STAGE_BYTES = R::NA * A_PLANE + R::NB * B_PLANE;
   static constexpr uint32_t ACC_COLS = R::NACC * BN;
   static constexpr uint32_t TMEM_COLS = tmem_cols_for(NBUF * ACC_COLS);
@@ -384,6 +387,7 @@ struct TcCfg {
   static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
   static_assert(NBUF * ACC_COLS <= 512, "accumulators exceed TMEM");
   static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "BN");
+  static_assert(CG == 1 || (CG == 2 && KIND != 2 && !R::P3D && BN % 128 == 0), "CTA pair");
   static_assert(SMEM_BYTES <= 232448, "shared memory");
 };
 
@@ -397,9 +401,10 @@ struct TcCfg {
  *   spans only n*128 bytes of K, which bounds the error it adds; used by the
  *   split-BF16 paths, whose contract is "error no worse than FP32".
  */
-template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2>
+template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
+          int CG = 1>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
-  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF>;
+  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG>;
   using KT = typename Cfg::KT;
   constexpr int BKE = KT::BKE;
   constexpr int ROWB = KT::ROWB;
@@ -416,6 +421,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  /* CTA pair: rank 0 (the leader) issues the MMAs and owns the full and
+   * TMEM-empty barriers both CTAs' producers and epilogues signal */
+  const uint32_t rank = CG == 2 ? cluster_ctarank() : 0u;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -424,7 +432,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4);
+      mbar_init(&tempty[b], 4 * CG);
     }
     mbar_fence_init();
   }
@@ -434,15 +442,26 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     for (int i = 0; i < NMB; ++i) tma_prefetch_desc(&p.tb[i]);
   }
   if (warp == 1) {
-    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
-    tmem_relinquish();
+    if constexpr (CG == 2) {
+      tmem_alloc_pair(tmem_slot, Cfg::TMEM_COLS);
+      tmem_relinquish_pair();
+    } else {
+      tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+      tmem_relinquish();
+    }
   }
   tc_fence_before();
-  __syncthreads();
+  __syncwarp();
+  if constexpr (CG == 2)
+    cluster_sync(); /* the peer's barriers are initialised before any signal */
+  else
+    __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  /* persistent loop over output tiles of (BM * CG) x BN, one per CTA group */
   const int num_tiles = p.tiles_m * p.tiles_n;
+  const int tile0 = blockIdx.x / CG, tile_step = gridDim.x / CG;
   const int kblocks = (p.k + BKE - 1) / BKE;
   const int chunk_kb = PROMOTE_KB > 0 ? PROMOTE_KB : kblocks;
 
@@ -452,40 +471,49 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
-      for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
+      for (int t = tile0; ok && t < num_tiles; t += tile_step) {
         const int tm = t % p.tiles_m, tn = t / p.tiles_m;
+        const int row0 = (tm * CG + (int)rank) * BM;               /* this CTA's A rows */
+        const int col0 = tn * BN + (int)rank * (int)Cfg::B_ROWS;   /* this CTA's B rows */
         for (int kb = 0; kb < kblocks; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
             ok = false;
             break;
           }
-          mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
+          /* the leader's full barrier counts both CTAs' bytes */
+          if (rank == 0) mbar_expect_tx(&full[s], CG * Cfg::STAGE_BYTES);
           uint8_t *st = smem + s * Cfg::STAGE_BYTES;
           const int k0 = p.k0 + kb * BKE;
+          auto load2d = [&](uint8_t *dst, const CUtensorMap *map, int c0, int c1) {
+            if constexpr (CG == 2)
+              tma_load_2d_pair(dst, map, mapa_shared(&full[s], 0), c0, c1);
+            else
+              tma_load_2d(dst, map, &full[s], c0, c1);
+          };
 #pragma unroll
           for (int a = 0; a < R::NA; ++a) {
             uint8_t *dst = st + a * Cfg::A_PLANE;
             if constexpr (R::P3D) {
-              tma_load_3d(dst, &p.ta[0], &full[s], k0, tm * BM, a);
+              tma_load_3d(dst, &p.ta[0], &full[s], k0, row0, a);
             } else if (!p.a_mn) {
-              tma_load_2d(dst, &p.ta[a], &full[s], k0, tm * BM);
+              load2d(dst, &p.ta[a], k0, row0);
             } else {
 #pragma unroll
               for (int j = 0; j < BM / 64; ++j)
-                tma_load_2d(dst + j * (BKE * ROWB), &p.ta[a], &full[s], tm * BM + j * 64, k0);
+                load2d(dst + j * (BKE * ROWB), &p.ta[a], row0 + j * 64, k0);
             }
           }
 #pragma unroll
           for (int b = 0; b < R::NB; ++b) {
             uint8_t *dst = st + R::NA * Cfg::A_PLANE + b * Cfg::B_PLANE;
             if constexpr (R::P3D) {
-              tma_load_3d(dst, &p.tb[0], &full[s], k0, tn * BN, b);
+              tma_load_3d(dst, &p.tb[0], &full[s], k0, col0, b);
             } else if (!p.b_mn) {
-              tma_load_2d(dst, &p.tb[b], &full[s], k0, tn * BN);
+              load2d(dst, &p.tb[b], k0, col0);
             } else {
 #pragma unroll
-              for (int j = 0; j < BN / 64; ++j)
-                tma_load_2d(dst + j * (BKE * ROWB), &p.tb[b], &full[s], tn * BN + j * 64, k0);
+              for (int j = 0; j < (int)Cfg::B_ROWS / 64; ++j)
+                load2d(dst + j * (BKE * ROWB), &p.tb[b], col0 + j * 64, k0);
             }
           }
           if (++s == STAGES) {
@@ -497,8 +525,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
   } else if (warp == 1) {
     /* ------------------------------------------------ MMA issuer -- */
-    if (lane == 0) {
-      const uint32_t idesc = make_idesc(KT::CFMT, KT::ABFMT, p.a_mn != 0, p.b_mn != 0, BM, BN);
+    if (lane == 0 && rank == 0) {
+      const uint32_t idesc =
+          make_idesc(KT::CFMT, KT::ABFMT, p.a_mn != 0, p.b_mn != 0, BM * CG, BN);
       const uint32_t a_lbo = p.a_mn ? BKE * ROWB : 16, b_lbo = p.b_mn ? BKE * ROWB : 16;
       const uint32_t a_kstep = p.a_mn ? KT::UK * ROWB : KT::UK * KT::ESZ;
       const uint32_t b_kstep = p.b_mn ? KT::UK * ROWB : KT::UK * KT::ESZ;
@@ -506,7 +535,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       uint32_t ph = 0;
       int ci = 0; /* chunk counter (all tiles): selects the TMEM buffer */
       bool ok = true;
-      for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
+      for (int t = tile0; ok && t < num_tiles; t += tile_step) {
         for (int kc = 0; ok && kc < kblocks; kc += chunk_kb, ++ci) {
           const int b = ci % NBUF;
           const uint32_t tph = (ci / NBUF) & 1;
@@ -536,17 +565,27 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
                 const uint32_t acc = (kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
                 if constexpr (KIND == 2)
                   mma_i8(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
+                else if constexpr (CG == 2)
+                  mma_f16_pair(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
                 else
                   mma_f16(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
               }
             }
-            mma_commit(&empty[s]);
+            if constexpr (CG == 2)
+              mma_commit_pair(&empty[s], 0x3); /* frees the stage in both CTAs */
+            else
+              mma_commit(&empty[s]);
             if (++s == STAGES) {
               s = 0;
               ph ^= 1u;
             }
           }
-          if (ok) mma_commit(&tfull[b]);
+          if (ok) {
+            if constexpr (CG == 2)
+              mma_commit_pair(&tfull[b], 0x3);
+            else
+              mma_commit(&tfull[b]);
+          }
         }
       }
     }
@@ -555,9 +594,18 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     const int q = warp & 3; /* TMEM lane quadrant of this warp */
     int ci = 0;
     bool ok = true;
-    for (int t = blockIdx.x; ok && t < num_tiles; t += gridDim.x) {
+    /* TMEM buffer released to the leader's MMA thread */
+    auto release = [&](int b) {
+      if (lane == 0) {
+        if constexpr (CG == 2)
+          mbar_arrive_cluster(mapa_shared(&tempty[b], 0));
+        else
+          mbar_arrive(&tempty[b]);
+      }
+    };
+    for (int t = tile0; ok && t < num_tiles; t += tile_step) {
       const int tm = t % p.tiles_m, tn = t / p.tiles_m;
-      const int m = tm * BM + q * 32 + lane;
+      const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
       if constexpr (PROMOTE_KB == 0) {
         const int b = ci % NBUF;
         const uint32_t tph = (ci / NBUF) & 1;
@@ -569,7 +617,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN);
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[b]);
+        release(b);
       } else {
         typename EPI::AccT acc[BN];
 #pragma unroll
@@ -587,7 +635,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
               kc / chunk_kb);
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(&tempty[b]);
+          release(b);
         }
         if (ok) EPI::template store_acc<BN>(p, acc, m, tn * BN);
       }
@@ -595,10 +643,17 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   }
 
   tc_fence_before();
-  __syncthreads();
+  __syncwarp();
+  if constexpr (CG == 2)
+    cluster_sync(); /* neither CTA leaves while the pair still uses its memory */
+  else
+    __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+    if constexpr (CG == 2)
+      tmem_dealloc_pair(tmem_base, Cfg::TMEM_COLS);
+    else
+      tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
   }
 }
 
@@ -675,26 +730,55 @@ static int make_map_planes(CUtensorMap *map, const void *base, uint64_t kdim, ui
   return HCBK_OK;
 }
 
-template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2>
+template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
+          int CG = 1>
 static int launch_tc(TcParams &p, void *stream) {
-  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF>;
-  auto kern = tc_gemm_kernel<BN, STAGES, R, KIND, EPI, PROMOTE_KB, NBUF>;
+  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG>;
+  auto kern = tc_gemm_kernel<BN, STAGES, R, KIND, EPI, PROMOTE_KB, NBUF, CG>;
   static bool attr_set[64] = {false};
+  static int pair_slots[64] = {0}; /* co-resident CTA pairs per device */
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+  if (dev < 0 || dev >= 64) return HCBK_ERR_LAUNCH;
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CG;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(192, 1, 1);
+  cfg.dynamicSmemBytes = Cfg::SMEM_BYTES;
+  cfg.stream = static_cast<cudaStream_t>(stream);
+  cfg.attrs = attr;
+  cfg.numAttrs = CG == 2 ? 1 : 0;
+  if (!attr_set[dev]) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              Cfg::SMEM_BYTES) != cudaSuccess)
       return HCBK_ERR_LAUNCH;
+    if (CG == 2) {
+      /* SMs pair up within a GPC, so fewer than sm_count / 2 pairs may fit */
+      int clusters = 0;
+      cfg.gridDim = dim3(2 * (hcbk_sm_count() / 2), 1, 1);
+      if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        return HCBK_ERR_LAUNCH;
+      }
+      pair_slots[dev] = clusters;
+    }
     attr_set[dev] = true;
   }
-  p.tiles_m = (p.m + BM - 1) / BM;
+  p.tiles_m = (p.m + BM * CG - 1) / (BM * CG);
   p.tiles_n = (p.n + BN - 1) / BN;
   const int tiles = p.tiles_m * p.tiles_n;
-  int grid = hcbk_sm_count();
-  if (tiles < grid) grid = tiles;
-  kern<<<grid, 192, Cfg::SMEM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
-  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+  int groups = CG == 2 ? pair_slots[dev] : hcbk_sm_count();
+  if (tiles < groups) groups = tiles;
+  cfg.gridDim = dim3((unsigned)(groups * CG), 1, 1);
+  if (cudaLaunchKernelEx(&cfg, kern, p) != cudaSuccess) {
+    cudaGetLastError();
+    return HCBK_ERR_LAUNCH;
+  }
+  return HCBK_OK;
 }
 
 }  // namespace tc
@@ -703,7 +787,7 @@ static int launch_tc(TcParams &p, void *stream) {
 using namespace hcbk::tc;
 
 /* f16 operands straight from the caller's matrices (column-major canonical). */
-extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int *err, void *stream) {
+extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream) {
   if (a->dtype != HCBK_H || a->batch != 1 || a->a_array || a->op_a == HCBK_OP_C ||
       a->op_b == HCBK_OP_C)
     return HCBK_ERR_ARGS;
@@ -726,7 +810,8 @@ extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int *err, void *st
   else
     rc = make_map(&p.ta[0], F16, 2, A, a->k, a->m, a->lda, 64, BM);
   if (rc) return rc;
-  const uint32_t bn_box = (uint32_t)bn;
+  if ((bn != 128 && bn != 256) || (pair && bn != 256)) return HCBK_ERR_ARGS;
+  const uint32_t bn_box = (uint32_t)(pair ? bn / 2 : bn); /* B rows per CTA */
   if (p.b_mn)
     rc = make_map(&p.tb[0], F16, 2, B, a->n, a->k, a->ldb, 64, 64);
   else
@@ -738,9 +823,10 @@ extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int *err, void *st
   p.beta = (float)a->beta_re;
   p.beta_nonzero = a->beta_re != 0.0;
   p.err = err;
-  if (bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EpiAlphaBeta<__half>>(p, stream);
-  if (bn == 128) return launch_tc<128, 6, RecipeSingle, 0, EpiAlphaBeta<__half>>(p, stream);
-  return HCBK_ERR_ARGS;
+  using EH = EpiAlphaBeta<__half>;
+  if (pair) return launch_tc<256, 6, RecipeSingle, 0, EH, 0, 2, 2>(p, stream);
+  if (bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EH>(p, stream);
+  return launch_tc<128, 6, RecipeSingle, 0, EH>(p, stream);
 }
 
 /* split-BF16 SGEMM on pre-split K-major planes:
@@ -756,11 +842,12 @@ extern "C" int hcbk_sgemm_split_tc(const hcbk_split_gemm *g, int *err, void *str
   p.b_mn = 0;
   const auto BF16 = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   const int planes = g->terms == 6 ? 3 : 2;
-  const uint32_t bn = (uint32_t)g->bn;
+  if (g->bn != 128) return HCBK_ERR_ARGS;
+  const uint32_t bn_box = g->pair ? 64u : 128u; /* B rows per CTA */
   for (int i = 0; i < planes; ++i) {
     int rc = make_map(&p.ta[i], BF16, 2, g->a_planes[i], g->k, g->m, g->ld_a, 64, BM);
     if (rc) return rc;
-    rc = make_map(&p.tb[i], BF16, 2, g->b_planes[i], g->k, g->n, g->ld_b, 64, bn);
+    rc = make_map(&p.tb[i], BF16, 2, g->b_planes[i], g->k, g->n, g->ld_b, 64, bn_box);
     if (rc) return rc;
   }
   p.c = g->c;
@@ -770,8 +857,15 @@ extern "C" int hcbk_sgemm_split_tc(const hcbk_split_gemm *g, int *err, void *str
   p.beta_nonzero = g->beta != 0.0;
   p.err = err;
   /* two accumulators per chunk, double-buffered: 2 x 2 x 128 TMEM columns */
-  if (g->bn != 128) return HCBK_ERR_ARGS;
   using EF = EpiAlphaBeta<float>;
+  if (g->pair) {
+    if (g->terms == 6) {
+      if (g->promote_kb == 4) return launch_tc<128, 3, RecipeBf16x6, 1, EF, 4, 2, 2>(p, stream);
+      return launch_tc<128, 3, RecipeBf16x6, 1, EF, 1, 2, 2>(p, stream);
+    }
+    if (g->promote_kb == 4) return launch_tc<128, 4, RecipeBf16x3, 1, EF, 4, 2, 2>(p, stream);
+    return launch_tc<128, 4, RecipeBf16x3, 1, EF, 1, 2, 2>(p, stream);
+  }
   if (g->terms == 6) {
     if (g->promote_kb == 4) return launch_tc<128, 2, RecipeBf16x6, 1, EF, 4>(p, stream);
     return launch_tc<128, 2, RecipeBf16x6, 1, EF, 1>(p, stream);
@@ -840,12 +934,13 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
   const auto F16 = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   int rc = make_map(&p.ta[0], F16, 2, g->a_plane, g->k, g->m, g->ld_a, 64, BM);
   if (rc) return rc;
-  rc = make_map(&p.tb[0], F16, 2, g->b_plane, g->k, g->n, g->ld_b, 64, 128);
+  rc = make_map(&p.tb[0], F16, 2, g->b_plane, g->k, g->n, g->ld_b, 64, g->pair ? 64 : 128);
   if (rc) return rc;
   p.c = g->t;
   p.ldc = g->ldt;
   p.modulus = g->modulus;
   p.inv_modulus = 1.0f / (float)g->modulus;
   p.err = err;
+  if (g->pair) return launch_tc<128, 8, RecipeSingle, 0, EpiModP, 16, 2, 2>(p, stream);
   return launch_tc<128, 6, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);
 }

@@ -307,11 +307,15 @@ hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
 /* Extension: set a named tuning knob on the handle.
  *   "split_promote_kb"  split-BF16 paths: 64-element K-slabs accumulated in
  *                       TMEM before each promotion to the IEEE f32
- *                       accumulator (1 or 4; default 1). */
+ *                       accumulator (1 or 4; default 1).
+ *   "tc_pair"           tensor-core paths (HGEMM, split-BF16, CRT): CTA-pair
+ *                       kernels (tcgen05 cta_group::2, 256-row tiles over two
+ *                       SMs): 0 never, 1 when the problem fills every SM pair
+ *                       (default), 2 always. */
 hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char *name, int value);
 
 /* Extension: the path the last GEMM call on this handle took (a short static
- * string such as "simt.d.128x128" or "tc.f16.128x256"). */
+ * string such as "simt.d.128x128" or "tc.h.256x256.pair"). */
 const char *hcblasGetLastPath(hcblasHandle_t handle);
 
 /* Extension: library version string. */

@@ -195,6 +195,23 @@ def test_crt_vs_dd_oracle(handle, want):
         assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
 
 
+def test_crt_pair_matches_single_cta(handle):
+    """The CRT residue GEMMs are exact, so CTA-pair and single-CTA kernels
+    must give bit-identical results."""
+    rng = np.random.default_rng(31)
+    for order, ta, tb, M, N, K in CRT_CASES:
+        A, lda, B, ldb, C, ldc = make_case(rng, "d", order, ta, tb, M, N, K)
+        outs = []
+        for pair in (0, 2):
+            assert hb.set_tuning(handle, "tc_pair", pair) == 0
+            try:
+                outs.append(run_crt(handle, 0, order, ta, tb, M, N, K, 1.5, -0.25, A, lda, B, ldb,
+                                    C, ldc)[0])
+            finally:
+                hb.set_tuning(handle, "tc_pair", 1)
+        assert np.array_equal(outs[0], outs[1]), (order, ta, tb, M, N, K)
+
+
 def test_crt_special_and_hard_range(handle):
     rng = np.random.default_rng(12)
     M, N, K = 96, 80, 700

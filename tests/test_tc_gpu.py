@@ -57,14 +57,25 @@ def run(handle, kind, order, ta, tb, M, N, K, alpha, beta, rng, ld_align=8):
 HSHAPES = [(128, 128, 64), (256, 512, 128), (1000, 777, 333), (129, 65, 17), (3000, 2500, 200)]
 
 
+@pytest.fixture
+def pair_mode(handle, request):
+    """tc_pair tuning knob: 0 = single-CTA kernels, 2 = CTA pairs
+    (tcgen05 cta_group::2) for every shape; restored to auto afterwards."""
+    assert hb.set_tuning(handle, "tc_pair", request.param) == 0
+    yield request.param
+    hb.set_tuning(handle, "tc_pair", 1)
+
+
+@pytest.mark.parametrize("pair_mode", [0, 2], indirect=True)
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
-def test_hgemm_tc_ops(handle, ta, tb):
+def test_hgemm_tc_ops(handle, ta, tb, pair_mode):
     rng = np.random.default_rng(40 + 2 * ta + tb)
     for (M, N, K) in HSHAPES:
         for order in (O.COL, O.ROW):
             err, ref, path, (A, lda, B, ldb, C, ldc) = run(handle, "h", order, ta, tb, M, N, K,
                                                            1.0, 0.5, rng)
             assert path.startswith("tc.h"), path
+            assert path.endswith(".pair") == (pair_mode == 2), path
             ab, cc = mag(order, ta, tb, M, N, K, 1.0, A, lda, B, ldb, 0.5, C, ldc)
             bound = 2.0 ** -11 * np.linalg.norm(ref) + 2 * g32(K) * np.linalg.norm(ab + cc)
             assert err <= bound, (M, N, K, order, ta, tb, err, bound, path)
@@ -98,9 +109,10 @@ def test_hgemm_misaligned_falls_back(handle):
 SSHAPES = [(256, 256, 256), (1000, 700, 300), (130, 200, 1000), (2048, 2048, 64)]
 
 
+@pytest.mark.parametrize("pair_mode", [0, 2], indirect=True)
 @pytest.mark.parametrize("terms", [3, 6])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
-def test_split_bf16_sgemm(handle, terms, ta, tb):
+def test_split_bf16_sgemm(handle, terms, ta, tb, pair_mode):
     rng = np.random.default_rng(100 + terms + 2 * ta + tb)
     assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_SPLIT_BF16, terms) == 0
     try:
@@ -110,6 +122,7 @@ def test_split_bf16_sgemm(handle, terms, ta, tb):
                 err, ref, path, (A, lda, B, ldb, C, ldc) = run(handle, "s", order, ta, tb, M, N, K,
                                                                alpha, beta, rng)
                 assert path.startswith(f"tc.split_bf16x{terms}"), path
+                assert (".pair" in path) == (pair_mode == 2), path
                 ab, cc = mag(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
                 if terms == 6:
                     bound = 2 * g32(K) * np.linalg.norm(ab + cc)
