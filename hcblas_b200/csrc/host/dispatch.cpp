@@ -45,7 +45,10 @@ int simt(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char 
 }
 
 /* CTA pairs (256-row tiles) once the problem has enough of them to fill
- * every SM pair; tc_pair = 2 forces them, 0 disables them. */
+ * every SM pair; tc_pair = 2 forces them, 0 disables them.  Auto mode is
+ * used by the 256 x 256 pair tiles (HGEMM, CRT); the split-BF16 paths, whose
+ * register accumulators cap them at 256 x 128 pair tiles, measured no
+ * faster with pairs and take them only when forced. */
 bool use_pair(const HcblasB200State *st, int64_t m, int64_t n, int64_t bn) {
   if (st->tc_pair == 0) return false;
   if (st->tc_pair == 2) return true;
@@ -115,7 +118,7 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   g.terms = terms;
   g.bn = 128;
   g.promote_kb = st->split_promote_kb;
-  g.pair = use_pair(st, a->m, a->n, 128) ? 1 : 0;
+  g.pair = st->tc_pair == 2 ? 1 : 0;
   for (int i = 0; i < 3; ++i) {
     g.a_planes[i] = pa.planes[i];
     g.b_planes[i] = pb.planes[i];
@@ -318,7 +321,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
   if (rc) return rc;
 
-  const int pair = use_pair(st, a->m, a->n, 128) ? 1 : 0;
+  const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
+  const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
   for (int i = 0; i < nmod && !rc; ++i) {
     hcbk_crt_gemm g;
     g.m = a->m;
@@ -332,6 +336,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
     g.t = reinterpret_cast<int16_t *>(t_base + i * t_pl);
     g.ldt = a->m;
     g.pair = pair;
+    g.bn = bn;
     rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   }
   if (rc) return rc;

@@ -210,7 +210,8 @@ typedef struct hcbk_crt_gemm {
   int modulus;
   int16_t *t;
   int64_t ldt;
-  int pair; /* 1: CTA pairs, 256 x 128 tiles */
+  int bn;   /* tile columns: 128 or 256 */
+  int pair; /* 1: CTA pairs, 256 x 256 tiles (bn = 256) */
 } hcbk_crt_gemm;
 int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
 

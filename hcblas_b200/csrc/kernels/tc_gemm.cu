@@ -140,6 +140,7 @@ __device__ __forceinline__ float load_out(const __half *p) { return __half2float
 
 /* f32 accumulator -> alpha*acc + beta*C in OutT (float or half) */
 template <typename OutT> struct EpiAlphaBeta {
+  static constexpr bool INPLACE = false;
   using AccT = float; /* register accumulator of the promoting path */
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
@@ -224,16 +225,21 @@ template <typename OutT> struct EpiAlphaBeta {
  *   C = alpha * 2^(ea_m + eb_n) * sum_d 2^(-7(d+2)) acc_d + beta * C   (FP64)
  * The group terms are exact in binary64 (|acc_d| < 2^31, power-of-two
  * weights) and are added smallest weight first. */
-/* Modular epilogue of the CRT scheme.  With f16 residues |r| <= 127
- * (moduli <= 255) every f32 chunk sum over 1024 K elements is an exact
- * integer below 2^24.  It is reduced modulo p on the FP32 pipe -- q =
- * rint(s / p) by the 1.5 * 2^23 rounding constant, r = fma(-q, p, s), exact
- * because r is a small integer -- and added to an f32 register accumulator
- * that stays a small exact integer.  The final residues are stored as
- * symmetric int16 values (C viewed as the column-major int16 residue plane).
- * No float->int conversion runs per chunk. */
+/* Modular epilogue of the CRT scheme, reducing in place in TMEM.
+ * With f16 residues |r| <= 127 (moduli <= 255) the tensor core's f32 sums
+ * are exact integers while below 2^24: 1024 * 127^2 + 1.5 * 255 < 2^24.
+ * The kernel therefore lets a TMEM accumulator grow over one 1024-element
+ * K chunk, and the epilogue warps then reduce it modulo p where it lies
+ * (tcgen05.ld -> q = rint(s / p) by the 1.5 * 2^23 rounding constant,
+ * r = fma(-q, p, s), exact because r is a small integer -> tcgen05.st),
+ * after which the MMAs keep accumulating on top of the reduced value.
+ * Chunks alternate between the two TMEM buffers, so one buffer is reduced
+ * while the tensor core fills the other; the last two chunks of a tile are
+ * combined, reduced, and stored as symmetric int16 residues (C viewed as
+ * the column-major int16 residue plane).  No register accumulator, no
+ * float->int conversion before the final store. */
 struct EpiModP {
-  using AccT = float;
+  static constexpr bool INPLACE = true;
   static constexpr float RND = 12582912.0f; /* 1.5 * 2^23 */
 
   /* exact x mod p into (-p, p) for integral |x| < 2^24 */
@@ -244,40 +250,53 @@ struct EpiModP {
 
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &, uint32_t, int, int) {
-    static_assert(NACC == 0, "the modular epilogue only runs on the promoting path");
+    static_assert(NACC == 0, "the modular epilogue only runs on the in-place path");
   }
 
-  template <int BN, int NACC>
-  static __device__ __forceinline__ void accumulate(const TcParams &p, uint32_t tbase,
-                                                    float (&acc)[BN], int /* chunk */) {
+  /* reduce this warp's 32 lanes x BN columns of one buffer in place */
+  template <int BN>
+  static __device__ __forceinline__ void rmw(const TcParams &p, uint32_t tbase) {
     const float pf = static_cast<float>(p.modulus);
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
       uint32_t r[32];
       tmem_ld_32x32b_x32(tbase + c, r);
       tmem_ld_wait();
-      /* each reduced chunk lies in (-p, p): the f32 sum stays an exact
-       * integer for up to 2^16 chunks (K < 2^26) */
 #pragma unroll
-      for (int j = 0; j < 32; ++j) acc[c + j] += mod_f(__uint_as_float(r[j]), pf, p.inv_modulus);
+      for (int j = 0; j < 32; ++j)
+        r[j] = __float_as_uint(mod_f(__uint_as_float(r[j]), pf, p.inv_modulus));
+      tmem_st_32x32b_x32(tbase + c, r);
     }
+    tmem_st_wait();
   }
 
+  /* T[m, n0 + j] = symmetric (buf_a + buf_b) mod p; has_b = 0 when the
+   * tile had a single chunk */
   template <int BN>
-  static __device__ __forceinline__ void store_acc(const TcParams &p, const float (&acc)[BN],
-                                                   int m, int n0) {
-    if (m >= p.m) return;
-    int16_t *T = static_cast<int16_t *>(p.c) + (long long)m + (long long)n0 * p.ldc;
-    const int nvalid = p.n - n0;
-    const int hp = (p.modulus - 1) >> 1;
+  static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint32_t tb,
+                                                     bool has_b, int m, int n0) {
     const float pf = static_cast<float>(p.modulus);
+    const float hp = static_cast<float>((p.modulus - 1) >> 1);
+    int16_t *T = static_cast<int16_t *>(p.c) + (long long)m + (long long)n0 * p.ldc;
+    const bool row_ok = m < p.m;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32) {
+      uint32_t ra[32], rb[32];
+      tmem_ld_32x32b_x32(ta + c, ra);
+      if (has_b) tmem_ld_32x32b_x32(tb + c, rb);
+      tmem_ld_wait();
+      if (!row_ok) continue;
+      const int nvalid = p.n - (n0 + c);
 #pragma unroll
-    for (int j = 0; j < BN; ++j) {
-      if (j < nvalid) {
-        int v = static_cast<int>(mod_f(acc[j], pf, p.inv_modulus)); /* exact, |v| < p */
-        if (v > hp) v -= p.modulus;
-        else if (v < -hp) v += p.modulus;
-        T[(long long)j * p.ldc] = static_cast<int16_t>(v);
+      for (int j = 0; j < 32; ++j) {
+        /* both terms are exact integers below 2^24 in magnitude; each is
+         * reduced first so that the sum stays exact */
+        float v = mod_f(__uint_as_float(ra[j]), pf, p.inv_modulus);
+        if (has_b) v += mod_f(__uint_as_float(rb[j]), pf, p.inv_modulus);
+        v = mod_f(v, pf, p.inv_modulus);
+        if (v > hp) v -= pf;
+        else if (v < -hp) v += pf;
+        if (j < nvalid) T[(long long)(c + j) * p.ldc] = static_cast<int16_t>(__float2int_rn(v));
       }
     }
   }
@@ -291,6 +310,7 @@ __device__ __forceinline__ double pow2_bits(int e) {
 }
 
 struct EpiOzaki {
+  static constexpr bool INPLACE = false;
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
     const bool row_ok = m < p.m;
@@ -534,12 +554,18 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       int s = 0;
       uint32_t ph = 0;
       int ci = 0; /* chunk counter (all tiles): selects the TMEM buffer */
+      uint32_t uses = 0u; /* in-place mode: bit b = parity of buffer b's acquisitions */
       bool ok = true;
       for (int t = tile0; ok && t < num_tiles; t += tile_step) {
-        for (int kc = 0; ok && kc < kblocks; kc += chunk_kb, ++ci) {
-          const int b = ci % NBUF;
-          const uint32_t tph = (ci / NBUF) & 1;
-          if (!mbar_wait(&tempty[b], tph ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
+        int c = 0; /* chunk index within the tile */
+        for (int kc = 0; ok && kc < kblocks; kc += chunk_kb, ++ci, ++c) {
+          /* in-place mode: chunk c of every tile accumulates into buffer
+           * c % 2 on top of the epilogue's reduced value of chunk c - 2 */
+          const int b = EPI::INPLACE ? (c & 1) : ci % NBUF;
+          const uint32_t tph = EPI::INPLACE ? (uses >> b) & 1u : (ci / NBUF) & 1;
+          if (EPI::INPLACE) uses ^= 1u << b;
+          const bool fresh = !EPI::INPLACE || c < 2;
+          if (!mbar_wait<CG == 2>(&tempty[b], tph ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
             ok = false;
             break;
           }
@@ -547,7 +573,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           const uint32_t dbase = tmem_base + b * Cfg::ACC_COLS;
           const int kend = (kc + chunk_kb < kblocks) ? kc + chunk_kb : kblocks;
           for (int kb = kc; kb < kend; ++kb) {
-            if (!mbar_wait(&full[s], ph, p.err, ERR_TIMEOUT_MMA_FULL)) {
+            if (!mbar_wait<CG == 2>(&full[s], ph, p.err, ERR_TIMEOUT_MMA_FULL)) {
               ok = false;
               break;
             }
@@ -562,7 +588,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
                     sbase + R::NA * Cfg::A_PLANE + R::pb(pi) * Cfg::B_PLANE + kk * b_kstep;
                 const uint64_t ad = smem_desc(aa, a_lbo, KT::SBO, KT::LAYOUT);
                 const uint64_t bd = smem_desc(ba, b_lbo, KT::SBO, KT::LAYOUT);
-                const uint32_t acc = (kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
+                const uint32_t acc = (!fresh || kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
                 if constexpr (KIND == 2)
                   mma_i8(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
                 else if constexpr (CG == 2)
@@ -603,6 +629,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           mbar_arrive(&tempty[b]);
       }
     };
+    uint32_t euses = 0u; /* in-place mode: bit b = parity of buffer b's acquisitions */
     for (int t = tile0; ok && t < num_tiles; t += tile_step) {
       const int tm = t % p.tiles_m, tn = t / p.tiles_m;
       const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
@@ -618,6 +645,36 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         tc_fence_before();
         __syncwarp();
         release(b);
+      } else if constexpr (EPI::INPLACE) {
+        /* chunks 0 .. n-3 are reduced in place and handed back; the last
+         * two (one if n == 1) stay held until the tile's final store */
+        const int nchunks = (kblocks + chunk_kb - 1) / chunk_kb;
+        const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+        for (int c = 0; c < nchunks; ++c) {
+          const int b = c & 1;
+          const uint32_t tph = (euses >> b) & 1u;
+          euses ^= 1u << b;
+          if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          if (c < nchunks - 2) {
+            EPI::template rmw<BN>(p, tmem_base + lane_off + b * Cfg::ACC_COLS);
+            tc_fence_before();
+            __syncwarp();
+            release(b);
+          }
+        }
+        if (!ok) break;
+        const int bl = (nchunks - 1) & 1; /* buffer of the last chunk */
+        EPI::template final_store<BN>(p, tmem_base + lane_off + bl * Cfg::ACC_COLS,
+                                      tmem_base + lane_off + (bl ^ 1) * Cfg::ACC_COLS,
+                                      nchunks > 1, m, tn * BN);
+        tc_fence_before();
+        __syncwarp();
+        release(bl);
+        if (nchunks > 1) release(bl ^ 1);
       } else {
         typename EPI::AccT acc[BN];
 #pragma unroll
@@ -919,12 +976,14 @@ extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stre
 }
 
 /* One modulus of the CRT scheme: f16 residue planes (K-major, |r| <= 127),
- * FP32 chunk sums exact over 1024-element K chunks (PROMOTE_KB = 16 slabs of
- * 64: 1024 * 127^2 < 2^24), reduced mod p in registers, int16 residues out.
- * K below 2^25 keeps the register sums (|chunk residue| < 1.5 p) exact. */
+ * tensor-core sums exact over 1024-element K chunks (PROMOTE_KB = 16 slabs
+ * of 64: 1024 * 127^2 + 383 < 2^24), reduced mod p in place in TMEM between
+ * chunks, int16 residues out.  Tiles: 256 x 256 over a CTA pair, or
+ * 128 x bn on one CTA. */
 extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) {
-  if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k >= (1LL << 25) || g->k <= 0 ||
-      g->modulus < 3 || g->modulus > 255 || (g->modulus & 1) == 0)
+  if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > 0x7fffffff || g->k <= 0 ||
+      g->modulus < 3 || g->modulus > 255 || (g->modulus & 1) == 0 ||
+      (g->bn != 128 && g->bn != 256) || (g->pair && g->bn != 256))
     return HCBK_ERR_ARGS;
   TcParams p;
   memset(&p, 0, sizeof(p));
@@ -934,13 +993,15 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
   const auto F16 = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   int rc = make_map(&p.ta[0], F16, 2, g->a_plane, g->k, g->m, g->ld_a, 64, BM);
   if (rc) return rc;
-  rc = make_map(&p.tb[0], F16, 2, g->b_plane, g->k, g->n, g->ld_b, 64, g->pair ? 64 : 128);
+  const uint32_t b_rows = g->pair ? g->bn / 2 : g->bn; /* B rows per CTA */
+  rc = make_map(&p.tb[0], F16, 2, g->b_plane, g->k, g->n, g->ld_b, 64, b_rows);
   if (rc) return rc;
   p.c = g->t;
   p.ldc = g->ldt;
   p.modulus = g->modulus;
   p.inv_modulus = 1.0f / (float)g->modulus;
   p.err = err;
-  if (g->pair) return launch_tc<128, 8, RecipeSingle, 0, EpiModP, 16, 2, 2>(p, stream);
+  if (g->pair) return launch_tc<256, 6, RecipeSingle, 0, EpiModP, 16, 2, 2>(p, stream);
+  if (g->bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);
   return launch_tc<128, 6, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);
 }

@@ -136,7 +136,9 @@ def test_ozaki_long_k(handle, kind):
 
 CRT_MODULI = [255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193, 191, 181,
               179, 173, 167]
-CRT_CASES = CASES + [(O.COL, 0, 1, 160, 96, 2500)]  # K over two 1024-element chunks
+# K over 3 and 5 1024-element chunks (the in-place modular reduction
+# alternates TMEM buffers, so odd chunk counts matter)
+CRT_CASES = CASES + [(O.COL, 0, 1, 160, 96, 2500), (O.ROW, 1, 0, 300, 260, 4100)]
 
 
 def crt_plan(K, want=0):
