@@ -267,7 +267,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int64_t kp = (a->k + 7) & ~int64_t(7); /* 16-byte f16 row pitch */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
   const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
-  const size_t t_pl = up1k((size_t)a->m * a->n * 2);
+  const int64_t ldt = (a->m + 1) & ~int64_t(1); /* even: the combine reads row pairs */
+  const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
   const size_t total = ea_bytes + eb_bytes + nmod * (a_pl + b_pl + t_pl);
   char *ws = static_cast<char *>(ensure_workspace(st, total));
@@ -334,7 +335,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
     g.ld_b = kp;
     g.modulus = mods[i];
     g.t = reinterpret_cast<int16_t *>(t_base + i * t_pl);
-    g.ldt = a->m;
+    g.ldt = ldt;
     g.pair = pair;
     g.bn = bn;
     rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
@@ -347,7 +348,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.nmod = nmod;
   cb.res = reinterpret_cast<const int16_t *>(t_base);
   cb.res_plane = (int64_t)(t_pl / 2);
-  cb.ldr = a->m;
+  cb.ldr = ldt;
   cb.exp_a = exp_a;
   cb.exp_b = exp_b;
   cb.shift = 2 * beta_bits;

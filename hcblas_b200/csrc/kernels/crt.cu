@@ -11,7 +11,7 @@
  *      exact, and every f16 x f16 product is exact in f32.
  *   3. One tensor-core GEMM per modulus computes T_i = A'_i B'_i mod p_i
  *      exactly (tc_gemm.cu, EpiModP: f32 sums stay integers below 2^24 over
- *      1024-element K chunks, then are reduced mod p_i with exact FP32 FMAs).
+ *      1024-element K chunks and are reduced mod p_i in place in TMEM).
  *   4. This file's combine kernel rebuilds the exact integer product
  *      P' = A' B' (|P'| < (p_1...p_n)/2, guaranteed by the choice of n and
  *      beta) from (T_1..T_n) with Garner's mixed-radix algorithm, evaluates
@@ -19,6 +19,13 @@
  *        C = alpha * P' * 2^(e_m + f_n - 2 beta) + beta * C.
  * The only roundings are the scaling in step 1 (relative 2^-(beta+1) of the
  * row / column maximum) and the final conversion to binary64.
+ *
+ * Both element-wise kernels keep their modular arithmetic on the FMA pipes:
+ * quotients are rounded with the 1.5 * 2^23 (f32) / 1.5 * 2^52 (f64)
+ * constants, small integers move between int16 and f32 through the
+ * exponent-bias trick, and the only conversion-unit instructions left are
+ * one f64 -> f32 per 16-bit limb and one packed f32x2 -> f16x2 per two
+ * residues.
  */
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -29,17 +36,39 @@
 
 namespace {
 
-/* symmetric residue of an integer-valued double |y| <= 2^53 modulo p:
- * q = rint(y / p) is within one of the true quotient (|y/p| error < 0.01),
- * and fma(-q, p, y) is exact because its exact value is a small integer. */
-__device__ __forceinline__ int sym_mod_d(double y, double p, double inv_p, int hp) {
-  const double q = rint(y * inv_p);
-  int r = static_cast<int>(fma(-q, p, y));
-  const int pi = static_cast<int>(p);
-  if (r > hp) r -= pi;
-  else if (r < -hp) r += pi;
-  return r;
+constexpr float RND_F = 12582912.0f;             /* 1.5 * 2^23 */
+constexpr double RND_D = 6755399441055744.0;     /* 1.5 * 2^52 */
+
+/* exact x mod p into (-1.5p, 1.5p) for integral |x| < 2^23; the rounded
+ * quotient may be one off, the remainder fma is exact either way */
+__device__ __forceinline__ float mod_f(float x, float p, float inv_p) {
+  const float q = fmaf(x, inv_p, RND_F) - RND_F;
+  return fmaf(-q, p, x);
 }
+
+/* fold (-1.5p, 1.5p) into the symmetric range [-(p-1)/2, (p-1)/2] */
+__device__ __forceinline__ float sym_f(float r, float p, float hp) {
+  r = r > hp ? r - p : r;
+  return r < -hp ? r + p : r;
+}
+
+/* the same in binary64 for integral |y| < 2^51 */
+__device__ __forceinline__ double sym_mod_d(double y, double q, double inv_q, double hq) {
+  const double t = fma(y, inv_q, RND_D) - RND_D;
+  double r = fma(-t, q, y);
+  r = r > hq ? r - q : r;
+  return r < -hq ? r + q : r;
+}
+
+/* small integer (|x| < 2^22) to f32 without the conversion unit */
+__device__ __forceinline__ float small_int_to_f(int x) {
+  return __int_as_float(0x4B400000 + x) - RND_F;
+}
+
+struct ModConst {
+  float p, inv_p, hp;
+  float c1, c2, c3; /* 2^16, 2^32, 2^48 mod p (symmetric) */
+};
 
 struct ResArgs {
   const double *src;
@@ -48,22 +77,47 @@ struct ResArgs {
   const int *exps;
   int beta;
   int nmod;
-  double p[HCBK_CRT_MAX_MODULI];
-  double inv_p[HCBK_CRT_MAX_MODULI];
+  ModConst mc[HCBK_CRT_MAX_MODULI];
   char *planes;
   int64_t plane_stride; /* bytes */
   int64_t ld_dst;       /* elements */
 };
 
-/* scaled integer of one element (0 for zero / non-finite rows) */
-__device__ __forceinline__ double scaled_int(double x, int e, int beta) {
-  if (e == HCBK_OZ_NONFINITE || e == HCBK_OZ_ZERO) return 0.0;
-  return rint(ldexp(x, beta - e));
+/* 16-bit limbs of the scaled integer y = rint(x 2^(beta - e)), |y| <= 2^53:
+ * y = l3 2^48 + l2 2^32 + l1 2^16 + l0 with |l0|,|l1|,|l2| <= 2^15 + 1 and
+ * |l3| <= 2^5 + 1, all exact in f32 (0 for zero / non-finite rows) */
+struct Limbs {
+  float l0, l1, l2, l3;
+};
+
+__device__ __forceinline__ Limbs limbs_of(double x, int e, int beta) {
+  Limbs L{0.f, 0.f, 0.f, 0.f};
+  if (e == HCBK_OZ_NONFINITE || e == HCBK_OZ_ZERO) return L;
+  const double y = rint(ldexp(x, beta - e));
+  const double h3 = rint(y * 0x1p-48);
+  double r = fma(-h3, 0x1p48, y);
+  const double h2 = rint(r * 0x1p-32);
+  r = fma(-h2, 0x1p32, r);
+  const double h1 = rint(r * 0x1p-16);
+  r = fma(-h1, 0x1p16, r);
+  L.l0 = static_cast<float>(r);
+  L.l1 = static_cast<float>(h1);
+  L.l2 = static_cast<float>(h2);
+  L.l3 = static_cast<float>(h3);
+  return L;
+}
+
+/* symmetric residue of the limb sum modulo one modulus; every partial sum
+ * stays an exact integer below 2^23 */
+__device__ __forceinline__ float residue(const Limbs &L, const ModConst &m) {
+  const float t1 = fmaf(L.l1, m.c1, L.l0);
+  const float t2 = fmaf(L.l3, m.c3, L.l2 * m.c2);
+  return sym_f(mod_f(t1 + t2, m.p, m.inv_p), m.p, m.hp);
 }
 
 /* K-contiguous source: 8 consecutive k per thread, 16-byte plane stores */
 __global__ void crt_res_kcontig(ResArgs a) {
-  struct alignas(16) H8 { __half v[8]; };
+  struct alignas(16) H8 { __half2 v[4]; };
   const int64_t kq = (a.kdim + 7) / 8;
   const int64_t total = a.rows * kq;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -71,28 +125,30 @@ __global__ void crt_res_kcontig(ResArgs a) {
     const int64_t r = idx / kq;
     const int64_t k0 = (idx % kq) * 8;
     const int e = a.exps[r];
-    double y[8];
+    Limbs L[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j)
-      y[j] = (k0 + j < a.kdim) ? scaled_int(a.src[r * a.ld + k0 + j], e, a.beta) : 0.0;
+      L[j] = limbs_of((k0 + j < a.kdim) ? a.src[r * a.ld + k0 + j] : 0.0, e, a.beta);
     for (int i = 0; i < a.nmod; ++i) {
-      const double p = a.p[i], ip = a.inv_p[i];
-      const int hp = (static_cast<int>(p) - 1) / 2;
+      const ModConst m = a.mc[i];
       H8 out;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) out.v[j] = __int2half_rn(sym_mod_d(y[j], p, ip, hp));
+      for (int j = 0; j < 4; ++j)
+        out.v[j] = __floats2half2_rn(residue(L[2 * j], m), residue(L[2 * j + 1], m));
       __half *d = reinterpret_cast<__half *>(a.planes + i * a.plane_stride) + r * a.ld_dst + k0;
       if (k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
         *reinterpret_cast<H8 *>(d) = out;
       } else {
+        const __half *h = reinterpret_cast<const __half *>(&out);
         for (int j = 0; j < 8; ++j)
-          if (k0 + j < a.kdim) d[j] = out.v[j];
+          if (k0 + j < a.kdim) d[j] = h[j];
       }
     }
   }
 }
 
-/* MN-contiguous source: 32x32 tile through shared memory */
+/* MN-contiguous source: 32x32 tile through shared memory, each thread then
+ * owns two consecutive k of one row (32-bit plane stores) */
 __global__ void crt_res_rcontig(ResArgs a) {
   __shared__ double tile[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
@@ -105,16 +161,26 @@ __global__ void crt_res_rcontig(ResArgs a) {
     tile[kl][tx] = (r < a.rows && k < a.kdim) ? a.src[r + k * a.ld] : 0.0;
   }
   __syncthreads();
+  /* 256 threads = 16 k-pairs x 16 rows, twice */
+  const int kp = (ty * 32 + tx) & 15, rl0 = (ty * 32 + tx) >> 4;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int rl = ty + 8 * i;
-    const int64_t r = r0 + rl, k = k0 + tx;
-    if (r < a.rows && k < a.kdim) {
-      const double y = scaled_int(tile[tx][rl], a.exps[r], a.beta);
-      for (int m = 0; m < a.nmod; ++m) {
-        const int hp = (static_cast<int>(a.p[m]) - 1) / 2;
-        reinterpret_cast<__half *>(a.planes + m * a.plane_stride)[r * a.ld_dst + k] =
-            __int2half_rn(sym_mod_d(y, a.p[m], a.inv_p[m], hp));
+  for (int h = 0; h < 2; ++h) {
+    const int rl = rl0 + 16 * h;
+    const int64_t r = r0 + rl, k = k0 + 2 * kp;
+    if (r >= a.rows || k >= a.kdim) continue;
+    const int e = a.exps[r];
+    const Limbs L0 = limbs_of(tile[2 * kp][rl], e, a.beta);
+    const Limbs L1 = limbs_of(tile[2 * kp + 1][rl], e, a.beta);
+    const bool two = k + 1 < a.kdim;
+    for (int i = 0; i < a.nmod; ++i) {
+      const ModConst m = a.mc[i];
+      const __half2 v = __floats2half2_rn(residue(L0, m), residue(L1, m));
+      __half *d = reinterpret_cast<__half *>(a.planes + i * a.plane_stride) + r * a.ld_dst + k;
+      if (two && (reinterpret_cast<uintptr_t>(d) & 3) == 0) {
+        *reinterpret_cast<__half2 *>(d) = v;
+      } else {
+        d[0] = __low2half(v);
+        if (two) d[1] = __high2half(v);
       }
     }
   }
@@ -127,15 +193,17 @@ constexpr int MAX_Q = (HCBK_CRT_MAX_MODULI + GROUP - 1) / GROUP;
 struct CombArgs {
   int64_t m, n;
   int nmod;
-  int p[HCBK_CRT_MAX_MODULI];
-  float inv_pf[HCBK_CRT_MAX_MODULI];
+  float p[HCBK_CRT_MAX_MODULI];
+  float inv_p[HCBK_CRT_MAX_MODULI];
+  float hp[HCBK_CRT_MAX_MODULI];
   /* minv[i] = (p_g0 ... p_(i-1))^-1 mod p_i over the moduli of i's group
    * before i (0 for a group's first modulus); gsize[j] = moduli in group j */
-  int minv[HCBK_CRT_MAX_MODULI];
+  float minv[HCBK_CRT_MAX_MODULI];
   int nq;
   int gsize[MAX_Q];
   double q[MAX_Q];
   double inv_q[MAX_Q];
+  double hq[MAX_Q];
   /* qinv[i][j] = q_j^-1 mod q_i (j < i) */
   double qinv[MAX_Q][MAX_Q];
   const int16_t *res;
@@ -150,98 +218,79 @@ struct CombArgs {
   int beta_nonzero;
 };
 
-/* symmetric residue of |v| < 2^22 modulo p (float reciprocal, one fix-up) */
-__device__ __forceinline__ int sym_mod_i(int v, int p, float inv_p) {
-  const int q = __float2int_rn(static_cast<float>(v) * inv_p);
-  int r = v - q * p;
-  const int hp = (p - 1) >> 1;
-  if (r > hp) r -= p;
-  else if (r < -hp) r += p;
-  return r;
-}
-
-__global__ void crt_combine_kernel(CombArgs a) {
-  const int64_t total = a.m * a.n;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = idx % a.m, col = idx / a.m;
-    const int ea = a.exp_a[row], eb = a.exp_b[col];
-    double out;
-    if (ea == HCBK_OZ_NONFINITE || eb == HCBK_OZ_NONFINITE) {
-      out = __longlong_as_double(0x7ff8000000000000ll);
-    } else if (ea == HCBK_OZ_ZERO || eb == HCBK_OZ_ZERO) {
-      out = 0.0;
-    } else {
-      const int16_t *t = a.res + row + col * a.ldr;
-      /* 1. merge each group: with x the symmetric residue modulo
-       *    Q = p_g0...p_(i-1), x += Q * ((r_i - x) Q^-1 mod p_i) is the
-       *    symmetric residue modulo Q p_i (Q < 2^16, |x| < 2^15: every int
-       *    product stays below 2^23) */
-      double u[MAX_Q];
+/* P' * 2^(ea + eb - shift) for one output element from its n residues
+ * (already in f32), Garner over groups of three moduli */
+__device__ __forceinline__ double crt_value(const CombArgs &a, const float (&t)[HCBK_CRT_MAX_MODULI],
+                                            int ea, int eb) {
+  if (ea == HCBK_OZ_NONFINITE || eb == HCBK_OZ_NONFINITE)
+    return __longlong_as_double(0x7ff8000000000000ll);
+  if (ea == HCBK_OZ_ZERO || eb == HCBK_OZ_ZERO) return 0.0;
+  /* 1. merge each group in f32: with x the symmetric residue modulo
+   *    Q = p_g0...p_(i-1), x += Q * (((r_i - x) mod p_i) Q^-1 mod p_i) is the
+   *    symmetric residue modulo Q p_i (Q < 2^16, |x| < 2^23: exact) */
+  double v[MAX_Q];
 #pragma unroll
-      for (int j = 0; j < MAX_Q; ++j) {
-        if (j >= a.nq) break;
-        const int i0 = GROUP * j;
-        int x = t[i0 * a.res_plane];
-        int qq = a.p[i0];
+  for (int j = 0; j < MAX_Q; ++j) {
+    if (j >= a.nq) break;
+    const int i0 = GROUP * j;
+    float x = t[i0];
+    float qq = a.p[i0];
 #pragma unroll
-        for (int g = 1; g < GROUP; ++g) {
-          if (g >= a.gsize[j]) break;
-          const int i = i0 + g;
-          const int r = t[i * a.res_plane];
-          const int d = sym_mod_i(sym_mod_i(r - x, a.p[i], a.inv_pf[i]) * a.minv[i], a.p[i],
-                                  a.inv_pf[i]);
-          x += qq * d;
-          qq *= a.p[i];
-        }
-        u[j] = static_cast<double>(x);
-      }
-      /* 2. Garner over the q_j (< 2^24): (x - v_j) * qinv < 2^48 is exact in
-       *    binary64 and sym_mod_d reduces it exactly */
-      double v[MAX_Q];
-#pragma unroll
-      for (int i = 0; i < MAX_Q; ++i) {
-        if (i >= a.nq) break;
-        double x = u[i];
-        const int hq = (static_cast<int>(a.q[i]) - 1) / 2;
-#pragma unroll
-        for (int j = 0; j < MAX_Q; ++j) {
-          if (j >= i) break;
-          x = static_cast<double>(sym_mod_d((x - v[j]) * a.qinv[i][j], a.q[i], a.inv_q[i], hq));
-        }
-        v[i] = x;
-      }
-      /* 3. P' = v_0 + q_0 (v_1 + q_1 (v_2 + ...)), in double-double */
-      double hi = 0.0, lo = 0.0;
-#pragma unroll
-      for (int i = MAX_Q - 1; i >= 0; --i) {
-        if (i >= a.nq) continue;
-        const double p = a.q[i];
-        const double ph = hi * p;
-        const double pl = fma(hi, p, -ph); /* exact product error */
-        double s = ph + v[i];
-        double bb = s - ph;
-        double err = (ph - (s - bb)) + (v[i] - bb);
-        lo = lo * p + pl + err;
-        hi = s + lo;
-        lo = lo - (hi - s);
-      }
-      const double x = hi + lo;
-      const int e = ea + eb - a.shift;
-      out = (e >= -1022 && e <= 1023) ? x * __longlong_as_double((long long)(e + 1023) << 52)
-                                      : ldexp(x, e);
+    for (int g = 1; g < GROUP; ++g) {
+      if (g >= a.gsize[j]) break;
+      const int i = i0 + g;
+      const float d0 = mod_f(t[i] - x, a.p[i], a.inv_p[i]);
+      const float d = sym_f(mod_f(d0 * a.minv[i], a.p[i], a.inv_p[i]), a.p[i], a.hp[i]);
+      x = fmaf(qq, d, x);
+      qq *= a.p[i];
     }
-    double *dst = a.c + row + col * a.ldc;
-    out *= a.alpha;
-    if (a.beta_nonzero) out = fma(a.beta, *dst, out);
-    *dst = out;
+    /* 2. Garner over the q_j (< 2^24): (x - v_j) qinv < 2^48, exact */
+    double xd = static_cast<double>(x);
+#pragma unroll
+    for (int l = 0; l < MAX_Q; ++l) {
+      if (l >= j) break;
+      xd = sym_mod_d((xd - v[l]) * a.qinv[j][l], a.q[j], a.inv_q[j], a.hq[j]);
+    }
+    v[j] = xd;
   }
+  /* 3. P' = v_0 + q_0 (v_1 + q_1 (v_2 + ...)), in double-double */
+  double hi = 0.0, lo = 0.0;
+#pragma unroll
+  for (int i = MAX_Q - 1; i >= 0; --i) {
+    if (i >= a.nq) continue;
+    const double p = a.q[i];
+    const double ph = hi * p;
+    const double pl = fma(hi, p, -ph); /* exact product error */
+    const double s = ph + v[i];
+    const double bb = s - ph;
+    const double err = (ph - (s - bb)) + (v[i] - bb);
+    lo = fma(lo, p, pl + err);
+    hi = s + lo;
+    lo = lo - (hi - s);
+  }
+  const double x = hi + lo;
+  const int e = ea + eb - a.shift;
+  return (e >= -1022 && e <= 1023) ? x * __longlong_as_double((long long)(e + 1023) << 52)
+                                   : ldexp(x, e);
 }
 
-static void fill_moduli(int nmod, const int *moduli, double *p, double *inv_p) {
-  for (int i = 0; i < nmod; ++i) {
-    p[i] = moduli[i];
-    inv_p[i] = 1.0 / moduli[i];
+/* one element per thread, consecutive threads on consecutive rows of one
+ * column (coalesced residue loads and C stores); grid.y strides columns */
+__global__ void __launch_bounds__(256) crt_combine_kernel(CombArgs a) {
+  for (int64_t col = blockIdx.y; col < a.n; col += gridDim.y) {
+    const int eb = a.exp_b[col];
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < a.m;
+         row += (int64_t)gridDim.x * blockDim.x) {
+      const int16_t *tp = a.res + row + col * a.ldr;
+      float t[HCBK_CRT_MAX_MODULI];
+#pragma unroll
+      for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i)
+        t[i] = i < a.nmod ? small_int_to_f(tp[i * a.res_plane]) : 0.f;
+      double *dst = a.c + row + col * a.ldc;
+      double o = a.alpha * crt_value(a, t, a.exp_a[row], eb);
+      if (a.beta_nonzero) o = fma(a.beta, *dst, o);
+      *dst = o;
+    }
   }
 }
 
@@ -259,6 +308,14 @@ static long long inv_mod_ll(long long a, long long m) {
   }
   if (t < 0) t += m;
   return t;
+}
+
+/* symmetric representative of 2^bits modulo p */
+static float pow2_mod_sym(int bits, int p) {
+  long long v = 1;
+  for (int i = 0; i < bits; ++i) v = (v * 2) % p;
+  if (v > (p - 1) / 2) v -= p;
+  return (float)v;
 }
 
 }  // namespace
@@ -286,7 +343,16 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
   a.exps = in->exps;
   a.beta = in->beta_bits;
   a.nmod = in->nmod;
-  fill_moduli(in->nmod, hcbk_crt_moduli(nullptr), a.p, a.inv_p);
+  const int *M = hcbk_crt_moduli(nullptr);
+  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
+    ModConst &m = a.mc[i];
+    m.p = (float)M[i];
+    m.inv_p = 1.0f / (float)M[i];
+    m.hp = (float)((M[i] - 1) / 2);
+    m.c1 = pow2_mod_sym(16, M[i]);
+    m.c2 = pow2_mod_sym(32, M[i]);
+    m.c3 = pow2_mod_sym(48, M[i]);
+  }
   a.planes = static_cast<char *>(in->planes);
   a.plane_stride = in->plane_stride;
   a.ld_dst = in->ld_dst;
@@ -306,7 +372,8 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
 
 extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (in->m <= 0 || in->n <= 0 || in->nmod < 2 || in->nmod > HCBK_CRT_MAX_MODULI)
+  if (in->m <= 0 || in->n <= 0 || in->nmod < 2 || in->nmod > HCBK_CRT_MAX_MODULI ||
+      (in->ldr & 1) || (in->res_plane & 1) || (reinterpret_cast<uintptr_t>(in->res) & 3))
     return HCBK_ERR_ARGS;
   CombArgs a;
   a.m = in->m;
@@ -314,25 +381,27 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.nmod = in->nmod;
   const int *M = hcbk_crt_moduli(nullptr);
   for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
-    a.p[i] = M[i];
-    a.inv_pf[i] = 1.0f / (float)M[i];
+    a.p[i] = (float)M[i];
+    a.inv_p[i] = 1.0f / (float)M[i];
+    a.hp[i] = (float)((M[i] - 1) / 2);
+    a.minv[i] = 0.f;
   }
   a.nq = (in->nmod + GROUP - 1) / GROUP;
   long long q[MAX_Q];
   for (int j = 0; j < MAX_Q; ++j) a.gsize[j] = 0;
-  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) a.minv[i] = 0;
   for (int j = 0; j < a.nq; ++j) {
     const int i0 = GROUP * j;
     const int gs = in->nmod - i0 < GROUP ? in->nmod - i0 : GROUP;
     a.gsize[j] = gs;
     long long qq = M[i0];
     for (int g = 1; g < gs; ++g) {
-      a.minv[i0 + g] = (int)inv_mod_ll(qq, M[i0 + g]);
+      a.minv[i0 + g] = (float)inv_mod_ll(qq, M[i0 + g]);
       qq *= M[i0 + g];
     }
     q[j] = qq;
     a.q[j] = (double)q[j];
     a.inv_q[j] = 1.0 / (double)q[j];
+    a.hq[j] = (double)((q[j] - 1) / 2);
   }
   for (int i = 0; i < MAX_Q; ++i)
     for (int j = 0; j < MAX_Q; ++j)
@@ -348,10 +417,9 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.alpha = in->alpha;
   a.beta = in->beta;
   a.beta_nonzero = in->beta != 0.0;
-  const int64_t total = a.m * a.n;
-  int64_t blocks = (total + 255) / 256;
-  const int64_t cap = (int64_t)hcbk_sm_count() * 32;
-  if (blocks > cap) blocks = cap;
-  crt_combine_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+  int64_t gx = (a.m + 255) / 256;
+  if (gx > 65535) gx = 65535;
+  const int64_t gy = a.n < 65535 ? a.n : 65535;
+  crt_combine_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
