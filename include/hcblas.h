@@ -336,6 +336,41 @@ int hcblasGetDeviceError(hcblasHandle_t handle);
 hcblasStatus_t hcblasSetProfiling(hcblasHandle_t handle, int on);
 int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap);
 
+/* Extension with no counterpart in the reference: split-BF16 SGEMM that
+ * allocates nothing, for callers that cannot let a library call cudaMalloc
+ * (code running under CUDA-graph stream capture, applications whose own pool
+ * allocator owns all device memory, services that allocate everything at
+ * start-up so that no later call can fail for memory or stall on the
+ * allocator's implicit synchronisation).
+ *
+ * Computes C = alpha * op(A) op(B) + beta * C, column-major, like
+ * hcblasSgemm under HCBLAS_MATH_SPLIT_BF16 with `terms` = 3 or 6 bf16
+ * products, on `stream` (a cudaStream_t; NULL = the legacy default stream)
+ * of the current device.  No handle is involved.  Its scratch is one static
+ * device array of HCBLAS_NOALLOC_SCRATCH_BYTES per GPU that loads the
+ * library (64 MiB), held until the process exits; a problem whose bf16
+ * planes need more -- (terms == 6 ? 3 : 2) * (round1024(m*kp*2) +
+ * round1024(n*kp*2)) bytes with kp = k rounded up to a multiple of 8, e.g.
+ * m = n = k = 2048 takes 32 MiB at 3 terms and 48 MiB at 6 -- is rejected
+ * with HCBLAS_STATUS_INVALID_VALUE.
+ * Status rules otherwise follow hcblasSgemm (negative sizes or NULL
+ * alpha/beta: INVALID_VALUE; an empty problem or a NULL matrix:
+ * EXECUTION_FAILED).
+ *
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current) and caches it: make that
+ * first call before any stream capture begins.  All calls on a device share
+ * the array and it keeps the last call's contents, so calls that overlap on
+ * the GPU (other streams, other host threads) race and must be serialised
+ * by the caller.  A device-side pipeline timeout (which a correct run never
+ * meets) leaves C undefined and is not reported here. */
+#define HCBLAS_NOALLOC_SCRATCH_BYTES (64u << 20)
+hcblasStatus_t hcblasSgemmSplitBF16NoAlloc(void *stream, hcblasOperation_t transa,
+                                           hcblasOperation_t transb, int m, int n, int k,
+                                           const float *alpha, const float *A, int lda,
+                                           const float *B, int ldb, const float *beta, float *C,
+                                           int ldc, int terms);
+
 #ifdef __cplusplus
 } /* extern "C" */
 
