@@ -57,7 +57,17 @@ EXPORTED = (
     "hcblasGetDeviceError", "hcblasSetTuningParam",
     "hcblasSetProfiling", "hcblasGetProfile", "hcblas_am_alloc", "hcblas_am_free",
     "hcblas_am_copy", "hcblas_view_wait", "hcblas_device_count", "hcblas_current_device",
+    "hcblasHgemmGrouped",
 )
+
+
+class GemmProblem(ctypes.Structure):
+    """One problem of hcblasHgemmGrouped (hcblasGemmProblem in hcblas.h)."""
+    _fields_ = [("transa", ctypes.c_ushort), ("transb", ctypes.c_ushort),
+                ("m", ctypes.c_int), ("n", ctypes.c_int), ("k", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_int),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_int),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_int)]
 
 
 class AcclView(ctypes.Structure):
@@ -166,6 +176,8 @@ def lib():
         L.hcblas_device_count.restype = ci
         L.hcblas_current_device.argtypes = []
         L.hcblas_current_device.restype = ci
+        L.hcblasHgemmGrouped.argtypes = [vp, ci, vp, vp, vp]
+        L.hcblasHgemmGrouped.restype = st
         _lib = L
     return _lib
 
@@ -359,3 +371,12 @@ def gemm_batched(handle, transa, transb, m, n, k, alpha, Aarr_dev, lda, Barr_dev
     f = getattr(lib(), f"hcblas{p}gemmBatched")
     return f(handle, transa, transb, m, n, k, al.ctypes.data, Aarr_dev, lda, Barr_dev, ldb,
              be.ctypes.data, Carr_dev, ldc, batch)
+
+
+def hgemm_grouped(handle, problems, alpha: float, beta: float) -> int:
+    """hcblasHgemmGrouped over a list of GemmProblem (device pointers inside)."""
+    arr = (GemmProblem * len(problems))(*problems)
+    a = np.array([alpha], dtype=np.float16).view(np.uint16)
+    b = np.array([beta], dtype=np.float16).view(np.uint16)
+    return lib().hcblasHgemmGrouped(handle, len(problems), ctypes.cast(arr, ctypes.c_void_p),
+                                    a.ctypes.data, b.ctypes.data)

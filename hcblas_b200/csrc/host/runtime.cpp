@@ -199,6 +199,17 @@ Hcblaslibrary::~Hcblaslibrary() {
       DeviceGuard g(impl->dev_err_device);
       cudaFree(impl->dev_err);
     }
+    HcblasGroupedPlan &gp = impl->grouped;
+    if (gp.upload_done) {
+      cudaEventSynchronize(static_cast<cudaEvent_t>(gp.upload_done));
+      cudaEventDestroy(static_cast<cudaEvent_t>(gp.upload_done));
+    }
+    if (gp.table) {
+      DeviceGuard g(gp.table_device);
+      cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
+      cudaFree(gp.table);
+    }
+    if (gp.staging) cudaFreeHost(gp.staging);
     delete impl;
     impl = nullptr;
   }

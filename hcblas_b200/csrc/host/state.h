@@ -19,6 +19,23 @@ struct HcblasProfRec {
   void *ev1;
 };
 
+/* The last grouped-GEMM plan of a handle: the device problem table (entries
+ * then tile prefix sums), its pinned host staging copy, and the key that lets
+ * an identical follow-up call skip the tensor-map encoding and the upload. */
+struct HcblasGroupedPlan {
+  void *table = nullptr; /* device */
+  size_t table_bytes = 0;
+  int table_device = -1;
+  void *staging = nullptr; /* pinned host */
+  size_t staging_bytes = 0;
+  void *upload_done = nullptr; /* cudaEvent_t recorded after the staging copy */
+  std::vector<unsigned char> key;
+  int count = 0;       /* problems in the device table */
+  int total_tiles = 0;
+  size_t tile_start_offset = 0;
+  std::vector<int> fallback; /* problems the table cannot hold (TMA alignment) */
+};
+
 struct HcblasB200State {
   int math_mode = 0;   /* HCBLAS_MATH_* */
   int math_param = 0;  /* terms (split-BF16) or slices (Ozaki) */
@@ -37,6 +54,7 @@ struct HcblasB200State {
   bool profiling = false;
   std::vector<HcblasProfRec> prof;
   std::vector<void *> event_pool;
+  HcblasGroupedPlan grouped;
 };
 
 namespace hcblas_b200 {

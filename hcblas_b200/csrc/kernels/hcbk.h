@@ -232,6 +232,48 @@ typedef struct hcbk_crt_combine_args {
 } hcbk_crt_combine_args;
 int hcbk_crt_combine(const hcbk_crt_combine_args *a, void *stream);
 
+/* ----------------------------------------------- grouped (uneven) GEMM -- */
+
+/* One problem of a grouped HGEMM, as the persistent kernel reads it from
+ * device memory: TMA tensor maps of op(A) and op(B) (encoded on the host by
+ * hcbk_grouped_encode), the C block and the problem shape.  128-byte maps,
+ * 64-byte aligned entries. */
+typedef struct alignas(64) hcbk_grouped_entry {
+  unsigned char map_a[128];
+  unsigned char map_b[128];
+  void *c;
+  int64_t ldc;
+  int32_t m, n, k;
+  int32_t a_mn, b_mn; /* operand is MN-major in memory */
+  int32_t tiles_m;
+} hcbk_grouped_entry;
+
+/* 2-D tensor map (128 bytes at `map`, 64-byte aligned) over 16-bit data
+ * (bf16 != 0: bf16, else f16): `inner` contiguous elements per line, `outer`
+ * lines `ld` elements apart, box {box_inner, box_outer}, 128-byte swizzle,
+ * zero fill out of bounds. */
+int hcbk_encode_tma_2d(void *map, int bf16, const void *base, uint64_t inner, uint64_t outer,
+                       uint64_t ld, uint32_t box_inner, uint32_t box_outer);
+
+/* Fill one table entry for column-major f16 C(m x n) = op(A) op(B):
+ * op_a/op_b HCBK_OP_N or HCBK_OP_T.  HCBK_ERR_ALIGN when a base address is
+ * not 16-byte aligned or lda/ldb is not a multiple of 8 (TMA rules). */
+int hcbk_grouped_encode(hcbk_grouped_entry *e, int op_a, int op_b, int64_t m, int64_t n,
+                        int64_t k, const void *a, int64_t lda, const void *b, int64_t ldb,
+                        void *c, int64_t ldc);
+
+/* Persistent grouped HGEMM: 128 x 128 tiles of every problem, enumerated by
+ * tile_start[] (count + 1 ascending prefix sums of each problem's tile
+ * count), C = alpha * op(A) op(B) + beta * C with f32 accumulation. */
+typedef struct hcbk_grouped_args {
+  const hcbk_grouped_entry *table; /* device */
+  const int32_t *tile_start;        /* device, count + 1 entries */
+  int32_t count;
+  int32_t total_tiles;
+  float alpha, beta;
+} hcbk_grouped_args;
+int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -843,6 +843,15 @@ static int launch_tc(TcParams &p, void *stream) {
 
 using namespace hcbk::tc;
 
+/* 2-D f16/bf16 tensor map with 128-byte swizzle (see make_map). */
+extern "C" int hcbk_encode_tma_2d(void *map, int bf16, const void *base, uint64_t inner,
+                                  uint64_t outer, uint64_t ld, uint32_t box_inner,
+                                  uint32_t box_outer) {
+  return make_map(static_cast<CUtensorMap *>(map),
+                  bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                  base, inner, outer, ld, box_inner, box_outer);
+}
+
 /* f16 operands straight from the caller's matrices (column-major canonical). */
 extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream) {
   if (a->dtype != HCBK_H || a->batch != 1 || a->a_array || a->op_a == HCBK_OP_C ||

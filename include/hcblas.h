@@ -231,6 +231,34 @@ hcblasStatus_t hcblasHgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_
                                          hcblasHalf *C, int ldc, long long strideC,
                                          int batchCount);
 
+/* Extension (no counterpart in the reference's C API): grouped GEMM --
+ * one call computes many independent, unevenly sized f16 GEMMs
+ *   C_i := alpha * op(A_i) * op(B_i) + beta * C_i,  i = 0 .. count-1
+ * in the handle's order (column-major by default), each problem with its own
+ * transposes, sizes, leading dimensions and device pointers; FP32
+ * accumulation.  One persistent tcgen05 kernel walks all problems' tiles
+ * from a device-side problem table; problems whose operands TMA cannot
+ * address (a base address not 16-byte aligned, or lda/ldb not a multiple of
+ * 8) run as single calls after it.  An identical follow-up call (same
+ * problem array contents) reuses the uploaded table.
+ * Status: NULL/uninitialised handle -> NOT_INITIALIZED; count < 0, a NULL
+ * problem array with count > 0, NULL alpha/beta, or a negative size ->
+ * INVALID_VALUE; a problem with a zero size or a NULL matrix ->
+ * EXECUTION_FAILED (the single-call rule); count == 0 -> SUCCESS. */
+typedef struct hcblasGemmProblem {
+  hcblasOperation_t transa, transb;
+  int m, n, k;
+  const void *A;
+  int lda;
+  const void *B;
+  int ldb;
+  void *C;
+  int ldc;
+} hcblasGemmProblem;
+hcblasStatus_t hcblasHgemmGrouped(hcblasHandle_t handle, int count,
+                                  const hcblasGemmProblem *problems, const hcblasHalf *alpha,
+                                  const hcblasHalf *beta);
+
 /* ------------------------------------------------ class-API C shims -- */
 
 /* C-ABI forms of the Hcblaslibrary::hcblas_Xgemm methods (include/hcblaslib.h;
