@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "../kernels/hcbk.h"
 
@@ -366,7 +367,48 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
 
 }  // namespace
 
+/* Strided-batched HGEMM as a special case of the grouped kernel: one table
+ * entry per batch element.  Declined (HCBK_ERR_ALIGN) unless every element
+ * is TMA-addressable, so that the batch never splits across paths. */
+int hgemm_strided_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *stream,
+                          const char **path) {
+  if (a->a_array || a->batch < 2 || a->batch > 0x7fffffff || a->m > 0x7fffffff ||
+      a->n > 0x7fffffff || a->k > 0x7fffffff || a->lda > 0x7fffffff || a->ldb > 0x7fffffff ||
+      a->ldc > 0x7fffffff)
+    return HCBK_ERR_ARGS;
+  if ((a->lda & 7) || (a->ldb & 7) || (a->stride_a & 7) || (a->stride_b & 7) ||
+      !aligned16(a->a, a->a_off, 2) || !aligned16(a->b, a->b_off, 2))
+    return HCBK_ERR_ALIGN;
+  std::vector<hcblasGemmProblem> probs((size_t)a->batch);
+  const uint16_t *A = static_cast<const uint16_t *>(a->a) + a->a_off; /* f16 storage */
+  const uint16_t *B = static_cast<const uint16_t *>(a->b) + a->b_off;
+  uint16_t *C = static_cast<uint16_t *>(a->c) + a->c_off;
+  for (int64_t i = 0; i < a->batch; ++i) {
+    hcblasGemmProblem &p = probs[(size_t)i];
+    p.transa = a->op_a == HCBK_OP_N ? HCBLAS_OP_N : HCBLAS_OP_T;
+    p.transb = a->op_b == HCBK_OP_N ? HCBLAS_OP_N : HCBLAS_OP_T;
+    p.m = (int)a->m;
+    p.n = (int)a->n;
+    p.k = (int)a->k;
+    p.A = A + i * a->stride_a;
+    p.lda = (int)a->lda;
+    p.B = B + i * a->stride_b;
+    p.ldb = (int)a->ldb;
+    p.C = C + i * a->stride_c;
+    p.ldc = (int)a->ldc;
+  }
+  int rc = grouped_hgemm(st, stream, ColMajor, (int)a->batch, probs.data(), (float)a->alpha_re,
+                         (float)a->beta_re);
+  *path = st->last_path;
+  return rc;
+}
+
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+  if (a->dtype == HCBK_H && a->batch > 1 && !a->a_array) {
+    int rc = hgemm_strided_grouped(st, a, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] strided hgemm grouped path declined (%d)\n", rc);
+  }
   if (a->dtype == HCBK_H && a->batch == 1 && !a->a_array) {
     int rc = hgemm_tc(st, a, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;

@@ -41,6 +41,11 @@ hcblasStatus run_gemm(Hcblaslibrary *h, const hc::accelerator_view &view, GemmCa
  * problem.  Returns an HCBK_* code; *path names the path taken. */
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path);
 
+/* Grouped HGEMM over `count` problems (grouped.cpp): builds or reuses the
+ * handle's device problem table and runs the persistent kernel. */
+int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,
+                  const hcblasGemmProblem *probs, float alpha, float beta);
+
 }  // namespace hcblas_b200
 
 #endif /* HCBLAS_B200_DISPATCH_H_ */

@@ -128,3 +128,36 @@ def test_grouped_status_rules(handle):
     L = hb.lib()
     assert L.hcblasHgemmGrouped(handle, -1, None, None, None) == hb.HCBLAS_STATUS_INVALID_VALUE
     assert L.hcblasHgemmGrouped(None, 1, None, None, None) == hb.HCBLAS_STATUS_NOT_INITIALIZED
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_strided_batched_hgemm_is_grouped(handle, ta, tb):
+    """hcblasHgemmStridedBatched with TMA-addressable strides runs as one
+    grouped launch (one table entry per batch element)."""
+    rng = np.random.default_rng(40 + 2 * ta + tb)
+    M, N, K, batch = 128, 96, 72, 24
+    lda = (M if ta == 0 else K) + 8
+    ldb = (K if tb == 0 else N) + 16
+    ldc = M + 3
+    sA = lda * (K if ta == 0 else M) + 64
+    sB = ldb * (N if tb == 0 else K) + 8
+    sC = ldc * N + 5
+    A = rng.uniform(-1, 1, sA * batch).astype(np.float16)
+    B = rng.uniform(-1, 1, sB * batch).astype(np.float16)
+    C = rng.uniform(-1, 1, sC * batch).astype(np.float16)
+    dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+    s = hb.gemm_strided_batched(handle, ta, tb, M, N, K, 0.5, dA, lda, sA, dB, ldb, sB, -1.0, dC,
+                                ldc, sC, batch)
+    assert s == hb.HCBLAS_STATUS_SUCCESS
+    assert hb.device_error(handle) == 0
+    assert hb.hcblasGetLastPath(handle) == "tc.h.grouped"
+    got = dC.download()
+    for i in range(batch):
+        Ai, Bi, Ci = A[i * sA:(i + 1) * sA], B[i * sB:(i + 1) * sB], C[i * sC:(i + 1) * sC]
+        _, ref = O.gemm(O.COL, ta, tb, M, N, K, 0.5, Ai, lda, Bi, ldb, -1.0, Ci, ldc)
+        gv = O.view_c(got[i * sC:(i + 1) * sC], O.COL, M, N, ldc).astype(np.float64)
+        Ad, Bd = np.abs(op_dense(Ai, ta, M, K, lda)), np.abs(op_dense(Bi, tb, K, N, ldb))
+        cc = np.abs(O.view_c(Ci, O.COL, M, N, ldc).astype(np.float64))
+        bound = 2.0 ** -11 * np.linalg.norm(ref) + 2 * g32(K) * np.linalg.norm(0.5 * (Ad @ Bd) + cc)
+        assert np.linalg.norm(gv - ref) <= bound, i
+        assert np.array_equal(got[i * sC + ldc * N:(i + 1) * sC], C[i * sC + ldc * N:(i + 1) * sC])
