@@ -365,6 +365,134 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   return timed_launch(st, stream, "crt.combine", [&] { return hcbk_crt_combine(&cb, stream); });
 }
 
+/* ZGEMM on the CRT path: 3M in modular arithmetic (exact), so one complex
+ * product costs three modular GEMMs per modulus.  Real and imaginary parts
+ * of a row share the row's exponent; the CRT range covers |Re|, |Im| <=
+ * 2 K 2^(2 beta) (crt_plan with 2K). */
+int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
+              const char **path) {
+  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  int nmod = 0, beta_bits = 0;
+  if (!crt_plan(2 * a->k, want, &nmod, &beta_bits)) return HCBK_ERR_ARGS;
+  const int *mods = hcbk_crt_moduli(nullptr);
+  const int64_t kp = (a->k + 7) & ~int64_t(7);
+  auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
+  const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
+  const int64_t ldt = (a->m + 1) & ~int64_t(1);
+  const size_t t_pl = up1k((size_t)ldt * a->n * 2);
+  /* the real view of an MN-contiguous operand has two real rows per row */
+  const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
+  const size_t ea_bytes = up1k(sizeof(int) * a->m * 2), eb_bytes = up1k(sizeof(int) * a->n * 2);
+  const size_t total = ea_bytes + eb_bytes + 3 * (size_t)nmod * (a_pl + b_pl + t_pl);
+  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  int *err = device_error_flag(st);
+  if (!ws || !err) return HCBK_ERR_NOMEM;
+  int *exp_a = reinterpret_cast<int *>(ws);
+  int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
+  char *pa_base = ws + ea_bytes + eb_bytes;
+  char *pb_base = pa_base + 3 * nmod * a_pl;
+  char *t_base = pb_base + 3 * nmod * b_pl;
+  const double *A = reinterpret_cast<const double *>(a->a) + 2 * a->a_off;
+  const double *B = reinterpret_cast<const double *>(a->b) + 2 * a->b_off;
+
+  /* exponents on the real views: K-contiguous rows hold 2K reals; an
+   * MN-contiguous operand becomes 2 x rows real rows of K */
+  hcbk_ozaki_prep ea;
+  std::memset(&ea, 0, sizeof(ea));
+  ea.src = A;
+  ea.ld = 2 * a->lda;
+  ea.k_contig = a_k;
+  ea.rows = a_k ? a->m : 2 * a->m;
+  ea.kdim = a_k ? 2 * a->k : a->k;
+  ea.exps = exp_a;
+  hcbk_ozaki_prep eb = ea;
+  eb.src = B;
+  eb.ld = 2 * a->ldb;
+  eb.k_contig = b_k;
+  eb.rows = b_k ? a->n : 2 * a->n;
+  eb.kdim = b_k ? 2 * a->k : a->k;
+  eb.exps = exp_b;
+  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); });
+  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); });
+  if (rc) return rc;
+
+  hcbk_zcrt_prep ra;
+  std::memset(&ra, 0, sizeof(ra));
+  ra.src = static_cast<const char *>(a->a) + 16 * a->a_off;
+  ra.ld = a->lda;
+  ra.k_contig = a_k;
+  ra.conj = a->op_a == HCBK_OP_C;
+  ra.rows = a->m;
+  ra.kdim = a->k;
+  ra.exps = exp_a;
+  ra.exp_pair = !a_k;
+  ra.beta_bits = beta_bits;
+  ra.nmod = nmod;
+  ra.planes = pa_base;
+  ra.plane_stride = (int64_t)a_pl;
+  ra.ld_dst = kp;
+  hcbk_zcrt_prep rb = ra;
+  rb.src = static_cast<const char *>(a->b) + 16 * a->b_off;
+  rb.ld = a->ldb;
+  rb.k_contig = b_k;
+  rb.conj = a->op_b == HCBK_OP_C;
+  rb.rows = a->n;
+  rb.exps = exp_b;
+  rb.exp_pair = !b_k;
+  rb.planes = pb_base;
+  rb.plane_stride = (int64_t)b_pl;
+  rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&ra, stream); });
+  if (!rc) rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&rb, stream); });
+  if (rc) return rc;
+
+  const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
+  const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  for (int set = 0; set < 3 && !rc; ++set) {
+    for (int i = 0; i < nmod && !rc; ++i) {
+      hcbk_crt_gemm g;
+      g.m = a->m;
+      g.n = a->n;
+      g.k = a->k;
+      g.a_plane = pa_base + (set * nmod + i) * a_pl;
+      g.b_plane = pb_base + (set * nmod + i) * b_pl;
+      g.ld_a = kp;
+      g.ld_b = kp;
+      g.modulus = mods[i];
+      g.t = reinterpret_cast<int16_t *>(t_base + (set * nmod + i) * t_pl);
+      g.ldt = ldt;
+      g.pair = pair;
+      g.bn = bn;
+      rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
+    }
+  }
+  if (rc) return rc;
+
+  hcbk_zcrt_combine_args cb;
+  cb.m = a->m;
+  cb.n = a->n;
+  cb.nmod = nmod;
+  cb.res = reinterpret_cast<const int16_t *>(t_base);
+  cb.res_plane = (int64_t)(t_pl / 2);
+  cb.ldr = ldt;
+  cb.exp_a = exp_a;
+  cb.exp_b = exp_b;
+  cb.exp_a_pair = !a_k;
+  cb.exp_b_pair = !b_k;
+  cb.shift = 2 * beta_bits;
+  cb.c = static_cast<char *>(a->c) + 16 * a->c_off;
+  cb.ldc = a->ldc;
+  cb.alpha_re = a->alpha_re;
+  cb.alpha_im = a->alpha_im;
+  cb.beta_re = a->beta_re;
+  cb.beta_im = a->beta_im;
+  static const char *names[HCBK_CRT_MAX_MODULI + 1] = {
+      "", "", "", "", "", "", "", "", "tc.zcrt3m_m8", "tc.zcrt3m_m9", "tc.zcrt3m_m10",
+      "tc.zcrt3m_m11", "tc.zcrt3m_m12", "tc.zcrt3m_m13", "tc.zcrt3m_m14", "tc.zcrt3m_m15",
+      "tc.zcrt3m_m16", "tc.zcrt3m_m17", "tc.zcrt3m_m18", "tc.zcrt3m_m19", "tc.zcrt3m_m20"};
+  *path = names[nmod];
+  return timed_launch(st, stream, "crt.zcombine", [&] { return hcbk_zcrt_combine(&cb, stream); });
+}
+
 }  // namespace
 
 /* Strided-batched HGEMM as a special case of the grouped kernel: one table
@@ -435,6 +563,12 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     int rc = dgemm_crt(st, a, st->math_param, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] crt path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_Z && st->math_mode == 4 /* HCBLAS_MATH_OZAKI_CRT */ && a->batch == 1 &&
+      !a->a_array) {
+    int rc = zgemm_crt(st, a, st->math_param, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] complex crt path declined (%d)\n", rc);
   }
   return simt(st, a, stream, path);
 }

@@ -318,6 +318,224 @@ static float pow2_mod_sym(int bits, int p) {
   return (float)v;
 }
 
+static void fill_mod_consts(ModConst (&mc)[HCBK_CRT_MAX_MODULI]) {
+  const int *M = hcbk_crt_moduli(nullptr);
+  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
+    ModConst &m = mc[i];
+    m.p = (float)M[i];
+    m.inv_p = 1.0f / (float)M[i];
+    m.hp = (float)((M[i] - 1) / 2);
+    m.c1 = pow2_mod_sym(16, M[i]);
+    m.c2 = pow2_mod_sym(32, M[i]);
+    m.c3 = pow2_mod_sym(48, M[i]);
+  }
+}
+
+/* moduli, group constants and Garner inverses of the combine */
+static void fill_comb_moduli(CombArgs &a, int nmod) {
+  const int *M = hcbk_crt_moduli(nullptr);
+  a.nmod = nmod;
+  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
+    a.p[i] = (float)M[i];
+    a.inv_p[i] = 1.0f / (float)M[i];
+    a.hp[i] = (float)((M[i] - 1) / 2);
+    a.minv[i] = 0.f;
+  }
+  a.nq = (nmod + GROUP - 1) / GROUP;
+  long long q[MAX_Q];
+  for (int j = 0; j < MAX_Q; ++j) a.gsize[j] = 0;
+  for (int j = 0; j < a.nq; ++j) {
+    const int i0 = GROUP * j;
+    const int gs = nmod - i0 < GROUP ? nmod - i0 : GROUP;
+    a.gsize[j] = gs;
+    long long qq = M[i0];
+    for (int g = 1; g < gs; ++g) {
+      a.minv[i0 + g] = (float)inv_mod_ll(qq, M[i0 + g]);
+      qq *= M[i0 + g];
+    }
+    q[j] = qq;
+    a.q[j] = (double)q[j];
+    a.inv_q[j] = 1.0 / (double)q[j];
+    a.hq[j] = (double)((q[j] - 1) / 2);
+  }
+  for (int i = 0; i < MAX_Q; ++i)
+    for (int j = 0; j < MAX_Q; ++j)
+      a.qinv[i][j] = (i < a.nq && j < i) ? (double)inv_mod_ll(q[j], q[i]) : 0.0;
+}
+
+/* ------------------------------------------------ complex (ZGEMM) path --
+ * 3M (Karatsuba) in modular arithmetic, where it is exact:
+ *   T1 = Ar Br, T2 = Ai Bi, T3 = (Ar + Ai)(Br + Bi)   (mod p, one GEMM each)
+ *   Re = T1 - T2,  Im = T3 - T1 - T2                  (mod p, then Garner)
+ * Real and imaginary parts of a row share one exponent (the larger), so
+ * Ar' + Ai' is the residue sum of one scaled integer pair. */
+
+struct ZResArgs {
+  const double2 *src;
+  int64_t ld;
+  int64_t rows, kdim;
+  const int *exps;
+  int exp_pair;    /* exponent of row r = max(exps[2r], exps[2r+1]) */
+  float im_sign;   /* -1 for a conjugate-transposed operand */
+  int beta;
+  int nmod;
+  ModConst mc[HCBK_CRT_MAX_MODULI];
+  char *planes;          /* plane (set, i) at planes + (set * nmod + i) * plane_stride */
+  int64_t plane_stride;  /* bytes; sets: 0 = real, 1 = imaginary, 2 = sum */
+  int64_t ld_dst;        /* elements */
+};
+
+__device__ __forceinline__ int row_exp(const int *exps, int pair, int64_t r) {
+  return pair ? max(exps[2 * r], exps[2 * r + 1]) : exps[r];
+}
+
+struct ZRes3 {
+  float re, im, sum;
+};
+
+__device__ __forceinline__ ZRes3 zresidue(const Limbs &lr, const Limbs &li, const ModConst &m,
+                                          float im_sign) {
+  ZRes3 o;
+  o.re = residue(lr, m);
+  o.im = im_sign * residue(li, m);
+  o.sum = sym_f(mod_f(o.re + o.im, m.p, m.inv_p), m.p, m.hp);
+  return o;
+}
+
+/* K-contiguous complex source: 8 consecutive k per thread, 16-byte stores */
+__global__ void zcrt_res_kcontig(ZResArgs a) {
+  struct alignas(16) H8 { __half2 v[4]; };
+  const int64_t kq = (a.kdim + 7) / 8;
+  const int64_t total = a.rows * kq;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / kq;
+    const int64_t k0 = (idx % kq) * 8;
+    const int e = row_exp(a.exps, a.exp_pair, r);
+    Limbs lr[8], li[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double2 z = (k0 + j < a.kdim) ? a.src[r * a.ld + k0 + j] : make_double2(0.0, 0.0);
+      lr[j] = limbs_of(z.x, e, a.beta);
+      li[j] = limbs_of(z.y, e, a.beta);
+    }
+    for (int i = 0; i < a.nmod; ++i) {
+      const ModConst m = a.mc[i];
+      H8 o[3];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const ZRes3 x0 = zresidue(lr[2 * j], li[2 * j], m, a.im_sign);
+        const ZRes3 x1 = zresidue(lr[2 * j + 1], li[2 * j + 1], m, a.im_sign);
+        o[0].v[j] = __floats2half2_rn(x0.re, x1.re);
+        o[1].v[j] = __floats2half2_rn(x0.im, x1.im);
+        o[2].v[j] = __floats2half2_rn(x0.sum, x1.sum);
+      }
+#pragma unroll
+      for (int set = 0; set < 3; ++set) {
+        __half *d = reinterpret_cast<__half *>(a.planes + (set * a.nmod + i) * a.plane_stride) +
+                    r * a.ld_dst + k0;
+        if (k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
+          *reinterpret_cast<H8 *>(d) = o[set];
+        } else {
+          const __half *h = reinterpret_cast<const __half *>(&o[set]);
+          for (int j = 0; j < 8; ++j)
+            if (k0 + j < a.kdim) d[j] = h[j];
+        }
+      }
+    }
+  }
+}
+
+/* MN-contiguous complex source: 32x32 tile through shared memory */
+__global__ void zcrt_res_rcontig(ZResArgs a) {
+  __shared__ double2 tile[32][33];
+  const int64_t r0 = (int64_t)blockIdx.x * 32;
+  const int64_t k0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int kl = ty + 8 * i;
+    const int64_t r = r0 + tx, k = k0 + kl;
+    tile[kl][tx] = (r < a.rows && k < a.kdim) ? a.src[r + k * a.ld] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const int kp = (ty * 32 + tx) & 15, rl0 = (ty * 32 + tx) >> 4;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int rl = rl0 + 16 * h;
+    const int64_t r = r0 + rl, k = k0 + 2 * kp;
+    if (r >= a.rows || k >= a.kdim) continue;
+    const int e = row_exp(a.exps, a.exp_pair, r);
+    const double2 z0 = tile[2 * kp][rl], z1 = tile[2 * kp + 1][rl];
+    const Limbs r0l = limbs_of(z0.x, e, a.beta), i0l = limbs_of(z0.y, e, a.beta);
+    const Limbs r1l = limbs_of(z1.x, e, a.beta), i1l = limbs_of(z1.y, e, a.beta);
+    const bool two = k + 1 < a.kdim;
+    for (int i = 0; i < a.nmod; ++i) {
+      const ModConst m = a.mc[i];
+      const ZRes3 x0 = zresidue(r0l, i0l, m, a.im_sign);
+      const ZRes3 x1 = zresidue(r1l, i1l, m, a.im_sign);
+      const __half2 v[3] = {__floats2half2_rn(x0.re, x1.re), __floats2half2_rn(x0.im, x1.im),
+                            __floats2half2_rn(x0.sum, x1.sum)};
+#pragma unroll
+      for (int set = 0; set < 3; ++set) {
+        __half *d = reinterpret_cast<__half *>(a.planes + (set * a.nmod + i) * a.plane_stride) +
+                    r * a.ld_dst + k;
+        if (two && (reinterpret_cast<uintptr_t>(d) & 3) == 0) {
+          *reinterpret_cast<__half2 *>(d) = v[set];
+        } else {
+          d[0] = __low2half(v[set]);
+          if (two) d[1] = __high2half(v[set]);
+        }
+      }
+    }
+  }
+}
+
+struct ZCombArgs {
+  CombArgs g;  /* moduli, Garner constants, residues (3 sets of nmod planes) */
+  int exp_a_pair, exp_b_pair;
+  double2 *c;
+  int64_t ldc;
+  double2 alpha, beta;
+};
+
+__global__ void __launch_bounds__(256) zcrt_combine_kernel(ZCombArgs a) {
+  const int nmod = a.g.nmod;
+  for (int64_t col = blockIdx.y; col < a.g.n; col += gridDim.y) {
+    const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < a.g.m;
+         row += (int64_t)gridDim.x * blockDim.x) {
+      const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row);
+      const int16_t *tp = a.g.res + row + col * a.g.ldr;
+      float tr[HCBK_CRT_MAX_MODULI], ti[HCBK_CRT_MAX_MODULI];
+#pragma unroll
+      for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
+        if (i >= nmod) {
+          tr[i] = ti[i] = 0.f;
+          continue;
+        }
+        const float t1 = small_int_to_f(tp[(int64_t)i * a.g.res_plane]);
+        const float t2 = small_int_to_f(tp[(int64_t)(nmod + i) * a.g.res_plane]);
+        const float t3 = small_int_to_f(tp[(int64_t)(2 * nmod + i) * a.g.res_plane]);
+        tr[i] = sym_f(mod_f(t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
+        ti[i] = sym_f(mod_f(t3 - t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
+      }
+      const double re = crt_value(a.g, tr, ea, eb);
+      const double im = crt_value(a.g, ti, ea, eb);
+      double2 *dst = a.c + row + col * a.ldc;
+      double2 o;
+      o.x = a.alpha.x * re - a.alpha.y * im;
+      o.y = a.alpha.x * im + a.alpha.y * re;
+      if (a.g.beta_nonzero) {
+        const double2 cv = *dst;
+        o.x = fma(a.beta.x, cv.x, fma(-a.beta.y, cv.y, o.x));
+        o.y = fma(a.beta.x, cv.y, fma(a.beta.y, cv.x, o.y));
+      }
+      *dst = o;
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" const int *hcbk_crt_moduli(int *count) {
@@ -343,16 +561,7 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
   a.exps = in->exps;
   a.beta = in->beta_bits;
   a.nmod = in->nmod;
-  const int *M = hcbk_crt_moduli(nullptr);
-  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
-    ModConst &m = a.mc[i];
-    m.p = (float)M[i];
-    m.inv_p = 1.0f / (float)M[i];
-    m.hp = (float)((M[i] - 1) / 2);
-    m.c1 = pow2_mod_sym(16, M[i]);
-    m.c2 = pow2_mod_sym(32, M[i]);
-    m.c3 = pow2_mod_sym(48, M[i]);
-  }
+  fill_mod_consts(a.mc);
   a.planes = static_cast<char *>(in->planes);
   a.plane_stride = in->plane_stride;
   a.ld_dst = in->ld_dst;
@@ -378,34 +587,7 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   CombArgs a;
   a.m = in->m;
   a.n = in->n;
-  a.nmod = in->nmod;
-  const int *M = hcbk_crt_moduli(nullptr);
-  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
-    a.p[i] = (float)M[i];
-    a.inv_p[i] = 1.0f / (float)M[i];
-    a.hp[i] = (float)((M[i] - 1) / 2);
-    a.minv[i] = 0.f;
-  }
-  a.nq = (in->nmod + GROUP - 1) / GROUP;
-  long long q[MAX_Q];
-  for (int j = 0; j < MAX_Q; ++j) a.gsize[j] = 0;
-  for (int j = 0; j < a.nq; ++j) {
-    const int i0 = GROUP * j;
-    const int gs = in->nmod - i0 < GROUP ? in->nmod - i0 : GROUP;
-    a.gsize[j] = gs;
-    long long qq = M[i0];
-    for (int g = 1; g < gs; ++g) {
-      a.minv[i0 + g] = (float)inv_mod_ll(qq, M[i0 + g]);
-      qq *= M[i0 + g];
-    }
-    q[j] = qq;
-    a.q[j] = (double)q[j];
-    a.inv_q[j] = 1.0 / (double)q[j];
-    a.hq[j] = (double)((q[j] - 1) / 2);
-  }
-  for (int i = 0; i < MAX_Q; ++i)
-    for (int j = 0; j < MAX_Q; ++j)
-      a.qinv[i][j] = (i < a.nq && j < i) ? (double)inv_mod_ll(q[j], q[i]) : 0.0;
+  fill_comb_moduli(a, in->nmod);
   a.res = in->res;
   a.res_plane = in->res_plane;
   a.ldr = in->ldr;
@@ -421,5 +603,70 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   if (gx > 65535) gx = 65535;
   const int64_t gy = a.n < 65535 ? a.n : 65535;
   crt_combine_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_zcrt_residues(const hcbk_zcrt_prep *in, void *stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (in->rows <= 0 || in->kdim <= 0 || in->nmod < 1 || in->nmod > HCBK_CRT_MAX_MODULI ||
+      in->beta_bits < 1 || in->beta_bits > 53)
+    return HCBK_ERR_ARGS;
+  ZResArgs a;
+  a.src = static_cast<const double2 *>(in->src);
+  a.ld = in->ld;
+  a.rows = in->rows;
+  a.kdim = in->kdim;
+  a.exps = in->exps;
+  a.exp_pair = in->exp_pair;
+  a.im_sign = in->conj ? -1.0f : 1.0f;
+  a.beta = in->beta_bits;
+  a.nmod = in->nmod;
+  fill_mod_consts(a.mc);
+  a.planes = static_cast<char *>(in->planes);
+  a.plane_stride = in->plane_stride;
+  a.ld_dst = in->ld_dst;
+  if (in->k_contig) {
+    const int64_t total = a.rows * ((a.kdim + 7) / 8);
+    int64_t blocks = (total + 255) / 256;
+    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    zcrt_res_kcontig<<<(unsigned)blocks, 256, 0, st>>>(a);
+  } else {
+    const int64_t gx = (a.rows + 31) / 32, gy = (a.kdim + 31) / 32;
+    if (gy > 65535) return HCBK_ERR_ARGS;
+    zcrt_res_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (in->m <= 0 || in->n <= 0 || in->nmod < 2 || in->nmod > HCBK_CRT_MAX_MODULI)
+    return HCBK_ERR_ARGS;
+  ZCombArgs a;
+  a.g.m = in->m;
+  a.g.n = in->n;
+  fill_comb_moduli(a.g, in->nmod);
+  a.g.res = in->res;
+  a.g.res_plane = in->res_plane;
+  a.g.ldr = in->ldr;
+  a.g.exp_a = in->exp_a;
+  a.g.exp_b = in->exp_b;
+  a.g.shift = in->shift;
+  a.g.c = nullptr;
+  a.g.ldc = 0;
+  a.g.alpha = 0.0;
+  a.g.beta = 0.0;
+  a.g.beta_nonzero = in->beta_re != 0.0 || in->beta_im != 0.0;
+  a.exp_a_pair = in->exp_a_pair;
+  a.exp_b_pair = in->exp_b_pair;
+  a.c = static_cast<double2 *>(in->c);
+  a.ldc = in->ldc;
+  a.alpha = make_double2(in->alpha_re, in->alpha_im);
+  a.beta = make_double2(in->beta_re, in->beta_im);
+  int64_t gx = (a.g.m + 255) / 256;
+  if (gx > 65535) gx = 65535;
+  const int64_t gy = a.g.n < 65535 ? a.g.n : 65535;
+  zcrt_combine_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -232,6 +232,49 @@ typedef struct hcbk_crt_combine_args {
 } hcbk_crt_combine_args;
 int hcbk_crt_combine(const hcbk_crt_combine_args *a, void *stream);
 
+/* ZGEMM on the CRT path (3M in modular arithmetic).  Residues of one complex
+ * operand (double2 storage, `ld` in complex elements; element (r, k) at
+ * src[k + r*ld] if k_contig else src[r + k*ld]): three plane sets of nmod
+ * planes -- real, imaginary (negated when conj), and their sum mod p --
+ * plane (set, i) at planes + (set*nmod + i)*plane_stride.  Row exponents come
+ * from hcbk_ozaki_exponents on the real view; exp_pair = 1 when that view
+ * split each complex row into two real rows (exponent = their max). */
+typedef struct hcbk_zcrt_prep {
+  const void *src;
+  int64_t ld;
+  int k_contig;
+  int conj;
+  int64_t rows, kdim;
+  const int *exps;
+  int exp_pair;
+  int beta_bits;
+  int nmod;
+  void *planes;
+  int64_t plane_stride; /* bytes */
+  int64_t ld_dst;       /* elements */
+} hcbk_zcrt_prep;
+int hcbk_zcrt_residues(const hcbk_zcrt_prep *a, void *stream);
+
+/* Complex combine: res holds 3 sets of nmod int16 planes (T1 = Ar Br,
+ * T2 = Ai Bi, T3 = (Ar+Ai)(Br+Bi) mod p_i); writes
+ * C = alpha * ((T1 - T2) + i (T3 - T1 - T2)) 2^(e_m + f_n - shift) + beta * C
+ * into the double2 matrix c. */
+typedef struct hcbk_zcrt_combine_args {
+  int64_t m, n;
+  int nmod;
+  const int16_t *res;
+  int64_t res_plane; /* elements between planes, even */
+  int64_t ldr;       /* even */
+  const int *exp_a;
+  const int *exp_b;
+  int exp_a_pair, exp_b_pair;
+  int shift;
+  void *c;
+  int64_t ldc;
+  double alpha_re, alpha_im, beta_re, beta_im;
+} hcbk_zcrt_combine_args;
+int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *a, void *stream);
+
 /* ----------------------------------------------- grouped (uneven) GEMM -- */
 
 /* One problem of a grouped HGEMM, as the persistent kernel reads it from

@@ -258,3 +258,78 @@ def test_ozaki_vs_native_accuracy(handle):
     assert errs["f16_s7"] <= errs["native"] * 4
     nmod, _ = crt_plan(K)
     assert errs[f"tc.crt_m{nmod}"] <= errs["native"]
+
+
+# ---------------------------------------------------------------- ZGEMM --
+# 3M in modular arithmetic: Re = Ar Br - Ai Bi and Im = (Ar+Ai)(Br+Bi) - Ar Br
+# - Ai Bi are exact integers of 2K products; the only errors are the scaling
+# of each entry to a beta-bit integer (relative 2^-(beta+1) of its row /
+# column maximum over real and imaginary parts) and the final rounding, so
+# per element |dC| <= 2 |alpha| 2K 2^(e_m + f_n) (2^-beta + 2^-2beta) + 4u|C|.
+
+def zcrt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta_bits, ref, beta, C, ldc):
+    Ad = op_dense(A, order, ta, M, K, lda, 0)
+    Bd = op_dense(B, order, tb, K, N, ldb, 0)
+    amax = np.maximum(np.abs(Ad.real), np.abs(Ad.imag)).max(axis=1)
+    bmax = np.maximum(np.abs(Bd.real), np.abs(Bd.imag)).max(axis=0)
+    ea = np.frexp(amax)[1].astype(np.float64)
+    eb = np.frexp(bmax)[1].astype(np.float64)
+    elem = 2 * abs(alpha) * 2 * K * np.exp2(ea[:, None] + eb[None, :]) * \
+        (2.0 ** -beta_bits + 2.0 ** (-2 * beta_bits))
+    out = np.linalg.norm(elem) + 4 * U * np.linalg.norm(ref)
+    if beta:
+        out += 4 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
+    return out
+
+
+ZCASES = [(O.COL, 2, 0, 200, 150, 300), (O.COL, 0, 0, 129, 77, 64), (O.ROW, 1, 2, 256, 100, 1000),
+          (O.COL, 2, 1, 90, 260, 2100), (O.ROW, 0, 0, 64, 64, 33)]
+
+
+@pytest.mark.parametrize("want", [0, 14, 16])
+def test_zgemm_crt_vs_dd_oracle(handle, want):
+    rng = np.random.default_rng(700 + want)
+    for order, ta, tb, M, N, K in ZCASES:
+        A, lda, B, ldb, C, ldc = make_case(rng, "z", order, ta, tb, M, N, K)
+        alpha, beta = (1 + 0.5j), (0.5 - 0.25j)
+        nmod, bb = crt_plan(2 * K, want)
+        assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, want) == 0
+        try:
+            dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+            rc = hb.lib_gemm(handle, order, TCH[ta], TCH[tb], M, N, K, alpha, dA, lda, dB, ldb,
+                             beta, dC, ldc)
+            assert rc == 0
+            assert hb.device_error(handle) == 0
+            path = hb.hcblasGetLastPath(handle)
+            got = dC.download()
+        finally:
+            hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+        assert path == f"tc.zcrt3m_m{nmod}", path
+        _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+        err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
+        bound = zcrt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, bb, ref, beta, C, ldc)
+        assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
+
+
+def test_zgemm_crt_vs_native_accuracy(handle):
+    """Complex config (conj-transposed A, N(0,1) parts): the CRT ZGEMM at full
+    width is no less accurate than the native FP64 kernel."""
+    rng = np.random.default_rng(4)
+    M = N = K = 512
+    A = (rng.standard_normal(M * K) + 1j * rng.standard_normal(M * K))
+    B = (rng.standard_normal(K * N) + 1j * rng.standard_normal(K * N))
+    C = (rng.standard_normal(M * N) + 1j * rng.standard_normal(M * N))
+    alpha, beta = (1 + 0.5j), (0.5 - 0.25j)
+    _, ref = O.gemm(O.COL, 2, 0, M, N, K, alpha, A, K, B, K, beta, C, M)
+    errs = {}
+    for mode in (hb.HCBLAS_MATH_NATIVE, hb.HCBLAS_MATH_OZAKI_CRT):
+        hb.hcblasSetMathMode(handle, mode, 0)
+        dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+        assert hb.lib_gemm(handle, O.COL, "c", "n", M, N, K, alpha, dA, K, dB, K, beta, dC, M) == 0
+        errs[hb.hcblasGetLastPath(handle)] = O.normwise_rel_error(
+            O.view_c(dC.download(), O.COL, M, N, M), ref)
+    hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+    print("zgemm native vs crt:", errs)
+    native = [v for k, v in errs.items() if k.startswith("simt")][0]
+    crt = [v for k, v in errs.items() if k.startswith("tc.zcrt")][0]
+    assert crt <= native
