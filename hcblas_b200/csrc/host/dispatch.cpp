@@ -139,6 +139,101 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   return timed_launch(st, stream, *path, [&] { return hcbk_sgemm_split_tc(&g, err, stream); });
 }
 
+/* CGEMM 3M on the split-BF16 path: T1 = Ar Br, T2 = Ai Bi,
+ * T3 = (Ar+Ai)(Br+Bi), each one split-BF16 tensor-core GEMM into an f32
+ * workspace matrix, then C = alpha ((T1 - T2) + i (T3 - T1 - T2)) + beta C.
+ * Three real products instead of four; conj-transposed operands carry
+ * negated imaginary planes. */
+int cgemm_split3m(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *stream,
+                  const char **path) {
+  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  const int nplanes = terms == 6 ? 3 : 2;
+  const int64_t kp = (a->k + 7) & ~int64_t(7);
+  auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
+  const size_t a_plane = up1k((size_t)a->m * kp * 2), b_plane = up1k((size_t)a->n * kp * 2);
+  const size_t t_bytes = up1k((size_t)a->m * a->n * 4);
+  const size_t total = 3 * nplanes * (a_plane + b_plane) + 3 * t_bytes;
+  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  int *err = device_error_flag(st);
+  if (!ws || !err) return HCBK_ERR_NOMEM;
+  char *pa_base = ws, *pb_base = ws + 3 * nplanes * a_plane;
+  float *T = reinterpret_cast<float *>(pb_base + 3 * nplanes * b_plane);
+  const int64_t t_elems = (int64_t)(t_bytes / 4);
+
+  hcbk_cpack_args pa;
+  std::memset(&pa, 0, sizeof(pa));
+  pa.src = static_cast<const char *>(a->a) + 8 * a->a_off;
+  pa.ld = a->lda;
+  pa.k_contig = a->op_a != HCBK_OP_N;
+  pa.conj = a->op_a == HCBK_OP_C;
+  pa.rows = a->m;
+  pa.kdim = a->k;
+  pa.nplanes = nplanes;
+  pa.ld_dst = kp;
+  for (int part = 0; part < 3; ++part)
+    for (int t = 0; t < nplanes; ++t) pa.planes[part][t] = pa_base + (part * nplanes + t) * a_plane;
+  hcbk_cpack_args pb;
+  std::memset(&pb, 0, sizeof(pb));
+  pb.src = static_cast<const char *>(a->b) + 8 * a->b_off;
+  pb.ld = a->ldb;
+  pb.k_contig = a->op_b == HCBK_OP_N;
+  pb.conj = a->op_b == HCBK_OP_C;
+  pb.rows = a->n;
+  pb.kdim = a->k;
+  pb.nplanes = nplanes;
+  pb.ld_dst = kp;
+  for (int part = 0; part < 3; ++part)
+    for (int t = 0; t < nplanes; ++t) pb.planes[part][t] = pb_base + (part * nplanes + t) * b_plane;
+  int rc = timed_launch(st, stream, "pack.split_bf16_complex",
+                        [&] { return hcbk_pack_split_bf16_complex(&pa, stream); });
+  if (!rc)
+    rc = timed_launch(st, stream, "pack.split_bf16_complex",
+                      [&] { return hcbk_pack_split_bf16_complex(&pb, stream); });
+  if (rc) return rc;
+
+  static const char *names[2][2] = {{"tc.split_bf16x3.128x128.p1", "tc.split_bf16x3.128x128.p4"},
+                                    {"tc.split_bf16x6.128x128.p1", "tc.split_bf16x6.128x128.p4"}};
+  for (int part = 0; part < 3 && !rc; ++part) {
+    hcbk_split_gemm g;
+    std::memset(&g, 0, sizeof(g));
+    g.m = a->m;
+    g.n = a->n;
+    g.k = a->k;
+    g.terms = terms;
+    g.bn = 128;
+    g.promote_kb = st->split_promote_kb;
+    g.pair = st->tc_pair == 2 ? 1 : 0;
+    for (int t = 0; t < nplanes; ++t) {
+      g.a_planes[t] = pa.planes[part][t];
+      g.b_planes[t] = pb.planes[part][t];
+    }
+    g.ld_a = kp;
+    g.ld_b = kp;
+    g.c = T + part * t_elems;
+    g.ldc = a->m;
+    g.alpha = 1.0;
+    g.beta = 0.0;
+    rc = timed_launch(st, stream, names[terms == 6][g.promote_kb == 4],
+                      [&] { return hcbk_sgemm_split_tc(&g, err, stream); });
+  }
+  if (rc) return rc;
+  hcbk_c3m_combine_args cb;
+  cb.t1 = T;
+  cb.t2 = T + t_elems;
+  cb.t3 = T + 2 * t_elems;
+  cb.ldt = a->m;
+  cb.m = a->m;
+  cb.n = a->n;
+  cb.c = static_cast<char *>(a->c) + 8 * a->c_off;
+  cb.ldc = a->ldc;
+  cb.alpha_re = (float)a->alpha_re;
+  cb.alpha_im = (float)a->alpha_im;
+  cb.beta_re = (float)a->beta_re;
+  cb.beta_im = (float)a->beta_im;
+  *path = terms == 6 ? "tc.csplit3m_bf16x6" : "tc.csplit3m_bf16x3";
+  return timed_launch(st, stream, "split.c3m_combine", [&] { return hcbk_c3m_combine(&cb, stream); });
+}
+
 /* Ozaki-scheme DGEMM on INT8 tensor cores: per-row / per-column exponents,
  * `s` int8 slices per operand, slice products exact in INT32, FP64 epilogue.
  * K is split so that every INT32 group sum stays exact. */
@@ -548,6 +643,13 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     int rc = sgemm_split(st, a, terms, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] split-bf16 path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_C && st->math_mode == 1 /* HCBLAS_MATH_SPLIT_BF16 */ && a->batch == 1 &&
+      !a->a_array) {
+    const int terms = st->math_param == 6 ? 6 : 3;
+    int rc = cgemm_split3m(st, a, terms, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] complex split-bf16 path declined (%d)\n", rc);
   }
   if (a->dtype == HCBK_D && (st->math_mode == 2 || st->math_mode == 3) && a->batch == 1 &&
       !a->a_array) {

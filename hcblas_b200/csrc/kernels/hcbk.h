@@ -123,6 +123,36 @@ typedef struct hcbk_pack_args {
 } hcbk_pack_args;
 int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream);
 
+/* CGEMM 3M on the split-BF16 path: split one complex f32 operand (float2
+ * storage, `ld` in complex elements; element (r, k) at src[k + r*ld] if
+ * k_contig else src[r + k*ld]) into bf16 planes of three parts -- real,
+ * imaginary (negated when conj), and their f32 sum -- planes[part][t] at
+ * [r*ld_dst + k]. */
+typedef struct hcbk_cpack_args {
+  const void *src;
+  int64_t ld;
+  int k_contig;
+  int conj;
+  int64_t rows, kdim;
+  void *planes[3][3];
+  int nplanes;
+  int64_t ld_dst;
+} hcbk_cpack_args;
+int hcbk_pack_split_bf16_complex(const hcbk_cpack_args *a, void *stream);
+
+/* C := alpha * ((T1 - T2) + i (T3 - T1 - T2)) + beta * C for f32 partial
+ * products T1 = Ar Br, T2 = Ai Bi, T3 = (Ar+Ai)(Br+Bi) (m x n, leading
+ * dimension ldt) and a float2 C. */
+typedef struct hcbk_c3m_combine_args {
+  const float *t1, *t2, *t3;
+  int64_t ldt;
+  int64_t m, n;
+  void *c;
+  int64_t ldc;
+  float alpha_re, alpha_im, beta_re, beta_im;
+} hcbk_c3m_combine_args;
+int hcbk_c3m_combine(const hcbk_c3m_combine_args *a, void *stream);
+
 /* ------------------------------------------------------- Ozaki DGEMM -- */
 
 /* exponent markers of the Ozaki scaling */

@@ -64,7 +64,9 @@ __global__ void pack_kcontig(hcbk_pack_args a) {
     __nv_bfloat16 t[4][3];
 #pragma unroll
     for (int e = 0; e < 4; ++e) split_terms(v[e], t[e]);
-    for (int p = 0; p < a.nplanes; ++p) {
+    #pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        if (p >= a.nplanes) break;
       __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(a.planes[p]) + r * a.ld_dst + k0;
 #pragma unroll
       for (int e = 0; e < 4; ++e)
@@ -93,13 +95,138 @@ __global__ void pack_rcontig(hcbk_pack_args a) {
     if (r < a.rows && k < a.kdim) {
       __nv_bfloat16 t[3];
       split_terms(tile[tx][rl], t);
-      for (int p = 0; p < a.nplanes; ++p)
-        static_cast<__nv_bfloat16 *>(a.planes[p])[r * a.ld_dst + k] = t[p];
+#pragma unroll
+      for (int p = 0; p < 3; ++p)
+        if (p < a.nplanes) static_cast<__nv_bfloat16 *>(a.planes[p])[r * a.ld_dst + k] = t[p];
+    }
+  }
+}
+
+/* complex source: parts 0 = real, 1 = imaginary (signed), 2 = their f32 sum */
+__device__ __forceinline__ void cparts(float2 z, float im_sign, float (&v)[3]) {
+  v[0] = z.x;
+  v[1] = im_sign * z.y;
+  v[2] = v[0] + v[1];
+}
+
+/* K-contiguous complex source: 4 k per thread */
+__global__ void cpack_kcontig(hcbk_cpack_args a) {
+  const int64_t kq = (a.kdim + 3) / 4;
+  const int64_t total = a.rows * kq;
+  const float im_sign = a.conj ? -1.f : 1.f;
+  const float2 *src = static_cast<const float2 *>(a.src);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / kq;
+    const int64_t k0 = (i % kq) * 4;
+    float v[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      cparts((k0 + e < a.kdim) ? src[r * a.ld + k0 + e] : make_float2(0.f, 0.f), im_sign, v[e]);
+#pragma unroll
+    for (int part = 0; part < 3; ++part) {
+      __nv_bfloat16 t[4][3];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) split_terms(v[e][part], t[e]);
+      #pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        if (p >= a.nplanes) break;
+        __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(a.planes[part][p]) + r * a.ld_dst + k0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (k0 + e < a.kdim) d[e] = t[e][p];
+      }
+    }
+  }
+}
+
+/* MN-contiguous complex source: 32x32 tiles */
+__global__ void cpack_rcontig(hcbk_cpack_args a) {
+  __shared__ float2 tile[32][33];
+  const int64_t r0 = (int64_t)blockIdx.x * 32;
+  const int64_t k0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
+  const float2 *src = static_cast<const float2 *>(a.src);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int kl = ty + 8 * i;
+    const int64_t r = r0 + tx, k = k0 + kl;
+    tile[kl][tx] = (r < a.rows && k < a.kdim) ? src[r + k * a.ld] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float im_sign = a.conj ? -1.f : 1.f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int rl = ty + 8 * i;
+    const int64_t r = r0 + rl, k = k0 + tx;
+    if (r < a.rows && k < a.kdim) {
+      float v[3];
+      cparts(tile[tx][rl], im_sign, v);
+#pragma unroll
+      for (int part = 0; part < 3; ++part) {
+        __nv_bfloat16 t[3];
+        split_terms(v[part], t);
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+          if (p < a.nplanes)
+            static_cast<__nv_bfloat16 *>(a.planes[part][p])[r * a.ld_dst + k] = t[p];
+      }
+    }
+  }
+}
+
+__global__ void c3m_combine_kernel(hcbk_c3m_combine_args a) {
+  const bool bnz = a.beta_re != 0.f || a.beta_im != 0.f;
+  float2 *C = static_cast<float2 *>(a.c);
+  for (int64_t col = blockIdx.y; col < a.n; col += gridDim.y) {
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < a.m;
+         row += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t t = row + col * a.ldt;
+      const float t1 = a.t1[t], t2 = a.t2[t], t3 = a.t3[t];
+      const float re = t1 - t2;
+      const float im = (t3 - t1) - t2;
+      float2 o;
+      o.x = a.alpha_re * re - a.alpha_im * im;
+      o.y = a.alpha_re * im + a.alpha_im * re;
+      float2 *dst = C + row + col * a.ldc;
+      if (bnz) {
+        const float2 cv = *dst;
+        o.x = fmaf(a.beta_re, cv.x, fmaf(-a.beta_im, cv.y, o.x));
+        o.y = fmaf(a.beta_re, cv.y, fmaf(a.beta_im, cv.x, o.y));
+      }
+      *dst = o;
     }
   }
 }
 
 }  // namespace
+
+extern "C" int hcbk_pack_split_bf16_complex(const hcbk_cpack_args *a, void *stream) {
+  if (a->rows <= 0 || a->kdim <= 0 || a->nplanes < 1 || a->nplanes > 3) return HCBK_ERR_ARGS;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (a->k_contig) {
+    const int64_t total = a->rows * ((a->kdim + 3) / 4);
+    int64_t blocks = (total + 255) / 256;
+    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    cpack_kcontig<<<(unsigned)blocks, 256, 0, st>>>(*a);
+  } else {
+    const int64_t gx = (a->rows + 31) / 32, gy = (a->kdim + 31) / 32;
+    if (gy > 65535) return HCBK_ERR_ARGS;
+    cpack_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(*a);
+  }
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_c3m_combine(const hcbk_c3m_combine_args *a, void *stream) {
+  if (a->m <= 0 || a->n <= 0) return HCBK_ERR_ARGS;
+  int64_t gx = (a->m + 255) / 256;
+  if (gx > 65535) gx = 65535;
+  const int64_t gy = a->n < 65535 ? a->n : 65535;
+  c3m_combine_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0,
+                       static_cast<cudaStream_t>(stream)>>>(*a);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
 
 extern "C" int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream) {
   if (a->rows <= 0 || a->kdim <= 0 || a->nplanes < 1 || a->nplanes > 3) return HCBK_ERR_ARGS;

@@ -305,8 +305,9 @@ int hcblasLibGemmBatched(hcblasHandle_t h, int dtype, int order, char typeA, cha
  *   HCBLAS_MATH_NATIVE     plain FP32 / FP64 arithmetic (default)
  *   HCBLAS_MATH_SPLIT_BF16 S/C: FP32 operands split into bf16 hi/lo terms,
  *                          products on tcgen05 tensor cores, FP32 accumulate
- *                          (`param` = number of terms: 3, or 6 for a 3-way split)
- *   HCBLAS_MATH_OZAKI_INT8 D/Z: Ozaki scheme, FP64 operands scaled per row/col
+ *                          (`param` = number of terms: 3, or 6 for a 3-way split);
+ *                          C runs 3M: Ar Br, Ai Bi, (Ar+Ai)(Br+Bi)
+ *   HCBLAS_MATH_OZAKI_INT8 D: Ozaki scheme, FP64 operands scaled per row/col
  *                          and sliced into `param` INT8 slices, slice products
  *                          exact in INT32 on tcgen05 tensor cores
  *                          (`param` = 3..8 slices of 7 bits; 0 = 7 slices)
@@ -315,13 +316,15 @@ int hcblasLibGemmBatched(hcblasHandle_t h, int dtype, int order, char typeA, cha
  *                          FP32 sums kept exact (integers < 2^24) and promoted
  *                          to FP64 per 32-element K slab (`param` = 3..7
  *                          slices of 8 bits; 0 = 7 slices, 56 bits)
- *   HCBLAS_MATH_OZAKI_CRT  D: integer-modular (CRT) scheme: operands scaled
+ *   HCBLAS_MATH_OZAKI_CRT  D/Z: integer-modular (CRT) scheme: operands scaled
  *                          to beta-bit integers per row/column, residues
  *                          modulo pairwise-coprime odd moduli <= 255 in
  *                          binary16, one exact tensor-core GEMM per modulus,
  *                          Garner reconstruction in double-double
  *                          (`param` = number of moduli 8..20; 0 = the fewest
- *                          giving beta = 53 bits for the call's K). */
+ *                          giving beta = 53 bits for the call's K); Z runs 3M
+ *                          in modular arithmetic (three exact GEMMs per
+ *                          modulus) with the range of 2K products. */
 enum {
   HCBLAS_MATH_NATIVE = 0,
   HCBLAS_MATH_SPLIT_BF16 = 1,

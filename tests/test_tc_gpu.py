@@ -162,3 +162,43 @@ def test_split_bf16_accuracy_vs_plain(handle):
     assert errs[(1, 6)] <= plain
     # three products are bounded by the 16-bit hi/lo representation
     assert errs[(1, 3)] <= 2.0 ** -16
+
+
+# ------------------------------------------------------------ CGEMM 3M --
+# T1 = Ar Br, T2 = Ai Bi, T3 = (Ar+Ai)(Br+Bi) each carry the split-BF16 error
+# of one real product (6 terms: the FP32 bound; 3 terms: + 2^-15 relative)
+# and the f32 sum Ar + Ai one more rounding; Re = T1 - T2, Im = T3 - T1 - T2.
+# Elementwise bound on |dRe| + |dIm|:
+#   (e + 4 u) |alpha| (|Ar||Br| + |Ai||Bi| + (|Ar|+|Ai|)(|Br|+|Bi|)) + 4u |beta||C|
+# with e = 2 gamma_{K+2} (6 terms) or 2^-15 + 2 gamma_{K+2} (3 terms).
+
+@pytest.mark.parametrize("terms", [3, 6])
+@pytest.mark.parametrize("ta,tb", [(2, 0), (0, 0), (1, 2), (2, 1)])
+def test_cgemm_split3m(handle, terms, ta, tb):
+    rng = np.random.default_rng(300 + 10 * terms + 3 * ta + tb)
+    assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_SPLIT_BF16, terms) == 0
+    try:
+        for order, (M, N, K) in ((O.COL, (300, 200, 500)), (O.ROW, (129, 77, 1000)),
+                                 (O.COL, (64, 256, 33))):
+            alpha, beta = (1 + 0.5j), (0.5 - 0.25j)
+            A, lda, B, ldb, C, ldc = make_case(rng, "c", order, ta, tb, M, N, K)
+            dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+            rc = hb.lib_gemm(handle, order, TCH[ta], TCH[tb], M, N, K, alpha, dA, lda, dB, ldb,
+                             beta, dC, ldc)
+            assert rc == 0
+            assert hb.device_error(handle) == 0
+            assert hb.hcblasGetLastPath(handle) == f"tc.csplit3m_bf16x{terms}"
+            got = dC.download()
+            _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+            Ad = op_dense(A, order, ta, M, K, lda, 0)
+            Bd = op_dense(B, order, tb, K, N, ldb, 0)
+            ar, ai, br, bi = np.abs(Ad.real), np.abs(Ad.imag), np.abs(Bd.real), np.abs(Bd.imag)
+            mag = ar @ br + ai @ bi + (ar + ai) @ (br + bi)
+            e = 2 * g32(K) + (2.0 ** -15 if terms == 3 else 0.0)
+            cc = np.abs(O.view_c(C, order, M, N, ldc))
+            bound = (e + 4 * U32) * abs(alpha) * np.linalg.norm(mag) + \
+                4 * U32 * abs(beta) * np.linalg.norm(cc)
+            err = np.linalg.norm(O.view_c(got, order, M, N, ldc).astype(np.complex128) - ref)
+            assert err <= bound, (terms, order, ta, tb, M, N, K, err, bound)
+    finally:
+        hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
