@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 #include <utility>
 
 #include "../../../include/hcblas.h"
@@ -38,6 +39,67 @@ hcblasTranspose char_from_op(hcblasOperation_t op) {
 }
 
 static bool is_complex(int dtype) { return dtype == HCBK_C || dtype == HCBK_Z; }
+
+/* Replay a captured CUDA graph of an identical earlier call, or run the call
+ * eagerly and capture its launch sequence for the next time.  The capture
+ * happens after the eager run, so every buffer, tensor map and attribute it
+ * needs already exists and nothing is allocated while capturing. */
+int dispatch_with_graph(HcblasB200State *st, const hcbk_gemm_args *a, void *stream,
+                        const char **path) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int knobs[6] = {st->math_mode, st->math_param, st->split_promote_kb, st->tc_pair, dev,
+                        (int)st->workspace_epoch};
+  std::vector<unsigned char> key(sizeof(*a) + sizeof(knobs) + sizeof(stream));
+  std::memcpy(key.data(), a, sizeof(*a));
+  std::memcpy(key.data() + sizeof(*a), knobs, sizeof(knobs));
+  std::memcpy(key.data() + sizeof(*a) + sizeof(knobs), &stream, sizeof(stream));
+  for (auto &e : st->graph_cache) {
+    if (e.key == key) {
+      if (cudaGraphLaunch(static_cast<cudaGraphExec_t>(e.exec), static_cast<cudaStream_t>(stream)) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        return HCBK_ERR_LAUNCH;
+      }
+      count_launch((int)e.launches);
+      *path = e.path;
+      return HCBK_OK;
+    }
+  }
+  int rc = dispatch_gemm(st, a, stream, path);
+  if (rc != HCBK_OK) return rc;
+  const unsigned epoch = st->workspace_epoch;
+  const long long before = launch_count();
+  cudaStream_t cs = static_cast<cudaStream_t>(stream);
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    return HCBK_OK;
+  }
+  const char *p2 = nullptr;
+  const int rc2 = dispatch_gemm(st, a, stream, &p2);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+  const long long captured = launch_count() - before;
+  count_launch((int)-captured); /* nothing ran while capturing */
+  cudaGraphExec_t exec = nullptr;
+  if (rc2 == HCBK_OK && ce == cudaSuccess && graph && st->workspace_epoch == epoch &&
+      cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+    if (st->graph_cache.size() >= 16) {
+      cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(st->graph_cache.front().exec));
+      st->graph_cache.erase(st->graph_cache.begin());
+    }
+    HcblasGraphEntry e;
+    e.key = key;
+    e.exec = exec;
+    e.launches = captured;
+    e.path = *path;
+    st->graph_cache.push_back(std::move(e));
+  } else {
+    cudaGetLastError();
+  }
+  if (graph) cudaGraphDestroy(graph);
+  return HCBK_OK;
+}
 
 hcblasStatus run_gemm(Hcblaslibrary *h, const hc::accelerator_view &view, GemmCall g) {
   /* quick return, exactly as the reference's class methods
@@ -104,6 +166,8 @@ hcblasStatus run_gemm(Hcblaslibrary *h, const hc::accelerator_view &view, GemmCa
     /* alpha == 0: C := beta*C, A and B are not referenced (CBLAS) */
     path = "scale";
     rc = timed_launch(h->impl, stream, path, [&] { return hcbk_scale_c(&a, stream); });
+  } else if (h->impl->graphs && !h->impl->profiling && stream != nullptr) {
+    rc = dispatch_with_graph(h->impl, &a, stream, &path);
   } else {
     rc = dispatch_gemm(h->impl, &a, stream, &path);
   }

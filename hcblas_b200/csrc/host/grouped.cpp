@@ -64,7 +64,7 @@ bool ensure_table(HcblasGroupedPlan &gp, size_t bytes, void *stream) {
   cudaGetDevice(&dev);
   if (gp.table && gp.table_bytes >= bytes && gp.table_device == dev) return true;
   if (gp.table) {
-    /* queued kernels may still read the old table */
+    /* queued kernels (or captured graphs) may still read the old table */
     cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
     DeviceGuard g(gp.table_device);
     cudaFree(gp.table);
@@ -133,6 +133,11 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
   const bool reuse = gp.table && gp.table_device == dev && key == gp.key;
 
   if (!reuse) {
+    /* captured graphs of earlier grouped calls read this table: drop them */
+    if (!st->graph_cache.empty()) {
+      cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+      clear_graph_cache(st);
+    }
     gp.key.clear();
     std::vector<hcbk_grouped_entry> ent((size_t)count);
     std::vector<int> ok_idx;

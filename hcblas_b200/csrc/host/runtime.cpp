@@ -47,6 +47,7 @@ void *ensure_workspace(HcblasB200State *st, size_t bytes) {
   if (st->workspace) {
     /* the previous workspace may still be read by queued kernels */
     cudaDeviceSynchronize();
+    clear_graph_cache(st);
     DeviceGuard g(st->workspace_device);
     cudaFree(st->workspace);
     st->workspace = nullptr;
@@ -64,11 +65,19 @@ void *ensure_workspace(HcblasB200State *st, size_t bytes) {
   return p;
 }
 
+void clear_graph_cache(HcblasB200State *st) {
+  for (auto &e : st->graph_cache)
+    if (e.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(e.exec));
+  st->graph_cache.clear();
+  ++st->workspace_epoch;
+}
+
 int *device_error_flag(HcblasB200State *st) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (st->dev_err && st->dev_err_device == dev) return st->dev_err;
   if (st->dev_err) {
+    clear_graph_cache(st);
     DeviceGuard g(st->dev_err_device);
     cudaFree(st->dev_err);
     st->dev_err = nullptr;
@@ -199,6 +208,8 @@ Hcblaslibrary::~Hcblaslibrary() {
       DeviceGuard g(impl->dev_err_device);
       cudaFree(impl->dev_err);
     }
+    cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
+    hcblas_b200::clear_graph_cache(impl);
     HcblasGroupedPlan &gp = impl->grouped;
     if (gp.upload_done) {
       cudaEventSynchronize(static_cast<cudaEvent_t>(gp.upload_done));
@@ -373,6 +384,12 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
   if (std::strcmp(name, "split_promote_kb") == 0) {
     if (value != 1 && value != 4) return HCBLAS_STATUS_INVALID_VALUE;
     handle->impl->split_promote_kb = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
+  if (std::strcmp(name, "graphs") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->graphs = value;
+    if (!value) hcblas_b200::clear_graph_cache(handle->impl);
     return HCBLAS_STATUS_SUCCESS;
   }
   if (std::strcmp(name, "tc_pair") == 0) {

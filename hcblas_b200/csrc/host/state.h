@@ -36,6 +36,16 @@ struct HcblasGroupedPlan {
   std::vector<int> fallback; /* problems the table cannot hold (TMA alignment) */
 };
 
+/* One captured call sequence (hcblasSetTuningParam "graphs"): the key is the
+ * canonical call, the knobs that steer dispatch, the stream and the
+ * workspace generation; `launches` is the number of kernels it replays. */
+struct HcblasGraphEntry {
+  std::vector<unsigned char> key;
+  void *exec = nullptr; /* cudaGraphExec_t */
+  long long launches = 0;
+  const char *path = "";
+};
+
 struct HcblasB200State {
   int math_mode = 0;   /* HCBLAS_MATH_* */
   int math_param = 0;  /* terms (split-BF16) or slices (Ozaki) */
@@ -55,6 +65,10 @@ struct HcblasB200State {
   std::vector<HcblasProfRec> prof;
   std::vector<void *> event_pool;
   HcblasGroupedPlan grouped;
+  /* CUDA-graph replay of repeated identical calls (off by default) */
+  int graphs = 0;
+  unsigned workspace_epoch = 0; /* bumped whenever a buffer a graph may reference moves */
+  std::vector<HcblasGraphEntry> graph_cache;
 };
 
 namespace hcblas_b200 {
@@ -106,6 +120,9 @@ void *ensure_workspace(HcblasB200State *st, size_t bytes);
 /* The handle's device error flag on the current device (allocated and
  * zeroed on first use); nullptr if it cannot be allocated. */
 int *device_error_flag(HcblasB200State *st);
+
+/* Destroy every cached graph (their buffers moved or the handle dies). */
+void clear_graph_cache(HcblasB200State *st);
 
 /* HCBLAS_LOG=1 prints one line per GEMM call with the path taken. */
 bool log_enabled();

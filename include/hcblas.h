@@ -339,6 +339,12 @@ hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
  *   "split_promote_kb"  split-BF16 paths: 64-element K-slabs accumulated in
  *                       TMEM before each promotion to the IEEE f32
  *                       accumulator (1 or 4; default 1).
+ *   "graphs"            1: a call identical to an earlier one (same
+ *                       arguments, pointers, math mode and knobs, same
+ *                       non-default stream) replays a CUDA graph captured
+ *                       from the earlier call's launch sequence instead of
+ *                       launching each kernel; 0 (default) launches directly.
+ *                       Graphs are dropped when the handle's workspace moves.
  *   "tc_pair"           tensor-core paths (HGEMM, split-BF16, CRT): CTA-pair
  *                       kernels (tcgen05 cta_group::2, 256-row tiles over two
  *                       SMs): 0 never, 1 when the problem fills every SM pair
