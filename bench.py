@@ -344,11 +344,11 @@ def main():
     value = world * FLOP / (ms * 1e-3) / 1e12
     assert hb.device_error(h) == 0
 
-    # dominant kernel: the one with the largest total time; its algorithmic
-    # work per launch is one exact 2*M*N*K f16 GEMM (one modulus)
+    # dominant kernel: the one with the largest total time; one launch of the
+    # modular GEMM computes an exact 2*M*N*K f16 product for every modulus
     dom, (cnt, tot) = max(prof.items(), key=lambda kv: kv[1][1])
     kernel_ms = tot / cnt
-    dom_flop = FLOP if dom.startswith("tc.") else None
+    dom_flop = FLOP * chosen if dom == "tc.crt_modgemm" else (FLOP if dom.startswith("tc.") else None)
     achieved = dom_flop / (kernel_ms * 1e-3) / 1e12 if dom_flop else None
     peak = peaks.get("bf16_tflops")
     breakdown = {k: {"launches_per_step": v[0] // args.steps,

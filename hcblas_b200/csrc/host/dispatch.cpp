@@ -418,24 +418,27 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
   if (rc) return rc;
 
+  /* every modulus in one persistent launch */
   const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
   const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
-  for (int i = 0; i < nmod && !rc; ++i) {
-    hcbk_crt_gemm g;
-    g.m = a->m;
-    g.n = a->n;
-    g.k = a->k;
-    g.a_plane = pa_base + i * a_pl;
-    g.b_plane = pb_base + i * b_pl;
-    g.ld_a = kp;
-    g.ld_b = kp;
-    g.modulus = mods[i];
-    g.t = reinterpret_cast<int16_t *>(t_base + i * t_pl);
-    g.ldt = ldt;
-    g.pair = pair;
-    g.bn = bn;
-    rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
-  }
+  hcbk_crt_gemm g;
+  g.m = a->m;
+  g.n = a->n;
+  g.k = a->k;
+  g.a_planes = pa_base;
+  g.b_planes = pb_base;
+  g.ld_a = kp;
+  g.ld_b = kp;
+  g.a_plane_stride = (int64_t)a_pl;
+  g.b_plane_stride = (int64_t)b_pl;
+  g.nmod = nmod;
+  g.moduli = mods;
+  g.t = reinterpret_cast<int16_t *>(t_base);
+  g.ldt = ldt;
+  g.t_plane_stride = (int64_t)(t_pl / 2);
+  g.pair = pair;
+  g.bn = bn;
+  rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   if (rc) return rc;
 
   hcbk_crt_combine_args cb;
@@ -542,23 +545,26 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
 
   const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
   const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  /* one launch per 3M product (all moduli in each) */
   for (int set = 0; set < 3 && !rc; ++set) {
-    for (int i = 0; i < nmod && !rc; ++i) {
-      hcbk_crt_gemm g;
-      g.m = a->m;
-      g.n = a->n;
-      g.k = a->k;
-      g.a_plane = pa_base + (set * nmod + i) * a_pl;
-      g.b_plane = pb_base + (set * nmod + i) * b_pl;
-      g.ld_a = kp;
-      g.ld_b = kp;
-      g.modulus = mods[i];
-      g.t = reinterpret_cast<int16_t *>(t_base + (set * nmod + i) * t_pl);
-      g.ldt = ldt;
-      g.pair = pair;
-      g.bn = bn;
-      rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
-    }
+    hcbk_crt_gemm g;
+    g.m = a->m;
+    g.n = a->n;
+    g.k = a->k;
+    g.a_planes = pa_base + set * nmod * a_pl;
+    g.b_planes = pb_base + set * nmod * b_pl;
+    g.ld_a = kp;
+    g.ld_b = kp;
+    g.a_plane_stride = (int64_t)a_pl;
+    g.b_plane_stride = (int64_t)b_pl;
+    g.nmod = nmod;
+    g.moduli = mods;
+    g.t = reinterpret_cast<int16_t *>(t_base + set * nmod * t_pl);
+    g.ldt = ldt;
+    g.t_plane_stride = (int64_t)(t_pl / 2);
+    g.pair = pair;
+    g.bn = bn;
+    rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   }
   if (rc) return rc;
 

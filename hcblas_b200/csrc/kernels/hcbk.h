@@ -230,16 +230,21 @@ typedef struct hcbk_crt_prep {
 } hcbk_crt_prep;
 int hcbk_crt_residues(const hcbk_crt_prep *a, void *stream);
 
-/* One modulus: T = A_res * B_res mod p on the f16 tensor path, written as
- * symmetric int16 residues, column-major M x N with leading dimension ldt. */
+/* All moduli in one launch: plane i of T = A_res_i * B_res_i mod moduli[i]
+ * on the f16 tensor path, written as symmetric int16 residues (column-major
+ * M x N, leading dimension ldt, planes t_plane_stride elements apart).
+ * Residue planes: M (resp. N) rows x ld_a (ld_b) f16, K contiguous, planes
+ * a_plane_stride (b_plane_stride) bytes apart. */
 typedef struct hcbk_crt_gemm {
   int64_t m, n, k;
-  const void *a_plane; /* M rows x ld_a f16, K contiguous */
-  const void *b_plane; /* N rows x ld_b f16, K contiguous */
+  const void *a_planes;
+  const void *b_planes;
   int64_t ld_a, ld_b;
-  int modulus;
+  int64_t a_plane_stride, b_plane_stride; /* bytes, multiples of 16 */
+  int nmod;
+  const int *moduli; /* host array of nmod moduli */
   int16_t *t;
-  int64_t ldt;
+  int64_t ldt, t_plane_stride;
   int bn;   /* tile columns: 128 or 256 */
   int pair; /* 1: CTA pairs, 256 x 256 tiles (bn = 256) */
 } hcbk_crt_gemm;

@@ -184,6 +184,17 @@ __device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *m
       : "memory");
 }
 
+/* 3-D form of tma_load_2d_pair (coordinates innermost first).  No multicast. */
+__device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map,
+                                                 uint32_t bar_cluster, int32_t c0, int32_t c1,
+                                                 int32_t c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
 /* ------------------------------------------------------------ tcgen05 -- */
 
 /* TMEM allocation for a CTA pair: one warp (same warp index) in each CTA

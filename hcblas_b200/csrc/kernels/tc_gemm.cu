@@ -61,9 +61,13 @@ struct TcParams {
   double alpha_d, beta_d;
   const int *exp_a;
   const int *exp_b;
-  /* modular (CRT) epilogue */
-  int modulus;
-  float inv_modulus;
+  /* modular (CRT) epilogue: output plane i is reduced modulo mod_tab[i];
+   * planes of A, B (3-D tensor maps) and C (c_plane_stride elements apart)
+   * are batched into one launch */
+  int nplanes;
+  long long c_plane_stride;
+  int mod_tab[HCBK_CRT_MAX_MODULI];
+  float inv_mod_tab[HCBK_CRT_MAX_MODULI];
 };
 
 /* ---------------------------------------------------------- recipes -- */
@@ -141,6 +145,7 @@ __device__ __forceinline__ float load_out(const __half *p) { return __half2float
 /* f32 accumulator -> alpha*acc + beta*C in OutT (float or half) */
 template <typename OutT> struct EpiAlphaBeta {
   static constexpr bool INPLACE = false;
+  static constexpr bool PLANE_BATCH = false;
   using AccT = float; /* register accumulator of the promoting path */
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
@@ -240,6 +245,7 @@ template <typename OutT> struct EpiAlphaBeta {
  * float->int conversion before the final store. */
 struct EpiModP {
   static constexpr bool INPLACE = true;
+  static constexpr bool PLANE_BATCH = true; /* one tile walk over every modulus */
   static constexpr float RND = 12582912.0f; /* 1.5 * 2^23 */
 
   /* exact x mod p into (-p, p) for integral |x| < 2^24 */
@@ -255,8 +261,9 @@ struct EpiModP {
 
   /* reduce this warp's 32 lanes x BN columns of one buffer in place */
   template <int BN>
-  static __device__ __forceinline__ void rmw(const TcParams &p, uint32_t tbase) {
-    const float pf = static_cast<float>(p.modulus);
+  static __device__ __forceinline__ void rmw(const TcParams &p, uint32_t tbase, int plane) {
+    const float pf = static_cast<float>(p.mod_tab[plane]);
+    const float inv = p.inv_mod_tab[plane];
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
       uint32_t r[32];
@@ -264,7 +271,7 @@ struct EpiModP {
       tmem_ld_wait();
 #pragma unroll
       for (int j = 0; j < 32; ++j)
-        r[j] = __float_as_uint(mod_f(__uint_as_float(r[j]), pf, p.inv_modulus));
+        r[j] = __float_as_uint(mod_f(__uint_as_float(r[j]), pf, inv));
       tmem_st_32x32b_x32(tbase + c, r);
     }
     tmem_st_wait();
@@ -274,10 +281,13 @@ struct EpiModP {
    * tile had a single chunk */
   template <int BN>
   static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint32_t tb,
-                                                     bool has_b, int m, int n0) {
-    const float pf = static_cast<float>(p.modulus);
-    const float hp = static_cast<float>((p.modulus - 1) >> 1);
-    int16_t *T = static_cast<int16_t *>(p.c) + (long long)m + (long long)n0 * p.ldc;
+                                                     bool has_b, int m, int n0, int plane) {
+    const int mod = p.mod_tab[plane];
+    const float pf = static_cast<float>(mod);
+    const float inv = p.inv_mod_tab[plane];
+    const float hp = static_cast<float>((mod - 1) >> 1);
+    int16_t *T = static_cast<int16_t *>(p.c) + plane * p.c_plane_stride + (long long)m +
+                 (long long)n0 * p.ldc;
     const bool row_ok = m < p.m;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
@@ -291,9 +301,9 @@ struct EpiModP {
       for (int j = 0; j < 32; ++j) {
         /* both terms are exact integers below 2^24 in magnitude; each is
          * reduced first so that the sum stays exact */
-        float v = mod_f(__uint_as_float(ra[j]), pf, p.inv_modulus);
-        if (has_b) v += mod_f(__uint_as_float(rb[j]), pf, p.inv_modulus);
-        v = mod_f(v, pf, p.inv_modulus);
+        float v = mod_f(__uint_as_float(ra[j]), pf, inv);
+        if (has_b) v += mod_f(__uint_as_float(rb[j]), pf, inv);
+        v = mod_f(v, pf, inv);
         if (v > hp) v -= pf;
         else if (v < -hp) v += pf;
         if (j < nvalid) T[(long long)(c + j) * p.ldc] = static_cast<int16_t>(__float2int_rn(v));
@@ -311,6 +321,7 @@ __device__ __forceinline__ double pow2_bits(int e) {
 
 struct EpiOzaki {
   static constexpr bool INPLACE = false;
+  static constexpr bool PLANE_BATCH = false;
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
     const bool row_ok = m < p.m;
@@ -479,8 +490,10 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  /* persistent loop over output tiles of (BM * CG) x BN, one per CTA group */
-  const int num_tiles = p.tiles_m * p.tiles_n;
+  /* persistent loop over output tiles of (BM * CG) x BN, one per CTA group
+   * (times the batched planes of a plane-batched epilogue) */
+  const int tiles_per_plane = p.tiles_m * p.tiles_n;
+  const int num_tiles = tiles_per_plane * (EPI::PLANE_BATCH ? p.nplanes : 1);
   const int tile0 = blockIdx.x / CG, tile_step = gridDim.x / CG;
   const int kblocks = (p.k + BKE - 1) / BKE;
   const int chunk_kb = PROMOTE_KB > 0 ? PROMOTE_KB : kblocks;
@@ -492,7 +505,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       uint32_t ph = 0;
       bool ok = true;
       for (int t = tile0; ok && t < num_tiles; t += tile_step) {
-        const int tm = t % p.tiles_m, tn = t / p.tiles_m;
+        const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
+        const int tt = t - plane * tiles_per_plane;
+        const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
         const int row0 = (tm * CG + (int)rank) * BM;               /* this CTA's A rows */
         const int col0 = tn * BN + (int)rank * (int)Cfg::B_ROWS;   /* this CTA's B rows */
         for (int kb = 0; kb < kblocks; ++kb) {
@@ -505,10 +520,16 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           uint8_t *st = smem + s * Cfg::STAGE_BYTES;
           const int k0 = p.k0 + kb * BKE;
           auto load2d = [&](uint8_t *dst, const CUtensorMap *map, int c0, int c1) {
-            if constexpr (CG == 2)
+            if constexpr (EPI::PLANE_BATCH) { /* 3-D maps: {K, rows, plane} */
+              if constexpr (CG == 2)
+                tma_load_3d_pair(dst, map, mapa_shared(&full[s], 0), c0, c1, plane);
+              else
+                tma_load_3d(dst, map, &full[s], c0, c1, plane);
+            } else if constexpr (CG == 2) {
               tma_load_2d_pair(dst, map, mapa_shared(&full[s], 0), c0, c1);
-            else
+            } else {
               tma_load_2d(dst, map, &full[s], c0, c1);
+            }
           };
 #pragma unroll
           for (int a = 0; a < R::NA; ++a) {
@@ -631,7 +652,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     };
     uint32_t euses = 0u; /* in-place mode: bit b = parity of buffer b's acquisitions */
     for (int t = tile0; ok && t < num_tiles; t += tile_step) {
-      const int tm = t % p.tiles_m, tn = t / p.tiles_m;
+      const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
+      const int tt = t - plane * tiles_per_plane;
+      const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
       const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
       if constexpr (PROMOTE_KB == 0) {
         const int b = ci % NBUF;
@@ -660,7 +683,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           }
           tc_fence_after();
           if (c < nchunks - 2) {
-            EPI::template rmw<BN>(p, tmem_base + lane_off + b * Cfg::ACC_COLS);
+            EPI::template rmw<BN>(p, tmem_base + lane_off + b * Cfg::ACC_COLS, plane);
             tc_fence_before();
             __syncwarp();
             release(b);
@@ -670,7 +693,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const int bl = (nchunks - 1) & 1; /* buffer of the last chunk */
         EPI::template final_store<BN>(p, tmem_base + lane_off + bl * Cfg::ACC_COLS,
                                       tmem_base + lane_off + (bl ^ 1) * Cfg::ACC_COLS,
-                                      nchunks > 1, m, tn * BN);
+                                      nchunks > 1, m, tn * BN, plane);
         tc_fence_before();
         __syncwarp();
         release(bl);
@@ -827,7 +850,7 @@ static int launch_tc(TcParams &p, void *stream) {
   }
   p.tiles_m = (p.m + BM * CG - 1) / (BM * CG);
   p.tiles_n = (p.n + BN - 1) / BN;
-  const int tiles = p.tiles_m * p.tiles_n;
+  const int tiles = p.tiles_m * p.tiles_n * (EPI::PLANE_BATCH ? p.nplanes : 1);
   int groups = CG == 2 ? pair_slots[dev] : hcbk_sm_count();
   if (tiles < groups) groups = tiles;
   cfg.gridDim = dim3((unsigned)(groups * CG), 1, 1);
@@ -984,31 +1007,57 @@ extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stre
   }
 }
 
-/* One modulus of the CRT scheme: f16 residue planes (K-major, |r| <= 127),
- * tensor-core sums exact over 1024-element K chunks (PROMOTE_KB = 16 slabs
- * of 64: 1024 * 127^2 + 383 < 2^24), reduced mod p in place in TMEM between
- * chunks, int16 residues out.  Tiles: 256 x 256 over a CTA pair, or
- * 128 x bn on one CTA. */
+/* 3-D map over `planes` f16 planes {K, rows, plane}: row pitch ld elements,
+ * plane pitch pstride bytes; box {64, box_rows, 1}, 128-byte swizzle. */
+static int make_map_planes_f16(CUtensorMap *map, const void *base, uint64_t kdim, uint64_t rows,
+                               uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return HCBK_ERR_DRIVER;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || (pstride & 15))
+    return HCBK_ERR_ALIGN;
+  cuuint64_t dims[3] = {kdim, rows, planes};
+  cuuint64_t strides[2] = {ld * 2, pstride};
+  cuuint32_t box[3] = {64, box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
+}
+
+/* Every modulus of the CRT scheme in one launch: f16 residue planes
+ * (K-major, |r| <= 127) read through 3-D tensor maps, tensor-core sums exact
+ * over 1024-element K chunks (PROMOTE_KB = 16 slabs of 64:
+ * 1024 * 127^2 + 383 < 2^24), reduced mod p in place in TMEM between chunks,
+ * int16 residues out; the persistent tile walk spans all planes.  Tiles:
+ * 256 x 256 over a CTA pair, or 128 x bn on one CTA. */
 extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) {
   if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > 0x7fffffff || g->k <= 0 ||
-      g->modulus < 3 || g->modulus > 255 || (g->modulus & 1) == 0 ||
+      g->nmod < 1 || g->nmod > HCBK_CRT_MAX_MODULI || !g->moduli ||
       (g->bn != 128 && g->bn != 256) || (g->pair && g->bn != 256))
     return HCBK_ERR_ARGS;
+  for (int i = 0; i < g->nmod; ++i)
+    if (g->moduli[i] < 3 || g->moduli[i] > 255 || (g->moduli[i] & 1) == 0) return HCBK_ERR_ARGS;
   TcParams p;
   memset(&p, 0, sizeof(p));
   p.m = (int)g->m;
   p.n = (int)g->n;
   p.k = (int)g->k;
-  const auto F16 = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-  int rc = make_map(&p.ta[0], F16, 2, g->a_plane, g->k, g->m, g->ld_a, 64, BM);
+  int rc = make_map_planes_f16(&p.ta[0], g->a_planes, g->k, g->m, g->nmod, g->ld_a,
+                               g->a_plane_stride, BM);
   if (rc) return rc;
   const uint32_t b_rows = g->pair ? g->bn / 2 : g->bn; /* B rows per CTA */
-  rc = make_map(&p.tb[0], F16, 2, g->b_plane, g->k, g->n, g->ld_b, 64, b_rows);
+  rc = make_map_planes_f16(&p.tb[0], g->b_planes, g->k, g->n, g->nmod, g->ld_b, g->b_plane_stride,
+                           b_rows);
   if (rc) return rc;
   p.c = g->t;
   p.ldc = g->ldt;
-  p.modulus = g->modulus;
-  p.inv_modulus = 1.0f / (float)g->modulus;
+  p.nplanes = g->nmod;
+  p.c_plane_stride = g->t_plane_stride;
+  for (int i = 0; i < g->nmod; ++i) {
+    p.mod_tab[i] = g->moduli[i];
+    p.inv_mod_tab[i] = 1.0f / (float)g->moduli[i];
+  }
   p.err = err;
   if (g->pair) return launch_tc<256, 6, RecipeSingle, 0, EpiModP, 16, 2, 2>(p, stream);
   if (g->bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);
