@@ -418,9 +418,11 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
   if (rc) return rc;
 
-  /* every modulus in one persistent launch */
-  const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
-  const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  /* every modulus in one persistent launch: the tile walk covers nmod
+   * planes, so the tile-count thresholds count all of them */
+  const int pair = st->tc_pair == 2 ||
+                   (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * nmod >= hcbk_sm_count() / 2);
+  const int bn = pair || tiles_of(a->m, a->n, 128, 256) * nmod >= hcbk_sm_count() ? 256 : 128;
   hcbk_crt_gemm g;
   g.m = a->m;
   g.n = a->n;
@@ -543,8 +545,9 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!rc) rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&rb, stream); });
   if (rc) return rc;
 
-  const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
-  const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  const int pair = st->tc_pair == 2 ||
+                   (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * nmod >= hcbk_sm_count() / 2);
+  const int bn = pair || tiles_of(a->m, a->n, 128, 256) * nmod >= hcbk_sm_count() ? 256 : 128;
   /* one launch per 3M product (all moduli in each) */
   for (int set = 0; set < 3 && !rc; ++set) {
     hcbk_crt_gemm g;

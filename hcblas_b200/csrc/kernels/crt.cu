@@ -220,8 +220,8 @@ struct CombArgs {
 
 /* P' * 2^(ea + eb - shift) for one output element from its n residues
  * (already in f32), Garner over groups of three moduli */
-__device__ __forceinline__ double crt_value(const CombArgs &a, const float (&t)[HCBK_CRT_MAX_MODULI],
-                                            int ea, int eb) {
+template <class Res>
+__device__ __forceinline__ double crt_value(const CombArgs &a, const Res &t, int ea, int eb) {
   if (ea == HCBK_OZ_NONFINITE || eb == HCBK_OZ_NONFINITE)
     return __longlong_as_double(0x7ff8000000000000ll);
   if (ea == HCBK_OZ_ZERO || eb == HCBK_OZ_ZERO) return 0.0;
@@ -499,29 +499,33 @@ struct ZCombArgs {
   double2 alpha, beta;
 };
 
+/* residues of one element kept in shared memory, [modulus][thread]: the
+ * complex combine holds two sets, which in registers would cut occupancy */
+struct SmemRes {
+  const float *base;
+  __device__ __forceinline__ float operator[](int i) const { return base[i * 256]; }
+};
+
 __global__ void __launch_bounds__(256) zcrt_combine_kernel(ZCombArgs a) {
+  __shared__ float sres[2][HCBK_CRT_MAX_MODULI][256];
   const int nmod = a.g.nmod;
+  const int tid = threadIdx.x;
   for (int64_t col = blockIdx.y; col < a.g.n; col += gridDim.y) {
     const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < a.g.m;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + tid; row < a.g.m;
          row += (int64_t)gridDim.x * blockDim.x) {
       const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row);
       const int16_t *tp = a.g.res + row + col * a.g.ldr;
-      float tr[HCBK_CRT_MAX_MODULI], ti[HCBK_CRT_MAX_MODULI];
-#pragma unroll
-      for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
-        if (i >= nmod) {
-          tr[i] = ti[i] = 0.f;
-          continue;
-        }
+#pragma unroll 4
+      for (int i = 0; i < nmod; ++i) {
         const float t1 = small_int_to_f(tp[(int64_t)i * a.g.res_plane]);
         const float t2 = small_int_to_f(tp[(int64_t)(nmod + i) * a.g.res_plane]);
         const float t3 = small_int_to_f(tp[(int64_t)(2 * nmod + i) * a.g.res_plane]);
-        tr[i] = sym_f(mod_f(t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
-        ti[i] = sym_f(mod_f(t3 - t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
+        sres[0][i][tid] = sym_f(mod_f(t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
+        sres[1][i][tid] = sym_f(mod_f(t3 - t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
       }
-      const double re = crt_value(a.g, tr, ea, eb);
-      const double im = crt_value(a.g, ti, ea, eb);
+      const double re = crt_value(a.g, SmemRes{&sres[0][0][tid]}, ea, eb);
+      const double im = crt_value(a.g, SmemRes{&sres[1][0][tid]}, ea, eb);
       double2 *dst = a.c + row + col * a.ldc;
       double2 o;
       o.x = a.alpha.x * re - a.alpha.y * im;

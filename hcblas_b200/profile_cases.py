@@ -1,0 +1,145 @@
+"""Named single-GEMM workloads for profiling the library's kernels.
+
+    python -m hcblas_b200.profile_cases <case> [<case> ...]
+    python -m hcblas_b200.profile_cases --list
+
+Each case allocates its operands on cuda:0 (seeded, synthetic), makes one
+warm-up call, then one more call of the same GEMM through the public C ABI,
+and synchronises: under a profiler, skip the warm-up call's launches (`-s`)
+and capture the second call's.  Sizes keep every case to a few GB of device
+memory and inputs larger than the 126 MB L2 where the workload allows.
+"""
+from __future__ import annotations
+
+import ctypes
+import sys
+
+import numpy as np
+
+import hcblas_b200 as hb
+
+N_, T_, C_ = hb.HCBLAS_OP_N, hb.HCBLAS_OP_T, hb.HCBLAS_OP_C
+
+
+def _dev(h, x):
+    return hb.DeviceArray(h, x)
+
+
+def _real(h, dtype, op_a, op_b, m, n, k, mode=0, param=0, seed=0):
+    rng = np.random.default_rng(seed)
+    ar, ac = (m, k) if op_a == N_ else (k, m)
+    br, bc = (k, n) if op_b == N_ else (n, k)
+    A = rng.standard_normal(ar * ac).astype(dtype)
+    B = rng.standard_normal(br * bc).astype(dtype)
+    C = np.zeros(m * n, dtype=dtype)
+    dA, dB, dC = _dev(h, A), _dev(h, B), _dev(h, C)
+    L = hb.lib()
+    f = {np.float16: L.hcblasHgemm, np.float32: L.hcblasSgemm, np.float64: L.hcblasDgemm}[dtype]
+    one, zero = hb.scalar_bytes(np.dtype(dtype), 1.0), hb.scalar_bytes(np.dtype(dtype), 0.0)
+    hb.hcblasSetMathMode(h, mode, param)
+
+    def call():
+        assert f(h, op_a, op_b, m, n, k, one.ctypes.data, dA.ptr, ar, dB.ptr, br,
+                 zero.ctypes.data, dC.ptr, m) == 0
+    return call, (dA, dB, dC)
+
+
+def _complex(h, dtype, op_a, op_b, m, n, k, mode=0, param=0, seed=4):
+    rng = np.random.default_rng(seed)
+    ar, ac = (m, k) if op_a == N_ else (k, m)
+    br, bc = (k, n) if op_b == N_ else (n, k)
+    A = (rng.standard_normal(ar * ac) + 1j * rng.standard_normal(ar * ac)).astype(dtype)
+    B = (rng.standard_normal(br * bc) + 1j * rng.standard_normal(br * bc)).astype(dtype)
+    C = np.zeros(m * n, dtype=dtype)
+    dA, dB, dC = _dev(h, A), _dev(h, B), _dev(h, C)
+    L = hb.lib()
+    f = L.hcblasCgemm if dtype == np.complex64 else L.hcblasZgemm
+    al = hb.scalar_bytes(np.dtype(dtype), 1 + 0.5j)
+    be = hb.scalar_bytes(np.dtype(dtype), 0.5 - 0.25j)
+    hb.hcblasSetMathMode(h, mode, param)
+
+    def call():
+        assert f(h, op_a, op_b, m, n, k, al.ctypes.data, dA.ptr, ar, dB.ptr, br, be.ctypes.data,
+                 dC.ptr, m) == 0
+    return call, (dA, dB, dC)
+
+
+def _grouped(h, count=4096, seed=3):
+    """Uneven grouped HGEMM: M, N, K log-uniform integers in [16, 1024],
+    mixed N/T, leading dimensions padded to 8 elements (TMA rule)."""
+    rng = np.random.default_rng(seed)
+    lu = lambda: int(np.exp(rng.uniform(np.log(16), np.log(1025))))
+    probs, keep = [], []
+    for _ in range(count):
+        ta, tb = int(rng.integers(0, 2)), int(rng.integers(0, 2))
+        m, n, k = lu(), lu(), lu()
+        r8 = lambda v: -(-v // 8) * 8
+        lda, ldb = r8(m if ta == 0 else k), r8(k if tb == 0 else n)
+        A = rng.uniform(-1, 1, lda * (k if ta == 0 else m)).astype(np.float16)
+        B = rng.uniform(-1, 1, ldb * (n if tb == 0 else k)).astype(np.float16)
+        dA, dB = _dev(h, A), _dev(h, B)
+        dC = hb.DeviceArray(h, nbytes=2 * m * n, dtype=np.float16)
+        keep += [dA, dB, dC]
+        probs.append(hb.GemmProblem(ta, tb, m, n, k, dA.ptr, lda, dB.ptr, ldb, dC.ptr, m))
+    arr = (hb.GemmProblem * count)(*probs)
+    one = np.array([1.0], np.float16).view(np.uint16)
+    zero = np.array([0.0], np.float16).view(np.uint16)
+
+    def call():
+        assert hb.lib().hcblasHgemmGrouped(h, count, ctypes.cast(arr, ctypes.c_void_p),
+                                           one.ctypes.data, zero.ctypes.data) == 0
+    return call, (keep, arr)
+
+
+def _strided(h, batch=512, n=128, seed=5):
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1, 1, n * n * batch).astype(np.float16)
+    B = rng.uniform(-1, 1, n * n * batch).astype(np.float16)
+    dA, dB = _dev(h, A), _dev(h, B)
+    dC = hb.DeviceArray(h, nbytes=2 * n * n * batch, dtype=np.float16)
+
+    def call():
+        assert hb.gemm_strided_batched(h, 0, 0, n, n, n, 1.0, dA, n, n * n, dB, n, n * n, 0.0,
+                                       dC, n, n * n, batch) == 0
+    return call, (dA, dB, dC)
+
+
+CASES = {
+    "hgemm_nt_8192": lambda h: _real(h, np.float16, N_, T_, 8192, 8192, 8192),
+    "sgemm_plain_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096),
+    "sgemm_split6_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096, 1, 6),
+    "sgemm_split3_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096, 1, 3),
+    "dgemm_native_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096),
+    "dgemm_crt15_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096, 4, 15),
+    "cgemm_plain_cn_2048": lambda h: _complex(h, np.complex64, C_, N_, 2048, 2048, 2048),
+    "cgemm_split3m_cn_2048": lambda h: _complex(h, np.complex64, C_, N_, 2048, 2048, 2048, 1, 6),
+    "zgemm_native_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048),
+    "zgemm_crt3m_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048, 4, 0),
+    "hgemm_grouped_4096": _grouped,
+    "hgemm_strided_512x128": _strided,
+}
+
+
+def main(argv):
+    if not argv or argv[0] == "--list":
+        print("\n".join(CASES))
+        return 0
+    import torch
+    torch.cuda.set_device(0)
+    s, h = hb.hcblasCreate(0)
+    assert s == 0
+    for name in argv:
+        call, keep = CASES[name](h)
+        call()  # warm-up (and plan / workspace set-up)
+        torch.cuda.synchronize()
+        call()  # the call to profile
+        torch.cuda.synchronize()
+        assert hb.device_error(h) == 0, name
+        print(f"{name}: path {hb.hcblasGetLastPath(h)}", flush=True)
+        del keep
+    hb.hcblasDestroy(h)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
