@@ -25,7 +25,11 @@ Printed (rank 0, one JSON line):
   secondary   the stated targets at 8192^3: emulated vs native DGEMM
               (column-major NT) and split-BF16 vs plain SGEMM (column-major
               TN, N(0,1) * 2^e, e ~ U{-8..8} per row / column, seed 2), each
-              with its error against the oracle on sampled columns
+              with its error against the oracle on sampled columns; plain
+              SGEMM row-major NN 1024^3; the f16 strided batch 512 x 128^3 and
+              the grouped batch of 4096 uneven problems against per-problem
+              calls; CGEMM (3M split-BF16 vs plain) and ZGEMM (CRT 3M vs
+              native) at 2048^3 with A conjugate-transposed
 
 Multi-GPU: GEMM calls are independent problems here (replicas only): every rank
 runs the same workload on its own GPU; no collective is in the data path.
@@ -522,7 +526,98 @@ def run_secondary(hb, L, h, stream, torch, O, n=8192, reps=3):
                    "ms": round(ms, 3), "normwise_err": err}
     s["speedup_x6_vs_plain"] = round(s["split_bf16x6"]["tflops"] / s["plain"]["tflops"], 3)
     out["sgemm_colmajor_TN_8192^3"] = s
+    del dA, dB, dC, A, B
+    out.update(run_secondary_small(hb, h, stream, torch, O, timed))
     hb.hcblasSetMathMode(h, MATH_CRT, 0)
+    return out
+
+
+def run_secondary_small(hb, h, stream, torch, O, timed):
+    """The other configurations of the metric: plain SGEMM row-major NN
+    1024^3; uniform strided and grouped uneven batches (f16); complex 2048^3
+    with A conjugate-transposed."""
+    import ctypes
+    out = {}
+    # C1: SGEMM row-major NN 1024^3, alpha 1, beta 0.5, U[-1,1) seed 0
+    n = 1024
+    rng = np.random.default_rng(0)
+    A, B, C = (rng.uniform(-1, 1, n * n).astype(np.float32) for _ in range(3))
+    dA, dB, dC = hb.DeviceArray(h, A), hb.DeviceArray(h, B), hb.DeviceArray(h, C)
+    hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
+    f = lambda: hb.lib_gemm(h, 0, "n", "n", n, n, n, 1.0, dA, n, dB, n, 0.5, dC, n)
+    ms = timed(f)
+    dC.upload(C)
+    assert f() == 0
+    _, ref = O.gemm(O.ROW, 0, 0, n, n, n, 1.0, A, n, B, n, 0.5, C, n)
+    err = O.normwise_rel_error(O.view_c(dC.download(), O.ROW, n, n, n), ref)
+    out["sgemm_rowmajor_NN_1024^3"] = {"path": hb.hcblasGetLastPath(h),
+                                       "tflops": round(2 * n ** 3 / ms / 1e9, 2),
+                                       "ms": round(ms, 4), "normwise_err": err}
+    # C4a: uniform strided HGEMM batch 512 x 128^3
+    b, n = 512, 128
+    A = rng.uniform(-1, 1, n * n * b).astype(np.float16)
+    B = rng.uniform(-1, 1, n * n * b).astype(np.float16)
+    dA, dB = hb.DeviceArray(h, A), hb.DeviceArray(h, B)
+    dC = hb.DeviceArray(h, nbytes=2 * n * n * b, dtype=np.float16)
+    f = lambda: hb.gemm_strided_batched(h, 0, 0, n, n, n, 1.0, dA, n, n * n, dB, n, n * n, 0.0,
+                                        dC, n, n * n, b)
+    ms = timed(f)
+    out["hgemm_strided_batch_512x128^3"] = {"path": hb.hcblasGetLastPath(h),
+                                            "tflops": round(2 * b * n ** 3 / ms / 1e9, 2),
+                                            "ms": round(ms, 4)}
+    del dA, dB, dC
+    # C4b: grouped 4096 problems, M, N, K log-uniform in [16, 1024], seed 3, mixed N/T
+    from hcblas_b200 import profile_cases
+    call, keep = profile_cases.CASES["hgemm_grouped_4096"](h)
+    ms = timed(call)
+    arr = keep[1]
+    flop = sum(2.0 * p.m * p.n * p.k for p in arr)
+    one = np.array([1.0], np.float16).view(np.uint16)
+    zero = np.array([0.0], np.float16).view(np.uint16)
+    L = hb.lib()
+
+    def per_problem():
+        for p in arr:
+            L.hcblasHgemm(h, p.transa, p.transb, p.m, p.n, p.k, one.ctypes.data, p.A, p.lda, p.B,
+                          p.ldb, zero.ctypes.data, p.C, p.ldc)
+    ms_single = timed(per_problem)
+    out["hgemm_grouped_4096_uneven"] = {
+        "path": "tc.h.grouped", "gflop": round(flop / 1e9, 2), "ms": round(ms, 4),
+        "tflops": round(flop / ms / 1e9, 2), "per_problem_calls_ms": round(ms_single, 3),
+        "speedup_vs_per_problem": round(ms_single / ms, 2)}
+    del keep, arr, call
+    # C5: complex 2048^3, op(A) = A^H, alpha (1, 0.5), beta (0.5, -0.25), seed 4
+    n = 2048
+    cols = np.random.default_rng(7).choice(n, 4, replace=False)
+    rng = np.random.default_rng(4)
+    for name, dt, modes in (("cgemm", np.complex64, (("plain_4m", MATH_NATIVE, 0),
+                                                     ("split3m_bf16x6", MATH_SPLIT, 6))),
+                            ("zgemm", np.complex128, (("native", MATH_NATIVE, 0),
+                                                      ("crt3m", MATH_CRT, 0)))):
+        A = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(dt)
+        B = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(dt)
+        C = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(dt)
+        dA, dB, dC = hb.DeviceArray(h, A), hb.DeviceArray(h, B), hb.DeviceArray(h, C)
+        al, be = (1 + 0.5j), (0.5 - 0.25j)
+        Bs = np.ascontiguousarray(B.reshape(n, n)[cols, :]).reshape(-1)
+        Cs = np.ascontiguousarray(C.reshape(n, n)[cols, :]).reshape(-1)
+        _, ref = O.gemm(O.COL, 2, 0, n, len(cols), n, al, A.astype(np.complex128), n,
+                        Bs.astype(np.complex128), n, be, Cs.astype(np.complex128), n)
+        d = {}
+        for label, mode, par in modes:
+            hb.hcblasSetMathMode(h, mode, par)
+            f = lambda: hb.lib_gemm(h, 1, "c", "n", n, n, n, al, dA, n, dB, n, be, dC, n)
+            ms = timed(f)
+            dC.upload(C)
+            assert f() == 0
+            got = dC.download().reshape(n, n).T[:, cols]
+            d[label] = {"path": hb.hcblasGetLastPath(h), "tflops": round(8 * n ** 3 / ms / 1e9, 2),
+                        "ms": round(ms, 4), "normwise_err": O.normwise_rel_error(got, ref)}
+        k0, k1 = (m[0] for m in modes)
+        d["speedup"] = round(d[k1]["tflops"] / d[k0]["tflops"], 3)
+        out[f"{name}_colmajor_CN_2048^3"] = d
+        del dA, dB, dC
+    hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
     return out
 
 
