@@ -37,6 +37,12 @@ int simt(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char 
   const int64_t big = (a->dtype == HCBK_C || a->dtype == HCBK_Z) ? 64 : 128;
   hcbk_simt_cfg cfg;
   cfg.variant = (tiles_of(a->m, a->n, big, big) * a->batch >= sms) ? 0 : 1;
+  if (st->autotune && a->beta_re == 0.0 && a->beta_im == 0.0) /* re-running is harmless */
+    cfg.variant = tune_choice(st, stream, tune_key("simt", a), 2, [&](int i) {
+      hcbk_simt_cfg c;
+      c.variant = i;
+      return hcbk_gemm_simt(a, c, stream);
+    }, cfg.variant);
   static const char *names[5][2] = {
       {"simt.s.128x128", "simt.s.64x64"}, {"simt.d.128x128", "simt.d.64x64"},
       {"simt.c.64x64", "simt.c.64x64"},   {"simt.z.64x64", "simt.z.64x64"},
@@ -64,8 +70,17 @@ int hgemm_tc(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const c
     return HCBK_ERR_ALIGN;
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;
-  const int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
-  const int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
+  int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
+  if (st->autotune && st->tc_pair == 1 && a->beta_re == 0.0) {
+    /* candidates: 128x128, 128x256, 256x256 over a CTA pair */
+    static const int cbn[3] = {128, 256, 256}, cpair[3] = {0, 0, 1};
+    const int c = tune_choice(st, stream, tune_key("hgemm_tc", a), 3, [&](int i) {
+      return hcbk_hgemm_tc(a, cbn[i], cpair[i], err, stream);
+    }, pair ? 2 : bn == 256 ? 1 : 0);
+    bn = cbn[c];
+    pair = cpair[c];
+  }
   *path = pair ? "tc.h.256x256.pair" : bn == 256 ? "tc.h.128x256" : "tc.h.128x128";
   return timed_launch(st, stream, *path,
                       [&] { return hcbk_hgemm_tc(a, bn, pair, err, stream); });
@@ -420,9 +435,9 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
 
   /* every modulus in one persistent launch: the tile walk covers nmod
    * planes, so the tile-count thresholds count all of them */
-  const int pair = st->tc_pair == 2 ||
-                   (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * nmod >= hcbk_sm_count() / 2);
-  const int bn = pair || tiles_of(a->m, a->n, 128, 256) * nmod >= hcbk_sm_count() ? 256 : 128;
+  int pair = st->tc_pair == 2 ||
+             (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * nmod >= hcbk_sm_count() / 2);
+  int bn = pair || tiles_of(a->m, a->n, 128, 256) * nmod >= hcbk_sm_count() ? 256 : 128;
   hcbk_crt_gemm g;
   g.m = a->m;
   g.n = a->n;
@@ -440,6 +455,18 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   g.t_plane_stride = (int64_t)(t_pl / 2);
   g.pair = pair;
   g.bn = bn;
+  if (st->autotune && st->tc_pair == 1) {
+    /* every candidate writes the same exact residues: tuning in place is safe */
+    static const int cbn[3] = {128, 256, 256}, cpair[3] = {0, 0, 1};
+    const int c = tune_choice(st, stream, tune_key("crt_modgemm", a), 3, [&](int i) {
+      hcbk_crt_gemm gi = g;
+      gi.bn = cbn[i];
+      gi.pair = cpair[i];
+      return hcbk_crt_gemm_tc(&gi, err, stream);
+    }, pair ? 2 : bn == 256 ? 1 : 0);
+    g.bn = cbn[c];
+    g.pair = cpair[c];
+  }
   rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   if (rc) return rc;
 

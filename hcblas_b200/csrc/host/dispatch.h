@@ -7,6 +7,9 @@
 
 #include <stdint.h>
 
+#include <functional>
+#include <string>
+
 #include "../../../include/hcblas.h"
 #include "../../../include/hcblaslib.h"
 #include "../kernels/hcbk.h"
@@ -40,6 +43,14 @@ hcblasStatus run_gemm(Hcblaslibrary *h, const hc::accelerator_view &view, GemmCa
 /* Choose and launch the kernel path for a canonical (column-major, alpha != 0)
  * problem.  Returns an HCBK_* code; *path names the path taken. */
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path);
+
+/* Autotuner (tune.cpp): the size-bucket key of a call for a kernel family,
+ * and the fastest of `ncand` candidates -- run(i) launches candidate i and
+ * returns an HCBK_* code -- measured once per key while the handle's
+ * "autotune" knob is on (else `fallback`). */
+std::string tune_key(const char *family, const hcbk_gemm_args *a);
+int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int ncand,
+                const std::function<int(int)> &run, int fallback);
 
 /* Grouped HGEMM over `count` problems (grouped.cpp): builds or reuses the
  * handle's device problem table and runs the persistent kernel. */

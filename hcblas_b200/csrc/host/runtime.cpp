@@ -386,6 +386,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->split_promote_kb = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "autotune") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->autotune = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   if (std::strcmp(name, "graphs") == 0) {
     if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
     handle->impl->graphs = value;

@@ -67,6 +67,8 @@ struct HcblasB200State {
   HcblasGroupedPlan grouped;
   /* CUDA-graph replay of repeated identical calls (off by default) */
   int graphs = 0;
+  /* time candidate tile configurations per size bucket (off by default) */
+  int autotune = 0;
   unsigned workspace_epoch = 0; /* bumped whenever a buffer a graph may reference moves */
   std::vector<HcblasGraphEntry> graph_cache;
 };

@@ -339,6 +339,15 @@ hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
  *   "split_promote_kb"  split-BF16 paths: 64-element K-slabs accumulated in
  *                       TMEM before each promotion to the IEEE f32
  *                       accumulator (1 or 4; default 1).
+ *   "autotune"          1: the first call in each size bucket (kernel family,
+ *                       type, transposes, ceil(log2) of M, N, K) times every
+ *                       candidate tile configuration (SIMT tile; HGEMM
+ *                       128x128 / 128x256 / CTA-pair 256x256; CRT modular
+ *                       GEMM the same three) and keeps the fastest, for this
+ *                       process and, when HCBLAS_AUTOTUNE_CACHE names a file,
+ *                       for later ones; only offered where re-running the
+ *                       kernel is harmless (beta == 0, or the CRT residues);
+ *                       0 (default): size heuristics.
  *   "graphs"            1: a call identical to an earlier one (same
  *                       arguments, pointers, math mode and knobs, same
  *                       non-default stream) replays a CUDA graph captured
