@@ -432,6 +432,31 @@ struct TcCfg {
  *   spans only n*128 bytes of K, which bounds the error it adds; used by the
  *   split-BF16 paths, whose contract is "error no worse than FP32".
  */
+/* The work sequence every role of a CTA walks, as (tile, chunk, slot)
+ * items.  Normally a CTA's tiles come one after the other, chunk by chunk.
+ * In the in-place modular mode its tiles go in pairs whose chunks alternate
+ * -- (X,0) (Y,0) (X,1) (Y,1) ... -- with X in TMEM buffer 0 and Y in buffer 1,
+ * so that while the epilogue reduces (or finally stores) one tile's buffer
+ * the tensor core fills the other's; an unpaired last tile uses buffer 0. */
+struct WorkItem {
+  int t, c, slot;
+};
+
+__device__ __forceinline__ WorkItem work_item(int i, int tile0, int step, int ntiles_local,
+                                              int nchunks, bool pairs) {
+  if (pairs) {
+    const int full = (ntiles_local >> 1) * 2 * nchunks;
+    if (i < full) {
+      const int pr = i / (2 * nchunks), r = i - pr * 2 * nchunks;
+      const int slot = r & 1;
+      return WorkItem{tile0 + (2 * pr + slot) * step, r >> 1, slot};
+    }
+    return WorkItem{tile0 + (ntiles_local - 1) * step, i - full, 0};
+  }
+  const int lt = i / nchunks;
+  return WorkItem{tile0 + lt * step, i - lt * nchunks, 0};
+}
+
 template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
           int CG = 1>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
@@ -497,6 +522,10 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   const int tile0 = blockIdx.x / CG, tile_step = gridDim.x / CG;
   const int kblocks = (p.k + BKE - 1) / BKE;
   const int chunk_kb = PROMOTE_KB > 0 ? PROMOTE_KB : kblocks;
+  const int nchunks = (kblocks + chunk_kb - 1) / chunk_kb;
+  const int ntiles_local = tile0 < num_tiles ? (num_tiles - tile0 + tile_step - 1) / tile_step : 0;
+  constexpr bool PAIRS = EPI::INPLACE && PROMOTE_KB > 0;
+  const int nitems = ntiles_local * nchunks;
 
   if (warp == 0) {
     /* ------------------------------------------------ TMA producer -- */
@@ -504,13 +533,16 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
-      for (int t = tile0; ok && t < num_tiles; t += tile_step) {
+      for (int i = 0; ok && i < nitems; ++i) {
+        const WorkItem w = work_item(i, tile0, tile_step, ntiles_local, nchunks, PAIRS);
+        const int t = w.t;
         const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
         const int tt = t - plane * tiles_per_plane;
         const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
         const int row0 = (tm * CG + (int)rank) * BM;               /* this CTA's A rows */
         const int col0 = tn * BN + (int)rank * (int)Cfg::B_ROWS;   /* this CTA's B rows */
-        for (int kb = 0; kb < kblocks; ++kb) {
+        const int kb_end = (w.c + 1) * chunk_kb < kblocks ? (w.c + 1) * chunk_kb : kblocks;
+        for (int kb = w.c * chunk_kb; kb < kb_end; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
             ok = false;
             break;
@@ -577,15 +609,16 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       int ci = 0; /* chunk counter (all tiles): selects the TMEM buffer */
       uint32_t uses = 0u; /* in-place mode: bit b = parity of buffer b's acquisitions */
       bool ok = true;
-      for (int t = tile0; ok && t < num_tiles; t += tile_step) {
-        int c = 0; /* chunk index within the tile */
-        for (int kc = 0; ok && kc < kblocks; kc += chunk_kb, ++ci, ++c) {
-          /* in-place mode: chunk c of every tile accumulates into buffer
-           * c % 2 on top of the epilogue's reduced value of chunk c - 2 */
-          const int b = EPI::INPLACE ? (c & 1) : ci % NBUF;
-          const uint32_t tph = EPI::INPLACE ? (uses >> b) & 1u : (ci / NBUF) & 1;
-          if (EPI::INPLACE) uses ^= 1u << b;
-          const bool fresh = !EPI::INPLACE || c < 2;
+      for (int i = 0; ok && i < nitems; ++i, ++ci) {
+        {
+          const WorkItem w = work_item(i, tile0, tile_step, ntiles_local, nchunks, PAIRS);
+          const int kc = w.c * chunk_kb;
+          /* in-place mode: chunk c of a tile accumulates into its slot's
+           * buffer on top of the epilogue's reduced value of chunk c - 1 */
+          const int b = PAIRS ? w.slot : ci % NBUF;
+          const uint32_t tph = PAIRS ? (uses >> b) & 1u : (ci / NBUF) & 1;
+          if (PAIRS) uses ^= 1u << b;
+          const bool fresh = !PAIRS || w.c == 0;
           if (!mbar_wait<CG == 2>(&tempty[b], tph ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
             ok = false;
             break;
@@ -651,6 +684,32 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       }
     };
     uint32_t euses = 0u; /* in-place mode: bit b = parity of buffer b's acquisitions */
+    if constexpr (PAIRS) {
+      /* in-place modular mode: every chunk but a tile's last is reduced in
+       * place and handed back; the last is reduced and stored from the same
+       * buffer while the tensor core works on the pair's other tile */
+      const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+      for (int i = 0; i < nitems; ++i) {
+        const WorkItem w = work_item(i, tile0, tile_step, ntiles_local, nchunks, true);
+        const int plane = EPI::PLANE_BATCH ? w.t / tiles_per_plane : 0;
+        const int tt = w.t - plane * tiles_per_plane;
+        const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
+        const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
+        const int b = w.slot;
+        const uint32_t tph = (euses >> b) & 1u;
+        euses ^= 1u << b;
+        if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) break;
+        tc_fence_after();
+        const uint32_t tb = tmem_base + lane_off + b * Cfg::ACC_COLS;
+        if (w.c < nchunks - 1)
+          EPI::template rmw<BN>(p, tb, plane);
+        else
+          EPI::template final_store<BN>(p, tb, tb, false, m, tn * BN, plane);
+        tc_fence_before();
+        __syncwarp();
+        release(b);
+      }
+    } else {
     for (int t = tile0; ok && t < num_tiles; t += tile_step) {
       const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
       const int tt = t - plane * tiles_per_plane;
@@ -668,36 +727,6 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         tc_fence_before();
         __syncwarp();
         release(b);
-      } else if constexpr (EPI::INPLACE) {
-        /* chunks 0 .. n-3 are reduced in place and handed back; the last
-         * two (one if n == 1) stay held until the tile's final store */
-        const int nchunks = (kblocks + chunk_kb - 1) / chunk_kb;
-        const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
-        for (int c = 0; c < nchunks; ++c) {
-          const int b = c & 1;
-          const uint32_t tph = (euses >> b) & 1u;
-          euses ^= 1u << b;
-          if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          if (c < nchunks - 2) {
-            EPI::template rmw<BN>(p, tmem_base + lane_off + b * Cfg::ACC_COLS, plane);
-            tc_fence_before();
-            __syncwarp();
-            release(b);
-          }
-        }
-        if (!ok) break;
-        const int bl = (nchunks - 1) & 1; /* buffer of the last chunk */
-        EPI::template final_store<BN>(p, tmem_base + lane_off + bl * Cfg::ACC_COLS,
-                                      tmem_base + lane_off + (bl ^ 1) * Cfg::ACC_COLS,
-                                      nchunks > 1, m, tn * BN, plane);
-        tc_fence_before();
-        __syncwarp();
-        release(bl);
-        if (nchunks > 1) release(bl ^ 1);
       } else {
         typename EPI::AccT acc[BN];
 #pragma unroll
@@ -719,6 +748,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         }
         if (ok) EPI::template store_acc<BN>(p, acc, m, tn * BN);
       }
+    }
     }
   }
 
