@@ -67,7 +67,7 @@ __device__ __forceinline__ float small_int_to_f(int x) {
 
 struct ModConst {
   float p, inv_p, hp;
-  float c1, c2, c3; /* 2^16, 2^32, 2^48 mod p (symmetric) */
+  float c1, c2, c3, c4; /* 2^11, 2^22, 2^33, 2^44 mod p (symmetric) */
 };
 
 struct ResArgs {
@@ -83,36 +83,44 @@ struct ResArgs {
   int64_t ld_dst;       /* elements */
 };
 
-/* 16-bit limbs of the scaled integer y = rint(x 2^(beta - e)), |y| <= 2^53:
- * y = l3 2^48 + l2 2^32 + l1 2^16 + l0 with |l0|,|l1|,|l2| <= 2^15 + 1 and
- * |l3| <= 2^5 + 1, all exact in f32 (0 for zero / non-finite rows) */
+/* 11-bit limbs of the scaled integer y = rint(x 2^(beta - e)), |y| <= 2^53:
+ * y = l4 2^44 + l3 2^33 + l2 2^22 + l1 2^11 + l0 with |l0..l3| <= 2^10 and
+ * |l4| <= 2^9, all exact in f32 (0 for zero / non-finite rows) */
 struct Limbs {
-  float l0, l1, l2, l3;
+  float l0, l1, l2, l3, l4;
 };
 
 __device__ __forceinline__ Limbs limbs_of(double x, int e, int beta) {
-  Limbs L{0.f, 0.f, 0.f, 0.f};
+  Limbs L{0.f, 0.f, 0.f, 0.f, 0.f};
   if (e == HCBK_OZ_NONFINITE || e == HCBK_OZ_ZERO) return L;
   const double y = rint(ldexp(x, beta - e));
-  const double h3 = rint(y * 0x1p-48);
-  double r = fma(-h3, 0x1p48, y);
-  const double h2 = rint(r * 0x1p-32);
-  r = fma(-h2, 0x1p32, r);
-  const double h1 = rint(r * 0x1p-16);
-  r = fma(-h1, 0x1p16, r);
+  const double h4 = rint(y * 0x1p-44);
+  double r = fma(-h4, 0x1p44, y);
+  const double h3 = rint(r * 0x1p-33);
+  r = fma(-h3, 0x1p33, r);
+  const double h2 = rint(r * 0x1p-22);
+  r = fma(-h2, 0x1p22, r);
+  const double h1 = rint(r * 0x1p-11);
+  r = fma(-h1, 0x1p11, r);
   L.l0 = static_cast<float>(r);
   L.l1 = static_cast<float>(h1);
   L.l2 = static_cast<float>(h2);
   L.l3 = static_cast<float>(h3);
+  L.l4 = static_cast<float>(h4);
   return L;
 }
 
-/* symmetric residue of the limb sum modulo one modulus; every partial sum
- * stays an exact integer below 2^23 */
+/* symmetric residue of the limb sum modulo one modulus.  |sum| <=
+ * 2^10 (1 + 4 * 127) < 2^19, so |sum / p| < 3200 and the f32 quotient
+ * sum * RN(1/p) is off by < 2e-4 -- less than the 0.5/p >= 0.002 distance of
+ * any x/p (p odd) from a half-integer: the rounded quotient is exact and the
+ * remainder already lies in [-(p-1)/2, (p-1)/2]. */
 __device__ __forceinline__ float residue(const Limbs &L, const ModConst &m) {
-  const float t1 = fmaf(L.l1, m.c1, L.l0);
-  const float t2 = fmaf(L.l3, m.c3, L.l2 * m.c2);
-  return sym_f(mod_f(t1 + t2, m.p, m.inv_p), m.p, m.hp);
+  float t = fmaf(L.l4, m.c4, L.l0);
+  t = fmaf(L.l3, m.c3, t);
+  t = fmaf(L.l2, m.c2, t);
+  t = fmaf(L.l1, m.c1, t);
+  return mod_f(t, m.p, m.inv_p);
 }
 
 /* K-contiguous source: 8 consecutive k per thread, 16-byte plane stores */
@@ -240,7 +248,8 @@ __device__ __forceinline__ double crt_value(const CombArgs &a, const Res &t, int
       if (g >= a.gsize[j]) break;
       const int i = i0 + g;
       const float d0 = mod_f(t[i] - x, a.p[i], a.inv_p[i]);
-      const float d = sym_f(mod_f(d0 * a.minv[i], a.p[i], a.inv_p[i]), a.p[i], a.hp[i]);
+      /* |d0 * minv| < 1.5 * 255 * 254 < 2^17: exact quotient, symmetric result */
+      const float d = mod_f(d0 * a.minv[i], a.p[i], a.inv_p[i]);
       x = fmaf(qq, d, x);
       qq *= a.p[i];
     }
@@ -325,9 +334,10 @@ static void fill_mod_consts(ModConst (&mc)[HCBK_CRT_MAX_MODULI]) {
     m.p = (float)M[i];
     m.inv_p = 1.0f / (float)M[i];
     m.hp = (float)((M[i] - 1) / 2);
-    m.c1 = pow2_mod_sym(16, M[i]);
-    m.c2 = pow2_mod_sym(32, M[i]);
-    m.c3 = pow2_mod_sym(48, M[i]);
+    m.c1 = pow2_mod_sym(11, M[i]);
+    m.c2 = pow2_mod_sym(22, M[i]);
+    m.c3 = pow2_mod_sym(33, M[i]);
+    m.c4 = pow2_mod_sym(44, M[i]);
   }
 }
 
@@ -398,7 +408,7 @@ __device__ __forceinline__ ZRes3 zresidue(const Limbs &lr, const Limbs &li, cons
   ZRes3 o;
   o.re = residue(lr, m);
   o.im = im_sign * residue(li, m);
-  o.sum = sym_f(mod_f(o.re + o.im, m.p, m.inv_p), m.p, m.hp);
+  o.sum = mod_f(o.re + o.im, m.p, m.inv_p); /* |re + im| <= 254: exact quotient */
   return o;
 }
 
