@@ -662,7 +662,33 @@ int hgemm_strided_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *st
   return rc;
 }
 
+/* Does the handle's math mode give this dtype an emulated path? */
+bool emulated_mode(const HcblasB200State *st, int dtype) {
+  switch (st->math_mode) {
+    case 1: return dtype == HCBK_S || dtype == HCBK_C;  /* split-BF16 */
+    case 2:
+    case 3: return dtype == HCBK_D;                     /* Ozaki-I */
+    case 4: return dtype == HCBK_D || dtype == HCBK_Z;  /* CRT */
+    default: return false;
+  }
+}
+
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+  if (a->batch > 1 && !a->a_array && emulated_mode(st, a->dtype)) {
+    /* strided batch under an emulated math mode: one emulated call per
+     * element, in order on the stream (they share the workspace) */
+    for (int64_t i = 0; i < a->batch; ++i) {
+      hcbk_gemm_args e = *a;
+      e.batch = 1;
+      e.a_off = a->a_off + i * a->stride_a;
+      e.b_off = a->b_off + i * a->stride_b;
+      e.c_off = a->c_off + i * a->stride_c;
+      e.stride_a = e.stride_b = e.stride_c = 0;
+      const int rc = dispatch_gemm(st, &e, stream, path);
+      if (rc) return rc;
+    }
+    return HCBK_OK;
+  }
   if (a->dtype == HCBK_H && a->batch > 1 && !a->a_array) {
     int rc = hgemm_strided_grouped(st, a, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;

@@ -333,3 +333,36 @@ def test_zgemm_crt_vs_native_accuracy(handle):
     native = [v for k, v in errs.items() if k.startswith("simt")][0]
     crt = [v for k, v in errs.items() if k.startswith("tc.zcrt")][0]
     assert crt <= native
+
+
+@pytest.mark.parametrize("kind,mode,param,prefix", [("d", hb.HCBLAS_MATH_OZAKI_CRT, 0, "tc.crt_m"),
+                                                    ("z", hb.HCBLAS_MATH_OZAKI_CRT, 0, "tc.zcrt3m_m"),
+                                                    ("s", hb.HCBLAS_MATH_SPLIT_BF16, 6, "tc.split_bf16x6"),
+                                                    ("c", hb.HCBLAS_MATH_SPLIT_BF16, 6, "tc.csplit3m_bf16x6")])
+def test_strided_batch_uses_emulated_mode(handle, kind, mode, param, prefix):
+    """A strided batch under an emulated math mode runs every element on the
+    emulated path (element-wise bound of that path, checked against the
+    oracle per element)."""
+    from tests.test_gemm_gpu import NP, rand_op
+    rng = np.random.default_rng(61)
+    M, N, K, batch = 96, 80, 200, 4
+    sA, sB, sC = M * K + 8, K * N + 8, M * N + 8
+    A, B, C = (rand_op(rng, kind, n * batch) for n in (sA, sB, sC))
+    dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+    assert hb.hcblasSetMathMode(handle, mode, param) == 0
+    try:
+        alpha = (1 + 0.5j) if kind in "cz" else 1.5
+        s = hb.gemm_strided_batched(handle, 0, 0, M, N, K, alpha, dA, M, sA, dB, K, sB, 0.0, dC,
+                                    M, sC, batch)
+        assert s == hb.HCBLAS_STATUS_SUCCESS
+        assert hb.device_error(handle) == 0
+        assert hb.hcblasGetLastPath(handle).startswith(prefix), hb.hcblasGetLastPath(handle)
+    finally:
+        hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+    got = dC.download()
+    tol = {"d": 1e-15, "z": 1e-15, "s": 2e-6, "c": 2e-6}[kind]
+    for i in range(batch):
+        _, ref = O.gemm(O.COL, 0, 0, M, N, K, alpha, A[i * sA:(i + 1) * sA], M,
+                        B[i * sB:(i + 1) * sB], K, 0.0, C[i * sC:(i + 1) * sC], M)
+        gv = O.view_c(got[i * sC:(i + 1) * sC], O.COL, M, N, M)
+        assert O.normwise_rel_error(gv, ref) < tol, i
