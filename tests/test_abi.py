@@ -157,3 +157,34 @@ def test_hc_half_from_float_rounding(cpp_caller):
     with np.errstate(over="ignore"):
         ref = xs.astype(np.float16).view(np.uint16)
     assert np.array_equal(got, ref)
+
+
+def hip_declared():
+    text = open(os.path.join(INCLUDE, "hipblas.h")).read()
+    return set(m.group(1) for m in re.finditer(r"^hipblasStatus_t\s+(\w+)\(", text, re.M))
+
+
+def test_hipblas_layer_exports_and_status_rules(built_lib):
+    """The hipBLAS-style layer (reference lib/src/hcc_detail/hipblas.cpp):
+    every declared entry point is exported; status rules hold without a GPU;
+    hipblasStatus_t keeps the reference's numbering (ARCH_MISMATCH at 4)."""
+    names = hip_declared()
+    assert len(names) >= 20, names
+    L = ctypes.CDLL(built_lib)
+    assert not [n for n in sorted(names) if not hasattr(L, n)]
+    L.hipblasCreate.argtypes = [ctypes.c_void_p]
+    L.hipblasCreate.restype = ctypes.c_int
+    L.hipblasDestroy.argtypes = [ctypes.c_void_p]
+    L.hipblasDestroy.restype = ctypes.c_int
+    assert L.hipblasCreate(None) == 3            # INVALID_VALUE
+    assert L.hipblasDestroy(None) == 1           # NOT_INITIALIZED
+    f = L.hipblasSgemm
+    vp, ci = ctypes.c_void_p, ctypes.c_int
+    f.argtypes = [vp, ci, ci, ci, ci, ci, vp, vp, ci, vp, ci, vp, vp, ci]
+    f.restype = ci
+    one = np.ones(1, np.float32)
+    p = one.ctypes.data
+    assert f(None, 0, 0, 4, 4, 4, p, p, 4, p, 4, p, p, 4) == 1   # NULL handle
+    text = open(os.path.join(INCLUDE, "hipblas.h")).read()
+    assert "HIPBLAS_STATUS_ARCH_MISMATCH = 4" in text
+    assert "HIPBLAS_STATUS_EXECUTION_FAILED = 6" in text
