@@ -57,7 +57,8 @@ EXPORTED = (
     "hcblasGetDeviceError", "hcblasSetTuningParam",
     "hcblasSetProfiling", "hcblasGetProfile", "hcblas_am_alloc", "hcblas_am_free",
     "hcblas_am_copy", "hcblas_view_wait", "hcblas_device_count", "hcblas_current_device",
-    "hcblasHgemmGrouped",
+    "hcblasHgemmGrouped", "hcblasSgemv", "hcblasDgemv", "hcblasSgemvBatched",
+    "hcblasDgemvBatched", "hcblasSger", "hcblasDger", "hcblasSgerBatched", "hcblasDgerBatched",
 )
 
 
@@ -178,6 +179,19 @@ def lib():
         L.hcblas_current_device.restype = ci
         L.hcblasHgemmGrouped.argtypes = [vp, ci, vp, vp, vp]
         L.hcblasHgemmGrouped.restype = st
+        for p in "SD":
+            f = getattr(L, f"hcblas{p}gemv")
+            f.argtypes = [vp, op, ci, ci, vp, vp, ci, vp, ci, vp, vp, ci]
+            f.restype = st
+            f = getattr(L, f"hcblas{p}gemvBatched")
+            f.argtypes = [vp, op, ci, ci, vp, vp, ci, vp, ci, vp, vp, ci, ci]
+            f.restype = st
+            f = getattr(L, f"hcblas{p}ger")
+            f.argtypes = [vp, ci, ci, vp, vp, ci, vp, ci, vp, ci]
+            f.restype = st
+            f = getattr(L, f"hcblas{p}gerBatched")
+            f.argtypes = [vp, ci, ci, vp, vp, ci, vp, ci, vp, ci, ci]
+            f.restype = st
         _lib = L
     return _lib
 
@@ -277,20 +291,26 @@ class DeviceArray:
         if host is not None:
             self.upload(host)
 
+    _CHUNK = 1 << 30  # bytes per hcblasSetMatrix / hcblasGetMatrix call (int sizes)
+
     def upload(self, host: np.ndarray):
         host = np.ascontiguousarray(host)
         assert host.nbytes == self.nbytes
-        s = hcblasSetMatrix(self.handle, host.nbytes, 1, 1, host.ctypes.data, host.nbytes,
-                            self.ptr, host.nbytes)
-        if s != HCBLAS_STATUS_SUCCESS:
-            raise RuntimeError(f"hcblasSetMatrix failed: {s}")
+        for off in range(0, host.nbytes, self._CHUNK):
+            nb = min(self._CHUNK, host.nbytes - off)
+            s = hcblasSetMatrix(self.handle, nb, 1, 1, host.ctypes.data + off, nb,
+                                self.ptr + off, nb)
+            if s != HCBLAS_STATUS_SUCCESS:
+                raise RuntimeError(f"hcblasSetMatrix failed: {s}")
 
     def download(self) -> np.ndarray:
         out = np.empty(self.size, dtype=self.dtype)
-        s = hcblasGetMatrix(self.handle, self.nbytes, 1, 1, self.ptr, self.nbytes,
-                            out.ctypes.data, self.nbytes)
-        if s != HCBLAS_STATUS_SUCCESS:
-            raise RuntimeError(f"hcblasGetMatrix failed: {s}")
+        for off in range(0, self.nbytes, self._CHUNK):
+            nb = min(self._CHUNK, self.nbytes - off)
+            s = hcblasGetMatrix(self.handle, nb, 1, 1, self.ptr + off, nb, out.ctypes.data + off,
+                                nb)
+            if s != HCBLAS_STATUS_SUCCESS:
+                raise RuntimeError(f"hcblasGetMatrix failed: {s}")
         return out
 
     def free(self):
@@ -380,3 +400,26 @@ def hgemm_grouped(handle, problems, alpha: float, beta: float) -> int:
     b = np.array([beta], dtype=np.float16).view(np.uint16)
     return lib().hcblasHgemmGrouped(handle, len(problems), ctypes.cast(arr, ctypes.c_void_p),
                                     a.ctypes.data, b.ctypes.data)
+
+
+def gemv(handle, trans, m, n, alpha, A, lda, x, incx, beta, y, incy, batch=None):
+    """hcblas{S,D}gemv[Batched] on DeviceArrays; the prefix follows ``A.dtype``."""
+    p = _PREFIX[np.dtype(A.dtype)]
+    al, be = scalar_bytes(A.dtype, alpha), scalar_bytes(A.dtype, beta)
+    if batch is None:
+        return getattr(lib(), f"hcblas{p}gemv")(handle, trans, m, n, al.ctypes.data, A.ptr, lda,
+                                                 x.ptr, incx, be.ctypes.data, y.ptr, incy)
+    return getattr(lib(), f"hcblas{p}gemvBatched")(handle, trans, m, n, al.ctypes.data, A.ptr,
+                                                    lda, x.ptr, incx, be.ctypes.data, y.ptr, incy,
+                                                    batch)
+
+
+def ger(handle, m, n, alpha, x, incx, y, incy, A, lda, batch=None):
+    """hcblas{S,D}ger[Batched] on DeviceArrays; the prefix follows ``A.dtype``."""
+    p = _PREFIX[np.dtype(A.dtype)]
+    al = scalar_bytes(A.dtype, alpha)
+    if batch is None:
+        return getattr(lib(), f"hcblas{p}ger")(handle, m, n, al.ctypes.data, x.ptr, incx, y.ptr,
+                                                incy, A.ptr, lda)
+    return getattr(lib(), f"hcblas{p}gerBatched")(handle, m, n, al.ctypes.data, x.ptr, incx,
+                                                   y.ptr, incy, A.ptr, lda, batch)

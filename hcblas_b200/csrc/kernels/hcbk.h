@@ -310,6 +310,45 @@ typedef struct hcbk_zcrt_combine_args {
 } hcbk_zcrt_combine_args;
 int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *a, void *stream);
 
+/* ------------------------------------------------------ GEMV and GER -- */
+
+/* y := alpha * op(A) x + beta * y for column-major A (m x n, lda),
+ * op = A (trans = 0: x has n, y has m entries) or A^T (trans = 1: x has m,
+ * y has n); positive increments; beta == 0 means y is not read.  Partial
+ * sums of at most max_splits slices go to `workspace` (see
+ * hcbk_gemv_workspace_elems, elements of the dtype). */
+typedef struct hcbk_gemv_args {
+  int dtype; /* HCBK_S or HCBK_D */
+  int trans;
+  int64_t m, n;
+  const void *a;
+  int64_t lda;
+  const void *x;
+  int64_t incx;
+  void *y;
+  int64_t incy;
+  double alpha, beta;
+  void *workspace;
+  int max_splits;
+} hcbk_gemv_args;
+int hcbk_gemv(const hcbk_gemv_args *g, void *stream);
+int64_t hcbk_gemv_workspace_elems(int64_t m, int64_t n, int trans, int max_splits);
+
+/* A := alpha * x y^T + A, column-major m x n; x, y point at their logical
+ * first elements (increments may be negative, not zero). */
+typedef struct hcbk_ger_args {
+  int dtype; /* HCBK_S or HCBK_D */
+  int64_t m, n;
+  double alpha;
+  const void *x;
+  int64_t incx;
+  const void *y;
+  int64_t incy;
+  void *a;
+  int64_t lda;
+} hcbk_ger_args;
+int hcbk_ger(const hcbk_ger_args *g, void *stream);
+
 /* ----------------------------------------------- grouped (uneven) GEMM -- */
 
 /* One problem of a grouped HGEMM, as the persistent kernel reads it from

@@ -104,6 +104,30 @@ def _strided(h, batch=512, n=128, seed=5):
     return call, (dA, dB, dC)
 
 
+def _gemv(h, dtype, trans, m, n, seed=6):
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1, 1, m * n).astype(dtype)
+    x = rng.uniform(-1, 1, n if trans == 0 else m).astype(dtype)
+    y = np.zeros(m if trans == 0 else n, dtype=dtype)
+    dA, dx, dy = _dev(h, A), _dev(h, x), _dev(h, y)
+
+    def call():
+        assert hb.gemv(h, trans, m, n, 1.0, dA, m, dx, 1, 0.0, dy, 1) == 0
+    return call, (dA, dx, dy)
+
+
+def _ger(h, dtype, m, n, seed=7):
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1, 1, m * n).astype(dtype)
+    x = rng.uniform(-1, 1, m).astype(dtype)
+    y = rng.uniform(-1, 1, n).astype(dtype)
+    dA, dx, dy = _dev(h, A), _dev(h, x), _dev(h, y)
+
+    def call():
+        assert hb.ger(h, m, n, 0.5, dx, 1, dy, 1, dA, m) == 0
+    return call, (dA, dx, dy)
+
+
 CASES = {
     "hgemm_nt_8192": lambda h: _real(h, np.float16, N_, T_, 8192, 8192, 8192),
     "sgemm_plain_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096),
@@ -117,6 +141,12 @@ CASES = {
     "zgemm_crt3m_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048, 4, 0),
     "hgemm_grouped_4096": _grouped,
     "hgemm_strided_512x128": _strided,
+    "sgemv_n_16384": lambda h: _gemv(h, np.float32, 0, 16384, 16384),
+    "sgemv_t_16384": lambda h: _gemv(h, np.float32, 1, 16384, 16384),
+    "dgemv_n_16384": lambda h: _gemv(h, np.float64, 0, 16384, 16384),
+    "dgemv_t_16384": lambda h: _gemv(h, np.float64, 1, 16384, 16384),
+    "sger_16384": lambda h: _ger(h, np.float32, 16384, 16384),
+    "dger_16384": lambda h: _ger(h, np.float64, 16384, 16384),
 }
 
 

@@ -231,6 +231,47 @@ hcblasStatus_t hcblasHgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_
                                          hcblasHalf *C, int ldc, long long strideC,
                                          int batchCount);
 
+/* ------------------------------------------------------- GEMV and GER -- */
+
+/* Reference: lib/include/hcblas.h:516-534, lib/src/hcblas.cpp:967-1060.
+ * y := alpha*op(A)*x + beta*y, A m x n in the handle's order; op(A) = A for
+ * HCBLAS_OP_N, A^T otherwise.  Status: NULL handle -> NOT_INITIALIZED;
+ * m, n < 0 or incx, incy == 0 -> INVALID_VALUE; m or n == 0, a NULL array or
+ * a negative increment -> EXECUTION_FAILED (the class layer's quick return,
+ * sgemv_array.cpp:833-836).  Batched: batchCount problems at the reference's
+ * implicit batch offsets -- A: m*n, x: length of x, y: length of y (in
+ * elements, whatever the increments; hcblas.cpp:1009-1019).  Unlike the
+ * reference, lda is honoured (the reference assumes lda == m). */
+hcblasStatus_t hcblasSgemv(hcblasHandle_t handle, hcblasOperation_t trans, int m, int n,
+                           const float *alpha, float *A, int lda, float *x, int incx,
+                           const float *beta, float *y, int incy);
+hcblasStatus_t hcblasSgemvBatched(hcblasHandle_t handle, hcblasOperation_t trans, int m, int n,
+                                  const float *alpha, float *A, int lda, float *x, int incx,
+                                  const float *beta, float *y, int incy, int batchCount);
+hcblasStatus_t hcblasDgemv(hcblasHandle_t handle, hcblasOperation_t trans, int m, int n,
+                           const double *alpha, double *A, int lda, double *x, int incx,
+                           const double *beta, double *y, int incy);
+hcblasStatus_t hcblasDgemvBatched(hcblasHandle_t handle, hcblasOperation_t trans, int m, int n,
+                                  const double *alpha, double *A, int lda, double *x, int incx,
+                                  const double *beta, double *y, int incy, int batchCount);
+
+/* Reference: lib/include/hcblas.h:573-586, lib/src/hcblas.cpp:1130-1230.
+ * A := alpha*x*y^T + A (m x n, handle's order).  Status as GEMV except that a
+ * negative increment is allowed (BLAS: the vector runs backwards from its
+ * last stored element); alpha == 0 leaves A untouched.  Batched offsets:
+ * x: m, y: n, A: m*n elements. */
+hcblasStatus_t hcblasSger(hcblasHandle_t handle, int m, int n, const float *alpha,
+                          const float *x, int incx, const float *y, int incy, float *A, int lda);
+hcblasStatus_t hcblasDger(hcblasHandle_t handle, int m, int n, const double *alpha,
+                          const double *x, int incx, const double *y, int incy, double *A,
+                          int lda);
+hcblasStatus_t hcblasSgerBatched(hcblasHandle_t handle, int m, int n, const float *alpha,
+                                 const float *x, int incx, const float *y, int incy, float *A,
+                                 int lda, int batchCount);
+hcblasStatus_t hcblasDgerBatched(hcblasHandle_t handle, int m, int n, const double *alpha,
+                                 const double *x, int incx, const double *y, int incy,
+                                 double *A, int lda, int batchCount);
+
 /* Extension (no counterpart in the reference's C API): grouped GEMM --
  * one call computes many independent, unevenly sized f16 GEMMs
  *   C_i := alpha * op(A_i) * op(B_i) + beta * C_i,  i = 0 .. count-1

@@ -153,6 +153,60 @@ struct Hcblaslibrary {
                             hc::short_vector::double_2 *C[], const int64_t cOffset,
                             const int64_t C_batchOffset, const int64_t ldc,
                             const int batchSize);
+
+  /* GEMV / GER (reference lib/include/hcblaslib.h:140-230): y = alpha op(A) x
+   * + beta y and A = alpha x y^T + A, element offsets, strided batches with
+   * explicit batch offsets.  Quick returns as the reference's
+   * (sgemv_array.cpp:833-836, sger_array.cpp:134-141): a NULL vector or
+   * matrix, M or N <= 0, or (GEMV) an increment <= 0 / (GER) == 0 ->
+   * HCBLAS_INVALID; GER with alpha == 0 leaves A untouched.  Unlike the
+   * reference, lda is honoured (the reference assumes lda == M). */
+  hcblasStatus hcblas_sgemv(hc::accelerator_view accl_view, hcblasOrder order,
+                            hcblasTranspose type, const int M, const int N, const float &alpha,
+                            float *A, const int64_t aOffset, const int lda, float *X,
+                            const int64_t xOffset, const int incX, const float &beta, float *Y,
+                            const int64_t yOffset, const int incY);
+  hcblasStatus hcblas_sgemv(hc::accelerator_view accl_view, hcblasOrder order,
+                            hcblasTranspose type, const int M, const int N, const float &alpha,
+                            float *A, const int64_t aOffset, const int64_t A_batchOffset,
+                            const int lda, float *X, const int64_t xOffset,
+                            const int64_t X_batchOffset, const int incX, const float &beta,
+                            float *Y, const int64_t yOffset, const int64_t Y_batchOffset,
+                            const int incY, const int batchSize);
+  hcblasStatus hcblas_dgemv(hc::accelerator_view accl_view, hcblasOrder order,
+                            hcblasTranspose type, const int M, const int N, const double &alpha,
+                            double *A, const int64_t aOffset, const int lda, double *X,
+                            const int64_t xOffset, const int incX, const double &beta,
+                            double *Y, const int64_t yOffset, const int incY);
+  hcblasStatus hcblas_dgemv(hc::accelerator_view accl_view, hcblasOrder order,
+                            hcblasTranspose type, const int M, const int N, const double &alpha,
+                            double *A, const int64_t aOffset, const int64_t A_batchOffset,
+                            const int lda, double *X, const int64_t xOffset,
+                            const int64_t X_batchOffset, const int incX, const double &beta,
+                            double *Y, const int64_t yOffset, const int64_t Y_batchOffset,
+                            const int incY, const int batchSize);
+  hcblasStatus hcblas_sger(hc::accelerator_view accl_view, hcblasOrder order, const int M,
+                           const int N, const float &alpha, const float *X,
+                           const int64_t xOffset, const int incX, const float *Y,
+                           const int64_t yOffset, const int incY, float *A,
+                           const int64_t aOffset, const int lda);
+  hcblasStatus hcblas_sger(hc::accelerator_view accl_view, hcblasOrder order, const int M,
+                           const int N, const float &alpha, const float *X,
+                           const int64_t xOffset, const int64_t X_batchOffset, const int incX,
+                           const float *Y, const int64_t yOffset, const int64_t Y_batchOffset,
+                           const int incY, float *A, const int64_t aOffset,
+                           const int64_t A_batchOffset, const int lda, const int batchSize);
+  hcblasStatus hcblas_dger(hc::accelerator_view accl_view, hcblasOrder order, const int M,
+                           const int N, const double &alpha, const double *X,
+                           const int64_t xOffset, const int incX, const double *Y,
+                           const int64_t yOffset, const int incY, double *A,
+                           const int64_t aOffset, const int lda);
+  hcblasStatus hcblas_dger(hc::accelerator_view accl_view, hcblasOrder order, const int M,
+                           const int N, const double &alpha, const double *X,
+                           const int64_t xOffset, const int64_t X_batchOffset, const int incX,
+                           const double *Y, const int64_t yOffset, const int64_t Y_batchOffset,
+                           const int incY, double *A, const int64_t aOffset,
+                           const int64_t A_batchOffset, const int lda, const int batchSize);
 };
 
 #endif /* HCBLAS_B200_HCBLASLIB_H_ */
