@@ -378,7 +378,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int64_t kp = (a->k + 7) & ~int64_t(7); /* 16-byte f16 row pitch */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
   const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
-  const int64_t ldt = (a->m + 1) & ~int64_t(1); /* even: the combine reads row pairs */
+  const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
   const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
   const size_t total = ea_bytes + eb_bytes + nmod * (a_pl + b_pl + t_pl);
@@ -484,6 +484,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.ldc = a->ldc;
   cb.alpha = a->alpha_re;
   cb.beta = a->beta_re;
+  cb.err = err;
   static const char *names[HCBK_CRT_MAX_MODULI + 1] = {
       "", "", "", "", "", "", "", "", "tc.crt_m8", "tc.crt_m9", "tc.crt_m10", "tc.crt_m11",
       "tc.crt_m12", "tc.crt_m13", "tc.crt_m14", "tc.crt_m15", "tc.crt_m16", "tc.crt_m17",
@@ -505,7 +506,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int64_t kp = (a->k + 7) & ~int64_t(7);
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
   const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
-  const int64_t ldt = (a->m + 1) & ~int64_t(1);
+  const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
   const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   /* the real view of an MN-contiguous operand has two real rows per row */
   const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
@@ -616,6 +617,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.alpha_im = a->alpha_im;
   cb.beta_re = a->beta_re;
   cb.beta_im = a->beta_im;
+  cb.err = err;
   static const char *names[HCBK_CRT_MAX_MODULI + 1] = {
       "", "", "", "", "", "", "", "", "tc.zcrt3m_m8", "tc.zcrt3m_m9", "tc.zcrt3m_m10",
       "tc.zcrt3m_m11", "tc.zcrt3m_m12", "tc.zcrt3m_m13", "tc.zcrt3m_m14", "tc.zcrt3m_m15",

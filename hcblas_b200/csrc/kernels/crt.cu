@@ -14,8 +14,9 @@
  *      1024-element K chunks and are reduced mod p_i in place in TMEM).
  *   4. This file's combine kernel rebuilds the exact integer product
  *      P' = A' B' (|P'| < (p_1...p_n)/2, guaranteed by the choice of n and
- *      beta) from (T_1..T_n) with Garner's mixed-radix algorithm, evaluates
- *      it in double-double, and writes
+ *      beta) from (T_1..T_n) with the CRT formula P' = sum_i T_i w_i mod M
+ *      (weights split into 40-bit chunks so every chunk sum is exact in
+ *      binary64), evaluates it in double-double, and writes
  *        C = alpha * P' * 2^(e_m + f_n - 2 beta) + beta * C.
  * The only roundings are the scaling in step 1 (relative 2^-(beta+1) of the
  * row / column maximum) and the final conversion to binary64.
@@ -33,6 +34,7 @@
 #include <stdint.h>
 
 #include "hcbk.h"
+#include "tc_common.cuh"
 
 namespace {
 
@@ -52,14 +54,6 @@ __device__ __forceinline__ float sym_f(float r, float p, float hp) {
   return r < -hp ? r + p : r;
 }
 
-/* the same in binary64 for integral |y| < 2^51 */
-__device__ __forceinline__ double sym_mod_d(double y, double q, double inv_q, double hq) {
-  const double t = fma(y, inv_q, RND_D) - RND_D;
-  double r = fma(-t, q, y);
-  r = r > hq ? r - q : r;
-  return r < -hq ? r + q : r;
-}
-
 /* small integer (|x| < 2^22) to f32 without the conversion unit */
 __device__ __forceinline__ float small_int_to_f(int x) {
   return __int_as_float(0x4B400000 + x) - RND_F;
@@ -70,6 +64,12 @@ struct ModConst {
   float c1, c2, c3, c4; /* 2^11, 2^22, 2^33, 2^44 mod p (symmetric) */
 };
 
+/* the same constants duplicated into (x, x) pairs for the packed f32x2
+ * instructions, and -p for the remainder fma */
+struct alignas(8) ModPair {
+  float2 c1, c2, c3, c4, inv_p, neg_p;
+};
+
 struct ResArgs {
   const double *src;
   int64_t ld;
@@ -77,7 +77,7 @@ struct ResArgs {
   const int *exps;
   int beta;
   int nmod;
-  ModConst mc[HCBK_CRT_MAX_MODULI];
+  ModPair mp[HCBK_CRT_MAX_MODULI];
   char *planes;
   int64_t plane_stride; /* bytes */
   int64_t ld_dst;       /* elements */
@@ -90,23 +90,37 @@ struct Limbs {
   float l0, l1, l2, l3, l4;
 };
 
+/* rint(v) of |v| < 2^51 as a double whose low word is rint(v) as an int */
+__device__ __forceinline__ double rnd_magic(double v) { return v + RND_D; }
+
+/* x * 2^s without the library's general ldexp path when 2^s is a normal
+ * number (a power-of-two scaling; an underflow only loses bits below 2^-1022,
+ * which the rint that follows discards anyway) */
+__device__ __forceinline__ double scale2(double x, int s) {
+  return (s >= -1022 && s <= 1023) ? x * __longlong_as_double((long long)(s + 1023) << 52)
+                                   : ldexp(x, s);
+}
+
 __device__ __forceinline__ Limbs limbs_of(double x, int e, int beta) {
   Limbs L{0.f, 0.f, 0.f, 0.f, 0.f};
   if (e == HCBK_OZ_NONFINITE || e == HCBK_OZ_ZERO) return L;
-  const double y = rint(ldexp(x, beta - e));
-  const double h4 = rint(y * 0x1p-44);
-  double r = fma(-h4, 0x1p44, y);
-  const double h3 = rint(r * 0x1p-33);
-  r = fma(-h3, 0x1p33, r);
-  const double h2 = rint(r * 0x1p-22);
-  r = fma(-h2, 0x1p22, r);
-  const double h1 = rint(r * 0x1p-11);
-  r = fma(-h1, 0x1p11, r);
-  L.l0 = static_cast<float>(r);
-  L.l1 = static_cast<float>(h1);
-  L.l2 = static_cast<float>(h2);
-  L.l3 = static_cast<float>(h3);
-  L.l4 = static_cast<float>(h4);
+  const double y = rint(scale2(x, beta - e));
+  /* each limb's rounded quotient comes out of the magic-constant add with
+   * the integer in the low word: no conversion-unit instructions */
+  const double t4 = rnd_magic(y * 0x1p-44);
+  double r = fma(-(t4 - RND_D), 0x1p44, y);
+  const double t3 = rnd_magic(r * 0x1p-33);
+  r = fma(-(t3 - RND_D), 0x1p33, r);
+  const double t2 = rnd_magic(r * 0x1p-22);
+  r = fma(-(t2 - RND_D), 0x1p22, r);
+  const double t1 = rnd_magic(r * 0x1p-11);
+  r = fma(-(t1 - RND_D), 0x1p11, r);
+  const double t0 = rnd_magic(r);
+  L.l0 = small_int_to_f(__double2loint(t0));
+  L.l1 = small_int_to_f(__double2loint(t1));
+  L.l2 = small_int_to_f(__double2loint(t2));
+  L.l3 = small_int_to_f(__double2loint(t3));
+  L.l4 = small_int_to_f(__double2loint(t4));
   return L;
 }
 
@@ -123,8 +137,55 @@ __device__ __forceinline__ float residue(const Limbs &L, const ModConst &m) {
   return mod_f(t, m.p, m.inv_p);
 }
 
+/* packed f32x2 arithmetic (two lanes per instruction, each rounded as the
+ * scalar operation) */
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t pk2(float2 v) { return pk2(v.x, v.y); }
+__device__ __forceinline__ float2 upk2(uint64_t r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+/* limbs of two elements, lane-paired */
+struct Limbs2 {
+  uint64_t l0, l1, l2, l3, l4;
+};
+
+__device__ __forceinline__ Limbs2 pair_limbs(const Limbs &a, const Limbs &b) {
+  return Limbs2{pk2(a.l0, b.l0), pk2(a.l1, b.l1), pk2(a.l2, b.l2), pk2(a.l3, b.l3),
+                pk2(a.l4, b.l4)};
+}
+
+/* residue() for two elements in seven packed instructions; the result pair
+ * converted to binary16 */
+__device__ __forceinline__ __half2 residue2_h(const Limbs2 &L, const ModPair &m) {
+  const uint64_t RND2 = pk2(RND_F, RND_F), NRND2 = pk2(-RND_F, -RND_F);
+  uint64_t t = fma2(L.l4, pk2(m.c4), L.l0);
+  t = fma2(L.l3, pk2(m.c3), t);
+  t = fma2(L.l2, pk2(m.c2), t);
+  t = fma2(L.l1, pk2(m.c1), t);
+  const uint64_t q = add2(fma2(t, pk2(m.inv_p), RND2), NRND2);
+  const float2 r = upk2(fma2(q, pk2(m.neg_p), t));
+  return __floats2half2_rn(r.x, r.y);
+}
+
 /* K-contiguous source: 8 consecutive k per thread, 16-byte plane stores */
-__global__ void crt_res_kcontig(ResArgs a) {
+__global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
   struct alignas(16) H8 { __half2 v[4]; };
   const int64_t kq = (a.kdim + 7) / 8;
   const int64_t total = a.rows * kq;
@@ -133,16 +194,22 @@ __global__ void crt_res_kcontig(ResArgs a) {
     const int64_t r = idx / kq;
     const int64_t k0 = (idx % kq) * 8;
     const int e = a.exps[r];
-    Limbs L[8];
+    Limbs2 L2[4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-      L[j] = limbs_of((k0 + j < a.kdim) ? a.src[r * a.ld + k0 + j] : 0.0, e, a.beta);
-    for (int i = 0; i < a.nmod; ++i) {
-      const ModConst m = a.mc[i];
+    for (int j = 0; j < 4; ++j) {
+      const Limbs x0 = limbs_of((k0 + 2 * j < a.kdim) ? a.src[r * a.ld + k0 + 2 * j] : 0.0, e,
+                                a.beta);
+      const Limbs x1 = limbs_of(
+          (k0 + 2 * j + 1 < a.kdim) ? a.src[r * a.ld + k0 + 2 * j + 1] : 0.0, e, a.beta);
+      L2[j] = pair_limbs(x0, x1);
+    }
+#pragma unroll
+    for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
+      if (i >= a.nmod) break;
+      const ModPair m = a.mp[i];
       H8 out;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        out.v[j] = __floats2half2_rn(residue(L[2 * j], m), residue(L[2 * j + 1], m));
+      for (int j = 0; j < 4; ++j) out.v[j] = residue2_h(L2[j], m);
       __half *d = reinterpret_cast<__half *>(a.planes + i * a.plane_stride) + r * a.ld_dst + k0;
       if (k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
         *reinterpret_cast<H8 *>(d) = out;
@@ -155,8 +222,9 @@ __global__ void crt_res_kcontig(ResArgs a) {
   }
 }
 
-/* MN-contiguous source: 32x32 tile through shared memory, each thread then
- * owns two consecutive k of one row (32-bit plane stores) */
+/* MN-contiguous source: 32x32 tile through shared memory; each thread then
+ * owns four consecutive k of one row (8-byte plane stores; eight threads
+ * write one row's 64 contiguous bytes) */
 __global__ void crt_res_rcontig(ResArgs a) {
   __shared__ double tile[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
@@ -169,51 +237,65 @@ __global__ void crt_res_rcontig(ResArgs a) {
     tile[kl][tx] = (r < a.rows && k < a.kdim) ? a.src[r + k * a.ld] : 0.0;
   }
   __syncthreads();
-  /* 256 threads = 16 k-pairs x 16 rows, twice */
-  const int kp = (ty * 32 + tx) & 15, rl0 = (ty * 32 + tx) >> 4;
+  const int t = ty * 32 + tx;
+  const int rl = t >> 3, kq = (t & 7) * 4;
+  const int64_t r = r0 + rl, k = k0 + kq;
+  if (r >= a.rows || k >= a.kdim) return;
+  const int e = a.exps[r];
+  Limbs2 L2[2];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int rl = rl0 + 16 * h;
-    const int64_t r = r0 + rl, k = k0 + 2 * kp;
-    if (r >= a.rows || k >= a.kdim) continue;
-    const int e = a.exps[r];
-    const Limbs L0 = limbs_of(tile[2 * kp][rl], e, a.beta);
-    const Limbs L1 = limbs_of(tile[2 * kp + 1][rl], e, a.beta);
-    const bool two = k + 1 < a.kdim;
-    for (int i = 0; i < a.nmod; ++i) {
-      const ModConst m = a.mc[i];
-      const __half2 v = __floats2half2_rn(residue(L0, m), residue(L1, m));
-      __half *d = reinterpret_cast<__half *>(a.planes + i * a.plane_stride) + r * a.ld_dst + k;
-      if (two && (reinterpret_cast<uintptr_t>(d) & 3) == 0) {
-        *reinterpret_cast<__half2 *>(d) = v;
-      } else {
-        d[0] = __low2half(v);
-        if (two) d[1] = __high2half(v);
-      }
+  for (int j = 0; j < 2; ++j)
+    L2[j] = pair_limbs(limbs_of(tile[kq + 2 * j][rl], e, a.beta),
+                       limbs_of(tile[kq + 2 * j + 1][rl], e, a.beta));
+  const int64_t left = a.kdim - k;
+  const int nk = left < 4 ? (int)left : 4;
+  char *d0 = a.planes + (r * a.ld_dst + k) * (int64_t)sizeof(__half);
+  const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & 7) == 0 && (a.plane_stride & 7) == 0;
+#pragma unroll
+  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
+    if (i >= a.nmod) break;
+    const ModPair m = a.mp[i];
+    __half2 v[2];
+    v[0] = residue2_h(L2[0], m);
+    v[1] = residue2_h(L2[1], m);
+    __half *d = reinterpret_cast<__half *>(d0 + i * a.plane_stride);
+    if (vec) {
+      *reinterpret_cast<uint2 *>(d) = *reinterpret_cast<const uint2 *>(v);
+    } else {
+      const __half h[4] = {__low2half(v[0]), __high2half(v[0]), __low2half(v[1]),
+                           __high2half(v[1])};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nk) d[j] = h[j];
     }
   }
 }
 
-/* residues merge in groups of GROUP moduli: q_j = p_3j p_3j+1 p_3j+2 < 2^24 */
-constexpr int GROUP = 3;
-constexpr int MAX_Q = (HCBK_CRT_MAX_MODULI + GROUP - 1) / GROUP;
+/* Reconstruction by the weighted residue sum (the CRT formula, as in Ozaki
+ * scheme II):  with M = p_1...p_n, M_i = M / p_i and y_i = M_i^-1 mod p_i,
+ *   P' = sum_i r_i w_i  mod M,   w_i = M_i y_i < M.
+ * Each w_i is held as NC 40-bit chunks w_i = sum_k w_ik 2^(40k); with
+ * |r_i| <= 127 and n <= 20 every chunk sum S_k = sum_i r_i w_ik is below
+ * 20 * 127 * 2^40 < 2^52.4 and exact in binary64.  The quotient
+ * q = rint(S / M) is below 2^12 and is exact from a binary64 estimate,
+ * because |P'| <= M / (2 * 2^0.01) keeps S / M at least 0.003 away from a
+ * half-integer (the count of moduli is chosen that way), far above the
+ * estimate's 2^-39 error.  D_k = S_k - q M_k is exact (< 2^53), carries
+ * normalise the chunks to |D_k| <= 2^39 below the top one, and the chunks are
+ * summed in double-double. */
+constexpr int CRT_CHUNK_BITS = 40;
+constexpr int MAX_NC = 4; /* 20 moduli: M < 2^155 */
 
 struct CombArgs {
   int64_t m, n;
   int nmod;
+  int nc;
   float p[HCBK_CRT_MAX_MODULI];
   float inv_p[HCBK_CRT_MAX_MODULI];
   float hp[HCBK_CRT_MAX_MODULI];
-  /* minv[i] = (p_g0 ... p_(i-1))^-1 mod p_i over the moduli of i's group
-   * before i (0 for a group's first modulus); gsize[j] = moduli in group j */
-  float minv[HCBK_CRT_MAX_MODULI];
-  int nq;
-  int gsize[MAX_Q];
-  double q[MAX_Q];
-  double inv_q[MAX_Q];
-  double hq[MAX_Q];
-  /* qinv[i][j] = q_j^-1 mod q_i (j < i) */
-  double qinv[MAX_Q][MAX_Q];
+  double w[HCBK_CRT_MAX_MODULI][MAX_NC]; /* 40-bit chunks of w_i, low first */
+  double mk[MAX_NC];                     /* 40-bit chunks of M, low first */
+  double inv_m;                          /* RN(1 / M) */
   const int16_t *res;
   int64_t res_plane; /* elements between residue planes */
   int64_t ldr;
@@ -224,83 +306,191 @@ struct CombArgs {
   int64_t ldc;
   double alpha, beta;
   int beta_nonzero;
+  int *err; /* device error flag (pipeline wait timed out) */
 };
 
-/* P' * 2^(ea + eb - shift) for one output element from its n residues
- * (already in f32), Garner over groups of three moduli */
-template <class Res>
-__device__ __forceinline__ double crt_value(const CombArgs &a, const Res &t, int ea, int eb) {
-  if (ea == HCBK_OZ_NONFINITE || eb == HCBK_OZ_NONFINITE)
-    return __longlong_as_double(0x7ff8000000000000ll);
-  if (ea == HCBK_OZ_ZERO || eb == HCBK_OZ_ZERO) return 0.0;
-  /* 1. merge each group in f32: with x the symmetric residue modulo
-   *    Q = p_g0...p_(i-1), x += Q * (((r_i - x) mod p_i) Q^-1 mod p_i) is the
-   *    symmetric residue modulo Q p_i (Q < 2^16, |x| < 2^23: exact) */
-  double v[MAX_Q];
-#pragma unroll
-  for (int j = 0; j < MAX_Q; ++j) {
-    if (j >= a.nq) break;
-    const int i0 = GROUP * j;
-    float x = t[i0];
-    float qq = a.p[i0];
-#pragma unroll
-    for (int g = 1; g < GROUP; ++g) {
-      if (g >= a.gsize[j]) break;
-      const int i = i0 + g;
-      const float d0 = mod_f(t[i] - x, a.p[i], a.inv_p[i]);
-      /* |d0 * minv| < 1.5 * 255 * 254 < 2^17: exact quotient, symmetric result */
-      const float d = mod_f(d0 * a.minv[i], a.p[i], a.inv_p[i]);
-      x = fmaf(qq, d, x);
-      qq *= a.p[i];
-    }
-    /* 2. Garner over the q_j (< 2^24): (x - v_j) qinv < 2^48, exact */
-    double xd = static_cast<double>(x);
-#pragma unroll
-    for (int l = 0; l < MAX_Q; ++l) {
-      if (l >= j) break;
-      xd = sym_mod_d((xd - v[l]) * a.qinv[j][l], a.q[j], a.inv_q[j], a.hq[j]);
-    }
-    v[j] = xd;
-  }
-  /* 3. P' = v_0 + q_0 (v_1 + q_1 (v_2 + ...)), in double-double */
-  double hi = 0.0, lo = 0.0;
-#pragma unroll
-  for (int i = MAX_Q - 1; i >= 0; --i) {
-    if (i >= a.nq) continue;
-    const double p = a.q[i];
-    const double ph = hi * p;
-    const double pl = fma(hi, p, -ph); /* exact product error */
-    const double s = ph + v[i];
-    const double bb = s - ph;
-    const double err = (ph - (s - bb)) + (v[i] - bb);
-    lo = fma(lo, p, pl + err);
-    hi = s + lo;
-    lo = lo - (hi - s);
-  }
-  const double x = hi + lo;
-  const int e = ea + eb - a.shift;
-  return (e >= -1022 && e <= 1023) ? x * __longlong_as_double((long long)(e + 1023) << 52)
-                                   : ldexp(x, e);
+/* small integer to binary64 without the conversion unit: the bit pattern
+ * 0x43300000:(r + 2^31) is 2^52 + 2^31 + r */
+__device__ __forceinline__ double small_int_to_d(int r) {
+  return __hiloint2double(0x43300000, r ^ (int)0x80000000) - 4503601774854144.0;
 }
 
-/* one element per thread, consecutive threads on consecutive rows of one
- * column (coalesced residue loads and C stores); grid.y strides columns */
-__global__ void __launch_bounds__(256) crt_combine_kernel(CombArgs a) {
-  for (int64_t col = blockIdx.y; col < a.n; col += gridDim.y) {
-    const int eb = a.exp_b[col];
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < a.m;
-         row += (int64_t)gridDim.x * blockDim.x) {
-      const int16_t *tp = a.res + row + col * a.ldr;
-      float t[HCBK_CRT_MAX_MODULI];
+template <int NC>
+struct CrtAcc {
+  double S[NC];
+
+  __device__ __forceinline__ CrtAcc() {
 #pragma unroll
-      for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i)
-        t[i] = i < a.nmod ? small_int_to_f(tp[i * a.res_plane]) : 0.f;
-      double *dst = a.c + row + col * a.ldc;
-      double o = a.alpha * crt_value(a, t, a.exp_a[row], eb);
-      if (a.beta_nonzero) o = fma(a.beta, *dst, o);
-      *dst = o;
-    }
+    for (int k = 0; k < NC; ++k) S[k] = 0.0;
   }
+
+  /* add residue r (|r| <= 127) with weight chunks w */
+  __device__ __forceinline__ void add(const double *w, int r) {
+    const double rd = small_int_to_d(r);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) S[k] = fma(rd, w[k], S[k]);
+  }
+
+  /* P' * 2^(ea + eb - shift) */
+  __device__ __forceinline__ double finish(const CombArgs &a, int ea, int eb) const {
+    if (ea == HCBK_OZ_NONFINITE || eb == HCBK_OZ_NONFINITE)
+      return __longlong_as_double(0x7ff8000000000000ll);
+    if (ea == HCBK_OZ_ZERO || eb == HCBK_OZ_ZERO) return 0.0;
+    constexpr double CH = 1099511627776.0;     /* 2^40 */
+    constexpr double INV_CH = 1.0 / 1099511627776.0;
+    double s = S[NC - 1];
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) s = fma(s, CH, S[k]);
+    const double q = fma(s, a.inv_m, RND_D) - RND_D;
+    double D[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) D[k] = fma(-q, a.mk[k], S[k]);
+#pragma unroll
+    for (int k = 0; k < NC - 1; ++k) {
+      const double cy = fma(D[k], INV_CH, RND_D) - RND_D;
+      D[k] = fma(-cy, CH, D[k]);
+      D[k + 1] += cy;
+    }
+    double hi = D[NC - 1], lo = 0.0;
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) {
+      hi *= CH;
+      lo *= CH;
+      const double sh = hi + D[k]; /* two-sum, exact error term */
+      const double bb = sh - hi;
+      lo += (hi - (sh - bb)) + (D[k] - bb);
+      hi = sh;
+    }
+    const double x = hi + lo;
+    const int e = ea + eb - a.shift;
+    return (e >= -1022 && e <= 1023) ? x * __longlong_as_double((long long)(e + 1023) << 52)
+                                     : ldexp(x, e);
+  }
+};
+
+/* ------------------------------------------------ combine pipeline --
+ * The residues of one output tile (ROWS consecutive rows of one column,
+ * every modulus plane) arrive in shared memory by 1-D bulk copies, several
+ * tiles ahead: one thread keeps tens of KB per SM in flight, where per-thread
+ * 2-byte loads left the kernel waiting on memory latency.  Requires the row
+ * pitch and plane stride to be multiples of 8 elements (16 bytes). */
+
+struct PipeArgs {
+  const int16_t *res;
+  int64_t res_plane, ldr;
+  int nplanes;
+  int64_t m, n;
+  int *err;
+};
+
+/* Runs tile(residues in shared memory, first row, column) for every tile of
+ * this block; all threads of the block take part. */
+template <int STAGES, int ROWS, class Tile>
+__device__ __forceinline__ void combine_pipeline(const PipeArgs &pa, int16_t *buf,
+                                                 uint64_t *full, Tile &&tile) {
+  using namespace hcbk::tc;
+  const int tid = threadIdx.x;
+  const int64_t row_tiles = (pa.m + ROWS - 1) / ROWS;
+  const int64_t ntiles = row_tiles * pa.n;
+  const int64_t first = blockIdx.x, stride = gridDim.x;
+  const size_t stage_elems = (size_t)pa.nplanes * ROWS;
+  auto issue = [&](int64_t t, int s) {
+    const int64_t r0 = (t % row_tiles) * ROWS, col = t / row_tiles;
+    const int64_t rows = pa.ldr - r0 < ROWS ? pa.ldr - r0 : ROWS;
+    const uint32_t bytes = (uint32_t)rows * 2u; /* ldr, r0 multiples of 8 */
+    mbar_expect_tx(&full[s], bytes * (uint32_t)pa.nplanes);
+    const int16_t *src = pa.res + col * pa.ldr + r0;
+    int16_t *dst = buf + s * stage_elems;
+    for (int p = 0; p < pa.nplanes; ++p)
+      bulk_load_1d(dst + p * ROWS, src + p * pa.res_plane, bytes, &full[s]);
+  };
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < STAGES; ++s)
+      if (first + s * stride < ntiles) issue(first + s * stride, s);
+  int j = 0;
+  for (int64_t t = first; t < ntiles; t += stride, ++j) {
+    const int s = j % STAGES;
+    const bool ok = mbar_wait(&full[s], (uint32_t)(j / STAGES) & 1u, pa.err, ERR_TIMEOUT_COMBINE);
+    if (ok) tile(buf + s * stage_elems, (t % row_tiles) * ROWS, t / row_tiles);
+    if (__syncthreads_or(!ok)) {
+      /* give the copies still in flight a bounded time to land before the
+       * block's shared memory is released */
+      if (tid == 0)
+        for (int k = 0; k < STAGES; ++k) {
+          if (t + k * stride >= ntiles) break;
+          const int sk = (j + k) % STAGES;
+          const uint32_t ph = (uint32_t)((j + k) / STAGES) & 1u;
+          for (int it = 0; it < (1 << 22) && !mbar_try_wait(&full[sk], ph); ++it) {
+          }
+        }
+      return;
+    }
+    if (tid == 0 && t + STAGES * stride < ntiles) issue(t + STAGES * stride, s);
+  }
+}
+
+/* the weight chunks in shared memory (the modulus loop indexes them at run
+ * time; register-resident weights would cost 2 NC registers a modulus) */
+template <int NC>
+__device__ __forceinline__ void load_weights(const CombArgs &a, double (*sw)[NC]) {
+  for (int j = threadIdx.x; j < HCBK_CRT_MAX_MODULI * NC; j += blockDim.x)
+    sw[j / NC][j % NC] = a.w[j / NC][j % NC];
+  __syncthreads();
+}
+
+/* real combine: 256 threads x 2 consecutive rows (one 4-byte residue load
+ * per modulus, weights read once for both rows); 3 stages of nmod KB */
+constexpr int CMB_THREADS = 256, CMB_RPT = 2, CMB_ROWS = CMB_THREADS * CMB_RPT;
+constexpr int CMB_STAGES = 3;
+/* complex combine: 256 threads x 1 row (two accumulators a row already);
+ * 3 stages of 1.5 nmod KB */
+constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 1, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
+constexpr int ZCMB_STAGES = 3;
+
+/* signed 16-bit halves of a 32-bit word */
+__device__ __forceinline__ int lo16(uint32_t w) { return (int)(w << 16) >> 16; }
+__device__ __forceinline__ int hi16(uint32_t w) { return (int)w >> 16; }
+
+template <int NC>
+__global__ void __launch_bounds__(CMB_THREADS) crt_combine_kernel(CombArgs a) {
+  extern __shared__ __align__(128) unsigned char cmb_smem[];
+  __shared__ double sw[HCBK_CRT_MAX_MODULI][NC];
+  __shared__ __align__(8) uint64_t full[CMB_STAGES];
+  if (blockDim.x != CMB_THREADS) { /* the tile covers CMB_ROWS rows only at this shape */
+    if (threadIdx.x == 0) atomicCAS(a.err, 0, (int)hcbk::tc::ERR_LAUNCH_SHAPE);
+    return;
+  }
+  load_weights<NC>(a, sw);
+  const int nmod = a.nmod;
+  const int tid = threadIdx.x;
+  const PipeArgs pa{a.res, a.res_plane, a.ldr, nmod, a.m, a.n, a.err};
+  combine_pipeline<CMB_STAGES, CMB_ROWS>(
+      pa, reinterpret_cast<int16_t *>(cmb_smem), full,
+      [&](const int16_t *R, int64_t r0, int64_t col) {
+        const int64_t row = r0 + CMB_RPT * tid;
+        if (row >= a.m) return;
+        CrtAcc<NC> acc[CMB_RPT];
+#pragma unroll 3
+        for (int i = 0; i < nmod; ++i) {
+          const uint32_t q = *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
+          acc[0].add(sw[i], lo16(q));
+          acc[1].add(sw[i], hi16(q));
+        }
+        const int eb = a.exp_b[col];
+        double *dst = a.c + row + col * a.ldc;
+#pragma unroll
+        for (int u = 0; u < CMB_RPT; ++u) {
+          if (row + u >= a.m) break;
+          double o = a.alpha * acc[u].finish(a, a.exp_a[row + u], eb);
+          if (a.beta_nonzero) o = fma(a.beta, dst[u], o);
+          dst[u] = o;
+        }
+      });
 }
 
 /* modular inverse by the extended Euclidean algorithm */
@@ -341,42 +531,113 @@ static void fill_mod_consts(ModConst (&mc)[HCBK_CRT_MAX_MODULI]) {
   }
 }
 
-/* moduli, group constants and Garner inverses of the combine */
+/* unsigned multi-word integer, 32-bit words, low first */
+struct BigU {
+  uint32_t w[8];
+  int len;
+};
+
+static void big_set(BigU &b, uint32_t v) {
+  for (int i = 0; i < 8; ++i) b.w[i] = 0;
+  b.w[0] = v;
+  b.len = 1;
+}
+
+static void big_mul_small(BigU &b, uint32_t s) {
+  uint64_t carry = 0;
+  for (int i = 0; i < b.len; ++i) {
+    const uint64_t t = (uint64_t)b.w[i] * s + carry;
+    b.w[i] = (uint32_t)t;
+    carry = t >> 32;
+  }
+  if (carry) b.w[b.len++] = (uint32_t)carry;
+}
+
+/* b /= d, returns b mod d */
+static uint32_t big_div_small(BigU &b, uint32_t d) {
+  uint64_t rem = 0;
+  for (int i = b.len - 1; i >= 0; --i) {
+    const uint64_t cur = (rem << 32) | b.w[i];
+    b.w[i] = (uint32_t)(cur / d);
+    rem = cur % d;
+  }
+  while (b.len > 1 && b.w[b.len - 1] == 0) --b.len;
+  return (uint32_t)rem;
+}
+
+static int big_bits(const BigU &b) {
+  int top = b.len - 1;
+  while (top > 0 && b.w[top] == 0) --top;
+  int bits = 32 * top;
+  for (uint32_t v = b.w[top]; v; v >>= 1) ++bits;
+  return bits;
+}
+
+/* bits [lo, lo + n) as a double (exact for n <= 53) */
+static double big_bits_at(const BigU &b, int lo, int n) {
+  double v = 0.0;
+  for (int j = n - 1; j >= 0; --j) {
+    const int bit = lo + j;
+    const int word = bit / 32;
+    const uint32_t set = word < b.len ? (b.w[word] >> (bit % 32)) & 1u : 0u;
+    v = v * 2.0 + (double)set;
+  }
+  return v;
+}
+
+static double big_to_double(const BigU &b) {
+  double v = 0.0;
+  for (int i = b.len - 1; i >= 0; --i) v = v * 4294967296.0 + (double)b.w[i];
+  return v;
+}
+
+static void fill_mod_pairs(ModPair (&mp)[HCBK_CRT_MAX_MODULI]) {
+  ModConst mc[HCBK_CRT_MAX_MODULI];
+  fill_mod_consts(mc);
+  for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
+    mp[i].c1 = make_float2(mc[i].c1, mc[i].c1);
+    mp[i].c2 = make_float2(mc[i].c2, mc[i].c2);
+    mp[i].c3 = make_float2(mc[i].c3, mc[i].c3);
+    mp[i].c4 = make_float2(mc[i].c4, mc[i].c4);
+    mp[i].inv_p = make_float2(mc[i].inv_p, mc[i].inv_p);
+    mp[i].neg_p = make_float2(-mc[i].p, -mc[i].p);
+  }
+}
+
+/* moduli and the weights, chunks and reciprocal of the reconstruction */
 static void fill_comb_moduli(CombArgs &a, int nmod) {
-  const int *M = hcbk_crt_moduli(nullptr);
+  const int *P = hcbk_crt_moduli(nullptr);
   a.nmod = nmod;
   for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) {
-    a.p[i] = (float)M[i];
-    a.inv_p[i] = 1.0f / (float)M[i];
-    a.hp[i] = (float)((M[i] - 1) / 2);
-    a.minv[i] = 0.f;
+    a.p[i] = (float)P[i];
+    a.inv_p[i] = 1.0f / (float)P[i];
+    a.hp[i] = (float)((P[i] - 1) / 2);
+    for (int k = 0; k < MAX_NC; ++k) a.w[i][k] = 0.0;
   }
-  a.nq = (nmod + GROUP - 1) / GROUP;
-  long long q[MAX_Q];
-  for (int j = 0; j < MAX_Q; ++j) a.gsize[j] = 0;
-  for (int j = 0; j < a.nq; ++j) {
-    const int i0 = GROUP * j;
-    const int gs = nmod - i0 < GROUP ? nmod - i0 : GROUP;
-    a.gsize[j] = gs;
-    long long qq = M[i0];
-    for (int g = 1; g < gs; ++g) {
-      a.minv[i0 + g] = (float)inv_mod_ll(qq, M[i0 + g]);
-      qq *= M[i0 + g];
-    }
-    q[j] = qq;
-    a.q[j] = (double)q[j];
-    a.inv_q[j] = 1.0 / (double)q[j];
-    a.hq[j] = (double)((q[j] - 1) / 2);
+  BigU M;
+  big_set(M, 1);
+  for (int i = 0; i < nmod; ++i) big_mul_small(M, (uint32_t)P[i]);
+  const int bits = big_bits(M);
+  a.nc = (bits + CRT_CHUNK_BITS - 1) / CRT_CHUNK_BITS;
+  for (int k = 0; k < MAX_NC; ++k)
+    a.mk[k] = k < a.nc ? big_bits_at(M, CRT_CHUNK_BITS * k, CRT_CHUNK_BITS) : 0.0;
+  a.inv_m = 1.0 / big_to_double(M);
+  for (int i = 0; i < nmod; ++i) {
+    BigU Mi = M;
+    big_div_small(Mi, (uint32_t)P[i]); /* exact: M_i = M / p_i */
+    BigU t = Mi;
+    const uint32_t mi_mod = big_div_small(t, (uint32_t)P[i]);
+    const uint32_t y = (uint32_t)inv_mod_ll(mi_mod, P[i]);
+    big_mul_small(Mi, y); /* w_i = M_i y_i < M */
+    for (int k = 0; k < a.nc; ++k)
+      a.w[i][k] = big_bits_at(Mi, CRT_CHUNK_BITS * k, CRT_CHUNK_BITS);
   }
-  for (int i = 0; i < MAX_Q; ++i)
-    for (int j = 0; j < MAX_Q; ++j)
-      a.qinv[i][j] = (i < a.nq && j < i) ? (double)inv_mod_ll(q[j], q[i]) : 0.0;
 }
 
 /* ------------------------------------------------ complex (ZGEMM) path --
  * 3M (Karatsuba) in modular arithmetic, where it is exact:
  *   T1 = Ar Br, T2 = Ai Bi, T3 = (Ar + Ai)(Br + Bi)   (mod p, one GEMM each)
- *   Re = T1 - T2,  Im = T3 - T1 - T2                  (mod p, then Garner)
+ *   Re = T1 - T2,  Im = T3 - T1 - T2                  (mod p, then the CRT sum)
  * Real and imaginary parts of a row share one exponent (the larger), so
  * Ar' + Ai' is the residue sum of one scaled integer pair. */
 
@@ -414,6 +675,11 @@ __device__ __forceinline__ ZRes3 zresidue(const Limbs &lr, const Limbs &li, cons
 
 /* K-contiguous complex source: 8 consecutive k per thread, 16-byte stores */
 __global__ void zcrt_res_kcontig(ZResArgs a) {
+  /* moduli constants in shared memory: 80 limb registers leave no room
+   * for them, and a run-time index into the parameter bank serialises */
+  __shared__ ModConst smc[HCBK_CRT_MAX_MODULI];
+  if (threadIdx.x < HCBK_CRT_MAX_MODULI) smc[threadIdx.x] = a.mc[threadIdx.x];
+  __syncthreads();
   struct alignas(16) H8 { __half2 v[4]; };
   const int64_t kq = (a.kdim + 7) / 8;
   const int64_t total = a.rows * kq;
@@ -430,7 +696,7 @@ __global__ void zcrt_res_kcontig(ZResArgs a) {
       li[j] = limbs_of(z.y, e, a.beta);
     }
     for (int i = 0; i < a.nmod; ++i) {
-      const ModConst m = a.mc[i];
+      const ModConst m = smc[i];
       H8 o[3];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -480,7 +746,11 @@ __global__ void zcrt_res_rcontig(ZResArgs a) {
     const Limbs r0l = limbs_of(z0.x, e, a.beta), i0l = limbs_of(z0.y, e, a.beta);
     const Limbs r1l = limbs_of(z1.x, e, a.beta), i1l = limbs_of(z1.y, e, a.beta);
     const bool two = k + 1 < a.kdim;
-    for (int i = 0; i < a.nmod; ++i) {
+    const bool vec = two && (a.plane_stride & 3) == 0 &&
+                     (reinterpret_cast<uintptr_t>(a.planes + (r * a.ld_dst + k) * 2) & 3) == 0;
+#pragma unroll
+    for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
+      if (i >= a.nmod) break;
       const ModConst m = a.mc[i];
       const ZRes3 x0 = zresidue(r0l, i0l, m, a.im_sign);
       const ZRes3 x1 = zresidue(r1l, i1l, m, a.im_sign);
@@ -490,7 +760,7 @@ __global__ void zcrt_res_rcontig(ZResArgs a) {
       for (int set = 0; set < 3; ++set) {
         __half *d = reinterpret_cast<__half *>(a.planes + (set * a.nmod + i) * a.plane_stride) +
                     r * a.ld_dst + k;
-        if (two && (reinterpret_cast<uintptr_t>(d) & 3) == 0) {
+        if (vec) {
           *reinterpret_cast<__half2 *>(d) = v[set];
         } else {
           d[0] = __low2half(v[set]);
@@ -502,52 +772,87 @@ __global__ void zcrt_res_rcontig(ZResArgs a) {
 }
 
 struct ZCombArgs {
-  CombArgs g;  /* moduli, Garner constants, residues (3 sets of nmod planes) */
+  CombArgs g;  /* moduli, reconstruction constants, residues (3 sets of nmod planes) */
   int exp_a_pair, exp_b_pair;
   double2 *c;
   int64_t ldc;
   double2 alpha, beta;
 };
 
-/* residues of one element kept in shared memory, [modulus][thread]: the
- * complex combine holds two sets, which in registers would cut occupancy */
-struct SmemRes {
-  const float *base;
-  __device__ __forceinline__ float operator[](int i) const { return base[i * 256]; }
-};
+/* f32 holding a small integer (|x| < 2^22) to int without the conversion unit */
+__device__ __forceinline__ int small_f_to_int(float x) {
+  return __float_as_int(x + RND_F) - 0x4B400000;
+}
 
-__global__ void __launch_bounds__(256) zcrt_combine_kernel(ZCombArgs a) {
-  __shared__ float sres[2][HCBK_CRT_MAX_MODULI][256];
+/* residues stream through the two accumulators, one modulus at a time: the
+ * weighted-sum reconstruction keeps no per-modulus state */
+template <int NC>
+__global__ void __launch_bounds__(ZCMB_THREADS) zcrt_combine_kernel(ZCombArgs a) {
+  extern __shared__ __align__(128) unsigned char cmb_smem[];
+  __shared__ double sw[HCBK_CRT_MAX_MODULI][NC];
+  __shared__ __align__(8) uint64_t full[ZCMB_STAGES];
+  if (blockDim.x != ZCMB_THREADS) { /* the tile covers ZCMB_ROWS rows only at this shape */
+    if (threadIdx.x == 0) atomicCAS(a.g.err, 0, (int)hcbk::tc::ERR_LAUNCH_SHAPE);
+    return;
+  }
+  load_weights<NC>(a.g, sw);
   const int nmod = a.g.nmod;
   const int tid = threadIdx.x;
-  for (int64_t col = blockIdx.y; col < a.g.n; col += gridDim.y) {
-    const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + tid; row < a.g.m;
-         row += (int64_t)gridDim.x * blockDim.x) {
-      const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row);
-      const int16_t *tp = a.g.res + row + col * a.g.ldr;
-#pragma unroll 4
-      for (int i = 0; i < nmod; ++i) {
-        const float t1 = small_int_to_f(tp[(int64_t)i * a.g.res_plane]);
-        const float t2 = small_int_to_f(tp[(int64_t)(nmod + i) * a.g.res_plane]);
-        const float t3 = small_int_to_f(tp[(int64_t)(2 * nmod + i) * a.g.res_plane]);
-        sres[0][i][tid] = sym_f(mod_f(t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
-        sres[1][i][tid] = sym_f(mod_f(t3 - t1 - t2, a.g.p[i], a.g.inv_p[i]), a.g.p[i], a.g.hp[i]);
-      }
-      const double re = crt_value(a.g, SmemRes{&sres[0][0][tid]}, ea, eb);
-      const double im = crt_value(a.g, SmemRes{&sres[1][0][tid]}, ea, eb);
-      double2 *dst = a.c + row + col * a.ldc;
-      double2 o;
-      o.x = a.alpha.x * re - a.alpha.y * im;
-      o.y = a.alpha.x * im + a.alpha.y * re;
-      if (a.g.beta_nonzero) {
-        const double2 cv = *dst;
-        o.x = fma(a.beta.x, cv.x, fma(-a.beta.y, cv.y, o.x));
-        o.y = fma(a.beta.x, cv.y, fma(a.beta.y, cv.x, o.y));
-      }
-      *dst = o;
-    }
-  }
+  const PipeArgs pa{a.g.res, a.g.res_plane, a.g.ldr, 3 * nmod, a.g.m, a.g.n, a.g.err};
+  combine_pipeline<ZCMB_STAGES, ZCMB_ROWS>(
+      pa, reinterpret_cast<int16_t *>(cmb_smem), full,
+      [&](const int16_t *R, int64_t r0, int64_t col) {
+        const int64_t row = r0 + ZCMB_RPT * tid;
+        if (row >= a.g.m) return;
+        CrtAcc<NC> acc_re[ZCMB_RPT], acc_im[ZCMB_RPT];
+#pragma unroll 2
+        for (int i = 0; i < nmod; ++i) {
+          const float t1 = small_int_to_f(R[i * ZCMB_ROWS + tid]);
+          const float t2 = small_int_to_f(R[(nmod + i) * ZCMB_ROWS + tid]);
+          const float t3 = small_int_to_f(R[(2 * nmod + i) * ZCMB_ROWS + tid]);
+          const float p = a.g.p[i], ip = a.g.inv_p[i], hp = a.g.hp[i];
+          acc_re[0].add(sw[i], small_f_to_int(sym_f(mod_f(t1 - t2, p, ip), p, hp)));
+          acc_im[0].add(sw[i], small_f_to_int(sym_f(mod_f(t3 - t1 - t2, p, ip), p, hp)));
+        }
+        const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
+#pragma unroll
+        for (int u = 0; u < ZCMB_RPT; ++u) {
+          if (row + u >= a.g.m) break;
+          const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row + u);
+          const double re = acc_re[u].finish(a.g, ea, eb);
+          const double im = acc_im[u].finish(a.g, ea, eb);
+          double2 *dst = a.c + row + u + col * a.ldc;
+          double2 o;
+          o.x = a.alpha.x * re - a.alpha.y * im;
+          o.y = a.alpha.x * im + a.alpha.y * re;
+          if (a.g.beta_nonzero) {
+            const double2 cv = *dst;
+            o.x = fma(a.beta.x, cv.x, fma(-a.beta.y, cv.y, o.x));
+            o.y = fma(a.beta.x, cv.y, fma(a.beta.y, cv.x, o.y));
+          }
+          *dst = o;
+        }
+      });
+}
+
+/* persistent grid for a combine kernel: as many blocks as fit, at most one
+ * per tile; opts in to the dynamic shared memory it needs */
+template <class K>
+static int combine_grid(K kernel, int threads, size_t smem, int64_t ntiles, int64_t *grid) {
+  /* static shared memory counts against the same 48 KB default, so opt in
+   * well below it */
+  if (smem > 32 * 1024 &&
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+    return HCBK_ERR_LAUNCH;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return HCBK_ERR_LAUNCH;
+  const int64_t cap = (int64_t)hcbk_sm_count() * per_sm;
+  *grid = ntiles < cap ? ntiles : cap;
+  return HCBK_OK;
 }
 
 }  // namespace
@@ -575,7 +880,7 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
   a.exps = in->exps;
   a.beta = in->beta_bits;
   a.nmod = in->nmod;
-  fill_mod_consts(a.mc);
+  fill_mod_pairs(a.mp);
   a.planes = static_cast<char *>(in->planes);
   a.plane_stride = in->plane_stride;
   a.ld_dst = in->ld_dst;
@@ -596,7 +901,8 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
 extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (in->m <= 0 || in->n <= 0 || in->nmod < 2 || in->nmod > HCBK_CRT_MAX_MODULI ||
-      (in->ldr & 1) || (in->res_plane & 1) || (reinterpret_cast<uintptr_t>(in->res) & 3))
+      in->ldr < in->m || (in->ldr & 7) || (in->res_plane & 7) ||
+      (reinterpret_cast<uintptr_t>(in->res) & 15) || !in->err)
     return HCBK_ERR_ARGS;
   CombArgs a;
   a.m = in->m;
@@ -613,10 +919,24 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.alpha = in->alpha;
   a.beta = in->beta;
   a.beta_nonzero = in->beta != 0.0;
-  int64_t gx = (a.m + 255) / 256;
-  if (gx > 65535) gx = 65535;
-  const int64_t gy = a.n < 65535 ? a.n : 65535;
-  crt_combine_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(a);
+  a.err = in->err;
+  const int64_t ntiles = (a.m + CMB_ROWS - 1) / CMB_ROWS * a.n;
+  const size_t smem = (size_t)CMB_STAGES * a.nmod * CMB_ROWS * sizeof(int16_t);
+  int64_t grid = 0;
+  int rc;
+  switch (a.nc) {
+    case 1: rc = combine_grid(crt_combine_kernel<1>, CMB_THREADS, smem, ntiles, &grid); break;
+    case 2: rc = combine_grid(crt_combine_kernel<2>, CMB_THREADS, smem, ntiles, &grid); break;
+    case 3: rc = combine_grid(crt_combine_kernel<3>, CMB_THREADS, smem, ntiles, &grid); break;
+    default: rc = combine_grid(crt_combine_kernel<4>, CMB_THREADS, smem, ntiles, &grid); break;
+  }
+  if (rc != HCBK_OK) return rc;
+  switch (a.nc) {
+    case 1: crt_combine_kernel<1><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
+    case 2: crt_combine_kernel<2><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
+    case 3: crt_combine_kernel<3><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
+    default: crt_combine_kernel<4><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
+  }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
@@ -655,7 +975,9 @@ extern "C" int hcbk_zcrt_residues(const hcbk_zcrt_prep *in, void *stream) {
 
 extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (in->m <= 0 || in->n <= 0 || in->nmod < 2 || in->nmod > HCBK_CRT_MAX_MODULI)
+  if (in->m <= 0 || in->n <= 0 || in->nmod < 2 || in->nmod > HCBK_CRT_MAX_MODULI ||
+      in->ldr < in->m || (in->ldr & 7) || (in->res_plane & 7) ||
+      (reinterpret_cast<uintptr_t>(in->res) & 15) || !in->err)
     return HCBK_ERR_ARGS;
   ZCombArgs a;
   a.g.m = in->m;
@@ -672,15 +994,29 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   a.g.alpha = 0.0;
   a.g.beta = 0.0;
   a.g.beta_nonzero = in->beta_re != 0.0 || in->beta_im != 0.0;
+  a.g.err = in->err;
   a.exp_a_pair = in->exp_a_pair;
   a.exp_b_pair = in->exp_b_pair;
   a.c = static_cast<double2 *>(in->c);
   a.ldc = in->ldc;
   a.alpha = make_double2(in->alpha_re, in->alpha_im);
   a.beta = make_double2(in->beta_re, in->beta_im);
-  int64_t gx = (a.g.m + 255) / 256;
-  if (gx > 65535) gx = 65535;
-  const int64_t gy = a.g.n < 65535 ? a.g.n : 65535;
-  zcrt_combine_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(a);
+  const int64_t ntiles = (a.g.m + ZCMB_ROWS - 1) / ZCMB_ROWS * a.g.n;
+  const size_t smem = (size_t)ZCMB_STAGES * 3 * a.g.nmod * ZCMB_ROWS * sizeof(int16_t);
+  int64_t grid = 0;
+  int rc;
+  switch (a.g.nc) {
+    case 1: rc = combine_grid(zcrt_combine_kernel<1>, ZCMB_THREADS, smem, ntiles, &grid); break;
+    case 2: rc = combine_grid(zcrt_combine_kernel<2>, ZCMB_THREADS, smem, ntiles, &grid); break;
+    case 3: rc = combine_grid(zcrt_combine_kernel<3>, ZCMB_THREADS, smem, ntiles, &grid); break;
+    default: rc = combine_grid(zcrt_combine_kernel<4>, ZCMB_THREADS, smem, ntiles, &grid); break;
+  }
+  if (rc != HCBK_OK) return rc;
+  switch (a.g.nc) {
+    case 1: zcrt_combine_kernel<1><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
+    case 2: zcrt_combine_kernel<2><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
+    case 3: zcrt_combine_kernel<3><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
+    default: zcrt_combine_kernel<4><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
+  }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -250,20 +250,23 @@ typedef struct hcbk_crt_gemm {
 } hcbk_crt_gemm;
 int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
 
-/* Garner reconstruction of P' from the residue planes and the epilogue
- * C = alpha * P' * 2^(exp_a[m] + exp_b[n] - shift) + beta * C. */
+/* CRT reconstruction of P' from the residue planes and the epilogue
+ * C = alpha * P' * 2^(exp_a[m] + exp_b[n] - shift) + beta * C.  Residues are
+ * read by 1-D bulk copies: res 16-byte aligned, ldr >= m and res_plane
+ * multiples of 8 elements. */
 typedef struct hcbk_crt_combine_args {
   int64_t m, n;
   int nmod;
   const int16_t *res;
-  int64_t res_plane; /* elements between planes */
-  int64_t ldr;
+  int64_t res_plane; /* elements between planes, multiple of 8 */
+  int64_t ldr;       /* >= m, multiple of 8 */
   const int *exp_a;
   const int *exp_b;
   int shift; /* 2 * beta_bits */
   double *c;
   int64_t ldc;
   double alpha, beta;
+  int *err; /* device error flag: set when the pipeline's wait times out */
 } hcbk_crt_combine_args;
 int hcbk_crt_combine(const hcbk_crt_combine_args *a, void *stream);
 
@@ -298,8 +301,8 @@ typedef struct hcbk_zcrt_combine_args {
   int64_t m, n;
   int nmod;
   const int16_t *res;
-  int64_t res_plane; /* elements between planes, even */
-  int64_t ldr;       /* even */
+  int64_t res_plane; /* elements between planes, multiple of 8 */
+  int64_t ldr;       /* >= m, multiple of 8 */
   const int *exp_a;
   const int *exp_b;
   int exp_a_pair, exp_b_pair;
@@ -307,6 +310,7 @@ typedef struct hcbk_zcrt_combine_args {
   void *c;
   int64_t ldc;
   double alpha_re, alpha_im, beta_re, beta_im;
+  int *err; /* device error flag: set when the pipeline's wait times out */
 } hcbk_zcrt_combine_args;
 int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *a, void *stream);
 

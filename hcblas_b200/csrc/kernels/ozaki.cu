@@ -42,38 +42,110 @@ __device__ __forceinline__ int exp_of(double x) {
   return e;
 }
 
-__device__ __forceinline__ int warp_max(int v) {
+/* |x| as an ordered bit pattern: the maximum over a row of these is the
+ * pattern of max |x| (Inf and NaN above every finite value), and exp_of is
+ * monotone in |x|, so one exp_of per row replaces one per element */
+__device__ __forceinline__ unsigned long long abs_bits(double x) {
+  return static_cast<unsigned long long>(__double_as_longlong(x)) & 0x7FFFFFFFFFFFFFFFull;
+}
+
+__device__ __forceinline__ int exp_of_bits(unsigned long long b) {
+  return exp_of(__longlong_as_double(static_cast<long long>(b)));
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
   return v;
 }
 
-/* K-contiguous source: one warp per row */
+/* K-contiguous source: one warp per row; VEC = 2 reads 16-byte pairs
+ * (row start 16-byte aligned, even kdim) */
+template <int VEC>
 __global__ void oz_exp_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
                                int *exps) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = warp; r < rows; r += nwarps) {
-    int e = HCBK_OZ_ZERO;
+    unsigned long long m = 0;
     const double *row = src + r * ld;
-    for (int64_t k = lane; k < kdim; k += 32) e = max(e, exp_of(row[k]));
-    e = warp_max(e);
-    if (lane == 0) exps[r] = e;
+    if (VEC == 2) {
+      const double2 *row2 = reinterpret_cast<const double2 *>(row);
+      const int64_t k2 = kdim / 2;
+      int64_t k = lane;
+      for (; k + 96 < k2; k += 128) { /* four 16-byte loads in flight */
+        double2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = row2[k + 32 * u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          m = max(m, abs_bits(v[u].x));
+          m = max(m, abs_bits(v[u].y));
+        }
+      }
+      for (; k < k2; k += 32) {
+        const double2 v = row2[k];
+        m = max(m, abs_bits(v.x));
+        m = max(m, abs_bits(v.y));
+      }
+    } else {
+      for (int64_t k = lane; k < kdim; k += 32) m = max(m, abs_bits(row[k]));
+    }
+    m = warp_max_u64(m);
+    if (lane == 0) exps[r] = exp_of_bits(m);
   }
 }
 
 /* MN-contiguous source: threads along rows, K split over blockIdx.y; the
- * partial maxima meet in exps[] (pre-set to HCBK_OZ_ZERO) via atomicMax */
+ * partial maxima meet in exps[] (pre-set to HCBK_OZ_ZERO) via atomicMax.
+ * VEC = 2: each thread owns two adjacent rows and reads 16-byte pairs (even
+ * rows and ld, 16-byte aligned source); eight loads in flight. */
+template <int VEC>
 __global__ void oz_exp_rcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
                                int64_t kchunk, int *exps) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t r = VEC * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
   if (r >= rows) return;
   const int64_t k0 = (int64_t)blockIdx.y * kchunk;
   const int64_t k1 = (k0 + kchunk < kdim) ? k0 + kchunk : kdim;
-  int e = HCBK_OZ_ZERO;
-  for (int64_t k = k0; k < k1; ++k) e = max(e, exp_of(src[r + k * ld]));
-  atomicMax(&exps[r], e);
+  if (VEC == 2) {
+    unsigned long long m0 = 0, m1 = 0;
+    const double2 *p = reinterpret_cast<const double2 *>(src + r);
+    const int64_t step = ld / 2;
+    int64_t k = k0;
+    for (; k + 8 <= k1; k += 8) {
+      double2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = p[(k + u) * step];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        m0 = max(m0, abs_bits(v[u].x));
+        m1 = max(m1, abs_bits(v[u].y));
+      }
+    }
+    for (; k < k1; ++k) {
+      const double2 v = p[k * step];
+      m0 = max(m0, abs_bits(v.x));
+      m1 = max(m1, abs_bits(v.y));
+    }
+    atomicMax(&exps[r], exp_of_bits(m0));
+    atomicMax(&exps[r + 1], exp_of_bits(m1));
+  } else {
+    unsigned long long m = 0;
+    int64_t k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = src[r + (k + u) * ld];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) m = max(m, abs_bits(v[u]));
+    }
+    for (; k < k1; ++k) m = max(m, abs_bits(src[r + k * ld]));
+    atomicMax(&exps[r], exp_of_bits(m));
+  }
 }
 
 __global__ void oz_fill(int *exps, int64_t n, int v) {
@@ -205,22 +277,31 @@ int launch_slice_any(const hcbk_ozaki_prep *a, cudaStream_t st) {
 extern "C" int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a->rows <= 0 || a->kdim <= 0) return HCBK_ERR_ARGS;
+  const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0;
   if (a->k_contig) {
     int64_t blocks = (a->rows * 32 + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    oz_exp_kcontig<<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, a->exps);
+    if (al16 && (a->kdim & 1) == 0)
+      oz_exp_kcontig<2><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, a->exps);
+    else
+      oz_exp_kcontig<1><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, a->exps);
   } else {
-    const int64_t gx = (a->rows + 255) / 256;
-    /* enough K-splits to give every SM a few blocks */
-    int64_t ky = ((int64_t)hcbk_sm_count() * 4 + gx - 1) / gx;
+    const int vec = (al16 && (a->rows & 1) == 0) ? 2 : 1;
+    const int64_t gx = (a->rows / vec + 255) / 256;
+    /* enough K-splits to give every SM several blocks */
+    int64_t ky = ((int64_t)hcbk_sm_count() * 8 + gx - 1) / gx;
     if (ky > 1024) ky = 1024;
     int64_t kchunk = (a->kdim + ky - 1) / ky;
-    if (kchunk < 64) kchunk = 64;
+    if (kchunk < 32) kchunk = 32;
     ky = (a->kdim + kchunk - 1) / kchunk;
+    if (ky > 65535) return HCBK_ERR_ARGS;
     oz_fill<<<(unsigned)((a->rows + 255) / 256), 256, 0, st>>>(a->exps, a->rows, HCBK_OZ_ZERO);
-    oz_exp_rcontig<<<dim3((unsigned)gx, (unsigned)ky), 256, 0, st>>>(a->src, a->ld, a->rows,
-                                                                     a->kdim, kchunk, a->exps);
+    const dim3 grid((unsigned)gx, (unsigned)ky);
+    if (vec == 2)
+      oz_exp_rcontig<2><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kchunk, a->exps);
+    else
+      oz_exp_rcontig<1><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kchunk, a->exps);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

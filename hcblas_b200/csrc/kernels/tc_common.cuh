@@ -34,6 +34,8 @@ enum : int {
   ERR_TIMEOUT_MMA_FULL = 2,
   ERR_TIMEOUT_MMA_TMEM = 3,
   ERR_TIMEOUT_EPILOGUE = 4,
+  ERR_TIMEOUT_COMBINE = 5,
+  ERR_LAUNCH_SHAPE = 6, /* a kernel was launched with a block shape it does not support */
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -148,6 +150,18 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
 
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+/* 1-D bulk copy from global memory into this CTA's shared memory: both
+ * addresses 16-byte aligned, `bytes` a multiple of 16; completion is
+ * signalled on `bar` (complete_tx).  No multicast. */
+__device__ __forceinline__ void bulk_load_1d(void *dst, const void *src, uint32_t bytes,
+                                             uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(static_cast<uint64_t>(__cvta_generic_to_global(src))), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
 
 /* 2-D tiled bulk tensor load into this CTA's shared memory; completion is

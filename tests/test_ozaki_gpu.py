@@ -311,6 +311,34 @@ def test_zgemm_crt_vs_dd_oracle(handle, want):
         assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
 
 
+@pytest.mark.parametrize("kind,order,ta,tb,M,N,K", [("d", O.COL, 0, 1, 1001, 3000, 40),
+                                                    ("d", O.ROW, 1, 0, 700, 2600, 24),
+                                                    ("z", O.COL, 2, 0, 520, 1500, 24)])
+def test_crt_combine_many_tiles_per_block(handle, kind, order, ta, tb, M, N, K):
+    """Thousands of output tiles: every combine block walks several tiles, so
+    each stage of its shared-memory ring is refilled (and the last row tile is
+    partial)."""
+    rng = np.random.default_rng(31 + M)
+    A, lda, B, ldb, C, ldc = make_case(rng, kind, order, ta, tb, M, N, K)
+    alpha, beta = ((1.5, -0.25) if kind == "d" else ((1 + 0.5j), (0.5 - 0.25j)))
+    kk = K if kind == "d" else 2 * K
+    nmod, bb = crt_plan(kk, 0)
+    assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, 0) == 0
+    try:
+        dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+        assert hb.lib_gemm(handle, order, TCH[ta], TCH[tb], M, N, K, alpha, dA, lda, dB, ldb,
+                           beta, dC, ldc) == 0
+        assert hb.device_error(handle) == 0
+        got = dC.download()
+    finally:
+        hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+    _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+    err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
+    bound = (crt_bound if kind == "d" else zcrt_bound)(order, ta, tb, M, N, K, alpha, A, lda, B,
+                                                        ldb, bb, ref, beta, C, ldc)
+    assert err <= bound, (kind, nmod, bb, err, bound)
+
+
 def test_zgemm_crt_vs_native_accuracy(handle):
     """Complex config (conj-transposed A, N(0,1) parts): the CRT ZGEMM at full
     width is no less accurate than the native FP64 kernel."""
