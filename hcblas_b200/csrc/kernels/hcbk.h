@@ -243,8 +243,8 @@ typedef struct hcbk_crt_gemm {
   int64_t a_plane_stride, b_plane_stride; /* bytes, multiples of 16 */
   int nmod;
   const int *moduli; /* host array of nmod moduli */
-  int16_t *t;
-  int64_t ldt, t_plane_stride;
+  int16_t *t;                       /* 16-byte aligned */
+  int64_t ldt, t_plane_stride;      /* elements, multiples of 8 */
   int bn;   /* tile columns: 128 or 256 */
   int pair; /* 1: CTA pairs, 256 x 256 tiles (bn = 256) */
 } hcbk_crt_gemm;

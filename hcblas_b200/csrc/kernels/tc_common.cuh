@@ -209,6 +209,40 @@ __device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *m
       : "memory");
 }
 
+/* 3-D tiled bulk tensor store from this CTA's shared memory (coordinates
+ * innermost first); out-of-range parts of the box are not written.  The
+ * writing threads issue fence_proxy_async_smem() before the store. */
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int32_t c0,
+                                             int32_t c1, int32_t c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+/* make this thread's generic-proxy shared-memory writes visible to the
+ * async proxy (bulk / tensor copies) */
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+/* wait until at most N of this thread's committed bulk groups still read
+ * their shared-memory source */
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+/* wait until all of this thread's committed bulk groups have completed */
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 /* ------------------------------------------------------------ tcgen05 -- */
 
 /* TMEM allocation for a CTA pair: one warp (same warp index) in each CTA

@@ -48,6 +48,7 @@ constexpr int BM = 128;
 struct TcParams {
   CUtensorMap ta[MAX_PLANES];
   CUtensorMap tb[MAX_PLANES];
+  CUtensorMap tc; /* modular epilogue: int16 residue planes {rows, cols, plane} */
   int m, n, k;
   int k0; /* first K coordinate (K split across launches) */
   int tiles_m, tiles_n;
@@ -146,6 +147,7 @@ __device__ __forceinline__ float load_out(const __half *p) { return __half2float
 template <typename OutT> struct EpiAlphaBeta {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = false;
+  static constexpr uint32_t OUT_SMEM = 0; /* no shared-memory output staging */
   using AccT = float; /* register accumulator of the promoting path */
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
@@ -277,36 +279,47 @@ struct EpiModP {
     tmem_st_wait();
   }
 
-  /* T[m, n0 + j] = symmetric (buf_a + buf_b) mod p; has_b = 0 when the
-   * tile had a single chunk */
+  /* output staging: per epilogue warp two 32 x 32 int16 boxes (2 KB each) */
+  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * 2;
+  static constexpr uint32_t OUT_WARP_BYTES = 2 * OUT_BOX_BYTES;
+  static constexpr uint32_t OUT_SMEM = 4 * OUT_WARP_BYTES;
+
+  /* T[m0 + lane, n0 + c + j] = symmetric buffer mod p, for this warp's 32
+   * rows: each 32-column group is written to one of the warp's two
+   * shared-memory boxes (column-major int16, as the plane) and stored by one
+   * TMA tensor store, which also drops rows >= m and columns >= n; a box is
+   * rewritten only after the store issued from it two groups earlier has
+   * read it.  `out` is this warp's OUT_WARP_BYTES of shared memory. */
   template <int BN>
-  static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint32_t tb,
-                                                     bool has_b, int m, int n0, int plane) {
+  static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint8_t *out,
+                                                     int m0, int n0, int plane) {
+    const int lane = threadIdx.x & 31;
     const int mod = p.mod_tab[plane];
     const float pf = static_cast<float>(mod);
     const float inv = p.inv_mod_tab[plane];
     const float hp = static_cast<float>((mod - 1) >> 1);
-    int16_t *T = static_cast<int16_t *>(p.c) + plane * p.c_plane_stride + (long long)m +
-                 (long long)n0 * p.ldc;
-    const bool row_ok = m < p.m;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
-      uint32_t ra[32], rb[32];
+      int16_t *box = reinterpret_cast<int16_t *>(out + ((c >> 5) & 1) * OUT_BOX_BYTES);
+      uint32_t ra[32];
       tmem_ld_32x32b_x32(ta + c, ra);
-      if (has_b) tmem_ld_32x32b_x32(tb + c, rb);
+      if (lane == 0) bulk_wait_read<1>(); /* the store from this box two groups ago */
+      __syncwarp();
       tmem_ld_wait();
-      if (!row_ok) continue;
-      const int nvalid = p.n - (n0 + c);
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
-        /* both terms are exact integers below 2^24 in magnitude; each is
-         * reduced first so that the sum stays exact */
+        /* an exact integer below 2^24 in magnitude, reduced to [-(p-1)/2, (p-1)/2] */
         float v = mod_f(__uint_as_float(ra[j]), pf, inv);
-        if (has_b) v += mod_f(__uint_as_float(rb[j]), pf, inv);
-        v = mod_f(v, pf, inv);
         if (v > hp) v -= pf;
         else if (v < -hp) v += pf;
-        if (j < nvalid) T[(long long)(c + j) * p.ldc] = static_cast<int16_t>(__float2int_rn(v));
+        /* low 16 bits of the 1.5 * 2^23 + v pattern: v as int16 */
+        box[j * 32 + lane] = static_cast<int16_t>(__float_as_int(v + RND));
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_3d(&p.tc, box, m0, n0 + c, plane);
+        bulk_commit();
       }
     }
   }
@@ -322,6 +335,7 @@ __device__ __forceinline__ double pow2_bits(int e) {
 struct EpiOzaki {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = false;
+  static constexpr uint32_t OUT_SMEM = 0;
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
     const bool row_ok = m < p.m;
@@ -405,7 +419,7 @@ __host__ __device__ constexpr uint32_t tmem_cols_for(uint32_t c) {
  * the MMAs of the next; 1 when the accumulators fill TMEM).
  * CG: CTAs per MMA (1, or 2 for a CTA pair computing a 256 x BN tile; each
  * CTA of a pair holds 128 rows of A and BN/2 rows of B per stage). */
-template <int BN, int STAGES, class R, int KIND, int NBUF = 2, int CG = 1>
+template <int BN, int STAGES, class R, int KIND, int NBUF = 2, int CG = 1, uint32_t OUT = 0>
 struct TcCfg {
   using KT = KindTraits<KIND>;
   static constexpr uint32_t A_PLANE = BM * KT::ROWB;
@@ -415,7 +429,10 @@ struct TcCfg {
   static constexpr uint32_t ACC_COLS = R::NACC * BN;
   static constexpr uint32_t TMEM_COLS = tmem_cols_for(NBUF * ACC_COLS);
   static constexpr uint32_t BAR_BYTES = 256;
-  static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+  /* epilogue output staging (OUT bytes) after the barriers, 1024-aligned */
+  static constexpr uint32_t OUT_OFF = STAGES * STAGE_BYTES + 1024;
+  static constexpr uint32_t SMEM_BYTES =
+      (OUT ? OUT_OFF + OUT : STAGES * STAGE_BYTES + BAR_BYTES) + 1024;
   static_assert(NBUF * ACC_COLS <= 512, "accumulators exceed TMEM");
   static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "BN");
   static_assert(CG == 1 || (CG == 2 && KIND != 2 && !R::P3D && BN % 128 == 0), "CTA pair");
@@ -460,7 +477,7 @@ __device__ __forceinline__ WorkItem work_item(int i, int tile0, int step, int nt
 template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
           int CG = 1>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
-  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG>;
+  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG, EPI::OUT_SMEM>;
   using KT = typename Cfg::KT;
   constexpr int BKE = KT::BKE;
   constexpr int ROWB = KT::ROWB;
@@ -704,11 +721,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         if (w.c < nchunks - 1)
           EPI::template rmw<BN>(p, tb, plane);
         else
-          EPI::template final_store<BN>(p, tb, tb, false, m, tn * BN, plane);
+          EPI::template final_store<BN>(p, tb, smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES,
+                                        m - lane, tn * BN, plane);
         tc_fence_before();
         __syncwarp();
         release(b);
       }
+      if (lane == 0) bulk_wait_all(); /* the last tensor stores have landed */
     } else {
     for (int t = tile0; ok && t < num_tiles; t += tile_step) {
       const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
@@ -843,7 +862,7 @@ static int make_map_planes(CUtensorMap *map, const void *base, uint64_t kdim, ui
 template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
           int CG = 1>
 static int launch_tc(TcParams &p, void *stream) {
-  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG>;
+  using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG, EPI::OUT_SMEM>;
   auto kern = tc_gemm_kernel<BN, STAGES, R, KIND, EPI, PROMOTE_KB, NBUF, CG>;
   static bool attr_set[64] = {false};
   static int pair_slots[64] = {0}; /* co-resident CTA pairs per device */
@@ -1055,11 +1074,31 @@ static int make_map_planes_f16(CUtensorMap *map, const void *base, uint64_t kdim
   return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
 }
 
+/* 3-D map over the int16 residue planes T {rows, cols, plane}: column pitch
+ * ld elements, plane pitch pstride elements; box {32, 32, 1}, no swizzle
+ * (the modular epilogue's tensor stores). */
+static int make_map_out_i16(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols,
+                            uint64_t planes, uint64_t ld, uint64_t pstride) {
+  auto fn = encode_fn();
+  if (!fn) return HCBK_ERR_DRIVER;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || ((pstride * 2) & 15))
+    return HCBK_ERR_ALIGN;
+  cuuint64_t dims[3] = {rows, cols, planes};
+  cuuint64_t strides[2] = {ld * 2, pstride * 2};
+  cuuint32_t box[3] = {32, 32, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
+}
+
 /* Every modulus of the CRT scheme in one launch: f16 residue planes
  * (K-major, |r| <= 127) read through 3-D tensor maps, tensor-core sums exact
  * over 1024-element K chunks (PROMOTE_KB = 16 slabs of 64:
  * 1024 * 127^2 + 383 < 2^24), reduced mod p in place in TMEM between chunks,
- * int16 residues out; the persistent tile walk spans all planes.  Tiles:
+ * int16 residues out by TMA tensor stores (t 16-byte aligned, ldt and
+ * t_plane_stride multiples of 8); the persistent tile walk spans all planes.  Tiles:
  * 256 x 256 over a CTA pair, or 128 x bn on one CTA. */
 extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) {
   if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > 0x7fffffff || g->k <= 0 ||
@@ -1084,6 +1123,8 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
   p.ldc = g->ldt;
   p.nplanes = g->nmod;
   p.c_plane_stride = g->t_plane_stride;
+  rc = make_map_out_i16(&p.tc, g->t, g->m, g->n, g->nmod, g->ldt, g->t_plane_stride);
+  if (rc) return rc;
   for (int i = 0; i < g->nmod; ++i) {
     p.mod_tab[i] = g->moduli[i];
     p.inv_mod_tab[i] = 1.0f / (float)g->moduli[i];
