@@ -70,7 +70,7 @@ hcblasStatus gemv_one(Hcblaslibrary *h, const hc::accelerator_view &view, hcblas
     g.workspace = ws;
     g.max_splits = kMaxSplits;
     rc = timed_launch(st, stream, trans ? "blas2.gemv_t" : "blas2.gemv_n",
-                      [&] { return hcbk_gemv(&g, stream); });
+                      [&] { return hcbk_gemv(&g, stream); }, 2 /* partial sums + finish */);
   }
   st->last_path = alpha == 0.0 ? "blas2.scale" : (trans ? "blas2.gemv_t" : "blas2.gemv_n");
   return rc == HCBK_OK ? HCBLAS_SUCCEEDS : HCBLAS_INVALID;

@@ -295,8 +295,8 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   pb.ld_dst = kp;
   pb.f16 = f16 ? 1 : 0;
 
-  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pa, stream); });
-  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pb, stream); });
+  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pa, stream); }, pa.k_contig ? 1 : 2);
+  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&pb, stream); }, pb.k_contig ? 1 : 2);
   if (!rc) rc = timed_launch(st, stream, "ozaki.slice", [&] { return hcbk_ozaki_slice(&pa, stream); });
   if (!rc) rc = timed_launch(st, stream, "ozaki.slice", [&] { return hcbk_ozaki_slice(&pb, stream); });
   if (rc) return rc;
@@ -367,8 +367,9 @@ bool crt_plan(int64_t k, int want, int *nmod, int *beta) {
 }
 
 /* CRT (Ozaki scheme II) DGEMM: exponents, residue planes of the scaled
- * integer operands, one modular tensor-core GEMM per modulus, Garner
- * reconstruction with the alpha/beta epilogue. */
+ * integer operands, one modular tensor-core GEMM launch over every modulus,
+ * CRT reconstruction (weighted residue sum mod M) with the alpha/beta
+ * epilogue. */
 int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
               const char **path) {
   if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
@@ -405,8 +406,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   eb.k_contig = a->op_b == HCBK_OP_N;
   eb.rows = a->n;
   eb.exps = exp_b;
-  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); });
-  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); });
+  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); }, ea.k_contig ? 1 : 2);
+  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); }, eb.k_contig ? 1 : 2);
   if (rc) return rc;
 
   hcbk_crt_prep ra;
@@ -540,8 +541,8 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   eb.rows = b_k ? a->n : 2 * a->n;
   eb.kdim = b_k ? 2 * a->k : a->k;
   eb.exps = exp_b;
-  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); });
-  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); });
+  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); }, ea.k_contig ? 1 : 2);
+  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); }, eb.k_contig ? 1 : 2);
   if (rc) return rc;
 
   hcbk_zcrt_prep ra;

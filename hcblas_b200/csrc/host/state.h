@@ -75,19 +75,17 @@ struct HcblasB200State {
 
 namespace hcblas_b200 {
 
-/* Launch one kernel through `fn` (returns an HCBK_* code); when profiling is
- * on, bracket it with CUDA events on `stream`.  Counts every launch. */
-template <typename F>
-int timed_launch(HcblasB200State *st, void *stream, const char *name, F &&fn);
-
 /* cumulative number of kernels launched by this library in this process */
 void count_launch(int n = 1);
 long long launch_count();
 void *prof_event(HcblasB200State *st);
 void prof_record(void *ev, void *stream);
 
+/* Run `fn` (one library call, returning an HCBK_* code, that launches
+ * `kernels` kernels); when profiling is on, bracket it with CUDA events on
+ * `stream`.  Counts every kernel launch. */
 template <typename F>
-int timed_launch(HcblasB200State *st, void *stream, const char *name, F &&fn) {
+int timed_launch(HcblasB200State *st, void *stream, const char *name, F &&fn, int kernels = 1) {
   if (st && st->profiling) {
     void *e0 = prof_event(st);
     void *e1 = prof_event(st);
@@ -95,11 +93,11 @@ int timed_launch(HcblasB200State *st, void *stream, const char *name, F &&fn) {
     int rc = fn();
     prof_record(e1, stream);
     st->prof.push_back(HcblasProfRec{name, e0, e1});
-    if (rc == 0) count_launch();
+    if (rc == 0) count_launch(kernels);
     return rc;
   }
   int rc = fn();
-  if (rc == 0) count_launch();
+  if (rc == 0) count_launch(kernels);
   return rc;
 }
 
