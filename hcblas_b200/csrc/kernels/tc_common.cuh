@@ -209,6 +209,17 @@ __device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *m
       : "memory");
 }
 
+/* 2-D tiled bulk tensor store from this CTA's shared memory (coordinates
+ * innermost first); out-of-range parts of the box are not written. */
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, const void *src, int32_t c0,
+                                             int32_t c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(c0), "r"(c1)
+      : "memory");
+}
+
 /* 3-D tiled bulk tensor store from this CTA's shared memory (coordinates
  * innermost first); out-of-range parts of the box are not written.  The
  * writing threads issue fence_proxy_async_smem() before the store. */

@@ -48,7 +48,8 @@ constexpr int BM = 128;
 struct TcParams {
   CUtensorMap ta[MAX_PLANES];
   CUtensorMap tb[MAX_PLANES];
-  CUtensorMap tc; /* modular epilogue: int16 residue planes {rows, cols, plane} */
+  CUtensorMap tc; /* output map: int16 residue planes {rows, cols, plane} of the
+                     modular epilogue, or f16 C {rows, cols} when out_tma is set */
   int m, n, k;
   int k0; /* first K coordinate (K split across launches) */
   int tiles_m, tiles_n;
@@ -57,6 +58,7 @@ struct TcParams {
   long long ldc;
   float alpha, beta;
   int beta_nonzero;
+  int out_tma; /* f16 epilogue: C read (beta != 0) and written by TMA via tc */
   int *err;
   /* Ozaki epilogue */
   double alpha_d, beta_d;
@@ -143,15 +145,90 @@ __device__ __forceinline__ void store_out(__half *p, float v) { *p = __float2hal
 __device__ __forceinline__ float load_out(const float *p) { return *p; }
 __device__ __forceinline__ float load_out(const __half *p) { return __half2float(*p); }
 
+/* An epilogue warp's output staging: its two 32 x 32 boxes in shared memory,
+ * the two mbarriers their C loads complete on, and the parity bit of each. */
+struct OutStage {
+  uint8_t *box;
+  uint64_t *bar;
+  uint32_t phase;
+};
+
 /* f32 accumulator -> alpha*acc + beta*C in OutT (float or half) */
 template <typename OutT> struct EpiAlphaBeta {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = false;
-  static constexpr uint32_t OUT_SMEM = 0; /* no shared-memory output staging */
+  /* f16 output: per epilogue warp two 32 x 32 boxes in shared memory for
+   * the TMA-store path (f32 outputs, written by the split paths whose stages
+   * fill shared memory, keep plain stores) */
+  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * sizeof(OutT);
+  static constexpr uint32_t OUT_WARP_BYTES = sizeof(OutT) == 2 ? 2 * OUT_BOX_BYTES : 0;
+  static constexpr uint32_t OUT_SMEM = 4 * OUT_WARP_BYTES;
   using AccT = float; /* register accumulator of the promoting path */
+
+  /* C addressable by a tensor map: each 32-column group of this warp's 32
+   * rows goes to one of the warp's two boxes (column-major, as C) and leaves
+   * by one TMA tensor store, which drops rows >= m and columns >= n.  With
+   * beta != 0 the C box of the next group is fetched by a TMA load into the
+   * other box while this one is computed.  A box is rewritten only after the
+   * store issued from it has read it. */
+  template <int BN>
+  static __device__ __forceinline__ void run_tma(const TcParams &p, uint32_t tbase, int m0,
+                                                 int n0, OutStage &os) {
+    const int lane = threadIdx.x & 31;
+    const bool ld_c = p.beta_nonzero != 0;
+    if (ld_c && lane == 0) {
+      bulk_wait_read<0>(); /* both boxes free */
+      mbar_expect_tx(&os.bar[0], OUT_BOX_BYTES);
+      tma_load_2d(os.box, &p.tc, &os.bar[0], m0, n0);
+    }
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32) {
+      const int b = (c >> 5) & 1;
+      OutT *box = reinterpret_cast<OutT *>(os.box + b * OUT_BOX_BYTES);
+      uint32_t r[32];
+      tmem_ld_32x32b_x32(tbase + c, r);
+      if (lane == 0) {
+        if (!ld_c) {
+          bulk_wait_read<1>(); /* the store from this box two groups ago */
+        } else if (c + 32 < BN) {
+          bulk_wait_read<0>(); /* the other box's store has read it */
+          mbar_expect_tx(&os.bar[b ^ 1], OUT_BOX_BYTES);
+          tma_load_2d(os.box + (b ^ 1) * OUT_BOX_BYTES, &p.tc, &os.bar[b ^ 1], m0, n0 + c + 32);
+        }
+      }
+      __syncwarp();
+      tmem_ld_wait();
+      if (ld_c) {
+        mbar_wait(&os.bar[b], (os.phase >> b) & 1u, p.err, ERR_TIMEOUT_EPILOGUE);
+        os.phase ^= 1u << b;
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          store_out(box + j * 32 + lane,
+                    fmaf(p.beta, load_out(box + j * 32 + lane), p.alpha * __uint_as_float(r[j])));
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          store_out(box + j * 32 + lane, p.alpha * __uint_as_float(r[j]));
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_2d(&p.tc, box, m0, n0 + c);
+        bulk_commit();
+      }
+    }
+  }
+
   template <int BN, int NACC>
-  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
+  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0,
+                                             OutStage &os) {
     static_assert(NACC == 1, "several accumulators need the promoting epilogue");
+    if constexpr (OUT_SMEM > 0) {
+      if (p.out_tma) {
+        run_tma<BN>(p, tbase, m - (int)(threadIdx.x & 31), n0, os);
+        return;
+      }
+    }
     const bool row_ok = m < p.m;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
@@ -257,7 +334,7 @@ struct EpiModP {
   }
 
   template <int BN, int NACC>
-  static __device__ __forceinline__ void run(const TcParams &, uint32_t, int, int) {
+  static __device__ __forceinline__ void run(const TcParams &, uint32_t, int, int, OutStage &) {
     static_assert(NACC == 0, "the modular epilogue only runs on the in-place path");
   }
 
@@ -335,9 +412,10 @@ __device__ __forceinline__ double pow2_bits(int e) {
 struct EpiOzaki {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = false;
-  static constexpr uint32_t OUT_SMEM = 0;
+  static constexpr uint32_t OUT_SMEM = 0, OUT_WARP_BYTES = 0;
   template <int BN, int NACC>
-  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0) {
+  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0,
+                                             OutStage &) {
     const bool row_ok = m < p.m;
     const int ea = row_ok ? p.exp_a[m] : 0;
     double *C = static_cast<double *>(p.c) + (long long)m;
@@ -491,6 +569,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   uint64_t *tfull = empty + STAGES;
   uint64_t *tempty = tfull + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+  uint64_t *obar = tempty + 4; /* output staging: two C-load barriers per epilogue warp */
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -507,6 +586,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4 * CG);
     }
+    if constexpr (EPI::OUT_SMEM > 0)
+      for (int b = 0; b < 8; ++b) mbar_init(&obar[b], 1);
     mbar_fence_init();
   }
   if (warp == 0 && lane == 0) {
@@ -691,6 +772,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     const int q = warp & 3; /* TMEM lane quadrant of this warp */
     int ci = 0;
     bool ok = true;
+    OutStage ostage{smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES, obar + 2 * q, 0u};
     /* TMEM buffer released to the leader's MMA thread */
     auto release = [&](int b) {
       if (lane == 0) {
@@ -721,13 +803,11 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         if (w.c < nchunks - 1)
           EPI::template rmw<BN>(p, tb, plane);
         else
-          EPI::template final_store<BN>(p, tb, smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES,
-                                        m - lane, tn * BN, plane);
+          EPI::template final_store<BN>(p, tb, ostage.box, m - lane, tn * BN, plane);
         tc_fence_before();
         __syncwarp();
         release(b);
       }
-      if (lane == 0) bulk_wait_all(); /* the last tensor stores have landed */
     } else {
     for (int t = tile0; ok && t < num_tiles; t += tile_step) {
       const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
@@ -742,7 +822,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         tc_fence_after();
         const uint32_t tbase =
             tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS;
-        EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN);
+        EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN, ostage);
         tc_fence_before();
         __syncwarp();
         release(b);
@@ -769,6 +849,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       }
     }
     }
+    if constexpr (EPI::OUT_SMEM > 0)
+      if (lane == 0) bulk_wait_all(); /* this warp's last tensor stores have landed */
   }
 
   tc_fence_before();
@@ -924,6 +1006,25 @@ extern "C" int hcbk_encode_tma_2d(void *map, int bf16, const void *base, uint64_
                   base, inner, outer, ld, box_inner, box_outer);
 }
 
+/* 2-D map over a column-major f16 C {rows, cols}, column pitch ld elements;
+ * box {32, 32}, no swizzle.  HCBK_ERR_ALIGN when C is not TMA-addressable
+ * (base not 16-byte aligned, pitch not a multiple of 8 elements). */
+static int make_map_out_f16(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols,
+                            uint64_t ld) {
+  auto fn = encode_fn();
+  if (!fn) return HCBK_ERR_DRIVER;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || rows == 0 || cols == 0)
+    return HCBK_ERR_ALIGN;
+  cuuint64_t dims[2] = {rows, cols};
+  cuuint64_t strides[1] = {ld * 2};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
+}
+
 /* f16 operands straight from the caller's matrices (column-major canonical). */
 extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream) {
   if (a->dtype != HCBK_H || a->batch != 1 || a->a_array || a->op_a == HCBK_OP_C ||
@@ -961,6 +1062,9 @@ extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err
   p.beta = (float)a->beta_re;
   p.beta_nonzero = a->beta_re != 0.0;
   p.err = err;
+  /* C tensor-map addressable: the epilogue stages 32 x 32 boxes in shared
+   * memory, reading C (beta != 0) and writing it by TMA */
+  p.out_tma = make_map_out_f16(&p.tc, p.c, a->m, a->n, a->ldc) == HCBK_OK;
   using EH = EpiAlphaBeta<__half>;
   if (pair) return launch_tc<256, 6, RecipeSingle, 0, EH, 0, 2, 2>(p, stream);
   if (bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EH>(p, stream);
