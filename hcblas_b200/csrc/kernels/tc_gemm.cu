@@ -552,6 +552,24 @@ __device__ __forceinline__ WorkItem work_item(int i, int tile0, int step, int nt
   return WorkItem{tile0 + lt * step, i - lt * nchunks, 0};
 }
 
+/* Tile order within a plane: bands of TILE_GROUP tile rows, walked column
+ * by column and down each column inside the band, so that the tiles running
+ * at the same time (one per SM or SM pair) cover about TILE_GROUP row tiles
+ * by (concurrent / TILE_GROUP) column tiles; their A and B panels then stay
+ * in L2 where a column-major walk over all tile rows streams the whole of A
+ * from DRAM once per wave. */
+constexpr int TILE_GROUP = 8;
+struct TileMN {
+  int m, n;
+};
+__device__ __forceinline__ TileMN tile_mn(int t, int tiles_m, int tiles_n) {
+  const int band = t / (TILE_GROUP * tiles_n);
+  const int first = band * TILE_GROUP;
+  const int rows = tiles_m - first < TILE_GROUP ? tiles_m - first : TILE_GROUP;
+  const int r = t - band * TILE_GROUP * tiles_n;
+  return TileMN{first + r % rows, r / rows};
+}
+
 template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
           int CG = 1>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
@@ -636,7 +654,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const int t = w.t;
         const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
         const int tt = t - plane * tiles_per_plane;
-        const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
+        const TileMN tc_ = tile_mn(tt, p.tiles_m, p.tiles_n);
+        const int tm = tc_.m, tn = tc_.n;
         const int row0 = (tm * CG + (int)rank) * BM;               /* this CTA's A rows */
         const int col0 = tn * BN + (int)rank * (int)Cfg::B_ROWS;   /* this CTA's B rows */
         const int kb_end = (w.c + 1) * chunk_kb < kblocks ? (w.c + 1) * chunk_kb : kblocks;
@@ -792,7 +811,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const WorkItem w = work_item(i, tile0, tile_step, ntiles_local, nchunks, true);
         const int plane = EPI::PLANE_BATCH ? w.t / tiles_per_plane : 0;
         const int tt = w.t - plane * tiles_per_plane;
-        const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
+        const TileMN tc_ = tile_mn(tt, p.tiles_m, p.tiles_n);
+        const int tm = tc_.m, tn = tc_.n;
         const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
         const int b = w.slot;
         const uint32_t tph = (euses >> b) & 1u;
@@ -812,7 +832,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     for (int t = tile0; ok && t < num_tiles; t += tile_step) {
       const int plane = EPI::PLANE_BATCH ? t / tiles_per_plane : 0;
       const int tt = t - plane * tiles_per_plane;
-      const int tm = tt % p.tiles_m, tn = tt / p.tiles_m;
+      const TileMN tc_ = tile_mn(tt, p.tiles_m, p.tiles_n);
+      const int tm = tc_.m, tn = tc_.n;
       const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
       if constexpr (PROMOTE_KB == 0) {
         const int b = ci % NBUF;
