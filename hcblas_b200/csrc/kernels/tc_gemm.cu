@@ -157,77 +157,86 @@ struct OutStage {
 template <typename OutT> struct EpiAlphaBeta {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = false;
-  /* f16 output: per epilogue warp two 32 x 32 boxes in shared memory for
-   * the TMA-store path (f32 outputs, written by the split paths whose stages
-   * fill shared memory, keep plain stores) */
+  /* output staging: per epilogue warp two 32 x 32 boxes of OutT in shared
+   * memory (a kernel configuration whose stages leave no room for them runs
+   * without: OutStage::box is then null and C is written by plain stores) */
   static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * sizeof(OutT);
-  static constexpr uint32_t OUT_WARP_BYTES = sizeof(OutT) == 2 ? 2 * OUT_BOX_BYTES : 0;
+  static constexpr uint32_t OUT_WARP_BYTES = 2 * OUT_BOX_BYTES;
   static constexpr uint32_t OUT_SMEM = 4 * OUT_WARP_BYTES;
   using AccT = float; /* register accumulator of the promoting path */
 
-  /* C addressable by a tensor map: each 32-column group of this warp's 32
-   * rows goes to one of the warp's two boxes (column-major, as C) and leaves
-   * by one TMA tensor store, which drops rows >= m and columns >= n.  With
-   * beta != 0 the C box of the next group is fetched by a TMA load into the
-   * other box while this one is computed.  A box is rewritten only after the
-   * store issued from it has read it. */
-  template <int BN>
-  static __device__ __forceinline__ void run_tma(const TcParams &p, uint32_t tbase, int m0,
-                                                 int n0, OutStage &os) {
+  /* One 32-column group c of this warp's 32 rows through box (c / 32) % 2:
+   * values alpha * v (+ beta * C, C fetched by a TMA load that the previous
+   * group started, or the tile's first group starts here) go to the box,
+   * column-major as C, and leave by one TMA tensor store, which drops rows
+   * >= m and columns >= n.  A box is rewritten only after the store issued
+   * from it has read it.  load_v(r) fills r with the group's 32 f32 values
+   * (bit patterns); it may start an asynchronous fetch that wait_v() ends. */
+  template <int BN, class LoadV, class WaitV>
+  static __device__ __forceinline__ void stage_group(const TcParams &p, int c, int m0, int n0,
+                                                     OutStage &os, LoadV &&load_v,
+                                                     WaitV &&wait_v) {
     const int lane = threadIdx.x & 31;
     const bool ld_c = p.beta_nonzero != 0;
-    if (ld_c && lane == 0) {
-      bulk_wait_read<0>(); /* both boxes free */
-      mbar_expect_tx(&os.bar[0], OUT_BOX_BYTES);
-      tma_load_2d(os.box, &p.tc, &os.bar[0], m0, n0);
-    }
-#pragma unroll 1
-    for (int c = 0; c < BN; c += 32) {
-      const int b = (c >> 5) & 1;
-      OutT *box = reinterpret_cast<OutT *>(os.box + b * OUT_BOX_BYTES);
-      uint32_t r[32];
-      tmem_ld_32x32b_x32(tbase + c, r);
-      if (lane == 0) {
-        if (!ld_c) {
-          bulk_wait_read<1>(); /* the store from this box two groups ago */
-        } else if (c + 32 < BN) {
-          bulk_wait_read<0>(); /* the other box's store has read it */
+    const int b = (c >> 5) & 1;
+    OutT *box = reinterpret_cast<OutT *>(os.box + b * OUT_BOX_BYTES);
+    uint32_t r[32];
+    load_v(r);
+    if (lane == 0) {
+      if (!ld_c) {
+        bulk_wait_read<1>(); /* the store from this box two groups ago */
+      } else {
+        if (c == 0) { /* first group of the tile: fetch its own C box */
+          bulk_wait_read<0>();
+          mbar_expect_tx(&os.bar[0], OUT_BOX_BYTES);
+          tma_load_2d(os.box, &p.tc, &os.bar[0], m0, n0);
+        }
+        if (c + 32 < BN) { /* prefetch the next group's C into the other box */
+          bulk_wait_read<0>();
           mbar_expect_tx(&os.bar[b ^ 1], OUT_BOX_BYTES);
           tma_load_2d(os.box + (b ^ 1) * OUT_BOX_BYTES, &p.tc, &os.bar[b ^ 1], m0, n0 + c + 32);
         }
       }
-      __syncwarp();
-      tmem_ld_wait();
-      if (ld_c) {
-        mbar_wait(&os.bar[b], (os.phase >> b) & 1u, p.err, ERR_TIMEOUT_EPILOGUE);
-        os.phase ^= 1u << b;
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          store_out(box + j * 32 + lane,
-                    fmaf(p.beta, load_out(box + j * 32 + lane), p.alpha * __uint_as_float(r[j])));
-      } else {
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          store_out(box + j * 32 + lane, p.alpha * __uint_as_float(r[j]));
-      }
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) {
-        tma_store_2d(&p.tc, box, m0, n0 + c);
-        bulk_commit();
-      }
     }
+    __syncwarp();
+    wait_v();
+    if (ld_c) {
+      mbar_wait(&os.bar[b], (os.phase >> b) & 1u, p.err, ERR_TIMEOUT_EPILOGUE);
+      os.phase ^= 1u << b;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        store_out(box + j * 32 + lane,
+                  fmaf(p.beta, load_out(box + j * 32 + lane), p.alpha * __uint_as_float(r[j])));
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) store_out(box + j * 32 + lane, p.alpha * __uint_as_float(r[j]));
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tma_store_2d(&p.tc, box, m0, n0 + c);
+      bulk_commit();
+    }
+  }
+
+  /* the TMEM accumulator of one tile through the staged path */
+  template <int BN>
+  static __device__ __forceinline__ void run_tma(const TcParams &p, uint32_t tbase, int m0,
+                                                 int n0, OutStage &os) {
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32)
+      stage_group<BN>(
+          p, c, m0, n0, os, [&](uint32_t(&r)[32]) { tmem_ld_32x32b_x32(tbase + c, r); },
+          [] { tmem_ld_wait(); });
   }
 
   template <int BN, int NACC>
   static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0,
                                              OutStage &os) {
     static_assert(NACC == 1, "several accumulators need the promoting epilogue");
-    if constexpr (OUT_SMEM > 0) {
-      if (p.out_tma) {
-        run_tma<BN>(p, tbase, m - (int)(threadIdx.x & 31), n0, os);
-        return;
-      }
+    if (os.box && p.out_tma) {
+      run_tma<BN>(p, tbase, m - (int)(threadIdx.x & 31), n0, os);
+      return;
     }
     const bool row_ok = m < p.m;
 #pragma unroll 1
@@ -292,7 +301,20 @@ template <typename OutT> struct EpiAlphaBeta {
 
   template <int BN>
   static __device__ __forceinline__ void store_acc(const TcParams &p, const float (&acc)[BN],
-                                                   int m, int n0) {
+                                                   int m, int n0, OutStage &os) {
+    if (os.box && p.out_tma) { /* every lane takes part: rows >= m are dropped by the store */
+      const int m0 = m - (int)(threadIdx.x & 31);
+#pragma unroll
+      for (int c = 0; c < BN; c += 32)
+        stage_group<BN>(
+            p, c, m0, n0, os,
+            [&](uint32_t(&r)[32]) {
+#pragma unroll
+              for (int j = 0; j < 32; ++j) r[j] = __float_as_uint(acc[c + j]);
+            },
+            [] {});
+      return;
+    }
     if (m >= p.m) return;
 #pragma unroll
     for (int c = 0; c < BN; c += 32) {
@@ -507,10 +529,12 @@ struct TcCfg {
   static constexpr uint32_t ACC_COLS = R::NACC * BN;
   static constexpr uint32_t TMEM_COLS = tmem_cols_for(NBUF * ACC_COLS);
   static constexpr uint32_t BAR_BYTES = 256;
-  /* epilogue output staging (OUT bytes) after the barriers, 1024-aligned */
+  /* epilogue output staging (OUT bytes wanted) after the barriers,
+   * 1024-aligned, when the stages leave room for it */
   static constexpr uint32_t OUT_OFF = STAGES * STAGE_BYTES + 1024;
+  static constexpr uint32_t OUT_BYTES = OUT_OFF + OUT + 1024 <= 232448 ? OUT : 0;
   static constexpr uint32_t SMEM_BYTES =
-      (OUT ? OUT_OFF + OUT : STAGES * STAGE_BYTES + BAR_BYTES) + 1024;
+      (OUT_BYTES ? OUT_OFF + OUT_BYTES : STAGES * STAGE_BYTES + BAR_BYTES) + 1024;
   static_assert(NBUF * ACC_COLS <= 512, "accumulators exceed TMEM");
   static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "BN");
   static_assert(CG == 1 || (CG == 2 && KIND != 2 && !R::P3D && BN % 128 == 0), "CTA pair");
@@ -604,7 +628,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4 * CG);
     }
-    if constexpr (EPI::OUT_SMEM > 0)
+    if constexpr (Cfg::OUT_BYTES > 0)
       for (int b = 0; b < 8; ++b) mbar_init(&obar[b], 1);
     mbar_fence_init();
   }
@@ -791,7 +815,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     const int q = warp & 3; /* TMEM lane quadrant of this warp */
     int ci = 0;
     bool ok = true;
-    OutStage ostage{smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES, obar + 2 * q, 0u};
+    OutStage ostage{Cfg::OUT_BYTES ? smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES : nullptr,
+                    obar + 2 * q, 0u};
+    static_assert(!EPI::INPLACE || Cfg::OUT_BYTES > 0, "the modular epilogue stores by TMA");
     /* TMEM buffer released to the leader's MMA thread */
     auto release = [&](int b) {
       if (lane == 0) {
@@ -817,7 +843,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const int b = w.slot;
         const uint32_t tph = (euses >> b) & 1u;
         euses ^= 1u << b;
-        if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) break;
+        if (!__all_sync(0xffffffffu, mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE))) break;
         tc_fence_after();
         const uint32_t tb = tmem_base + lane_off + b * Cfg::ACC_COLS;
         if (w.c < nchunks - 1)
@@ -839,7 +865,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const int b = ci % NBUF;
         const uint32_t tph = (ci / NBUF) & 1;
         ++ci;
-        if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) break;
+        if (!__all_sync(0xffffffffu, mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE))) break;
         tc_fence_after();
         const uint32_t tbase =
             tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS;
@@ -854,7 +880,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         for (int kc = 0; kc < kblocks; kc += chunk_kb, ++ci) {
           const int b = ci % NBUF;
           const uint32_t tph = (ci / NBUF) & 1;
-          if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) {
+          if (!__all_sync(0xffffffffu, mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE))) {
             ok = false;
             break;
           }
@@ -866,11 +892,11 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           __syncwarp();
           release(b);
         }
-        if (ok) EPI::template store_acc<BN>(p, acc, m, tn * BN);
+        if (ok) EPI::template store_acc<BN>(p, acc, m, tn * BN, ostage);
       }
     }
     }
-    if constexpr (EPI::OUT_SMEM > 0)
+    if constexpr (Cfg::OUT_BYTES > 0)
       if (lane == 0) bulk_wait_all(); /* this warp's last tensor stores have landed */
   }
 
@@ -1027,22 +1053,23 @@ extern "C" int hcbk_encode_tma_2d(void *map, int bf16, const void *base, uint64_
                   base, inner, outer, ld, box_inner, box_outer);
 }
 
-/* 2-D map over a column-major f16 C {rows, cols}, column pitch ld elements;
- * box {32, 32}, no swizzle.  HCBK_ERR_ALIGN when C is not TMA-addressable
- * (base not 16-byte aligned, pitch not a multiple of 8 elements). */
-static int make_map_out_f16(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols,
-                            uint64_t ld) {
+/* 2-D map over a column-major C {rows, cols} of esz-byte elements, column
+ * pitch ld elements; box {32, 32}, no swizzle.  HCBK_ERR_ALIGN when C is not
+ * TMA-addressable (base not 16-byte aligned, pitch not a multiple of 16
+ * bytes). */
+static int make_map_out(CUtensorMap *map, CUtensorMapDataType dt, uint32_t esz, void *base,
+                        uint64_t rows, uint64_t cols, uint64_t ld) {
   auto fn = encode_fn();
   if (!fn) return HCBK_ERR_DRIVER;
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || rows == 0 || cols == 0)
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * esz) & 15) || rows == 0 || cols == 0)
     return HCBK_ERR_ALIGN;
   cuuint64_t dims[2] = {rows, cols};
-  cuuint64_t strides[1] = {ld * 2};
+  cuuint64_t strides[1] = {ld * esz};
   cuuint32_t box[2] = {32, 32};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = fn(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
 }
 
@@ -1085,7 +1112,8 @@ extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err
   p.err = err;
   /* C tensor-map addressable: the epilogue stages 32 x 32 boxes in shared
    * memory, reading C (beta != 0) and writing it by TMA */
-  p.out_tma = make_map_out_f16(&p.tc, p.c, a->m, a->n, a->ldc) == HCBK_OK;
+  p.out_tma =
+      make_map_out(&p.tc, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, p.c, a->m, a->n, a->ldc) == HCBK_OK;
   using EH = EpiAlphaBeta<__half>;
   if (pair) return launch_tc<256, 6, RecipeSingle, 0, EH, 0, 2, 2>(p, stream);
   if (bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EH>(p, stream);
@@ -1120,6 +1148,10 @@ extern "C" int hcbk_sgemm_split_tc(const hcbk_split_gemm *g, int *err, void *str
   p.beta_nonzero = g->beta != 0.0;
   p.err = err;
   /* two accumulators per chunk, double-buffered: 2 x 2 x 128 TMEM columns */
+  /* C tensor-map addressable: configurations with room stage the epilogue
+   * through shared memory and TMA */
+  p.out_tma = make_map_out(&p.tc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, p.c, g->m, g->n,
+                           g->ldc) == HCBK_OK;
   using EF = EpiAlphaBeta<float>;
   if (g->pair) {
     if (g->terms == 6) {
