@@ -15,8 +15,10 @@ Printed (rank 0, one JSON line):
               step per GPU / max-over-ranks time)
   native      the native FP64 DGEMM kernel on the same workload and its
               error; speedup = value / native
-  e2e         the same metric through hcblasSetMatrix (H2D from pinned host
-              memory) + hcblasDgemm + hcblasGetMatrix (D2H) per step
+  e2e         the same metric through hcblasSetMatrixAsync (H2D from pinned
+              host memory) + hcblasDgemm + hcblasGetMatrixAsync (D2H) per
+              step, neighbouring steps' copies overlapping the GEMM (the
+              serial form, every copy waited for, is reported beside it)
   roofline    the dominant kernel (one modular f16 GEMM per modulus) against
               the measured dense bf16/f16 tensor peak, with its ncu DRAM
               traffic per launch from profiles/traffic.json
@@ -440,26 +442,76 @@ def main():
                  for k, v in prof.items()}
 
     # ---- end to end through the C ABI with host buffers ----
+    # Each step copies its inputs from pinned host memory (hcblasSetMatrixAsync
+    # on a copy-in stream), runs hcblasDgemm on the handle's stream and copies
+    # C back (hcblasGetMatrixAsync on a copy-out stream); two device buffer
+    # sets let step i+1's inputs and step i-1's result cross PCIe while step i
+    # computes, as a caller streaming GEMMs would run them.  Events order the
+    # three streams.  The serial form (every copy waited for) is reported too.
     pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    hA, hB, hC = pin(M * K), pin(N * K), pin(M * N)
+    hA, hB = pin(M * K), pin(N * K)
+    hC = [pin(M * N), pin(M * N)]
     hA[:] = A
     hB[:] = B
-    e2e_steps = max(1, min(args.steps, 5))
-    hb.hcblasSetMatrix(h, M, K, 8, hA.ctypes.data, M, dA.ptr, M)
+    e2e_steps = max(3, min(args.steps, 10))
+    bufs = [(dA, dB, dC)] + [tuple(hb.DeviceArray(h, nbytes=8 * x, dtype=np.float64)
+                                   for x in (M * K, N * K, M * N))]
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    ev = lambda: torch.cuda.Event()
+    ev_in, ev_comp, ev_out = [ev(), ev()], [ev(), ev()], [ev(), ev()]
+
+    def e2e_step(i):
+        b = i & 1
+        a_, b_, c_ = bufs[b]
+        s_in.wait_event(ev_comp[b])  # the GEMM that last read these inputs is done
+        assert hb.hcblasSetMatrixAsync(h, M, K, 8, hA.ctypes.data, M, a_.ptr, M,
+                                       s_in.cuda_stream) == 0
+        assert hb.hcblasSetMatrixAsync(h, N, K, 8, hB.ctypes.data, N, b_.ptr, N,
+                                       s_in.cuda_stream) == 0
+        ev_in[b].record(s_in)
+        stream.wait_event(ev_in[b])
+        stream.wait_event(ev_out[b])  # C of two steps ago has left
+        assert L.hcblasDgemm(h, hb.HCBLAS_OP_N, hb.HCBLAS_OP_T, M, N, K, one.ctypes.data,
+                             a_.ptr, M, b_.ptr, N, zero.ctypes.data, c_.ptr, M) == 0
+        ev_comp[b].record(stream)
+        s_out.wait_event(ev_comp[b])
+        assert hb.hcblasGetMatrixAsync(h, M, N, 8, c_.ptr, M, hC[b].ctypes.data, M,
+                                       s_out.cuda_stream) == 0
+        ev_out[b].record(s_out)
+
+    for i in range(2):  # warm-up of the pipeline
+        e2e_step(i)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
+    e0.record(s_in)
+    stream.wait_event(e0)
+    s_out.wait_event(e0)
+    for i in range(e2e_steps):
+        e2e_step(i)
+    s_in.wait_event(ev_out[0])
+    s_in.wait_event(ev_out[1])
+    e1.record(s_in)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    assert hb.device_error(h) == 0
+    err_e2e = oracle_err(O, hC[(e2e_steps - 1) & 1].reshape(N, M).T, A, M, 0, B, N, 1, M, K,
+                         cols, N)
+    # serial form: every copy waited for
+    es0 = torch.cuda.Event(enable_timing=True)
+    es1 = torch.cuda.Event(enable_timing=True)
+    es0.record(stream)
+    for _ in range(3):
         assert hb.hcblasSetMatrix(h, M, K, 8, hA.ctypes.data, M, dA.ptr, M) == 0
         assert hb.hcblasSetMatrix(h, N, K, 8, hB.ctypes.data, N, dB.ptr, N) == 0
         step()
-        assert hb.hcblasGetMatrix(h, M, N, 8, dC.ptr, M, hC.ctypes.data, M) == 0
-    e1.record(stream)
+        assert hb.hcblasGetMatrix(h, M, N, 8, dC.ptr, M, hC[0].ctypes.data, M) == 0
+    es1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    e2e_serial_ms = es0.elapsed_time(es1) / 3
+    del bufs[1]
     if dist:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -469,7 +521,7 @@ def main():
     # ---- accuracy (rank 0), hard variant, CPU baseline (rank 0, N = 1) ----
     line = None
     if rank == 0:
-        Cg = hC.reshape(N, M).T  # (M, N) view of the column-major result
+        Cg = hC[0].reshape(N, M).T  # (M, N) view of the serial end-to-end result
         err_dd = oracle_err(O, Cg, A, M, 0, B, N, 1, M, K, cols, N)
         # hard variant: N(0,1) * 2^e, e ~ U{-20..20} per row of A / column of op(B)
         hr = np.random.default_rng(11)
@@ -512,7 +564,13 @@ def main():
                        "speedup_emulated_vs_native": round(value / world / native_tflops, 3)},
             "e2e": {"value": round(e2e, 3), "unit": "TFLOPS",
                     "h2d_bytes_per_step": 8 * (M * K + N * K),
-                    "d2h_bytes_per_step": 8 * M * N, "ms_per_step": round(e2e_ms, 3)},
+                    "d2h_bytes_per_step": 8 * M * N, "ms_per_step": round(e2e_ms, 3),
+                    "steps": e2e_steps,
+                    "form": "hcblasSetMatrixAsync (pinned) -> hcblasDgemm -> "
+                            "hcblasGetMatrixAsync per step, copies of neighbouring steps "
+                            "overlapping the GEMM on three streams",
+                    "serial_ms_per_step": round(e2e_serial_ms, 3),
+                    "normwise_err_last_step": err_e2e},
             "roofline": {"kernel": dom, "bound": "tensor",
                          "achieved": round(achieved, 2) if achieved else None,
                          "peak": peak, "unit": "TFLOP/s",

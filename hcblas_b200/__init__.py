@@ -46,7 +46,7 @@ HCBLAS_MATH_OZAKI_CRT = 4
 EXPORTED = (
     "hcblasCreate", "hcblasDestroy", "hcblasSetAcclView", "hcblasGetAcclView",
     "hcblasSetStream", "hcblasSetVector", "hcblasGetVector", "hcblasSetMatrix",
-    "hcblasGetMatrix", "hcblasSgemm", "hcblasDgemm", "hcblasCgemm", "hcblasZgemm",
+    "hcblasGetMatrix", "hcblasSetMatrixAsync", "hcblasGetMatrixAsync", "hcblasSgemm", "hcblasDgemm", "hcblasCgemm", "hcblasZgemm",
     "hcblasHgemm", "hcblasSgemmBatched", "hcblasCgemmBatched", "hcblasDgemmBatched",
     "hcblasZgemmBatched", "hcblasHgemmBatched", "hcblasSgemmStridedBatched",
     "hcblasDgemmStridedBatched", "hcblasCgemmStridedBatched", "hcblasZgemmStridedBatched",
@@ -122,6 +122,10 @@ def lib():
         for n in ("hcblasSetMatrix", "hcblasGetMatrix"):
             f = getattr(L, n)
             f.argtypes = [vp, ci, ci, ci, vp, ci, vp, ci]
+            f.restype = st
+        for n in ("hcblasSetMatrixAsync", "hcblasGetMatrixAsync"):
+            f = getattr(L, n)
+            f.argtypes = [vp, ci, ci, ci, vp, ci, vp, ci, vp]
             f.restype = st
         for p in "SDCZH":
             f = getattr(L, f"hcblas{p}gemm")
@@ -271,6 +275,19 @@ def hcblasSetMatrix(handle, rows, cols, elem_size, host_ptr, lda, dev_ptr, ldb):
 
 def hcblasGetMatrix(handle, rows, cols, elem_size, dev_ptr, lda, host_ptr, ldb):
     return lib().hcblasGetMatrix(handle, rows, cols, elem_size, dev_ptr, lda, host_ptr, ldb)
+
+
+def hcblasSetMatrixAsync(handle, rows, cols, elem_size, host_ptr, lda, dev_ptr, ldb, stream):
+    """hcblasSetMatrix enqueued on `stream` (a cudaStream_t as int; 0 = the
+    handle's stream) without waiting; host memory should be pinned."""
+    return lib().hcblasSetMatrixAsync(handle, rows, cols, elem_size, host_ptr, lda, dev_ptr, ldb,
+                                      stream)
+
+
+def hcblasGetMatrixAsync(handle, rows, cols, elem_size, dev_ptr, lda, host_ptr, ldb, stream):
+    """hcblasGetMatrix enqueued on `stream` without waiting."""
+    return lib().hcblasGetMatrixAsync(handle, rows, cols, elem_size, dev_ptr, lda, host_ptr, ldb,
+                                      stream)
 
 
 class DeviceArray:

@@ -285,16 +285,19 @@ extern "C" hcblasStatus_t hcblasSetStream(hcblasHandle_t handle, void *stream) {
 namespace {
 
 /* 2-D copy of `cols` columns of `rows` elements, then wait on the stream. */
+/* one pitched copy on `stream` (the handle's stream when null); waits for it
+ * unless `async` */
 hcblasStatus_t copy2d(hcblasHandle_t h, const void *src, size_t spitch, void *dst,
-                      size_t dpitch, size_t width, size_t height) {
+                      size_t dpitch, size_t width, size_t height, void *stream = nullptr,
+                      bool async = false) {
   DeviceGuard g(h->currentAcclView.device_id);
-  cudaStream_t s = static_cast<cudaStream_t>(h->currentAcclView.stream);
+  cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : h->currentAcclView.stream);
   cudaError_t e;
   if (spitch == width && dpitch == width)
     e = cudaMemcpyAsync(dst, src, width * height, cudaMemcpyDefault, s);
   else
     e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDefault, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && !async) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return HCBLAS_STATUS_MAPPING_ERROR;
@@ -303,7 +306,8 @@ hcblasStatus_t copy2d(hcblasHandle_t h, const void *src, size_t spitch, void *ds
 }
 
 hcblasStatus_t copy_matrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
-                           const void *A, int lda, void *B, int ldb) {
+                           const void *A, int lda, void *B, int ldb, void *stream = nullptr,
+                           bool async = false) {
   if (handle == nullptr || !handle->initialized) return HCBLAS_STATUS_NOT_INITIALIZED;
   if (rows < 0 || cols < 0 || lda <= 0 || ldb <= 0 || elemSize <= 0)
     return HCBLAS_STATUS_INVALID_VALUE;
@@ -312,10 +316,10 @@ hcblasStatus_t copy_matrix(hcblasHandle_t handle, int rows, int cols, int elemSi
   const size_t es = (size_t)elemSize;
   if (lda >= rows && ldb >= rows)
     return copy2d(handle, A, (size_t)lda * es, B, (size_t)ldb * es, (size_t)rows * es,
-                  (size_t)cols);
+                  (size_t)cols, stream, async);
   /* the reference's behaviour: rows*cols contiguous elements */
   const size_t w = (size_t)rows * (size_t)cols * es;
-  return copy2d(handle, A, w, B, w, w, 1);
+  return copy2d(handle, A, w, B, w, w, 1, stream, async);
 }
 
 hcblasStatus_t copy_vector(hcblasHandle_t handle, int n, int elemSize, const void *x, int incx,
@@ -348,6 +352,18 @@ extern "C" hcblasStatus_t hcblasSetMatrix(hcblasHandle_t handle, int rows, int c
 extern "C" hcblasStatus_t hcblasGetMatrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
                                           const void *A, int lda, void *B, int ldb) {
   return copy_matrix(handle, rows, cols, elemSize, A, lda, B, ldb);
+}
+
+extern "C" hcblasStatus_t hcblasSetMatrixAsync(hcblasHandle_t handle, int rows, int cols,
+                                               int elemSize, const void *A, int lda, void *B,
+                                               int ldb, void *stream) {
+  return copy_matrix(handle, rows, cols, elemSize, A, lda, B, ldb, stream, true);
+}
+
+extern "C" hcblasStatus_t hcblasGetMatrixAsync(hcblasHandle_t handle, int rows, int cols,
+                                               int elemSize, const void *A, int lda, void *B,
+                                               int ldb, void *stream) {
+  return copy_matrix(handle, rows, cols, elemSize, A, lda, B, ldb, stream, true);
 }
 
 extern "C" hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param) {

@@ -125,6 +125,17 @@ hcblasStatus_t hcblasSetMatrix(hcblasHandle_t handle, int rows, int cols, int el
 hcblasStatus_t hcblasGetMatrix(hcblasHandle_t handle, int rows, int cols, int elemSize,
                                const void *A, int lda, void *B, int ldb);
 
+/* Extension with no counterpart in the reference (cuBLAS-style): the same
+ * copies enqueued on `stream` (the handle's stream when null) without
+ * waiting, so that a caller streaming many GEMMs overlaps the next inputs'
+ * host->device copy and the last result's device->host copy with the
+ * current GEMM.  Host memory must be pinned for the copy to be asynchronous;
+ * ordering against the GEMM's stream is the caller's (events). */
+hcblasStatus_t hcblasSetMatrixAsync(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                                    const void *A, int lda, void *B, int ldb, void *stream);
+hcblasStatus_t hcblasGetMatrixAsync(hcblasHandle_t handle, int rows, int cols, int elemSize,
+                                    const void *A, int lda, void *B, int ldb, void *stream);
+
 /* ------------------------------------------------------------------ GEMM -- */
 
 /* Reference: lib/include/hcblas.h:662-665, lib/src/hcblas.cpp:1304-1327. */

@@ -395,3 +395,30 @@ def test_set_get_matrix_strided(handle):
     assert hb.hcblasSetMatrix(handle, -1, cols, 8, A.ctypes.data, lda, dB, ldb) == \
         hb.HCBLAS_STATUS_INVALID_VALUE
     hb.am_free(dB)
+
+
+def test_set_get_matrix_async_on_a_stream(handle):
+    """The asynchronous copies enqueue on the given stream (pinned host
+    memory) and complete once that stream is synchronised; bad sizes are
+    rejected before anything is enqueued."""
+    import torch
+    rng = np.random.default_rng(4)
+    rows, cols, lda, ldb = 300, 70, 301, 304
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    A = pin(lda * cols)
+    A[:] = rng.standard_normal(lda * cols)
+    out = pin(lda * cols)
+    out[:] = -1.0
+    dB = hb.am_alloc(8 * ldb * cols)
+    s = torch.cuda.Stream()
+    assert hb.hcblasSetMatrixAsync(handle, rows, cols, 8, A.ctypes.data, lda, dB, ldb,
+                                   s.cuda_stream) == 0
+    assert hb.hcblasGetMatrixAsync(handle, rows, cols, 8, dB, ldb, out.ctypes.data, lda,
+                                   s.cuda_stream) == 0
+    s.synchronize()
+    for j in range(cols):
+        assert np.array_equal(out[j * lda:j * lda + rows], A[j * lda:j * lda + rows])
+        assert np.all(out[j * lda + rows:(j + 1) * lda] == -1.0)
+    assert hb.hcblasSetMatrixAsync(handle, rows, -1, 8, A.ctypes.data, lda, dB, ldb,
+                                   s.cuda_stream) == hb.HCBLAS_STATUS_INVALID_VALUE
+    hb.am_free(dB)
