@@ -150,7 +150,9 @@ __device__ __forceinline__ float load_out(const __half *p) { return __half2float
 struct OutStage {
   uint8_t *box;
   uint64_t *bar;
-  uint32_t phase;
+  uint32_t phase; /* bit x: parity of box x's next C load */
+  uint32_t pend;  /* bit x: a C load into box x is in flight */
+  int pre;        /* the current tile's first two C boxes are already loading */
 };
 
 /* f32 accumulator -> alpha*acc + beta*C in OutT (float or half) */
@@ -172,6 +174,26 @@ template <typename OutT> struct EpiAlphaBeta {
    * >= m and columns >= n.  A box is rewritten only after the store issued
    * from it has read it.  load_v(r) fills r with the group's 32 f32 values
    * (bit patterns); it may start an asynchronous fetch that wait_v() ends. */
+  /* Start the C loads of a tile's first two 32-column groups (beta != 0),
+   * before the tile's accumulator is ready, so that they overlap its MMAs. */
+  template <int BN>
+  static __device__ __forceinline__ void prefetch_c(const TcParams &p, int m0, int n0,
+                                                    OutStage &os) {
+    if (!os.box || !p.out_tma || !p.beta_nonzero || os.pre) return;
+    if ((threadIdx.x & 31) == 0) {
+      bulk_wait_read<0>(); /* the previous tile's stores have read both boxes */
+#pragma unroll
+      for (int x = 0; x < 2; ++x)
+        if (x * 32 < BN) {
+          mbar_expect_tx(&os.bar[x], OUT_BOX_BYTES);
+          tma_load_2d(os.box + x * OUT_BOX_BYTES, &p.tc, &os.bar[x], m0, n0 + 32 * x);
+        }
+    }
+    os.pend |= BN > 32 ? 3u : 1u;
+    os.pre = 1;
+    __syncwarp();
+  }
+
   template <int BN, class LoadV, class WaitV>
   static __device__ __forceinline__ void stage_group(const TcParams &p, int c, int m0, int n0,
                                                      OutStage &os, LoadV &&load_v,
@@ -182,27 +204,29 @@ template <typename OutT> struct EpiAlphaBeta {
     OutT *box = reinterpret_cast<OutT *>(os.box + b * OUT_BOX_BYTES);
     uint32_t r[32];
     load_v(r);
+    const bool load_first = ld_c && c == 0 && !os.pre;
+    const bool load_next = ld_c && c + 32 < BN && !(os.pre && c == 0);
     if (lane == 0) {
-      if (!ld_c) {
-        bulk_wait_read<1>(); /* the store from this box two groups ago */
-      } else {
-        if (c == 0) { /* first group of the tile: fetch its own C box */
-          bulk_wait_read<0>();
-          mbar_expect_tx(&os.bar[0], OUT_BOX_BYTES);
-          tma_load_2d(os.box, &p.tc, &os.bar[0], m0, n0);
-        }
-        if (c + 32 < BN) { /* prefetch the next group's C into the other box */
-          bulk_wait_read<0>();
-          mbar_expect_tx(&os.bar[b ^ 1], OUT_BOX_BYTES);
-          tma_load_2d(os.box + (b ^ 1) * OUT_BOX_BYTES, &p.tc, &os.bar[b ^ 1], m0, n0 + c + 32);
-        }
+      if (!ld_c) bulk_wait_read<1>(); /* the store from this box two groups ago */
+      if (load_first) { /* the tile's first group was not prefetched */
+        bulk_wait_read<0>();
+        mbar_expect_tx(&os.bar[0], OUT_BOX_BYTES);
+        tma_load_2d(os.box, &p.tc, &os.bar[0], m0, n0);
+      }
+      if (load_next) { /* the next group's C into the other box */
+        bulk_wait_read<0>(); /* that box's store has read it */
+        mbar_expect_tx(&os.bar[b ^ 1], OUT_BOX_BYTES);
+        tma_load_2d(os.box + (b ^ 1) * OUT_BOX_BYTES, &p.tc, &os.bar[b ^ 1], m0, n0 + c + 32);
       }
     }
+    if (load_first) os.pend |= 1u;
+    if (load_next) os.pend |= 1u << (b ^ 1);
     __syncwarp();
     wait_v();
     if (ld_c) {
       mbar_wait(&os.bar[b], (os.phase >> b) & 1u, p.err, ERR_TIMEOUT_EPILOGUE);
       os.phase ^= 1u << b;
+      os.pend &= ~(1u << b);
 #pragma unroll
       for (int j = 0; j < 32; ++j)
         store_out(box + j * 32 + lane,
@@ -228,6 +252,7 @@ template <typename OutT> struct EpiAlphaBeta {
       stage_group<BN>(
           p, c, m0, n0, os, [&](uint32_t(&r)[32]) { tmem_ld_32x32b_x32(tbase + c, r); },
           [] { tmem_ld_wait(); });
+    os.pre = 0;
   }
 
   template <int BN, int NACC>
@@ -313,6 +338,7 @@ template <typename OutT> struct EpiAlphaBeta {
               for (int j = 0; j < 32; ++j) r[j] = __float_as_uint(acc[c + j]);
             },
             [] {});
+      os.pre = 0;
       return;
     }
     if (m >= p.m) return;
@@ -816,7 +842,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     int ci = 0;
     bool ok = true;
     OutStage ostage{Cfg::OUT_BYTES ? smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES : nullptr,
-                    obar + 2 * q, 0u};
+                    obar + 2 * q, 0u, 0u, 0};
     static_assert(!EPI::INPLACE || Cfg::OUT_BYTES > 0, "the modular epilogue stores by TMA");
     /* TMEM buffer released to the leader's MMA thread */
     auto release = [&](int b) {
@@ -861,6 +887,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       const TileMN tc_ = tile_mn(tt, p.tiles_m, p.tiles_n);
       const int tm = tc_.m, tn = tc_.n;
       const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
+      if constexpr (Cfg::OUT_BYTES > 0) EPI::template prefetch_c<BN>(p, m - lane, tn * BN, ostage);
       if constexpr (PROMOTE_KB == 0) {
         const int b = ci % NBUF;
         const uint32_t tph = (ci / NBUF) & 1;
@@ -896,8 +923,19 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       }
     }
     }
-    if constexpr (Cfg::OUT_BYTES > 0)
-      if (lane == 0) bulk_wait_all(); /* this warp's last tensor stores have landed */
+    if constexpr (Cfg::OUT_BYTES > 0) {
+      if (lane == 0) {
+        /* C loads still in flight (only after a failed wait): give them a
+         * bounded time to land before the CTA's shared memory is released */
+#pragma unroll
+        for (int x = 0; x < 2; ++x)
+          if ((ostage.pend >> x) & 1u)
+            for (int it = 0; it < (1 << 22) && !mbar_try_wait(&ostage.bar[x], (ostage.phase >> x) & 1u);
+                 ++it) {
+            }
+        bulk_wait_all(); /* this warp's last tensor stores have landed */
+      }
+    }
   }
 
   tc_fence_before();

@@ -25,22 +25,22 @@ def _dev(h, x):
     return hb.DeviceArray(h, x)
 
 
-def _real(h, dtype, op_a, op_b, m, n, k, mode=0, param=0, seed=0):
+def _real(h, dtype, op_a, op_b, m, n, k, mode=0, param=0, seed=0, beta=0.0):
     rng = np.random.default_rng(seed)
     ar, ac = (m, k) if op_a == N_ else (k, m)
     br, bc = (k, n) if op_b == N_ else (n, k)
     A = rng.standard_normal(ar * ac).astype(dtype)
     B = rng.standard_normal(br * bc).astype(dtype)
-    C = np.zeros(m * n, dtype=dtype)
+    C = (rng.standard_normal(m * n) if beta else np.zeros(m * n)).astype(dtype)
     dA, dB, dC = _dev(h, A), _dev(h, B), _dev(h, C)
     L = hb.lib()
     f = {np.float16: L.hcblasHgemm, np.float32: L.hcblasSgemm, np.float64: L.hcblasDgemm}[dtype]
-    one, zero = hb.scalar_bytes(np.dtype(dtype), 1.0), hb.scalar_bytes(np.dtype(dtype), 0.0)
+    one, bb = hb.scalar_bytes(np.dtype(dtype), 1.0), hb.scalar_bytes(np.dtype(dtype), beta)
     hb.hcblasSetMathMode(h, mode, param)
 
     def call():
         assert f(h, op_a, op_b, m, n, k, one.ctypes.data, dA.ptr, ar, dB.ptr, br,
-                 zero.ctypes.data, dC.ptr, m) == 0
+                 bb.ctypes.data, dC.ptr, m) == 0
     return call, (dA, dB, dC)
 
 
@@ -130,6 +130,11 @@ def _ger(h, dtype, m, n, seed=7):
 
 CASES = {
     "hgemm_nt_8192": lambda h: _real(h, np.float16, N_, T_, 8192, 8192, 8192),
+    "hgemm_nt_8192_beta05": lambda h: _real(h, np.float16, N_, T_, 8192, 8192, 8192, beta=0.5),
+    "sgemm_split6_tn_8192x8192x256_beta1": lambda h: _real(h, np.float32, T_, N_, 8192, 8192, 256,
+                                                           1, 6, beta=1.0),
+    "sgemm_plain_tn_8192x8192x256_beta1": lambda h: _real(h, np.float32, T_, N_, 8192, 8192, 256,
+                                                          beta=1.0),
     "sgemm_plain_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096),
     "sgemm_split6_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096, 1, 6),
     "sgemm_split3_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096, 1, 3),
