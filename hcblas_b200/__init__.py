@@ -57,13 +57,13 @@ EXPORTED = (
     "hcblasGetDeviceError", "hcblasSetTuningParam",
     "hcblasSetProfiling", "hcblasGetProfile", "hcblas_am_alloc", "hcblas_am_free",
     "hcblas_am_copy", "hcblas_view_wait", "hcblas_device_count", "hcblas_current_device",
-    "hcblasHgemmGrouped", "hcblasSgemv", "hcblasDgemv", "hcblasSgemvBatched",
+    "hcblasHgemmGrouped", "hcblasSgemmGrouped", "hcblasSgemv", "hcblasDgemv", "hcblasSgemvBatched",
     "hcblasDgemvBatched", "hcblasSger", "hcblasDger", "hcblasSgerBatched", "hcblasDgerBatched",
 )
 
 
 class GemmProblem(ctypes.Structure):
-    """One problem of hcblasHgemmGrouped (hcblasGemmProblem in hcblas.h)."""
+    """One problem of hcblasHgemmGrouped / hcblasSgemmGrouped (hcblasGemmProblem)."""
     _fields_ = [("transa", ctypes.c_ushort), ("transb", ctypes.c_ushort),
                 ("m", ctypes.c_int), ("n", ctypes.c_int), ("k", ctypes.c_int),
                 ("A", ctypes.c_void_p), ("lda", ctypes.c_int),
@@ -183,6 +183,8 @@ def lib():
         L.hcblas_current_device.restype = ci
         L.hcblasHgemmGrouped.argtypes = [vp, ci, vp, vp, vp]
         L.hcblasHgemmGrouped.restype = st
+        L.hcblasSgemmGrouped.argtypes = [vp, ci, vp, vp, vp]
+        L.hcblasSgemmGrouped.restype = st
         for p in "SD":
             f = getattr(L, f"hcblas{p}gemv")
             f.argtypes = [vp, op, ci, ci, vp, vp, ci, vp, ci, vp, vp, ci]
@@ -416,6 +418,15 @@ def hgemm_grouped(handle, problems, alpha: float, beta: float) -> int:
     a = np.array([alpha], dtype=np.float16).view(np.uint16)
     b = np.array([beta], dtype=np.float16).view(np.uint16)
     return lib().hcblasHgemmGrouped(handle, len(problems), ctypes.cast(arr, ctypes.c_void_p),
+                                    a.ctypes.data, b.ctypes.data)
+
+
+def sgemm_grouped(handle, problems, alpha: float, beta: float) -> int:
+    """hcblasSgemmGrouped (f32 problems on the split-BF16 tensor-core path)."""
+    arr = (GemmProblem * len(problems))(*problems)
+    a = np.array([alpha], dtype=np.float32)
+    b = np.array([beta], dtype=np.float32)
+    return lib().hcblasSgemmGrouped(handle, len(problems), ctypes.cast(arr, ctypes.c_void_p),
                                     a.ctypes.data, b.ctypes.data)
 
 

@@ -57,6 +57,10 @@ int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int n
 int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,
                   const hcblasGemmProblem *probs, float alpha, float beta);
 
+/* Grouped FP32 GEMM on the split-BF16 tensor-core path (terms 3 or 6). */
+int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, int count,
+                        const hcblasGemmProblem *probs, float alpha, float beta, int terms);
+
 }  // namespace hcblas_b200
 
 #endif /* HCBLAS_B200_DISPATCH_H_ */

@@ -237,6 +237,200 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
   return HCBK_OK;
 }
 
+/* Grouped FP32 GEMM, split-BF16: the plan holds every problem's bf16 plane
+ * layout (one device allocation), the pack jobs that fill it and the GEMM
+ * table whose 3-D maps read it; each call packs the current operands (one
+ * launch) and runs the grouped tensor-core kernel (one launch). */
+int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, int count,
+                        const hcblasGemmProblem *probs, float alpha, float beta, int terms) {
+  if (alpha == 0.0f) { /* C_i := beta*C_i, A and B not referenced (CBLAS) */
+    for (int i = 0; i < count; ++i) {
+      const Canon c = canonical(probs[i], order);
+      hcbk_gemm_args a;
+      std::memset(&a, 0, sizeof(a));
+      a.dtype = HCBK_S;
+      a.m = c.m;
+      a.n = c.n;
+      a.k = c.k;
+      a.c = c.c;
+      a.ldc = c.ldc;
+      a.batch = 1;
+      a.beta_re = beta;
+      int rc = timed_launch(st, stream, "scale", [&] { return hcbk_scale_c(&a, stream); });
+      if (rc) return rc;
+    }
+    st->last_path = "scale";
+    return HCBK_OK;
+  }
+  const int nplanes = terms == 6 ? 3 : 2;
+  HcblasGroupedPlan &gp = st->grouped_split;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::vector<unsigned char> key(sizeof(hcblasGemmProblem) * (size_t)count + 3);
+  std::memcpy(key.data(), probs, sizeof(hcblasGemmProblem) * (size_t)count);
+  key[key.size() - 3] = static_cast<unsigned char>(order);
+  key[key.size() - 2] = static_cast<unsigned char>(dev);
+  key[key.size() - 1] = static_cast<unsigned char>(terms);
+  const bool reuse = gp.table && gp.planes && gp.table_device == dev && key == gp.key;
+
+  if (!reuse) {
+    if (!st->graph_cache.empty()) {
+      cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+      clear_graph_cache(st);
+    }
+    gp.key.clear();
+    /* plane layout: per problem, A planes then B planes, each plane
+     * rows x kp bf16 (kp = K rounded up to 8: 16-byte rows), problems
+     * 1 KiB aligned */
+    std::vector<Canon> cn((size_t)count);
+    std::vector<size_t> a_off((size_t)count), b_off((size_t)count);
+    size_t total_planes = 0;
+    for (int i = 0; i < count; ++i) {
+      cn[i] = canonical(probs[i], order);
+      const int64_t kp = (cn[i].k + 7) & ~int64_t(7);
+      a_off[i] = total_planes;
+      total_planes += (size_t)nplanes * cn[i].m * kp * 2;
+      b_off[i] = total_planes;
+      total_planes += (size_t)nplanes * cn[i].n * kp * 2;
+      total_planes = (total_planes + 1023) & ~size_t(1023);
+    }
+    if (gp.planes && (gp.planes_bytes < total_planes || gp.table_device != dev)) {
+      cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+      DeviceGuard g(gp.table_device);
+      cudaFree(gp.planes);
+      gp.planes = nullptr;
+      gp.planes_bytes = 0;
+    }
+    if (!gp.planes) {
+      if (cudaMalloc(&gp.planes, total_planes) != cudaSuccess) {
+        cudaGetLastError();
+        gp.planes = nullptr;
+        return HCBK_ERR_NOMEM;
+      }
+      gp.planes_bytes = total_planes;
+    }
+    char *pl = static_cast<char *>(gp.planes);
+    std::vector<hcbk_grouped_entry> ent((size_t)count);
+    std::vector<hcbk_gpack_job> jobs((size_t)count * 2);
+    for (int i = 0; i < count; ++i) {
+      const Canon &c = cn[i];
+      const int64_t kp = (c.k + 7) & ~int64_t(7);
+      if (c.m > 0x7fffffff || c.n > 0x7fffffff || c.k > 0x7fffffff) return HCBK_ERR_ARGS;
+      hcbk_grouped_entry &e = ent[i];
+      std::memset(&e, 0, sizeof(e));
+      int rc = hcbk_encode_tma_3d_planes(e.map_a, 1, pl + a_off[i], c.k, c.m, nplanes, kp,
+                                         (uint64_t)c.m * kp * 2, 128);
+      if (!rc)
+        rc = hcbk_encode_tma_3d_planes(e.map_b, 1, pl + b_off[i], c.k, c.n, nplanes, kp,
+                                       (uint64_t)c.n * kp * 2, 128);
+      if (rc) return rc;
+      e.c = c.c;
+      e.ldc = c.ldc;
+      e.m = (int32_t)c.m;
+      e.n = (int32_t)c.n;
+      e.k = (int32_t)c.k;
+      e.tiles_m = (int32_t)((c.m + 127) / 128);
+      /* op(A) rows m: column-major A is M-contiguous for N, K-contiguous for T;
+       * op(B) rows n: B is K-contiguous for N, N-contiguous for T */
+      for (int side = 0; side < 2; ++side) {
+        hcbk_gpack_job &j = jobs[2 * i + side];
+        std::memset(&j, 0, sizeof(j));
+        j.src = static_cast<const float *>(side ? c.b : c.a);
+        j.ld = side ? c.ldb : c.lda;
+        j.k_contig = side ? (c.op_b == HCBK_OP_N) : (c.op_a != HCBK_OP_N);
+        j.rows = (int32_t)(side ? c.n : c.m);
+        j.kdim = (int32_t)c.k;
+        j.ld_dst = (int32_t)kp;
+        j.planes = pl + (side ? b_off[i] : a_off[i]);
+        j.plane_stride = (int64_t)j.rows * kp;
+        j.tiles_r = (j.rows + 31) / 32;
+      }
+    }
+    std::vector<int> order_idx((size_t)count);
+    for (int i = 0; i < count; ++i) order_idx[i] = i;
+    auto work = [&](int i) {
+      const hcbk_grouped_entry &e = ent[i];
+      return (int64_t)e.tiles_m * ((e.n + 127) / 128) * ((e.k + 63) / 64);
+    };
+    std::stable_sort(order_idx.begin(), order_idx.end(),
+                     [&](int x, int y) { return work(x) > work(y); });
+    /* table: entries | tile prefix | pack jobs | pack tile prefix */
+    const size_t ent_bytes = sizeof(hcbk_grouped_entry) * (size_t)count;
+    const size_t ts_off = (ent_bytes + 255) & ~size_t(255);
+    const size_t job_off = (ts_off + sizeof(int32_t) * ((size_t)count + 1) + 255) & ~size_t(255);
+    const size_t njobs = (size_t)count * 2;
+    const size_t jts_off = (job_off + sizeof(hcbk_gpack_job) * njobs + 255) & ~size_t(255);
+    const size_t bytes = jts_off + sizeof(int32_t) * (njobs + 1);
+    if (!ensure_table(gp, bytes, stream) || !ensure_staging(gp, bytes)) return HCBK_ERR_NOMEM;
+    unsigned char *stg = static_cast<unsigned char *>(gp.staging);
+    auto *dst = reinterpret_cast<hcbk_grouped_entry *>(stg);
+    auto *ts = reinterpret_cast<int32_t *>(stg + ts_off);
+    auto *jdst = reinterpret_cast<hcbk_gpack_job *>(stg + job_off);
+    auto *jts = reinterpret_cast<int32_t *>(stg + jts_off);
+    int64_t total = 0;
+    for (int x = 0; x < count; ++x) {
+      const hcbk_grouped_entry &e = ent[order_idx[x]];
+      std::memcpy(&dst[x], &e, sizeof(e));
+      ts[x] = (int32_t)total;
+      total += (int64_t)e.tiles_m * ((e.n + 127) / 128);
+      if (total > 0x7fffffff) return HCBK_ERR_ARGS;
+    }
+    ts[count] = (int32_t)total;
+    int64_t ptotal = 0;
+    for (size_t x = 0; x < njobs; ++x) {
+      jdst[x] = jobs[x];
+      jts[x] = (int32_t)ptotal;
+      ptotal += (int64_t)jobs[x].tiles_r * ((jobs[x].kdim + 31) / 32);
+      if (ptotal > 0x7fffffff) return HCBK_ERR_ARGS;
+    }
+    jts[njobs] = (int32_t)ptotal;
+    if (cudaMemcpyAsync(gp.table, stg, bytes, cudaMemcpyHostToDevice,
+                        static_cast<cudaStream_t>(stream)) != cudaSuccess)
+      return HCBK_ERR_LAUNCH;
+    if (!gp.upload_done &&
+        cudaEventCreateWithFlags(reinterpret_cast<cudaEvent_t *>(&gp.upload_done),
+                                 cudaEventDisableTiming) != cudaSuccess) {
+      gp.upload_done = nullptr;
+      cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    } else {
+      cudaEventRecord(static_cast<cudaEvent_t>(gp.upload_done),
+                      static_cast<cudaStream_t>(stream));
+    }
+    gp.count = count;
+    gp.total_tiles = (int)total;
+    gp.tile_start_offset = ts_off;
+    gp.pack_count = (int)njobs;
+    gp.pack_tiles = (int)ptotal;
+    gp.pack_offset = job_off;
+    gp.pack_ts_offset = jts_off;
+    gp.fallback.clear();
+    gp.key = key;
+  }
+
+  int *err = device_error_flag(st);
+  if (!err) return HCBK_ERR_NOMEM;
+  char *tb = static_cast<char *>(gp.table);
+  int rc = timed_launch(st, stream, "pack.split_bf16.grouped", [&] {
+    return hcbk_grouped_pack(reinterpret_cast<const hcbk_gpack_job *>(tb + gp.pack_offset),
+                             reinterpret_cast<const int32_t *>(tb + gp.pack_ts_offset),
+                             gp.pack_count, gp.pack_tiles, nplanes, stream);
+  });
+  if (rc) return rc;
+  hcbk_grouped_args g;
+  g.table = reinterpret_cast<const hcbk_grouped_entry *>(tb);
+  g.tile_start = reinterpret_cast<const int32_t *>(tb + gp.tile_start_offset);
+  g.count = gp.count;
+  g.total_tiles = gp.total_tiles;
+  g.alpha = alpha;
+  g.beta = beta;
+  const char *path = terms == 6 ? "tc.s.grouped_split_bf16x6" : "tc.s.grouped_split_bf16x3";
+  rc = timed_launch(st, stream, path,
+                    [&] { return hcbk_sgemm_grouped_split_tc(&g, terms, err, stream); });
+  if (rc) return rc;
+  st->last_path = path;
+  return HCBK_OK;
+}
+
 }  // namespace hcblas_b200
 
 extern "C" hcblasStatus_t hcblasHgemmGrouped(hcblasHandle_t handle, int count,
@@ -263,6 +457,37 @@ extern "C" hcblasStatus_t hcblasHgemmGrouped(hcblasHandle_t handle, int count,
                          problems, a, b);
   if (log_enabled())
     std::fprintf(stderr, "[hcblas] grouped count=%d path=%s rc=%d\n", count,
+                 handle->impl->last_path, rc);
+  return rc == HCBK_OK ? HCBLAS_STATUS_SUCCESS : HCBLAS_STATUS_EXECUTION_FAILED;
+}
+
+extern "C" hcblasStatus_t hcblasSgemmGrouped(hcblasHandle_t handle, int count,
+                                             const hcblasGemmProblem *problems,
+                                             const float *alpha, const float *beta) {
+  using namespace hcblas_b200;
+  if (handle == nullptr || !handle->initialized || handle->impl == nullptr)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (count < 0 || (count > 0 && problems == nullptr) || alpha == nullptr || beta == nullptr)
+    return HCBLAS_STATUS_INVALID_VALUE;
+  for (int i = 0; i < count; ++i)
+    if (problems[i].m < 0 || problems[i].n < 0 || problems[i].k < 0)
+      return HCBLAS_STATUS_INVALID_VALUE;
+  for (int i = 0; i < count; ++i) {
+    const hcblasGemmProblem &p = problems[i];
+    if (p.m == 0 || p.n == 0 || p.k == 0 || p.A == nullptr || p.B == nullptr || p.C == nullptr)
+      return HCBLAS_STATUS_EXECUTION_FAILED;
+  }
+  if (count == 0) return HCBLAS_STATUS_SUCCESS;
+  DeviceGuard dev(handle->currentAcclView.device_id);
+  if (!dev.ok()) return HCBLAS_STATUS_EXECUTION_FAILED;
+  /* 3 products when the handle asks for the 3-term split, else 6 (error no
+   * worse than plain FP32) */
+  const HcblasB200State *st = handle->impl;
+  const int terms = (st->math_mode == HCBLAS_MATH_SPLIT_BF16 && st->math_param == 3) ? 3 : 6;
+  int rc = grouped_sgemm_split(handle->impl, handle->currentAcclView.stream, handle->Order, count,
+                               problems, *alpha, *beta, terms);
+  if (log_enabled())
+    std::fprintf(stderr, "[hcblas] grouped sgemm count=%d path=%s rc=%d\n", count,
                  handle->impl->last_path, rc);
   return rc == HCBK_OK ? HCBLAS_STATUS_SUCCESS : HCBLAS_STATUS_EXECUTION_FAILED;
 }

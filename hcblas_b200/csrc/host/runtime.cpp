@@ -210,17 +210,20 @@ Hcblaslibrary::~Hcblaslibrary() {
     }
     cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
     hcblas_b200::clear_graph_cache(impl);
-    HcblasGroupedPlan &gp = impl->grouped;
-    if (gp.upload_done) {
-      cudaEventSynchronize(static_cast<cudaEvent_t>(gp.upload_done));
-      cudaEventDestroy(static_cast<cudaEvent_t>(gp.upload_done));
+    for (HcblasGroupedPlan *pp : {&impl->grouped, &impl->grouped_split}) {
+      HcblasGroupedPlan &gp = *pp;
+      if (gp.upload_done) {
+        cudaEventSynchronize(static_cast<cudaEvent_t>(gp.upload_done));
+        cudaEventDestroy(static_cast<cudaEvent_t>(gp.upload_done));
+      }
+      if (gp.table || gp.planes) {
+        DeviceGuard g(gp.table_device);
+        cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
+        if (gp.table) cudaFree(gp.table);
+        if (gp.planes) cudaFree(gp.planes);
+      }
+      if (gp.staging) cudaFreeHost(gp.staging);
     }
-    if (gp.table) {
-      DeviceGuard g(gp.table_device);
-      cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
-      cudaFree(gp.table);
-    }
-    if (gp.staging) cudaFreeHost(gp.staging);
     delete impl;
     impl = nullptr;
   }

@@ -34,6 +34,14 @@ struct HcblasGroupedPlan {
   int total_tiles = 0;
   size_t tile_start_offset = 0;
   std::vector<int> fallback; /* problems the table cannot hold (TMA alignment) */
+  /* split-BF16 SGEMM plans only: the bf16 planes of every problem (device),
+   * and the pack jobs' place in the table */
+  void *planes = nullptr;
+  size_t planes_bytes = 0;
+  int pack_count = 0;
+  int pack_tiles = 0;
+  size_t pack_offset = 0;
+  size_t pack_ts_offset = 0;
 };
 
 /* One captured call sequence (hcblasSetTuningParam "graphs"): the key is the
@@ -65,6 +73,7 @@ struct HcblasB200State {
   std::vector<HcblasProfRec> prof;
   std::vector<void *> event_pool;
   HcblasGroupedPlan grouped;
+  HcblasGroupedPlan grouped_split; /* hcblasSgemmGrouped (split-BF16) */
   /* CUDA-graph replay of repeated identical calls (off by default) */
   int graphs = 0;
   /* time candidate tile configurations per size bucket (off by default) */

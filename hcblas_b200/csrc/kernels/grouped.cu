@@ -28,6 +28,7 @@
 #include <string.h>
 
 #include "hcbk.h"
+#include "split_bf16.cuh"
 #include "tc_common.cuh"
 
 namespace hcbk {
@@ -248,6 +249,275 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
   }
 }
 
+/* ------------------------------------------------------------------------
+ * Grouped split-BF16 SGEMM.  The host splits every problem's op(A) and op(B)
+ * into K-major bf16 planes (grouped_pack_kernel, one launch for all
+ * problems); each table entry then holds 3-D plane maps {K, rows, plane}.
+ * The tile walk, roles and bounded waits are those of the HGEMM kernel
+ * above; per 64-K slab the MMA warp issues the recipe's plane products into
+ * NACC accumulators (RecipeBf16x3 / RecipeBf16x6), and the epilogue promotes
+ * every slab's TMEM sums into f32 registers -- the tensor core's own f32
+ * accumulation then never spans more than 64 K, which keeps the result's
+ * error at or below plain FP32's -- and finally writes
+ * alpha * acc + beta * C in f32.
+ * ---------------------------------------------------------------------- */
+
+template <class R, int ST>
+struct SplitCfg {
+  static constexpr int STAGES = ST;
+  static constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128;
+  static constexpr uint32_t STAGE_BYTES = R::NA * A_BYTES + R::NB * B_BYTES;
+  static constexpr uint32_t SMEM_BYTES = ST * STAGE_BYTES + 256 + 1024;
+  static constexpr uint32_t ACC_COLS = R::NACC * BN;
+  static constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;
+  static_assert(SMEM_BYTES <= 232448, "shared memory");
+  static_assert(TMEM_COLS <= 512, "TMEM");
+};
+using SplitCfg3 = SplitCfg<RecipeBf16x3, 3>;
+using SplitCfg6 = SplitCfg<RecipeBf16x6, 2>;
+
+template <class R, class Cfg>
+__global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_constant__ Params p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  constexpr int S = Cfg::STAGES;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + S * Cfg::STAGE_BYTES);
+  uint64_t *empty = full + S;
+  uint64_t *tfull = empty + S;
+  uint64_t *tempty = tfull + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_fence_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    /* ------------------------------------------------ TMA producer -- */
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
+        const TileRef r = tile_ref(p, t);
+        const CUtensorMap *ma = reinterpret_cast<const CUtensorMap *>(r.e->map_a);
+        const CUtensorMap *mb = reinterpret_cast<const CUtensorMap *>(r.e->map_b);
+        const int kblocks = (__ldg(&r.e->k) + BK - 1) / BK;
+        for (int kb = 0; kb < kblocks; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
+          uint8_t *st = smem + s * Cfg::STAGE_BYTES;
+#pragma unroll
+          for (int a = 0; a < R::NA; ++a)
+            tma_load_3d(st + a * Cfg::A_BYTES, ma, &full[s], kb * BK, r.tm * BM, a);
+#pragma unroll
+          for (int b = 0; b < R::NB; ++b)
+            tma_load_3d(st + R::NA * Cfg::A_BYTES + b * Cfg::B_BYTES, mb, &full[s], kb * BK,
+                        r.tn * BN, b);
+          if (++s == S) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    /* ------------------------------------------------ MMA issuer -- */
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc(1, 1, false, false, BM, BN); /* bf16 x bf16 -> f32 */
+      int s = 0;
+      uint32_t ph = 0;
+      int ci = 0; /* 64-K slabs so far: selects the TMEM buffer */
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
+        const TileRef r = tile_ref(p, t);
+        const int kblocks = (__ldg(&r.e->k) + BK - 1) / BK;
+        for (int kb = 0; ok && kb < kblocks; ++kb, ++ci) {
+          const int b = ci & 1;
+          if (!mbar_wait(&tempty[b], ((ci >> 1) & 1) ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          if (!mbar_wait(&full[s], ph, p.err, ERR_TIMEOUT_MMA_FULL)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dbase = tmem_base + b * Cfg::ACC_COLS;
+          const uint32_t sa = smem_u32(smem + s * Cfg::STAGE_BYTES);
+          const uint32_t sb = sa + R::NA * Cfg::A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+            for (int pi = 0; pi < R::NP; ++pi) {
+              const uint64_t ad = smem_desc(sa + R::pa(pi) * Cfg::A_BYTES + kk * 32, 16, 1024, 2);
+              const uint64_t bd = smem_desc(sb + R::pb(pi) * Cfg::B_BYTES + kk * 32, 16, 1024, 2);
+              mma_f16(dbase + R::pacc(pi) * BN, ad, bd, idesc,
+                      (kk > 0 || !R::first(pi)) ? 1u : 0u);
+            }
+          }
+          mma_commit(&empty[s]);
+          mma_commit(&tfull[b]);
+          if (++s == S) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+    }
+  } else {
+    /* ------------------------------------------------ epilogue -- */
+    const int q = warp & 3; /* TMEM lane quadrant */
+    int ci = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
+      const TileRef r = tile_ref(p, t);
+      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n);
+      const int kblocks = (__ldg(&r.e->k) + BK - 1) / BK;
+      float acc[BN];
+#pragma unroll
+      for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+      for (int kb = 0; kb < kblocks; ++kb, ++ci) {
+        const int b = ci & 1;
+        if (!__all_sync(0xffffffffu,
+                        mbar_wait(&tfull[b], (ci >> 1) & 1, p.err, ERR_TIMEOUT_EPILOGUE))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tbase =
+            tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS;
+        /* this slab's products, correction accumulator first, added to acc
+         * with IEEE round-to-nearest */
+#pragma unroll
+        for (int c = 0; c < BN; c += 32) {
+          float part[32];
+#pragma unroll
+          for (int a = R::NACC - 1; a >= 0; --a) {
+            uint32_t v[32];
+            tmem_ld_32x32b_x32(tbase + a * BN + c, v);
+            tmem_ld_wait();
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              part[j] = (a == R::NACC - 1) ? __uint_as_float(v[j]) : part[j] + __uint_as_float(v[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) acc[c + j] += part[j];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[b]);
+      }
+      if (!ok) break;
+      const int m = r.tm * BM + q * 32 + lane;
+      const int n0 = r.tn * BN;
+      if (m < pm) {
+        const long long ldc = __ldg(&r.e->ldc);
+        float *C = static_cast<float *>(r.e->c) + (long long)m + (long long)n0 * ldc;
+#pragma unroll
+        for (int c = 0; c < BN; c += 32) {
+          const int nvalid = pn - (n0 + c);
+          if (nvalid <= 0) break;
+          float *cp = C + (long long)c * ldc;
+          float cv[32];
+          if (p.beta_nonzero) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) cv[j] = (j < nvalid) ? cp[(long long)j * ldc] : 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            if (j < nvalid) {
+              float o = p.alpha * acc[c + j];
+              if (p.beta_nonzero) o = fmaf(p.beta, cv[j], o);
+              cp[(long long)j * ldc] = o;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncwarp();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+  }
+}
+
+/* Split every job's f32 operand into nplanes K-major bf16 planes: one
+ * 32 x 32 tile (rows x K) per iteration, read coalesced along whichever
+ * dimension is contiguous in the source and written along K. */
+__global__ void __launch_bounds__(256) grouped_pack_kernel(const hcbk_gpack_job *jobs,
+                                                           const int32_t *ts, int count,
+                                                           int total, int nplanes) {
+  __shared__ float tile[32][33]; /* [k][r] */
+  const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    const int g = find_problem(ts, count, t);
+    const hcbk_gpack_job *j = jobs + g;
+    const int lt = t - __ldg(ts + g);
+    const int tiles_r = __ldg(&j->tiles_r);
+    const int rows = __ldg(&j->rows), kdim = __ldg(&j->kdim);
+    const int64_t ld = __ldg(&j->ld);
+    const int r0 = (lt % tiles_r) * 32, k0 = (lt / tiles_r) * 32;
+    const float *src = j->src;
+    __syncthreads(); /* the previous tile's reads of `tile` are done */
+    if (__ldg(&j->k_contig)) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = r0 + ty + 8 * i, k = k0 + tx;
+        tile[tx][ty + 8 * i] = (r < rows && k < kdim) ? src[(int64_t)r * ld + k] : 0.f;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = r0 + tx, k = k0 + ty + 8 * i;
+        tile[ty + 8 * i][tx] = (r < rows && k < kdim) ? src[r + (int64_t)k * ld] : 0.f;
+      }
+    }
+    __syncthreads();
+    __nv_bfloat16 *planes = static_cast<__nv_bfloat16 *>(j->planes);
+    const int64_t pstride = __ldg(&j->plane_stride);
+    const int ld_dst = __ldg(&j->ld_dst);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = r0 + ty + 8 * i, k = k0 + tx;
+      if (r < rows && k < kdim) {
+        __nv_bfloat16 v[3];
+        split_terms(tile[tx][ty + 8 * i], v);
+#pragma unroll
+        for (int pl = 0; pl < 3; ++pl)
+          if (pl < nplanes) planes[pl * pstride + (int64_t)r * ld_dst + k] = v[pl];
+      }
+    }
+  }
+}
+
 }  // namespace grouped
 }  // namespace hcbk
 
@@ -299,4 +569,54 @@ extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void 
   if (g->total_tiles < grid) grid = g->total_tiles;
   grouped_hgemm_kernel<<<grid, 192, SMEM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_grouped_pack(const hcbk_gpack_job *jobs, const int32_t *tile_start,
+                                 int32_t count, int32_t total_tiles, int nplanes, void *stream) {
+  using namespace hcbk::grouped;
+  if (count <= 0 || total_tiles <= 0 || (nplanes != 2 && nplanes != 3)) return HCBK_ERR_ARGS;
+  int grid = hcbk_sm_count() * 8;
+  if (total_tiles < grid) grid = total_tiles;
+  grouped_pack_kernel<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
+      jobs, tile_start, count, total_tiles, nplanes);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+namespace {
+template <class R, class Cfg>
+int launch_grouped_split(const hcbk_grouped_args *g, int *err, void *stream) {
+  using namespace hcbk::grouped;
+  auto kern = grouped_split_kernel<R, Cfg>;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HCBK_ERR_LAUNCH;
+  if (!attr_set[dev]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Cfg::SMEM_BYTES) != cudaSuccess)
+      return HCBK_ERR_LAUNCH;
+    attr_set[dev] = true;
+  }
+  Params p;
+  p.table = g->table;
+  p.tile_start = g->tile_start;
+  p.count = g->count;
+  p.total_tiles = g->total_tiles;
+  p.alpha = g->alpha;
+  p.beta = g->beta;
+  p.beta_nonzero = g->beta != 0.0f;
+  p.err = err;
+  int grid = hcbk_sm_count();
+  if (g->total_tiles < grid) grid = g->total_tiles;
+  kern<<<grid, 192, Cfg::SMEM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+}  // namespace
+
+extern "C" int hcbk_sgemm_grouped_split_tc(const hcbk_grouped_args *g, int terms, int *err,
+                                           void *stream) {
+  using namespace hcbk::grouped;
+  if (g->count <= 0 || g->total_tiles <= 0) return HCBK_ERR_ARGS;
+  if (terms == 6) return launch_grouped_split<hcbk::tc::RecipeBf16x6, SplitCfg6>(g, err, stream);
+  if (terms == 3) return launch_grouped_split<hcbk::tc::RecipeBf16x3, SplitCfg3>(g, err, stream);
+  return HCBK_ERR_ARGS;
 }

@@ -395,6 +395,41 @@ typedef struct hcbk_grouped_args {
 } hcbk_grouped_args;
 int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
 
+/* ------------------------------------------ grouped split-BF16 SGEMM -- */
+
+/* One operand of one grouped problem to split into bf16 planes:
+ * element (r, k) of the f32 source at src[k + r*ld] if k_contig else
+ * src[r + k*ld]; plane t at planes + t * plane_stride (elements), K-major
+ * [r * ld_dst + k]; tiles = ceil(rows / 32) * ceil(kdim / 32). */
+typedef struct hcbk_gpack_job {
+  const float *src;
+  int64_t ld;
+  void *planes;
+  int64_t plane_stride;
+  int32_t k_contig;
+  int32_t rows, kdim, ld_dst;
+  int32_t tiles_r;
+  int32_t pad_;
+} hcbk_gpack_job;
+
+/* Split every job's operand in one launch: 32 x 32 tiles enumerated by
+ * tile_start[] (count + 1 ascending prefix sums, device). */
+int hcbk_grouped_pack(const hcbk_gpack_job *jobs, const int32_t *tile_start, int32_t count,
+                      int32_t total_tiles, int nplanes, void *stream);
+
+/* 3-D tensor map (128 bytes at `map`) over `planes` 16-bit K-major planes
+ * {kdim, rows, plane}: row pitch ld elements, plane pitch pstride bytes;
+ * box {64, box_rows, 1}, 128-byte swizzle, zero fill beyond kdim and rows. */
+int hcbk_encode_tma_3d_planes(void *map, int bf16, const void *base, uint64_t kdim,
+                              uint64_t rows, uint64_t planes, uint64_t ld, uint64_t pstride,
+                              uint32_t box_rows);
+
+/* Persistent grouped split-BF16 SGEMM over a table whose map_a / map_b are
+ * 3-D plane maps (hcbk_encode_tma_3d_planes) of the split operands and whose
+ * C is f32: C = alpha * op(A) op(B) + beta * C with the products of `terms`
+ * (3 or 6) and the TMEM sums promoted into f32 registers every 64 K. */
+int hcbk_sgemm_grouped_split_tc(const hcbk_grouped_args *g, int terms, int *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,23 +22,9 @@
 #include <stdint.h>
 
 #include "hcbk.h"
+#include "split_bf16.cuh"
 
 namespace {
-
-__device__ __forceinline__ void split_terms(float x, __nv_bfloat16 (&t)[3]) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(x);
-  const float hf = __bfloat162float(h);
-  t[0] = h;
-  if (!isfinite(hf)) {
-    t[1] = __float2bfloat16_rn(0.f);
-    t[2] = t[1];
-    return;
-  }
-  const float r1 = x - hf;
-  const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-  t[1] = m;
-  t[2] = __float2bfloat16_rn(r1 - __bfloat162float(m));
-}
 
 /* source K-contiguous: element (r, k) at src[k + r*ld]; 4 k per thread */
 __global__ void pack_kcontig(hcbk_pack_args a) {

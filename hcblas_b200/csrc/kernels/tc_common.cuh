@@ -431,6 +431,36 @@ __host__ __device__ constexpr uint32_t make_idesc(uint32_t c_fmt, uint32_t ab_fm
          ((M >> 4) << 24);
 }
 
+/* ------------------------------------------------ split-BF16 recipes --
+ * One plane pair per product: A plane pa(i) x B plane pb(i) -> accumulator
+ * pacc(i); first(i) marks the first product written to its accumulator. */
+
+/* bf16x3: lo*hi + hi*lo into accumulator 1, hi*hi into accumulator 0
+ * (lo*lo dropped).  Keeping the correction terms (2^-8 smaller) apart from
+ * the leading term keeps them from being truncated against it. */
+struct RecipeBf16x3 {
+  static constexpr int NA = 2, NB = 2, NP = 3, NACC = 2;
+  static constexpr bool P3D = false;
+  __host__ __device__ static constexpr int pa(int i) { return i == 0 ? 1 : 0; }
+  __host__ __device__ static constexpr int pb(int i) { return i == 1 ? 1 : 0; }
+  __host__ __device__ static constexpr int pacc(int i) { return i == 2 ? 0 : 1; }
+  __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 2; }
+};
+/* bf16x6: three-way split, every product of total order <= 2; hi*hi into
+ * accumulator 0, the five correction products into accumulator 1 */
+struct RecipeBf16x6 {
+  static constexpr int NA = 3, NB = 3, NP = 6, NACC = 2;
+  static constexpr bool P3D = false;
+  __host__ __device__ static constexpr int pa(int i) {
+    return i == 0 ? 2 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 1 : 0;
+  }
+  __host__ __device__ static constexpr int pb(int i) {
+    return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 2 : i == 3 ? 0 : i == 4 ? 1 : 0;
+  }
+  __host__ __device__ static constexpr int pacc(int i) { return i == 5 ? 0 : 1; }
+  __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 5; }
+};
+
 }  // namespace tc
 }  // namespace hcbk
 

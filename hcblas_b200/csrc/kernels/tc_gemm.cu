@@ -85,31 +85,7 @@ struct RecipeSingle {
   __host__ __device__ static constexpr int pacc(int) { return 0; }
   __host__ __device__ static constexpr bool first(int i) { return i == 0; }
 };
-/* bf16x3: lo*hi + hi*lo into accumulator 1, hi*hi into accumulator 0
- * (lo*lo dropped).  Keeping the correction terms (2^-8 smaller) apart from
- * the leading term keeps them from being truncated against it. */
-struct RecipeBf16x3 {
-  static constexpr int NA = 2, NB = 2, NP = 3, NACC = 2;
-  static constexpr bool P3D = false;
-  __host__ __device__ static constexpr int pa(int i) { return i == 0 ? 1 : 0; }
-  __host__ __device__ static constexpr int pb(int i) { return i == 1 ? 1 : 0; }
-  __host__ __device__ static constexpr int pacc(int i) { return i == 2 ? 0 : 1; }
-  __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 2; }
-};
-/* bf16x6: three-way split, every product of total order <= 2; hi*hi into
- * accumulator 0, the five correction products into accumulator 1 */
-struct RecipeBf16x6 {
-  static constexpr int NA = 3, NB = 3, NP = 6, NACC = 2;
-  static constexpr bool P3D = false;
-  __host__ __device__ static constexpr int pa(int i) {
-    return i == 0 ? 2 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 1 : 0;
-  }
-  __host__ __device__ static constexpr int pb(int i) {
-    return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 2 : i == 3 ? 0 : i == 4 ? 1 : 0;
-  }
-  __host__ __device__ static constexpr int pacc(int i) { return i == 5 ? 0 : 1; }
-  __host__ __device__ static constexpr bool first(int i) { return i == 0 || i == 5; }
-};
+/* RecipeBf16x3 / RecipeBf16x6: tc_common.cuh (shared with the grouped kernel) */
 /* Ozaki, S int8 slices per operand: every pair (i, j) with i + j < S,
  * enumerated by weight d = i + j, accumulated exactly into INT32
  * accumulator d.  All planes of an operand share one 3-D tensor map
@@ -1253,8 +1229,9 @@ extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stre
 
 /* 3-D map over `planes` f16 planes {K, rows, plane}: row pitch ld elements,
  * plane pitch pstride bytes; box {64, box_rows, 1}, 128-byte swizzle. */
-static int make_map_planes_f16(CUtensorMap *map, const void *base, uint64_t kdim, uint64_t rows,
-                               uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
+static int make_map_planes(CUtensorMap *map, CUtensorMapDataType dt, const void *base,
+                           uint64_t kdim, uint64_t rows, uint64_t planes, uint64_t ld,
+                           uint64_t pstride, uint32_t box_rows) {
   auto fn = encode_fn();
   if (!fn) return HCBK_ERR_DRIVER;
   if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || (pstride & 15))
@@ -1263,10 +1240,24 @@ static int make_map_planes_f16(CUtensorMap *map, const void *base, uint64_t kdim
   cuuint64_t strides[2] = {ld * 2, pstride};
   cuuint32_t box[3] = {64, box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(base), dims, strides,
-                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+  CUresult r = fn(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
+}
+
+static int make_map_planes_f16(CUtensorMap *map, const void *base, uint64_t kdim, uint64_t rows,
+                               uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
+  return make_map_planes(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, base, kdim, rows, planes, ld,
+                         pstride, box_rows);
+}
+
+extern "C" int hcbk_encode_tma_3d_planes(void *map, int bf16, const void *base, uint64_t kdim,
+                                         uint64_t rows, uint64_t planes, uint64_t ld,
+                                         uint64_t pstride, uint32_t box_rows) {
+  return make_map_planes(static_cast<CUtensorMap *>(map),
+                         bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                         base, kdim, rows, planes, ld, pstride, box_rows);
 }
 
 /* 3-D map over the int16 residue planes T {rows, cols, plane}: column pitch

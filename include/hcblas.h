@@ -311,6 +311,20 @@ hcblasStatus_t hcblasHgemmGrouped(hcblasHandle_t handle, int count,
                                   const hcblasGemmProblem *problems, const hcblasHalf *alpha,
                                   const hcblasHalf *beta);
 
+/* Extension (no counterpart in the reference): the grouped GEMM for f32
+ * problems (the same hcblasGemmProblem array, f32 device matrices), computed
+ * on the tensor cores by the split-BF16 scheme -- every problem's op(A) and
+ * op(B) are split into bf16 planes by one packing launch, then one
+ * persistent kernel walks all problems' 128 x 128 tiles with 6 plane
+ * products (3 when the handle's math mode is HCBLAS_MATH_SPLIT_BF16 with
+ * param 3), its f32 sums promoted into registers every 64 K, so the error
+ * stays at or below plain FP32's.  Any alignment and leading dimension; the
+ * plan (plane layout, tables) is cached per handle for an identical
+ * follow-up problem array.  Status rules as hcblasHgemmGrouped. */
+hcblasStatus_t hcblasSgemmGrouped(hcblasHandle_t handle, int count,
+                                  const hcblasGemmProblem *problems, const float *alpha,
+                                  const float *beta);
+
 /* ------------------------------------------------ class-API C shims -- */
 
 /* C-ABI forms of the Hcblaslibrary::hcblas_Xgemm methods (include/hcblaslib.h;

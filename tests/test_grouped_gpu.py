@@ -31,7 +31,8 @@ def loguniform(rng, lo, hi):
     return int(np.exp(rng.uniform(np.log(lo), np.log(hi + 1))))
 
 
-def make_problems(handle, rng, count, lo=16, hi=600, align=8, misalign=()):
+def make_problems(handle, rng, count, lo=16, hi=600, align=8, misalign=(), dtype=np.float16,
+                  pad=None):
     probs, host, dev = [], [], []
     for i in range(count):
         ta, tb = int(rng.integers(0, 2)), int(rng.integers(0, 2))
@@ -40,10 +41,12 @@ def make_problems(handle, rng, count, lo=16, hi=600, align=8, misalign=()):
         rnd = lambda v: -(-v // align) * align
         lda = rnd(ra) + (1 if i in misalign else 0)
         ldb = rnd(rb)
+        if pad is not None:  # arbitrary leading dimensions
+            lda, ldb = ra + int(rng.integers(0, pad)), rb + int(rng.integers(0, pad))
         ldc = M + int(rng.integers(0, 3))
-        A = rng.uniform(-1, 1, lda * (K if ta == 0 else M)).astype(np.float16)
-        B = rng.uniform(-1, 1, ldb * (N if tb == 0 else K)).astype(np.float16)
-        C = rng.uniform(-1, 1, ldc * N).astype(np.float16)
+        A = rng.uniform(-1, 1, lda * (K if ta == 0 else M)).astype(dtype)
+        B = rng.uniform(-1, 1, ldb * (N if tb == 0 else K)).astype(dtype)
+        C = rng.uniform(-1, 1, ldc * N).astype(dtype)
         dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
         probs.append(hb.GemmProblem(ta, tb, M, N, K, dA.ptr, lda, dB.ptr, ldb, dC.ptr, ldc))
         host.append((ta, tb, M, N, K, A, lda, B, ldb, C, ldc))
@@ -161,3 +164,70 @@ def test_strided_batched_hgemm_is_grouped(handle, ta, tb):
         bound = 2.0 ** -11 * np.linalg.norm(ref) + 2 * g32(K) * np.linalg.norm(0.5 * (Ad @ Bd) + cc)
         assert np.linalg.norm(gv - ref) <= bound, i
         assert np.array_equal(got[i * sC + ldc * N:(i + 1) * sC], C[i * sC + ldc * N:(i + 1) * sC])
+
+
+# ------------------------------------------------- grouped FP32 (split-BF16)
+
+def check_f32(host, dev, alpha, beta, rel=0.0):
+    """Per problem: the plain-FP32 normwise bound
+        ||C_gpu - C_ref||_F <= gamma_{K+2}(f32) || |alpha||A||B| + |beta||C| ||_F
+    (+ rel ||C_ref||_F for the 3-term split, whose planes carry ~16 bits)."""
+    for (ta, tb, M, N, K, A, lda, B, ldb, C, ldc), (_, _, dC) in zip(host, dev):
+        got = dC.download()
+        _, ref = O.gemm(O.COL, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+        gv = O.view_c(got, O.COL, M, N, ldc).astype(np.float64)
+        Ad, Bd = np.abs(op_dense(A, ta, M, K, lda)), np.abs(op_dense(B, tb, K, N, ldb))
+        cc = abs(beta) * np.abs(O.view_c(C, O.COL, M, N, ldc).astype(np.float64))
+        bound = g32(K) * np.linalg.norm(abs(alpha) * (Ad @ Bd) + cc) + rel * np.linalg.norm(ref)
+        err = np.linalg.norm(gv - ref)
+        assert err <= bound, (ta, tb, M, N, K, err, bound)
+        assert np.array_equal(got[: ldc * N].reshape(N, ldc)[:, M:],
+                              C[: ldc * N].reshape(N, ldc)[:, M:])
+
+
+def test_sgemm_grouped_split_uneven_any_leading_dimension(handle):
+    """f32 problems with unpadded, odd leading dimensions and mixed
+    transposes, all in one packing launch and one grouped tensor-core launch;
+    6 products keep every problem within the plain FP32 bound."""
+    rng = np.random.default_rng(30)
+    probs, host, dev = make_problems(handle, rng, 40, lo=8, hi=400, dtype=np.float32, pad=4)
+    assert hb.sgemm_grouped(handle, probs, 1.25, 0.5) == 0
+    assert hb.device_error(handle) == 0
+    assert hb.hcblasGetLastPath(handle) == "tc.s.grouped_split_bf16x6"
+    check_f32(host, dev, 1.25, 0.5)
+
+
+def test_sgemm_grouped_split3_and_plan_reuse(handle):
+    """The 3-term split under HCBLAS_MATH_SPLIT_BF16 param 3; a second call
+    with the same problem array reuses the plan but packs the new contents."""
+    rng = np.random.default_rng(31)
+    probs, host, dev = make_problems(handle, rng, 16, lo=16, hi=300, dtype=np.float32, pad=3)
+    assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_SPLIT_BF16, 3) == 0
+    try:
+        assert hb.sgemm_grouped(handle, probs, 1.0, 0.0) == 0
+        assert hb.hcblasGetLastPath(handle) == "tc.s.grouped_split_bf16x3"
+        new_host = []
+        for (ta, tb, M, N, K, A, lda, B, ldb, C, ldc), (dA, dB, dC) in zip(host, dev):
+            A2 = rng.uniform(-1, 1, A.size).astype(np.float32)
+            dA.upload(A2)
+            dC.upload(C)
+            new_host.append((ta, tb, M, N, K, A2, lda, B, ldb, C, ldc))
+        assert hb.sgemm_grouped(handle, probs, -0.5, 2.0) == 0
+        assert hb.device_error(handle) == 0
+    finally:
+        hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+    check_f32(new_host, dev, -0.5, 2.0, rel=2.0 ** -14)
+
+
+def test_sgemm_grouped_alpha_zero_and_status(handle):
+    rng = np.random.default_rng(32)
+    probs, host, dev = make_problems(handle, rng, 5, lo=8, hi=90, dtype=np.float32, pad=2)
+    assert hb.sgemm_grouped(handle, probs, 0.0, 0.5) == 0
+    for (ta, tb, M, N, K, A, lda, B, ldb, C, ldc), (_, _, dC) in zip(host, dev):
+        got = O.view_c(dC.download(), O.COL, M, N, ldc)
+        assert np.array_equal(got, 0.5 * O.view_c(C, O.COL, M, N, ldc))
+    assert hb.sgemm_grouped(handle, [], 1.0, 0.0) == hb.HCBLAS_STATUS_SUCCESS
+    bad = [hb.GemmProblem(0, 0, 4, -1, 4, probs[0].A, 8, probs[0].B, 8, probs[0].C, 8)]
+    assert hb.sgemm_grouped(handle, probs + bad, 1.0, 0.0) == hb.HCBLAS_STATUS_INVALID_VALUE
+    L = hb.lib()
+    assert L.hcblasSgemmGrouped(None, 1, None, None, None) == hb.HCBLAS_STATUS_NOT_INITIALIZED
