@@ -731,6 +731,46 @@ def run_secondary_small(hb, h, stream, torch, O, timed):
         "tflops": round(flop / ms / 1e9, 2), "per_problem_calls_ms": round(ms_single, 3),
         "speedup_vs_per_problem": round(ms_single / ms, 2)}
     del keep, arr, call
+    # C4b, FP32 via split-BF16: the same problem list in f32 through
+    # hcblasSgemmGrouped, against per-problem plain FP32 hcblasSgemm calls;
+    # accuracy on 16 problems against the oracle, as a fraction of the plain
+    # FP32 bound gamma_{K+2} || |A||B| ||_F
+    hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
+    call, keep = profile_cases.CASES["sgemm_grouped_4096"](h)
+    ms = timed(call)
+    path_g = hb.hcblasGetLastPath(h)
+    dev_arrays, arr = keep
+    one32, zero32 = np.array([1.0], np.float32), np.array([0.0], np.float32)
+
+    def per_problem32():
+        for p in arr:
+            L.hcblasSgemm(h, p.transa, p.transb, p.m, p.n, p.k, one32.ctypes.data, p.A, p.lda,
+                          p.B, p.ldb, zero32.ctypes.data, p.C, p.ldc)
+    call()
+    torch.cuda.synchronize()
+    sample = np.random.default_rng(8).choice(len(arr), 16, replace=False)
+    u32 = 2.0 ** -24
+    worst = 0.0
+    for i in sample:
+        p = arr[int(i)]
+        dA, dB, dC = dev_arrays[3 * int(i):3 * int(i) + 3]
+        Ah = dA.download().astype(np.float64)
+        Bh = dB.download().astype(np.float64)
+        got = dC.download().astype(np.float64)
+        _, ref = O.gemm(O.COL, p.transa, p.transb, p.m, p.n, p.k, 1.0, Ah, p.lda, Bh, p.ldb, 0.0,
+                        np.zeros(p.m * p.n), p.m)
+        Ad = Ah.reshape(-1, p.lda)[:, :p.m].T if p.transa == 0 else Ah.reshape(-1, p.lda)[:, :p.k]
+        Bd = Bh.reshape(-1, p.ldb)[:, :p.k].T if p.transb == 0 else Bh.reshape(-1, p.ldb)[:, :p.n]
+        bound = (p.k + 2) * u32 * np.linalg.norm(np.abs(Ad) @ np.abs(Bd))
+        err = np.linalg.norm(O.view_c(got, O.COL, p.m, p.n, p.m) - ref)
+        worst = max(worst, err / bound)
+    ms_single = timed(per_problem32)
+    out["sgemm_grouped_4096_uneven_split_bf16x6"] = {
+        "path": path_g, "gflop": round(flop / 1e9, 2), "ms": round(ms, 4),
+        "tflops": round(flop / ms / 1e9, 2), "per_problem_plain_calls_ms": round(ms_single, 3),
+        "speedup_vs_per_problem_plain": round(ms_single / ms, 2),
+        "worst_err_over_plain_fp32_bound_16_problems": round(worst, 4)}
+    del keep, arr, call, dev_arrays
     # C5: complex 2048^3, op(A) = A^H, alpha (1, 0.5), beta (0.5, -0.25), seed 4
     n = 2048
     cols = np.random.default_rng(7).choice(n, 4, replace=False)

@@ -64,30 +64,37 @@ def _complex(h, dtype, op_a, op_b, m, n, k, mode=0, param=0, seed=4):
     return call, (dA, dB, dC)
 
 
-def _grouped(h, count=4096, seed=3):
-    """Uneven grouped HGEMM: M, N, K log-uniform integers in [16, 1024],
-    mixed N/T, leading dimensions padded to 8 elements (TMA rule)."""
+def _grouped(h, count=4096, seed=3, dtype=np.float16):
+    """Uneven grouped GEMM: M, N, K log-uniform integers in [16, 1024], mixed
+    N/T; f16 (hcblasHgemmGrouped, leading dimensions padded to 8 elements for
+    TMA) or f32 (hcblasSgemmGrouped on the split-BF16 path, unpadded)."""
     rng = np.random.default_rng(seed)
     lu = lambda: int(np.exp(rng.uniform(np.log(16), np.log(1025))))
     probs, keep = [], []
+    esz = np.dtype(dtype).itemsize
     for _ in range(count):
         ta, tb = int(rng.integers(0, 2)), int(rng.integers(0, 2))
         m, n, k = lu(), lu(), lu()
-        r8 = lambda v: -(-v // 8) * 8
+        r8 = (lambda v: -(-v // 8) * 8) if esz == 2 else (lambda v: v)
         lda, ldb = r8(m if ta == 0 else k), r8(k if tb == 0 else n)
-        A = rng.uniform(-1, 1, lda * (k if ta == 0 else m)).astype(np.float16)
-        B = rng.uniform(-1, 1, ldb * (n if tb == 0 else k)).astype(np.float16)
+        A = rng.uniform(-1, 1, lda * (k if ta == 0 else m)).astype(dtype)
+        B = rng.uniform(-1, 1, ldb * (n if tb == 0 else k)).astype(dtype)
         dA, dB = _dev(h, A), _dev(h, B)
-        dC = hb.DeviceArray(h, nbytes=2 * m * n, dtype=np.float16)
+        dC = hb.DeviceArray(h, nbytes=esz * m * n, dtype=dtype)
         keep += [dA, dB, dC]
         probs.append(hb.GemmProblem(ta, tb, m, n, k, dA.ptr, lda, dB.ptr, ldb, dC.ptr, m))
     arr = (hb.GemmProblem * count)(*probs)
-    one = np.array([1.0], np.float16).view(np.uint16)
-    zero = np.array([0.0], np.float16).view(np.uint16)
+    if esz == 2:
+        one = np.array([1.0], np.float16).view(np.uint16)
+        zero = np.array([0.0], np.float16).view(np.uint16)
+        fn = hb.lib().hcblasHgemmGrouped
+    else:
+        one, zero = np.array([1.0], np.float32), np.array([0.0], np.float32)
+        fn = hb.lib().hcblasSgemmGrouped
 
     def call():
-        assert hb.lib().hcblasHgemmGrouped(h, count, ctypes.cast(arr, ctypes.c_void_p),
-                                           one.ctypes.data, zero.ctypes.data) == 0
+        assert fn(h, count, ctypes.cast(arr, ctypes.c_void_p), one.ctypes.data,
+                  zero.ctypes.data) == 0
     return call, (keep, arr)
 
 
@@ -145,6 +152,7 @@ CASES = {
     "zgemm_native_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048),
     "zgemm_crt3m_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048, 4, 0),
     "hgemm_grouped_4096": _grouped,
+    "sgemm_grouped_4096": lambda h: _grouped(h, dtype=np.float32),
     "hgemm_strided_512x128": _strided,
     "sgemv_n_16384": lambda h: _gemv(h, np.float32, 0, 16384, 16384),
     "sgemv_t_16384": lambda h: _gemv(h, np.float32, 1, 16384, 16384),
