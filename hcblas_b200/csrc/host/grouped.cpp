@@ -280,14 +280,14 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
     }
     gp.key.clear();
     /* plane layout: per problem, A planes then B planes, each plane
-     * rows x kp bf16 (kp = K rounded up to 8: 16-byte rows), problems
-     * 1 KiB aligned */
+     * rows x kp bf16 (kp = K rounded up to 16: rows on 32-byte sectors),
+     * problems 1 KiB aligned */
     std::vector<Canon> cn((size_t)count);
     std::vector<size_t> a_off((size_t)count), b_off((size_t)count);
     size_t total_planes = 0;
     for (int i = 0; i < count; ++i) {
       cn[i] = canonical(probs[i], order);
-      const int64_t kp = (cn[i].k + 7) & ~int64_t(7);
+      const int64_t kp = (cn[i].k + 15) & ~int64_t(15);
       a_off[i] = total_planes;
       total_planes += (size_t)nplanes * cn[i].m * kp * 2;
       b_off[i] = total_planes;
@@ -314,7 +314,7 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
     std::vector<hcbk_gpack_job> jobs((size_t)count * 2);
     for (int i = 0; i < count; ++i) {
       const Canon &c = cn[i];
-      const int64_t kp = (c.k + 7) & ~int64_t(7);
+      const int64_t kp = (c.k + 15) & ~int64_t(15);
       if (c.m > 0x7fffffff || c.n > 0x7fffffff || c.k > 0x7fffffff) return HCBK_ERR_ARGS;
       hcbk_grouped_entry &e = ent[i];
       std::memset(&e, 0, sizeof(e));
@@ -380,7 +380,7 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
     for (size_t x = 0; x < njobs; ++x) {
       jdst[x] = jobs[x];
       jts[x] = (int32_t)ptotal;
-      ptotal += (int64_t)jobs[x].tiles_r * ((jobs[x].kdim + 31) / 32);
+      ptotal += (int64_t)jobs[x].tiles_r * ((jobs[x].kdim + 63) / 64);
       if (ptotal > 0x7fffffff) return HCBK_ERR_ARGS;
     }
     jts[njobs] = (int32_t)ptotal;

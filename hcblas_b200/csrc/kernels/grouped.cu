@@ -469,50 +469,110 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
   }
 }
 
-/* Split every job's f32 operand into nplanes K-major bf16 planes: one
- * 32 x 32 tile (rows x K) per iteration, read coalesced along whichever
- * dimension is contiguous in the source and written along K. */
+/* One pack job's fields, read once per job (tiles of a job are consecutive). */
+struct PackJob {
+  const float *src;
+  __nv_bfloat16 *planes;
+  int64_t ld, pstride;
+  int rows, kdim, ld_dst, tiles_r, k_contig;
+};
+
+__device__ __forceinline__ PackJob load_job(const hcbk_gpack_job *j) {
+  PackJob o;
+  o.src = j->src;
+  o.planes = static_cast<__nv_bfloat16 *>(j->planes);
+  o.ld = __ldg(&j->ld);
+  o.pstride = __ldg(&j->plane_stride);
+  o.rows = __ldg(&j->rows);
+  o.kdim = __ldg(&j->kdim);
+  o.ld_dst = __ldg(&j->ld_dst);
+  o.tiles_r = __ldg(&j->tiles_r);
+  o.k_contig = __ldg(&j->k_contig);
+  return o;
+}
+
+/* this thread's eight source values of tile (r0, k0) */
+__device__ __forceinline__ void pack_load(const PackJob &j, int r0, int k0, float (&v)[8]) {
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  if (j.k_contig) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = r0 + ty + 8 * (i & 3), k = k0 + tx + 32 * (i >> 2);
+      v[i] = (r < j.rows && k < j.kdim) ? __ldg(j.src + (int64_t)r * j.ld + k) : 0.f;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = r0 + tx, k = k0 + ty + 8 * i;
+      v[i] = (r < j.rows && k < j.kdim) ? __ldg(j.src + r + (int64_t)k * j.ld) : 0.f;
+    }
+  }
+}
+
+/* Split every job's f32 operand into nplanes K-major bf16 planes, one
+ * 32 x 64 tile (rows x K) per iteration, read coalesced along whichever
+ * dimension is contiguous in the source and written along K as bf16 pairs
+ * (128 contiguous bytes per warp and plane).  Each block takes a contiguous
+ * range of the tile sequence -- one binary search finds its first job, the
+ * rest follow by stepping forward, and a job's fields are read once -- and
+ * the next tile's loads are in flight while the current one is written. */
 __global__ void __launch_bounds__(256) grouped_pack_kernel(const hcbk_gpack_job *jobs,
                                                            const int32_t *ts, int count,
                                                            int total, int nplanes) {
-  __shared__ float tile[32][33]; /* [k][r] */
+  __shared__ float tile[64][33]; /* [k][r] */
   const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
-  for (int t = blockIdx.x; t < total; t += gridDim.x) {
-    const int g = find_problem(ts, count, t);
-    const hcbk_gpack_job *j = jobs + g;
-    const int lt = t - __ldg(ts + g);
-    const int tiles_r = __ldg(&j->tiles_r);
-    const int rows = __ldg(&j->rows), kdim = __ldg(&j->kdim);
-    const int64_t ld = __ldg(&j->ld);
-    const int r0 = (lt % tiles_r) * 32, k0 = (lt / tiles_r) * 32;
-    const float *src = j->src;
+  const int t_begin = (int)((int64_t)total * blockIdx.x / gridDim.x);
+  const int t_end = (int)((int64_t)total * (blockIdx.x + 1) / gridDim.x);
+  if (t_begin >= t_end) return;
+  int g = find_problem(ts, count, t_begin);
+  int g_first = __ldg(ts + g), g_next = __ldg(ts + g + 1);
+  PackJob nj = load_job(jobs + g);
+  int lt = t_begin - g_first;
+  int nr0 = (lt % nj.tiles_r) * 32, nk0 = (lt / nj.tiles_r) * 64;
+  float v[8];
+  pack_load(nj, nr0, nk0, v);
+  for (int t = t_begin; t < t_end; ++t) {
+    const PackJob j = nj; /* the tile whose values are in v */
+    const int r0 = nr0, k0 = nk0;
     __syncthreads(); /* the previous tile's reads of `tile` are done */
-    if (__ldg(&j->k_contig)) {
+    if (j.k_contig) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int r = r0 + ty + 8 * i, k = k0 + tx;
-        tile[tx][ty + 8 * i] = (r < rows && k < kdim) ? src[(int64_t)r * ld + k] : 0.f;
-      }
+      for (int i = 0; i < 8; ++i) tile[tx + 32 * (i >> 2)][ty + 8 * (i & 3)] = v[i];
     } else {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int r = r0 + tx, k = k0 + ty + 8 * i;
-        tile[ty + 8 * i][tx] = (r < rows && k < kdim) ? src[r + (int64_t)k * ld] : 0.f;
-      }
+      for (int i = 0; i < 8; ++i) tile[ty + 8 * i][tx] = v[i];
     }
     __syncthreads();
-    __nv_bfloat16 *planes = static_cast<__nv_bfloat16 *>(j->planes);
-    const int64_t pstride = __ldg(&j->plane_stride);
-    const int ld_dst = __ldg(&j->ld_dst);
+    if (t + 1 < t_end) { /* start the next tile's loads */
+      if (t + 1 >= g_next) {
+        while (t + 1 >= g_next) {
+          ++g;
+          g_next = __ldg(ts + g + 1);
+        }
+        g_first = __ldg(ts + g);
+        nj = load_job(jobs + g);
+      }
+      lt = t + 1 - g_first;
+      nr0 = (lt % nj.tiles_r) * 32;
+      nk0 = (lt / nj.tiles_r) * 64;
+      pack_load(nj, nr0, nk0, v);
+    }
+    /* this thread's k pair; the row's padding up to ld_dst (a multiple of
+     * 16: rows start on 32-byte sectors) is written too, as zeros, so that
+     * every sector is written whole and L2 never fetches one to merge */
+    const int k = k0 + 2 * tx;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int r = r0 + ty + 8 * i, k = k0 + tx;
-      if (r < rows && k < kdim) {
-        __nv_bfloat16 v[3];
-        split_terms(tile[tx][ty + 8 * i], v);
+      const int rl = ty + 8 * i, r = r0 + rl;
+      if (r >= j.rows || k >= j.ld_dst) continue;
+      __nv_bfloat16 a[3], b[3];
+      split_terms(tile[2 * tx][rl], a);
+      split_terms(tile[2 * tx + 1][rl], b);
+      __nv_bfloat16 *d = j.planes + (int64_t)r * j.ld_dst + k;
 #pragma unroll
-        for (int pl = 0; pl < 3; ++pl)
-          if (pl < nplanes) planes[pl * pstride + (int64_t)r * ld_dst + k] = v[pl];
+      for (int pl = 0; pl < 3; ++pl) {
+        if (pl >= nplanes) break;
+        *reinterpret_cast<__nv_bfloat162 *>(d + pl * j.pstride) = __halves2bfloat162(a[pl], b[pl]);
       }
     }
   }

@@ -400,7 +400,8 @@ int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
 /* One operand of one grouped problem to split into bf16 planes:
  * element (r, k) of the f32 source at src[k + r*ld] if k_contig else
  * src[r + k*ld]; plane t at planes + t * plane_stride (elements), K-major
- * [r * ld_dst + k]; tiles = ceil(rows / 32) * ceil(kdim / 32). */
+ * [r * ld_dst + k] with ld_dst a multiple of 16 (the padding k >= kdim is
+ * written as zeros); the job's tiles are ceil(rows / 32) x ceil(kdim / 64). */
 typedef struct hcbk_gpack_job {
   const float *src;
   int64_t ld;
@@ -412,7 +413,7 @@ typedef struct hcbk_gpack_job {
   int32_t pad_;
 } hcbk_gpack_job;
 
-/* Split every job's operand in one launch: 32 x 32 tiles enumerated by
+/* Split every job's operand in one launch: 32 x 64 tiles enumerated by
  * tile_start[] (count + 1 ascending prefix sums, device). */
 int hcbk_grouped_pack(const hcbk_gpack_job *jobs, const int32_t *tile_start, int32_t count,
                       int32_t total_tiles, int nplanes, void *stream);
