@@ -171,17 +171,31 @@ __device__ __forceinline__ Limbs2 pair_limbs(const Limbs &a, const Limbs &b) {
                 pk2(a.l4, b.l4)};
 }
 
-/* residue() for two elements in seven packed instructions; the result pair
- * converted to binary16 */
-__device__ __forceinline__ __half2 residue2_h(const Limbs2 &L, const ModPair &m) {
+/* x - rint(x / p) p for a pair of exact integers whose quotient rounds
+ * exactly (|x| < 2^19) */
+__device__ __forceinline__ uint64_t mod2(uint64_t t, const ModPair &m) {
   const uint64_t RND2 = pk2(RND_F, RND_F), NRND2 = pk2(-RND_F, -RND_F);
+  const uint64_t q = add2(fma2(t, pk2(m.inv_p), RND2), NRND2);
+  return fma2(q, pk2(m.neg_p), t);
+}
+
+/* residue() for two elements in seven packed instructions */
+__device__ __forceinline__ uint64_t residue2(const Limbs2 &L, const ModPair &m) {
   uint64_t t = fma2(L.l4, pk2(m.c4), L.l0);
   t = fma2(L.l3, pk2(m.c3), t);
   t = fma2(L.l2, pk2(m.c2), t);
   t = fma2(L.l1, pk2(m.c1), t);
-  const uint64_t q = add2(fma2(t, pk2(m.inv_p), RND2), NRND2);
-  const float2 r = upk2(fma2(q, pk2(m.neg_p), t));
-  return __floats2half2_rn(r.x, r.y);
+  return mod2(t, m);
+}
+
+__device__ __forceinline__ __half2 to_h2(uint64_t r) {
+  const float2 f = upk2(r);
+  return __floats2half2_rn(f.x, f.y);
+}
+
+/* the residue pair converted to binary16 */
+__device__ __forceinline__ __half2 residue2_h(const Limbs2 &L, const ModPair &m) {
+  return to_h2(residue2(L, m));
 }
 
 /* K-contiguous source: 8 consecutive k per thread, 16-byte plane stores */
@@ -651,6 +665,7 @@ struct ZResArgs {
   int beta;
   int nmod;
   ModConst mc[HCBK_CRT_MAX_MODULI];
+  ModPair mp[HCBK_CRT_MAX_MODULI];
   char *planes;          /* plane (set, i) at planes + (set * nmod + i) * plane_stride */
   int64_t plane_stride;  /* bytes; sets: 0 = real, 1 = imaginary, 2 = sum */
   int64_t ld_dst;        /* elements */
@@ -673,49 +688,55 @@ __device__ __forceinline__ ZRes3 zresidue(const Limbs &lr, const Limbs &li, cons
   return o;
 }
 
-/* K-contiguous complex source: 8 consecutive k per thread, 16-byte stores */
-__global__ void zcrt_res_kcontig(ZResArgs a) {
-  /* moduli constants in shared memory: 80 limb registers leave no room
-   * for them, and a run-time index into the parameter bank serialises */
-  __shared__ ModConst smc[HCBK_CRT_MAX_MODULI];
-  if (threadIdx.x < HCBK_CRT_MAX_MODULI) smc[threadIdx.x] = a.mc[threadIdx.x];
-  __syncthreads();
-  struct alignas(16) H8 { __half2 v[4]; };
-  const int64_t kq = (a.kdim + 7) / 8;
+/* K-contiguous complex source: 4 consecutive k per thread (40 limb
+ * registers), residues of element pairs by packed f32x2 arithmetic with the
+ * moduli constants as constant-bank operands, 8-byte stores per plane */
+__global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
+  const int64_t kq = (a.kdim + 3) / 4;
   const int64_t total = a.rows * kq;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = idx / kq;
-    const int64_t k0 = (idx % kq) * 8;
+    const int64_t k0 = (idx % kq) * 4;
     const int e = row_exp(a.exps, a.exp_pair, r);
-    Limbs lr[8], li[8];
+    Limbs2 lr[2], li[2]; /* element pairs (0, 1), (2, 3); im carries the conj sign */
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const double2 z = (k0 + j < a.kdim) ? a.src[r * a.ld + k0 + j] : make_double2(0.0, 0.0);
-      lr[j] = limbs_of(z.x, e, a.beta);
-      li[j] = limbs_of(z.y, e, a.beta);
+    for (int j = 0; j < 2; ++j) {
+      const double2 z0 =
+          (k0 + 2 * j < a.kdim) ? a.src[r * a.ld + k0 + 2 * j] : make_double2(0.0, 0.0);
+      const double2 z1 =
+          (k0 + 2 * j + 1 < a.kdim) ? a.src[r * a.ld + k0 + 2 * j + 1] : make_double2(0.0, 0.0);
+      lr[j] = pair_limbs(limbs_of(z0.x, e, a.beta), limbs_of(z1.x, e, a.beta));
+      li[j] = pair_limbs(limbs_of(a.im_sign * z0.y, e, a.beta),
+                         limbs_of(a.im_sign * z1.y, e, a.beta));
     }
-    for (int i = 0; i < a.nmod; ++i) {
-      const ModConst m = smc[i];
-      H8 o[3];
+    const int64_t left = a.kdim - k0;
+    const int nk = left < 4 ? (int)left : 4;
+    char *d0 = a.planes + (r * a.ld_dst + k0) * (int64_t)sizeof(__half);
+    const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & 7) == 0 && (a.plane_stride & 7) == 0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const ZRes3 x0 = zresidue(lr[2 * j], li[2 * j], m, a.im_sign);
-        const ZRes3 x1 = zresidue(lr[2 * j + 1], li[2 * j + 1], m, a.im_sign);
-        o[0].v[j] = __floats2half2_rn(x0.re, x1.re);
-        o[1].v[j] = __floats2half2_rn(x0.im, x1.im);
-        o[2].v[j] = __floats2half2_rn(x0.sum, x1.sum);
+    for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
+      if (i >= a.nmod) break;
+      const ModPair m = a.mp[i];
+      __half2 o[3][2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const uint64_t re = residue2(lr[j], m), im = residue2(li[j], m);
+        o[0][j] = to_h2(re);
+        o[1][j] = to_h2(im);
+        o[2][j] = to_h2(mod2(add2(re, im), m)); /* |re + im| <= 254: exact quotient */
       }
 #pragma unroll
       for (int set = 0; set < 3; ++set) {
-        __half *d = reinterpret_cast<__half *>(a.planes + (set * a.nmod + i) * a.plane_stride) +
-                    r * a.ld_dst + k0;
-        if (k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
-          *reinterpret_cast<H8 *>(d) = o[set];
+        __half *d = reinterpret_cast<__half *>(d0 + (set * a.nmod + i) * a.plane_stride);
+        if (vec) {
+          *reinterpret_cast<uint2 *>(d) = *reinterpret_cast<const uint2 *>(o[set]);
         } else {
-          const __half *h = reinterpret_cast<const __half *>(&o[set]);
-          for (int j = 0; j < 8; ++j)
-            if (k0 + j < a.kdim) d[j] = h[j];
+          const __half h[4] = {__low2half(o[set][0]), __high2half(o[set][0]),
+                               __low2half(o[set][1]), __high2half(o[set][1])};
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (j < nk) d[j] = h[j];
         }
       }
     }
@@ -956,13 +977,14 @@ extern "C" int hcbk_zcrt_residues(const hcbk_zcrt_prep *in, void *stream) {
   a.beta = in->beta_bits;
   a.nmod = in->nmod;
   fill_mod_consts(a.mc);
+  fill_mod_pairs(a.mp);
   a.planes = static_cast<char *>(in->planes);
   a.plane_stride = in->plane_stride;
   a.ld_dst = in->ld_dst;
   if (in->k_contig) {
-    const int64_t total = a.rows * ((a.kdim + 7) / 8);
+    const int64_t total = a.rows * ((a.kdim + 3) / 4);
     int64_t blocks = (total + 255) / 256;
-    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+    const int64_t cap = (int64_t)hcbk_sm_count() * 12;
     if (blocks > cap) blocks = cap;
     zcrt_res_kcontig<<<(unsigned)blocks, 256, 0, st>>>(a);
   } else {
