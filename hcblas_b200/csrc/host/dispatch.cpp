@@ -366,6 +366,42 @@ bool crt_plan(int64_t k, int want, int *nmod, int *beta) {
   return false;
 }
 
+/* CRT plan of the real (DGEMM) path.  Operands are scaled to integers of
+ * up to 53 bits, x' = rint(x 2^(53 - e_r)) per row/column.  Two bounds keep
+ * |P'| = |sum_k a'_k b'_k| below M / (2 * 2^0.01): K 2^106 when the moduli
+ * are that wide (then e_r is the frexp exponent of the row maximum), else
+ * ||a'||_2 ||b'||_2 <= (2^nb + sqrt(K) / 2)^2 with the row exponents raised
+ * so that every row norm is below 2^nb (Cauchy-Schwarz): rows that are not
+ * dominated by one entry then keep about log2(max |x| sqrt(K) / ||x||_2)
+ * more bits than scaling for the worst case K 2^(2 beta) allows.
+ * want = 0 picks the fewest moduli with the first bound (full binary64
+ * width whatever the data); want = n uses n moduli. */
+bool crt_plan_rows(int64_t k, int want, int *nmod, int *shift, bool *norm) {
+  int count = 0;
+  const int *mods = hcbk_crt_moduli(&count);
+  const double lk = std::ceil(std::log2((double)(k > 1 ? k : 2)));
+  /* rint of the rounded product x f: at most 3/4 of a unit per element */
+  const double rnd_norm = 0.75 * std::sqrt((double)k);
+  double cum = 0.0;
+  for (int i = 0; i < count; ++i) {
+    cum += std::log2((double)mods[i]);
+    const int n = i + 1;
+    const bool full = cum >= 2.0 * 53 + 1.0 + lk + 0.01;
+    if ((want == 0 && full) || want == n || (want == 0 && n == count)) {
+      *nmod = n;
+      *norm = !full;
+      *shift = 0;
+      if (full) return true;
+      int nb = (int)std::floor((cum - 1.02) / 2.0);
+      while (nb > 0 && 2.0 * std::log2(std::ldexp(1.0, nb) + rnd_norm) + 0.01 >= cum - 1.0) --nb;
+      if (nb < 8) return false;
+      *shift = 53 - nb;
+      return true;
+    }
+  }
+  return false;
+}
+
 /* CRT (Ozaki scheme II) DGEMM: exponents, residue planes of the scaled
  * integer operands, one modular tensor-core GEMM launch over every modulus,
  * CRT reconstruction (weighted residue sum mod M) with the alpha/beta
@@ -373,8 +409,10 @@ bool crt_plan(int64_t k, int want, int *nmod, int *beta) {
 int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
               const char **path) {
   if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
-  int nmod = 0, beta_bits = 0;
-  if (!crt_plan(a->k, want, &nmod, &beta_bits)) return HCBK_ERR_ARGS;
+  int nmod = 0, shift = 0;
+  bool norm = false;
+  if (!crt_plan_rows(a->k, want, &nmod, &shift, &norm)) return HCBK_ERR_ARGS;
+  const int beta_bits = 53;
   const int *mods = hcbk_crt_moduli(nullptr);
   const int64_t kp = (a->k + 7) & ~int64_t(7); /* 16-byte f16 row pitch */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
@@ -382,13 +420,24 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
   const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
-  const size_t total = ea_bytes + eb_bytes + nmod * (a_pl + b_pl + t_pl);
+  const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
+  const size_t fa_bytes = norm ? up1k(sizeof(double) * a->m) : 0;
+  const size_t fb_bytes = norm ? up1k(sizeof(double) * a->n) : 0;
+  const size_t wa_bytes =
+      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a->m, a->k, a_k)) : 0;
+  const size_t wb_bytes =
+      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a->n, a->k, b_k)) : 0;
+  const size_t total = ea_bytes + eb_bytes + fa_bytes + fb_bytes + wa_bytes + wb_bytes +
+                       nmod * (a_pl + b_pl + t_pl);
   char *ws = static_cast<char *>(ensure_workspace(st, total));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
   int *exp_a = reinterpret_cast<int *>(ws);
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
-  char *pa_base = ws + ea_bytes + eb_bytes;
+  double *frac_a = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes) : nullptr;
+  double *frac_b = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes + fa_bytes) : nullptr;
+  char *wa = ws + ea_bytes + eb_bytes + fa_bytes + fb_bytes, *wb = wa + wa_bytes;
+  char *pa_base = wb + wb_bytes;
   char *pb_base = pa_base + nmod * a_pl;
   char *t_base = pb_base + nmod * b_pl;
 
@@ -406,8 +455,16 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   eb.k_contig = a->op_b == HCBK_OP_N;
   eb.rows = a->n;
   eb.exps = exp_b;
-  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); }, ea.k_contig ? 1 : 2);
-  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); }, eb.k_contig ? 1 : 2);
+  /* row exponents: the row maximum's; when the moduli are too few for the
+   * worst case, exponent and 8-bit fraction from the row norm instead */
+  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, char *w, size_t wbytes) {
+    return timed_launch(st, stream, "ozaki.exponents", [&] {
+      return norm ? hcbk_crt_row_scales(&p, 53 - shift, frac, w, (int64_t)wbytes, stream)
+                  : hcbk_ozaki_exponents(&p, stream);
+    }, p.k_contig ? 1 : 2);
+  };
+  int rc = exps(ea, frac_a, wa, wa_bytes);
+  if (!rc) rc = exps(eb, frac_b, wb, wb_bytes);
   if (rc) return rc;
 
   hcbk_crt_prep ra;
@@ -417,6 +474,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   ra.rows = a->m;
   ra.kdim = a->k;
   ra.exps = exp_a;
+  ra.frac = frac_a;
   ra.beta_bits = beta_bits;
   ra.nmod = nmod;
   ra.planes = pa_base;
@@ -428,6 +486,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   rb.k_contig = eb.k_contig;
   rb.rows = a->n;
   rb.exps = exp_b;
+  rb.frac = frac_b;
   rb.planes = pb_base;
   rb.plane_stride = (int64_t)b_pl;
   rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&ra, stream); });
@@ -480,6 +539,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.ldr = ldt;
   cb.exp_a = exp_a;
   cb.exp_b = exp_b;
+  cb.frac_a = frac_a;
+  cb.frac_b = frac_b;
   cb.shift = 2 * beta_bits;
   cb.c = static_cast<double *>(a->c) + a->c_off;
   cb.ldc = a->ldc;

@@ -75,6 +75,7 @@ struct ResArgs {
   int64_t ld;
   int64_t rows, kdim;
   const int *exps;
+  const double *frac; /* optional: x * frac[r] is scaled */
   int beta;
   int nmod;
   ModPair mp[HCBK_CRT_MAX_MODULI];
@@ -208,13 +209,14 @@ __global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
     const int64_t r = idx / kq;
     const int64_t k0 = (idx % kq) * 8;
     const int e = a.exps[r];
+    const double f = a.frac ? a.frac[r] : 1.0;
     Limbs2 L2[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const Limbs x0 = limbs_of((k0 + 2 * j < a.kdim) ? a.src[r * a.ld + k0 + 2 * j] : 0.0, e,
-                                a.beta);
+      const Limbs x0 = limbs_of(
+          f * ((k0 + 2 * j < a.kdim) ? a.src[r * a.ld + k0 + 2 * j] : 0.0), e, a.beta);
       const Limbs x1 = limbs_of(
-          (k0 + 2 * j + 1 < a.kdim) ? a.src[r * a.ld + k0 + 2 * j + 1] : 0.0, e, a.beta);
+          f * ((k0 + 2 * j + 1 < a.kdim) ? a.src[r * a.ld + k0 + 2 * j + 1] : 0.0), e, a.beta);
       L2[j] = pair_limbs(x0, x1);
     }
 #pragma unroll
@@ -256,11 +258,12 @@ __global__ void crt_res_rcontig(ResArgs a) {
   const int64_t r = r0 + rl, k = k0 + kq;
   if (r >= a.rows || k >= a.kdim) return;
   const int e = a.exps[r];
+  const double f = a.frac ? a.frac[r] : 1.0;
   Limbs2 L2[2];
 #pragma unroll
   for (int j = 0; j < 2; ++j)
-    L2[j] = pair_limbs(limbs_of(tile[kq + 2 * j][rl], e, a.beta),
-                       limbs_of(tile[kq + 2 * j + 1][rl], e, a.beta));
+    L2[j] = pair_limbs(limbs_of(f * tile[kq + 2 * j][rl], e, a.beta),
+                       limbs_of(f * tile[kq + 2 * j + 1][rl], e, a.beta));
   const int64_t left = a.kdim - k;
   const int nk = left < 4 ? (int)left : 4;
   char *d0 = a.planes + (r * a.ld_dst + k) * (int64_t)sizeof(__half);
@@ -315,6 +318,7 @@ struct CombArgs {
   int64_t ldr;
   const int *exp_a;
   const int *exp_b;
+  const double *frac_a, *frac_b; /* optional row fractions of the scaling */
   int shift;
   double *c;
   int64_t ldc;
@@ -496,11 +500,14 @@ __global__ void __launch_bounds__(CMB_THREADS) crt_combine_kernel(CombArgs a) {
           acc[1].add(sw[i], hi16(q));
         }
         const int eb = a.exp_b[col];
+        const double fb = a.frac_b ? a.frac_b[col] : 1.0;
         double *dst = a.c + row + col * a.ldc;
 #pragma unroll
         for (int u = 0; u < CMB_RPT; ++u) {
           if (row + u >= a.m) break;
-          double o = a.alpha * acc[u].finish(a, a.exp_a[row + u], eb);
+          double v = acc[u].finish(a, a.exp_a[row + u], eb);
+          if (a.frac_a) v /= a.frac_a[row + u] * fb; /* 8-bit fractions: an exact product */
+          double o = a.alpha * v;
           if (a.beta_nonzero) o = fma(a.beta, dst[u], o);
           dst[u] = o;
         }
@@ -899,6 +906,7 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
   a.rows = in->rows;
   a.kdim = in->kdim;
   a.exps = in->exps;
+  a.frac = in->frac;
   a.beta = in->beta_bits;
   a.nmod = in->nmod;
   fill_mod_pairs(a.mp);
@@ -934,6 +942,8 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.ldr = in->ldr;
   a.exp_a = in->exp_a;
   a.exp_b = in->exp_b;
+  a.frac_a = in->frac_a;
+  a.frac_b = in->frac_b;
   a.shift = in->shift;
   a.c = in->c;
   a.ldc = in->ldc;
@@ -1010,6 +1020,8 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   a.g.ldr = in->ldr;
   a.g.exp_a = in->exp_a;
   a.g.exp_b = in->exp_b;
+  a.g.frac_a = nullptr;
+  a.g.frac_b = nullptr;
   a.g.shift = in->shift;
   a.g.c = nullptr;
   a.g.ldc = 0;

@@ -272,6 +272,224 @@ int launch_slice_any(const hcbk_ozaki_prep *a, cudaStream_t st) {
   return a->f16 ? launch_slice<S, __half>(a, st) : launch_slice<S, int8_t>(a, st);
 }
 
+/* ---------------------------------------------------------------------
+ * Row scales with a norm constraint (the CRT path): x(r,k) becomes the
+ * integer rint(x f_r 2^(53 - e_r)) with |x| f 2^(53-e) < 2^53 (e_r at least
+ * the frexp exponent of the row maximum) and the row norm
+ * ||x(r,:)|| f 2^(53-e) <= 2^nb.  The norm comes from one pass: a sum of squares scaled by
+ * the running maximum exponent (taken 2^-40 larger to cover its rounding);
+ * rows split over several blocks merge their partials in a fixed order, so
+ * the result does not depend on timing.
+ * --------------------------------------------------------------------- */
+
+/* 2^e for -1022 <= e <= 1023, from its bit pattern */
+__device__ __forceinline__ double pow2i(int e) {
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+/* Running sum of squares scaled by the running maximum exponent, in the
+ * manner of the reference BLAS dnrm2: s = sum (x 2^-e)^2 with e the frexp
+ * exponent of the largest |x| so far; a larger exponent rescales s.  Zeros
+ * and non-finite values are skipped (the maximum flags the latter). */
+struct NormAcc {
+  int e;     /* -1100: nothing yet */
+  double s;
+  double sc; /* 2^-e, 0 when outside the normal range */
+};
+
+__device__ __forceinline__ void na_init(NormAcc &a) {
+  a.e = -1100;
+  a.s = 0.0;
+  a.sc = 0.0;
+}
+
+__device__ __forceinline__ void na_add(NormAcc &a, double x) {
+  const int be = (int)((static_cast<unsigned long long>(__double_as_longlong(x)) >> 52) & 0x7FF);
+  if (be == 0x7FF || x == 0.0) return;
+  const int e = be == 0 ? -1021 : be - 1022; /* subnormals: an upper bound */
+  if (e > a.e) {
+    const int d = 2 * (a.e - e); /* < 0 */
+    a.s = d >= -1022 ? a.s * pow2i(d) : 0.0;
+    a.e = e;
+    a.sc = (e >= -1022 && e <= 1022) ? pow2i(-e) : 0.0;
+  }
+  const double y = a.sc != 0.0 ? x * a.sc : ldexp(x, -a.e);
+  a.s = fma(y, y, a.s);
+}
+
+/* merge a partial (be, bs) into a */
+__device__ __forceinline__ void na_merge(NormAcc &a, int be, double bs) {
+  if (be <= -1100) return;
+  if (be > a.e) {
+    const int d = 2 * (a.e - be);
+    a.s = (d >= -1022 ? a.s * pow2i(d) : 0.0) + bs;
+    a.e = be;
+  } else {
+    const int d = 2 * (be - a.e);
+    a.s += d >= -1022 ? bs * pow2i(d) : 0.0;
+  }
+}
+
+/* The scale f 2^(53 - e) of a row from its maximum's frexp exponent emax
+ * (HCBK_OZ_ZERO / HCBK_OZ_NONFINITE pass through with f = 1) and its running
+ * sum (||x|| = 2^acc_e sqrt(s)): e >= emax keeps |x| f 2^(53-e) < 2^53, and
+ * f in (1/2, 1] -- rounded down to 8 significant bits, so that products of
+ * two of them are exact -- keeps ||x|| f 2^(53-e) <= 2^nb. */
+__device__ __forceinline__ void row_scale(int emax, int acc_e, double s, int nb, int *e_out,
+                                          double *f_out) {
+  if (emax == HCBK_OZ_NONFINITE || emax == HCBK_OZ_ZERO) {
+    *e_out = emax;
+    *f_out = 1.0;
+    return;
+  }
+  const double rt = sqrt(s * (1.0 + 0x1p-40)) * (1.0 + 0x1p-50); /* ||x|| <= 2^acc_e rt */
+  int er;
+  frexp(rt, &er); /* rt < 2^er */
+  int e = acc_e + er + 52 - nb;
+  if (e < emax) e = emax;
+  double f = ldexp(1.0 / rt, nb - 53 + e - acc_e); /* 2^(nb - 53 + e) / ||x|| */
+  if (f >= 1.0) {
+    f = 1.0;
+  } else {
+    f = ldexp(floor(ldexp(f, 8) * (1.0 - 0x1p-50)), -8); /* 8 bits, rounded down */
+  }
+  *e_out = e;
+  *f_out = f;
+}
+
+/* K-contiguous source: one warp per row, one pass (16-byte pairs when the
+ * row allows) */
+template <int VEC>
+__global__ void crt_rowexp_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
+                                   int nb, int *exps, double *frac) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < rows; r += nwarps) {
+    const double *row = src + r * ld;
+    unsigned long long m = 0;
+    NormAcc acc;
+    na_init(acc);
+    if (VEC == 2) {
+      const double2 *row2 = reinterpret_cast<const double2 *>(row);
+      for (int64_t k = lane; k < kdim / 2; k += 32) {
+        const double2 v = row2[k];
+        m = max(m, max(abs_bits(v.x), abs_bits(v.y)));
+        na_add(acc, v.x);
+        na_add(acc, v.y);
+      }
+    } else {
+      for (int64_t k = lane; k < kdim; k += 32) {
+        const double x = row[k];
+        m = max(m, abs_bits(x));
+        na_add(acc, x);
+      }
+    }
+    const int emax = exp_of_bits(warp_max_u64(m));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int oe = __shfl_xor_sync(0xffffffffu, acc.e, o);
+      const double os = __shfl_xor_sync(0xffffffffu, acc.s, o);
+      na_merge(acc, oe, os);
+    }
+    if (lane == 0) row_scale(emax, acc.e, acc.s, nb, exps + r, frac + r);
+  }
+}
+
+/* MN-contiguous source: threads along rows (two adjacent rows by 16-byte
+ * pairs when VEC = 2), K split over blockIdx.y; each (chunk, row) writes its
+ * maximum's bit pattern and its running sum (exponent, sum) */
+template <int VEC>
+__global__ void crt_rowexp_rcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
+                                   int64_t kchunk, unsigned long long *pm, int *pe, double *ps) {
+  const int64_t r = VEC * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+  if (r >= rows) return;
+  const int64_t k0 = (int64_t)blockIdx.y * kchunk;
+  const int64_t k1 = (k0 + kchunk < kdim) ? k0 + kchunk : kdim;
+  unsigned long long m[VEC];
+  NormAcc acc[VEC];
+#pragma unroll
+  for (int u = 0; u < VEC; ++u) {
+    m[u] = 0;
+    na_init(acc[u]);
+  }
+  if (VEC == 2) {
+    const double2 *p = reinterpret_cast<const double2 *>(src + r);
+    const int64_t step = ld / 2;
+    int64_t k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      double2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = p[(k + u) * step];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        m[0] = max(m[0], abs_bits(v[u].x));
+        m[VEC - 1] = max(m[VEC - 1], abs_bits(v[u].y));
+        na_add(acc[0], v[u].x);
+        na_add(acc[VEC - 1], v[u].y);
+      }
+    }
+    for (; k < k1; ++k) {
+      const double2 v = p[k * step];
+      m[0] = max(m[0], abs_bits(v.x));
+      m[VEC - 1] = max(m[VEC - 1], abs_bits(v.y));
+      na_add(acc[0], v.x);
+      na_add(acc[VEC - 1], v.y);
+    }
+  } else {
+    for (int64_t k = k0; k < k1; ++k) {
+      const double x = src[r + k * ld];
+      m[0] = max(m[0], abs_bits(x));
+      na_add(acc[0], x);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < VEC; ++u) { /* partials stored [row][chunk] for the finish */
+    const int64_t o = (r + u) * gridDim.y + blockIdx.y;
+    pm[o] = m[u];
+    pe[o] = acc[u].e;
+    ps[o] = acc[u].s;
+  }
+}
+
+/* one warp per row: lanes merge chunks lane, lane + 32, ... in order, then a
+ * fixed butterfly merges the lanes -- the same sum every run */
+__global__ void crt_rowexp_finish(const unsigned long long *pm, const int *pe, const double *ps,
+                                  int64_t rows, int nchunks, int nb, int *exps, double *frac) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < rows; r += nwarps) {
+    unsigned long long m = 0;
+    NormAcc acc;
+    na_init(acc);
+    for (int c = lane; c < nchunks; c += 32) {
+      const int64_t o = r * nchunks + c;
+      m = max(m, pm[o]);
+      na_merge(acc, pe[o], ps[o]);
+    }
+    m = warp_max_u64(m);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int oe = __shfl_xor_sync(0xffffffffu, acc.e, o);
+      const double os = __shfl_xor_sync(0xffffffffu, acc.s, o);
+      na_merge(acc, oe, os);
+    }
+    if (lane == 0) row_scale(exp_of_bits(m), acc.e, acc.s, nb, exps + r, frac + r);
+  }
+}
+
+/* the K split of the MN-contiguous row-exponent pass */
+static void rowexp_split(int64_t rows, int64_t kdim, int64_t *ky, int64_t *kchunk) {
+  const int64_t gx = (rows + 511) / 512;
+  int64_t y = ((int64_t)hcbk_sm_count() * 8 + gx - 1) / gx;
+  if (y > 1024) y = 1024;
+  int64_t kc = (kdim + y - 1) / y;
+  if (kc < 32) kc = 32;
+  *ky = (kdim + kc - 1) / kc;
+  *kchunk = kc;
+}
+
 }  // namespace
 
 extern "C" int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream) {
@@ -318,4 +536,50 @@ extern "C" int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream) {
     case 8: return launch_slice_any<8>(a, st);
     default: return HCBK_ERR_ARGS;
   }
+}
+
+extern "C" int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, int k_contig) {
+  if (k_contig || rows <= 0 || kdim <= 0) return 0;
+  int64_t ky, kc;
+  rowexp_split(rows, kdim, &ky, &kc);
+  return ky * rows * (int64_t)(sizeof(unsigned long long) + sizeof(double) + sizeof(int)) + 256;
+}
+
+extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, void *work,
+                                   int64_t work_bytes, void *stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (a->rows <= 0 || a->kdim <= 0 || !frac) return HCBK_ERR_ARGS;
+  const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0;
+  if (a->k_contig) {
+    int64_t blocks = (a->rows * 32 + 255) / 256;
+    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    if (al16 && (a->kdim & 1) == 0)
+      crt_rowexp_kcontig<2><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, nb,
+                                                              a->exps, frac);
+    else
+      crt_rowexp_kcontig<1><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, nb,
+                                                              a->exps, frac);
+  } else {
+    int64_t ky, kc;
+    rowexp_split(a->rows, a->kdim, &ky, &kc);
+    if (ky > 65535 || !work ||
+        work_bytes < hcbk_crt_row_exponents_workspace(a->rows, a->kdim, 0))
+      return HCBK_ERR_ARGS;
+    unsigned long long *pm = static_cast<unsigned long long *>(work);
+    double *ps = reinterpret_cast<double *>(pm + ky * a->rows);
+    int *pe = reinterpret_cast<int *>(ps + ky * a->rows);
+    const int vec = (al16 && (a->rows & 1) == 0) ? 2 : 1;
+    const dim3 grid((unsigned)((a->rows / vec + 255) / 256), (unsigned)ky);
+    if (vec == 2)
+      crt_rowexp_rcontig<2><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kc, pm, pe, ps);
+    else
+      crt_rowexp_rcontig<1><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kc, pm, pe, ps);
+    int64_t fb = (a->rows * 32 + 255) / 256;
+    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+    if (fb > cap) fb = cap;
+    crt_rowexp_finish<<<(unsigned)fb, 256, 0, st>>>(pm, pe, ps, a->rows, (int)ky, nb, a->exps,
+                                                     frac);
+  }
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

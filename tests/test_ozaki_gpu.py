@@ -153,15 +153,58 @@ def crt_plan(K, want=0):
     return len(CRT_MODULI), min(53, int(np.floor((cum - 1.0 - lk - 0.01) / 2.0)))
 
 
-def crt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta_bits, ref, beta=0.0, C=None,
-              ldc=None):
-    """|alpha| K 2^(e_m + f_n) (2^-beta + 2^-2beta) + 4u|C| (+ 2u|beta C|)."""
+def crt_plan_rows(K, want=0):
+    """Moduli count and norm shift of the real (DGEMM) CRT path, as the
+    library chooses them: integers of up to 53 bits; when the moduli are too
+    few for the worst case K 2^106, every row is scaled so that its norm
+    stays below 2^(53 - shift) (Cauchy-Schwarz on the integer products; the
+    per-element rounding adds at most 3/4 sqrt(K))."""
+    lk = np.ceil(np.log2(max(K, 2)))
+    hr = 0.75 * np.sqrt(K)
+    cum = 0.0
+    for i, p in enumerate(CRT_MODULI):
+        cum += np.log2(p)
+        n = i + 1
+        full = cum >= 2 * 53 + 1 + lk + 0.01
+        if (want == 0 and full) or want == n or (want == 0 and n == len(CRT_MODULI)):
+            if full:
+                return n, None
+            nb = int(np.floor((cum - 1.02) / 2))
+            while nb > 0 and 2 * np.log2(2.0 ** nb + hr) + 0.01 >= cum - 1:
+                nb -= 1
+            return n, 53 - nb
+    raise AssertionError("no plan")
+
+
+def row_deltas(X, shift):
+    """Upper bounds of the per-element rounding error of the rows of X (2-D)
+    as the library scales them.  Full width: x' = rint(x 2^(53 - e)), e the
+    row maximum's frexp exponent, error 2^(e - 54).  Norm scaling: x' =
+    rint(fl(x f) 2^(53 - e)) with f in [1/2, 1] rounded down to 8 bits and
+    the scale f 2^-e the smaller of 2^-e_max and 2^(nb - 53) / ||x||, so the
+    error is at most 3/4 2^-53 max(2^e_max, ||x|| 2^(53 - nb)) (1 + 2^-6)."""
+    mx = np.max(np.abs(X), axis=1)
+    e = np.frexp(mx)[1].astype(np.float64)
+    if shift is None:
+        return np.where(mx > 0, np.exp2(e - 54), 0.0)
+    nb = 53 - shift
+    nrm = np.linalg.norm(X, axis=1)
+    inv_scale = np.maximum(np.exp2(e), nrm * 2.0 ** (53 - nb)) * (1 + 2.0 ** -6)
+    return np.where(mx > 0, 0.75 * 2.0 ** -53 * inv_scale, 0.0)
+
+
+def crt_bound_rows(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, shift, ref, beta=0.0, C=None,
+                   ldc=None):
+    """|alpha| (da_m sum_k |b_kn| + db_n sum_k |a_mk| + K da_m db_n) with the
+    per-element rounding bounds da, db of the scaled rows, plus 4u|C| (and
+    2u|beta C|) for the reconstruction and epilogue roundings."""
     Ad = op_dense(A, order, ta, M, K, lda, 0)
     Bd = op_dense(B, order, tb, K, N, ldb, 0)
-    ea = np.frexp(np.max(np.abs(Ad), axis=1))[1].astype(np.float64)
-    eb = np.frexp(np.max(np.abs(Bd), axis=0))[1].astype(np.float64)
-    scale = np.exp2(ea[:, None] + eb[None, :])
-    elem = abs(alpha) * K * scale * (2.0 ** -beta_bits + 2.0 ** (-2 * beta_bits))
+    da = row_deltas(Ad, shift)
+    db = row_deltas(Bd.T, shift)
+    elem = abs(alpha) * (da[:, None] * np.sum(np.abs(Bd), axis=0)[None, :] +
+                         np.sum(np.abs(Ad), axis=1)[:, None] * db[None, :] +
+                         K * da[:, None] * db[None, :])
     out = np.linalg.norm(elem) + 4 * U * np.linalg.norm(ref)
     if beta and C is not None:
         out += 2 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
@@ -187,14 +230,15 @@ def test_crt_vs_dd_oracle(handle, want):
     for order, ta, tb, M, N, K in CRT_CASES:
         A, lda, B, ldb, C, ldc = make_case(rng, "d", order, ta, tb, M, N, K)
         alpha, beta = 1.5, -0.25
-        nmod, bb = crt_plan(K, want)
+        nmod, shift = crt_plan_rows(K, want)
         got, path = run_crt(handle, want, order, ta, tb, M, N, K, alpha, beta, A, lda, B, ldb, C,
                             ldc)
         assert path == f"tc.crt_m{nmod}", path
         _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
         err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
-        bound = crt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, bb, ref, beta, C, ldc)
-        assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
+        bound = crt_bound_rows(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, shift, ref, beta, C,
+                               ldc)
+        assert err <= bound, (want, nmod, shift, order, ta, tb, M, N, K, err, bound)
 
 
 def test_crt_pair_matches_single_cta(handle):
@@ -230,8 +274,8 @@ def test_crt_special_and_hard_range(handle):
     ok[9] = False
     A0 = np.where(np.isfinite(A), A, 0.0)
     _, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, 0.5, C, M)
-    _, bb = crt_plan(K)
-    bound = crt_bound(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, bb, ref, 0.5, C, M)
+    _, shift = crt_plan_rows(K)
+    bound = crt_bound_rows(O.COL, 0, 0, M, N, K, 1.0, A0, M, B, K, shift, ref, 0.5, C, M)
     assert np.linalg.norm(gv[ok] - ref[ok]) <= bound
 
 
@@ -256,7 +300,7 @@ def test_ozaki_vs_native_accuracy(handle):
     print("native vs ozaki normwise errors:", errs)
     assert errs["i8_s8"] <= errs["native"] * 4
     assert errs["f16_s7"] <= errs["native"] * 4
-    nmod, _ = crt_plan(K)
+    nmod, _ = crt_plan_rows(K)
     assert errs[f"tc.crt_m{nmod}"] <= errs["native"]
 
 
@@ -321,8 +365,10 @@ def test_crt_combine_many_tiles_per_block(handle, kind, order, ta, tb, M, N, K):
     rng = np.random.default_rng(31 + M)
     A, lda, B, ldb, C, ldc = make_case(rng, kind, order, ta, tb, M, N, K)
     alpha, beta = ((1.5, -0.25) if kind == "d" else ((1 + 0.5j), (0.5 - 0.25j)))
-    kk = K if kind == "d" else 2 * K
-    nmod, bb = crt_plan(kk, 0)
+    if kind == "d":
+        nmod, bb = crt_plan_rows(K, 0)
+    else:
+        nmod, bb = crt_plan(2 * K, 0)
     assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, 0) == 0
     try:
         dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
@@ -334,8 +380,8 @@ def test_crt_combine_many_tiles_per_block(handle, kind, order, ta, tb, M, N, K):
         hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
     _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
     err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
-    bound = (crt_bound if kind == "d" else zcrt_bound)(order, ta, tb, M, N, K, alpha, A, lda, B,
-                                                        ldb, bb, ref, beta, C, ldc)
+    bound = (crt_bound_rows if kind == "d" else zcrt_bound)(order, ta, tb, M, N, K, alpha, A, lda,
+                                                             B, ldb, bb, ref, beta, C, ldc)
     assert err <= bound, (kind, nmod, bb, err, bound)
 
 
