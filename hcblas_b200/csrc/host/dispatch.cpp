@@ -414,9 +414,13 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!crt_plan_rows(a->k, want, &nmod, &shift, &norm)) return HCBK_ERR_ARGS;
   const int beta_bits = 53;
   const int *mods = hcbk_crt_moduli(nullptr);
-  const int64_t kp = (a->k + 7) & ~int64_t(7); /* 16-byte f16 row pitch */
+  /* int8 residues on kind::i8 (INT32 sums exact over all of K) unless K is
+   * too long for them or the knob asks for the binary16 path */
+  const bool i8 = st->crt_i8 && a->k <= HCBK_CRT_I8_MAX_K;
+  const int esz = i8 ? 1 : 2;
+  const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for both element sizes */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
-  const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
+  const size_t a_pl = up1k((size_t)a->m * kp * esz), b_pl = up1k((size_t)a->n * kp * esz);
   const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
   const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
@@ -480,6 +484,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   ra.planes = pa_base;
   ra.plane_stride = (int64_t)a_pl;
   ra.ld_dst = kp;
+  ra.i8 = i8 ? 1 : 0;
   hcbk_crt_prep rb = ra;
   rb.src = eb.src;
   rb.ld = eb.ld;
@@ -515,6 +520,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   g.t_plane_stride = (int64_t)(t_pl / 2);
   g.pair = pair;
   g.bn = bn;
+  g.i8 = i8 ? 1 : 0;
   if (st->autotune && st->tc_pair == 1) {
     /* every candidate writes the same exact residues: tuning in place is safe */
     static const int cbn[3] = {128, 256, 256}, cpair[3] = {0, 0, 1};
@@ -657,6 +663,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
     g.t_plane_stride = (int64_t)(t_pl / 2);
     g.pair = pair;
     g.bn = bn;
+    g.i8 = 0; /* binary16 residue planes (hcbk_zcrt_residues) */
     rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   }
   if (rc) return rc;

@@ -421,6 +421,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->tc_pair = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "crt_i8") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->crt_i8 = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   return HCBLAS_STATUS_INVALID_VALUE;
 }
 

@@ -59,6 +59,7 @@ struct HcblasB200State {
   int math_param = 0;  /* terms (split-BF16) or slices (Ozaki) */
   int split_promote_kb = 1; /* split-BF16: K-slabs per TMEM chunk (tuning knob) */
   int tc_pair = 1; /* CTA-pair (cta_group::2) tensor-core kernels: 0 never, 1 auto, 2 always */
+  int crt_i8 = 1;  /* CRT DGEMM modular GEMMs: 1 int8 residues on kind::i8, 0 binary16 */
   int ozaki_default_slices = 7; /* Ozaki slices when the mode's param is 0 */
   const char *last_path = "none";
   /* device workspace owned by the handle (grown on demand, freed at destroy) */

@@ -199,9 +199,19 @@ __device__ __forceinline__ __half2 residue2_h(const Limbs2 &L, const ModPair &m)
   return to_h2(residue2(L, m));
 }
 
-/* K-contiguous source: 8 consecutive k per thread, 16-byte plane stores */
+/* the residue pair (|r| <= 127) as two int8 in the low 16 bits: the low
+ * byte of the 1.5 * 2^23 + r pattern is r in two's complement */
+__device__ __forceinline__ uint32_t residue2_s8(const Limbs2 &L, const ModPair &m) {
+  const float2 f = upk2(add2(residue2(L, m), pk2(RND_F, RND_F)));
+  return __byte_perm(__float_as_uint(f.x), __float_as_uint(f.y), 0x0040);
+}
+
+/* K-contiguous source: 8 consecutive k per thread, 16-byte (binary16) or
+ * 8-byte (int8) plane stores */
+template <bool I8>
 __global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
   struct alignas(16) H8 { __half2 v[4]; };
+  constexpr int ESZ = I8 ? 1 : 2;
   const int64_t kq = (a.kdim + 7) / 8;
   const int64_t total = a.rows * kq;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -223,25 +233,41 @@ __global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
     for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
       if (i >= a.nmod) break;
       const ModPair m = a.mp[i];
-      H8 out;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) out.v[j] = residue2_h(L2[j], m);
-      __half *d = reinterpret_cast<__half *>(a.planes + i * a.plane_stride) + r * a.ld_dst + k0;
-      if (k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
-        *reinterpret_cast<H8 *>(d) = out;
+      char *d = a.planes + i * a.plane_stride + (r * a.ld_dst + k0) * ESZ;
+      const bool whole = k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & (8 * ESZ - 1)) == 0;
+      if constexpr (I8) {
+        uint2 out;
+        out.x = __byte_perm(residue2_s8(L2[0], m), residue2_s8(L2[1], m), 0x5410);
+        out.y = __byte_perm(residue2_s8(L2[2], m), residue2_s8(L2[3], m), 0x5410);
+        if (whole) {
+          *reinterpret_cast<uint2 *>(d) = out;
+        } else {
+          const int8_t *h = reinterpret_cast<const int8_t *>(&out);
+          for (int j = 0; j < 8; ++j)
+            if (k0 + j < a.kdim) reinterpret_cast<int8_t *>(d)[j] = h[j];
+        }
       } else {
-        const __half *h = reinterpret_cast<const __half *>(&out);
-        for (int j = 0; j < 8; ++j)
-          if (k0 + j < a.kdim) d[j] = h[j];
+        H8 out;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out.v[j] = residue2_h(L2[j], m);
+        if (whole) {
+          *reinterpret_cast<H8 *>(d) = out;
+        } else {
+          const __half *h = reinterpret_cast<const __half *>(&out);
+          for (int j = 0; j < 8; ++j)
+            if (k0 + j < a.kdim) reinterpret_cast<__half *>(d)[j] = h[j];
+        }
       }
     }
   }
 }
 
 /* MN-contiguous source: 32x32 tile through shared memory; each thread then
- * owns four consecutive k of one row (8-byte plane stores; eight threads
- * write one row's 64 contiguous bytes) */
+ * owns four consecutive k of one row (8-byte binary16 or 4-byte int8 plane
+ * stores; eight threads write one row's 64 or 32 contiguous bytes) */
+template <bool I8>
 __global__ void crt_res_rcontig(ResArgs a) {
+  constexpr int ESZ = I8 ? 1 : 2;
   __shared__ double tile[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
   const int64_t k0 = (int64_t)blockIdx.y * 32;
@@ -266,12 +292,23 @@ __global__ void crt_res_rcontig(ResArgs a) {
                        limbs_of(f * tile[kq + 2 * j + 1][rl], e, a.beta));
   const int64_t left = a.kdim - k;
   const int nk = left < 4 ? (int)left : 4;
-  char *d0 = a.planes + (r * a.ld_dst + k) * (int64_t)sizeof(__half);
-  const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & 7) == 0 && (a.plane_stride & 7) == 0;
+  char *d0 = a.planes + (r * a.ld_dst + k) * (int64_t)ESZ;
+  const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & (4 * ESZ - 1)) == 0 &&
+                   (a.plane_stride & (4 * ESZ - 1)) == 0;
 #pragma unroll
   for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
     if (i >= a.nmod) break;
     const ModPair m = a.mp[i];
+    if constexpr (I8) {
+      const uint32_t w = __byte_perm(residue2_s8(L2[0], m), residue2_s8(L2[1], m), 0x5410);
+      int8_t *d = reinterpret_cast<int8_t *>(d0 + i * a.plane_stride);
+      if (vec) {
+        *reinterpret_cast<uint32_t *>(d) = w;
+      } else {
+        for (int j = 0; j < nk; ++j) d[j] = (int8_t)(w >> (8 * j));
+      }
+      continue;
+    }
     __half2 v[2];
     v[0] = residue2_h(L2[0], m);
     v[1] = residue2_h(L2[1], m);
@@ -918,11 +955,17 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    crt_res_kcontig<<<(unsigned)blocks, 256, 0, st>>>(a);
+    if (in->i8)
+      crt_res_kcontig<true><<<(unsigned)blocks, 256, 0, st>>>(a);
+    else
+      crt_res_kcontig<false><<<(unsigned)blocks, 256, 0, st>>>(a);
   } else {
     const int64_t gx = (a.rows + 31) / 32, gy = (a.kdim + 31) / 32;
     if (gy > 65535) return HCBK_ERR_ARGS;
-    crt_res_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+    if (in->i8)
+      crt_res_rcontig<true><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+    else
+      crt_res_rcontig<false><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -223,8 +223,9 @@ const int *hcbk_crt_moduli(int *count);
 
 /* Residues of the scaled integer operand: for row r (exponent exps[r], from
  * hcbk_ozaki_exponents) A'(r,k) = rint(x(r,k) * 2^(beta_bits - exps[r])) and
- * plane i holds the symmetric residue A' mod moduli[i] as binary16 at
- * [r*ld_dst + k] (planes plane_stride bytes apart). */
+ * plane i holds the symmetric residue A' mod moduli[i] (|r| <= 127) as
+ * binary16, or as int8 when i8 is set, at [r*ld_dst + k] (planes
+ * plane_stride bytes apart). */
 typedef struct hcbk_crt_prep {
   const double *src;
   int64_t ld;
@@ -237,14 +238,19 @@ typedef struct hcbk_crt_prep {
   void *planes;
   int64_t plane_stride; /* bytes */
   int64_t ld_dst;       /* elements */
+  int i8;               /* 1: int8 planes (hcbk_crt_gemm's i8 path), 0: binary16 */
 } hcbk_crt_prep;
 int hcbk_crt_residues(const hcbk_crt_prep *a, void *stream);
 
 /* All moduli in one launch: plane i of T = A_res_i * B_res_i mod moduli[i]
- * on the f16 tensor path, written as symmetric int16 residues (column-major
+ * on the tensor cores, written as symmetric int16 residues (column-major
  * M x N, leading dimension ldt, planes t_plane_stride elements apart).
- * Residue planes: M (resp. N) rows x ld_a (ld_b) f16, K contiguous, planes
- * a_plane_stride (b_plane_stride) bytes apart. */
+ * Residue planes: M (resp. N) rows x ld_a (ld_b) elements, K contiguous,
+ * planes a_plane_stride (b_plane_stride) bytes apart; f16 elements
+ * (kind::f16, sums reduced mod p every 1024 K), or int8 when i8 is set
+ * (kind::i8, INT32 sums exact over the whole K, which must then be at most
+ * HCBK_CRT_I8_MAX_K). */
+#define HCBK_CRT_I8_MAX_K 131072 /* 131072 * 127^2 < 2^31 */
 typedef struct hcbk_crt_gemm {
   int64_t m, n, k;
   const void *a_planes;
@@ -257,6 +263,7 @@ typedef struct hcbk_crt_gemm {
   int64_t ldt, t_plane_stride;      /* elements, multiples of 8 */
   int bn;   /* tile columns: 128 or 256 */
   int pair; /* 1: CTA pairs, 256 x 256 tiles (bn = 256) */
+  int i8;   /* 1: int8 residue planes on kind::i8 */
 } hcbk_crt_gemm;
 int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
 

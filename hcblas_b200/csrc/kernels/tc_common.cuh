@@ -288,6 +288,17 @@ __device__ __forceinline__ void mma_f16_pair(uint32_t d_tmem, uint64_t adesc, ui
       : "memory");
 }
 
+/* The pair MMA with 8-bit integer operands and an s32 accumulator. */
+__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 /* Arrive once on the mbarrier at this shared-memory offset in every CTA of
  * `cta_mask` when all prior pair MMAs of this thread have completed. */
 __device__ __forceinline__ void mma_commit_pair(uint64_t *bar, uint16_t cta_mask) {

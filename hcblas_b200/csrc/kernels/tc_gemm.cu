@@ -426,6 +426,71 @@ struct EpiModP {
   }
 };
 
+/* Modular epilogue of the int8 path: the INT32 accumulator holds the
+ * exact sum over all of K (|s| <= K 127^2 < 2^31), reduced once per tile:
+ * s = hi 2^16 + lo (hi = s >> 16, 0 <= lo < 2^16) turns into the f32-exact
+ * y = hi (2^16 mod p) + lo, |y| < 2^15 127 + 2^16 < 2^23, whose remainder
+ * comes from the same rounding-constant quotient as the f16 path; stored as
+ * symmetric int16 residues by TMA tensor stores. */
+struct EpiModPi8 {
+  static constexpr bool INPLACE = false;
+  static constexpr bool PLANE_BATCH = true;
+  static constexpr float RND = 12582912.0f; /* 1.5 * 2^23 */
+  static constexpr uint32_t OUT_BOX_BYTES = EpiModP::OUT_BOX_BYTES;
+  static constexpr uint32_t OUT_WARP_BYTES = EpiModP::OUT_WARP_BYTES;
+  static constexpr uint32_t OUT_SMEM = EpiModP::OUT_SMEM;
+
+  template <int BN>
+  static __device__ __forceinline__ void prefetch_c(const TcParams &, int, int, OutStage &) {}
+
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void run(const TcParams &, uint32_t, int, int, OutStage &) {
+    static_assert(NACC == 0, "the modular epilogue stores through final_store");
+  }
+
+  /* |v| < 2^22 to f32 through the 1.5 * 2^23 bit pattern */
+  static __device__ __forceinline__ float small_to_f(int v) {
+    return __int_as_float(0x4B400000 + v) - RND;
+  }
+
+  template <int BN>
+  static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint8_t *out,
+                                                     int m0, int n0, int plane) {
+    const int lane = threadIdx.x & 31;
+    const int mod = p.mod_tab[plane];
+    const float pf = static_cast<float>(mod);
+    const float inv = p.inv_mod_tab[plane];
+    const float hp = static_cast<float>((mod - 1) >> 1);
+    int c16 = (1 << 16) % mod; /* 2^16 mod p, symmetric */
+    if (c16 > (mod - 1) / 2) c16 -= mod;
+    const float c16f = static_cast<float>(c16);
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32) {
+      int16_t *box = reinterpret_cast<int16_t *>(out + ((c >> 5) & 1) * OUT_BOX_BYTES);
+      uint32_t ra[32];
+      tmem_ld_32x32b_x32(ta + c, ra);
+      if (lane == 0) bulk_wait_read<1>(); /* the store from this box two groups ago */
+      __syncwarp();
+      tmem_ld_wait();
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int sv = static_cast<int>(ra[j]);
+        const float y = fmaf(small_to_f(sv >> 16), c16f, small_to_f(sv & 0xFFFF));
+        float v = EpiModP::mod_f(y, pf, inv);
+        if (v > hp) v -= pf;
+        else if (v < -hp) v += pf;
+        box[j * 32 + lane] = static_cast<int16_t>(__float_as_int(v + RND));
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_3d(&p.tc, box, m0, n0 + c, plane);
+        bulk_commit();
+      }
+    }
+  }
+};
+
 /* 2^e built from its binary64 bit pattern (exact; normal range
  * -1022 <= e <= 1023 only).  Deliberately not recursive: device recursion
  * consumes the (1 KB default) call stack. */
@@ -511,6 +576,10 @@ template <> struct KindTraits<1> { /* bf16, 128-byte swizzle */
 template <> struct KindTraits<2> { /* s8 -> s32, 64-byte swizzle */
   static constexpr int ROWB = 64, BKE = 64, UK = 32, ESZ = 1;
   static constexpr uint32_t CFMT = 2, ABFMT = 1, LAYOUT = 4, SBO = 512;
+};
+template <> struct KindTraits<3> { /* s8 -> s32, 128-byte swizzle: 128 K per slab */
+  static constexpr int ROWB = 128, BKE = 128, UK = 32, ESZ = 1;
+  static constexpr uint32_t CFMT = 2, ABFMT = 1, LAYOUT = 2, SBO = 1024;
 };
 
 __host__ __device__ constexpr uint32_t tmem_cols_for(uint32_t c) {
@@ -786,8 +855,10 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
                 const uint64_t ad = smem_desc(aa, a_lbo, KT::SBO, KT::LAYOUT);
                 const uint64_t bd = smem_desc(ba, b_lbo, KT::SBO, KT::LAYOUT);
                 const uint32_t acc = (!fresh || kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
-                if constexpr (KIND == 2)
+                if constexpr (KIND == 2 || (KIND == 3 && CG == 1))
                   mma_i8(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
+                else if constexpr (KIND == 3)
+                  mma_i8_pair(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
                 else if constexpr (CG == 2)
                   mma_f16_pair(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
                 else
@@ -872,7 +943,10 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         tc_fence_after();
         const uint32_t tbase =
             tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS;
-        EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN, ostage);
+        if constexpr (EPI::PLANE_BATCH)
+          EPI::template final_store<BN>(p, tbase, ostage.box, m - lane, tn * BN, plane);
+        else
+          EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN, ostage);
         tc_fence_before();
         __syncwarp();
         release(b);
@@ -1231,14 +1305,14 @@ extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stre
  * plane pitch pstride bytes; box {64, box_rows, 1}, 128-byte swizzle. */
 static int make_map_planes(CUtensorMap *map, CUtensorMapDataType dt, const void *base,
                            uint64_t kdim, uint64_t rows, uint64_t planes, uint64_t ld,
-                           uint64_t pstride, uint32_t box_rows) {
+                           uint64_t pstride, uint32_t box_rows, uint32_t esz = 2) {
   auto fn = encode_fn();
   if (!fn) return HCBK_ERR_DRIVER;
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || (pstride & 15))
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * esz) & 15) || (pstride & 15))
     return HCBK_ERR_ALIGN;
   cuuint64_t dims[3] = {kdim, rows, planes};
-  cuuint64_t strides[2] = {ld * 2, pstride};
-  cuuint32_t box[3] = {64, box_rows, 1};
+  cuuint64_t strides[2] = {ld * esz, pstride};
+  cuuint32_t box[3] = {128 / esz, box_rows, 1}; /* one 128-byte swizzle row of K */
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -1250,6 +1324,13 @@ static int make_map_planes_f16(CUtensorMap *map, const void *base, uint64_t kdim
                                uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
   return make_map_planes(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, base, kdim, rows, planes, ld,
                          pstride, box_rows);
+}
+
+/* int8 residue planes: box {128, box_rows, 1} (one 128-byte swizzle row) */
+static int make_map_planes_s8(CUtensorMap *map, const void *base, uint64_t kdim, uint64_t rows,
+                              uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
+  return make_map_planes(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, base, kdim, rows, planes, ld,
+                         pstride, box_rows, 1);
 }
 
 extern "C" int hcbk_encode_tma_3d_planes(void *map, int bf16, const void *base, uint64_t kdim,
@@ -1293,17 +1374,17 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
     return HCBK_ERR_ARGS;
   for (int i = 0; i < g->nmod; ++i)
     if (g->moduli[i] < 3 || g->moduli[i] > 255 || (g->moduli[i] & 1) == 0) return HCBK_ERR_ARGS;
+  if (g->i8 && g->k > HCBK_CRT_I8_MAX_K) return HCBK_ERR_ARGS;
   TcParams p;
   memset(&p, 0, sizeof(p));
   p.m = (int)g->m;
   p.n = (int)g->n;
   p.k = (int)g->k;
-  int rc = make_map_planes_f16(&p.ta[0], g->a_planes, g->k, g->m, g->nmod, g->ld_a,
-                               g->a_plane_stride, BM);
+  auto planes_map = g->i8 ? make_map_planes_s8 : make_map_planes_f16;
+  int rc = planes_map(&p.ta[0], g->a_planes, g->k, g->m, g->nmod, g->ld_a, g->a_plane_stride, BM);
   if (rc) return rc;
   const uint32_t b_rows = g->pair ? g->bn / 2 : g->bn; /* B rows per CTA */
-  rc = make_map_planes_f16(&p.tb[0], g->b_planes, g->k, g->n, g->nmod, g->ld_b, g->b_plane_stride,
-                           b_rows);
+  rc = planes_map(&p.tb[0], g->b_planes, g->k, g->n, g->nmod, g->ld_b, g->b_plane_stride, b_rows);
   if (rc) return rc;
   p.c = g->t;
   p.ldc = g->ldt;
@@ -1316,6 +1397,11 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
     p.inv_mod_tab[i] = 1.0f / (float)g->moduli[i];
   }
   p.err = err;
+  if (g->i8) {
+    if (g->pair) return launch_tc<256, 6, RecipeSingle, 3, EpiModPi8, 0, 2, 2>(p, stream);
+    if (g->bn == 256) return launch_tc<256, 4, RecipeSingle, 3, EpiModPi8, 0, 2>(p, stream);
+    return launch_tc<128, 6, RecipeSingle, 3, EpiModPi8, 0, 2>(p, stream);
+  }
   if (g->pair) return launch_tc<256, 6, RecipeSingle, 0, EpiModP, 16, 2, 2>(p, stream);
   if (g->bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);
   return launch_tc<128, 6, RecipeSingle, 0, EpiModP, 16, 2>(p, stream);

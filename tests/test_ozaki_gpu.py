@@ -258,6 +258,25 @@ def test_crt_pair_matches_single_cta(handle):
         assert np.array_equal(outs[0], outs[1]), (order, ta, tb, M, N, K)
 
 
+@pytest.mark.parametrize("want", [0, 14])
+def test_crt_i8_matches_f16(handle, want):
+    """The int8 (kind::i8, INT32 sums over all of K) and binary16 (kind::f16,
+    sums reduced mod p every 1024 K) modular GEMMs both produce the exact
+    residues, so the two paths must give bit-identical results."""
+    rng = np.random.default_rng(77 + want)
+    for order, ta, tb, M, N, K in CRT_CASES + [(O.COL, 1, 0, 130, 70, 129)]:
+        A, lda, B, ldb, C, ldc = make_case(rng, "d", order, ta, tb, M, N, K)
+        outs = []
+        for i8 in (1, 0):
+            assert hb.set_tuning(handle, "crt_i8", i8) == 0
+            try:
+                outs.append(run_crt(handle, want, order, ta, tb, M, N, K, 1.5, -0.25, A, lda, B,
+                                    ldb, C, ldc)[0])
+            finally:
+                hb.set_tuning(handle, "crt_i8", 1)
+        assert np.array_equal(outs[0], outs[1]), (want, order, ta, tb, M, N, K)
+
+
 def test_crt_special_and_hard_range(handle):
     rng = np.random.default_rng(12)
     M, N, K = 96, 80, 700
