@@ -580,8 +580,9 @@ def main():
                          "frac": round(achieved / peak, 4) if achieved else None,
                          "peak_source": (f"2 x {peak_src} dense bf16 burst (MEASURED_PEAKS.json "
                                          f"bf16_tflops): the modular GEMMs run kind::i8, whose "
-                                         f"dense rate is twice kind::f16's (2.05x in an "
-                                         f"issue-rate probe; profiles/tc_gemm_crt_modgemm_i8_"
+                                         f"nominal dense rate is twice kind::f16's (4.5 vs 2.25 "
+                                         f"POPS); cuBLASLt's int8 GEMM at 8192^3 measures 2800 "
+                                         f"TOPS on this part (profiles/tc_gemm_crt_modgemm_i8_"
                                          f"pair_nt_4096.md)")
                                         if dom == "tc.crt_modgemm" else
                                         f"{peak_src} dense bf16 burst (MEASURED_PEAKS.json "

@@ -571,9 +571,11 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   int nmod = 0, beta_bits = 0;
   if (!crt_plan(2 * a->k, want, &nmod, &beta_bits)) return HCBK_ERR_ARGS;
   const int *mods = hcbk_crt_moduli(nullptr);
-  const int64_t kp = (a->k + 7) & ~int64_t(7);
+  const bool i8 = st->crt_i8 && a->k <= HCBK_CRT_I8_MAX_K; /* as in dgemm_crt */
+  const int esz = i8 ? 1 : 2;
+  const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for both element sizes */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
-  const size_t a_pl = up1k((size_t)a->m * kp * 2), b_pl = up1k((size_t)a->n * kp * 2);
+  const size_t a_pl = up1k((size_t)a->m * kp * esz), b_pl = up1k((size_t)a->n * kp * esz);
   const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
   const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   /* the real view of an MN-contiguous operand has two real rows per row */
@@ -627,6 +629,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   ra.planes = pa_base;
   ra.plane_stride = (int64_t)a_pl;
   ra.ld_dst = kp;
+  ra.i8 = i8 ? 1 : 0;
   hcbk_zcrt_prep rb = ra;
   rb.src = static_cast<const char *>(a->b) + 16 * a->b_off;
   rb.ld = a->ldb;
@@ -663,7 +666,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
     g.t_plane_stride = (int64_t)(t_pl / 2);
     g.pair = pair;
     g.bn = bn;
-    g.i8 = 0; /* binary16 residue planes (hcbk_zcrt_residues) */
+    g.i8 = i8 ? 1 : 0;
     rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   }
   if (rc) return rc;

@@ -199,11 +199,16 @@ __device__ __forceinline__ __half2 residue2_h(const Limbs2 &L, const ModPair &m)
   return to_h2(residue2(L, m));
 }
 
-/* the residue pair (|r| <= 127) as two int8 in the low 16 bits: the low
- * byte of the 1.5 * 2^23 + r pattern is r in two's complement */
-__device__ __forceinline__ uint32_t residue2_s8(const Limbs2 &L, const ModPair &m) {
-  const float2 f = upk2(add2(residue2(L, m), pk2(RND_F, RND_F)));
+/* a pair of small integers (|r| <= 127, f32x2) as two int8 in the low 16
+ * bits: the low byte of the 1.5 * 2^23 + r pattern is r in two's complement */
+__device__ __forceinline__ uint32_t to_s8x2(uint64_t r) {
+  const float2 f = upk2(add2(r, pk2(RND_F, RND_F)));
   return __byte_perm(__float_as_uint(f.x), __float_as_uint(f.y), 0x0040);
+}
+
+/* the residue pair as two int8 */
+__device__ __forceinline__ uint32_t residue2_s8(const Limbs2 &L, const ModPair &m) {
+  return to_s8x2(residue2(L, m));
 }
 
 /* K-contiguous source: 8 consecutive k per thread, 16-byte (binary16) or
@@ -734,8 +739,11 @@ __device__ __forceinline__ ZRes3 zresidue(const Limbs &lr, const Limbs &li, cons
 
 /* K-contiguous complex source: 4 consecutive k per thread (40 limb
  * registers), residues of element pairs by packed f32x2 arithmetic with the
- * moduli constants as constant-bank operands, 8-byte stores per plane */
+ * moduli constants as constant-bank operands, 8-byte (binary16) or 4-byte
+ * (int8) stores per plane */
+template <bool I8>
 __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
+  constexpr int ESZ = I8 ? 1 : 2;
   const int64_t kq = (a.kdim + 3) / 4;
   const int64_t total = a.rows * kq;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -756,12 +764,34 @@ __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
     }
     const int64_t left = a.kdim - k0;
     const int nk = left < 4 ? (int)left : 4;
-    char *d0 = a.planes + (r * a.ld_dst + k0) * (int64_t)sizeof(__half);
-    const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & 7) == 0 && (a.plane_stride & 7) == 0;
+    char *d0 = a.planes + (r * a.ld_dst + k0) * (int64_t)ESZ;
+    const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & (4 * ESZ - 1)) == 0 &&
+                     (a.plane_stride & (4 * ESZ - 1)) == 0;
 #pragma unroll
     for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
       if (i >= a.nmod) break;
       const ModPair m = a.mp[i];
+      if constexpr (I8) {
+        uint32_t w[3][2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const uint64_t re = residue2(lr[j], m), im = residue2(li[j], m);
+          w[0][j] = to_s8x2(re);
+          w[1][j] = to_s8x2(im);
+          w[2][j] = to_s8x2(mod2(add2(re, im), m));
+        }
+#pragma unroll
+        for (int set = 0; set < 3; ++set) {
+          const uint32_t v = __byte_perm(w[set][0], w[set][1], 0x5410);
+          int8_t *d = reinterpret_cast<int8_t *>(d0 + (set * a.nmod + i) * a.plane_stride);
+          if (vec) {
+            *reinterpret_cast<uint32_t *>(d) = v;
+          } else {
+            for (int j = 0; j < nk; ++j) d[j] = (int8_t)(v >> (8 * j));
+          }
+        }
+        continue;
+      }
       __half2 o[3][2];
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
@@ -787,8 +817,11 @@ __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
   }
 }
 
-/* MN-contiguous complex source: 32x32 tile through shared memory */
+/* MN-contiguous complex source: 32x32 tile through shared memory; two
+ * consecutive k per thread (binary16 or int8 planes) */
+template <bool I8>
 __global__ void zcrt_res_rcontig(ZResArgs a) {
+  constexpr int ESZ = I8 ? 1 : 2;
   __shared__ double2 tile[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
   const int64_t k0 = (int64_t)blockIdx.y * 32;
@@ -811,14 +844,31 @@ __global__ void zcrt_res_rcontig(ZResArgs a) {
     const Limbs r0l = limbs_of(z0.x, e, a.beta), i0l = limbs_of(z0.y, e, a.beta);
     const Limbs r1l = limbs_of(z1.x, e, a.beta), i1l = limbs_of(z1.y, e, a.beta);
     const bool two = k + 1 < a.kdim;
-    const bool vec = two && (a.plane_stride & 3) == 0 &&
-                     (reinterpret_cast<uintptr_t>(a.planes + (r * a.ld_dst + k) * 2) & 3) == 0;
+    const bool vec = two && (a.plane_stride & (2 * ESZ - 1)) == 0 &&
+                     (reinterpret_cast<uintptr_t>(a.planes + (r * a.ld_dst + k) * ESZ) &
+                      (2 * ESZ - 1)) == 0;
 #pragma unroll
     for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
       if (i >= a.nmod) break;
       const ModConst m = a.mc[i];
       const ZRes3 x0 = zresidue(r0l, i0l, m, a.im_sign);
       const ZRes3 x1 = zresidue(r1l, i1l, m, a.im_sign);
+      if constexpr (I8) {
+        const uint32_t w[3] = {to_s8x2(pk2(x0.re, x1.re)), to_s8x2(pk2(x0.im, x1.im)),
+                               to_s8x2(pk2(x0.sum, x1.sum))};
+#pragma unroll
+        for (int set = 0; set < 3; ++set) {
+          int8_t *d = reinterpret_cast<int8_t *>(a.planes + (set * a.nmod + i) * a.plane_stride) +
+                      r * a.ld_dst + k;
+          if (vec) {
+            *reinterpret_cast<uint16_t *>(d) = (uint16_t)w[set];
+          } else {
+            d[0] = (int8_t)w[set];
+            if (two) d[1] = (int8_t)(w[set] >> 8);
+          }
+        }
+        continue;
+      }
       const __half2 v[3] = {__floats2half2_rn(x0.re, x1.re), __floats2half2_rn(x0.im, x1.im),
                             __floats2half2_rn(x0.sum, x1.sum)};
 #pragma unroll
@@ -1039,11 +1089,17 @@ extern "C" int hcbk_zcrt_residues(const hcbk_zcrt_prep *in, void *stream) {
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 12;
     if (blocks > cap) blocks = cap;
-    zcrt_res_kcontig<<<(unsigned)blocks, 256, 0, st>>>(a);
+    if (in->i8)
+      zcrt_res_kcontig<true><<<(unsigned)blocks, 256, 0, st>>>(a);
+    else
+      zcrt_res_kcontig<false><<<(unsigned)blocks, 256, 0, st>>>(a);
   } else {
     const int64_t gx = (a.rows + 31) / 32, gy = (a.kdim + 31) / 32;
     if (gy > 65535) return HCBK_ERR_ARGS;
-    zcrt_res_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+    if (in->i8)
+      zcrt_res_rcontig<true><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+    else
+      zcrt_res_rcontig<false><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

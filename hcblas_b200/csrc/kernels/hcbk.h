@@ -309,6 +309,7 @@ typedef struct hcbk_zcrt_prep {
   void *planes;
   int64_t plane_stride; /* bytes */
   int64_t ld_dst;       /* elements */
+  int i8;               /* 1: int8 planes (hcbk_crt_gemm's i8 path), 0: binary16 */
 } hcbk_zcrt_prep;
 int hcbk_zcrt_residues(const hcbk_zcrt_prep *a, void *stream);
 

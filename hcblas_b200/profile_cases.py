@@ -135,6 +135,32 @@ def _ger(h, dtype, m, n, seed=7):
     return call, (dA, dx, dy)
 
 
+def _cublas_int8(h, n=8192, reps=20):
+    """Reference rate of the int8 tensor cores: cuBLASLt's int8 GEMM
+    (torch._int_mm, s8 x s8 -> s32, n^3, uniform s8 data), timed with CUDA
+    events over `reps` back-to-back calls; prints TOPS.  Library code, not
+    part of this library's paths."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(11)
+    a = torch.randint(-127, 128, (n, n), device="cuda", dtype=torch.int8, generator=g)
+    b = torch.randint(-127, 128, (n, n), device="cuda", dtype=torch.int8, generator=g)
+    bt = b.t().contiguous().t()
+
+    def call():
+        for _ in range(3):
+            torch._int_mm(a, bt)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            torch._int_mm(a, bt)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        print(f"cublas int8 {n}^3: {ms:.4f} ms -> {2 * n ** 3 / ms / 1e9:.1f} TOPS", flush=True)
+    return call, (a, bt)
+
+
 CASES = {
     "hgemm_nt_8192": lambda h: _real(h, np.float16, N_, T_, 8192, 8192, 8192),
     "hgemm_nt_8192_beta05": lambda h: _real(h, np.float16, N_, T_, 8192, 8192, 8192, beta=0.5),
@@ -147,6 +173,8 @@ CASES = {
     "sgemm_split3_tn_4096": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096, 1, 3),
     "dgemm_native_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096),
     "dgemm_crt15_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096, 4, 15),
+    "dgemm_crt14_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096, 4, 14),
+    "cublas_int8_8192": _cublas_int8,
     "cgemm_plain_cn_2048": lambda h: _complex(h, np.complex64, C_, N_, 2048, 2048, 2048),
     "cgemm_split3m_cn_2048": lambda h: _complex(h, np.complex64, C_, N_, 2048, 2048, 2048, 1, 6),
     "zgemm_native_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048),

@@ -424,7 +424,7 @@ hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
  *                       kernels (tcgen05 cta_group::2, 256-row tiles over two
  *                       SMs): 0 never, 1 when the problem fills every SM pair
  *                       (default), 2 always.
- *   "crt_i8"            CRT DGEMM (HCBLAS_MATH_OZAKI_CRT): 1 (default) int8
+ *   "crt_i8"            CRT DGEMM / ZGEMM (HCBLAS_MATH_OZAKI_CRT): 1 (default) int8
  *                       residue planes on the int8 tensor cores with INT32
  *                       sums exact over all of K (K <= 131072, else as 0);
  *                       0 binary16 residue planes on the f16 tensor cores,

@@ -374,6 +374,29 @@ def test_zgemm_crt_vs_dd_oracle(handle, want):
         assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
 
 
+def test_zgemm_crt_i8_matches_f16(handle):
+    """Complex CRT: int8 and binary16 residue planes give the same exact
+    modular products, hence bit-identical results."""
+    rng = np.random.default_rng(707)
+    for order, ta, tb, M, N, K in ZCASES:
+        A, lda, B, ldb, C, ldc = make_case(rng, "z", order, ta, tb, M, N, K)
+        alpha, beta = (1 + 0.5j), (0.5 - 0.25j)
+        outs = []
+        for i8 in (1, 0):
+            assert hb.set_tuning(handle, "crt_i8", i8) == 0
+            assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, 0) == 0
+            try:
+                dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+                assert hb.lib_gemm(handle, order, TCH[ta], TCH[tb], M, N, K, alpha, dA, lda, dB,
+                                   ldb, beta, dC, ldc) == 0
+                assert hb.device_error(handle) == 0
+                outs.append(dC.download())
+            finally:
+                hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+                hb.set_tuning(handle, "crt_i8", 1)
+        assert np.array_equal(outs[0], outs[1]), (order, ta, tb, M, N, K)
+
+
 @pytest.mark.parametrize("kind,order,ta,tb,M,N,K", [("d", O.COL, 0, 1, 1001, 3000, 40),
                                                     ("d", O.ROW, 1, 0, 700, 2600, 24),
                                                     ("z", O.COL, 2, 0, 520, 1500, 24)])
