@@ -425,8 +425,9 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const size_t t_pl = up1k((size_t)ldt * a->n * 2);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
   const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
-  const size_t fa_bytes = norm ? up1k(sizeof(double) * a->m) : 0;
-  const size_t fb_bytes = norm ? up1k(sizeof(double) * a->n) : 0;
+  /* per row: the fraction and its reciprocal */
+  const size_t fa_bytes = norm ? up1k(2 * sizeof(double) * a->m) : 0;
+  const size_t fb_bytes = norm ? up1k(2 * sizeof(double) * a->n) : 0;
   const size_t wa_bytes =
       norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a->m, a->k, a_k)) : 0;
   const size_t wb_bytes =
@@ -440,6 +441,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
   double *frac_a = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes) : nullptr;
   double *frac_b = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes + fa_bytes) : nullptr;
+  double *inv_a = norm ? frac_a + a->m : nullptr;
+  double *inv_b = norm ? frac_b + a->n : nullptr;
   char *wa = ws + ea_bytes + eb_bytes + fa_bytes + fb_bytes, *wb = wa + wa_bytes;
   char *pa_base = wb + wb_bytes;
   char *pb_base = pa_base + nmod * a_pl;
@@ -461,14 +464,14 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   eb.exps = exp_b;
   /* row exponents: the row maximum's; when the moduli are too few for the
    * worst case, exponent and 8-bit fraction from the row norm instead */
-  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, char *w, size_t wbytes) {
+  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes) {
     return timed_launch(st, stream, "ozaki.exponents", [&] {
-      return norm ? hcbk_crt_row_scales(&p, 53 - shift, frac, w, (int64_t)wbytes, stream)
+      return norm ? hcbk_crt_row_scales(&p, 53 - shift, frac, inv, w, (int64_t)wbytes, stream)
                   : hcbk_ozaki_exponents(&p, stream);
     }, p.k_contig ? 1 : 2);
   };
-  int rc = exps(ea, frac_a, wa, wa_bytes);
-  if (!rc) rc = exps(eb, frac_b, wb, wb_bytes);
+  int rc = exps(ea, frac_a, inv_a, wa, wa_bytes);
+  if (!rc) rc = exps(eb, frac_b, inv_b, wb, wb_bytes);
   if (rc) return rc;
 
   hcbk_crt_prep ra;
@@ -545,8 +548,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.ldr = ldt;
   cb.exp_a = exp_a;
   cb.exp_b = exp_b;
-  cb.frac_a = frac_a;
-  cb.frac_b = frac_b;
+  cb.inv_a = inv_a;
+  cb.inv_b = inv_b;
   cb.shift = 2 * beta_bits;
   cb.c = static_cast<double *>(a->c) + a->c_off;
   cb.ldc = a->ldc;

@@ -360,7 +360,7 @@ struct CombArgs {
   int64_t ldr;
   const int *exp_a;
   const int *exp_b;
-  const double *frac_a, *frac_b; /* optional row fractions of the scaling */
+  const double *inv_a, *inv_b; /* optional reciprocals of the row fractions */
   int shift;
   double *c;
   int64_t ldc;
@@ -411,17 +411,16 @@ struct CrtAcc {
       D[k] = fma(-cy, CH, D[k]);
       D[k + 1] += cy;
     }
-    double hi = D[NC - 1], lo = 0.0;
+    /* Horner from the low chunk: with |D_k| <= 2^39 below the top chunk the
+     * partial sums stay below half the top chunk's unit, so the rounded
+     * result is within 1.5 ulp of P' */
+    double x = D[0];
+    double w = CH;
 #pragma unroll
-    for (int k = NC - 2; k >= 0; --k) {
-      hi *= CH;
-      lo *= CH;
-      const double sh = hi + D[k]; /* two-sum, exact error term */
-      const double bb = sh - hi;
-      lo += (hi - (sh - bb)) + (D[k] - bb);
-      hi = sh;
+    for (int k = 1; k < NC; ++k) {
+      x = fma(D[k], w, x);
+      w *= CH;
     }
-    const double x = hi + lo;
     const int e = ea + eb - a.shift;
     return (e >= -1022 && e <= 1023) ? x * __longlong_as_double((long long)(e + 1023) << 52)
                                      : ldexp(x, e);
@@ -516,44 +515,114 @@ constexpr int ZCMB_STAGES = 3;
 __device__ __forceinline__ int lo16(uint32_t w) { return (int)(w << 16) >> 16; }
 __device__ __forceinline__ int hi16(uint32_t w) { return (int)w >> 16; }
 
+/* Real combine, warp-specialised: warps 0-7 reconstruct 512-row tiles (two
+ * consecutive rows per thread, one 4-byte load of a residue pair per
+ * modulus), warp 8's lane 0 keeps CMB_STAGES tiles of residues in flight by
+ * 1-D bulk copies.  Per stage a `full` barrier (transaction bytes) and an
+ * `empty` barrier (one arrival per consumer warp) replace block-wide
+ * barriers, so consumer warps run up to CMB_STAGES - 1 tiles apart.  The
+ * modulus loop is unrolled over the maximum count, so every weight chunk is
+ * a constant-bank operand of its FMA.  Requires the row pitch and plane
+ * stride to be multiples of 8 elements (16 bytes). */
+constexpr int CMB_CONSUMERS = CMB_THREADS / 32;
+constexpr int CMB_BLOCK = CMB_THREADS + 32;
+
 template <int NC>
-__global__ void __launch_bounds__(CMB_THREADS) crt_combine_kernel(CombArgs a) {
+__global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_constant__ CombArgs a) {
+  using namespace hcbk::tc;
   extern __shared__ __align__(128) unsigned char cmb_smem[];
-  __shared__ double sw[HCBK_CRT_MAX_MODULI][NC];
-  __shared__ __align__(8) uint64_t full[CMB_STAGES];
-  if (blockDim.x != CMB_THREADS) { /* the tile covers CMB_ROWS rows only at this shape */
-    if (threadIdx.x == 0) atomicCAS(a.err, 0, (int)hcbk::tc::ERR_LAUNCH_SHAPE);
+  __shared__ __align__(8) uint64_t full[CMB_STAGES], empty[CMB_STAGES];
+  if (blockDim.x != CMB_BLOCK) { /* the tile covers CMB_ROWS rows only at this shape */
+    if (threadIdx.x == 0) atomicCAS(a.err, 0, (int)ERR_LAUNCH_SHAPE);
     return;
   }
-  load_weights<NC>(a, sw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = a.nmod;
-  const int tid = threadIdx.x;
-  const PipeArgs pa{a.res, a.res_plane, a.ldr, nmod, a.m, a.n, a.err};
-  combine_pipeline<CMB_STAGES, CMB_ROWS>(
-      pa, reinterpret_cast<int16_t *>(cmb_smem), full,
-      [&](const int16_t *R, int64_t r0, int64_t col) {
-        const int64_t row = r0 + CMB_RPT * tid;
-        if (row >= a.m) return;
-        CrtAcc<NC> acc[CMB_RPT];
-#pragma unroll 3
-        for (int i = 0; i < nmod; ++i) {
-          const uint32_t q = *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
-          acc[0].add(sw[i], lo16(q));
-          acc[1].add(sw[i], hi16(q));
-        }
-        const int eb = a.exp_b[col];
-        const double fb = a.frac_b ? a.frac_b[col] : 1.0;
-        double *dst = a.c + row + col * a.ldc;
+  int16_t *buf = reinterpret_cast<int16_t *>(cmb_smem);
+  const int64_t row_tiles = (a.m + CMB_ROWS - 1) / CMB_ROWS;
+  const int64_t ntiles = row_tiles * a.n;
+  const int64_t first = blockIdx.x, stride = gridDim.x;
+  const size_t stage_elems = (size_t)nmod * CMB_ROWS;
+  if (tid == 0) {
+    for (int s = 0; s < CMB_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], CMB_CONSUMERS);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  if (warp == CMB_CONSUMERS) {
+    /* ------------------------------------------------ producer -- */
+    if (lane != 0) return;
+    int64_t j = 0;
+    for (int64_t t = first; t < ntiles; t += stride, ++j) {
+      const int s = (int)(j % CMB_STAGES);
+      if (j >= CMB_STAGES &&
+          !mbar_wait(&empty[s], (uint32_t)((j / CMB_STAGES) - 1) & 1u, a.err, ERR_TIMEOUT_COMBINE))
+        break;
+      const int64_t r0 = (t % row_tiles) * CMB_ROWS, col = t / row_tiles;
+      const int64_t rows = a.ldr - r0 < CMB_ROWS ? a.ldr - r0 : CMB_ROWS;
+      const uint32_t bytes = (uint32_t)rows * 2u; /* ldr, r0 multiples of 8 */
+      mbar_expect_tx(&full[s], bytes * (uint32_t)nmod);
+      const int16_t *src = a.res + col * a.ldr + r0;
+      int16_t *dst = buf + s * stage_elems;
+      for (int p = 0; p < nmod; ++p)
+        bulk_load_1d(dst + p * CMB_ROWS, src + p * a.res_plane, bytes, &full[s]);
+    }
+    /* the last copies issued land before the block's shared memory is
+     * released (immediately when the consumers took them; bounded when a
+     * wait failed) */
+    for (int64_t k = (j > CMB_STAGES ? j - CMB_STAGES : 0); k < j; ++k) {
+      const int s = (int)(k % CMB_STAGES);
+      const uint32_t ph = (uint32_t)(k / CMB_STAGES) & 1u;
+      for (int it = 0; it < (1 << 22) && !mbar_try_wait(&full[s], ph); ++it) {
+      }
+    }
+    return;
+  }
+
+  /* ------------------------------------------------ consumers -- */
+  int64_t j = 0;
+  for (int64_t t = first; t < ntiles; t += stride, ++j) {
+    const int s = (int)(j % CMB_STAGES);
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)(j / CMB_STAGES) & 1u, a.err,
+                                           ERR_TIMEOUT_COMBINE)))
+      break;
+    const int16_t *R = buf + s * stage_elems;
+    const int64_t row = (t % row_tiles) * CMB_ROWS + CMB_RPT * tid, col = t / row_tiles;
+    if (row < a.m) {
+      CrtAcc<NC> acc[CMB_RPT];
 #pragma unroll
-        for (int u = 0; u < CMB_RPT; ++u) {
-          if (row + u >= a.m) break;
-          double v = acc[u].finish(a, a.exp_a[row + u], eb);
-          if (a.frac_a) v /= a.frac_a[row + u] * fb; /* 8-bit fractions: an exact product */
-          double o = a.alpha * v;
-          if (a.beta_nonzero) o = fma(a.beta, dst[u], o);
-          dst[u] = o;
+      for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights */
+        if (i >= nmod) break;
+        const uint32_t q = *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
+        const double r0 = small_int_to_d(lo16(q)), r1 = small_int_to_d(hi16(q));
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+          acc[0].S[k] = fma(r0, a.w[i][k], acc[0].S[k]);
+          acc[1].S[k] = fma(r1, a.w[i][k], acc[1].S[k]);
         }
-      });
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]); /* the stage's residues are in registers */
+      const int eb = a.exp_b[col];
+      const double ib = a.inv_b ? a.inv_b[col] : 1.0;
+      double *dst = a.c + row + col * a.ldc;
+#pragma unroll
+      for (int u = 0; u < CMB_RPT; ++u) {
+        if (row + u >= a.m) break;
+        double v = acc[u].finish(a, a.exp_a[row + u], eb);
+        if (a.inv_a) v *= a.inv_a[row + u] * ib;
+        double o = a.alpha * v;
+        if (a.beta_nonzero) o = fma(a.beta, dst[u], o);
+        dst[u] = o;
+      }
+    } else {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
 }
 
 /* modular inverse by the extended Euclidean algorithm */
@@ -1035,8 +1104,8 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.ldr = in->ldr;
   a.exp_a = in->exp_a;
   a.exp_b = in->exp_b;
-  a.frac_a = in->frac_a;
-  a.frac_b = in->frac_b;
+  a.inv_a = in->inv_a;
+  a.inv_b = in->inv_b;
   a.shift = in->shift;
   a.c = in->c;
   a.ldc = in->ldc;
@@ -1049,17 +1118,17 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   int64_t grid = 0;
   int rc;
   switch (a.nc) {
-    case 1: rc = combine_grid(crt_combine_kernel<1>, CMB_THREADS, smem, ntiles, &grid); break;
-    case 2: rc = combine_grid(crt_combine_kernel<2>, CMB_THREADS, smem, ntiles, &grid); break;
-    case 3: rc = combine_grid(crt_combine_kernel<3>, CMB_THREADS, smem, ntiles, &grid); break;
-    default: rc = combine_grid(crt_combine_kernel<4>, CMB_THREADS, smem, ntiles, &grid); break;
+    case 1: rc = combine_grid(crt_combine_kernel<1>, CMB_BLOCK, smem, ntiles, &grid); break;
+    case 2: rc = combine_grid(crt_combine_kernel<2>, CMB_BLOCK, smem, ntiles, &grid); break;
+    case 3: rc = combine_grid(crt_combine_kernel<3>, CMB_BLOCK, smem, ntiles, &grid); break;
+    default: rc = combine_grid(crt_combine_kernel<4>, CMB_BLOCK, smem, ntiles, &grid); break;
   }
   if (rc != HCBK_OK) return rc;
   switch (a.nc) {
-    case 1: crt_combine_kernel<1><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
-    case 2: crt_combine_kernel<2><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
-    case 3: crt_combine_kernel<3><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
-    default: crt_combine_kernel<4><<<(unsigned)grid, CMB_THREADS, smem, st>>>(a); break;
+    case 1: crt_combine_kernel<1><<<(unsigned)grid, CMB_BLOCK, smem, st>>>(a); break;
+    case 2: crt_combine_kernel<2><<<(unsigned)grid, CMB_BLOCK, smem, st>>>(a); break;
+    case 3: crt_combine_kernel<3><<<(unsigned)grid, CMB_BLOCK, smem, st>>>(a); break;
+    default: crt_combine_kernel<4><<<(unsigned)grid, CMB_BLOCK, smem, st>>>(a); break;
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
@@ -1119,8 +1188,8 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   a.g.ldr = in->ldr;
   a.g.exp_a = in->exp_a;
   a.g.exp_b = in->exp_b;
-  a.g.frac_a = nullptr;
-  a.g.frac_b = nullptr;
+  a.g.inv_a = nullptr;
+  a.g.inv_b = nullptr;
   a.g.shift = in->shift;
   a.g.c = nullptr;
   a.g.ldc = 0;

@@ -179,13 +179,13 @@ typedef struct hcbk_ozaki_prep {
 int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
 
 /* CRT row scales: x(r,k) is to become rint(x f_r 2^(53 - e_r)), e_r in
- * a->exps and f_r in frac[r] (1/2 <= f <= 1, 8 significant bits, so the
- * product of two is exact), with |x| f 2^(53-e) < 2^53 and row norm
+ * a->exps and f_r in frac[r] (1/2 <= f <= 1, 8 significant bits; inv[r] =
+ * RN(1 / f_r)), with |x| f 2^(53-e) < 2^53 and row norm
  * ||x(r,:)|| f 2^(53-e) <= 2^nb.  MN-contiguous operands need `work` of
  * hcbk_crt_row_exponents_workspace bytes (partial sums per K chunk). */
 int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, int k_contig);
-int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, void *work,
-                        int64_t work_bytes, void *stream);
+int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, double *inv,
+                        void *work, int64_t work_bytes, void *stream);
 int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream);
 
 /* The slice-product GEMM and FP64 epilogue over K range [k0, k0 + k):
@@ -279,8 +279,9 @@ typedef struct hcbk_crt_combine_args {
   int64_t ldr;       /* >= m, multiple of 8 */
   const int *exp_a;
   const int *exp_b;
-  const double *frac_a, *frac_b; /* optional row fractions (hcbk_crt_row_scales): the
-                                   result is divided by frac_a[m] * frac_b[n] */
+  const double *inv_a, *inv_b; /* optional reciprocals of the row fractions
+                                  (hcbk_crt_row_scales): the result is multiplied
+                                  by inv_a[m] * inv_b[n] */
   int shift; /* 2 * beta_bits */
   double *c;
   int64_t ldc;

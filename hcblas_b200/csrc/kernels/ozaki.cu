@@ -336,10 +336,11 @@ __device__ __forceinline__ void na_merge(NormAcc &a, int be, double bs) {
  * f in (1/2, 1] -- rounded down to 8 significant bits, so that products of
  * two of them are exact -- keeps ||x|| f 2^(53-e) <= 2^nb. */
 __device__ __forceinline__ void row_scale(int emax, int acc_e, double s, int nb, int *e_out,
-                                          double *f_out) {
+                                          double *f_out, double *inv_out) {
   if (emax == HCBK_OZ_NONFINITE || emax == HCBK_OZ_ZERO) {
     *e_out = emax;
     *f_out = 1.0;
+    *inv_out = 1.0;
     return;
   }
   const double rt = sqrt(s * (1.0 + 0x1p-40)) * (1.0 + 0x1p-50); /* ||x|| <= 2^acc_e rt */
@@ -355,13 +356,14 @@ __device__ __forceinline__ void row_scale(int emax, int acc_e, double s, int nb,
   }
   *e_out = e;
   *f_out = f;
+  *inv_out = 1.0 / f;
 }
 
 /* K-contiguous source: one warp per row, one pass (16-byte pairs when the
  * row allows) */
 template <int VEC>
 __global__ void crt_rowexp_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
-                                   int nb, int *exps, double *frac) {
+                                   int nb, int *exps, double *frac, double *inv) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -392,7 +394,7 @@ __global__ void crt_rowexp_kcontig(const double *src, int64_t ld, int64_t rows, 
       const double os = __shfl_xor_sync(0xffffffffu, acc.s, o);
       na_merge(acc, oe, os);
     }
-    if (lane == 0) row_scale(emax, acc.e, acc.s, nb, exps + r, frac + r);
+    if (lane == 0) row_scale(emax, acc.e, acc.s, nb, exps + r, frac + r, inv + r);
   }
 }
 
@@ -455,7 +457,7 @@ __global__ void crt_rowexp_rcontig(const double *src, int64_t ld, int64_t rows, 
 /* one warp per row: lanes merge chunks lane, lane + 32, ... in order, then a
  * fixed butterfly merges the lanes -- the same sum every run */
 __global__ void crt_rowexp_finish(const unsigned long long *pm, const int *pe, const double *ps,
-                                  int64_t rows, int nchunks, int nb, int *exps, double *frac) {
+                                  int64_t rows, int nchunks, int nb, int *exps, double *frac, double *inv) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -475,7 +477,7 @@ __global__ void crt_rowexp_finish(const unsigned long long *pm, const int *pe, c
       const double os = __shfl_xor_sync(0xffffffffu, acc.s, o);
       na_merge(acc, oe, os);
     }
-    if (lane == 0) row_scale(exp_of_bits(m), acc.e, acc.s, nb, exps + r, frac + r);
+    if (lane == 0) row_scale(exp_of_bits(m), acc.e, acc.s, nb, exps + r, frac + r, inv + r);
   }
 }
 
@@ -545,10 +547,10 @@ extern "C" int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, 
   return ky * rows * (int64_t)(sizeof(unsigned long long) + sizeof(double) + sizeof(int)) + 256;
 }
 
-extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, void *work,
-                                   int64_t work_bytes, void *stream) {
+extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, double *inv,
+                                   void *work, int64_t work_bytes, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (a->rows <= 0 || a->kdim <= 0 || !frac) return HCBK_ERR_ARGS;
+  if (a->rows <= 0 || a->kdim <= 0 || !frac || !inv) return HCBK_ERR_ARGS;
   const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0;
   if (a->k_contig) {
     int64_t blocks = (a->rows * 32 + 255) / 256;
@@ -556,10 +558,10 @@ extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *fra
     if (blocks > cap) blocks = cap;
     if (al16 && (a->kdim & 1) == 0)
       crt_rowexp_kcontig<2><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, nb,
-                                                              a->exps, frac);
+                                                              a->exps, frac, inv);
     else
       crt_rowexp_kcontig<1><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, nb,
-                                                              a->exps, frac);
+                                                              a->exps, frac, inv);
   } else {
     int64_t ky, kc;
     rowexp_split(a->rows, a->kdim, &ky, &kc);
@@ -579,7 +581,7 @@ extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *fra
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (fb > cap) fb = cap;
     crt_rowexp_finish<<<(unsigned)fb, 256, 0, st>>>(pm, pe, ps, a->rows, (int)ky, nb, a->exps,
-                                                     frac);
+                                                     frac, inv);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -196,8 +196,10 @@ def row_deltas(X, shift):
 def crt_bound_rows(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, shift, ref, beta=0.0, C=None,
                    ldc=None):
     """|alpha| (da_m sum_k |b_kn| + db_n sum_k |a_mk| + K da_m db_n) with the
-    per-element rounding bounds da, db of the scaled rows, plus 4u|C| (and
-    2u|beta C|) for the reconstruction and epilogue roundings."""
+    per-element rounding bounds da, db of the scaled rows, plus 10u|C| (and
+    2u|beta C|) for the reconstruction and epilogue roundings: P' to binary64
+    within 1.5 ulp (3u), the reciprocals of the row fractions and their
+    product with the result (4u), alpha and the beta fma (2u)."""
     Ad = op_dense(A, order, ta, M, K, lda, 0)
     Bd = op_dense(B, order, tb, K, N, ldb, 0)
     da = row_deltas(Ad, shift)
@@ -205,7 +207,7 @@ def crt_bound_rows(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, shift, ref, be
     elem = abs(alpha) * (da[:, None] * np.sum(np.abs(Bd), axis=0)[None, :] +
                          np.sum(np.abs(Ad), axis=1)[:, None] * db[None, :] +
                          K * da[:, None] * db[None, :])
-    out = np.linalg.norm(elem) + 4 * U * np.linalg.norm(ref)
+    out = np.linalg.norm(elem) + 10 * U * np.linalg.norm(ref)
     if beta and C is not None:
         out += 2 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
     return out
@@ -328,7 +330,8 @@ def test_ozaki_vs_native_accuracy(handle):
 # - Ai Bi are exact integers of 2K products; the only errors are the scaling
 # of each entry to a beta-bit integer (relative 2^-(beta+1) of its row /
 # column maximum over real and imaginary parts) and the final rounding, so
-# per element |dC| <= 2 |alpha| 2K 2^(e_m + f_n) (2^-beta + 2^-2beta) + 4u|C|.
+# per element |dC| <= 2 |alpha| 2K 2^(e_m + f_n) (2^-beta + 2^-2beta) + 6u|C|
+# (P' to binary64 within 1.5 ulp, then the complex alpha).
 
 def zcrt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta_bits, ref, beta, C, ldc):
     Ad = op_dense(A, order, ta, M, K, lda, 0)
@@ -339,7 +342,7 @@ def zcrt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta_bits, ref, be
     eb = np.frexp(bmax)[1].astype(np.float64)
     elem = 2 * abs(alpha) * 2 * K * np.exp2(ea[:, None] + eb[None, :]) * \
         (2.0 ** -beta_bits + 2.0 ** (-2 * beta_bits))
-    out = np.linalg.norm(elem) + 4 * U * np.linalg.norm(ref)
+    out = np.linalg.norm(elem) + 6 * U * np.linalg.norm(ref)
     if beta:
         out += 4 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
     return out
