@@ -61,13 +61,13 @@ __device__ __forceinline__ float small_int_to_f(int x) {
 
 struct ModConst {
   float p, inv_p, hp;
-  float c1, c2, c3, c4; /* 2^11, 2^22, 2^33, 2^44 mod p (symmetric) */
+  float c1, c2, c3; /* 2^14, 2^28, 2^42 mod p (symmetric) */
 };
 
 /* the same constants duplicated into (x, x) pairs for the packed f32x2
  * instructions, and -p for the remainder fma */
 struct alignas(8) ModPair {
-  float2 c1, c2, c3, c4, inv_p, neg_p;
+  float2 c1, c2, c3, inv_p, neg_p;
 };
 
 struct ResArgs {
@@ -84,11 +84,11 @@ struct ResArgs {
   int64_t ld_dst;       /* elements */
 };
 
-/* 11-bit limbs of the scaled integer y = rint(x 2^(beta - e)), |y| <= 2^53:
- * y = l4 2^44 + l3 2^33 + l2 2^22 + l1 2^11 + l0 with |l0..l3| <= 2^10 and
- * |l4| <= 2^9, all exact in f32 (0 for zero / non-finite rows) */
+/* 14-bit limbs of the scaled integer y = rint(x 2^(beta - e)), |y| <= 2^53:
+ * y = l3 2^42 + l2 2^28 + l1 2^14 + l0 with |l0..l2| <= 2^13 and
+ * |l3| <= 2^11, all exact in f32 (0 for zero / non-finite rows) */
 struct Limbs {
-  float l0, l1, l2, l3, l4;
+  float l0, l1, l2, l3;
 };
 
 /* rint(v) of |v| < 2^51 as a double whose low word is rint(v) as an int */
@@ -103,36 +103,33 @@ __device__ __forceinline__ double scale2(double x, int s) {
 }
 
 __device__ __forceinline__ Limbs limbs_of(double x, int e, int beta) {
-  Limbs L{0.f, 0.f, 0.f, 0.f, 0.f};
+  Limbs L{0.f, 0.f, 0.f, 0.f};
   if (e == HCBK_OZ_NONFINITE || e == HCBK_OZ_ZERO) return L;
   const double y = rint(scale2(x, beta - e));
   /* each limb's rounded quotient comes out of the magic-constant add with
    * the integer in the low word: no conversion-unit instructions */
-  const double t4 = rnd_magic(y * 0x1p-44);
-  double r = fma(-(t4 - RND_D), 0x1p44, y);
-  const double t3 = rnd_magic(r * 0x1p-33);
-  r = fma(-(t3 - RND_D), 0x1p33, r);
-  const double t2 = rnd_magic(r * 0x1p-22);
-  r = fma(-(t2 - RND_D), 0x1p22, r);
-  const double t1 = rnd_magic(r * 0x1p-11);
-  r = fma(-(t1 - RND_D), 0x1p11, r);
+  const double t3 = rnd_magic(y * 0x1p-42);
+  double r = fma(-(t3 - RND_D), 0x1p42, y);
+  const double t2 = rnd_magic(r * 0x1p-28);
+  r = fma(-(t2 - RND_D), 0x1p28, r);
+  const double t1 = rnd_magic(r * 0x1p-14);
+  r = fma(-(t1 - RND_D), 0x1p14, r);
   const double t0 = rnd_magic(r);
   L.l0 = small_int_to_f(__double2loint(t0));
   L.l1 = small_int_to_f(__double2loint(t1));
   L.l2 = small_int_to_f(__double2loint(t2));
   L.l3 = small_int_to_f(__double2loint(t3));
-  L.l4 = small_int_to_f(__double2loint(t4));
   return L;
 }
 
 /* symmetric residue of the limb sum modulo one modulus.  |sum| <=
- * 2^10 (1 + 4 * 127) < 2^19, so |sum / p| < 3200 and the f32 quotient
- * sum * RN(1/p) is off by < 2e-4 -- less than the 0.5/p >= 0.002 distance of
- * any x/p (p odd) from a half-integer: the rounded quotient is exact and the
- * remainder already lies in [-(p-1)/2, (p-1)/2]. */
+ * 2^13 (1 + 2 * 127) + 2^11 * 127 < 2^21.2, so |sum / p| < 14100 (p >= 167)
+ * and the f32 quotient sum * RN(1/p) is off by < 8.5e-4 -- less than the
+ * 0.5/p >= 0.00196 distance of any x/p (p odd) from a half-integer: the
+ * rounded quotient is exact and the remainder already lies in
+ * [-(p-1)/2, (p-1)/2]. */
 __device__ __forceinline__ float residue(const Limbs &L, const ModConst &m) {
-  float t = fmaf(L.l4, m.c4, L.l0);
-  t = fmaf(L.l3, m.c3, t);
+  float t = fmaf(L.l3, m.c3, L.l0);
   t = fmaf(L.l2, m.c2, t);
   t = fmaf(L.l1, m.c1, t);
   return mod_f(t, m.p, m.inv_p);
@@ -164,26 +161,24 @@ __device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
 
 /* limbs of two elements, lane-paired */
 struct Limbs2 {
-  uint64_t l0, l1, l2, l3, l4;
+  uint64_t l0, l1, l2, l3;
 };
 
 __device__ __forceinline__ Limbs2 pair_limbs(const Limbs &a, const Limbs &b) {
-  return Limbs2{pk2(a.l0, b.l0), pk2(a.l1, b.l1), pk2(a.l2, b.l2), pk2(a.l3, b.l3),
-                pk2(a.l4, b.l4)};
+  return Limbs2{pk2(a.l0, b.l0), pk2(a.l1, b.l1), pk2(a.l2, b.l2), pk2(a.l3, b.l3)};
 }
 
 /* x - rint(x / p) p for a pair of exact integers whose quotient rounds
- * exactly (|x| < 2^19) */
+ * exactly (the limb sums above, or |x| < 2^19) */
 __device__ __forceinline__ uint64_t mod2(uint64_t t, const ModPair &m) {
   const uint64_t RND2 = pk2(RND_F, RND_F), NRND2 = pk2(-RND_F, -RND_F);
   const uint64_t q = add2(fma2(t, pk2(m.inv_p), RND2), NRND2);
   return fma2(q, pk2(m.neg_p), t);
 }
 
-/* residue() for two elements in seven packed instructions */
+/* residue() for two elements in six packed instructions */
 __device__ __forceinline__ uint64_t residue2(const Limbs2 &L, const ModPair &m) {
-  uint64_t t = fma2(L.l4, pk2(m.c4), L.l0);
-  t = fma2(L.l3, pk2(m.c3), t);
+  uint64_t t = fma2(L.l3, pk2(m.c3), L.l0);
   t = fma2(L.l2, pk2(m.c2), t);
   t = fma2(L.l1, pk2(m.c1), t);
   return mod2(t, m);
@@ -267,65 +262,61 @@ __global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
   }
 }
 
-/* MN-contiguous source: 32x32 tile through shared memory; each thread then
- * owns four consecutive k of one row (8-byte binary16 or 4-byte int8 plane
- * stores; eight threads write one row's 64 or 32 contiguous bytes) */
+/* MN-contiguous source: a 32-row x KT tile (KT = 64 for int8 planes, 32 for
+ * binary16) through shared memory; each thread then owns KT / 8 consecutive
+ * k of one row (8-byte plane stores; eight threads write one row's 64
+ * contiguous bytes), so each modulus's constants serve KT / 16 element pairs */
 template <bool I8>
-__global__ void crt_res_rcontig(ResArgs a) {
+__global__ void __launch_bounds__(256) crt_res_rcontig(ResArgs a) {
   constexpr int ESZ = I8 ? 1 : 2;
-  __shared__ double tile[32][33];
+  constexpr int KT = I8 ? 64 : 32, KPT = KT / 8, NP = KPT / 2;
+  __shared__ double tile[KT][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
-  const int64_t k0 = (int64_t)blockIdx.y * 32;
+  const int64_t k0 = (int64_t)blockIdx.y * KT;
   const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < KT / 8; ++i) {
     const int kl = ty + 8 * i;
     const int64_t r = r0 + tx, k = k0 + kl;
     tile[kl][tx] = (r < a.rows && k < a.kdim) ? a.src[r + k * a.ld] : 0.0;
   }
   __syncthreads();
   const int t = ty * 32 + tx;
-  const int rl = t >> 3, kq = (t & 7) * 4;
+  const int rl = t >> 3, kq = (t & 7) * KPT;
   const int64_t r = r0 + rl, k = k0 + kq;
   if (r >= a.rows || k >= a.kdim) return;
   const int e = a.exps[r];
   const double f = a.frac ? a.frac[r] : 1.0;
-  Limbs2 L2[2];
+  Limbs2 L2[NP];
 #pragma unroll
-  for (int j = 0; j < 2; ++j)
+  for (int j = 0; j < NP; ++j)
     L2[j] = pair_limbs(limbs_of(f * tile[kq + 2 * j][rl], e, a.beta),
                        limbs_of(f * tile[kq + 2 * j + 1][rl], e, a.beta));
   const int64_t left = a.kdim - k;
-  const int nk = left < 4 ? (int)left : 4;
+  const int nk = left < KPT ? (int)left : KPT;
   char *d0 = a.planes + (r * a.ld_dst + k) * (int64_t)ESZ;
-  const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & (4 * ESZ - 1)) == 0 &&
-                   (a.plane_stride & (4 * ESZ - 1)) == 0;
+  const bool vec = nk == KPT && (reinterpret_cast<uintptr_t>(d0) & 7) == 0 &&
+                   (a.plane_stride & 7) == 0;
 #pragma unroll
   for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
     if (i >= a.nmod) break;
     const ModPair m = a.mp[i];
+    uint2 w; /* KPT residues: 8 bytes either way */
     if constexpr (I8) {
-      const uint32_t w = __byte_perm(residue2_s8(L2[0], m), residue2_s8(L2[1], m), 0x5410);
-      int8_t *d = reinterpret_cast<int8_t *>(d0 + i * a.plane_stride);
-      if (vec) {
-        *reinterpret_cast<uint32_t *>(d) = w;
-      } else {
-        for (int j = 0; j < nk; ++j) d[j] = (int8_t)(w >> (8 * j));
-      }
-      continue;
-    }
-    __half2 v[2];
-    v[0] = residue2_h(L2[0], m);
-    v[1] = residue2_h(L2[1], m);
-    __half *d = reinterpret_cast<__half *>(d0 + i * a.plane_stride);
-    if (vec) {
-      *reinterpret_cast<uint2 *>(d) = *reinterpret_cast<const uint2 *>(v);
+      w.x = __byte_perm(residue2_s8(L2[0], m), residue2_s8(L2[1], m), 0x5410);
+      w.y = __byte_perm(residue2_s8(L2[2], m), residue2_s8(L2[3], m), 0x5410);
     } else {
-      const __half h[4] = {__low2half(v[0]), __high2half(v[0]), __low2half(v[1]),
-                           __high2half(v[1])};
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (j < nk) d[j] = h[j];
+      __half2 v[2];
+      v[0] = residue2_h(L2[0], m);
+      v[1] = residue2_h(L2[1], m);
+      w = *reinterpret_cast<const uint2 *>(v);
+    }
+    char *d = d0 + i * a.plane_stride;
+    if (vec) {
+      *reinterpret_cast<uint2 *>(d) = w;
+    } else {
+      const uint64_t wv = (static_cast<uint64_t>(w.y) << 32) | w.x;
+      for (int j = 0; j < nk * ESZ; ++j) d[j] = static_cast<char>(wv >> (8 * j));
     }
   }
 }
@@ -427,93 +418,54 @@ struct CrtAcc {
   }
 };
 
-/* ------------------------------------------------ combine pipeline --
- * The residues of one output tile (ROWS consecutive rows of one column,
- * every modulus plane) arrive in shared memory by 1-D bulk copies, several
- * tiles ahead: one thread keeps tens of KB per SM in flight, where per-thread
- * 2-byte loads left the kernel waiting on memory latency.  Requires the row
- * pitch and plane stride to be multiples of 8 elements (16 bytes). */
-
-struct PipeArgs {
-  const int16_t *res;
-  int64_t res_plane, ldr;
-  int nplanes;
-  int64_t m, n;
-  int *err;
-};
-
-/* Runs tile(residues in shared memory, first row, column) for every tile of
- * this block; all threads of the block take part. */
-template <int STAGES, int ROWS, class Tile>
-__device__ __forceinline__ void combine_pipeline(const PipeArgs &pa, int16_t *buf,
-                                                 uint64_t *full, Tile &&tile) {
-  using namespace hcbk::tc;
-  const int tid = threadIdx.x;
-  const int64_t row_tiles = (pa.m + ROWS - 1) / ROWS;
-  const int64_t ntiles = row_tiles * pa.n;
-  const int64_t first = blockIdx.x, stride = gridDim.x;
-  const size_t stage_elems = (size_t)pa.nplanes * ROWS;
-  auto issue = [&](int64_t t, int s) {
-    const int64_t r0 = (t % row_tiles) * ROWS, col = t / row_tiles;
-    const int64_t rows = pa.ldr - r0 < ROWS ? pa.ldr - r0 : ROWS;
-    const uint32_t bytes = (uint32_t)rows * 2u; /* ldr, r0 multiples of 8 */
-    mbar_expect_tx(&full[s], bytes * (uint32_t)pa.nplanes);
-    const int16_t *src = pa.res + col * pa.ldr + r0;
-    int16_t *dst = buf + s * stage_elems;
-    for (int p = 0; p < pa.nplanes; ++p)
-      bulk_load_1d(dst + p * ROWS, src + p * pa.res_plane, bytes, &full[s]);
-  };
-  if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  if (tid == 0)
-    for (int s = 0; s < STAGES; ++s)
-      if (first + s * stride < ntiles) issue(first + s * stride, s);
-  int j = 0;
-  for (int64_t t = first; t < ntiles; t += stride, ++j) {
-    const int s = j % STAGES;
-    const bool ok = mbar_wait(&full[s], (uint32_t)(j / STAGES) & 1u, pa.err, ERR_TIMEOUT_COMBINE);
-    if (ok) tile(buf + s * stage_elems, (t % row_tiles) * ROWS, t / row_tiles);
-    if (__syncthreads_or(!ok)) {
-      /* give the copies still in flight a bounded time to land before the
-       * block's shared memory is released */
-      if (tid == 0)
-        for (int k = 0; k < STAGES; ++k) {
-          if (t + k * stride >= ntiles) break;
-          const int sk = (j + k) % STAGES;
-          const uint32_t ph = (uint32_t)((j + k) / STAGES) & 1u;
-          for (int it = 0; it < (1 << 22) && !mbar_try_wait(&full[sk], ph); ++it) {
-          }
-        }
-      return;
-    }
-    if (tid == 0 && t + STAGES * stride < ntiles) issue(t + STAGES * stride, s);
-  }
-}
-
-/* the weight chunks in shared memory (the modulus loop indexes them at run
- * time; register-resident weights would cost 2 NC registers a modulus) */
-template <int NC>
-__device__ __forceinline__ void load_weights(const CombArgs &a, double (*sw)[NC]) {
-  for (int j = threadIdx.x; j < HCBK_CRT_MAX_MODULI * NC; j += blockDim.x)
-    sw[j / NC][j % NC] = a.w[j / NC][j % NC];
-  __syncthreads();
-}
-
-/* real combine: 256 threads x 2 consecutive rows (one 4-byte residue load
- * per modulus, weights read once for both rows); 3 stages of nmod KB */
+/* real combine: 256 consumer threads x 2 consecutive rows (one 4-byte
+ * residue load per modulus); 3 stages of nmod KB */
 constexpr int CMB_THREADS = 256, CMB_RPT = 2, CMB_ROWS = CMB_THREADS * CMB_RPT;
 constexpr int CMB_STAGES = 3;
-/* complex combine: 256 threads x 1 row (two accumulators a row already);
- * 3 stages of 1.5 nmod KB */
+/* complex combine: 256 consumer threads x 1 row (two accumulators a row
+ * already); 3 stages of 1.5 nmod KB */
 constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 1, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
 constexpr int ZCMB_STAGES = 3;
 
 /* signed 16-bit halves of a 32-bit word */
 __device__ __forceinline__ int lo16(uint32_t w) { return (int)(w << 16) >> 16; }
 __device__ __forceinline__ int hi16(uint32_t w) { return (int)w >> 16; }
+
+/* Producer of a warp-specialised combine (one thread): tile j of this block
+ * (ROWS rows of one column, every residue plane) goes to stage j % STAGES by
+ * 1-D bulk copies once the consumers have released the stage's previous
+ * tile; before returning it lets the last copies land (immediately when the
+ * consumers took them; bounded when a wait failed), so that no copy writes
+ * shared memory after the block has left. */
+template <int STAGES, int ROWS>
+__device__ __forceinline__ void ws_produce(const int16_t *res, int64_t res_plane, int64_t ldr,
+                                           int nplanes, int64_t row_tiles, int64_t ntiles,
+                                           int16_t *buf, uint64_t *full, uint64_t *empty,
+                                           int *err) {
+  using namespace hcbk::tc;
+  const size_t stage_elems = (size_t)nplanes * ROWS;
+  int64_t j = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+    const int s = (int)(j % STAGES);
+    if (j >= STAGES &&
+        !mbar_wait(&empty[s], (uint32_t)((j / STAGES) - 1) & 1u, err, ERR_TIMEOUT_COMBINE))
+      break;
+    const int64_t r0 = (t % row_tiles) * ROWS, col = t / row_tiles;
+    const int64_t rows = ldr - r0 < ROWS ? ldr - r0 : ROWS;
+    const uint32_t bytes = (uint32_t)rows * 2u; /* ldr, r0 multiples of 8 */
+    mbar_expect_tx(&full[s], bytes * (uint32_t)nplanes);
+    const int16_t *src = res + col * ldr + r0;
+    int16_t *dst = buf + s * stage_elems;
+    for (int p = 0; p < nplanes; ++p)
+      bulk_load_1d(dst + p * ROWS, src + p * res_plane, bytes, &full[s]);
+  }
+  for (int64_t k = (j > STAGES ? j - STAGES : 0); k < j; ++k) {
+    const int s = (int)(k % STAGES);
+    const uint32_t ph = (uint32_t)(k / STAGES) & 1u;
+    for (int it = 0; it < (1 << 22) && !mbar_try_wait(&full[s], ph); ++it) {
+    }
+  }
+}
 
 /* Real combine, warp-specialised: warps 0-7 reconstruct 512-row tiles (two
  * consecutive rows per thread, one 4-byte load of a residue pair per
@@ -552,33 +504,10 @@ __global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_
   }
   __syncthreads();
 
-  if (warp == CMB_CONSUMERS) {
-    /* ------------------------------------------------ producer -- */
-    if (lane != 0) return;
-    int64_t j = 0;
-    for (int64_t t = first; t < ntiles; t += stride, ++j) {
-      const int s = (int)(j % CMB_STAGES);
-      if (j >= CMB_STAGES &&
-          !mbar_wait(&empty[s], (uint32_t)((j / CMB_STAGES) - 1) & 1u, a.err, ERR_TIMEOUT_COMBINE))
-        break;
-      const int64_t r0 = (t % row_tiles) * CMB_ROWS, col = t / row_tiles;
-      const int64_t rows = a.ldr - r0 < CMB_ROWS ? a.ldr - r0 : CMB_ROWS;
-      const uint32_t bytes = (uint32_t)rows * 2u; /* ldr, r0 multiples of 8 */
-      mbar_expect_tx(&full[s], bytes * (uint32_t)nmod);
-      const int16_t *src = a.res + col * a.ldr + r0;
-      int16_t *dst = buf + s * stage_elems;
-      for (int p = 0; p < nmod; ++p)
-        bulk_load_1d(dst + p * CMB_ROWS, src + p * a.res_plane, bytes, &full[s]);
-    }
-    /* the last copies issued land before the block's shared memory is
-     * released (immediately when the consumers took them; bounded when a
-     * wait failed) */
-    for (int64_t k = (j > CMB_STAGES ? j - CMB_STAGES : 0); k < j; ++k) {
-      const int s = (int)(k % CMB_STAGES);
-      const uint32_t ph = (uint32_t)(k / CMB_STAGES) & 1u;
-      for (int it = 0; it < (1 << 22) && !mbar_try_wait(&full[s], ph); ++it) {
-      }
-    }
+  if (warp == CMB_CONSUMERS) { /* producer */
+    if (lane == 0)
+      ws_produce<CMB_STAGES, CMB_ROWS>(a.res, a.res_plane, a.ldr, nmod, row_tiles, ntiles, buf,
+                                       full, empty, a.err);
     return;
   }
 
@@ -656,10 +585,9 @@ static void fill_mod_consts(ModConst (&mc)[HCBK_CRT_MAX_MODULI]) {
     m.p = (float)M[i];
     m.inv_p = 1.0f / (float)M[i];
     m.hp = (float)((M[i] - 1) / 2);
-    m.c1 = pow2_mod_sym(11, M[i]);
-    m.c2 = pow2_mod_sym(22, M[i]);
-    m.c3 = pow2_mod_sym(33, M[i]);
-    m.c4 = pow2_mod_sym(44, M[i]);
+    m.c1 = pow2_mod_sym(14, M[i]);
+    m.c2 = pow2_mod_sym(28, M[i]);
+    m.c3 = pow2_mod_sym(42, M[i]);
   }
 }
 
@@ -730,7 +658,6 @@ static void fill_mod_pairs(ModPair (&mp)[HCBK_CRT_MAX_MODULI]) {
     mp[i].c1 = make_float2(mc[i].c1, mc[i].c1);
     mp[i].c2 = make_float2(mc[i].c2, mc[i].c2);
     mp[i].c3 = make_float2(mc[i].c3, mc[i].c3);
-    mp[i].c4 = make_float2(mc[i].c4, mc[i].c4);
     mp[i].inv_p = make_float2(mc[i].inv_p, mc[i].inv_p);
     mp[i].neg_p = make_float2(-mc[i].p, -mc[i].p);
   }
@@ -969,54 +896,86 @@ __device__ __forceinline__ int small_f_to_int(float x) {
 }
 
 /* residues stream through the two accumulators, one modulus at a time: the
- * weighted-sum reconstruction keeps no per-modulus state */
+ * weighted-sum reconstruction keeps no per-modulus state.  Warp-specialised
+ * like the real combine: warps 0-7 reconstruct 256-row tiles (one row per
+ * thread), warp 8's lane 0 keeps the residues of ZCMB_STAGES tiles in flight. */
+constexpr int ZCMB_CONSUMERS = ZCMB_THREADS / 32;
+constexpr int ZCMB_BLOCK = ZCMB_THREADS + 32;
+
 template <int NC>
-__global__ void __launch_bounds__(ZCMB_THREADS) zcrt_combine_kernel(ZCombArgs a) {
+__global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __grid_constant__ ZCombArgs a) {
+  using namespace hcbk::tc;
   extern __shared__ __align__(128) unsigned char cmb_smem[];
-  __shared__ double sw[HCBK_CRT_MAX_MODULI][NC];
-  __shared__ __align__(8) uint64_t full[ZCMB_STAGES];
-  if (blockDim.x != ZCMB_THREADS) { /* the tile covers ZCMB_ROWS rows only at this shape */
-    if (threadIdx.x == 0) atomicCAS(a.g.err, 0, (int)hcbk::tc::ERR_LAUNCH_SHAPE);
+  __shared__ __align__(8) uint64_t full[ZCMB_STAGES], empty[ZCMB_STAGES];
+  if (blockDim.x != ZCMB_BLOCK) { /* the tile covers ZCMB_ROWS rows only at this shape */
+    if (threadIdx.x == 0) atomicCAS(a.g.err, 0, (int)ERR_LAUNCH_SHAPE);
     return;
   }
-  load_weights<NC>(a.g, sw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = a.g.nmod;
-  const int tid = threadIdx.x;
-  const PipeArgs pa{a.g.res, a.g.res_plane, a.g.ldr, 3 * nmod, a.g.m, a.g.n, a.g.err};
-  combine_pipeline<ZCMB_STAGES, ZCMB_ROWS>(
-      pa, reinterpret_cast<int16_t *>(cmb_smem), full,
-      [&](const int16_t *R, int64_t r0, int64_t col) {
-        const int64_t row = r0 + ZCMB_RPT * tid;
-        if (row >= a.g.m) return;
-        CrtAcc<NC> acc_re[ZCMB_RPT], acc_im[ZCMB_RPT];
-#pragma unroll 2
-        for (int i = 0; i < nmod; ++i) {
-          const float t1 = small_int_to_f(R[i * ZCMB_ROWS + tid]);
-          const float t2 = small_int_to_f(R[(nmod + i) * ZCMB_ROWS + tid]);
-          const float t3 = small_int_to_f(R[(2 * nmod + i) * ZCMB_ROWS + tid]);
-          const float p = a.g.p[i], ip = a.g.inv_p[i], hp = a.g.hp[i];
-          acc_re[0].add(sw[i], small_f_to_int(sym_f(mod_f(t1 - t2, p, ip), p, hp)));
-          acc_im[0].add(sw[i], small_f_to_int(sym_f(mod_f(t3 - t1 - t2, p, ip), p, hp)));
-        }
-        const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
+  int16_t *buf = reinterpret_cast<int16_t *>(cmb_smem);
+  const int64_t row_tiles = (a.g.m + ZCMB_ROWS - 1) / ZCMB_ROWS;
+  const int64_t ntiles = row_tiles * a.g.n;
+  const size_t stage_elems = (size_t)3 * nmod * ZCMB_ROWS;
+  if (tid == 0) {
+    for (int s = 0; s < ZCMB_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], ZCMB_CONSUMERS);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (warp == ZCMB_CONSUMERS) { /* producer */
+    if (lane == 0)
+      ws_produce<ZCMB_STAGES, ZCMB_ROWS>(a.g.res, a.g.res_plane, a.g.ldr, 3 * nmod, row_tiles,
+                                         ntiles, buf, full, empty, a.g.err);
+    return;
+  }
+  int64_t j = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+    const int s = (int)(j % ZCMB_STAGES);
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)(j / ZCMB_STAGES) & 1u, a.g.err,
+                                           ERR_TIMEOUT_COMBINE)))
+      break;
+    const int16_t *R = buf + s * stage_elems;
+    const int64_t row = (t % row_tiles) * ZCMB_ROWS + tid, col = t / row_tiles;
+    CrtAcc<NC> acc_re, acc_im;
+    if (row < a.g.m) {
 #pragma unroll
-        for (int u = 0; u < ZCMB_RPT; ++u) {
-          if (row + u >= a.g.m) break;
-          const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row + u);
-          const double re = acc_re[u].finish(a.g, ea, eb);
-          const double im = acc_im[u].finish(a.g, ea, eb);
-          double2 *dst = a.c + row + u + col * a.ldc;
-          double2 o;
-          o.x = a.alpha.x * re - a.alpha.y * im;
-          o.y = a.alpha.x * im + a.alpha.y * re;
-          if (a.g.beta_nonzero) {
-            const double2 cv = *dst;
-            o.x = fma(a.beta.x, cv.x, fma(-a.beta.y, cv.y, o.x));
-            o.y = fma(a.beta.x, cv.y, fma(a.beta.y, cv.x, o.y));
-          }
-          *dst = o;
+      for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights and moduli */
+        if (i >= nmod) break;
+        const float t1 = small_int_to_f(R[i * ZCMB_ROWS + tid]);
+        const float t2 = small_int_to_f(R[(nmod + i) * ZCMB_ROWS + tid]);
+        const float t3 = small_int_to_f(R[(2 * nmod + i) * ZCMB_ROWS + tid]);
+        const float p = a.g.p[i], ip = a.g.inv_p[i], hp = a.g.hp[i];
+        const double re = small_int_to_d(small_f_to_int(sym_f(mod_f(t1 - t2, p, ip), p, hp)));
+        const double im = small_int_to_d(small_f_to_int(sym_f(mod_f(t3 - t1 - t2, p, ip), p, hp)));
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+          acc_re.S[k] = fma(re, a.g.w[i][k], acc_re.S[k]);
+          acc_im.S[k] = fma(im, a.g.w[i][k], acc_im.S[k]);
         }
-      });
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]); /* the stage's residues are in registers */
+    if (row < a.g.m) {
+      const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
+      const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row);
+      const double re = acc_re.finish(a.g, ea, eb);
+      const double im = acc_im.finish(a.g, ea, eb);
+      double2 *dst = a.c + row + col * a.ldc;
+      double2 o;
+      o.x = a.alpha.x * re - a.alpha.y * im;
+      o.y = a.alpha.x * im + a.alpha.y * re;
+      if (a.g.beta_nonzero) {
+        const double2 cv = *dst;
+        o.x = fma(a.beta.x, cv.x, fma(-a.beta.y, cv.y, o.x));
+        o.y = fma(a.beta.x, cv.y, fma(a.beta.y, cv.x, o.y));
+      }
+      *dst = o;
+    }
+  }
 }
 
 /* persistent grid for a combine kernel: as many blocks as fit, at most one
@@ -1079,7 +1038,8 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
     else
       crt_res_kcontig<false><<<(unsigned)blocks, 256, 0, st>>>(a);
   } else {
-    const int64_t gx = (a.rows + 31) / 32, gy = (a.kdim + 31) / 32;
+    const int64_t kt = in->i8 ? 64 : 32; /* k per tile (crt_res_rcontig's KT) */
+    const int64_t gx = (a.rows + 31) / 32, gy = (a.kdim + kt - 1) / kt;
     if (gy > 65535) return HCBK_ERR_ARGS;
     if (in->i8)
       crt_res_rcontig<true><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
@@ -1208,17 +1168,17 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   int64_t grid = 0;
   int rc;
   switch (a.g.nc) {
-    case 1: rc = combine_grid(zcrt_combine_kernel<1>, ZCMB_THREADS, smem, ntiles, &grid); break;
-    case 2: rc = combine_grid(zcrt_combine_kernel<2>, ZCMB_THREADS, smem, ntiles, &grid); break;
-    case 3: rc = combine_grid(zcrt_combine_kernel<3>, ZCMB_THREADS, smem, ntiles, &grid); break;
-    default: rc = combine_grid(zcrt_combine_kernel<4>, ZCMB_THREADS, smem, ntiles, &grid); break;
+    case 1: rc = combine_grid(zcrt_combine_kernel<1>, ZCMB_BLOCK, smem, ntiles, &grid); break;
+    case 2: rc = combine_grid(zcrt_combine_kernel<2>, ZCMB_BLOCK, smem, ntiles, &grid); break;
+    case 3: rc = combine_grid(zcrt_combine_kernel<3>, ZCMB_BLOCK, smem, ntiles, &grid); break;
+    default: rc = combine_grid(zcrt_combine_kernel<4>, ZCMB_BLOCK, smem, ntiles, &grid); break;
   }
   if (rc != HCBK_OK) return rc;
   switch (a.g.nc) {
-    case 1: zcrt_combine_kernel<1><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
-    case 2: zcrt_combine_kernel<2><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
-    case 3: zcrt_combine_kernel<3><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
-    default: zcrt_combine_kernel<4><<<(unsigned)grid, ZCMB_THREADS, smem, st>>>(a); break;
+    case 1: zcrt_combine_kernel<1><<<(unsigned)grid, ZCMB_BLOCK, smem, st>>>(a); break;
+    case 2: zcrt_combine_kernel<2><<<(unsigned)grid, ZCMB_BLOCK, smem, st>>>(a); break;
+    case 3: zcrt_combine_kernel<3><<<(unsigned)grid, ZCMB_BLOCK, smem, st>>>(a); break;
+    default: zcrt_combine_kernel<4><<<(unsigned)grid, ZCMB_BLOCK, smem, st>>>(a); break;
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
