@@ -249,9 +249,11 @@ int cgemm_split3m(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void 
   return timed_launch(st, stream, "split.c3m_combine", [&] { return hcbk_c3m_combine(&cb, stream); });
 }
 
-/* Ozaki-scheme DGEMM on INT8 tensor cores: per-row / per-column exponents,
- * `s` int8 slices per operand, slice products exact in INT32, FP64 epilogue.
- * K is split so that every INT32 group sum stays exact. */
+/* Ozaki-scheme DGEMM (Ozaki-I): per-row / per-column exponents, `s` slices
+ * per operand.  INT8 slices: the slice products of each weight group summed
+ * exactly in INT32 on the int8 tensor cores (K split so that every group sum
+ * stays exact), then an FP64 element-wise weighting pass; 8-bit slices in
+ * binary16: f16 tensor cores with per-slab FP64 promotion. */
 int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, void *stream,
                 const char **path) {
   if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
@@ -261,7 +263,10 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
   const size_t a_pl = up1k((size_t)a->m * kp * esz), b_pl = up1k((size_t)a->n * kp * esz);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
-  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl);
+  /* int8 path: the s slice-group INT32 sums of C, column-major */
+  const int64_t ldd = (a->m + 3) & ~int64_t(3);
+  const size_t d_bytes = f16 ? 0 : up1k((size_t)s * ldd * a->n * sizeof(int32_t));
+  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl) + d_bytes;
   char *ws = static_cast<char *>(ensure_workspace(st, total));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
@@ -269,6 +274,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
   char *pa_base = ws + ea_bytes + eb_bytes;
   char *pb_base = pa_base + s * a_pl;
+  int32_t *dsum = reinterpret_cast<int32_t *>(pb_base + s * b_pl);
 
   hcbk_ozaki_prep pa;
   pa.src = static_cast<const double *>(a->a) + a->a_off;
@@ -306,9 +312,50 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   static const char *names16[8] = {"", "", "", "tc.ozaki_f16_s3", "tc.ozaki_f16_s4",
                                     "tc.ozaki_f16_s5", "tc.ozaki_f16_s6", "tc.ozaki_f16_s7"};
   *path = f16 ? names16[s] : names[s];
-  /* INT32 exactness bounds one INT8 launch's K; the f16 kernel promotes per
-   * K-slab and takes any K */
-  const int64_t kmax = f16 ? a->k : hcbk_ozaki_max_k(s);
+  if (!f16) {
+    /* one launch of every slice group per K range (INT32 exactness bounds
+     * the range), then the FP64 weighting, scaling and alpha / beta */
+    const int64_t kmax = hcbk_ozaki_max_k(s);
+    hcbk_ozaki_groups g;
+    g.m = a->m;
+    g.n = a->n;
+    g.slices = s;
+    g.a_planes = pa_base;
+    g.b_planes = pb_base;
+    g.ld_a = kp;
+    g.ld_b = kp;
+    g.a_plane_stride = (int64_t)a_pl;
+    g.b_plane_stride = (int64_t)b_pl;
+    g.d = dsum;
+    g.ldd = ldd;
+    g.d_plane = ldd * a->n;
+    g.pair = st->tc_pair == 2 ||
+             (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * s >= hcbk_sm_count() / 2);
+    hcbk_ozaki_groups_combine_args cb;
+    cb.m = a->m;
+    cb.n = a->n;
+    cb.slices = s;
+    cb.d = dsum;
+    cb.ldd = ldd;
+    cb.d_plane = ldd * a->n;
+    cb.exp_a = exp_a;
+    cb.exp_b = exp_b;
+    cb.c = static_cast<double *>(a->c) + a->c_off;
+    cb.ldc = a->ldc;
+    cb.alpha = a->alpha_re;
+    for (int64_t k0 = 0; k0 < a->k; k0 += kmax) {
+      g.k0 = k0;
+      g.k = (a->k - k0 < kmax) ? a->k - k0 : kmax;
+      cb.beta = (k0 == 0) ? a->beta_re : 1.0;
+      rc = timed_launch(st, stream, *path, [&] { return hcbk_ozaki_groups_tc(&g, err, stream); });
+      if (!rc)
+        rc = timed_launch(st, stream, "ozaki.groups_combine",
+                          [&] { return hcbk_ozaki_groups_combine(&cb, stream); });
+      if (rc) return rc;
+    }
+    return HCBK_OK;
+  }
+  const int64_t kmax = a->k; /* the f16 kernel promotes per K-slab and takes any K */
   hcbk_ozaki_gemm g;
   g.m = a->m;
   g.n = a->n;
@@ -328,9 +375,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
     g.k0 = k0;
     g.k = (a->k - k0 < kmax) ? a->k - k0 : kmax;
     g.beta = (k0 == 0) ? a->beta_re : 1.0;
-    rc = timed_launch(st, stream, *path, [&] {
-      return f16 ? hcbk_ozaki16_gemm_tc(&g, err, stream) : hcbk_ozaki_gemm_tc(&g, err, stream);
-    });
+    rc = timed_launch(st, stream, *path, [&] { return hcbk_ozaki16_gemm_tc(&g, err, stream); });
     if (rc) return rc;
   }
   return HCBK_OK;

@@ -188,11 +188,11 @@ int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, double *
                         void *work, int64_t work_bytes, void *stream);
 int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream);
 
-/* The slice-product GEMM and FP64 epilogue over K range [k0, k0 + k):
- *   C := alpha * 2^(ea_m + eb_n) * sum_{i+j<s} 2^(-7(i+j+2)) a_i . b_j + beta * C
- * a_planes: M rows, b_planes: N rows, both K-major int8 with row pitch ld
- * (bytes) and plane pitch plane_stride; C column-major FP64.  k must keep the
- * INT32 group sums exact: s * k * 127^2 < 2^31. */
+/* Slice-product GEMM operands over K range [k0, k0 + k): a_planes M rows,
+ * b_planes N rows, K-major with row pitch ld and plane pitch plane_stride
+ * (bytes); C column-major FP64:
+ *   C := alpha * 2^(ea_m + eb_n) * sum_{i+j<s} w^(i+j+2) a_i . b_j + beta * C
+ * (used by the f16 path, w = 2^-8). */
 typedef struct hcbk_ozaki_gemm {
   int64_t m, n, k, k0;
   int slices;
@@ -206,12 +206,46 @@ typedef struct hcbk_ozaki_gemm {
   int64_t ldc;
   double alpha, beta;
 } hcbk_ozaki_gemm;
-int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream);
-/* The same product on the f16 tensor path: binary16 planes holding 8-bit
+/* INT8 Ozaki-I slice groups on the int8 tensor cores: for every group
+ * d = 0 .. slices-1 one INT32 GEMM over the concatenated K of its slice pairs,
+ *   D_d = sum_{i <= d} a_i . b_(d-i)   (K range [k0, k0 + k)),
+ * exact while slices * k * 127^2 < 2^31 (k <= hcbk_ozaki_max_k, a multiple
+ * of 128 unless it ends the operand); every group in one persistent launch,
+ * largest first.  Slice planes int8, K-major, row pitch ld_a / ld_b bytes and
+ * plane pitches multiples of 16; D_d column-major int32 at d + d*d_plane
+ * with leading dimension ldd (ldd, d_plane multiples of 4 elements, d
+ * 16-byte aligned).  Tiles 256 x 256 over CTA pairs (pair = 1) or 128 x 256. */
+typedef struct hcbk_ozaki_groups {
+  int64_t m, n, k, k0;
+  int slices;
+  const void *a_planes;
+  const void *b_planes;
+  int64_t ld_a, ld_b;
+  int64_t a_plane_stride, b_plane_stride;
+  int32_t *d;
+  int64_t ldd, d_plane;
+  int pair;
+} hcbk_ozaki_groups;
+int hcbk_ozaki_groups_tc(const hcbk_ozaki_groups *g, int *err, void *stream);
+/* C := alpha * 2^(exp_a[m] + exp_b[n]) * sum_d 2^(-7(d+2)) D_d + beta * C,
+ * the groups summed in binary64 smallest weight first (FP64 element-wise). */
+typedef struct hcbk_ozaki_groups_combine_args {
+  int64_t m, n;
+  int slices;
+  const int32_t *d;
+  int64_t ldd, d_plane;
+  const int *exp_a;
+  const int *exp_b;
+  double *c;
+  int64_t ldc;
+  double alpha, beta;
+} hcbk_ozaki_groups_combine_args;
+int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a, void *stream);
+/* The product on the f16 tensor path: binary16 planes holding 8-bit
  * integer slices (ld_a / ld_b in elements), weights 2^(-8(i+j+2)); any K
  * (k0 must be 0), slices 3..7. */
 int hcbk_ozaki16_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream);
-/* largest K per launch for s slices (INT32 exactness), multiple of 64 */
+/* largest K per launch for s slices (INT32 exactness), multiple of 128 */
 int64_t hcbk_ozaki_max_k(int slices);
 
 /* ----------------------------------------- CRT (Ozaki scheme II) DGEMM -- */

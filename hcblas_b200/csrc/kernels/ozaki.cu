@@ -481,6 +481,63 @@ __global__ void crt_rowexp_finish(const unsigned long long *pm, const int *pe, c
   }
 }
 
+/* int32 to binary64 without the conversion unit: the pattern
+ * 0x43300000:(v + 2^31) is 2^52 + 2^31 + v */
+__device__ __forceinline__ double i32_to_d(int v) {
+  return __hiloint2double(0x43300000, v ^ (int)0x80000000) - 4503601774854144.0;
+}
+
+/* Ozaki-I slice-group combine: four consecutive rows of one column per
+ * thread (16-byte loads of each group's int32 sums), groups added smallest
+ * weight first, then the exponent scaling and alpha / beta in FP64. */
+__global__ void __launch_bounds__(256) oz_groups_combine(const hcbk_ozaki_groups_combine_args a) {
+  const int64_t rows4 = (a.m + 3) / 4;
+  const int64_t total = rows4 * a.n;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = idx / rows4, r0 = (idx - col * rows4) * 4;
+    const bool whole = r0 + 4 <= a.m;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int d = a.slices - 1; d >= 0; --d) {
+      const int32_t *src = a.d + d * a.d_plane + col * a.ldd + r0;
+      int4 q = make_int4(0, 0, 0, 0);
+      if (whole) {
+        q = __ldcs(reinterpret_cast<const int4 *>(src)); /* read once: stream past L2 */
+      } else {
+        int t[4] = {0, 0, 0, 0};
+        for (int u = 0; u < 4; ++u)
+          if (r0 + u < a.m) t[u] = src[u];
+        q = make_int4(t[0], t[1], t[2], t[3]);
+      }
+      const double w = __longlong_as_double((long long)(1023 - 7 * (d + 2)) << 52);
+      v[0] = fma(i32_to_d(q.x), w, v[0]);
+      v[1] = fma(i32_to_d(q.y), w, v[1]);
+      v[2] = fma(i32_to_d(q.z), w, v[2]);
+      v[3] = fma(i32_to_d(q.w), w, v[3]);
+    }
+    const int eb = a.exp_b[col];
+    double *dst = a.c + col * a.ldc + r0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (r0 + u >= a.m) break;
+      const int ea = a.exp_a[r0 + u];
+      double o;
+      if (ea == HCBK_OZ_NONFINITE || eb == HCBK_OZ_NONFINITE) {
+        o = __longlong_as_double(0x7ff8000000000000ll);
+      } else if (ea == HCBK_OZ_ZERO || eb == HCBK_OZ_ZERO) {
+        o = 0.0;
+      } else {
+        const int e = ea + eb;
+        o = (e >= -1022 && e <= 1023) ? v[u] * __longlong_as_double((long long)(e + 1023) << 52)
+                                      : ldexp(v[u], e);
+      }
+      o *= a.alpha;
+      if (a.beta != 0.0) o = fma(a.beta, dst[u], o);
+      dst[u] = o;
+    }
+  }
+}
+
 /* the K split of the MN-contiguous row-exponent pass */
 static void rowexp_split(int64_t rows, int64_t kdim, int64_t *ky, int64_t *kchunk) {
   const int64_t gx = (rows + 511) / 512;
@@ -523,6 +580,18 @@ extern "C" int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream) {
     else
       oz_exp_rcontig<1><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kchunk, a->exps);
   }
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a, void *stream) {
+  if (a->m <= 0 || a->n <= 0 || a->slices < 1 || a->slices > 8 || a->ldd < a->m ||
+      (a->ldd & 3) || (a->d_plane & 3) || (reinterpret_cast<uintptr_t>(a->d) & 15))
+    return HCBK_ERR_ARGS;
+  const int64_t total = (a->m + 3) / 4 * a->n;
+  int64_t blocks = (total + 255) / 256;
+  const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  oz_groups_combine<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(*a);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 

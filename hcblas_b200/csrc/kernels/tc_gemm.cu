@@ -36,6 +36,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <type_traits>
+
 #include "hcbk.h"
 #include "tc_common.cuh"
 
@@ -60,10 +62,6 @@ struct TcParams {
   int beta_nonzero;
   int out_tma; /* f16 epilogue: C read (beta != 0) and written by TMA via tc */
   int *err;
-  /* Ozaki epilogue */
-  double alpha_d, beta_d;
-  const int *exp_a;
-  const int *exp_b;
   /* modular (CRT) epilogue: output plane i is reduced modulo mod_tab[i];
    * planes of A, B (3-D tensor maps) and C (c_plane_stride elements apart)
    * are batched into one launch */
@@ -86,33 +84,6 @@ struct RecipeSingle {
   __host__ __device__ static constexpr bool first(int i) { return i == 0; }
 };
 /* RecipeBf16x3 / RecipeBf16x6: tc_common.cuh (shared with the grouped kernel) */
-/* Ozaki, S int8 slices per operand: every pair (i, j) with i + j < S,
- * enumerated by weight d = i + j, accumulated exactly into INT32
- * accumulator d.  All planes of an operand share one 3-D tensor map
- * {K, rows, plane}. */
-template <int S> struct RecipeOzaki {
-  static constexpr int NA = S, NB = S, NP = S * (S + 1) / 2, NACC = S;
-  static constexpr bool P3D = true;
-  __host__ __device__ static constexpr int pd(int pi) {
-    int d = 0;
-    while (pi > d) {
-      pi -= d + 1;
-      ++d;
-    }
-    return d;
-  }
-  __host__ __device__ static constexpr int pa(int pi) {
-    int d = 0;
-    while (pi > d) {
-      pi -= d + 1;
-      ++d;
-    }
-    return pi;
-  }
-  __host__ __device__ static constexpr int pb(int pi) { return pd(pi) - pa(pi); }
-  __host__ __device__ static constexpr int pacc(int pi) { return pd(pi); }
-  __host__ __device__ static constexpr bool first(int pi) { return pa(pi) == 0; }
-};
 
 /* ---------------------------------------------------------- epilogues -- */
 
@@ -329,10 +300,6 @@ template <typename OutT> struct EpiAlphaBeta {
   }
 };
 
-/* Ozaki epilogue: NACC exact INT32 group sums acc_d (d = i + j) ->
- *   C = alpha * 2^(ea_m + eb_n) * sum_d 2^(-7(d+2)) acc_d + beta * C   (FP64)
- * The group terms are exact in binary64 (|acc_d| < 2^31, power-of-two
- * weights) and are added smallest weight first. */
 /* Modular epilogue of the CRT scheme, reducing in place in TMEM.
  * With f16 residues |r| <= 127 (moduli <= 255) the tensor core's f32 sums
  * are exact integers while below 2^24: 1024 * 127^2 + 1.5 * 255 < 2^24.
@@ -426,6 +393,61 @@ struct EpiModP {
   }
 };
 
+/* Ozaki-I slice-group epilogue (concatenated-K mode, see CatK): the tile's
+ * INT32 group sum D_d goes out unchanged, through per-warp shared-memory
+ * boxes (32 x 32 int32, column-major) and TMA tensor stores into plane d of
+ * the int32 output {rows, cols, group}; the FP64 weighting, exponent scaling
+ * and alpha / beta happen in a separate element-wise pass. */
+struct EpiI32Cat {
+  static constexpr bool INPLACE = false;
+  static constexpr bool PLANE_BATCH = true;
+  static constexpr bool CAT_K = true;
+  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * 4;
+  static constexpr uint32_t OUT_WARP_BYTES = 2 * OUT_BOX_BYTES;
+  static constexpr uint32_t OUT_SMEM = 4 * OUT_WARP_BYTES;
+
+  template <int BN>
+  static __device__ __forceinline__ void prefetch_c(const TcParams &, int, int, OutStage &) {}
+
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void run(const TcParams &, uint32_t, int, int, OutStage &) {
+    static_assert(NACC == 0, "the slice-group epilogue stores through final_store");
+  }
+
+  /* `plane` is the walk's plane index; the group it holds is nplanes - 1 - plane */
+  template <int BN>
+  static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint8_t *out,
+                                                     int m0, int n0, int plane) {
+    const int lane = threadIdx.x & 31;
+    const int d = p.nplanes - 1 - plane;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 32) {
+      uint32_t *box = reinterpret_cast<uint32_t *>(out + ((c >> 5) & 1) * OUT_BOX_BYTES);
+      uint32_t ra[32];
+      tmem_ld_32x32b_x32(ta + c, ra);
+      if (lane == 0) bulk_wait_read<1>(); /* the store from this box two groups ago */
+      __syncwarp();
+      tmem_ld_wait();
+#pragma unroll
+      for (int j = 0; j < 32; ++j) box[j * 32 + lane] = ra[j];
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_3d(&p.tc, box, m0, n0 + c, d);
+        bulk_commit();
+      }
+    }
+  }
+};
+
+/* Concatenated-K mode of an epilogue (CAT_K): the walk's plane index q
+ * stands for the group d = nplanes - 1 - q (largest first) and the tile's K
+ * loop runs over (d + 1) * kblocks slabs, slab j reading A plane j / kblocks
+ * and B plane d - j / kblocks: D_d = sum_{i <= d} A_i B_(d-i)^T in one
+ * accumulator. */
+template <class E, class = void> struct CatK : std::false_type {};
+template <class E> struct CatK<E, std::void_t<decltype(E::CAT_K)>> : std::bool_constant<E::CAT_K> {};
+
 /* Modular epilogue of the int8 path: the INT32 accumulator holds the
  * exact sum over all of K (|s| <= K 127^2 < 2^31), reduced once per tile:
  * s = hi 2^16 + lo (hi = s >> 16, 0 <= lo < 2^16) turns into the f32-exact
@@ -491,74 +513,6 @@ struct EpiModPi8 {
   }
 };
 
-/* 2^e built from its binary64 bit pattern (exact; normal range
- * -1022 <= e <= 1023 only).  Deliberately not recursive: device recursion
- * consumes the (1 KB default) call stack. */
-__device__ __forceinline__ double pow2_bits(int e) {
-  return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
-}
-
-struct EpiOzaki {
-  static constexpr bool INPLACE = false;
-  static constexpr bool PLANE_BATCH = false;
-  static constexpr uint32_t OUT_SMEM = 0, OUT_WARP_BYTES = 0;
-  template <int BN, int NACC>
-  static __device__ __forceinline__ void run(const TcParams &p, uint32_t tbase, int m, int n0,
-                                             OutStage &) {
-    const bool row_ok = m < p.m;
-    const int ea = row_ok ? p.exp_a[m] : 0;
-    double *C = static_cast<double *>(p.c) + (long long)m;
-#pragma unroll 1
-    for (int c = 0; c < BN; c += 32) {
-      double v[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = 0.0;
-#pragma unroll
-      for (int d = NACC - 1; d >= 0; --d) {
-        uint32_t r[32];
-        tmem_ld_32x32b_x32(tbase + d * BN + c, r);
-        tmem_ld_wait();
-        const double w = pow2_bits(-7 * (d + 2)); /* exact group weight */
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          v[j] = fma(static_cast<double>(static_cast<int>(r[j])), w, v[j]);
-      }
-      if (!row_ok) continue;
-#pragma unroll
-      for (int c8 = 0; c8 < 32; c8 += 8) {
-        const int nvalid = p.n - (n0 + c + c8);
-        if (nvalid <= 0) break;
-        double cv[8];
-        int eb[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) eb[j] = (j < nvalid) ? p.exp_b[n0 + c + c8 + j] : 0;
-        if (p.beta_nonzero) {
-#pragma unroll
-          for (int j = 0; j < 8; ++j)
-            cv[j] = (j < nvalid) ? C[(long long)(n0 + c + c8 + j) * p.ldc] : 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (j < nvalid) {
-            const int e = ea + eb[j];
-            double o;
-            if (ea == HCBK_OZ_NONFINITE || eb[j] == HCBK_OZ_NONFINITE)
-              o = __longlong_as_double(0x7ff8000000000000ll);
-            else if (ea == HCBK_OZ_ZERO || eb[j] == HCBK_OZ_ZERO)
-              o = 0.0;
-            else if (e >= -1022 && e <= 1023)
-              o = v[c8 + j] * pow2_bits(e); /* exact scaling */
-            else
-              o = ldexp(v[c8 + j], e);
-            o *= p.alpha_d;
-            if (p.beta_nonzero) o = fma(p.beta_d, cv[j], o);
-            C[(long long)(n0 + c + c8 + j) * p.ldc] = o;
-          }
-        }
-      }
-    }
-  }
-};
 
 /* ------------------------------------------------------------- kernel -- */
 
@@ -572,10 +526,6 @@ template <> struct KindTraits<0> { /* f16, 128-byte swizzle */
 template <> struct KindTraits<1> { /* bf16, 128-byte swizzle */
   static constexpr int ROWB = 128, BKE = 64, UK = 16, ESZ = 2;
   static constexpr uint32_t CFMT = 1, ABFMT = 1, LAYOUT = 2, SBO = 1024;
-};
-template <> struct KindTraits<2> { /* s8 -> s32, 64-byte swizzle */
-  static constexpr int ROWB = 64, BKE = 64, UK = 32, ESZ = 1;
-  static constexpr uint32_t CFMT = 2, ABFMT = 1, LAYOUT = 4, SBO = 512;
 };
 template <> struct KindTraits<3> { /* s8 -> s32, 128-byte swizzle: 128 K per slab */
   static constexpr int ROWB = 128, BKE = 128, UK = 32, ESZ = 1;
@@ -608,7 +558,7 @@ struct TcCfg {
       (OUT_BYTES ? OUT_OFF + OUT_BYTES : STAGES * STAGE_BYTES + BAR_BYTES) + 1024;
   static_assert(NBUF * ACC_COLS <= 512, "accumulators exceed TMEM");
   static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "BN");
-  static_assert(CG == 1 || (CG == 2 && KIND != 2 && !R::P3D && BN % 128 == 0), "CTA pair");
+  static_assert(CG == 1 || (CG == 2 && !R::P3D && BN % 128 == 0), "CTA pair");
   static_assert(SMEM_BYTES <= 232448, "shared memory");
 };
 
@@ -753,6 +703,32 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const int tm = tc_.m, tn = tc_.n;
         const int row0 = (tm * CG + (int)rank) * BM;               /* this CTA's A rows */
         const int col0 = tn * BN + (int)rank * (int)Cfg::B_ROWS;   /* this CTA's B rows */
+        if constexpr (CatK<EPI>::value) {
+          const int d = p.nplanes - 1 - plane;
+          for (int j = 0; j < (d + 1) * kblocks; ++j) {
+            const int ia = j / kblocks, kb = j - ia * kblocks;
+            if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
+              ok = false;
+              break;
+            }
+            if (rank == 0) mbar_expect_tx(&full[s], CG * Cfg::STAGE_BYTES);
+            uint8_t *st = smem + s * Cfg::STAGE_BYTES;
+            const int k0 = p.k0 + kb * BKE;
+            if constexpr (CG == 2) {
+              tma_load_3d_pair(st, &p.ta[0], mapa_shared(&full[s], 0), k0, row0, ia);
+              tma_load_3d_pair(st + Cfg::A_PLANE, &p.tb[0], mapa_shared(&full[s], 0), k0, col0,
+                               d - ia);
+            } else {
+              tma_load_3d(st, &p.ta[0], &full[s], k0, row0, ia);
+              tma_load_3d(st + Cfg::A_PLANE, &p.tb[0], &full[s], k0, col0, d - ia);
+            }
+            if (++s == STAGES) {
+              s = 0;
+              ph ^= 1u;
+            }
+          }
+          continue;
+        }
         const int kb_end = (w.c + 1) * chunk_kb < kblocks ? (w.c + 1) * chunk_kb : kblocks;
         for (int kb = w.c * chunk_kb; kb < kb_end; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
@@ -837,7 +813,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           }
           tc_fence_after();
           const uint32_t dbase = tmem_base + b * Cfg::ACC_COLS;
-          const int kend = (kc + chunk_kb < kblocks) ? kc + chunk_kb : kblocks;
+          int kend = (kc + chunk_kb < kblocks) ? kc + chunk_kb : kblocks;
+          if constexpr (CatK<EPI>::value)
+            kend = (p.nplanes - (w.t / tiles_per_plane)) * kblocks; /* (d + 1) * kblocks */
           for (int kb = kc; kb < kend; ++kb) {
             if (!mbar_wait<CG == 2>(&full[s], ph, p.err, ERR_TIMEOUT_MMA_FULL)) {
               ok = false;
@@ -855,7 +833,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
                 const uint64_t ad = smem_desc(aa, a_lbo, KT::SBO, KT::LAYOUT);
                 const uint64_t bd = smem_desc(ba, b_lbo, KT::SBO, KT::LAYOUT);
                 const uint32_t acc = (!fresh || kb > kc || kk > 0 || !R::first(pi)) ? 1u : 0u;
-                if constexpr (KIND == 2 || (KIND == 3 && CG == 1))
+                if constexpr (KIND == 3 && CG == 1)
                   mma_i8(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
                 else if constexpr (KIND == 3)
                   mma_i8_pair(dbase + R::pacc(pi) * BN, ad, bd, idesc, acc);
@@ -891,6 +869,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     OutStage ostage{Cfg::OUT_BYTES ? smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES : nullptr,
                     obar + 2 * q, 0u, 0u, 0};
     static_assert(!EPI::INPLACE || Cfg::OUT_BYTES > 0, "the modular epilogue stores by TMA");
+    static_assert(!EPI::PLANE_BATCH || Cfg::OUT_BYTES > 0, "plane-batched epilogues store by TMA");
     /* TMEM buffer released to the leader's MMA thread */
     auto release = [&](int b) {
       if (lane == 0) {
@@ -1048,29 +1027,6 @@ static int make_map(CUtensorMap *map, CUtensorMapDataType dt, int esz, const voi
               "stride=%llu box={%u,%u}\n",
               (int)r, base, (unsigned long long)inner, (unsigned long long)outer,
               (unsigned long long)(ld * esz), box_inner, box_outer);
-    return HCBK_ERR_ALIGN;
-  }
-  return HCBK_OK;
-}
-
-/* 3-D map over `planes` int8 slices: {K, rows, plane}, row pitch ld bytes,
- * plane pitch `pstride` bytes; box = {64, box_rows, 1}, 64-byte swizzle. */
-static int make_map_planes(CUtensorMap *map, const void *base, uint64_t kdim, uint64_t rows,
-                           uint64_t planes, uint64_t ld, uint64_t pstride, uint32_t box_rows) {
-  auto fn = encode_fn();
-  if (!fn) return HCBK_ERR_DRIVER;
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld & 15) || (pstride & 15)) return HCBK_ERR_ALIGN;
-  cuuint64_t dims[3] = {kdim, rows, planes};
-  cuuint64_t strides[2] = {ld, pstride};
-  cuuint32_t box[3] = {64, box_rows, 1};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides,
-                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    const char *e = getenv("HCBLAS_LOG");
-    if (e && e[0] == '1')
-      fprintf(stderr, "[hcblas] cuTensorMapEncodeTiled(3d) failed (%d)\n", (int)r);
     return HCBK_ERR_ALIGN;
   }
   return HCBK_OK;
@@ -1261,44 +1217,7 @@ extern "C" int64_t hcbk_ozaki_max_k(int slices) {
   if (slices < 1) return 0;
   /* |acc_d| <= slices * K * 127^2 must stay below 2^31 */
   const int64_t k = (int64_t)0x7fffffff / ((int64_t)slices * 127 * 127);
-  return k & ~int64_t(63);
-}
-
-/* Ozaki slice-product GEMM with the FP64 epilogue (one K range). */
-extern "C" int hcbk_ozaki_gemm_tc(const hcbk_ozaki_gemm *g, int *err, void *stream) {
-  if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > hcbk_ozaki_max_k(g->slices) ||
-      g->k0 + g->k > 0x7fffffff || g->k <= 0)
-    return HCBK_ERR_ARGS;
-  TcParams p;
-  memset(&p, 0, sizeof(p));
-  p.m = (int)g->m;
-  p.n = (int)g->n;
-  p.k = (int)g->k;
-  p.k0 = (int)g->k0;
-  const int s = g->slices;
-  const uint32_t bn = s <= 4 ? 128 : 64;
-  const uint64_t kdim = (uint64_t)(g->k0 + g->k);
-  int rc = make_map_planes(&p.ta[0], g->a_planes, kdim, g->m, s, g->ld_a, g->a_plane_stride, BM);
-  if (rc) return rc;
-  rc = make_map_planes(&p.tb[0], g->b_planes, kdim, g->n, s, g->ld_b, g->b_plane_stride, bn);
-  if (rc) return rc;
-  p.c = g->c;
-  p.ldc = g->ldc;
-  p.alpha_d = g->alpha;
-  p.beta_d = g->beta;
-  p.beta_nonzero = g->beta != 0.0;
-  p.exp_a = g->exp_a;
-  p.exp_b = g->exp_b;
-  p.err = err;
-  switch (s) {
-    case 3: return launch_tc<128, 4, RecipeOzaki<3>, 2, EpiOzaki, 0, 1>(p, stream);
-    case 4: return launch_tc<128, 3, RecipeOzaki<4>, 2, EpiOzaki, 0, 1>(p, stream);
-    case 5: return launch_tc<64, 3, RecipeOzaki<5>, 2, EpiOzaki, 0, 1>(p, stream);
-    case 6: return launch_tc<64, 3, RecipeOzaki<6>, 2, EpiOzaki, 0, 1>(p, stream);
-    case 7: return launch_tc<64, 2, RecipeOzaki<7>, 2, EpiOzaki, 0, 1>(p, stream);
-    case 8: return launch_tc<64, 2, RecipeOzaki<8>, 2, EpiOzaki, 0, 1>(p, stream);
-    default: return HCBK_ERR_ARGS;
-  }
+  return k & ~int64_t(127); /* whole 128-element K slabs of the int8 kernel */
 }
 
 /* 3-D map over `planes` f16 planes {K, rows, plane}: row pitch ld elements,
@@ -1358,6 +1277,51 @@ static int make_map_out_i16(CUtensorMap *map, void *base, uint64_t rows, uint64_
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
+}
+
+/* 3-D map over the int32 slice-group sums D {rows, cols, group}: column
+ * pitch ld elements, group pitch pstride elements; box {32, 32, 1}, no
+ * swizzle (the slice-group epilogue's tensor stores). */
+static int make_map_out_i32(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols,
+                            uint64_t planes, uint64_t ld, uint64_t pstride) {
+  auto fn = encode_fn();
+  if (!fn) return HCBK_ERR_DRIVER;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 4) & 15) || ((pstride * 4) & 15))
+    return HCBK_ERR_ALIGN;
+  cuuint64_t dims[3] = {rows, cols, planes};
+  cuuint64_t strides[2] = {ld * 4, pstride * 4};
+  cuuint32_t box[3] = {32, 32, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_INT32, 3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
+}
+
+extern "C" int hcbk_ozaki_groups_tc(const hcbk_ozaki_groups *g, int *err, void *stream) {
+  if (g->m <= 0 || g->n <= 0 || g->k <= 0 || g->m > 0x7fffffff || g->n > 0x7fffffff ||
+      g->k > hcbk_ozaki_max_k(g->slices) || g->k0 < 0 || g->k0 + g->k > 0x7fffffff ||
+      g->slices < 1 || g->slices > 8 || (g->k0 & 127) || !g->d)
+    return HCBK_ERR_ARGS;
+  TcParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = (int)g->m;
+  p.n = (int)g->n;
+  p.k = (int)g->k;
+  p.k0 = (int)g->k0;
+  const uint64_t kdim = (uint64_t)(g->k0 + g->k); /* zero fill beyond the range's end */
+  int rc = make_map_planes_s8(&p.ta[0], g->a_planes, kdim, g->m, g->slices, g->ld_a,
+                              g->a_plane_stride, BM);
+  if (rc) return rc;
+  rc = make_map_planes_s8(&p.tb[0], g->b_planes, kdim, g->n, g->slices, g->ld_b,
+                          g->b_plane_stride, g->pair ? 128 : 256);
+  if (rc) return rc;
+  rc = make_map_out_i32(&p.tc, g->d, g->m, g->n, g->slices, g->ldd, g->d_plane);
+  if (rc) return rc;
+  p.nplanes = g->slices;
+  p.err = err;
+  if (g->pair) return launch_tc<256, 6, RecipeSingle, 3, EpiI32Cat, 0, 2, 2>(p, stream);
+  return launch_tc<256, 4, RecipeSingle, 3, EpiI32Cat, 0, 2>(p, stream);
 }
 
 /* Every modulus of the CRT scheme in one launch: f16 residue planes

@@ -120,10 +120,28 @@ def test_ozaki_special_rows(handle, kind):
     assert np.linalg.norm(gv[ok] - ref[ok]) <= bound
 
 
+def test_ozaki_i8_pair_matches_single_cta(handle):
+    """The INT8 slice-group sums are exact, so the CTA-pair and single-CTA
+    launches give bit-identical results."""
+    rng = np.random.default_rng(41)
+    for order, ta, tb, M, N, K in CASES + [(O.COL, 0, 1, 600, 520, 300)]:
+        A, lda, B, ldb, C, ldc = make_case(rng, "d", order, ta, tb, M, N, K)
+        outs = []
+        for pair in (0, 2):
+            assert hb.set_tuning(handle, "tc_pair", pair) == 0
+            try:
+                outs.append(run_ozaki(handle, "i8", 6, order, ta, tb, M, N, K, 1.5, -0.25, A, lda,
+                                      B, ldb, C, ldc)[0])
+            finally:
+                hb.set_tuning(handle, "tc_pair", 1)
+        assert np.array_equal(outs[0], outs[1]), (order, ta, tb, M, N, K)
+
+
 @pytest.mark.parametrize("kind", ["i8", "f16"])
 def test_ozaki_long_k(handle, kind):
-    """K beyond one INT8 launch's INT32-exact range (~16.6k for s = 8) is split
-    into launches; the f16 kernel promotes per slab and runs it in one."""
+    """K beyond one INT8 launch's INT32-exact range (16640 for s = 8) is split
+    into launches of whole 128-element slabs; the f16 kernel promotes per
+    slab and runs it in one."""
     rng = np.random.default_rng(6)
     M, N, K = 40, 36, 17000
     s = 8 if kind == "i8" else 7
