@@ -26,7 +26,8 @@ Printed (rank 0, one JSON line):
               profiles/traffic.json
   cpu_baseline  host CBLAS (OpenBLAS's cblas_dgemm, all host threads) on a
               bounded column sample of the same problem
-  secondary   the stated targets at 8192^3: emulated vs native DGEMM
+  secondary   Ozaki-I INT8 slices 5 / 6 / 7 vs native on the headline
+              workload; the stated targets at 8192^3: emulated vs native DGEMM
               (column-major NT) and split-BF16 vs plain SGEMM (column-major
               TN, N(0,1) * 2^e, e ~ U{-8..8} per row / column, seed 2), each
               with its error against the oracle on sampled columns; plain
@@ -60,7 +61,7 @@ M = N = K = 4096
 ALPHA, BETA = 1.0, 0.0
 FLOP = 2.0 * M * N * K
 WORKLOAD = "dgemm_colmajor_NT_4096^3_alpha1_beta0_N01_seed1"
-MATH_NATIVE, MATH_SPLIT, MATH_CRT = 0, 1, 4
+MATH_NATIVE, MATH_SPLIT, MATH_OZAKI_INT8, MATH_CRT = 0, 1, 2, 4
 CRT_CANDIDATES = (12, 13, 14, 15, 16, 17, 18)
 
 
@@ -626,6 +627,34 @@ def run_secondary(hb, L, h, stream, torch, O, n=8192, reps=3):
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
+
+    # Ozaki-I INT8 slices at 5 / 6 / 7 on the headline workload (DGEMM
+    # column-major NT 4096^3, N(0,1) seed 1), with native FP64 beside them
+    n4 = 4096
+    rng = np.random.default_rng(1)
+    A4 = rng.standard_normal(n4 * n4)
+    B4 = rng.standard_normal(n4 * n4)
+    cols4 = np.random.default_rng(5).choice(n4, 8, replace=False)
+    dA, dB = hb.DeviceArray(h, A4), hb.DeviceArray(h, B4)
+    dC = hb.DeviceArray(h, nbytes=8 * n4 * n4, dtype=np.float64)
+    one, zero = np.array([1.0]), np.array([0.0])
+    f = lambda: L.hcblasDgemm(h, hb.HCBLAS_OP_N, hb.HCBLAS_OP_T, n4, n4, n4, one.ctypes.data,
+                              dA.ptr, n4, dB.ptr, n4, zero.ctypes.data, dC.ptr, n4)
+    d = {}
+    for name, mode, par in (("native", MATH_NATIVE, 0), ("ozaki_i8_s5", MATH_OZAKI_INT8, 5),
+                            ("ozaki_i8_s6", MATH_OZAKI_INT8, 6),
+                            ("ozaki_i8_s7", MATH_OZAKI_INT8, 7)):
+        hb.hcblasSetMathMode(h, mode, par)
+        ms = timed(f)
+        assert hb.device_error(h) == 0
+        err = oracle_err(O, dC.download().reshape(n4, n4).T, A4, n4, 0, B4, n4, 1, n4, n4, cols4,
+                         n4)
+        d[name] = {"path": hb.hcblasGetLastPath(h), "tflops": round(2.0 * n4 ** 3 / ms / 1e9, 2),
+                   "ms": round(ms, 3), "normwise_err": err}
+        if mode != MATH_NATIVE:
+            d[name]["speedup_vs_native"] = round(d["native"]["ms"] / ms, 3)
+    out["dgemm_colmajor_NT_4096^3_ozaki_int8_slices"] = d
+    del dA, dB, dC, A4, B4
 
     # DGEMM column-major NT, N(0,1) seed 1
     rng = np.random.default_rng(1)
