@@ -823,7 +823,9 @@ def run_secondary_small(hb, h, stream, torch, O, timed):
     for name, dt, modes in (("cgemm", np.complex64, (("plain_4m", MATH_NATIVE, 0),
                                                      ("split3m_bf16x6", MATH_SPLIT, 6))),
                             ("zgemm", np.complex128, (("native", MATH_NATIVE, 0),
-                                                      ("crt3m", MATH_CRT, 0)))):
+                                                      ("crt3m_m13", MATH_CRT, 13),
+                                                      ("crt3m_m14", MATH_CRT, 14),
+                                                      ("crt3m_m16", MATH_CRT, 16)))):
         A = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(dt)
         B = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(dt)
         C = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(dt)
@@ -843,7 +845,12 @@ def run_secondary_small(hb, h, stream, torch, O, timed):
             got = dC.download().reshape(n, n).T[:, cols]
             d[label] = {"path": hb.hcblasGetLastPath(h), "tflops": round(8 * n ** 3 / ms / 1e9, 2),
                         "ms": round(ms, 4), "normwise_err": O.normwise_rel_error(got, ref)}
-        k0, k1 = (m[0] for m in modes)
+        k0 = modes[0][0]
+        # the emulated entry with the fewest terms whose error is no worse
+        # than the plain / native kernel's
+        k1 = next((m[0] for m in modes[1:]
+                   if d[m[0]]["normwise_err"] <= d[k0]["normwise_err"]), modes[-1][0])
+        d["matched_error"] = k1
         d["speedup"] = round(d[k1]["tflops"] / d[k0]["tflops"], 3)
         out[f"{name}_colmajor_CN_2048^3"] = d
         del dA, dB, dC

@@ -381,36 +381,6 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   return HCBK_OK;
 }
 
-/* Choose the number of moduli and the integer width beta for K so that the
- * exact product fits the CRT range: prod(p_i) > 2 K 2^(2 beta).  `want` = 0
- * asks for full binary64 width (beta = 53) with the fewest moduli. */
-bool crt_plan(int64_t k, int want, int *nmod, int *beta) {
-  int count = 0;
-  const int *mods = hcbk_crt_moduli(&count);
-  const double lk = std::ceil(std::log2((double)(k > 1 ? k : 2)));
-  double cum = 0.0;
-  for (int i = 0; i < count; ++i) {
-    cum += std::log2((double)mods[i]);
-    const int n = i + 1;
-    int b = (int)std::floor((cum - 1.0 - lk - 0.01) / 2.0);
-    if (b > 53) b = 53;
-    if ((want == 0 && b >= 53) || (want == n)) {
-      if (b < 8) return false;
-      *nmod = n;
-      *beta = b;
-      return true;
-    }
-  }
-  if (want == 0) { /* K too large for 53 bits: use every modulus */
-    const int b = (int)std::floor((cum - 1.0 - lk - 0.01) / 2.0);
-    if (b < 8) return false;
-    *nmod = count;
-    *beta = b > 53 ? 53 : b;
-    return true;
-  }
-  return false;
-}
-
 /* CRT plan of the real (DGEMM) path.  Operands are scaled to integers of
  * up to 53 bits, x' = rint(x 2^(53 - e_r)) per row/column.  Two bounds keep
  * |P'| = |sum_k a'_k b'_k| below M / (2 * 2^0.01): K 2^106 when the moduli
@@ -511,7 +481,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
    * worst case, exponent and 8-bit fraction from the row norm instead */
   auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes) {
     return timed_launch(st, stream, "ozaki.exponents", [&] {
-      return norm ? hcbk_crt_row_scales(&p, 53 - shift, frac, inv, w, (int64_t)wbytes, stream)
+      return norm ? hcbk_crt_row_scales(&p, 53 - shift, 0, frac, inv, w, (int64_t)wbytes, stream)
                   : hcbk_ozaki_exponents(&p, stream);
     }, p.k_contig ? 1 : 2);
   };
@@ -611,13 +581,18 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
 
 /* ZGEMM on the CRT path: 3M in modular arithmetic (exact), so one complex
  * product costs three modular GEMMs per modulus.  Real and imaginary parts
- * of a row share the row's exponent; the CRT range covers |Re|, |Im| <=
- * 2 K 2^(2 beta) (crt_plan with 2K). */
+ * of a row share the row's scale.  The plan is the real one over the 2K
+ * reals of a complex row (crt_plan_rows(2K)): with full width every row is
+ * scaled to its largest part; with fewer moduli each complex row's norm is
+ * kept below 2^nb, which bounds |Re P'| and |Im P'| (both at most
+ * sum_k |a'_k||b'_k| <= ||a'|| ||b'||). */
 int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
               const char **path) {
   if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
-  int nmod = 0, beta_bits = 0;
-  if (!crt_plan(2 * a->k, want, &nmod, &beta_bits)) return HCBK_ERR_ARGS;
+  int nmod = 0, shift = 0;
+  bool norm = false;
+  if (!crt_plan_rows(2 * a->k, want, &nmod, &shift, &norm)) return HCBK_ERR_ARGS;
+  const int beta_bits = 53;
   const int *mods = hcbk_crt_moduli(nullptr);
   const bool i8 = st->crt_i8 && a->k <= HCBK_CRT_I8_MAX_K; /* as in dgemm_crt */
   const int esz = i8 ? 1 : 2;
@@ -629,13 +604,32 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   /* the real view of an MN-contiguous operand has two real rows per row */
   const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
   const size_t ea_bytes = up1k(sizeof(int) * a->m * 2), eb_bytes = up1k(sizeof(int) * a->n * 2);
-  const size_t total = ea_bytes + eb_bytes + 3 * (size_t)nmod * (a_pl + b_pl + t_pl);
+  /* norm scaling: per complex row the fraction and its reciprocal, and the
+   * row-norm pass's partials over the real view */
+  const size_t fa_bytes = norm ? up1k(2 * sizeof(double) * a->m) : 0;
+  const size_t fb_bytes = norm ? up1k(2 * sizeof(double) * a->n) : 0;
+  const size_t wa_bytes =
+      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a_k ? a->m : 2 * a->m,
+                                                           a_k ? 2 * a->k : a->k, a_k))
+           : 0;
+  const size_t wb_bytes =
+      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(b_k ? a->n : 2 * a->n,
+                                                           b_k ? 2 * a->k : a->k, b_k))
+           : 0;
+  const size_t total = ea_bytes + eb_bytes + fa_bytes + fb_bytes + wa_bytes + wb_bytes +
+                       3 * (size_t)nmod * (a_pl + b_pl + t_pl);
   char *ws = static_cast<char *>(ensure_workspace(st, total));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
   int *exp_a = reinterpret_cast<int *>(ws);
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
-  char *pa_base = ws + ea_bytes + eb_bytes;
+  double *frac_a = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes) : nullptr;
+  double *frac_b = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes + fa_bytes) : nullptr;
+  double *inv_a = norm ? frac_a + a->m : nullptr;
+  double *inv_b = norm ? frac_b + a->n : nullptr;
+  char *wa = ws + ea_bytes + eb_bytes + fa_bytes + fb_bytes, *wb = wa + wa_bytes;
+  ws = wb + wb_bytes; /* the planes follow */
+  char *pa_base = ws;
   char *pb_base = pa_base + 3 * nmod * a_pl;
   char *t_base = pb_base + 3 * nmod * b_pl;
   const double *A = reinterpret_cast<const double *>(a->a) + 2 * a->a_off;
@@ -658,8 +652,15 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   eb.rows = b_k ? a->n : 2 * a->n;
   eb.kdim = b_k ? 2 * a->k : a->k;
   eb.exps = exp_b;
-  int rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&ea, stream); }, ea.k_contig ? 1 : 2);
-  if (!rc) rc = timed_launch(st, stream, "ozaki.exponents", [&] { return hcbk_ozaki_exponents(&eb, stream); }, eb.k_contig ? 1 : 2);
+  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes) {
+    return timed_launch(st, stream, "ozaki.exponents", [&] {
+      return norm ? hcbk_crt_row_scales(&p, 53 - shift, p.k_contig ? 0 : 1, frac, inv, w,
+                                        (int64_t)wbytes, stream)
+                  : hcbk_ozaki_exponents(&p, stream);
+    }, p.k_contig ? 1 : 2);
+  };
+  int rc = exps(ea, frac_a, inv_a, wa, wa_bytes);
+  if (!rc) rc = exps(eb, frac_b, inv_b, wb, wb_bytes);
   if (rc) return rc;
 
   hcbk_zcrt_prep ra;
@@ -671,7 +672,8 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   ra.rows = a->m;
   ra.kdim = a->k;
   ra.exps = exp_a;
-  ra.exp_pair = !a_k;
+  ra.exp_pair = norm ? 0 : !a_k; /* norm scales are per complex row already */
+  ra.frac = frac_a;
   ra.beta_bits = beta_bits;
   ra.nmod = nmod;
   ra.planes = pa_base;
@@ -685,7 +687,8 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   rb.conj = a->op_b == HCBK_OP_C;
   rb.rows = a->n;
   rb.exps = exp_b;
-  rb.exp_pair = !b_k;
+  rb.exp_pair = norm ? 0 : !b_k;
+  rb.frac = frac_b;
   rb.planes = pb_base;
   rb.plane_stride = (int64_t)b_pl;
   rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&ra, stream); });
@@ -728,8 +731,10 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.ldr = ldt;
   cb.exp_a = exp_a;
   cb.exp_b = exp_b;
-  cb.exp_a_pair = !a_k;
-  cb.exp_b_pair = !b_k;
+  cb.exp_a_pair = norm ? 0 : !a_k;
+  cb.exp_b_pair = norm ? 0 : !b_k;
+  cb.inv_a = inv_a;
+  cb.inv_b = inv_b;
   cb.shift = 2 * beta_bits;
   cb.c = static_cast<char *>(a->c) + 16 * a->c_off;
   cb.ldc = a->ldc;

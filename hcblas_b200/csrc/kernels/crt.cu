@@ -706,6 +706,7 @@ struct ZResArgs {
   int64_t rows, kdim;
   const int *exps;
   int exp_pair;    /* exponent of row r = max(exps[2r], exps[2r+1]) */
+  const double *frac; /* optional row fractions: z * frac[r] is scaled */
   float im_sign;   /* -1 for a conjugate-transposed operand */
   int beta;
   int nmod;
@@ -747,6 +748,7 @@ __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
     const int64_t r = idx / kq;
     const int64_t k0 = (idx % kq) * 4;
     const int e = row_exp(a.exps, a.exp_pair, r);
+    const double f = a.frac ? a.frac[r] : 1.0;
     Limbs2 lr[2], li[2]; /* element pairs (0, 1), (2, 3); im carries the conj sign */
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -754,9 +756,9 @@ __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
           (k0 + 2 * j < a.kdim) ? a.src[r * a.ld + k0 + 2 * j] : make_double2(0.0, 0.0);
       const double2 z1 =
           (k0 + 2 * j + 1 < a.kdim) ? a.src[r * a.ld + k0 + 2 * j + 1] : make_double2(0.0, 0.0);
-      lr[j] = pair_limbs(limbs_of(z0.x, e, a.beta), limbs_of(z1.x, e, a.beta));
-      li[j] = pair_limbs(limbs_of(a.im_sign * z0.y, e, a.beta),
-                         limbs_of(a.im_sign * z1.y, e, a.beta));
+      lr[j] = pair_limbs(limbs_of(f * z0.x, e, a.beta), limbs_of(f * z1.x, e, a.beta));
+      li[j] = pair_limbs(limbs_of(a.im_sign * (f * z0.y), e, a.beta),
+                         limbs_of(a.im_sign * (f * z1.y), e, a.beta));
     }
     const int64_t left = a.kdim - k0;
     const int nk = left < 4 ? (int)left : 4;
@@ -836,9 +838,10 @@ __global__ void zcrt_res_rcontig(ZResArgs a) {
     const int64_t r = r0 + rl, k = k0 + 2 * kp;
     if (r >= a.rows || k >= a.kdim) continue;
     const int e = row_exp(a.exps, a.exp_pair, r);
+    const double f = a.frac ? a.frac[r] : 1.0;
     const double2 z0 = tile[2 * kp][rl], z1 = tile[2 * kp + 1][rl];
-    const Limbs r0l = limbs_of(z0.x, e, a.beta), i0l = limbs_of(z0.y, e, a.beta);
-    const Limbs r1l = limbs_of(z1.x, e, a.beta), i1l = limbs_of(z1.y, e, a.beta);
+    const Limbs r0l = limbs_of(f * z0.x, e, a.beta), i0l = limbs_of(f * z0.y, e, a.beta);
+    const Limbs r1l = limbs_of(f * z1.x, e, a.beta), i1l = limbs_of(f * z1.y, e, a.beta);
     const bool two = k + 1 < a.kdim;
     const bool vec = two && (a.plane_stride & (2 * ESZ - 1)) == 0 &&
                      (reinterpret_cast<uintptr_t>(a.planes + (r * a.ld_dst + k) * ESZ) &
@@ -962,8 +965,13 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
     if (row < a.g.m) {
       const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
       const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row);
-      const double re = acc_re.finish(a.g, ea, eb);
-      const double im = acc_im.finish(a.g, ea, eb);
+      double re = acc_re.finish(a.g, ea, eb);
+      double im = acc_im.finish(a.g, ea, eb);
+      if (a.g.inv_a) {
+        const double sc = a.g.inv_a[row] * a.g.inv_b[col];
+        re *= sc;
+        im *= sc;
+      }
       double2 *dst = a.c + row + col * a.ldc;
       double2 o;
       o.x = a.alpha.x * re - a.alpha.y * im;
@@ -1105,6 +1113,7 @@ extern "C" int hcbk_zcrt_residues(const hcbk_zcrt_prep *in, void *stream) {
   a.kdim = in->kdim;
   a.exps = in->exps;
   a.exp_pair = in->exp_pair;
+  a.frac = in->frac;
   a.im_sign = in->conj ? -1.0f : 1.0f;
   a.beta = in->beta_bits;
   a.nmod = in->nmod;
@@ -1148,8 +1157,8 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   a.g.ldr = in->ldr;
   a.g.exp_a = in->exp_a;
   a.g.exp_b = in->exp_b;
-  a.g.inv_a = nullptr;
-  a.g.inv_b = nullptr;
+  a.g.inv_a = in->inv_a;
+  a.g.inv_b = in->inv_b;
   a.g.shift = in->shift;
   a.g.c = nullptr;
   a.g.ldc = 0;

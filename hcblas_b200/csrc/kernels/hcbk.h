@@ -182,10 +182,13 @@ int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
  * a->exps and f_r in frac[r] (1/2 <= f <= 1, 8 significant bits; inv[r] =
  * RN(1 / f_r)), with |x| f 2^(53-e) < 2^53 and row norm
  * ||x(r,:)|| f 2^(53-e) <= 2^nb.  MN-contiguous operands need `work` of
- * hcbk_crt_row_exponents_workspace bytes (partial sums per K chunk). */
+ * hcbk_crt_row_exponents_workspace bytes (partial sums per K chunk).
+ * pair_rows (MN-contiguous only, even rows): rows 2r and 2r+1 share one
+ * scale (the real and imaginary rows of a complex operand's real view);
+ * exps / frac / inv then hold rows / 2 entries. */
 int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, int k_contig);
-int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, double *inv,
-                        void *work, int64_t work_bytes, void *stream);
+int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, int pair_rows, double *frac,
+                        double *inv, void *work, int64_t work_bytes, void *stream);
 int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream);
 
 /* Slice-product GEMM operands over K range [k0, k0 + k): a_planes M rows,
@@ -339,6 +342,7 @@ typedef struct hcbk_zcrt_prep {
   int64_t rows, kdim;
   const int *exps;
   int exp_pair;
+  const double *frac; /* optional row fractions (exp_pair 0): z * f_r is what gets scaled */
   int beta_bits;
   int nmod;
   void *planes;
@@ -361,6 +365,7 @@ typedef struct hcbk_zcrt_combine_args {
   const int *exp_a;
   const int *exp_b;
   int exp_a_pair, exp_b_pair;
+  const double *inv_a, *inv_b; /* optional reciprocals of the row fractions */
   int shift;
   void *c;
   int64_t ldc;

@@ -374,14 +374,38 @@ __global__ void crt_rowexp_kcontig(const double *src, int64_t ld, int64_t rows, 
     na_init(acc);
     if (VEC == 2) {
       const double2 *row2 = reinterpret_cast<const double2 *>(row);
-      for (int64_t k = lane; k < kdim / 2; k += 32) {
+      const int64_t n2 = kdim / 2;
+      int64_t k = lane;
+      for (; k + 7 * 32 < n2; k += 8 * 32) { /* eight 16-byte loads in flight per lane */
+        double2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = row2[k + 32 * u];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          m = max(m, max(abs_bits(v[u].x), abs_bits(v[u].y)));
+          na_add(acc, v[u].x);
+          na_add(acc, v[u].y);
+        }
+      }
+      for (; k < n2; k += 32) {
         const double2 v = row2[k];
         m = max(m, max(abs_bits(v.x), abs_bits(v.y)));
         na_add(acc, v.x);
         na_add(acc, v.y);
       }
     } else {
-      for (int64_t k = lane; k < kdim; k += 32) {
+      int64_t k = lane;
+      for (; k + 7 * 32 < kdim; k += 8 * 32) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = row[k + 32 * u];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          m = max(m, abs_bits(v[u]));
+          na_add(acc, v[u]);
+        }
+      }
+      for (; k < kdim; k += 32) {
         const double x = row[k];
         m = max(m, abs_bits(x));
         na_add(acc, x);
@@ -419,12 +443,12 @@ __global__ void crt_rowexp_rcontig(const double *src, int64_t ld, int64_t rows, 
     const double2 *p = reinterpret_cast<const double2 *>(src + r);
     const int64_t step = ld / 2;
     int64_t k = k0;
-    for (; k + 4 <= k1; k += 4) {
-      double2 v[4];
+    for (; k + 8 <= k1; k += 8) { /* eight 16-byte loads in flight per thread */
+      double2 v[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = p[(k + u) * step];
+      for (int u = 0; u < 8; ++u) v[u] = p[(k + u) * step];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         m[0] = max(m[0], abs_bits(v[u].x));
         m[VEC - 1] = max(m[VEC - 1], abs_bits(v[u].y));
         na_add(acc[0], v[u].x);
@@ -540,10 +564,12 @@ __global__ void __launch_bounds__(256) oz_groups_combine(const hcbk_ozaki_groups
 
 /* the K split of the MN-contiguous row-exponent pass */
 static void rowexp_split(int64_t rows, int64_t kdim, int64_t *ky, int64_t *kchunk) {
+  /* about four 256-thread blocks per SM in all: one wave */
   const int64_t gx = (rows + 511) / 512;
-  int64_t y = ((int64_t)hcbk_sm_count() * 8 + gx - 1) / gx;
+  int64_t y = ((int64_t)hcbk_sm_count() * 4 + gx - 1) / gx;
   if (y > 1024) y = 1024;
   int64_t kc = (kdim + y - 1) / y;
+  kc = (kc + 7) & ~int64_t(7);
   if (kc < 32) kc = 32;
   *ky = (kdim + kc - 1) / kc;
   *kchunk = kc;
@@ -616,10 +642,11 @@ extern "C" int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, 
   return ky * rows * (int64_t)(sizeof(unsigned long long) + sizeof(double) + sizeof(int)) + 256;
 }
 
-extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *frac, double *inv,
-                                   void *work, int64_t work_bytes, void *stream) {
+extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, int pair_rows, double *frac,
+                                   double *inv, void *work, int64_t work_bytes, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a->rows <= 0 || a->kdim <= 0 || !frac || !inv) return HCBK_ERR_ARGS;
+  if (pair_rows && (a->k_contig || (a->rows & 1))) return HCBK_ERR_ARGS;
   const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0;
   if (a->k_contig) {
     int64_t blocks = (a->rows * 32 + 255) / 256;
@@ -649,8 +676,11 @@ extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, double *fra
     int64_t fb = (a->rows * 32 + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (fb > cap) fb = cap;
-    crt_rowexp_finish<<<(unsigned)fb, 256, 0, st>>>(pm, pe, ps, a->rows, (int)ky, nb, a->exps,
-                                                     frac, inv);
+    /* partials sit [row][chunk]: two consecutive rows merged are one row of
+     * twice the chunks */
+    const int g = pair_rows ? 2 : 1;
+    crt_rowexp_finish<<<(unsigned)fb, 256, 0, st>>>(pm, pe, ps, a->rows / g, (int)ky * g, nb,
+                                                     a->exps, frac, inv);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -159,18 +159,6 @@ CRT_MODULI = [255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 1
 CRT_CASES = CASES + [(O.COL, 0, 1, 160, 96, 2500), (O.ROW, 1, 0, 300, 260, 4100)]
 
 
-def crt_plan(K, want=0):
-    """Moduli count and integer width beta, as the library chooses them."""
-    lk = np.ceil(np.log2(max(K, 2)))
-    cum = 0.0
-    for i, p in enumerate(CRT_MODULI):
-        cum += np.log2(p)
-        b = min(53, int(np.floor((cum - 1.0 - lk - 0.01) / 2.0)))
-        if (want == 0 and b >= 53) or want == i + 1:
-            return i + 1, b
-    return len(CRT_MODULI), min(53, int(np.floor((cum - 1.0 - lk - 0.01) / 2.0)))
-
-
 def crt_plan_rows(K, want=0):
     """Moduli count and norm shift of the real (DGEMM) CRT path, as the
     library chooses them: integers of up to 53 bits; when the moduli are too
@@ -346,21 +334,23 @@ def test_ozaki_vs_native_accuracy(handle):
 # ---------------------------------------------------------------- ZGEMM --
 # 3M in modular arithmetic: Re = Ar Br - Ai Bi and Im = (Ar+Ai)(Br+Bi) - Ar Br
 # - Ai Bi are exact integers of 2K products; the only errors are the scaling
-# of each entry to a beta-bit integer (relative 2^-(beta+1) of its row /
-# column maximum over real and imaginary parts) and the final rounding, so
-# per element |dC| <= 2 |alpha| 2K 2^(e_m + f_n) (2^-beta + 2^-2beta) + 6u|C|
-# (P' to binary64 within 1.5 ulp, then the complex alpha).
+# of each complex row to integers (real and imaginary parts share the row's
+# scale, planned like a real row of 2K entries) and the final roundings, so
+# with the per-part rounding bounds d of row_deltas over the row's 2K reals
+# (|complex error| <= sqrt(2) d) per element
+#   |dC| <= |alpha| (sqrt2 da_m sum_k |b_kn| + sqrt2 db_n sum_k |a_mk| + 2K da db)
+#           + 10u|C| + 4u|beta C|.
 
-def zcrt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta_bits, ref, beta, C, ldc):
+def zcrt_bound_rows(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, shift, ref, beta, C, ldc):
     Ad = op_dense(A, order, ta, M, K, lda, 0)
     Bd = op_dense(B, order, tb, K, N, ldb, 0)
-    amax = np.maximum(np.abs(Ad.real), np.abs(Ad.imag)).max(axis=1)
-    bmax = np.maximum(np.abs(Bd.real), np.abs(Bd.imag)).max(axis=0)
-    ea = np.frexp(amax)[1].astype(np.float64)
-    eb = np.frexp(bmax)[1].astype(np.float64)
-    elem = 2 * abs(alpha) * 2 * K * np.exp2(ea[:, None] + eb[None, :]) * \
-        (2.0 ** -beta_bits + 2.0 ** (-2 * beta_bits))
-    out = np.linalg.norm(elem) + 6 * U * np.linalg.norm(ref)
+    da = row_deltas(np.concatenate([Ad.real, Ad.imag], axis=1), shift)
+    db = row_deltas(np.concatenate([Bd.T.real, Bd.T.imag], axis=1), shift)
+    r2 = np.sqrt(2.0)
+    elem = abs(alpha) * (r2 * da[:, None] * np.sum(np.abs(Bd), axis=0)[None, :] +
+                         r2 * np.sum(np.abs(Ad), axis=1)[:, None] * db[None, :] +
+                         2 * K * da[:, None] * db[None, :])
+    out = np.linalg.norm(elem) + 10 * U * np.linalg.norm(ref)
     if beta:
         out += 4 * U * abs(beta) * np.linalg.norm(O.view_c(C, order, M, N, ldc))
     return out
@@ -370,13 +360,13 @@ ZCASES = [(O.COL, 2, 0, 200, 150, 300), (O.COL, 0, 0, 129, 77, 64), (O.ROW, 1, 2
           (O.COL, 2, 1, 90, 260, 2100), (O.ROW, 0, 0, 64, 64, 33)]
 
 
-@pytest.mark.parametrize("want", [0, 14, 16])
+@pytest.mark.parametrize("want", [0, 12, 14, 16])
 def test_zgemm_crt_vs_dd_oracle(handle, want):
     rng = np.random.default_rng(700 + want)
     for order, ta, tb, M, N, K in ZCASES:
         A, lda, B, ldb, C, ldc = make_case(rng, "z", order, ta, tb, M, N, K)
         alpha, beta = (1 + 0.5j), (0.5 - 0.25j)
-        nmod, bb = crt_plan(2 * K, want)
+        nmod, bb = crt_plan_rows(2 * K, want)
         assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, want) == 0
         try:
             dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
@@ -391,7 +381,8 @@ def test_zgemm_crt_vs_dd_oracle(handle, want):
         assert path == f"tc.zcrt3m_m{nmod}", path
         _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
         err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
-        bound = zcrt_bound(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, bb, ref, beta, C, ldc)
+        bound = zcrt_bound_rows(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, bb, ref, beta, C,
+                                ldc)
         assert err <= bound, (want, nmod, bb, order, ta, tb, M, N, K, err, bound)
 
 
@@ -431,7 +422,7 @@ def test_crt_combine_many_tiles_per_block(handle, kind, order, ta, tb, M, N, K):
     if kind == "d":
         nmod, bb = crt_plan_rows(K, 0)
     else:
-        nmod, bb = crt_plan(2 * K, 0)
+        nmod, bb = crt_plan_rows(2 * K, 0)
     assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_OZAKI_CRT, 0) == 0
     try:
         dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
@@ -443,8 +434,8 @@ def test_crt_combine_many_tiles_per_block(handle, kind, order, ta, tb, M, N, K):
         hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
     _, ref = O.gemm(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
     err = np.linalg.norm(O.view_c(got, order, M, N, ldc) - ref)
-    bound = (crt_bound_rows if kind == "d" else zcrt_bound)(order, ta, tb, M, N, K, alpha, A, lda,
-                                                             B, ldb, bb, ref, beta, C, ldc)
+    bound_fn = crt_bound_rows if kind == "d" else zcrt_bound_rows
+    bound = bound_fn(order, ta, tb, M, N, K, alpha, A, lda, B, ldb, bb, ref, beta, C, ldc)
     assert err <= bound, (kind, nmod, bb, err, bound)
 
 
