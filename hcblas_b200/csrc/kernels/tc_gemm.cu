@@ -11,14 +11,15 @@
  *   (the "recipe" template describes which operand planes are multiplied
  *    into which accumulator, so emulated schemes reuse the same pipeline).
  *
- * CTA organisation (192 threads, 1 CTA per SM, persistent over output tiles):
+ * CTA organisation (192 threads -- 320 with eight epilogue warps --, 1 CTA
+ * per SM, persistent over output tiles):
  *   warp 0      TMA producer: one elected lane streams A/B K-slabs into a
  *               STAGES-deep shared-memory ring (full/empty mbarriers)
  *   warp 1      allocates TMEM; one lane issues tcgen05.mma for each K-slab
  *               and commits the slab back to the producer; accumulators are
  *               double-buffered in TMEM so the next tile's MMAs overlap the
  *               previous tile's epilogue
- *   warps 2..5  epilogue: tcgen05.ld (32 lanes x 32 columns per load) ->
+ *   warps 2..5  epilogue (2..9 with eight): tcgen05.ld (32 lanes x 32 columns) ->
  *               alpha*acc + beta*C in registers -> column-major C; each warp
  *               owns one 32-lane TMEM quadrant, so every store instruction
  *               writes 32 consecutive rows of one column (coalesced)
@@ -446,21 +447,38 @@ struct EpiI32Cat {
  * and B plane d - j / kblocks: D_d = sum_{i <= d} A_i B_(d-i)^T in one
  * accumulator. */
 template <class E, class = void> struct CatK : std::false_type {};
+/* epilogue warps (EPI_WARPS, default 4): with 8, two warps share each TMEM
+ * lane quadrant and take half of the tile's columns each (plane-batched
+ * TMA-store epilogues only) */
+template <class E, class = void> struct EpiWarps {
+  static constexpr int value = 4;
+};
+template <class E> struct EpiWarps<E, std::void_t<decltype(E::EPI_WARPS)>> {
+  static constexpr int value = E::EPI_WARPS;
+};
 template <class E> struct CatK<E, std::void_t<decltype(E::CAT_K)>> : std::bool_constant<E::CAT_K> {};
 
 /* Modular epilogue of the int8 path: the INT32 accumulator holds the
- * exact sum over all of K (|s| <= K 127^2 < 2^31), reduced once per tile:
- * s = hi 2^16 + lo (hi = s >> 16, 0 <= lo < 2^16) turns into the f32-exact
- * y = hi (2^16 mod p) + lo, |y| < 2^15 127 + 2^16 < 2^23, whose remainder
- * comes from the same rounding-constant quotient as the f16 path; stored as
- * symmetric int16 residues by TMA tensor stores. */
+ * exact sum over all of K (|s| <= K 127^2 <= 2114125824 for K <= 131072),
+ * reduced once per tile: s = hi 2^16 + lo with hi = (s + 2^15) >> 16 and
+ * |lo| <= 2^15 gives y = hi (2^16 mod p) + lo, exact in int32 with
+ * |y| <= 32259 * 127 + 2^15 < 2^22, so RND + y (RND = 1.5 * 2^23) is the f32
+ * with bit pattern 0x4B400000 + y.  Since |y / p| < 25200 the f32 quotient
+ * y * RN(1/p) is within 1.6e-3 of y / p, below the 1/(2p) >= 1.96e-3 that
+ * separates y / p (p odd) from any half-integer: q = rint(y / p) exactly,
+ * and RND + y - q p = RND + r with r already in [-(p-1)/2, (p-1)/2], whose
+ * low 16 bits are r as an int16.  Eight epilogue warps (two per TMEM lane
+ * quadrant, half of the columns each) read TMEM 64 columns at a time (one
+ * wait per 64) into two 32 x 32 int16 shared-memory boxes per warp, each
+ * written by one TMA tensor store. */
 struct EpiModPi8 {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = true;
   static constexpr float RND = 12582912.0f; /* 1.5 * 2^23 */
-  static constexpr uint32_t OUT_BOX_BYTES = EpiModP::OUT_BOX_BYTES;
-  static constexpr uint32_t OUT_WARP_BYTES = EpiModP::OUT_WARP_BYTES;
-  static constexpr uint32_t OUT_SMEM = EpiModP::OUT_SMEM;
+  static constexpr int EPI_WARPS = 8;
+  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * 2;
+  static constexpr uint32_t OUT_WARP_BYTES = 2 * OUT_BOX_BYTES;
+  static constexpr uint32_t OUT_SMEM = EPI_WARPS * OUT_WARP_BYTES;
 
   template <int BN>
   static __device__ __forceinline__ void prefetch_c(const TcParams &, int, int, OutStage &) {}
@@ -470,43 +488,46 @@ struct EpiModPi8 {
     static_assert(NACC == 0, "the modular epilogue stores through final_store");
   }
 
-  /* |v| < 2^22 to f32 through the 1.5 * 2^23 bit pattern */
-  static __device__ __forceinline__ float small_to_f(int v) {
-    return __int_as_float(0x4B400000 + v) - RND;
+  /* the symmetric residue of s as an int16 (see above) */
+  static __device__ __forceinline__ int16_t residue(uint32_t s, int c16, float pf, float inv) {
+    const int sv = static_cast<int>(s);
+    const int hi = (sv + 0x8000) >> 16;
+    const int y = hi * c16 + (sv - hi * 65536);
+    const float yr = __int_as_float(0x4B400000 + y); /* RND + y */
+    const float q = fmaf(yr - RND, inv, RND) - RND;
+    return static_cast<int16_t>(__float_as_int(fmaf(-q, pf, yr)));
   }
 
   template <int BN>
   static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint8_t *out,
                                                      int m0, int n0, int plane) {
+    static_assert(BN % 64 == 0, "64 columns per TMEM wait");
     const int lane = threadIdx.x & 31;
     const int mod = p.mod_tab[plane];
     const float pf = static_cast<float>(mod);
     const float inv = p.inv_mod_tab[plane];
-    const float hp = static_cast<float>((mod - 1) >> 1);
     int c16 = (1 << 16) % mod; /* 2^16 mod p, symmetric */
     if (c16 > (mod - 1) / 2) c16 -= mod;
-    const float c16f = static_cast<float>(c16);
 #pragma unroll 1
-    for (int c = 0; c < BN; c += 32) {
-      int16_t *box = reinterpret_cast<int16_t *>(out + ((c >> 5) & 1) * OUT_BOX_BYTES);
-      uint32_t ra[32];
+    for (int c = 0; c < BN; c += 64) {
+      int16_t *box = reinterpret_cast<int16_t *>(out);
+      uint32_t ra[32], rb[32];
       tmem_ld_32x32b_x32(ta + c, ra);
-      if (lane == 0) bulk_wait_read<1>(); /* the store from this box two groups ago */
+      tmem_ld_32x32b_x32(ta + c + 32, rb);
+      if (lane == 0) bulk_wait_read<0>(); /* the last two stores have read the boxes */
       __syncwarp();
       tmem_ld_wait();
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
-        const int sv = static_cast<int>(ra[j]);
-        const float y = fmaf(small_to_f(sv >> 16), c16f, small_to_f(sv & 0xFFFF));
-        float v = EpiModP::mod_f(y, pf, inv);
-        if (v > hp) v -= pf;
-        else if (v < -hp) v += pf;
-        box[j * 32 + lane] = static_cast<int16_t>(__float_as_int(v + RND));
+        box[j * 32 + lane] = residue(ra[j], c16, pf, inv);
+        box[1024 + j * 32 + lane] = residue(rb[j], c16, pf, inv);
       }
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) {
         tma_store_3d(&p.tc, box, m0, n0 + c, plane);
+        bulk_commit();
+        tma_store_3d(&p.tc, box + 1024, m0, n0 + c + 32, plane);
         bulk_commit();
       }
     }
@@ -617,7 +638,8 @@ __device__ __forceinline__ TileMN tile_mn(int t, int tiles_m, int tiles_n) {
 
 template <int BN, int STAGES, class R, int KIND, class EPI, int PROMOTE_KB = 0, int NBUF = 2,
           int CG = 1>
-__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
+__global__ void __launch_bounds__(64 + 32 * EpiWarps<EPI>::value, 1)
+    tc_gemm_kernel(const __grid_constant__ TcParams p) {
   using Cfg = TcCfg<BN, STAGES, R, KIND, NBUF, CG, EPI::OUT_SMEM>;
   using KT = typename Cfg::KT;
   constexpr int BKE = KT::BKE;
@@ -633,6 +655,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   uint64_t *tempty = tfull + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
   uint64_t *obar = tempty + 4; /* output staging: two C-load barriers per epilogue warp */
+  constexpr int EW = EpiWarps<EPI>::value;
+  static_assert(EW == 4 || (EW == 8 && EPI::PLANE_BATCH && !EPI::INPLACE && BN % 128 == 0),
+                "eight epilogue warps: plane-batched TMA-store epilogues");
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -647,10 +672,10 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4 * CG);
+      mbar_init(&tempty[b], EW * CG);
     }
     if constexpr (Cfg::OUT_BYTES > 0)
-      for (int b = 0; b < 8; ++b) mbar_init(&obar[b], 1);
+      for (int b = 0; b < 2 * EW; ++b) mbar_init(&obar[b], 1);
     mbar_fence_init();
   }
   if (warp == 0 && lane == 0) {
@@ -863,11 +888,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
   } else {
     /* ------------------------------------------------ epilogue -- */
-    const int q = warp & 3; /* TMEM lane quadrant of this warp */
+    const int q = warp & 3;      /* TMEM lane quadrant of this warp */
+    const int ew = warp - 2;     /* epilogue warp index */
+    const int half = ew >> 2;    /* with eight warps: which half of the columns */
     int ci = 0;
     bool ok = true;
-    OutStage ostage{Cfg::OUT_BYTES ? smem + Cfg::OUT_OFF + q * EPI::OUT_WARP_BYTES : nullptr,
-                    obar + 2 * q, 0u, 0u, 0};
+    OutStage ostage{Cfg::OUT_BYTES ? smem + Cfg::OUT_OFF + ew * EPI::OUT_WARP_BYTES : nullptr,
+                    obar + 2 * ew, 0u, 0u, 0};
     static_assert(!EPI::INPLACE || Cfg::OUT_BYTES > 0, "the modular epilogue stores by TMA");
     static_assert(!EPI::PLANE_BATCH || Cfg::OUT_BYTES > 0, "plane-batched epilogues store by TMA");
     /* TMEM buffer released to the leader's MMA thread */
@@ -922,9 +949,11 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         tc_fence_after();
         const uint32_t tbase =
             tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * Cfg::ACC_COLS;
-        if constexpr (EPI::PLANE_BATCH)
-          EPI::template final_store<BN>(p, tbase, ostage.box, m - lane, tn * BN, plane);
-        else
+        if constexpr (EPI::PLANE_BATCH) {
+          constexpr int COLS = BN / (EW / 4); /* this warp's columns */
+          EPI::template final_store<COLS>(p, tbase + half * COLS, ostage.box, m - lane,
+                                          tn * BN + half * COLS, plane);
+        } else
           EPI::template run<BN, R::NACC>(p, tbase, m, tn * BN, ostage);
         tc_fence_before();
         __syncwarp();
@@ -1049,7 +1078,7 @@ static int launch_tc(TcParams &p, void *stream) {
   attr[0].val.clusterDim.x = CG;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
-  cfg.blockDim = dim3(192, 1, 1);
+  cfg.blockDim = dim3(64 + 32 * EpiWarps<EPI>::value, 1, 1);
   cfg.dynamicSmemBytes = Cfg::SMEM_BYTES;
   cfg.stream = static_cast<cudaStream_t>(stream);
   cfg.attrs = attr;
