@@ -30,7 +30,8 @@ Printed (rank 0, one JSON line):
               bounded column sample of the same problem
   secondary   Ozaki-I INT8 slices 5 / 6 / 7 vs native on the headline
               workload; the stated targets at 8192^3: emulated vs native DGEMM
-              (column-major NT) and split-BF16 vs plain SGEMM (column-major
+              (column-major NT) and split-BF16 (and Ozaki-I INT8 with 3 / 4
+              slices) vs plain SGEMM (column-major
               TN, N(0,1) * 2^e, e ~ U{-8..8} per row / column, seed 2), each
               with its error against the oracle on sampled columns; plain
               SGEMM row-major NN 1024^3; the f16 strided batch 512 x 128^3 and
@@ -716,7 +717,9 @@ def run_secondary(hb, L, h, stream, torch, O, n=8192, reps=3):
         flop_s = 2.0 * n * n * kk
         s = {}
         for name, mode, par in (("plain", MATH_NATIVE, 0), ("split_bf16x6", MATH_SPLIT, 6),
-                                ("split_bf16x3", MATH_SPLIT, 3)):
+                                ("split_bf16x3", MATH_SPLIT, 3),
+                                ("ozaki_i8_s3", MATH_OZAKI_INT8, 3),
+                                ("ozaki_i8_s4", MATH_OZAKI_INT8, 4)):
             hb.hcblasSetMathMode(h, mode, par)
             dC.upload(C0)
             g()
@@ -730,6 +733,8 @@ def run_secondary(hb, L, h, stream, torch, O, n=8192, reps=3):
                        "ms": round(ms, 4), "normwise_err": err}
         s["speedup_x6_vs_plain"] = round(s["split_bf16x6"]["tflops"] / s["plain"]["tflops"], 3)
         s["speedup_x3_vs_plain"] = round(s["split_bf16x3"]["tflops"] / s["plain"]["tflops"], 3)
+        for nm in ("ozaki_i8_s3", "ozaki_i8_s4"):
+            s[f"speedup_{nm}_vs_plain"] = round(s[nm]["tflops"] / s["plain"]["tflops"], 3)
         out[key] = s
         del dA, dB, dC, A, B, C0
     out.update(run_secondary_small(hb, h, stream, torch, O, timed))

@@ -254,10 +254,24 @@ int cgemm_split3m(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void 
  * exactly in INT32 on the int8 tensor cores (K split so that every group sum
  * stays exact), then an FP64 element-wise weighting pass; 8-bit slices in
  * binary16: f16 tensor cores with per-slab FP64 promotion. */
-int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, void *stream,
+int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16, void *stream,
                 const char **path) {
-  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
+  if (a_in->batch != 1 || a_in->a_array) return HCBK_ERR_ARGS;
   if (s < 3 || s > (f16 ? 7 : 8)) return HCBK_ERR_ARGS;
+  /* SGEMM on the INT8 path: the FP32 operands are widened to FP64 copies in
+   * the workspace (exact), which the FP64 exponent and slicing passes read;
+   * the group combine rounds the FP64 result once into the FP32 C */
+  const bool f32 = a_in->dtype == HCBK_S;
+  if (f32 && f16) return HCBK_ERR_ARGS;
+  hcbk_gemm_args aw = *a_in;
+  const hcbk_gemm_args *a = &aw;
+  const int64_t a_inner = a_in->op_a == HCBK_OP_N ? a_in->m : a_in->k;
+  const int64_t a_outer = a_in->op_a == HCBK_OP_N ? a_in->k : a_in->m;
+  const int64_t b_inner = a_in->op_b == HCBK_OP_N ? a_in->k : a_in->n;
+  const int64_t b_outer = a_in->op_b == HCBK_OP_N ? a_in->n : a_in->k;
+  const int64_t lda64 = (a_inner + 1) & ~int64_t(1), ldb64 = (b_inner + 1) & ~int64_t(1);
+  const size_t wide_a = f32 ? (((size_t)lda64 * a_outer * 8 + 1023) & ~size_t(1023)) : 0;
+  const size_t wide_b = f32 ? (((size_t)ldb64 * b_outer * 8 + 1023) & ~size_t(1023)) : 0;
   const int esz = f16 ? 2 : 1;
   const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for either slice type */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
@@ -266,10 +280,30 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
   /* int8 path: the s slice-group INT32 sums of C, column-major */
   const int64_t ldd = (a->m + 3) & ~int64_t(3);
   const size_t d_bytes = f16 ? 0 : up1k((size_t)s * ldd * a->n * sizeof(int32_t));
-  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl) + d_bytes;
+  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl) + d_bytes + wide_a + wide_b;
   char *ws = static_cast<char *>(ensure_workspace(st, total));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
+  if (f32) {
+    double *wa = reinterpret_cast<double *>(ws + (total - wide_a - wide_b));
+    double *wb = reinterpret_cast<double *>(ws + (total - wide_b));
+    int rc = timed_launch(st, stream, "ozaki.widen", [&] {
+      return hcbk_widen_f32(static_cast<const float *>(a_in->a) + a_in->a_off, a_in->lda, a_inner,
+                            a_outer, wa, lda64, stream);
+    });
+    if (!rc)
+      rc = timed_launch(st, stream, "ozaki.widen", [&] {
+        return hcbk_widen_f32(static_cast<const float *>(a_in->b) + a_in->b_off, a_in->ldb,
+                              b_inner, b_outer, wb, ldb64, stream);
+      });
+    if (rc) return rc;
+    aw.a = wa;
+    aw.a_off = 0;
+    aw.lda = lda64;
+    aw.b = wb;
+    aw.b_off = 0;
+    aw.ldb = ldb64;
+  }
   int *exp_a = reinterpret_cast<int *>(ws);
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
   char *pa_base = ws + ea_bytes + eb_bytes;
@@ -311,7 +345,10 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
                                   "tc.ozaki_i8_s6", "tc.ozaki_i8_s7", "tc.ozaki_i8_s8"};
   static const char *names16[8] = {"", "", "", "tc.ozaki_f16_s3", "tc.ozaki_f16_s4",
                                     "tc.ozaki_f16_s5", "tc.ozaki_f16_s6", "tc.ozaki_f16_s7"};
-  *path = f16 ? names16[s] : names[s];
+  static const char *names32[9] = {"", "", "", "tc.sozaki_i8_s3", "tc.sozaki_i8_s4",
+                                   "tc.sozaki_i8_s5", "tc.sozaki_i8_s6", "tc.sozaki_i8_s7",
+                                   "tc.sozaki_i8_s8"};
+  *path = f16 ? names16[s] : f32 ? names32[s] : names[s];
   if (!f16) {
     /* one launch of every slice group per K range (INT32 exactness bounds
      * the range), then the FP64 weighting, scaling and alpha / beta */
@@ -340,7 +377,8 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a, int s, bool f16, v
     cb.d_plane = ldd * a->n;
     cb.exp_a = exp_a;
     cb.exp_b = exp_b;
-    cb.c = static_cast<double *>(a->c) + a->c_off;
+    cb.c = f32 ? nullptr : static_cast<double *>(a->c) + a->c_off;
+    cb.c_f32 = f32 ? static_cast<float *>(a->c) + a->c_off : nullptr;
     cb.ldc = a->ldc;
     cb.alpha = a->alpha_re;
     for (int64_t k0 = 0; k0 < a->k; k0 += kmax) {
@@ -839,6 +877,13 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     int rc = cgemm_split3m(st, a, terms, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] complex split-bf16 path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_S && st->math_mode == 2 /* HCBLAS_MATH_OZAKI_INT8 */ && a->batch == 1 &&
+      !a->a_array) {
+    const int s = st->math_param > 0 ? st->math_param : 4; /* 28 bits >= FP32's 24 */
+    int rc = dgemm_ozaki(st, a, s, false, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] sgemm ozaki path declined (%d)\n", rc);
   }
   if (a->dtype == HCBK_D && (st->math_mode == 2 || st->math_mode == 3) && a->batch == 1 &&
       !a->a_array) {

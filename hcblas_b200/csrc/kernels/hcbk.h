@@ -240,9 +240,14 @@ typedef struct hcbk_ozaki_groups_combine_args {
   const int *exp_a;
   const int *exp_b;
   double *c;
+  float *c_f32; /* when set, C is FP32 (c unused): the FP64 result rounded once */
   int64_t ldc;
   double alpha, beta;
 } hcbk_ozaki_groups_combine_args;
+/* dst(i, j) = src(i, j) widened to FP64 for i < inner, j < outer (lines of
+ * `inner` contiguous elements, ld / ldd apart). */
+int hcbk_widen_f32(const float *src, int64_t ld, int64_t inner, int64_t outer, double *dst,
+                   int64_t ldd, void *stream);
 int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a, void *stream);
 /* The product on the f16 tensor path: binary16 planes holding 8-bit
  * integer slices (ld_a / ld_b in elements), weights 2^(-8(i+j+2)); any K

@@ -540,7 +540,6 @@ __global__ void __launch_bounds__(256) oz_groups_combine(const hcbk_ozaki_groups
       v[3] = fma(i32_to_d(q.w), w, v[3]);
     }
     const int eb = a.exp_b[col];
-    double *dst = a.c + col * a.ldc + r0;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       if (r0 + u >= a.m) break;
@@ -556,9 +555,27 @@ __global__ void __launch_bounds__(256) oz_groups_combine(const hcbk_ozaki_groups
                                       : ldexp(v[u], e);
       }
       o *= a.alpha;
-      if (a.beta != 0.0) o = fma(a.beta, dst[u], o);
-      dst[u] = o;
+      const int64_t ci = col * a.ldc + r0 + u;
+      if (a.c_f32) {
+        if (a.beta != 0.0) o = fma(a.beta, static_cast<double>(a.c_f32[ci]), o);
+        a.c_f32[ci] = static_cast<float>(o);
+      } else {
+        if (a.beta != 0.0) o = fma(a.beta, a.c[ci], o);
+        a.c[ci] = o;
+      }
     }
+  }
+}
+
+/* FP32 -> FP64 copy of a strided matrix (one element per thread, lines of
+ * `inner` elements) */
+__global__ void __launch_bounds__(256) widen_f32(const float *src, int64_t ld, int64_t inner,
+                                                 int64_t outer, double *dst, int64_t ldd) {
+  const int64_t total = inner * outer;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = i / inner, r = i - j * inner;
+    dst[j * ldd + r] = static_cast<double>(src[j * ld + r]);
   }
 }
 
@@ -618,6 +635,18 @@ extern "C" int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a
   const int64_t cap = (int64_t)hcbk_sm_count() * 16;
   if (blocks > cap) blocks = cap;
   oz_groups_combine<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(*a);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_widen_f32(const float *src, int64_t ld, int64_t inner, int64_t outer,
+                              double *dst, int64_t ldd, void *stream) {
+  if (inner <= 0 || outer <= 0 || ld < inner || ldd < inner) return HCBK_ERR_ARGS;
+  const int64_t total = inner * outer;
+  int64_t blocks = (total + 255) / 256;
+  const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  widen_f32<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(src, ld, inner, outer,
+                                                                             dst, ldd);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
