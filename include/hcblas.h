@@ -373,24 +373,33 @@ int hcblasLibGemmBatched(hcblasHandle_t h, int dtype, int order, char typeA, cha
  *                          products on tcgen05 tensor cores, FP32 accumulate
  *                          (`param` = number of terms: 3, or 6 for a 3-way split);
  *                          C runs 3M: Ar Br, Ai Bi, (Ar+Ai)(Br+Bi)
- *   HCBLAS_MATH_OZAKI_INT8 D: Ozaki scheme, FP64 operands scaled per row/col
- *                          and sliced into `param` INT8 slices, slice products
- *                          exact in INT32 on tcgen05 tensor cores
- *                          (`param` = 3..8 slices of 7 bits; 0 = 7 slices)
+ *   HCBLAS_MATH_OZAKI_INT8 D/S: Ozaki scheme, operands scaled per row/col and
+ *                          sliced into `param` INT8 slices; for every slice
+ *                          weight one INT32 GEMM (exact) over the concatenated
+ *                          K of its slice pairs on the int8 tensor cores, then
+ *                          an FP64 weighting pass (`param` = 3..8 slices of 7
+ *                          bits; 0 = 7 slices for D, 4 for S).  S widens its
+ *                          FP32 operands to FP64 first and rounds the FP64
+ *                          result once into C.
  *   HCBLAS_MATH_OZAKI_F16  D: the same scheme with 8-bit integer slices held
  *                          in binary16, products on the tcgen05 f16 path with
  *                          FP32 sums kept exact (integers < 2^24) and promoted
  *                          to FP64 per 32-element K slab (`param` = 3..7
  *                          slices of 8 bits; 0 = 7 slices, 56 bits)
  *   HCBLAS_MATH_OZAKI_CRT  D/Z: integer-modular (CRT) scheme: operands scaled
- *                          to beta-bit integers per row/column, residues
- *                          modulo pairwise-coprime odd moduli <= 255 in
- *                          binary16, one exact tensor-core GEMM per modulus,
- *                          Garner reconstruction in double-double
+ *                          per row/column to integers of up to 53 bits,
+ *                          residues modulo pairwise-coprime odd moduli <= 255
+ *                          as int8 (tuning knob "crt_i8"), all moduli's exact
+ *                          GEMMs in one int8 tensor-core launch, reconstruction
+ *                          by the CRT weighted sum in binary64 chunks
  *                          (`param` = number of moduli 8..20; 0 = the fewest
- *                          giving beta = 53 bits for the call's K); Z runs 3M
- *                          in modular arithmetic (three exact GEMMs per
- *                          modulus) with the range of 2K products. */
+ *                          keeping all 53 bits of every row for the call's
+ *                          K).  With fewer moduli each row is scaled so that
+ *                          its norm fits the range (Cauchy-Schwarz); 14 moduli
+ *                          match native FP64 accuracy at K = 4096-8192.  Z runs
+ *                          3M in modular arithmetic (three exact GEMMs per
+ *                          modulus), its complex rows planned like real rows
+ *                          of 2K entries. */
 enum {
   HCBLAS_MATH_NATIVE = 0,
   HCBLAS_MATH_SPLIT_BF16 = 1,
