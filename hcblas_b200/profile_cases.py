@@ -175,6 +175,8 @@ CASES = {
     "dgemm_crt15_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096, 4, 15),
     "dgemm_crt14_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096, 4, 14),
     "dgemm_ozaki_i8_s6_nt_4096": lambda h: _real(h, np.float64, N_, T_, 4096, 4096, 4096, 2, 6),
+    "sgemm_ozaki_i8_s4_tn_4096_beta1": lambda h: _real(h, np.float32, T_, N_, 4096, 4096, 4096,
+                                                       2, 4, beta=1.0),
     "cublas_int8_8192": _cublas_int8,
     "cgemm_plain_cn_2048": lambda h: _complex(h, np.complex64, C_, N_, 2048, 2048, 2048),
     "cgemm_split3m_cn_2048": lambda h: _complex(h, np.complex64, C_, N_, 2048, 2048, 2048, 1, 6),
