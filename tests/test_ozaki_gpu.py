@@ -285,6 +285,28 @@ def test_crt_i8_matches_f16(handle, want):
         assert np.array_equal(outs[0], outs[1]), (want, order, ta, tb, M, N, K)
 
 
+def test_crt_k_beyond_int8_range(handle):
+    """K above 131072 (the INT32-exact range of the int8 modular GEMM) falls
+    back to the binary16 residue path, which reduces every 1024 K: the result
+    equals the forced binary16 path bit for bit and meets the bound."""
+    rng = np.random.default_rng(91)
+    M, N, K = 40, 36, 131072 + 200
+    A, lda, B, ldb, C, ldc = make_case(rng, "d", O.COL, 1, 0, M, N, K)
+    got, path = run_crt(handle, 14, O.COL, 1, 0, M, N, K, 1.0, 0.5, A, lda, B, ldb, C, ldc)
+    assert path == "tc.crt_m14", path
+    assert hb.set_tuning(handle, "crt_i8", 0) == 0
+    try:
+        forced, _ = run_crt(handle, 14, O.COL, 1, 0, M, N, K, 1.0, 0.5, A, lda, B, ldb, C, ldc)
+    finally:
+        hb.set_tuning(handle, "crt_i8", 1)
+    assert np.array_equal(got, forced)
+    _, ref = O.gemm(O.COL, 1, 0, M, N, K, 1.0, A, lda, B, ldb, 0.5, C, ldc)
+    _, shift = crt_plan_rows(K, 14)
+    err = np.linalg.norm(O.view_c(got, O.COL, M, N, ldc) - ref)
+    assert err <= crt_bound_rows(O.COL, 1, 0, M, N, K, 1.0, A, lda, B, ldb, shift, ref, 0.5, C,
+                                 ldc)
+
+
 def test_crt_special_and_hard_range(handle):
     rng = np.random.default_rng(12)
     M, N, K = 96, 80, 700
