@@ -269,7 +269,8 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   const int64_t a_outer = a_in->op_a == HCBK_OP_N ? a_in->k : a_in->m;
   const int64_t b_inner = a_in->op_b == HCBK_OP_N ? a_in->k : a_in->n;
   const int64_t b_outer = a_in->op_b == HCBK_OP_N ? a_in->n : a_in->k;
-  const int64_t lda64 = (a_inner + 1) & ~int64_t(1), ldb64 = (b_inner + 1) & ~int64_t(1);
+  /* even pitches (16-byte double pairs), multiples of 4 when the FP32 lines are */
+  const int64_t lda64 = (a_inner + 3) & ~int64_t(3), ldb64 = (b_inner + 3) & ~int64_t(3);
   const size_t wide_a = f32 ? (((size_t)lda64 * a_outer * 8 + 1023) & ~size_t(1023)) : 0;
   const size_t wide_b = f32 ? (((size_t)ldb64 * b_outer * 8 + 1023) & ~size_t(1023)) : 0;
   const int esz = f16 ? 2 : 1;

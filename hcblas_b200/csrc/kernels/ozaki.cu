@@ -567,15 +567,25 @@ __global__ void __launch_bounds__(256) oz_groups_combine(const hcbk_ozaki_groups
   }
 }
 
-/* FP32 -> FP64 copy of a strided matrix (one element per thread, lines of
- * `inner` elements) */
+/* FP32 -> FP64 copy of a strided matrix, lines of `inner` elements.  VEC =
+ * 4: four consecutive elements per thread (16-byte loads, two 16-byte
+ * stores; inner, ld and ldd multiples of 4, 16-byte aligned bases). */
+template <int VEC>
 __global__ void __launch_bounds__(256) widen_f32(const float *src, int64_t ld, int64_t inner,
                                                  int64_t outer, double *dst, int64_t ldd) {
-  const int64_t total = inner * outer;
+  const int64_t iv = inner / VEC;
+  const int64_t total = iv * outer;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t j = i / inner, r = i - j * inner;
-    dst[j * ldd + r] = static_cast<double>(src[j * ld + r]);
+    const int64_t j = i / iv, r = (i - j * iv) * VEC;
+    if constexpr (VEC == 4) {
+      const float4 v = *reinterpret_cast<const float4 *>(src + j * ld + r);
+      double2 *d = reinterpret_cast<double2 *>(dst + j * ldd + r);
+      d[0] = make_double2(v.x, v.y);
+      d[1] = make_double2(v.z, v.w);
+    } else {
+      dst[j * ldd + r] = static_cast<double>(src[j * ld + r]);
+    }
   }
 }
 
@@ -641,12 +651,18 @@ extern "C" int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a
 extern "C" int hcbk_widen_f32(const float *src, int64_t ld, int64_t inner, int64_t outer,
                               double *dst, int64_t ldd, void *stream) {
   if (inner <= 0 || outer <= 0 || ld < inner || ldd < inner) return HCBK_ERR_ARGS;
-  const int64_t total = inner * outer;
+  const bool v4 = (inner & 3) == 0 && (ld & 3) == 0 && (ldd & 3) == 0 &&
+                  (reinterpret_cast<uintptr_t>(src) & 15) == 0 &&
+                  (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+  const int64_t total = inner * outer / (v4 ? 4 : 1);
   int64_t blocks = (total + 255) / 256;
   const int64_t cap = (int64_t)hcbk_sm_count() * 16;
   if (blocks > cap) blocks = cap;
-  widen_f32<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(src, ld, inner, outer,
-                                                                             dst, ldd);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (v4)
+    widen_f32<4><<<(unsigned)blocks, 256, 0, st>>>(src, ld, inner, outer, dst, ldd);
+  else
+    widen_f32<1><<<(unsigned)blocks, 256, 0, st>>>(src, ld, inner, outer, dst, ldd);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
