@@ -258,21 +258,12 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
                 const char **path) {
   if (a_in->batch != 1 || a_in->a_array) return HCBK_ERR_ARGS;
   if (s < 3 || s > (f16 ? 7 : 8)) return HCBK_ERR_ARGS;
-  /* SGEMM on the INT8 path: the FP32 operands are widened to FP64 copies in
-   * the workspace (exact), which the FP64 exponent and slicing passes read;
-   * the group combine rounds the FP64 result once into the FP32 C */
+  /* SGEMM on the INT8 path: the exponent and slicing passes read the FP32
+   * operands directly (widened in registers, exact); the group combine rounds
+   * the FP64 result once into the FP32 C */
   const bool f32 = a_in->dtype == HCBK_S;
   if (f32 && f16) return HCBK_ERR_ARGS;
-  hcbk_gemm_args aw = *a_in;
-  const hcbk_gemm_args *a = &aw;
-  const int64_t a_inner = a_in->op_a == HCBK_OP_N ? a_in->m : a_in->k;
-  const int64_t a_outer = a_in->op_a == HCBK_OP_N ? a_in->k : a_in->m;
-  const int64_t b_inner = a_in->op_b == HCBK_OP_N ? a_in->k : a_in->n;
-  const int64_t b_outer = a_in->op_b == HCBK_OP_N ? a_in->n : a_in->k;
-  /* even pitches (16-byte double pairs), multiples of 4 when the FP32 lines are */
-  const int64_t lda64 = (a_inner + 3) & ~int64_t(3), ldb64 = (b_inner + 3) & ~int64_t(3);
-  const size_t wide_a = f32 ? (((size_t)lda64 * a_outer * 8 + 1023) & ~size_t(1023)) : 0;
-  const size_t wide_b = f32 ? (((size_t)ldb64 * b_outer * 8 + 1023) & ~size_t(1023)) : 0;
+  const hcbk_gemm_args *a = a_in;
   const int esz = f16 ? 2 : 1;
   const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for either slice type */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
@@ -281,30 +272,11 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   /* int8 path: the s slice-group INT32 sums of C, column-major */
   const int64_t ldd = (a->m + 3) & ~int64_t(3);
   const size_t d_bytes = f16 ? 0 : up1k((size_t)s * ldd * a->n * sizeof(int32_t));
-  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl) + d_bytes + wide_a + wide_b;
+  const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl) + d_bytes;
   char *ws = static_cast<char *>(ensure_workspace(st, total));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
-  if (f32) {
-    double *wa = reinterpret_cast<double *>(ws + (total - wide_a - wide_b));
-    double *wb = reinterpret_cast<double *>(ws + (total - wide_b));
-    int rc = timed_launch(st, stream, "ozaki.widen", [&] {
-      return hcbk_widen_f32(static_cast<const float *>(a_in->a) + a_in->a_off, a_in->lda, a_inner,
-                            a_outer, wa, lda64, stream);
-    });
-    if (!rc)
-      rc = timed_launch(st, stream, "ozaki.widen", [&] {
-        return hcbk_widen_f32(static_cast<const float *>(a_in->b) + a_in->b_off, a_in->ldb,
-                              b_inner, b_outer, wb, ldb64, stream);
-      });
-    if (rc) return rc;
-    aw.a = wa;
-    aw.a_off = 0;
-    aw.lda = lda64;
-    aw.b = wb;
-    aw.b_off = 0;
-    aw.ldb = ldb64;
-  }
+
   int *exp_a = reinterpret_cast<int *>(ws);
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
   char *pa_base = ws + ea_bytes + eb_bytes;
@@ -312,7 +284,8 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   int32_t *dsum = reinterpret_cast<int32_t *>(pb_base + s * b_pl);
 
   hcbk_ozaki_prep pa;
-  pa.src = static_cast<const double *>(a->a) + a->a_off;
+  pa.src = f32 ? nullptr : static_cast<const double *>(a->a) + a->a_off;
+  pa.src_f32 = f32 ? static_cast<const float *>(a->a) + a->a_off : nullptr;
   pa.ld = a->lda;
   pa.k_contig = a->op_a != HCBK_OP_N;
   pa.rows = a->m;
@@ -324,7 +297,8 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   pa.ld_dst = kp;
   pa.f16 = f16 ? 1 : 0;
   hcbk_ozaki_prep pb;
-  pb.src = static_cast<const double *>(a->b) + a->b_off;
+  pb.src = f32 ? nullptr : static_cast<const double *>(a->b) + a->b_off;
+  pb.src_f32 = f32 ? static_cast<const float *>(a->b) + a->b_off : nullptr;
   pb.ld = a->ldb;
   pb.k_contig = a->op_b == HCBK_OP_N;
   pb.rows = a->n;

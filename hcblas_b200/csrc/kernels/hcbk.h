@@ -175,6 +175,7 @@ typedef struct hcbk_ozaki_prep {
   int64_t plane_stride; /* bytes between planes */
   int64_t ld_dst;       /* elements between rows */
   int f16;              /* 0: int8 slices of 7 bits; 1: binary16 slices of 8 bits */
+  const float *src_f32; /* exponents and slices only: an FP32 source instead of src */
 } hcbk_ozaki_prep;
 int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
 
@@ -244,10 +245,7 @@ typedef struct hcbk_ozaki_groups_combine_args {
   int64_t ldc;
   double alpha, beta;
 } hcbk_ozaki_groups_combine_args;
-/* dst(i, j) = src(i, j) widened to FP64 for i < inner, j < outer (lines of
- * `inner` contiguous elements, ld / ldd apart). */
-int hcbk_widen_f32(const float *src, int64_t ld, int64_t inner, int64_t outer, double *dst,
-                   int64_t ldd, void *stream);
+
 int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a, void *stream);
 /* The product on the f16 tensor path: binary16 planes holding 8-bit
  * integer slices (ld_a / ld_b in elements), weights 2^(-8(i+j+2)); any K

@@ -64,16 +64,16 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
 
 /* K-contiguous source: one warp per row; VEC = 2 reads 16-byte pairs
  * (row start 16-byte aligned, even kdim) */
-template <int VEC>
-__global__ void oz_exp_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
+template <int VEC, typename T = double>
+__global__ void oz_exp_kcontig(const T *src, int64_t ld, int64_t rows, int64_t kdim,
                                int *exps) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = warp; r < rows; r += nwarps) {
     unsigned long long m = 0;
-    const double *row = src + r * ld;
-    if (VEC == 2) {
+    const T *row = src + r * ld;
+    if constexpr (VEC == 2) {
       const double2 *row2 = reinterpret_cast<const double2 *>(row);
       const int64_t k2 = kdim / 2;
       int64_t k = lane;
@@ -93,7 +93,7 @@ __global__ void oz_exp_kcontig(const double *src, int64_t ld, int64_t rows, int6
         m = max(m, abs_bits(v.y));
       }
     } else {
-      for (int64_t k = lane; k < kdim; k += 32) m = max(m, abs_bits(row[k]));
+      for (int64_t k = lane; k < kdim; k += 32) m = max(m, abs_bits(static_cast<double>(row[k])));
     }
     m = warp_max_u64(m);
     if (lane == 0) exps[r] = exp_of_bits(m);
@@ -104,14 +104,14 @@ __global__ void oz_exp_kcontig(const double *src, int64_t ld, int64_t rows, int6
  * partial maxima meet in exps[] (pre-set to HCBK_OZ_ZERO) via atomicMax.
  * VEC = 2: each thread owns two adjacent rows and reads 16-byte pairs (even
  * rows and ld, 16-byte aligned source); eight loads in flight. */
-template <int VEC>
-__global__ void oz_exp_rcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
+template <int VEC, typename T = double>
+__global__ void oz_exp_rcontig(const T *src, int64_t ld, int64_t rows, int64_t kdim,
                                int64_t kchunk, int *exps) {
   const int64_t r = VEC * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
   if (r >= rows) return;
   const int64_t k0 = (int64_t)blockIdx.y * kchunk;
   const int64_t k1 = (k0 + kchunk < kdim) ? k0 + kchunk : kdim;
-  if (VEC == 2) {
+  if constexpr (VEC == 2) {
     unsigned long long m0 = 0, m1 = 0;
     const double2 *p = reinterpret_cast<const double2 *>(src + r);
     const int64_t step = ld / 2;
@@ -139,11 +139,11 @@ __global__ void oz_exp_rcontig(const double *src, int64_t ld, int64_t rows, int6
     for (; k + 4 <= k1; k += 4) {
       double v[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = src[r + (k + u) * ld];
+      for (int u = 0; u < 4; ++u) v[u] = static_cast<double>(src[r + (k + u) * ld]);
 #pragma unroll
       for (int u = 0; u < 4; ++u) m = max(m, abs_bits(v[u]));
     }
-    for (; k < k1; ++k) m = max(m, abs_bits(src[r + k * ld]));
+    for (; k < k1; ++k) m = max(m, abs_bits(static_cast<double>(src[r + k * ld])));
     atomicMax(&exps[r], exp_of_bits(m));
   }
 }
@@ -185,8 +185,8 @@ __device__ __forceinline__ void slice_value(double x, int e, ST (&a)[S]) {
 
 /* K-contiguous source: 8 consecutive k per thread, one vector store of the
  * 8 slices per plane (8 bytes for int8, 16 bytes for binary16) */
-template <int S, typename ST>
-__global__ void oz_slice_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
+template <int S, typename ST, typename T = double>
+__global__ void oz_slice_kcontig(const T *src, int64_t ld, int64_t rows, int64_t kdim,
                                  const int *exps, char *planes, int64_t plane_stride,
                                  int64_t ld_dst) {
   struct alignas(8 * sizeof(ST)) Vec8 { ST v[8]; };
@@ -201,7 +201,7 @@ __global__ void oz_slice_kcontig(const double *src, int64_t ld, int64_t rows, in
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       ST a[S];
-      const double x = (k0 + j < kdim) ? src[r * ld + k0 + j] : 0.0;
+      const double x = (k0 + j < kdim) ? static_cast<double>(src[r * ld + k0 + j]) : 0.0;
       slice_value<S, ST>(x, e, a);
 #pragma unroll
       for (int i = 0; i < S; ++i) out[i].v[j] = a[i];
@@ -219,8 +219,8 @@ __global__ void oz_slice_kcontig(const double *src, int64_t ld, int64_t rows, in
 }
 
 /* MN-contiguous source: 32x32 tile through shared memory */
-template <int S, typename ST>
-__global__ void oz_slice_rcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
+template <int S, typename ST, typename T = double>
+__global__ void oz_slice_rcontig(const T *src, int64_t ld, int64_t rows, int64_t kdim,
                                  const int *exps, char *planes, int64_t plane_stride,
                                  int64_t ld_dst) {
   __shared__ double tile[32][33];
@@ -231,7 +231,7 @@ __global__ void oz_slice_rcontig(const double *src, int64_t ld, int64_t rows, in
   for (int i = 0; i < 4; ++i) {
     const int kl = ty + 8 * i;
     const int64_t r = r0 + tx, k = k0 + kl;
-    tile[kl][tx] = (r < rows && k < kdim) ? src[r + k * ld] : 0.0;
+    tile[kl][tx] = (r < rows && k < kdim) ? static_cast<double>(src[r + k * ld]) : 0.0;
   }
   __syncthreads();
 #pragma unroll
@@ -248,23 +248,29 @@ __global__ void oz_slice_rcontig(const double *src, int64_t ld, int64_t rows, in
   }
 }
 
-template <int S, typename ST>
-int launch_slice(const hcbk_ozaki_prep *a, cudaStream_t st) {
+template <int S, typename ST, typename T>
+int launch_slice_src(const hcbk_ozaki_prep *a, const T *src, cudaStream_t st) {
   char *planes = static_cast<char *>(a->planes);
   if (a->k_contig) {
     const int64_t total = a->rows * ((a->kdim + 7) / 8);
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    oz_slice_kcontig<S, ST><<<(unsigned)blocks, 256, 0, st>>>(
-        a->src, a->ld, a->rows, a->kdim, a->exps, planes, a->plane_stride, a->ld_dst);
+    oz_slice_kcontig<S, ST, T><<<(unsigned)blocks, 256, 0, st>>>(
+        src, a->ld, a->rows, a->kdim, a->exps, planes, a->plane_stride, a->ld_dst);
   } else {
     const int64_t gx = (a->rows + 31) / 32, gy = (a->kdim + 31) / 32;
     if (gy > 65535) return HCBK_ERR_ARGS;
-    oz_slice_rcontig<S, ST><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(
-        a->src, a->ld, a->rows, a->kdim, a->exps, planes, a->plane_stride, a->ld_dst);
+    oz_slice_rcontig<S, ST, T><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(
+        src, a->ld, a->rows, a->kdim, a->exps, planes, a->plane_stride, a->ld_dst);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+template <int S, typename ST>
+int launch_slice(const hcbk_ozaki_prep *a, cudaStream_t st) {
+  return a->src_f32 ? launch_slice_src<S, ST, float>(a, a->src_f32, st)
+                    : launch_slice_src<S, ST, double>(a, a->src, st);
 }
 
 template <int S>
@@ -567,28 +573,6 @@ __global__ void __launch_bounds__(256) oz_groups_combine(const hcbk_ozaki_groups
   }
 }
 
-/* FP32 -> FP64 copy of a strided matrix, lines of `inner` elements.  VEC =
- * 4: four consecutive elements per thread (16-byte loads, two 16-byte
- * stores; inner, ld and ldd multiples of 4, 16-byte aligned bases). */
-template <int VEC>
-__global__ void __launch_bounds__(256) widen_f32(const float *src, int64_t ld, int64_t inner,
-                                                 int64_t outer, double *dst, int64_t ldd) {
-  const int64_t iv = inner / VEC;
-  const int64_t total = iv * outer;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t j = i / iv, r = (i - j * iv) * VEC;
-    if constexpr (VEC == 4) {
-      const float4 v = *reinterpret_cast<const float4 *>(src + j * ld + r);
-      double2 *d = reinterpret_cast<double2 *>(dst + j * ldd + r);
-      d[0] = make_double2(v.x, v.y);
-      d[1] = make_double2(v.z, v.w);
-    } else {
-      dst[j * ldd + r] = static_cast<double>(src[j * ld + r]);
-    }
-  }
-}
-
 /* the K split of the MN-contiguous row-exponent pass */
 static void rowexp_split(int64_t rows, int64_t kdim, int64_t *ky, int64_t *kchunk) {
   /* about four 256-thread blocks per SM in all: one wave */
@@ -607,6 +591,27 @@ static void rowexp_split(int64_t rows, int64_t kdim, int64_t *ky, int64_t *kchun
 extern "C" int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a->rows <= 0 || a->kdim <= 0) return HCBK_ERR_ARGS;
+  if (a->src_f32) { /* FP32 source: element loads, widened in registers */
+    if (a->k_contig) {
+      int64_t blocks = (a->rows * 32 + 255) / 256;
+      const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+      if (blocks > cap) blocks = cap;
+      oz_exp_kcontig<1, float><<<(unsigned)blocks, 256, 0, st>>>(a->src_f32, a->ld, a->rows,
+                                                                  a->kdim, a->exps);
+    } else {
+      const int64_t gx = (a->rows + 255) / 256;
+      int64_t ky = ((int64_t)hcbk_sm_count() * 8 + gx - 1) / gx;
+      if (ky > 1024) ky = 1024;
+      int64_t kchunk = (a->kdim + ky - 1) / ky;
+      if (kchunk < 32) kchunk = 32;
+      ky = (a->kdim + kchunk - 1) / kchunk;
+      if (ky > 65535) return HCBK_ERR_ARGS;
+      oz_fill<<<(unsigned)((a->rows + 255) / 256), 256, 0, st>>>(a->exps, a->rows, HCBK_OZ_ZERO);
+      oz_exp_rcontig<1, float><<<dim3((unsigned)gx, (unsigned)ky), 256, 0, st>>>(
+          a->src_f32, a->ld, a->rows, a->kdim, kchunk, a->exps);
+    }
+    return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+  }
   const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0;
   if (a->k_contig) {
     int64_t blocks = (a->rows * 32 + 255) / 256;
@@ -645,24 +650,6 @@ extern "C" int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a
   const int64_t cap = (int64_t)hcbk_sm_count() * 16;
   if (blocks > cap) blocks = cap;
   oz_groups_combine<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(*a);
-  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
-}
-
-extern "C" int hcbk_widen_f32(const float *src, int64_t ld, int64_t inner, int64_t outer,
-                              double *dst, int64_t ldd, void *stream) {
-  if (inner <= 0 || outer <= 0 || ld < inner || ldd < inner) return HCBK_ERR_ARGS;
-  const bool v4 = (inner & 3) == 0 && (ld & 3) == 0 && (ldd & 3) == 0 &&
-                  (reinterpret_cast<uintptr_t>(src) & 15) == 0 &&
-                  (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
-  const int64_t total = inner * outer / (v4 ? 4 : 1);
-  int64_t blocks = (total + 255) / 256;
-  const int64_t cap = (int64_t)hcbk_sm_count() * 16;
-  if (blocks > cap) blocks = cap;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (v4)
-    widen_f32<4><<<(unsigned)blocks, 256, 0, st>>>(src, ld, inner, outer, dst, ldd);
-  else
-    widen_f32<1><<<(unsigned)blocks, 256, 0, st>>>(src, ld, inner, outer, dst, ldd);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
