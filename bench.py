@@ -777,7 +777,7 @@ def run_secondary_small(hb, h, stream, torch, O, timed):
                                             "ms": round(ms, 4)}
     del dA, dB, dC
     # C4b: grouped 4096 problems, M, N, K log-uniform in [16, 1024], seed 3, mixed N/T
-    from hcblas_b200 import profile_cases
+    import bench_cases as profile_cases
     call, keep = profile_cases.CASES["hgemm_grouped_4096"](h)
     ms = timed(call)
     arr = keep[1]

@@ -1,7 +1,8 @@
-"""Named single-GEMM workloads for profiling the library's kernels.
+"""Named single-GEMM workloads for profiling the library's kernels (a
+harness beside bench.py, not part of the library package).
 
-    python -m hcblas_b200.profile_cases <case> [<case> ...]
-    python -m hcblas_b200.profile_cases --list
+    python bench_cases.py <case> [<case> ...]
+    python bench_cases.py --list
 
 Each case allocates its operands on cuda:0 (seeded, synthetic), makes one
 warm-up call, then one more call of the same GEMM through the public C ABI,

@@ -52,7 +52,7 @@ hcblasStatus gemv_one(Hcblaslibrary *h, const hc::accelerator_view &view, hcblas
     rc = timed_launch(st, stream, "blas2.scale", [&] { return hcbk_scale_c(&a, stream); });
   } else {
     const int64_t elems = hcbk_gemv_workspace_elems(m, n, trans, kMaxSplits);
-    void *ws = ensure_workspace(st, (size_t)elems * sizeof(T));
+    void *ws = ensure_workspace(st, (size_t)elems * sizeof(T), stream);
     if (!ws) return HCBLAS_INVALID;
     hcbk_gemv_args g;
     g.dtype = dtype_of<T>();

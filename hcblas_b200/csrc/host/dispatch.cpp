@@ -70,6 +70,14 @@ int hgemm_tc(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const c
     return HCBK_ERR_ALIGN;
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;
+  if (st->inject_timeout) { /* failure-detection test: one call, then disarmed */
+    st->inject_timeout = 0;
+    *path = "tc.h.128x128.inject_timeout";
+    const int rc = timed_launch(st, stream, *path,
+                                [&] { return hcbk_hgemm_tc_inject_timeout(a, err, stream); });
+    /* a shape the injection does not accept fails the call (no fallback) */
+    return rc == HCBK_ERR_ARGS || rc == HCBK_ERR_ALIGN ? HCBK_ERR_LAUNCH : rc;
+  }
   int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
   int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
   if (st->autotune && st->tc_pair == 1 && a->beta_re == 0.0) {
@@ -96,7 +104,7 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   const size_t a_plane = (size_t)a->m * kp * 2, b_plane = (size_t)a->n * kp * 2;
   const size_t a_bytes = (a_plane + 1023) & ~size_t(1023);
   const size_t b_bytes = (b_plane + 1023) & ~size_t(1023);
-  char *ws = static_cast<char *>(ensure_workspace(st, nplanes * (a_bytes + b_bytes)));
+  char *ws = static_cast<char *>(ensure_workspace(st, nplanes * (a_bytes + b_bytes), stream));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
 
@@ -168,7 +176,7 @@ int cgemm_split3m(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void 
   const size_t a_plane = up1k((size_t)a->m * kp * 2), b_plane = up1k((size_t)a->n * kp * 2);
   const size_t t_bytes = up1k((size_t)a->m * a->n * 4);
   const size_t total = 3 * nplanes * (a_plane + b_plane) + 3 * t_bytes;
-  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  char *ws = static_cast<char *>(ensure_workspace(st, total, stream));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
   char *pa_base = ws, *pb_base = ws + 3 * nplanes * a_plane;
@@ -273,7 +281,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   const int64_t ldd = (a->m + 3) & ~int64_t(3);
   const size_t d_bytes = f16 ? 0 : up1k((size_t)s * ldd * a->n * sizeof(int32_t));
   const size_t total = ea_bytes + eb_bytes + s * (a_pl + b_pl) + d_bytes;
-  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  char *ws = static_cast<char *>(ensure_workspace(st, total, stream));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
 
@@ -462,7 +470,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
       norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a->n, a->k, b_k)) : 0;
   const size_t total = ea_bytes + eb_bytes + fa_bytes + fb_bytes + wa_bytes + wb_bytes +
                        nmod * (a_pl + b_pl + t_pl);
-  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  char *ws = static_cast<char *>(ensure_workspace(st, total, stream));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
   int *exp_a = reinterpret_cast<int *>(ws);
@@ -631,7 +639,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
            : 0;
   const size_t total = ea_bytes + eb_bytes + fa_bytes + fb_bytes + wa_bytes + wb_bytes +
                        3 * (size_t)nmod * (a_pl + b_pl + t_pl);
-  char *ws = static_cast<char *>(ensure_workspace(st, total));
+  char *ws = static_cast<char *>(ensure_workspace(st, total, stream));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
   int *exp_a = reinterpret_cast<int *>(ws);

@@ -166,7 +166,8 @@ hcblasStatus run_gemm(Hcblaslibrary *h, const hc::accelerator_view &view, GemmCa
     /* alpha == 0: C := beta*C, A and B are not referenced (CBLAS) */
     path = "scale";
     rc = timed_launch(h->impl, stream, path, [&] { return hcbk_scale_c(&a, stream); });
-  } else if (h->impl->graphs && !h->impl->profiling && stream != nullptr) {
+  } else if (h->impl->graphs && !h->impl->profiling && !h->impl->inject_timeout &&
+             stream != nullptr) {
     rc = dispatch_with_graph(h->impl, &a, stream, &path);
   } else {
     rc = dispatch_gemm(h->impl, &a, stream, &path);

@@ -39,29 +39,77 @@ DeviceGuard::~DeviceGuard() {
   if (prev_ >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev_) cudaSetDevice(prev_);
 }
 
-void *ensure_workspace(HcblasB200State *st, size_t bytes) {
+/* Order `stream` after the last work that used the workspace on another
+ * stream (class-API calls may name a different accelerator view per call). */
+static void order_after_last_use(HcblasB200State *st, cudaStream_t stream) {
+  cudaStream_t last = static_cast<cudaStream_t>(st->workspace_stream);
+  if (last == stream) return;
+  if (!st->workspace_event &&
+      cudaEventCreateWithFlags(reinterpret_cast<cudaEvent_t *>(&st->workspace_event),
+                               cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    st->workspace_event = nullptr;
+  }
+  cudaEvent_t ev = static_cast<cudaEvent_t>(st->workspace_event);
+  if (!ev || cudaEventRecord(ev, last) != cudaSuccess ||
+      cudaStreamWaitEvent(stream, ev, 0) != cudaSuccess) {
+    /* the earlier stream is gone (destroyed by the caller): its work can
+     * only be waited for as a whole */
+    cudaGetLastError();
+    cudaDeviceSynchronize();
+  }
+}
+
+void *ensure_workspace(HcblasB200State *st, size_t bytes, void *stream_v) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
   int dev = 0;
   cudaGetDevice(&dev);
-  if (st->workspace && st->workspace_bytes >= bytes && st->workspace_device == dev)
-    return st->workspace;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusNone;
+  }
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  if (st->workspace && st->workspace_device == dev) {
+    if (!capturing) order_after_last_use(st, stream);
+    if (st->workspace_bytes >= bytes) {
+      st->workspace_stream = stream;
+      return st->workspace;
+    }
+  }
+  /* growing: not while the stream is being captured (an allocation would
+   * belong to the graph), and never beyond the handle's limit */
+  if (capturing || (st->workspace_limit && bytes > st->workspace_limit)) {
+    if (log_enabled())
+      std::fprintf(stderr, "[hcblas] workspace of %zu bytes refused (%s)\n", bytes,
+                   capturing ? "stream capture in progress" : "over the handle's limit");
+    return nullptr;
+  }
   if (st->workspace) {
-    /* the previous workspace may still be read by queued kernels */
-    cudaDeviceSynchronize();
+    /* stream-ordered release: queued kernels that still read the old
+     * workspace finish before the memory is reused; no device-wide wait */
     clear_graph_cache(st);
-    DeviceGuard g(st->workspace_device);
-    cudaFree(st->workspace);
+    if (st->workspace_device == dev) {
+      cudaFreeAsync(st->workspace, stream);
+    } else {
+      DeviceGuard g(st->workspace_device);
+      cudaFreeAsync(st->workspace, static_cast<cudaStream_t>(st->workspace_stream));
+    }
+    cudaGetLastError();
     st->workspace = nullptr;
     st->workspace_bytes = 0;
   }
   size_t want = bytes < (size_t)(64u << 20) ? (size_t)(64u << 20) : bytes;
+  if (st->workspace_limit && want > st->workspace_limit) want = bytes;
   void *p = nullptr;
-  if (cudaMalloc(&p, want) != cudaSuccess) {
+  if (cudaMallocAsync(&p, want, stream) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
   st->workspace = p;
   st->workspace_bytes = want;
   st->workspace_device = dev;
+  st->workspace_stream = stream;
   return p;
 }
 
@@ -82,12 +130,19 @@ int *device_error_flag(HcblasB200State *st) {
     cudaFree(st->dev_err);
     st->dev_err = nullptr;
   }
+  /* the device error block: int 0 the code, ints 2-3 the wait limit (ns) */
   void *p = nullptr;
-  if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) {
+  if (cudaMalloc(&p, 4 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
-  cudaMemset(p, 0, sizeof(int));
+  int block[4] = {0, 0, 0, 0};
+  std::memcpy(block + 2, &st->wait_limit_ns, sizeof(st->wait_limit_ns));
+  if (cudaMemcpy(p, block, sizeof(block), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(p);
+    return nullptr;
+  }
   st->dev_err = static_cast<int *>(p);
   st->dev_err_device = dev;
   return st->dev_err;
@@ -196,9 +251,14 @@ Hcblaslibrary::~Hcblaslibrary() {
   if (impl) {
     if (impl->workspace) {
       DeviceGuard g(impl->workspace_device);
-      cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
-      cudaFree(impl->workspace);
+      cudaStream_t ws = static_cast<cudaStream_t>(impl->workspace_stream);
+      if (cudaFreeAsync(impl->workspace, ws) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(impl->workspace, nullptr);
+      }
+      if (cudaStreamSynchronize(ws) != cudaSuccess) cudaGetLastError();
     }
+    if (impl->workspace_event) cudaEventDestroy(static_cast<cudaEvent_t>(impl->workspace_event));
     for (auto &r : impl->prof) {
       cudaEventDestroy(static_cast<cudaEvent_t>(r.ev0));
       cudaEventDestroy(static_cast<cudaEvent_t>(r.ev1));
@@ -426,6 +486,33 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->crt_i8 = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "workspace_mb") == 0) {
+    if (value < 0) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->workspace_limit = (size_t)value << 20;
+    return HCBLAS_STATUS_SUCCESS;
+  }
+  if (std::strcmp(name, "wait_timeout_us") == 0) {
+    if (value < 0) return HCBLAS_STATUS_INVALID_VALUE;
+    HcblasB200State *st = handle->impl;
+    st->wait_limit_ns = (unsigned long long)value * 1000ull;
+    if (st->dev_err) {
+      /* ordered after the handle's queued work, like a kernel argument */
+      DeviceGuard g(st->dev_err_device);
+      cudaStream_t cs = static_cast<cudaStream_t>(handle->currentAcclView.stream);
+      if (cudaStreamSynchronize(cs) != cudaSuccess ||
+          cudaMemcpy(st->dev_err + 2, &st->wait_limit_ns, sizeof(st->wait_limit_ns),
+                     cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        return HCBLAS_STATUS_EXECUTION_FAILED;
+      }
+    }
+    return HCBLAS_STATUS_SUCCESS;
+  }
+  if (std::strcmp(name, "inject_timeout") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->inject_timeout = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   return HCBLAS_STATUS_INVALID_VALUE;
 }
 
@@ -434,7 +521,9 @@ extern "C" const char *hcblasGetLastPath(hcblasHandle_t handle) {
   return handle->impl->last_path;
 }
 
-extern "C" const char *hcblasGetVersionString(void) { return "hcblas-b200 0.1.0 (sm_100a)"; }
+extern "C" const char *hcblasGetVersionString(void) {
+  return "hcblas-b200 " HCBLAS_B200_VERSION " (sm_100a)";
+}
 
 extern "C" long long hcblasGetKernelLaunchCount(void) { return hcblas_b200::launch_count(); }
 

@@ -12,6 +12,9 @@
 #include <string>
 #include <vector>
 
+/* library version: hcblasGetVersionString, and part of every autotune key */
+#define HCBLAS_B200_VERSION "0.2.0"
+
 /* one timed kernel launch (events recorded on the launch stream) */
 struct HcblasProfRec {
   const char *name;
@@ -63,12 +66,18 @@ struct HcblasB200State {
   int ozaki_default_slices = 7; /* Ozaki slices when the mode's param is 0 */
   const char *last_path = "none";
   /* device workspace owned by the handle (grown on demand, freed at destroy) */
-  void *workspace = nullptr;
+  void *workspace = nullptr; /* cudaMallocAsync'd, released stream-ordered */
   size_t workspace_bytes = 0;
   int workspace_device = -1;
-  /* device int that tensor-core kernels set when a pipeline wait times out */
+  void *workspace_stream = nullptr; /* stream of the last call that used it */
+  void *workspace_event = nullptr;  /* cudaEvent_t ordering a new stream after it */
+  size_t workspace_limit = 0;       /* tuning knob "workspace_mb" (0 = none) */
+  /* device error block of the tensor-core kernels: int 0 is set when a
+   * pipeline wait times out, ints 2-3 hold the wait limit in ns */
   int *dev_err = nullptr;
   int dev_err_device = -1;
+  unsigned long long wait_limit_ns = 0; /* tuning knob "wait_timeout_us" (0 = 2 s) */
+  int inject_timeout = 0; /* tuning knob "inject_timeout": arms the next HGEMM call */
   /* per-kernel CUDA-event timing (hcblasSetProfiling) */
   bool profiling = false;
   std::vector<HcblasProfRec> prof;
@@ -124,8 +133,14 @@ class DeviceGuard {
   bool ok_ = false;
 };
 
-/* Grow the handle's workspace to at least `bytes` on the current device. */
-void *ensure_workspace(HcblasB200State *st, size_t bytes);
+/* The handle's workspace of at least `bytes` on the current device, for
+ * work enqueued on `stream`: the stream is ordered after the workspace's
+ * last use on another stream; growth releases the old buffer and allocates
+ * the new one stream-ordered (cudaFreeAsync / cudaMallocAsync), so no
+ * device-wide wait is made.  nullptr when the workspace must grow while
+ * `stream` is being captured, beyond the "workspace_mb" limit, or when the
+ * allocation fails. */
+void *ensure_workspace(HcblasB200State *st, size_t bytes, void *stream);
 
 /* The handle's device error flag on the current device (allocated and
  * zeroed on first use); nullptr if it cannot be allocated. */

@@ -3,8 +3,11 @@
  * every candidate tile configuration of a kernel family once on the call
  * that first lands in the bucket, keep the fastest.
  *
- * Bucket key: family, dtype, transposes, ceil(log2) of M, N and K, and the
- * device (ordinal and name).  The cache is process-wide; when the
+ * Bucket key: the library version, the driver version, the device (name and
+ * ordinal), family, dtype, transposes, ceil(log2) of M, N and K; a decision
+ * made by another library or driver version is never reused.  Cache lines
+ * that do not parse, or whose choice is out of range for the family, are
+ * ignored and the bucket is tuned again.  The cache is process-wide; when the
  * environment variable HCBLAS_AUTOTUNE_CACHE names a file, the cache is read
  * from it on first use and every new decision is appended to it, so later
  * processes start tuned.  Candidates run through the kernels' own C entry
@@ -80,10 +83,12 @@ std::string tune_key(const char *family, const hcbk_gemm_args *a) {
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) cudaGetLastError();
   for (char *c = prop.name; *c; ++c)
     if (*c == ' ') *c = '_';
-  char buf[256];
-  std::snprintf(buf, sizeof(buf), "v1|%s|%d|%s|dt%d|op%d%d|m%d|n%d|k%d|b%d", prop.name, dev, family,
-                a->dtype, a->op_a, a->op_b, ilog2_ceil(a->m), ilog2_ceil(a->n), ilog2_ceil(a->k),
-                a->batch > 1 ? 1 : 0);
+  int drv = 0;
+  if (cudaDriverGetVersion(&drv) != cudaSuccess) cudaGetLastError();
+  char buf[320];
+  std::snprintf(buf, sizeof(buf), "v2|%s|drv%d|%s|%d|%s|dt%d|op%d%d|m%d|n%d|k%d|b%d",
+                HCBLAS_B200_VERSION, drv, prop.name, dev, family, a->dtype, a->op_a, a->op_b,
+                ilog2_ceil(a->m), ilog2_ceil(a->n), ilog2_ceil(a->k), a->batch > 1 ? 1 : 0);
   return buf;
 }
 

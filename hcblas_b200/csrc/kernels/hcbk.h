@@ -88,6 +88,12 @@ int hcbk_sm_count(void);
  * `err` is a device int that receives a nonzero code if a pipeline wait
  * times out (the kernel then exits instead of hanging). */
 int hcbk_hgemm_tc(const hcbk_gemm_args *args, int bn, int pair, int *err, void *stream);
+/* Failure-detection test of the bounded pipeline waits: the HGEMM kernel on
+ * one 128 x 128 tile of one K block (beta == 0) whose producer arms the
+ * stage barrier without issuing its load, so that the MMA warp's wait runs
+ * out after the wait limit in err[2..3]; nothing asynchronous is in flight
+ * when the kernel unwinds.  HCBK_ERR_ARGS for any other shape. */
+int hcbk_hgemm_tc_inject_timeout(const hcbk_gemm_args *args, int *err, void *stream);
 
 /* Split-BF16 SGEMM: operands already split into bf16 planes, K-major:
  * a_planes[t] is M rows x ld_a elements (row m holds op(A)(m, 0..K-1)),

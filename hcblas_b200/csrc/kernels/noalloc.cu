@@ -5,12 +5,12 @@
  * The split-BF16 path (hcblasSgemm with HCBLAS_MATH_SPLIT_BF16) needs scratch
  * memory for the bf16 planes of both operands; the handle-based entry point
  * takes it from a workspace it grows with cudaMalloc.  Some callers cannot
- * let a library call cudaMalloc: code that runs while a CUDA graph is being
- * captured (an allocation breaks or escapes the capture), applications with
- * their own pool allocator that own every device byte and forbid hidden
- * allocations, and real-time or inference services that allocate everything
- * once at start-up so that no call can fail later for want of memory or
- * stall on the allocator's implicit synchronisation.
+ * let a library call cudaMalloc: applications with their own pool allocator
+ * that own every device byte and forbid hidden allocations, plug-ins hosted
+ * inside another framework that accounts for all device memory itself, and
+ * real-time or inference services that allocate everything once at start-up
+ * so that no call can fail later for want of memory or stall on the
+ * allocator's implicit synchronisation.
  *
  * hcblasSgemmSplitBF16NoAlloc serves them: its scratch is one file-scope
  * static __device__ array of HCBLAS_NOALLOC_SCRATCH_BYTES (64 MiB), created
@@ -20,18 +20,22 @@
  * planes do not fit are rejected with HCBLAS_STATUS_INVALID_VALUE.
  *
  * The host code never dereferences the array's name (in host code it only
- * stands in for the symbol): the first call on each device, with that device
- * current, asks the runtime for the array's device address with
- * cudaGetSymbolAddress and caches it; that first call should therefore be
+ * stands in for the symbol): the first call in each CUDA context of a
+ * device, with that device current, asks the runtime for the array's device
+ * address with cudaGetSymbolAddress and caches it together with the context
+ * it belongs to; a call from another context (for example after
+ * cudaDeviceReset) looks the address up again.  That first call should be
  * made before any stream capture begins.
  *
  * Every call on a device shares the one array, and the array keeps the last
  * call's contents.  The pack kernel rewrites every plane element the GEMM
  * reads, and the pipeline-timeout flag (the only state that must start at
- * zero) is cleared on the caller's stream at the start of each call.  Calls
+ * zero) is cleared on the caller's stream at the start of each call;
+ * hcblasSgemmSplitBF16NoAllocStatus reads it back after the call.  Calls
  * that overlap on the GPU -- on different streams, or from several host
  * threads -- race on the array and must be serialised by the caller.
  */
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -47,13 +51,16 @@ namespace {
 constexpr size_t kScratchBytes = HCBLAS_NOALLOC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
 
-/* the scratch and the pipeline-timeout flag; device addresses come from
- * cudaGetSymbolAddress, never from taking these names' addresses on the host */
+/* the scratch and the device error block of the tensor-core kernels
+ * (int 0: the pipeline-timeout code; ints 2-3: the wait limit, 0 = the
+ * kernels' default); device addresses come from cudaGetSymbolAddress, never
+ * from taking these names' addresses on the host */
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
-static __device__ __align__(256) int g_timeout_flag;
+static __device__ __align__(256) int g_timeout_flag[4];
 
 struct DeviceScratch {
   bool ready;
+  CUcontext ctx; /* the context the cached addresses belong to */
   unsigned char *scratch;
   int *flag;
 };
@@ -61,12 +68,35 @@ struct DeviceScratch {
 std::mutex g_setup_mutex;
 DeviceScratch g_dev[kMaxDevices];
 
-/* once per device, with that device current */
+/* the current CUDA context, through the driver entry point the runtime
+ * exposes (nullptr if it cannot be found) */
+CUcontext current_context() {
+  typedef CUresult (*PFN_ctx_get)(CUcontext *);
+  static PFN_ctx_get fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_ctx_get>(ptr);
+    else
+      cudaGetLastError();
+    looked = true;
+  }
+  CUcontext c = nullptr;
+  if (fn == nullptr || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+/* once per device and context, with that device current */
 bool device_scratch(int dev, DeviceScratch *out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
+  const CUcontext ctx = current_context();
   DeviceScratch &d = g_dev[dev];
-  if (!d.ready) {
+  if (!d.ready || d.ctx != ctx) {
     void *s = nullptr, *f = nullptr;
+    d.ready = false;
     if (cudaGetSymbolAddress(&s, g_scratch) != cudaSuccess) {
       cudaGetLastError();
       return false;
@@ -77,6 +107,7 @@ bool device_scratch(int dev, DeviceScratch *out) {
     }
     d.scratch = static_cast<unsigned char *>(s);
     d.flag = static_cast<int *>(f);
+    d.ctx = current_context(); /* the symbol lookup may have created the primary context */
     d.ready = true;
   }
   *out = d;
@@ -103,8 +134,13 @@ extern "C" hcblasStatus_t hcblasSgemmSplitBF16NoAlloc(void *stream, hcblasOperat
 
   const int nplanes = terms == 6 ? 3 : 2;
   const int64_t kp = ((int64_t)k + 7) & ~int64_t(7); /* 16-byte plane row pitch */
+  /* m, n, kp < 2^31: each plane's size fits size_t; reject either operand
+   * alone before the sum and the plane count are applied, so that nothing
+   * below can wrap */
   const size_t a_bytes = round_1k((size_t)m * kp * 2), b_bytes = round_1k((size_t)n * kp * 2);
-  if ((a_bytes + b_bytes) * nplanes > kScratchBytes) return HCBLAS_STATUS_INVALID_VALUE;
+  if (a_bytes > kScratchBytes || b_bytes > kScratchBytes ||
+      (a_bytes + b_bytes) * nplanes > kScratchBytes)
+    return HCBLAS_STATUS_INVALID_VALUE;
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -180,4 +216,24 @@ extern "C" hcblasStatus_t hcblasSgemmSplitBF16NoAlloc(void *stream, hcblasOperat
   g.beta = *beta;
   return hcbk_sgemm_split_tc(&g, ds.flag, stream) == HCBK_OK ? HCBLAS_STATUS_SUCCESS
                                                              : HCBLAS_STATUS_EXECUTION_FAILED;
+}
+
+extern "C" int hcblasSgemmSplitBF16NoAllocStatus(void *stream) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return -1;
+  }
+  DeviceScratch ds;
+  if (!device_scratch(dev, &ds)) return -1;
+  if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  int code = 0;
+  if (cudaMemcpy(&code, ds.flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return code;
 }

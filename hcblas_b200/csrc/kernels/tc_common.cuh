@@ -8,10 +8,16 @@
  * "instruction descriptor"): they were cross-checked against the field
  * definitions in CUTLASS's cute/arch/mma_sm100_desc.hpp.
  *
- * Every wait on an mbarrier is bounded: after HCBK_WAIT_TIMEOUT_NS of
+ * Every wait on an mbarrier is bounded: after the wait limit of
  * %globaltimer time the wait records an error code in a device flag and
  * returns false, and the kernel unwinds (frees TMEM, exits) instead of
  * hanging the GPU.
+ *
+ * The flag is the first int of the device error block each tensor-core
+ * kernel receives as `err` (16 bytes, 8-byte aligned): err[0] the error code
+ * (0 = none), err[2..3] the wait limit in nanoseconds as one 64-bit value
+ * (0 = HCBK_WAIT_TIMEOUT_NS).  The limit is read once per wait, when the
+ * first try finds the phase incomplete.
  */
 #ifndef HCBLAS_B200_TC_COMMON_CUH_
 #define HCBLAS_B200_TC_COMMON_CUH_
@@ -105,12 +111,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   };
   if (try_once()) return true;
   const uint64_t t0 = globaltimer();
+  const uint64_t set = *reinterpret_cast<volatile unsigned long long *>(err + 2);
+  const uint64_t limit = set ? set : HCBK_WAIT_TIMEOUT_NS;
   uint32_t n = 0;
   while (true) {
     if (try_once()) return true;
     if ((++n & 1023u) == 0) {
       if (*reinterpret_cast<volatile int *>(err) != 0) return false;
-      if (globaltimer() - t0 > HCBK_WAIT_TIMEOUT_NS) {
+      if (globaltimer() - t0 > limit) {
         atomicCAS(err, 0, code);
         return false;
       }

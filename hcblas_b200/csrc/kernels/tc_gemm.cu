@@ -63,6 +63,11 @@ struct TcParams {
   int beta_nonzero;
   int out_tma; /* f16 epilogue: C read (beta != 0) and written by TMA via tc */
   int *err;
+  /* failure-detection test: the producer arms the first stage's barrier
+   * with its byte count but issues no load for it, so the MMA warp's wait
+   * on that stage runs out (accepted only for one tile of one K block with
+   * beta == 0, where nothing else is in flight) */
+  int inject_skip_load;
   /* modular (CRT) epilogue: output plane i is reduced modulo mod_tab[i];
    * planes of A, B (3-D tensor maps) and C (c_plane_stride elements apart)
    * are batched into one launch */
@@ -762,6 +767,13 @@ __global__ void __launch_bounds__(64 + 32 * EpiWarps<EPI>::value, 1)
           }
           /* the leader's full barrier counts both CTAs' bytes */
           if (rank == 0) mbar_expect_tx(&full[s], CG * Cfg::STAGE_BYTES);
+          if (p.inject_skip_load && i == 0 && kb == w.c * chunk_kb) {
+            if (++s == STAGES) {
+              s = 0;
+              ph ^= 1u;
+            }
+            continue;
+          }
           uint8_t *st = smem + s * Cfg::STAGE_BYTES;
           const int k0 = p.k0 + kb * BKE;
           auto load2d = [&](uint8_t *dst, const CUtensorMap *map, int c0, int c1) {
@@ -1147,7 +1159,8 @@ static int make_map_out(CUtensorMap *map, CUtensorMapDataType dt, uint32_t esz, 
 }
 
 /* f16 operands straight from the caller's matrices (column-major canonical). */
-extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream) {
+static int hgemm_tc_impl(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream,
+                         int inject_skip_load) {
   if (a->dtype != HCBK_H || a->batch != 1 || a->a_array || a->op_a == HCBK_OP_C ||
       a->op_b == HCBK_OP_C)
     return HCBK_ERR_ARGS;
@@ -1188,9 +1201,24 @@ extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err
   p.out_tma =
       make_map_out(&p.tc, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, p.c, a->m, a->n, a->ldc) == HCBK_OK;
   using EH = EpiAlphaBeta<__half>;
+  if (inject_skip_load) {
+    /* one 128 x 128 tile of one 64-wide K block, beta == 0: the only load
+     * the kernel would issue is the skipped one, the epilogue reads no C */
+    if (a->m > BM || a->n > 128 || a->k > 64 || p.beta_nonzero || pair || bn != 128)
+      return HCBK_ERR_ARGS;
+    p.inject_skip_load = 1;
+  }
   if (pair) return launch_tc<256, 6, RecipeSingle, 0, EH, 0, 2, 2>(p, stream);
   if (bn == 256) return launch_tc<256, 4, RecipeSingle, 0, EH>(p, stream);
   return launch_tc<128, 6, RecipeSingle, 0, EH>(p, stream);
+}
+
+extern "C" int hcbk_hgemm_tc(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream) {
+  return hgemm_tc_impl(a, bn, pair, err, stream, 0);
+}
+
+extern "C" int hcbk_hgemm_tc_inject_timeout(const hcbk_gemm_args *a, int *err, void *stream) {
+  return hgemm_tc_impl(a, 128, 0, err, stream, 1);
 }
 
 /* split-BF16 SGEMM on pre-split K-major planes:

@@ -438,7 +438,26 @@ hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
  *                       sums exact over all of K (K <= 131072, else as 0);
  *                       0 binary16 residue planes on the f16 tensor cores,
  *                       sums reduced mod p every 1024 K.  Both give
- *                       bit-identical results. */
+ *                       bit-identical results.
+ *   "workspace_mb"      upper limit of the handle's device workspace in MiB
+ *                       (0, the default: none).  A call whose path needs more
+ *                       returns HCBLAS_STATUS_EXECUTION_FAILED without
+ *                       launching anything.  The workspace is allocated and
+ *                       released stream-ordered (cudaMallocAsync /
+ *                       cudaFreeAsync on the call's stream); it cannot grow
+ *                       while that stream is being captured (the call then
+ *                       fails the same way).
+ *   "wait_timeout_us"   limit of every bounded pipeline wait in the
+ *                       tensor-core kernels, in microseconds (0, the default:
+ *                       2 s).  A wait that runs out records its code in the
+ *                       handle's device error flag (hcblasGetDeviceError)
+ *                       and the kernel unwinds, leaving C incomplete.
+ *   "inject_timeout"    failure-detection testing: 1 arms the handle's next
+ *                       HGEMM call to run its tensor-core pipeline with the
+ *                       first operand load withheld, so that a pipeline wait
+ *                       runs out; only a single 128 x 128 tile of one 64-wide
+ *                       K block with beta == 0 is accepted (anything else
+ *                       returns EXECUTION_FAILED).  Disarmed after that call. */
 hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char *name, int value);
 
 /* Extension: the path the last GEMM call on this handle took (a short static
@@ -465,10 +484,11 @@ int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap);
 
 /* Extension with no counterpart in the reference: split-BF16 SGEMM that
  * allocates nothing, for callers that cannot let a library call cudaMalloc
- * (code running under CUDA-graph stream capture, applications whose own pool
- * allocator owns all device memory, services that allocate everything at
- * start-up so that no later call can fail for memory or stall on the
- * allocator's implicit synchronisation).
+ * (applications whose own pool allocator owns all device memory and forbids
+ * hidden allocations, plug-ins hosted inside a framework that accounts for
+ * every device byte itself, services that allocate everything at start-up
+ * so that no later call can fail for memory or stall on the allocator's
+ * implicit synchronisation).
  *
  * Computes C = alpha * op(A) op(B) + beta * C, column-major, like
  * hcblasSgemm under HCBLAS_MATH_SPLIT_BF16 with `terms` = 3 or 6 bf16
@@ -484,19 +504,25 @@ int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap);
  * alpha/beta: INVALID_VALUE; an empty problem or a NULL matrix:
  * EXECUTION_FAILED).
  *
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current) and caches it: make that
- * first call before any stream capture begins.  All calls on a device share
- * the array and it keeps the last call's contents, so calls that overlap on
- * the GPU (other streams, other host threads) race and must be serialised
- * by the caller.  A device-side pipeline timeout (which a correct run never
- * meets) leaves C undefined and is not reported here. */
+ * The first call in each CUDA context of a device looks up the array's
+ * device address (cudaGetSymbolAddress, with that device current) and
+ * caches it with the context; make that first call before any stream
+ * capture begins.  All calls on a device share the array and it keeps the
+ * last call's contents, so calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
 #define HCBLAS_NOALLOC_SCRATCH_BYTES (64u << 20)
 hcblasStatus_t hcblasSgemmSplitBF16NoAlloc(void *stream, hcblasOperation_t transa,
                                            hcblasOperation_t transb, int m, int n, int k,
                                            const float *alpha, const float *A, int lda,
                                            const float *B, int ldb, const float *beta, float *C,
                                            int ldc, int terms);
+/* Extension with no counterpart in the reference: the outcome of the most
+ * recent hcblasSgemmSplitBF16NoAlloc call on the current device.  Waits for
+ * `stream`, then returns 0 when that call's tensor-core pipeline finished,
+ * the pipeline-timeout code (> 0; C is then incomplete) when one of its
+ * bounded waits gave up, or -1 when the state cannot be read.  Allocates
+ * nothing; each no-allocation call clears the code when it starts. */
+int hcblasSgemmSplitBF16NoAllocStatus(void *stream);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -12,8 +12,14 @@ split-BF16 tests:
   * 3 products: (2^-15 + 2 gamma_{K+2}(f32)) || |alpha||A||B| ||_F
                 + 2 gamma_{K+2}(f32) || |beta||C| ||_F
 The second call also shows that the reused scratch carries nothing over.
+After each call hcblasSgemmSplitBF16NoAllocStatus must report no pipeline
+timeout.  The fresh-process case runs in a child interpreter whose first GEMM
+call is the no-allocation entry point.
 """
 import ctypes
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -46,6 +52,21 @@ def entry():
     return f
 
 
+def status():
+    f = hb.lib().hcblasSgemmSplitBF16NoAllocStatus
+    f.argtypes = [ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    return f(None)
+
+
+def bound_of(terms, K, alpha, beta, Ad, Bd, Cd):
+    ab = abs(alpha) * (np.abs(Ad) @ np.abs(Bd))
+    cc = abs(beta) * np.abs(Cd)
+    if terms == 6:
+        return 2 * g32(K) * np.linalg.norm(ab + cc)
+    return (2.0 ** -15 + 2 * g32(K)) * np.linalg.norm(ab) + 2 * g32(K) * np.linalg.norm(cc)
+
+
 def make(rng, ta, tb, M, N, K):
     lda = (M if ta == 0 else K) + 3
     ldb = (K if tb == 0 else N) + 5
@@ -71,6 +92,7 @@ def test_no_alloc_matches_handle_path(handle, terms):
         st = f(None, OPS[ta], OPS[tb], M, N, K, al.ctypes.data, dA.ptr, lda, dB.ptr, ldb,
                be.ctypes.data, dC_new.ptr, ldc, terms)
         assert st == hb.HCBLAS_STATUS_SUCCESS, st
+        assert status() == 0
         got_new = dC_new.download()
 
         assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_SPLIT_BF16, terms) == 0
@@ -86,13 +108,7 @@ def test_no_alloc_matches_handle_path(handle, terms):
 
         Ad, Bd = op_dense(A, ta, M, K, lda), op_dense(B, tb, K, N, ldb)
         Cd = C[: ldc * N].reshape(N, ldc)[:, :M].T.astype(np.float64)
-        ab = abs(alpha) * (np.abs(Ad) @ np.abs(Bd))
-        cc = abs(beta) * np.abs(Cd)
-        if terms == 6:
-            bound = 2 * g32(K) * np.linalg.norm(ab + cc)
-        else:
-            bound = (2.0 ** -15 + 2 * g32(K)) * np.linalg.norm(ab) + \
-                2 * g32(K) * np.linalg.norm(cc)
+        bound = bound_of(terms, K, alpha, beta, Ad, Bd, Cd)
         view = lambda X: X[: ldc * N].reshape(N, ldc)[:, :M].T.astype(np.float64)
         _, ref = O.gemm(O.COL, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
         assert np.linalg.norm(view(got_new) - view(got_old)) <= bound
@@ -115,3 +131,48 @@ def test_no_alloc_rejects_oversize_and_bad_args(handle):
              3) == hb.HCBLAS_STATUS_INVALID_VALUE
     assert f(None, 0, 0, 0, 8, 8, one.ctypes.data, fake, 8, fake, 8, one.ctypes.data, fake, 8,
              3) == hb.HCBLAS_STATUS_EXECUTION_FAILED
+    # the largest sizes: each operand's planes alone exceed the scratch, and
+    # their byte counts summed over the planes would wrap a 64-bit size
+    big = 2 ** 31 - 1
+    for terms in (3, 6):
+        assert f(None, 0, 0, big, big, big, one.ctypes.data, fake, big, fake, big,
+                 one.ctypes.data, fake, big, terms) == hb.HCBLAS_STATUS_INVALID_VALUE
+
+
+def _fresh_process_case():
+    """Body of the child process: the no-allocation entry point is the
+    first GEMM this process calls, so its first call performs the per-device
+    set-up; two calls in a row, each checked against the oracle."""
+    s, h = hb.hcblasCreate(0)
+    assert s == hb.HCBLAS_STATUS_SUCCESS
+    f = entry()
+    rng = np.random.default_rng(77)
+    try:
+        for ta, tb, M, N, K, alpha, beta, terms in [(0, 1, 200, 130, 300, 1.0, 0.5, 6),
+                                                    (1, 0, 96, 257, 520, -0.5, 0.0, 3)]:
+            A, lda, B, ldb, C, ldc = make(rng, ta, tb, M, N, K)
+            al, be = np.array([alpha], np.float32), np.array([beta], np.float32)
+            dA, dB, dC = hb.DeviceArray(h, A), hb.DeviceArray(h, B), hb.DeviceArray(h, C)
+            st = f(None, OPS[ta], OPS[tb], M, N, K, al.ctypes.data, dA.ptr, lda, dB.ptr, ldb,
+                   be.ctypes.data, dC.ptr, ldc, terms)
+            assert st == hb.HCBLAS_STATUS_SUCCESS, st
+            assert status() == 0
+            got = dC.download()
+            Ad, Bd = op_dense(A, ta, M, K, lda), op_dense(B, tb, K, N, ldb)
+            Cd = C[: ldc * N].reshape(N, ldc)[:, :M].T.astype(np.float64)
+            _, ref = O.gemm(O.COL, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+            view = got[: ldc * N].reshape(N, ldc)[:, :M].T.astype(np.float64)
+            err = np.linalg.norm(view - ref)
+            assert err <= bound_of(terms, K, alpha, beta, Ad, Bd, Cd), err
+    finally:
+        hb.hcblasDestroy(h)
+    print("fresh-process no-allocation calls ok")
+
+
+def test_no_alloc_in_fresh_process():
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c",
+                        "import tests.test_zz_no_alloc as t; t._fresh_process_case()"],
+                       cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "fresh-process no-allocation calls ok" in r.stdout
