@@ -6,10 +6,12 @@ M = N = K = 4096, alpha = 1, beta = 0, entries i.i.d. N(0,1) from seed 1 --
 one hcblasDgemm call through the library's C ABI (libhcblas.so) on inputs
 already resident in HBM, computed by the emulated FP64 path at matched
 error: the integer-modular (CRT, Ozaki scheme II) DGEMM on the int8 tensor
-cores with the fewest moduli whose normwise error against the double-double
-oracle is no worse than the native FP64 kernel's on the same call; the timed
-steps replay the call's kernel sequence as a CUDA graph (the library's
-"graphs" knob).  A, B, C take 3 x 128 MiB > the 126 MB L2, so consecutive
+cores with the moduli count the library's planner picks for the accuracy
+target "native FP64" (hcblasSetAccuracyTarget(h, HCBLAS_ACCURACY_NATIVE),
+no count given); its normwise error against the double-double oracle is
+checked beside the native FP64 kernel's on the same call (untimed); the
+timed steps replay the call's kernel sequence as a CUDA graph (the
+library's "graphs" knob).  A, B, C take 3 x 128 MiB > the 126 MB L2, so consecutive
 steps do not hit in L2.
 
 Printed (rank 0, one JSON line):
@@ -22,10 +24,11 @@ Printed (rank 0, one JSON line):
               step, neighbouring steps' copies overlapping the GEMM (the
               serial form, every copy waited for, is reported beside it)
   roofline    the dominant kernel (one launch: the modular int8 GEMMs of
-              every modulus) against the dense int8 tensor peak, taken as
-              twice the measured dense bf16 peak (kind::i8 issues at twice
-              the kind::f16 rate), with its ncu DRAM traffic per launch from
-              profiles/traffic.json
+              every modulus) against the dense int8 GEMM rate measured in
+              the same run (the vendor library's int8 GEMM at 8192^3, best of
+              10, as MEASURED_PEAKS.json measures bf16), with its ncu DRAM
+              traffic per launch from profiles/traffic.json
+  summary     (last key) the headline comparisons and their errors
   cpu_baseline  host CBLAS (OpenBLAS's cblas_dgemm, all host threads) on a
               bounded column sample of the same problem
   secondary   Ozaki-I INT8 slices 5 / 6 / 7 vs native on the headline
@@ -65,7 +68,6 @@ ALPHA, BETA = 1.0, 0.0
 FLOP = 2.0 * M * N * K
 WORKLOAD = "dgemm_colmajor_NT_4096^3_alpha1_beta0_N01_seed1"
 MATH_NATIVE, MATH_SPLIT, MATH_OZAKI_INT8, MATH_CRT = 0, 1, 2, 4
-CRT_CANDIDATES = (12, 13, 14, 15, 16, 17, 18)
 
 
 def env_int(name, default):
@@ -303,6 +305,35 @@ def load_traffic(kernel):
         return None
 
 
+def measure_int8_peak(torch, n=8192, reps=10):
+    """Dense int8 GEMM rate of this GPU measured the way MEASURED_PEAKS.json
+    measures the bf16 one: the vendor library's GEMM (cuBLASLt int8 through
+    torch._int_mm, s8 x s8 -> s32, n^3) timed with CUDA events, best of
+    `reps` single calls.  It is the roofline denominator of the int8
+    modular GEMM; library code, never on this library's paths."""
+    try:
+        g = torch.Generator(device="cuda").manual_seed(11)
+        a = torch.randint(-127, 128, (n, n), device="cuda", dtype=torch.int8, generator=g)
+        b = torch.randint(-127, 128, (n, n), device="cuda", dtype=torch.int8, generator=g)
+        bt = b.t().contiguous().t()
+        for _ in range(3):
+            torch._int_mm(a, bt)
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, bt)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        del a, b, bt
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
 def oracle_err(O, Cg, A, lda, ta, B, ldb, tb, m, k, cols, ncol_total, beta=0.0, C0=None):
     """normwise error of the (m x ncol_total) column-major result Cg on the
     sampled columns against the double-double oracle (alpha = 1; beta * C0
@@ -378,8 +409,10 @@ def main():
         torch.cuda.synchronize()
         return ev0.elapsed_time(ev1) / nsteps
 
-    # ---- matched-error calibration (untimed): native error, then the
-    # fewest CRT moduli whose error is no worse ----
+    # ---- the moduli count: the library's planner for the accuracy target
+    # "native FP64" (no oracle involved); then, untimed, a check against the
+    # double-double oracle: the native error and the error of the planned
+    # count and of its neighbours ----
     cols = np.random.default_rng(5).choice(N, 8, replace=False)
     hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
     step()
@@ -387,18 +420,15 @@ def main():
     native_path = hb.hcblasGetLastPath(h)
     Cg = dC.download().reshape(N, M).T
     err_native = oracle_err(O, Cg, A, M, 0, B, N, 1, M, K, cols, N)
-    chosen, calib = None, {}
-    for nm in CRT_CANDIDATES:
+    pst, chosen, model_bits = hb.plan_emulation(MATH_CRT, 0, hb.HCBLAS_ACCURACY_NATIVE, "d", K)
+    assert pst == 0, pst
+    calib = {}
+    for nm in (chosen - 1, chosen, chosen + 1):
         hb.hcblasSetMathMode(h, MATH_CRT, nm)
         step()
         assert hb.device_error(h) == 0
-        e = oracle_err(O, dC.download().reshape(N, M).T, A, M, 0, B, N, 1, M, K, cols, N)
-        calib[nm] = e
-        if e <= err_native:
-            chosen = nm
-            break
-    if chosen is None:
-        chosen = CRT_CANDIDATES[-1]
+        calib[nm] = oracle_err(O, dC.download().reshape(N, M).T, A, M, 0, B, N, 1, M, K, cols, N)
+    fewest_by_oracle = min([nm for nm, e in calib.items() if e <= err_native], default=None)
 
     # native timing (same workload, same clocks window)
     hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
@@ -407,7 +437,10 @@ def main():
     native_ms = time_steps(max(3, args.steps // 2))
     native_tflops = FLOP / (native_ms * 1e-3) / 1e12
 
-    hb.hcblasSetMathMode(h, MATH_CRT, chosen)
+    # the emulated mode with no count given: the planner picks it from the
+    # handle's accuracy target
+    hb.hcblasSetMathMode(h, MATH_CRT, 0)
+    hb.hcblasSetAccuracyTarget(h, hb.HCBLAS_ACCURACY_NATIVE)
     # the call sequence is replayed as a CUDA graph (tuning knob "graphs"):
     # the first warm-up call runs eagerly and is captured, the rest replay
     hb.set_tuning(h, "graphs", 1)
@@ -450,8 +483,14 @@ def main():
     kernel_ms = tot / cnt
     dom_flop = FLOP * chosen if dom == "tc.crt_modgemm" else (FLOP if dom.startswith("tc.") else None)
     achieved = dom_flop / (kernel_ms * 1e-3) / 1e12 if dom_flop else None
-    # int8 tensor peak: twice the measured dense bf16 rate
-    peak = 2.0 * peaks.get("bf16_tflops") if dom == "tc.crt_modgemm" else peaks.get("bf16_tflops")
+    # int8 tensor peak: the measured dense int8 GEMM rate (cuBLASLt, best of
+    # 10 at 8192^3, as MEASURED_PEAKS.json measures bf16); twice the measured
+    # bf16 rate if that measurement is unavailable
+    int8_peak = measure_int8_peak(torch) if dom == "tc.crt_modgemm" else None
+    if dom == "tc.crt_modgemm":
+        peak = round(int8_peak, 1) if int8_peak else 2.0 * peaks.get("bf16_tflops")
+    else:
+        peak = peaks.get("bf16_tflops")
     breakdown = {k: {"launches_per_step": v[0] // args.steps,
                      "ms_per_step": round(v[1] / args.steps, 4),
                      "share": round(v[1] / sum(x[1] for x in prof.values()), 4)}
@@ -546,13 +585,13 @@ def main():
         hard = {}
         dA.upload(Ah)
         dB.upload(Bh)
-        for name, mode, par in (("native", MATH_NATIVE, 0), (path, MATH_CRT, chosen)):
-            hb.hcblasSetMathMode(h, mode, par)
+        for name, mode in (("native", MATH_NATIVE), (path, MATH_CRT)):
+            hb.hcblasSetMathMode(h, mode, 0)
             step()
             assert hb.device_error(h) == 0
             hard[name] = oracle_err(O, dC.download().reshape(N, M).T, Ah, M, 0, Bh, N, 1, M, K,
                                     cols[:4], N)
-        hb.hcblasSetMathMode(h, MATH_CRT, chosen)
+        hb.hcblasSetMathMode(h, MATH_CRT, 0)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             tf, nb, thr, Cs, secs = cpu_cblas_sample(A, B, target_s=8.0)
@@ -593,15 +632,22 @@ def main():
                          "achieved": round(achieved, 2) if achieved else None,
                          "peak": peak, "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4) if achieved else None,
-                         "peak_source": (f"2 x {peak_src} dense bf16 burst (MEASURED_PEAKS.json "
-                                         f"bf16_tflops): the modular GEMMs run kind::i8, whose "
-                                         f"nominal dense rate is twice kind::f16's (4.5 vs 2.25 "
-                                         f"POPS); cuBLASLt's int8 GEMM at 8192^3 measures 2800 "
-                                         f"TOPS on this part (profiles/tc_gemm_crt_modgemm_i8_"
-                                         f"pair_nt_4096.md)")
+                         "peak_source": (("measured in this run: dense int8 GEMM (cuBLASLt "
+                                          "s8 x s8 -> s32, 8192^3, best of 10 CUDA-event "
+                                          "timings), the int8 analogue of MEASURED_PEAKS.json's "
+                                          "bf16 figure")
+                                         if int8_peak else
+                                         f"2 x {peak_src} dense bf16 burst (MEASURED_PEAKS.json "
+                                         f"bf16_tflops): no int8 measurement in this run")
                                         if dom == "tc.crt_modgemm" else
                                         f"{peak_src} dense bf16 burst (MEASURED_PEAKS.json "
                                         f"bf16_tflops)",
+                         "frac_of_2x_bf16_burst": (round(achieved / (2.0 * peaks["bf16_tflops"]), 4)
+                                                   if achieved and dom == "tc.crt_modgemm"
+                                                   and peaks.get("bf16_tflops") else None),
+                         "frac_of_nominal_int8_4500": (round(achieved / 4500.0, 4)
+                                                       if achieved and dom == "tc.crt_modgemm"
+                                                       else None),
                          "traffic": traffic, "kernel_ms": round(kernel_ms, 4),
                          "kernel_ms_source": "CUDA events around each launch in the eager "
                                              "profiled pass of the same steps",
@@ -610,13 +656,17 @@ def main():
             "cpu_baseline": cpu,
             "accuracy": {"normwise_err_vs_double_double_oracle": err_dd,
                          "native_normwise_err": err_native,
-                         "calibration_err_by_moduli": calib,
+                         "planner": {"accuracy_target_bits": 53, "moduli": chosen,
+                                     "model_bits": model_bits},
+                         "oracle_check_err_by_moduli": calib,
+                         "fewest_moduli_matching_native_by_oracle": fewest_by_oracle,
                          "oracle_columns": len(cols),
                          "hard_variant_e_U-20..20": hard},
             "secondary": secondary,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
+        line["summary"] = summarize(line)
     hb.hcblasDestroy(h)
     if dist:
         dist.barrier()
@@ -624,6 +674,62 @@ def main():
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def summarize(line):
+    """The headline comparisons in one small object, printed last in the
+    JSON line: native vs emulated at 4096^3 and 8192^3 (DGEMM), split-BF16 vs
+    plain SGEMM (8192^3 and 8192 x 8192 x 256), grouped vs per-problem
+    calls, complex at 2048^3; each with the errors behind it."""
+    out = {"dgemm_4096": {"native_tflops": line["native"]["tflops"],
+                          "native_err": line["accuracy"]["native_normwise_err"],
+                          "crt_tflops": line["value"],
+                          "crt_err": line["accuracy"]["normwise_err_vs_double_double_oracle"],
+                          "crt_moduli": line["config"]["crt_moduli"],
+                          "speedup": line["native"]["speedup_emulated_vs_native"]}}
+    sec = line.get("secondary") or {}
+
+    def pick(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+    d8 = sec.get("dgemm_colmajor_NT_8192^3")
+    if d8:
+        m = d8.get("matched_error")
+        out["dgemm_8192"] = {"native_tflops": pick(d8, "native", "tflops"),
+                             "native_err": pick(d8, "native", "normwise_err"),
+                             "matched": m, "tflops": pick(d8, m, "tflops"),
+                             "err": pick(d8, m, "normwise_err"),
+                             "speedup": d8.get("speedup_matched_vs_native"),
+                             "target": ">= 2x native at error <= native"}
+    for key, short in (("sgemm_colmajor_TN_8192^3_beta1", "sgemm_8192"),
+                       ("sgemm_colmajor_TN_8192x8192x256_beta1", "sgemm_8192x8192x256")):
+        s3 = sec.get(key)
+        if s3:
+            out[short] = {"plain_tflops": pick(s3, "plain", "tflops"),
+                          "plain_err": pick(s3, "plain", "normwise_err"),
+                          "split6_tflops": pick(s3, "split_bf16x6", "tflops"),
+                          "split6_err": pick(s3, "split_bf16x6", "normwise_err"),
+                          "speedup": s3.get("speedup_x6_vs_plain"),
+                          "target": ">= 3x plain at error <= plain"}
+    for key, short in (("hgemm_grouped_4096_uneven", "grouped_f16"),
+                       ("sgemm_grouped_4096_uneven_split_bf16x6", "grouped_f32_split")):
+        gq = sec.get(key)
+        if gq:
+            out[short] = {"ms": gq.get("ms"), "tflops": gq.get("tflops"),
+                          "speedup_vs_per_problem": gq.get("speedup_vs_per_problem",
+                                                           gq.get("speedup_vs_per_problem_plain")),
+                          "target": ">= 1.5x per-problem launches"}
+    for key, short in (("cgemm_colmajor_CN_2048^3", "cgemm_2048"),
+                       ("zgemm_colmajor_CN_2048^3", "zgemm_2048")):
+        c5 = sec.get(key)
+        if c5:
+            out[short] = {k: (v if not isinstance(v, dict) else
+                              {kk: v.get(kk) for kk in ("tflops", "normwise_err")})
+                          for k, v in c5.items()}
+    return out
 
 
 def run_secondary(hb, L, h, stream, torch, O, n=8192, reps=3):

@@ -59,7 +59,12 @@ EXPORTED = (
     "hcblas_am_copy", "hcblas_view_wait", "hcblas_device_count", "hcblas_current_device",
     "hcblasHgemmGrouped", "hcblasSgemmGrouped", "hcblasSgemv", "hcblasDgemv", "hcblasSgemvBatched",
     "hcblasDgemvBatched", "hcblasSger", "hcblasDger", "hcblasSgerBatched", "hcblasDgerBatched",
+    "hcblasSetAccuracyTarget", "hcblasGetAccuracyTarget", "hcblasPlanEmulation",
+    "hcblasSgemmSplitBF16NoAlloc", "hcblasSgemmSplitBF16NoAllocStatus",
 )
+
+# accuracy targets (extension)
+HCBLAS_ACCURACY_DEFAULT, HCBLAS_ACCURACY_NATIVE = 0, -1
 
 
 class GemmProblem(ctypes.Structure):
@@ -227,6 +232,25 @@ def hcblasSetMathMode(handle, mode, param=0):
 
 def hcblasGetLastPath(handle) -> str:
     return lib().hcblasGetLastPath(handle).decode()
+
+
+def hcblasSetAccuracyTarget(handle, bits: int) -> int:
+    f = lib().hcblasSetAccuracyTarget
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    f.restype = ctypes.c_ushort
+    return f(handle, bits)
+
+
+def plan_emulation(mode: int, param: int, bits: int, dtype: str, k: int):
+    """(status, count, model_bits) of hcblasPlanEmulation; dtype 's', 'd',
+    'c' or 'z'."""
+    f = lib().hcblasPlanEmulation
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
+                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    f.restype = ctypes.c_ushort
+    c, mb = ctypes.c_int(0), ctypes.c_double(0.0)
+    s = f(mode, param, bits, "sdcz".index(dtype), k, ctypes.byref(c), ctypes.byref(mb))
+    return s, c.value, mb.value
 
 
 def set_tuning(handle, name: str, value: int):

@@ -402,42 +402,6 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   return HCBK_OK;
 }
 
-/* CRT plan of the real (DGEMM) path.  Operands are scaled to integers of
- * up to 53 bits, x' = rint(x 2^(53 - e_r)) per row/column.  Two bounds keep
- * |P'| = |sum_k a'_k b'_k| below M / (2 * 2^0.01): K 2^106 when the moduli
- * are that wide (then e_r is the frexp exponent of the row maximum), else
- * ||a'||_2 ||b'||_2 <= (2^nb + sqrt(K) / 2)^2 with the row exponents raised
- * so that every row norm is below 2^nb (Cauchy-Schwarz): rows that are not
- * dominated by one entry then keep about log2(max |x| sqrt(K) / ||x||_2)
- * more bits than scaling for the worst case K 2^(2 beta) allows.
- * want = 0 picks the fewest moduli with the first bound (full binary64
- * width whatever the data); want = n uses n moduli. */
-bool crt_plan_rows(int64_t k, int want, int *nmod, int *shift, bool *norm) {
-  int count = 0;
-  const int *mods = hcbk_crt_moduli(&count);
-  const double lk = std::ceil(std::log2((double)(k > 1 ? k : 2)));
-  /* rint of the rounded product x f: at most 3/4 of a unit per element */
-  const double rnd_norm = 0.75 * std::sqrt((double)k);
-  double cum = 0.0;
-  for (int i = 0; i < count; ++i) {
-    cum += std::log2((double)mods[i]);
-    const int n = i + 1;
-    const bool full = cum >= 2.0 * 53 + 1.0 + lk + 0.01;
-    if ((want == 0 && full) || want == n || (want == 0 && n == count)) {
-      *nmod = n;
-      *norm = !full;
-      *shift = 0;
-      if (full) return true;
-      int nb = (int)std::floor((cum - 1.02) / 2.0);
-      while (nb > 0 && 2.0 * std::log2(std::ldexp(1.0, nb) + rnd_norm) + 0.01 >= cum - 1.0) --nb;
-      if (nb < 8) return false;
-      *shift = 53 - nb;
-      return true;
-    }
-  }
-  return false;
-}
-
 /* CRT (Ozaki scheme II) DGEMM: exponents, residue planes of the scaled
  * integer operands, one modular tensor-core GEMM launch over every modulus,
  * CRT reconstruction (weighted residue sum mod M) with the alpha/beta
@@ -774,6 +738,43 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
 
 }  // namespace
 
+/* CRT plan of the real (DGEMM) path.  Operands are scaled to integers of
+ * up to 53 bits, x' = rint(x 2^(53 - e_r)) per row/column.  Two bounds keep
+ * |P'| = |sum_k a'_k b'_k| below M / (2 * 2^0.01): K 2^106 when the moduli
+ * are that wide (then e_r is the frexp exponent of the row maximum), else
+ * ||a'||_2 ||b'||_2 <= (2^nb + sqrt(K) / 2)^2 with the row exponents raised
+ * so that every row norm is below 2^nb (Cauchy-Schwarz): rows that are not
+ * dominated by one entry then keep about log2(max |x| sqrt(K) / ||x||_2)
+ * more bits than scaling for the worst case K 2^(2 beta) allows.
+ * want = 0 picks the fewest moduli with the first bound (full binary64
+ * width whatever the data); want = n uses n moduli. */
+bool crt_plan_rows(int64_t k, int want, int *nmod, int *shift, bool *norm) {
+  int count = 0;
+  const int *mods = hcbk_crt_moduli(&count);
+  const double lk = std::ceil(std::log2((double)(k > 1 ? k : 2)));
+  /* rint of the rounded product x f: at most 3/4 of a unit per element */
+  const double rnd_norm = 0.75 * std::sqrt((double)k);
+  double cum = 0.0;
+  for (int i = 0; i < count; ++i) {
+    cum += std::log2((double)mods[i]);
+    const int n = i + 1;
+    const bool full = cum >= 2.0 * 53 + 1.0 + lk + 0.01;
+    if ((want == 0 && full) || want == n || (want == 0 && n == count)) {
+      *nmod = n;
+      *norm = !full;
+      *shift = 0;
+      if (full) return true;
+      int nb = (int)std::floor((cum - 1.02) / 2.0);
+      while (nb > 0 && 2.0 * std::log2(std::ldexp(1.0, nb) + rnd_norm) + 0.01 >= cum - 1.0) --nb;
+      if (nb < 8) return false;
+      *shift = 53 - nb;
+      return true;
+    }
+  }
+  return false;
+}
+
+
 /* Strided-batched HGEMM as a special case of the grouped kernel: one table
  * entry per batch element.  Declined (HCBK_ERR_ALIGN) unless every element
  * is TMA-addressable, so that the batch never splits across paths. */
@@ -814,8 +815,8 @@ int hgemm_strided_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *st
 bool emulated_mode(const HcblasB200State *st, int dtype) {
   switch (st->math_mode) {
     case 1: return dtype == HCBK_S || dtype == HCBK_C;  /* split-BF16 */
-    case 2:
-    case 3: return dtype == HCBK_D;                     /* Ozaki-I */
+    case 2: return dtype == HCBK_D || dtype == HCBK_S;  /* Ozaki-I int8 */
+    case 3: return dtype == HCBK_D;                     /* Ozaki-I binary16 */
     case 4: return dtype == HCBK_D || dtype == HCBK_Z;  /* CRT */
     default: return false;
   }
@@ -849,21 +850,22 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
   }
   if (a->dtype == HCBK_S && st->math_mode == 1 /* HCBLAS_MATH_SPLIT_BF16 */ && a->batch == 1 &&
       !a->a_array) {
-    const int terms = st->math_param == 6 ? 6 : 3;
+    const int terms = plan_emulation(1, st->math_param, st->accuracy_bits, HCBK_S, a->k, nullptr);
     int rc = sgemm_split(st, a, terms, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] split-bf16 path declined (%d)\n", rc);
   }
   if (a->dtype == HCBK_C && st->math_mode == 1 /* HCBLAS_MATH_SPLIT_BF16 */ && a->batch == 1 &&
       !a->a_array) {
-    const int terms = st->math_param == 6 ? 6 : 3;
+    const int terms = plan_emulation(1, st->math_param, st->accuracy_bits, HCBK_C, a->k, nullptr);
     int rc = cgemm_split3m(st, a, terms, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] complex split-bf16 path declined (%d)\n", rc);
   }
   if (a->dtype == HCBK_S && st->math_mode == 2 /* HCBLAS_MATH_OZAKI_INT8 */ && a->batch == 1 &&
       !a->a_array) {
-    const int s = st->math_param > 0 ? st->math_param : 4; /* 28 bits >= FP32's 24 */
+    /* 4 slices (28 bits) unless a count or an accuracy target is set */
+    const int s = plan_emulation(2, st->math_param, st->accuracy_bits, HCBK_S, a->k, nullptr);
     int rc = dgemm_ozaki(st, a, s, false, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] sgemm ozaki path declined (%d)\n", rc);
@@ -872,20 +874,25 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
       !a->a_array) {
     /* 2: HCBLAS_MATH_OZAKI_INT8, 3: HCBLAS_MATH_OZAKI_F16 */
     const bool f16 = st->math_mode == 3;
-    const int s = st->math_param > 0 ? st->math_param : (f16 ? 7 : st->ozaki_default_slices);
+    const int s = st->math_param > 0 || st->accuracy_bits != 0
+                      ? plan_emulation(st->math_mode, st->math_param, st->accuracy_bits, HCBK_D,
+                                       a->k, nullptr)
+                      : (f16 ? 7 : st->ozaki_default_slices);
     int rc = dgemm_ozaki(st, a, s, f16, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] ozaki path declined (%d)\n", rc);
   }
   if (a->dtype == HCBK_D && st->math_mode == 4 /* HCBLAS_MATH_OZAKI_CRT */ && a->batch == 1 &&
       !a->a_array) {
-    int rc = dgemm_crt(st, a, st->math_param, stream, path);
+    const int want = plan_emulation(4, st->math_param, st->accuracy_bits, HCBK_D, a->k, nullptr);
+    int rc = dgemm_crt(st, a, want, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] crt path declined (%d)\n", rc);
   }
   if (a->dtype == HCBK_Z && st->math_mode == 4 /* HCBLAS_MATH_OZAKI_CRT */ && a->batch == 1 &&
       !a->a_array) {
-    int rc = zgemm_crt(st, a, st->math_param, stream, path);
+    const int want = plan_emulation(4, st->math_param, st->accuracy_bits, HCBK_Z, a->k, nullptr);
+    int rc = zgemm_crt(st, a, want, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] complex crt path declined (%d)\n", rc);
   }

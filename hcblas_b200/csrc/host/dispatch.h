@@ -52,6 +52,21 @@ std::string tune_key(const char *family, const hcbk_gemm_args *a);
 int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int ncand,
                 const std::function<int(int)> &run, int fallback);
 
+/* CRT plan of a real row of length k (dispatch.cpp): the moduli count, the
+ * shift below 53 bits of the norm-scaled integers and whether rows are
+ * norm-scaled; want = 0 picks the fewest moduli that keep every row at its
+ * full 53 bits, want = n uses n moduli.  false when n moduli are too few. */
+bool crt_plan_rows(int64_t k, int want, int *nmod, int *shift, bool *norm);
+
+/* The emulated modes' planner (plan.cpp): the count (terms, slices or
+ * moduli) a call of `dtype` with inner dimension k uses under math mode
+ * `mode` -- `param` when it is > 0, else the smallest count whose model
+ * error reaches `bits` (-1: the format's native precision), else (bits == 0)
+ * the mode's default; 0 when the mode does not apply to the dtype.
+ * *model_bits (optional) receives the count's model accuracy in bits. */
+int plan_emulation(int mode, int param, int bits, int dtype, int64_t k, double *model_bits);
+double emulation_model_bits(int mode, int dtype, int64_t k, int count);
+
 /* Grouped HGEMM over `count` problems (grouped.cpp): builds or reuses the
  * handle's device problem table and runs the persistent kernel. */
 int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,

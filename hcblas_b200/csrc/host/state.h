@@ -64,6 +64,9 @@ struct HcblasB200State {
   int tc_pair = 1; /* CTA-pair (cta_group::2) tensor-core kernels: 0 never, 1 auto, 2 always */
   int crt_i8 = 1;  /* CRT DGEMM modular GEMMs: 1 int8 residues on kind::i8, 0 binary16 */
   int ozaki_default_slices = 7; /* Ozaki slices when the mode's param is 0 */
+  /* requested accuracy of the emulated modes in bits (hcblasSetAccuracyTarget;
+   * 0: each mode's default count, -1: the format's native precision) */
+  int accuracy_bits = 0;
   const char *last_path = "none";
   /* device workspace owned by the handle (grown on demand, freed at destroy) */
   void *workspace = nullptr; /* cudaMallocAsync'd, released stream-ordered */

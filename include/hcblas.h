@@ -410,6 +410,33 @@ enum {
 hcblasStatus_t hcblasSetMathMode(hcblasHandle_t handle, int mode, int param);
 hcblasStatus_t hcblasGetMathMode(hcblasHandle_t handle, int *mode, int *param);
 
+/* Extension: requested accuracy of the emulated math modes.  When the math
+ * mode's `param` is 0, the count (split-BF16 terms, Ozaki slices, CRT
+ * moduli) is the smallest whose model error reaches `bits`:
+ *     RMS(error of c_ij) <= 2^-bits * ||row i of op(A)||_2 * ||col j of op(B)||_2,
+ * the error level of a dot product accumulated in a binary format with a
+ * bits-bit significand, so 53 asks for native FP64 accuracy and 24 for
+ * native FP32.  HCBLAS_ACCURACY_NATIVE (-1) means 53 for D/Z and 24 for S/C;
+ * HCBLAS_ACCURACY_DEFAULT (0, the initial value) keeps each mode's default
+ * count (CRT: the fewest moduli keeping every row's full 53 bits; Ozaki-I:
+ * 7 slices for D, 4 for S; split-BF16: 3 terms).  Model per scheme: CRT
+ * with norm-scaled rows keeps nb bits whatever the data and K (14 moduli:
+ * nb = 54); Ozaki-I keeps b*s - log2(1.33 sqrt(K (s-1)) + 1.63) bits in the
+ * worst case over the data; split-BF16 keeps 15 (3 terms) or 24 (6 terms).
+ * A target no count reaches gets the mode's largest count.
+ * Status: NOT_INITIALIZED for a bad handle; INVALID_VALUE outside -1..64. */
+#define HCBLAS_ACCURACY_DEFAULT 0
+#define HCBLAS_ACCURACY_NATIVE (-1)
+hcblasStatus_t hcblasSetAccuracyTarget(hcblasHandle_t handle, int bits);
+hcblasStatus_t hcblasGetAccuracyTarget(hcblasHandle_t handle, int *bits);
+/* The plan without a handle or a GPU: the count a call of `dtype` (0 = S,
+ * 1 = D, 2 = C, 3 = Z) with inner dimension k takes under math mode `mode`
+ * with parameter `param` and accuracy target `bits`, and that count's model
+ * accuracy in bits (+inf when the scheme represents the operands exactly).
+ * INVALID_VALUE when the mode does not emulate that dtype. */
+hcblasStatus_t hcblasPlanEmulation(int mode, int param, int bits, int dtype, long long k,
+                                   int *count, double *model_bits);
+
 /* Extension: set a named tuning knob on the handle.
  *   "split_promote_kb"  split-BF16 paths: 64-element K-slabs accumulated in
  *                       TMEM before each promotion to the IEEE f32
