@@ -421,8 +421,10 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for both element sizes */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
   const size_t a_pl = up1k((size_t)a->m * kp * esz), b_pl = up1k((size_t)a->n * kp * esz);
-  const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
-  const size_t t_pl = up1k((size_t)ldt * a->n * 2);
+  /* int8 residues of C: 16-byte columns for the tensor stores and the
+   * combine's bulk copies */
+  const int64_t ldt = (a->m + 15) & ~int64_t(15);
+  const size_t t_pl = up1k((size_t)ldt * a->n);
   const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
   const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
   /* per row: the fraction and its reciprocal */
@@ -518,9 +520,9 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   g.b_plane_stride = (int64_t)b_pl;
   g.nmod = nmod;
   g.moduli = mods;
-  g.t = reinterpret_cast<int16_t *>(t_base);
+  g.t = reinterpret_cast<int8_t *>(t_base);
   g.ldt = ldt;
-  g.t_plane_stride = (int64_t)(t_pl / 2);
+  g.t_plane_stride = (int64_t)t_pl;
   g.pair = pair;
   g.bn = bn;
   g.i8 = i8 ? 1 : 0;
@@ -543,8 +545,8 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.m = a->m;
   cb.n = a->n;
   cb.nmod = nmod;
-  cb.res = reinterpret_cast<const int16_t *>(t_base);
-  cb.res_plane = (int64_t)(t_pl / 2);
+  cb.res = reinterpret_cast<const int8_t *>(t_base);
+  cb.res_plane = (int64_t)t_pl;
   cb.ldr = ldt;
   cb.exp_a = exp_a;
   cb.exp_b = exp_b;
@@ -584,8 +586,10 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int64_t kp = (a->k + 15) & ~int64_t(15); /* 16-byte row pitch for both element sizes */
   auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
   const size_t a_pl = up1k((size_t)a->m * kp * esz), b_pl = up1k((size_t)a->n * kp * esz);
-  const int64_t ldt = (a->m + 7) & ~int64_t(7); /* 16-byte rows: the combine's bulk copies */
-  const size_t t_pl = up1k((size_t)ldt * a->n * 2);
+  /* int8 residues of C: 16-byte columns for the tensor stores and the
+   * combine's bulk copies */
+  const int64_t ldt = (a->m + 15) & ~int64_t(15);
+  const size_t t_pl = up1k((size_t)ldt * a->n);
   /* the real view of an MN-contiguous operand has two real rows per row */
   const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
   const size_t ea_bytes = up1k(sizeof(int) * a->m * 2), eb_bytes = up1k(sizeof(int) * a->n * 2);
@@ -697,9 +701,9 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
     g.b_plane_stride = (int64_t)b_pl;
     g.nmod = nmod;
     g.moduli = mods;
-    g.t = reinterpret_cast<int16_t *>(t_base + set * nmod * t_pl);
+    g.t = reinterpret_cast<int8_t *>(t_base + set * nmod * t_pl);
     g.ldt = ldt;
-    g.t_plane_stride = (int64_t)(t_pl / 2);
+    g.t_plane_stride = (int64_t)t_pl;
     g.pair = pair;
     g.bn = bn;
     g.i8 = i8 ? 1 : 0;
@@ -711,8 +715,8 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.m = a->m;
   cb.n = a->n;
   cb.nmod = nmod;
-  cb.res = reinterpret_cast<const int16_t *>(t_base);
-  cb.res_plane = (int64_t)(t_pl / 2);
+  cb.res = reinterpret_cast<const int8_t *>(t_base);
+  cb.res_plane = (int64_t)t_pl;
   cb.ldr = ldt;
   cb.exp_a = exp_a;
   cb.exp_b = exp_b;

@@ -346,8 +346,8 @@ struct CombArgs {
   double w[HCBK_CRT_MAX_MODULI][MAX_NC]; /* 40-bit chunks of w_i, low first */
   double mk[MAX_NC];                     /* 40-bit chunks of M, low first */
   double inv_m;                          /* RN(1 / M) */
-  const int16_t *res;
-  int64_t res_plane; /* elements between residue planes */
+  const int8_t *res;
+  int64_t res_plane; /* bytes between residue planes */
   int64_t ldr;
   const int *exp_a;
   const int *exp_b;
@@ -418,18 +418,18 @@ struct CrtAcc {
   }
 };
 
-/* real combine: 256 consumer threads x 2 consecutive rows (one 4-byte
- * residue load per modulus); 3 stages of nmod KB */
+/* real combine: 256 consumer threads x 2 consecutive rows (one 2-byte
+ * load of two int8 residues per modulus); 3 stages of nmod / 2 KB */
 constexpr int CMB_THREADS = 256, CMB_RPT = 2, CMB_ROWS = CMB_THREADS * CMB_RPT;
 constexpr int CMB_STAGES = 3;
 /* complex combine: 256 consumer threads x 1 row (two accumulators a row
- * already); 3 stages of 1.5 nmod KB */
+ * already); 3 stages of 0.75 nmod KB */
 constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 1, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
 constexpr int ZCMB_STAGES = 3;
 
-/* signed 16-bit halves of a 32-bit word */
-__device__ __forceinline__ int lo16(uint32_t w) { return (int)(w << 16) >> 16; }
-__device__ __forceinline__ int hi16(uint32_t w) { return (int)w >> 16; }
+/* the two signed bytes of a 16-bit word */
+__device__ __forceinline__ int lo8(uint32_t w) { return (int)(w << 24) >> 24; }
+__device__ __forceinline__ int hi8(uint32_t w) { return (int)(w << 16) >> 24; }
 
 /* Producer of a warp-specialised combine (one thread): tile j of this block
  * (ROWS rows of one column, every residue plane) goes to stage j % STAGES by
@@ -438,9 +438,9 @@ __device__ __forceinline__ int hi16(uint32_t w) { return (int)w >> 16; }
  * consumers took them; bounded when a wait failed), so that no copy writes
  * shared memory after the block has left. */
 template <int STAGES, int ROWS>
-__device__ __forceinline__ void ws_produce(const int16_t *res, int64_t res_plane, int64_t ldr,
+__device__ __forceinline__ void ws_produce(const int8_t *res, int64_t res_plane, int64_t ldr,
                                            int nplanes, int64_t row_tiles, int64_t ntiles,
-                                           int16_t *buf, uint64_t *full, uint64_t *empty,
+                                           int8_t *buf, uint64_t *full, uint64_t *empty,
                                            int *err) {
   using namespace hcbk::tc;
   const size_t stage_elems = (size_t)nplanes * ROWS;
@@ -452,10 +452,10 @@ __device__ __forceinline__ void ws_produce(const int16_t *res, int64_t res_plane
       break;
     const int64_t r0 = (t % row_tiles) * ROWS, col = t / row_tiles;
     const int64_t rows = ldr - r0 < ROWS ? ldr - r0 : ROWS;
-    const uint32_t bytes = (uint32_t)rows * 2u; /* ldr, r0 multiples of 8 */
+    const uint32_t bytes = (uint32_t)rows; /* ldr, r0 multiples of 16 */
     mbar_expect_tx(&full[s], bytes * (uint32_t)nplanes);
-    const int16_t *src = res + col * ldr + r0;
-    int16_t *dst = buf + s * stage_elems;
+    const int8_t *src = res + col * ldr + r0;
+    int8_t *dst = buf + s * stage_elems;
     for (int p = 0; p < nplanes; ++p)
       bulk_load_1d(dst + p * ROWS, src + p * res_plane, bytes, &full[s]);
   }
@@ -468,14 +468,14 @@ __device__ __forceinline__ void ws_produce(const int16_t *res, int64_t res_plane
 }
 
 /* Real combine, warp-specialised: warps 0-7 reconstruct 512-row tiles (two
- * consecutive rows per thread, one 4-byte load of a residue pair per
+ * consecutive rows per thread, one 2-byte load of an int8 residue pair per
  * modulus), warp 8's lane 0 keeps CMB_STAGES tiles of residues in flight by
  * 1-D bulk copies.  Per stage a `full` barrier (transaction bytes) and an
  * `empty` barrier (one arrival per consumer warp) replace block-wide
  * barriers, so consumer warps run up to CMB_STAGES - 1 tiles apart.  The
  * modulus loop is unrolled over the maximum count, so every weight chunk is
  * a constant-bank operand of its FMA.  Requires the row pitch and plane
- * stride to be multiples of 8 elements (16 bytes). */
+ * stride to be multiples of 16 bytes. */
 constexpr int CMB_CONSUMERS = CMB_THREADS / 32;
 constexpr int CMB_BLOCK = CMB_THREADS + 32;
 
@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_
   }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = a.nmod;
-  int16_t *buf = reinterpret_cast<int16_t *>(cmb_smem);
+  int8_t *buf = reinterpret_cast<int8_t *>(cmb_smem);
   const int64_t row_tiles = (a.m + CMB_ROWS - 1) / CMB_ROWS;
   const int64_t ntiles = row_tiles * a.n;
   const int64_t first = blockIdx.x, stride = gridDim.x;
@@ -518,15 +518,15 @@ __global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_
     if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)(j / CMB_STAGES) & 1u, a.err,
                                            ERR_TIMEOUT_COMBINE)))
       break;
-    const int16_t *R = buf + s * stage_elems;
+    const int8_t *R = buf + s * stage_elems;
     const int64_t row = (t % row_tiles) * CMB_ROWS + CMB_RPT * tid, col = t / row_tiles;
     if (row < a.m) {
       CrtAcc<NC> acc[CMB_RPT];
 #pragma unroll
       for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights */
         if (i >= nmod) break;
-        const uint32_t q = *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
-        const double r0 = small_int_to_d(lo16(q)), r1 = small_int_to_d(hi16(q));
+        const uint32_t q = *reinterpret_cast<const uint16_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
+        const double r0 = small_int_to_d(lo8(q)), r1 = small_int_to_d(hi8(q));
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           acc[0].S[k] = fma(r0, a.w[i][k], acc[0].S[k]);
@@ -916,7 +916,7 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
   }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = a.g.nmod;
-  int16_t *buf = reinterpret_cast<int16_t *>(cmb_smem);
+  int8_t *buf = reinterpret_cast<int8_t *>(cmb_smem);
   const int64_t row_tiles = (a.g.m + ZCMB_ROWS - 1) / ZCMB_ROWS;
   const int64_t ntiles = row_tiles * a.g.n;
   const size_t stage_elems = (size_t)3 * nmod * ZCMB_ROWS;
@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
     if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)(j / ZCMB_STAGES) & 1u, a.g.err,
                                            ERR_TIMEOUT_COMBINE)))
       break;
-    const int16_t *R = buf + s * stage_elems;
+    const int8_t *R = buf + s * stage_elems;
     const int64_t row = (t % row_tiles) * ZCMB_ROWS + tid, col = t / row_tiles;
     CrtAcc<NC> acc_re, acc_im;
     if (row < a.g.m) {
@@ -1082,7 +1082,7 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.beta_nonzero = in->beta != 0.0;
   a.err = in->err;
   const int64_t ntiles = (a.m + CMB_ROWS - 1) / CMB_ROWS * a.n;
-  const size_t smem = (size_t)CMB_STAGES * a.nmod * CMB_ROWS * sizeof(int16_t);
+  const size_t smem = (size_t)CMB_STAGES * a.nmod * CMB_ROWS * sizeof(int8_t);
   int64_t grid = 0;
   int rc;
   switch (a.nc) {
@@ -1173,7 +1173,7 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   a.alpha = make_double2(in->alpha_re, in->alpha_im);
   a.beta = make_double2(in->beta_re, in->beta_im);
   const int64_t ntiles = (a.g.m + ZCMB_ROWS - 1) / ZCMB_ROWS * a.g.n;
-  const size_t smem = (size_t)ZCMB_STAGES * 3 * a.g.nmod * ZCMB_ROWS * sizeof(int16_t);
+  const size_t smem = (size_t)ZCMB_STAGES * 3 * a.g.nmod * ZCMB_ROWS * sizeof(int8_t);
   int64_t grid = 0;
   int rc;
   switch (a.g.nc) {

@@ -305,24 +305,24 @@ typedef struct hcbk_crt_gemm {
   int64_t a_plane_stride, b_plane_stride; /* bytes, multiples of 16 */
   int nmod;
   const int *moduli; /* host array of nmod moduli */
-  int16_t *t;                       /* 16-byte aligned */
-  int64_t ldt, t_plane_stride;      /* elements, multiples of 8 */
+  int8_t *t;                        /* residues of C, 16-byte aligned */
+  int64_t ldt, t_plane_stride;      /* bytes, multiples of 16 */
   int bn;   /* tile columns: 128 or 256 */
   int pair; /* 1: CTA pairs, 256 x 256 tiles (bn = 256) */
   int i8;   /* 1: int8 residue planes on kind::i8 */
 } hcbk_crt_gemm;
 int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
 
-/* CRT reconstruction of P' from the residue planes and the epilogue
- * C = alpha * P' * 2^(exp_a[m] + exp_b[n] - shift) + beta * C.  Residues are
- * read by 1-D bulk copies: res 16-byte aligned, ldr >= m and res_plane
- * multiples of 8 elements. */
+/* CRT reconstruction of P' from the int8 residue planes (|r| <= 127) and
+ * the epilogue C = alpha * P' * 2^(exp_a[m] + exp_b[n] - shift) + beta * C.
+ * Residues are read by 1-D bulk copies: res 16-byte aligned, ldr >= m and
+ * res_plane multiples of 16. */
 typedef struct hcbk_crt_combine_args {
   int64_t m, n;
   int nmod;
-  const int16_t *res;
-  int64_t res_plane; /* elements between planes, multiple of 8 */
-  int64_t ldr;       /* >= m, multiple of 8 */
+  const int8_t *res;
+  int64_t res_plane; /* bytes between planes, multiple of 16 */
+  int64_t ldr;       /* >= m, multiple of 16 */
   const int *exp_a;
   const int *exp_b;
   const double *inv_a, *inv_b; /* optional reciprocals of the row fractions
@@ -361,16 +361,16 @@ typedef struct hcbk_zcrt_prep {
 } hcbk_zcrt_prep;
 int hcbk_zcrt_residues(const hcbk_zcrt_prep *a, void *stream);
 
-/* Complex combine: res holds 3 sets of nmod int16 planes (T1 = Ar Br,
+/* Complex combine: res holds 3 sets of nmod int8 planes (T1 = Ar Br,
  * T2 = Ai Bi, T3 = (Ar+Ai)(Br+Bi) mod p_i); writes
  * C = alpha * ((T1 - T2) + i (T3 - T1 - T2)) 2^(e_m + f_n - shift) + beta * C
  * into the double2 matrix c. */
 typedef struct hcbk_zcrt_combine_args {
   int64_t m, n;
   int nmod;
-  const int16_t *res;
-  int64_t res_plane; /* elements between planes, multiple of 8 */
-  int64_t ldr;       /* >= m, multiple of 8 */
+  const int8_t *res;
+  int64_t res_plane; /* bytes between planes, multiple of 16 */
+  int64_t ldr;       /* >= m, multiple of 16 */
   const int *exp_a;
   const int *exp_b;
   int exp_a_pair, exp_b_pair;

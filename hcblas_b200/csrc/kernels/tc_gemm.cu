@@ -51,7 +51,7 @@ constexpr int BM = 128;
 struct TcParams {
   CUtensorMap ta[MAX_PLANES];
   CUtensorMap tb[MAX_PLANES];
-  CUtensorMap tc; /* output map: int16 residue planes {rows, cols, plane} of the
+  CUtensorMap tc; /* output map: int8 residue planes {rows, cols, plane} of the
                      modular epilogue, or f16 C {rows, cols} when out_tma is set */
   int m, n, k;
   int k0; /* first K coordinate (K split across launches) */
@@ -316,8 +316,8 @@ template <typename OutT> struct EpiAlphaBeta {
  * after which the MMAs keep accumulating on top of the reduced value.
  * Chunks alternate between the two TMEM buffers, so one buffer is reduced
  * while the tensor core fills the other; the last two chunks of a tile are
- * combined, reduced, and stored as symmetric int16 residues (C viewed as
- * the column-major int16 residue plane).  No register accumulator, no
+ * combined, reduced, and stored as symmetric int8 residues (C viewed as
+ * the column-major int8 residue plane).  No register accumulator, no
  * float->int conversion before the final store. */
 struct EpiModP {
   static constexpr bool INPLACE = true;
@@ -353,14 +353,14 @@ struct EpiModP {
     tmem_st_wait();
   }
 
-  /* output staging: per epilogue warp two 32 x 32 int16 boxes (2 KB each) */
-  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * 2;
+  /* output staging: per epilogue warp two 32 x 32 int8 boxes (1 KB each) */
+  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32; /* int8 residues */
   static constexpr uint32_t OUT_WARP_BYTES = 2 * OUT_BOX_BYTES;
   static constexpr uint32_t OUT_SMEM = 4 * OUT_WARP_BYTES;
 
   /* T[m0 + lane, n0 + c + j] = symmetric buffer mod p, for this warp's 32
    * rows: each 32-column group is written to one of the warp's two
-   * shared-memory boxes (column-major int16, as the plane) and stored by one
+   * shared-memory boxes (column-major int8, as the plane) and stored by one
    * TMA tensor store, which also drops rows >= m and columns >= n; a box is
    * rewritten only after the store issued from it two groups earlier has
    * read it.  `out` is this warp's OUT_WARP_BYTES of shared memory. */
@@ -374,7 +374,7 @@ struct EpiModP {
     const float hp = static_cast<float>((mod - 1) >> 1);
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
-      int16_t *box = reinterpret_cast<int16_t *>(out + ((c >> 5) & 1) * OUT_BOX_BYTES);
+      int8_t *box = reinterpret_cast<int8_t *>(out + ((c >> 5) & 1) * OUT_BOX_BYTES);
       uint32_t ra[32];
       tmem_ld_32x32b_x32(ta + c, ra);
       if (lane == 0) bulk_wait_read<1>(); /* the store from this box two groups ago */
@@ -386,8 +386,8 @@ struct EpiModP {
         float v = mod_f(__uint_as_float(ra[j]), pf, inv);
         if (v > hp) v -= pf;
         else if (v < -hp) v += pf;
-        /* low 16 bits of the 1.5 * 2^23 + v pattern: v as int16 */
-        box[j * 32 + lane] = static_cast<int16_t>(__float_as_int(v + RND));
+        /* low 8 bits of the 1.5 * 2^23 + v pattern: v as int8 (|v| <= 127) */
+        box[j * 32 + lane] = static_cast<int8_t>(__float_as_int(v + RND));
       }
       fence_proxy_async_smem();
       __syncwarp();
@@ -472,16 +472,16 @@ template <class E> struct CatK<E, std::void_t<decltype(E::CAT_K)>> : std::bool_c
  * y * RN(1/p) is within 1.6e-3 of y / p, below the 1/(2p) >= 1.96e-3 that
  * separates y / p (p odd) from any half-integer: q = rint(y / p) exactly,
  * and RND + y - q p = RND + r with r already in [-(p-1)/2, (p-1)/2], whose
- * low 16 bits are r as an int16.  Eight epilogue warps (two per TMEM lane
+ * low 8 bits are r as an int8 (|r| <= 127).  Eight epilogue warps (two per TMEM lane
  * quadrant, half of the columns each) read TMEM 64 columns at a time (one
- * wait per 64) into two 32 x 32 int16 shared-memory boxes per warp, each
+ * wait per 64) into two 32 x 32 int8 shared-memory boxes per warp, each
  * written by one TMA tensor store. */
 struct EpiModPi8 {
   static constexpr bool INPLACE = false;
   static constexpr bool PLANE_BATCH = true;
   static constexpr float RND = 12582912.0f; /* 1.5 * 2^23 */
   static constexpr int EPI_WARPS = 8;
-  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32 * 2;
+  static constexpr uint32_t OUT_BOX_BYTES = 32 * 32; /* int8 residues */
   static constexpr uint32_t OUT_WARP_BYTES = 2 * OUT_BOX_BYTES;
   static constexpr uint32_t OUT_SMEM = EPI_WARPS * OUT_WARP_BYTES;
 
@@ -493,14 +493,14 @@ struct EpiModPi8 {
     static_assert(NACC == 0, "the modular epilogue stores through final_store");
   }
 
-  /* the symmetric residue of s as an int16 (see above) */
-  static __device__ __forceinline__ int16_t residue(uint32_t s, int c16, float pf, float inv) {
+  /* the symmetric residue of s as an int8 (see above; |r| <= 127) */
+  static __device__ __forceinline__ int8_t residue(uint32_t s, int c16, float pf, float inv) {
     const int sv = static_cast<int>(s);
     const int hi = (sv + 0x8000) >> 16;
     const int y = hi * c16 + (sv - hi * 65536);
     const float yr = __int_as_float(0x4B400000 + y); /* RND + y */
     const float q = fmaf(yr - RND, inv, RND) - RND;
-    return static_cast<int16_t>(__float_as_int(fmaf(-q, pf, yr)));
+    return static_cast<int8_t>(__float_as_int(fmaf(-q, pf, yr)));
   }
 
   template <int BN>
@@ -515,7 +515,7 @@ struct EpiModPi8 {
     if (c16 > (mod - 1) / 2) c16 -= mod;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 64) {
-      int16_t *box = reinterpret_cast<int16_t *>(out);
+      int8_t *box = reinterpret_cast<int8_t *>(out);
       uint32_t ra[32], rb[32];
       tmem_ld_32x32b_x32(ta + c, ra);
       tmem_ld_32x32b_x32(ta + c + 32, rb);
@@ -1317,20 +1317,20 @@ extern "C" int hcbk_encode_tma_3d_planes(void *map, int bf16, const void *base, 
                          base, kdim, rows, planes, ld, pstride, box_rows);
 }
 
-/* 3-D map over the int16 residue planes T {rows, cols, plane}: column pitch
- * ld elements, plane pitch pstride elements; box {32, 32, 1}, no swizzle
- * (the modular epilogue's tensor stores). */
-static int make_map_out_i16(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols,
-                            uint64_t planes, uint64_t ld, uint64_t pstride) {
+/* 3-D map over the int8 residue planes T {rows, cols, plane}: column pitch
+ * ld bytes, plane pitch pstride bytes (multiples of 16); box {32, 32, 1}, no
+ * swizzle (the modular epilogue's tensor stores). */
+static int make_map_out_i8(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols,
+                           uint64_t planes, uint64_t ld, uint64_t pstride) {
   auto fn = encode_fn();
   if (!fn) return HCBK_ERR_DRIVER;
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 2) & 15) || ((pstride * 2) & 15))
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld & 15) || (pstride & 15))
     return HCBK_ERR_ALIGN;
   cuuint64_t dims[3] = {rows, cols, planes};
-  cuuint64_t strides[2] = {ld * 2, pstride * 2};
+  cuuint64_t strides[2] = {ld, pstride};
   cuuint32_t box[3] = {32, 32, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims, strides, box, estr,
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
@@ -1385,8 +1385,8 @@ extern "C" int hcbk_ozaki_groups_tc(const hcbk_ozaki_groups *g, int *err, void *
  * (K-major, |r| <= 127) read through 3-D tensor maps, tensor-core sums exact
  * over 1024-element K chunks (PROMOTE_KB = 16 slabs of 64:
  * 1024 * 127^2 + 383 < 2^24), reduced mod p in place in TMEM between chunks,
- * int16 residues out by TMA tensor stores (t 16-byte aligned, ldt and
- * t_plane_stride multiples of 8); the persistent tile walk spans all planes.  Tiles:
+ * int8 residues out by TMA tensor stores (t 16-byte aligned, ldt and
+ * t_plane_stride multiples of 16 bytes); the persistent tile walk spans all planes.  Tiles:
  * 256 x 256 over a CTA pair, or 128 x bn on one CTA. */
 extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) {
   if (g->m > 0x7fffffff || g->n > 0x7fffffff || g->k > 0x7fffffff || g->k <= 0 ||
@@ -1411,7 +1411,7 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
   p.ldc = g->ldt;
   p.nplanes = g->nmod;
   p.c_plane_stride = g->t_plane_stride;
-  rc = make_map_out_i16(&p.tc, g->t, g->m, g->n, g->nmod, g->ldt, g->t_plane_stride);
+  rc = make_map_out_i8(&p.tc, g->t, g->m, g->n, g->nmod, g->ldt, g->t_plane_stride);
   if (rc) return rc;
   for (int i = 0; i < g->nmod; ++i) {
     p.mod_tab[i] = g->moduli[i];

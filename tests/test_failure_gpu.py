@@ -80,7 +80,7 @@ def test_pipeline_wait_timeout_is_reported_and_handle_recovers(fresh_handle):
         assert hb.device_error(h) == 0
         assert hb.hcblasGetLastPath(h).startswith("tc.h.")
         _, ref = O.gemm(O.COL, 0, 0, M2, N2, K2, 1.0, A2, M2, B2, K2, 0.0,
-                        np.zeros(M2 * N2), M2)
+                        np.zeros(M2 * N2, np.float16), M2)
         got = O.view_c(dC.download().astype(np.float64), O.COL, M2, N2, M2)
         assert O.normwise_rel_error(got, ref) < 2e-3
 
@@ -143,7 +143,7 @@ def test_corrupted_autotune_cache_is_retuned(tmp_path):
         "dC = hb.DeviceArray(h, np.zeros(M*N, np.float16))\n"
         "assert hb.lib_gemm(h, O.COL, 'n', 'n', M, N, K, 1.0, dA, M, dB, K, 0.0, dC, M) == 0\n"
         "assert hb.device_error(h) == 0\n"
-        "_, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, np.zeros(M*N), M)\n"
+        "_, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, np.zeros(M*N, np.float16), M)\n"
         "got = O.view_c(dC.download().astype(np.float64), O.COL, M, N, M)\n"
         "assert O.normwise_rel_error(got, ref) < 2e-3\n"
         "print('ok')\n" % ROOT)
