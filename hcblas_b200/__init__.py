@@ -61,6 +61,7 @@ EXPORTED = (
     "hcblasDgemvBatched", "hcblasSger", "hcblasDger", "hcblasSgerBatched", "hcblasDgerBatched",
     "hcblasSetAccuracyTarget", "hcblasGetAccuracyTarget", "hcblasPlanEmulation",
     "hcblasSgemmSplitBF16NoAlloc", "hcblasSgemmSplitBF16NoAllocStatus",
+    "hcblasDgemmGrouped", "hcblasCgemmGrouped", "hcblasZgemmGrouped",
 )
 
 # accuracy targets (extension)

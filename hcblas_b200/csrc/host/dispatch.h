@@ -72,6 +72,12 @@ double emulation_model_bits(int mode, int dtype, int64_t k, int count);
 int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,
                   const hcblasGemmProblem *probs, float alpha, float beta);
 
+/* Grouped GEMM of S/D/C/Z problems on the CUDA cores (one persistent
+ * launch); scalars as real and imaginary parts. */
+int grouped_simt(HcblasB200State *st, void *stream, int dtype, hcblasOrder order, int count,
+                 const hcblasGemmProblem *probs, double alpha_re, double alpha_im,
+                 double beta_re, double beta_im);
+
 /* Grouped FP32 GEMM on the split-BF16 tensor-core path (terms 3 or 6). */
 int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, int count,
                         const hcblasGemmProblem *probs, float alpha, float beta, int terms);

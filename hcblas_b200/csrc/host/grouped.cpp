@@ -36,11 +36,15 @@ struct Canon {
   int64_t ldc;
 };
 
-/* column-major form; for real data the conjugate transpose is the transpose */
-Canon canonical(const hcblasGemmProblem &p, hcblasOrder order) {
+/* column-major form; for real data the conjugate transpose is the
+ * transpose, complex data keeps it */
+Canon canonical(const hcblasGemmProblem &p, hcblasOrder order, bool cplx = false) {
   Canon c;
-  c.op_a = p.transa == HCBLAS_OP_N ? HCBK_OP_N : HCBK_OP_T;
-  c.op_b = p.transb == HCBLAS_OP_N ? HCBK_OP_N : HCBK_OP_T;
+  auto op = [&](hcblasOperation_t t) {
+    return t == HCBLAS_OP_N ? HCBK_OP_N : (cplx && t == HCBLAS_OP_C) ? HCBK_OP_C : HCBK_OP_T;
+  };
+  c.op_a = op(p.transa);
+  c.op_b = op(p.transb);
   c.m = p.m;
   c.n = p.n;
   c.k = p.k;
@@ -431,6 +435,128 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
   return HCBK_OK;
 }
 
+/* Grouped GEMM on the CUDA cores for S/D/C/Z in their own arithmetic: one
+ * persistent launch over the device problem table (hcbk_gemm_simt_grouped),
+ * problems ordered by decreasing work; the table is cached per handle for
+ * a byte-identical follow-up problem array. */
+int grouped_simt(HcblasB200State *st, void *stream, int dtype, hcblasOrder order, int count,
+                 const hcblasGemmProblem *probs, double alpha_re, double alpha_im,
+                 double beta_re, double beta_im) {
+  const bool cplx = dtype == HCBK_C || dtype == HCBK_Z;
+  if (alpha_re == 0.0 && alpha_im == 0.0) { /* C_i := beta*C_i, A and B not referenced */
+    for (int i = 0; i < count; ++i) {
+      const Canon c = canonical(probs[i], order, cplx);
+      hcbk_gemm_args a;
+      std::memset(&a, 0, sizeof(a));
+      a.dtype = dtype;
+      a.m = c.m;
+      a.n = c.n;
+      a.k = c.k;
+      a.c = c.c;
+      a.ldc = c.ldc;
+      a.batch = 1;
+      a.beta_re = beta_re;
+      a.beta_im = beta_im;
+      int rc = timed_launch(st, stream, "scale", [&] { return hcbk_scale_c(&a, stream); });
+      if (rc) return rc;
+    }
+    st->last_path = "scale";
+    return HCBK_OK;
+  }
+  int bm = 0, bn = 0;
+  if (hcbk_simt_grouped_tile(dtype, &bm, &bn) != HCBK_OK) return HCBK_ERR_ARGS;
+  HcblasGroupedPlan &gp = st->grouped_simt;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::vector<unsigned char> key(sizeof(hcblasGemmProblem) * (size_t)count + 3);
+  std::memcpy(key.data(), probs, sizeof(hcblasGemmProblem) * (size_t)count);
+  key[key.size() - 3] = static_cast<unsigned char>(order);
+  key[key.size() - 2] = static_cast<unsigned char>(dev);
+  key[key.size() - 1] = static_cast<unsigned char>(dtype);
+  const bool reuse = gp.table && gp.table_device == dev && key == gp.key;
+  if (!reuse) {
+    if (!st->graph_cache.empty()) {
+      cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+      clear_graph_cache(st);
+    }
+    gp.key.clear();
+    std::vector<hcbk_simt_entry> ent((size_t)count);
+    std::vector<int> order_idx((size_t)count);
+    for (int i = 0; i < count; ++i) {
+      const Canon c = canonical(probs[i], order, cplx);
+      if (c.m > 0x7fffffff || c.n > 0x7fffffff || c.k > 0x7fffffff) return HCBK_ERR_ARGS;
+      hcbk_simt_entry &e = ent[i];
+      e.a = c.a;
+      e.b = c.b;
+      e.c = c.c;
+      e.lda = c.lda;
+      e.ldb = c.ldb;
+      e.ldc = c.ldc;
+      e.m = (int32_t)c.m;
+      e.n = (int32_t)c.n;
+      e.k = (int32_t)c.k;
+      e.op_a = c.op_a;
+      e.op_b = c.op_b;
+      e.tiles_m = (int32_t)((c.m + bm - 1) / bm);
+      order_idx[i] = i;
+    }
+    auto work = [&](int i) {
+      const hcbk_simt_entry &e = ent[i];
+      return (int64_t)e.tiles_m * ((e.n + bn - 1) / bn) * (int64_t)e.k;
+    };
+    std::stable_sort(order_idx.begin(), order_idx.end(),
+                     [&](int x, int y) { return work(x) > work(y); });
+    const size_t ent_bytes = sizeof(hcbk_simt_entry) * (size_t)count;
+    const size_t ts_off = (ent_bytes + 255) & ~size_t(255);
+    const size_t bytes = ts_off + sizeof(int32_t) * ((size_t)count + 1);
+    if (!ensure_table(gp, bytes, stream) || !ensure_staging(gp, bytes)) return HCBK_ERR_NOMEM;
+    unsigned char *stg = static_cast<unsigned char *>(gp.staging);
+    auto *dst = reinterpret_cast<hcbk_simt_entry *>(stg);
+    auto *ts = reinterpret_cast<int32_t *>(stg + ts_off);
+    int64_t total = 0;
+    for (int j = 0; j < count; ++j) {
+      const hcbk_simt_entry &e = ent[order_idx[j]];
+      dst[j] = e;
+      ts[j] = (int32_t)total;
+      total += (int64_t)e.tiles_m * ((e.n + bn - 1) / bn);
+      if (total > 0x7fffffff) return HCBK_ERR_ARGS;
+    }
+    ts[count] = (int32_t)total;
+    if (cudaMemcpyAsync(gp.table, stg, bytes, cudaMemcpyHostToDevice,
+                        static_cast<cudaStream_t>(stream)) != cudaSuccess)
+      return HCBK_ERR_LAUNCH;
+    if (!gp.upload_done &&
+        cudaEventCreateWithFlags(reinterpret_cast<cudaEvent_t *>(&gp.upload_done),
+                                 cudaEventDisableTiming) != cudaSuccess) {
+      gp.upload_done = nullptr;
+      cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    } else {
+      cudaEventRecord(static_cast<cudaEvent_t>(gp.upload_done),
+                      static_cast<cudaStream_t>(stream));
+    }
+    gp.count = count;
+    gp.total_tiles = (int)total;
+    gp.tile_start_offset = ts_off;
+    gp.key = key;
+  }
+  hcbk_simt_grouped_args g;
+  g.dtype = dtype;
+  g.table = static_cast<const hcbk_simt_entry *>(gp.table);
+  g.tile_start =
+      reinterpret_cast<const int32_t *>(static_cast<char *>(gp.table) + gp.tile_start_offset);
+  g.count = gp.count;
+  g.total_tiles = gp.total_tiles;
+  g.alpha_re = alpha_re;
+  g.alpha_im = cplx ? alpha_im : 0.0;
+  g.beta_re = beta_re;
+  g.beta_im = cplx ? beta_im : 0.0;
+  static const char *names[4] = {"simt.s.grouped", "simt.d.grouped", "simt.c.grouped",
+                                 "simt.z.grouped"};
+  st->last_path = names[dtype];
+  return timed_launch(st, stream, names[dtype],
+                      [&] { return hcbk_gemm_simt_grouped(&g, stream); });
+}
+
 }  // namespace hcblas_b200
 
 extern "C" hcblasStatus_t hcblasHgemmGrouped(hcblasHandle_t handle, int count,
@@ -490,4 +616,74 @@ extern "C" hcblasStatus_t hcblasSgemmGrouped(hcblasHandle_t handle, int count,
     std::fprintf(stderr, "[hcblas] grouped sgemm count=%d path=%s rc=%d\n", count,
                  handle->impl->last_path, rc);
   return rc == HCBK_OK ? HCBLAS_STATUS_SUCCESS : HCBLAS_STATUS_EXECUTION_FAILED;
+}
+
+namespace {
+
+/* the status rules of hcblasHgemmGrouped, then the SIMT grouped kernel */
+hcblasStatus_t simt_grouped_call(hcblasHandle_t handle, int dtype, int count,
+                                 const hcblasGemmProblem *problems, const void *alpha,
+                                 const void *beta) {
+  using namespace hcblas_b200;
+  if (handle == nullptr || !handle->initialized || handle->impl == nullptr)
+    return HCBLAS_STATUS_NOT_INITIALIZED;
+  if (count < 0 || (count > 0 && problems == nullptr) || alpha == nullptr || beta == nullptr)
+    return HCBLAS_STATUS_INVALID_VALUE;
+  for (int i = 0; i < count; ++i)
+    if (problems[i].m < 0 || problems[i].n < 0 || problems[i].k < 0)
+      return HCBLAS_STATUS_INVALID_VALUE;
+  for (int i = 0; i < count; ++i) {
+    const hcblasGemmProblem &p = problems[i];
+    if (p.m == 0 || p.n == 0 || p.k == 0 || p.A == nullptr || p.B == nullptr || p.C == nullptr)
+      return HCBLAS_STATUS_EXECUTION_FAILED;
+  }
+  if (count == 0) return HCBLAS_STATUS_SUCCESS;
+  DeviceGuard dev(handle->currentAcclView.device_id);
+  if (!dev.ok()) return HCBLAS_STATUS_EXECUTION_FAILED;
+  double ar = 0, ai = 0, br = 0, bi = 0;
+  switch (dtype) {
+    case HCBK_D:
+      ar = *static_cast<const double *>(alpha);
+      br = *static_cast<const double *>(beta);
+      break;
+    case HCBK_C: {
+      const hcComplex *a = static_cast<const hcComplex *>(alpha);
+      const hcComplex *b = static_cast<const hcComplex *>(beta);
+      ar = a->x, ai = a->y, br = b->x, bi = b->y;
+      break;
+    }
+    default: {
+      const hcDoubleComplex *a = static_cast<const hcDoubleComplex *>(alpha);
+      const hcDoubleComplex *b = static_cast<const hcDoubleComplex *>(beta);
+      ar = a->x, ai = a->y, br = b->x, bi = b->y;
+      break;
+    }
+  }
+  int rc = grouped_simt(handle->impl, handle->currentAcclView.stream, dtype, handle->Order, count,
+                        problems, ar, ai, br, bi);
+  if (log_enabled())
+    std::fprintf(stderr, "[hcblas] grouped dtype=%d count=%d path=%s rc=%d\n", dtype, count,
+                 handle->impl->last_path, rc);
+  return rc == HCBK_OK ? HCBLAS_STATUS_SUCCESS : HCBLAS_STATUS_EXECUTION_FAILED;
+}
+
+}  // namespace
+
+extern "C" hcblasStatus_t hcblasDgemmGrouped(hcblasHandle_t handle, int count,
+                                             const hcblasGemmProblem *problems,
+                                             const double *alpha, const double *beta) {
+  return simt_grouped_call(handle, HCBK_D, count, problems, alpha, beta);
+}
+
+extern "C" hcblasStatus_t hcblasCgemmGrouped(hcblasHandle_t handle, int count,
+                                             const hcblasGemmProblem *problems,
+                                             const hcComplex *alpha, const hcComplex *beta) {
+  return simt_grouped_call(handle, HCBK_C, count, problems, alpha, beta);
+}
+
+extern "C" hcblasStatus_t hcblasZgemmGrouped(hcblasHandle_t handle, int count,
+                                             const hcblasGemmProblem *problems,
+                                             const hcDoubleComplex *alpha,
+                                             const hcDoubleComplex *beta) {
+  return simt_grouped_call(handle, HCBK_Z, count, problems, alpha, beta);
 }

@@ -87,6 +87,7 @@ struct HcblasB200State {
   std::vector<void *> event_pool;
   HcblasGroupedPlan grouped;
   HcblasGroupedPlan grouped_split; /* hcblasSgemmGrouped (split-BF16) */
+  HcblasGroupedPlan grouped_simt;  /* hcblas{D,C,Z}gemmGrouped (CUDA cores) */
   /* CUDA-graph replay of repeated identical calls (off by default) */
   int graphs = 0;
   /* time candidate tile configurations per size bucket (off by default) */

@@ -464,6 +464,34 @@ typedef struct hcbk_grouped_args {
 } hcbk_grouped_args;
 int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
 
+/* ---------------------------------------------- grouped SIMT GEMM -- */
+
+/* One problem of the persistent grouped GEMM on the CUDA cores (any dtype):
+ * column-major C(m x n) = alpha op(A) op(B) + beta C, op_a/op_b HCBK_OP_*,
+ * pointers already offset, tiles_m = ceil(m / bm) of the dtype's tile. */
+typedef struct hcbk_simt_entry {
+  const void *a;
+  const void *b;
+  void *c;
+  int64_t lda, ldb, ldc;
+  int32_t m, n, k;
+  int32_t op_a, op_b;
+  int32_t tiles_m;
+} hcbk_simt_entry;
+
+typedef struct hcbk_simt_grouped_args {
+  int dtype;
+  const hcbk_simt_entry *table; /* device */
+  const int32_t *tile_start;    /* device, count + 1 ascending prefix sums */
+  int32_t count;
+  int32_t total_tiles;
+  double alpha_re, alpha_im, beta_re, beta_im;
+} hcbk_simt_grouped_args;
+
+/* the tile (bm x bn) the grouped kernel uses for a dtype */
+int hcbk_simt_grouped_tile(int dtype, int *bm, int *bn);
+int hcbk_gemm_simt_grouped(const hcbk_simt_grouped_args *g, void *stream);
+
 /* ------------------------------------------ grouped split-BF16 SGEMM -- */
 
 /* One operand of one grouped problem to split into bf16 planes:

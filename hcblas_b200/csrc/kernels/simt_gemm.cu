@@ -160,13 +160,36 @@ template <typename T, int VW> struct alignas(16) Vec {
 
 /* ---------------------------------------------------------------- kernel -- */
 
+/* One output tile's problem: op(A) is m x k, op(B) is k x n, C m x n, all
+ * column-major with their leading dimensions (pointers already offset). */
+template <typename T> struct TileJob {
+  int64_t m, n, k;
+  const T *A;
+  int64_t lda;
+  const T *B;
+  int64_t ldb;
+  T *C;
+  int64_t ldc;
+};
+
+/* the double-buffered K-slabs of both operands, as [k][mn] */
+template <typename Acc, int BM, int BN, int BK> struct SimtSmem {
+  static constexpr int PAD = 16 / (int)sizeof(Acc);
+  Acc As[2][BK][BM + PAD];
+  Acc Bs[2][BK][BN + PAD];
+};
+
 /*
+ * One BM x BN tile of C = alpha op(A) op(B) + beta C at (m0, n0), computed by
+ * the whole block.
  * OP_A / OP_B: 0 = N, 1 = T, 2 = C (column-major canonical).
  *   op(A) MN-contiguous iff OP_A == N;  op(B) K-contiguous iff OP_B == N.
  */
 template <typename T, int BM, int BN, int BK, int TM, int TN, int OP_A, int OP_B>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
-simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
+__device__ __forceinline__ void simt_tile(const TileJob<T> &p, typename AccOf<T>::type alpha,
+                                          typename AccOf<T>::type beta, bool rd, int64_t m0,
+                                          int64_t n0,
+                                          SimtSmem<typename AccOf<T>::type, BM, BN, BK> &sm) {
   using Acc = typename AccOf<T>::type;
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int VW = 16 / (int)sizeof(T);              /* storage elems / 16 B */
@@ -174,9 +197,6 @@ simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
   constexpr int GB = (TN * (int)sizeof(Acc)) / 16;
   constexpr int GSA = TM / GA;                           /* elems per group */
   constexpr int GSB = TN / GB;
-  constexpr int PAD = 16 / (int)sizeof(Acc);
-  constexpr int LDA_S = BM + PAD;
-  constexpr int LDB_S = BN + PAD;
   constexpr bool A_MN = (OP_A == HCBK_OP_N);
   constexpr bool B_MN = (OP_B != HCBK_OP_N);
   constexpr bool CJ_A = (OP_A == HCBK_OP_C);
@@ -188,13 +208,183 @@ simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
   static_assert(VB * VW * NT == BN * BK, "B slab must split evenly");
   static_assert(GA >= 1 && GB >= 1 && GSA * GA == TM && GSB * GB == TN, "fragment groups");
   static_assert(BK % VW == 0 || (A_MN && B_MN), "K-contiguous loads need BK % VW == 0");
-
-  __shared__ __align__(16) Acc As[2][BK][LDA_S];
-  __shared__ __align__(16) Acc Bs[2][BK][LDB_S];
+  auto &As = sm.As;
+  auto &Bs = sm.Bs;
 
   const int tid = threadIdx.x;
   const int tx = tid % (BM / TM);
   const int ty = tid / (BM / TM);
+  const T *A = p.A;
+  const T *B = p.B;
+
+  const bool vec_a = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
+                     (((p.lda * (int64_t)sizeof(T)) & 15) == 0);
+  const bool vec_b = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) &&
+                     (((p.ldb * (int64_t)sizeof(T)) & 15) == 0);
+
+  Vec<T, VW> ra[VA];
+  Vec<T, VW> rb[VB];
+
+  /* fetch the K-slab starting at k0 into registers (zero-filled) */
+  auto fetch = [&](int64_t k0) {
+#pragma unroll
+    for (int v = 0; v < VA; ++v) {
+      const int idx = tid + v * NT;
+      int64_t mn, kk;
+      if (A_MN) {
+        mn = m0 + (int64_t)(idx % (BM / VW)) * VW;
+        kk = k0 + idx / (BM / VW);
+      } else {
+        mn = m0 + idx / (BK / VW);
+        kk = k0 + (int64_t)(idx % (BK / VW)) * VW;
+      }
+      if (A_MN) {
+        const T *src = A + mn + kk * p.lda;
+        if (kk < p.k && mn + VW <= p.m && vec_a) {
+          ra[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            ra[v].v[e] = (kk < p.k && mn + e < p.m) ? src[e] : T();
+        }
+      } else {
+        const T *src = A + kk + mn * p.lda;
+        if (mn < p.m && kk + VW <= p.k && vec_a) {
+          ra[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            ra[v].v[e] = (mn < p.m && kk + e < p.k) ? src[e] : T();
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < VB; ++v) {
+      const int idx = tid + v * NT;
+      int64_t mn, kk;
+      if (B_MN) {
+        mn = n0 + (int64_t)(idx % (BN / VW)) * VW;
+        kk = k0 + idx / (BN / VW);
+      } else {
+        mn = n0 + idx / (BK / VW);
+        kk = k0 + (int64_t)(idx % (BK / VW)) * VW;
+      }
+      if (B_MN) {
+        const T *src = B + mn + kk * p.ldb;
+        if (kk < p.k && mn + VW <= p.n && vec_b) {
+          rb[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            rb[v].v[e] = (kk < p.k && mn + e < p.n) ? src[e] : T();
+        }
+      } else {
+        const T *src = B + kk + mn * p.ldb;
+        if (mn < p.n && kk + VW <= p.k && vec_b) {
+          rb[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            rb[v].v[e] = (mn < p.n && kk + e < p.k) ? src[e] : T();
+        }
+      }
+    }
+  };
+
+  /* registers -> shared buffer s, as [k][mn] in the compute type */
+  auto stash = [&](int s) {
+#pragma unroll
+    for (int v = 0; v < VA; ++v) {
+      const int idx = tid + v * NT;
+      if (A_MN) {
+        const int mn = (idx % (BM / VW)) * VW;
+        const int kk = idx / (BM / VW);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) As[s][kk][mn + e] = to_acc(ra[v].v[e], CJ_A);
+      } else {
+        const int mn = idx / (BK / VW);
+        const int kk = (idx % (BK / VW)) * VW;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) As[s][kk + e][mn] = to_acc(ra[v].v[e], CJ_A);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < VB; ++v) {
+      const int idx = tid + v * NT;
+      if (B_MN) {
+        const int mn = (idx % (BN / VW)) * VW;
+        const int kk = idx / (BN / VW);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) Bs[s][kk][mn + e] = to_acc(rb[v].v[e], CJ_B);
+      } else {
+        const int mn = idx / (BK / VW);
+        const int kk = (idx % (BK / VW)) * VW;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) Bs[s][kk + e][mn] = to_acc(rb[v].v[e], CJ_B);
+      }
+    }
+  };
+
+  Acc acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = zero_of<Acc>();
+
+  const int64_t ktiles = (p.k + BK - 1) / BK;
+  fetch(0);
+  stash(0);
+  __syncthreads();
+
+  for (int64_t kt = 0; kt < ktiles; ++kt) {
+    const int s = (int)(kt & 1);
+    if (kt + 1 < ktiles) fetch((kt + 1) * BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      Acc af[TM], bf[TN];
+#pragma unroll
+      for (int g = 0; g < GA; ++g) {
+        const Acc *src = &As[s][kk][g * (BM / GA) + tx * GSA];
+#pragma unroll
+        for (int e = 0; e < GSA; ++e) af[g * GSA + e] = src[e];
+      }
+#pragma unroll
+      for (int g = 0; g < GB; ++g) {
+        const Acc *src = &Bs[s][kk][g * (BN / GB) + ty * GSB];
+#pragma unroll
+        for (int e = 0; e < GSB; ++e) bf[g * GSB + e] = src[e];
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) mac(acc[i][j], af[i], bf[j]);
+    }
+    if (kt + 1 < ktiles) stash(s ^ 1);
+    __syncthreads();
+  }
+
+  /* ---- epilogue: C = alpha * acc + beta * C ---- */
+#pragma unroll
+  for (int j = 0; j < TN; ++j) {
+    const int64_t col = n0 + (j / GSB) * (BN / GB) + ty * GSB + (j % GSB);
+    if (col >= p.n) continue;
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int64_t row = m0 + (i / GSA) * (BM / GA) + tx * GSA + (i % GSA);
+      if (row < p.m) {
+        T *dst = p.C + row + col * p.ldc;
+        Acc cv = rd ? c_load(dst) : zero_of<Acc>();
+        c_store(dst, axpby(alpha, acc[i][j], beta, cv, rd));
+      }
+    }
+  }
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN, int OP_A, int OP_B>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
+  using Acc = typename AccOf<T>::type;
+  __shared__ __align__(16) SimtSmem<Acc, BM, BN, BK> sm;
 
   /* ---- tile rasterisation (bands of 8 M-tiles) ---- */
   const int64_t tiles_m = (p.m + BM - 1) / BM;
@@ -212,173 +402,82 @@ simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
   const int64_t n0 = tile_n * BN;
 
   for (int64_t bidx = blockIdx.y; bidx < p.batch; bidx += gridDim.y) {
-    const T *A = (p.a_arr ? p.a_arr[bidx] : p.a) + p.a_off + bidx * p.sa;
-    const T *B = (p.b_arr ? p.b_arr[bidx] : p.b) + p.b_off + bidx * p.sb;
-    T *C = (p.c_arr ? p.c_arr[bidx] : p.c) + p.c_off + bidx * p.sc;
-
-    const bool vec_a = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
-                       (((p.lda * (int64_t)sizeof(T)) & 15) == 0);
-    const bool vec_b = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) &&
-                       (((p.ldb * (int64_t)sizeof(T)) & 15) == 0);
-
-    Vec<T, VW> ra[VA];
-    Vec<T, VW> rb[VB];
-
-    /* fetch the K-slab starting at k0 into registers (zero-filled) */
-    auto fetch = [&](int64_t k0) {
-#pragma unroll
-      for (int v = 0; v < VA; ++v) {
-        const int idx = tid + v * NT;
-        int64_t mn, kk;
-        if (A_MN) {
-          mn = m0 + (int64_t)(idx % (BM / VW)) * VW;
-          kk = k0 + idx / (BM / VW);
-        } else {
-          mn = m0 + idx / (BK / VW);
-          kk = k0 + (int64_t)(idx % (BK / VW)) * VW;
-        }
-        if (A_MN) {
-          const T *src = A + mn + kk * p.lda;
-          if (kk < p.k && mn + VW <= p.m && vec_a) {
-            ra[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
-          } else {
-#pragma unroll
-            for (int e = 0; e < VW; ++e)
-              ra[v].v[e] = (kk < p.k && mn + e < p.m) ? src[e] : T();
-          }
-        } else {
-          const T *src = A + kk + mn * p.lda;
-          if (mn < p.m && kk + VW <= p.k && vec_a) {
-            ra[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
-          } else {
-#pragma unroll
-            for (int e = 0; e < VW; ++e)
-              ra[v].v[e] = (mn < p.m && kk + e < p.k) ? src[e] : T();
-          }
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < VB; ++v) {
-        const int idx = tid + v * NT;
-        int64_t mn, kk;
-        if (B_MN) {
-          mn = n0 + (int64_t)(idx % (BN / VW)) * VW;
-          kk = k0 + idx / (BN / VW);
-        } else {
-          mn = n0 + idx / (BK / VW);
-          kk = k0 + (int64_t)(idx % (BK / VW)) * VW;
-        }
-        if (B_MN) {
-          const T *src = B + mn + kk * p.ldb;
-          if (kk < p.k && mn + VW <= p.n && vec_b) {
-            rb[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
-          } else {
-#pragma unroll
-            for (int e = 0; e < VW; ++e)
-              rb[v].v[e] = (kk < p.k && mn + e < p.n) ? src[e] : T();
-          }
-        } else {
-          const T *src = B + kk + mn * p.ldb;
-          if (mn < p.n && kk + VW <= p.k && vec_b) {
-            rb[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
-          } else {
-#pragma unroll
-            for (int e = 0; e < VW; ++e)
-              rb[v].v[e] = (mn < p.n && kk + e < p.k) ? src[e] : T();
-          }
-        }
-      }
-    };
-
-    /* registers -> shared buffer s, as [k][mn] in the compute type */
-    auto stash = [&](int s) {
-#pragma unroll
-      for (int v = 0; v < VA; ++v) {
-        const int idx = tid + v * NT;
-        if (A_MN) {
-          const int mn = (idx % (BM / VW)) * VW;
-          const int kk = idx / (BM / VW);
-#pragma unroll
-          for (int e = 0; e < VW; ++e) As[s][kk][mn + e] = to_acc(ra[v].v[e], CJ_A);
-        } else {
-          const int mn = idx / (BK / VW);
-          const int kk = (idx % (BK / VW)) * VW;
-#pragma unroll
-          for (int e = 0; e < VW; ++e) As[s][kk + e][mn] = to_acc(ra[v].v[e], CJ_A);
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < VB; ++v) {
-        const int idx = tid + v * NT;
-        if (B_MN) {
-          const int mn = (idx % (BN / VW)) * VW;
-          const int kk = idx / (BN / VW);
-#pragma unroll
-          for (int e = 0; e < VW; ++e) Bs[s][kk][mn + e] = to_acc(rb[v].v[e], CJ_B);
-        } else {
-          const int mn = idx / (BK / VW);
-          const int kk = (idx % (BK / VW)) * VW;
-#pragma unroll
-          for (int e = 0; e < VW; ++e) Bs[s][kk + e][mn] = to_acc(rb[v].v[e], CJ_B);
-        }
-      }
-    };
-
-    Acc acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TN; ++j) acc[i][j] = zero_of<Acc>();
-
-    const int64_t ktiles = (p.k + BK - 1) / BK;
-    fetch(0);
-    stash(0);
-    __syncthreads();
-
-    for (int64_t kt = 0; kt < ktiles; ++kt) {
-      const int s = (int)(kt & 1);
-      if (kt + 1 < ktiles) fetch((kt + 1) * BK);
-#pragma unroll
-      for (int kk = 0; kk < BK; ++kk) {
-        Acc af[TM], bf[TN];
-#pragma unroll
-        for (int g = 0; g < GA; ++g) {
-          const Acc *src = &As[s][kk][g * (BM / GA) + tx * GSA];
-#pragma unroll
-          for (int e = 0; e < GSA; ++e) af[g * GSA + e] = src[e];
-        }
-#pragma unroll
-        for (int g = 0; g < GB; ++g) {
-          const Acc *src = &Bs[s][kk][g * (BN / GB) + ty * GSB];
-#pragma unroll
-          for (int e = 0; e < GSB; ++e) bf[g * GSB + e] = src[e];
-        }
-#pragma unroll
-        for (int i = 0; i < TM; ++i)
-#pragma unroll
-          for (int j = 0; j < TN; ++j) mac(acc[i][j], af[i], bf[j]);
-      }
-      if (kt + 1 < ktiles) stash(s ^ 1);
-      __syncthreads();
-    }
-
-    /* ---- epilogue: C = alpha * acc + beta * C ---- */
-    const bool rd = p.beta_nonzero != 0;
-#pragma unroll
-    for (int j = 0; j < TN; ++j) {
-      const int64_t col = n0 + (j / GSB) * (BN / GB) + ty * GSB + (j % GSB);
-      if (col >= p.n) continue;
-#pragma unroll
-      for (int i = 0; i < TM; ++i) {
-        const int64_t row = m0 + (i / GSA) * (BM / GA) + tx * GSA + (i % GSA);
-        if (row < p.m) {
-          T *dst = C + row + col * p.ldc;
-          Acc cv = rd ? c_load(dst) : zero_of<Acc>();
-          c_store(dst, axpby(p.alpha, acc[i][j], p.beta, cv, rd));
-        }
-      }
-    }
+    TileJob<T> j;
+    j.m = p.m;
+    j.n = p.n;
+    j.k = p.k;
+    j.A = (p.a_arr ? p.a_arr[bidx] : p.a) + p.a_off + bidx * p.sa;
+    j.B = (p.b_arr ? p.b_arr[bidx] : p.b) + p.b_off + bidx * p.sb;
+    j.C = (p.c_arr ? p.c_arr[bidx] : p.c) + p.c_off + bidx * p.sc;
+    j.lda = p.lda;
+    j.ldb = p.ldb;
+    j.ldc = p.ldc;
+    simt_tile<T, BM, BN, BK, TM, TN, OP_A, OP_B>(j, p.alpha, p.beta, p.beta_nonzero != 0, m0, n0,
+                                                 sm);
     if (p.batch > 1) __syncthreads(); /* shared buffers are reused by the next batch entry */
+  }
+}
+
+/*
+ * Persistent grouped GEMM on the CUDA cores: one launch walks the tiles of
+ * every problem of a device-side problem table (each its own shape,
+ * transposes, leading dimensions and pointers).  Global tile t belongs to the
+ * last problem g with tile_start[g] <= t (binary search over the prefix sums
+ * of the problems' tile counts); tiles are column-major within a problem.
+ * The op(A) x op(B) combination of each problem selects the tile body, so
+ * the per-combination code is the same as the single-problem kernel's.
+ */
+__device__ __forceinline__ int simt_find_problem(const int32_t *ts, int count, int t) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(ts + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+simt_grouped_kernel(const hcbk_simt_entry *table, const int32_t *tile_start, int count,
+                    int total_tiles, typename AccOf<T>::type alpha,
+                    typename AccOf<T>::type beta, int beta_nonzero) {
+  using Acc = typename AccOf<T>::type;
+  __shared__ __align__(16) SimtSmem<Acc, BM, BN, BK> sm;
+  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    const int g = simt_find_problem(tile_start, count, t);
+    const hcbk_simt_entry *e = table + g;
+    const int lt = t - __ldg(tile_start + g);
+    const int tiles_m = __ldg(&e->tiles_m);
+    const int64_t m0 = (int64_t)(lt % tiles_m) * BM, n0 = (int64_t)(lt / tiles_m) * BN;
+    TileJob<T> j;
+    j.m = __ldg(&e->m);
+    j.n = __ldg(&e->n);
+    j.k = __ldg(&e->k);
+    j.A = static_cast<const T *>(e->a);
+    j.B = static_cast<const T *>(e->b);
+    j.C = static_cast<T *>(e->c);
+    j.lda = __ldg(&e->lda);
+    j.ldb = __ldg(&e->ldb);
+    j.ldc = __ldg(&e->ldc);
+    const bool rd = beta_nonzero != 0;
+    switch (__ldg(&e->op_a) * 3 + __ldg(&e->op_b)) {
+#define HCBK_GT(OA, OB)                                                                    \
+  case OA * 3 + OB:                                                                        \
+    simt_tile<T, BM, BN, BK, TM, TN, OA, OB>(j, alpha, beta, rd, m0, n0, sm);              \
+    break;
+      HCBK_GT(0, 0) HCBK_GT(0, 1) HCBK_GT(1, 0) HCBK_GT(1, 1)
+      default:
+        if constexpr (IsComplex<T>::value) {
+          switch (__ldg(&e->op_a) * 3 + __ldg(&e->op_b)) {
+            HCBK_GT(0, 2) HCBK_GT(2, 0) HCBK_GT(2, 2) HCBK_GT(1, 2) HCBK_GT(2, 1)
+            default: break;
+          }
+        }
+        break;
+#undef HCBK_GT
+    }
+    __syncthreads(); /* the shared buffers are reused by the next tile */
   }
 }
 
@@ -419,10 +518,50 @@ int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
   return HCBK_ERR_ARGS;
 }
 
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+int launch_grouped(const hcbk_simt_grouped_args *g, cudaStream_t st) {
+  using Acc = typename AccOf<T>::type;
+  auto kern = simt_grouped_kernel<T, BM, BN, BK, TM, TN>;
+  constexpr int threads = (BM / TM) * (BN / TN);
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return HCBK_ERR_LAUNCH;
+  }
+  int64_t grid = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+  if (grid > g->total_tiles) grid = g->total_tiles;
+  kern<<<(unsigned)grid, threads, 0, st>>>(
+      g->table, g->tile_start, g->count, g->total_tiles,
+      HostScalar<Acc>::make(g->alpha_re, g->alpha_im), HostScalar<Acc>::make(g->beta_re, g->beta_im),
+      (g->beta_re != 0.0 || g->beta_im != 0.0) ? 1 : 0);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
 }  // namespace
 }  // namespace hcbk
 
 using namespace hcbk;
+
+extern "C" int hcbk_simt_grouped_tile(int dtype, int *bm, int *bn) {
+  if (dtype < HCBK_S || dtype > HCBK_Z) return HCBK_ERR_ARGS;
+  *bm = 64;
+  *bn = 64;
+  return HCBK_OK;
+}
+
+extern "C" int hcbk_gemm_simt_grouped(const hcbk_simt_grouped_args *g, void *stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (g->count <= 0 || g->total_tiles <= 0) return HCBK_ERR_ARGS;
+  switch (g->dtype) {
+    case HCBK_S: return launch_grouped<float, 64, 64, 16, 4, 4>(g, st);
+    case HCBK_D: return launch_grouped<double, 64, 64, 8, 4, 4>(g, st);
+    case HCBK_C: return launch_grouped<float2, 64, 64, 8, 4, 4>(g, st);
+    case HCBK_Z: return launch_grouped<double2, 64, 64, 8, 4, 4>(g, st);
+    default: return HCBK_ERR_ARGS; /* f16 problems take the tensor-core grouped kernel */
+  }
+}
 
 extern "C" int hcbk_gemm_simt(const hcbk_gemm_args *a, hcbk_simt_cfg cfg, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -325,6 +325,26 @@ hcblasStatus_t hcblasSgemmGrouped(hcblasHandle_t handle, int count,
                                   const hcblasGemmProblem *problems, const float *alpha,
                                   const float *beta);
 
+/* Extension (no counterpart in the reference; the reference's batched
+ * D/C/Z entry points lib/src/hcblas.cpp:1600-1675 take uniform problems):
+ * grouped GEMM for FP64, complex FP32 and complex FP64 problems (the same
+ * hcblasGemmProblem array; device matrices of the call's type; complex
+ * problems honour HCBLAS_OP_C as the conjugate transpose), computed in the
+ * type's own arithmetic by one persistent CUDA-core kernel that walks every
+ * problem's 64 x 64 tiles from a device-side problem table (problems ordered
+ * by decreasing work).  Any alignment and leading dimension.  An identical
+ * follow-up call (same problem array contents) reuses the uploaded table.
+ * Status rules as hcblasHgemmGrouped. */
+hcblasStatus_t hcblasDgemmGrouped(hcblasHandle_t handle, int count,
+                                  const hcblasGemmProblem *problems, const double *alpha,
+                                  const double *beta);
+hcblasStatus_t hcblasCgemmGrouped(hcblasHandle_t handle, int count,
+                                  const hcblasGemmProblem *problems, const hcComplex *alpha,
+                                  const hcComplex *beta);
+hcblasStatus_t hcblasZgemmGrouped(hcblasHandle_t handle, int count,
+                                  const hcblasGemmProblem *problems,
+                                  const hcDoubleComplex *alpha, const hcDoubleComplex *beta);
+
 /* ------------------------------------------------ class-API C shims -- */
 
 /* C-ABI forms of the Hcblaslibrary::hcblas_Xgemm methods (include/hcblaslib.h;

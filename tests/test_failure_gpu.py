@@ -73,12 +73,12 @@ def test_pipeline_wait_timeout_is_reported_and_handle_recovers(fresh_handle):
     finally:
         assert hb.set_tuning(h, "wait_timeout_us", 0) == 0
     # the injection is disarmed after one call; the handle keeps working
-    for M2, N2, K2 in [(M, N, K), (300, 200, 500)]:
+    for M2, N2, K2 in [(M, N, K), (320, 200, 504)]:  # leading dimensions TMA can address
         A2, B2 = hgemm_case(rng, M2, N2, K2)
         rc, dC = run_hgemm(h, A2, B2, M2, N2, K2, np.zeros(M2 * N2, np.float16))
         assert rc == 0
         assert hb.device_error(h) == 0
-        assert hb.hcblasGetLastPath(h).startswith("tc.h.")
+        assert hb.hcblasGetLastPath(h).startswith("tc.h."), hb.hcblasGetLastPath(h)
         _, ref = O.gemm(O.COL, 0, 0, M2, N2, K2, 1.0, A2, M2, B2, K2, 0.0,
                         np.zeros(M2 * N2, np.float16), M2)
         got = O.view_c(dC.download().astype(np.float64), O.COL, M2, N2, M2)
@@ -180,7 +180,8 @@ def test_workspace_follows_stream_switches(fresh_handle):
         assert hb.hcblasSetStream(h, 0) == 0
         assert hb.device_error(h) == 0
         for A, B, dC, n in outs:
-            _, ref = O.gemm(O.COL, 0, 1, n, n, n, 1.0, A, n, B, n, 0.0, np.zeros(n * n), n)
+            _, ref = O.gemm(O.COL, 0, 1, n, n, n, 1.0, A, n, B, n, 0.0,
+                            np.zeros(n * n, np.float32), n)
             assert O.normwise_rel_error(O.view_c(dC.download(), O.COL, n, n, n), ref) < 1e-6
     finally:
         hb.hcblasSetStream(h, 0)
