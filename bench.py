@@ -714,6 +714,10 @@ def summarize(line):
                           "split6_err": pick(s3, "split_bf16x6", "normwise_err"),
                           "speedup": s3.get("speedup_x6_vs_plain"),
                           "target": ">= 3x plain at error <= plain"}
+    c4a = sec.get("hgemm_ptr_batch_512x128^3")
+    if c4a:
+        out["batch_f16_ptr_512x128"] = {"ms": c4a.get("ms"), "tflops": c4a.get("tflops"),
+                                        "speedup_vs_per_problem": c4a.get("speedup_vs_per_problem")}
     for key, short in (("hgemm_grouped_4096_uneven", "grouped_f16"),
                        ("sgemm_grouped_4096_uneven_split_bf16x6", "grouped_f32_split")):
         gq = sec.get(key)
@@ -881,7 +885,66 @@ def run_secondary_small(hb, h, stream, torch, O, timed):
     out["hgemm_strided_batch_512x128^3"] = {"path": hb.hcblasGetLastPath(h),
                                             "tflops": round(2 * b * n ** 3 / ms / 1e9, 2),
                                             "ms": round(ms, 4)}
-    del dA, dB, dC
+    # the same batch through the pointer-array entry point (device-resident
+    # arrays, table built on the GPU) and as 512 single calls
+    L = hb.lib()
+    ptrs = lambda base, esz: hb.DeviceArray(h, np.array(
+        [base.ptr + i * n * n * esz for i in range(b)], dtype=np.uint64))
+    pA, pB, pC = ptrs(dA, 2), ptrs(dB, 2), ptrs(dC, 2)
+    fp = lambda: hb.gemm_batched(h, 0, 0, n, n, n, 1.0, pA.ptr, n, pB.ptr, n, 0.0, pC.ptr, n, b,
+                                 np.float16)
+    ms_p = timed(fp)
+    one16 = hb.scalar_bytes(np.float16, 1.0)
+    zero16 = hb.scalar_bytes(np.float16, 0.0)
+
+    def singles16():
+        for i in range(b):
+            L.hcblasHgemm(h, 0, 0, n, n, n, one16.ctypes.data, dA.ptr + 2 * i * n * n, n,
+                          dB.ptr + 2 * i * n * n, n, zero16.ctypes.data, dC.ptr + 2 * i * n * n, n)
+    ms_s = timed(singles16)
+    out["hgemm_ptr_batch_512x128^3"] = {"path": "tc.h.grouped.ptr" if fp() == 0 else "failed",
+                                        "tflops": round(2 * b * n ** 3 / ms_p / 1e9, 2),
+                                        "ms": round(ms_p, 4), "per_problem_calls_ms": round(ms_s, 4),
+                                        "speedup_vs_per_problem": round(ms_s / ms_p, 2)}
+    del dA, dB, dC, pA, pB, pC
+    # SGEMM batch 512 x 128^3 (f32, U[-1,1)) on the split-BF16 grouped path
+    # (6 products), strided and pointer-array, against plain FP32 (one SIMT
+    # launch for the batch, and per-problem calls)
+    A32 = rng.uniform(-1, 1, n * n * b).astype(np.float32)
+    B32 = rng.uniform(-1, 1, n * n * b).astype(np.float32)
+    dA, dB = hb.DeviceArray(h, A32), hb.DeviceArray(h, B32)
+    dC = hb.DeviceArray(h, nbytes=4 * n * n * b, dtype=np.float32)
+    pA, pB, pC = ptrs(dA, 4), ptrs(dB, 4), ptrs(dC, 4)
+    fs = lambda: hb.gemm_strided_batched(h, 0, 0, n, n, n, 1.0, dA, n, n * n, dB, n, n * n, 0.0,
+                                         dC, n, n * n, b)
+    fsp = lambda: hb.gemm_batched(h, 0, 0, n, n, n, 1.0, pA.ptr, n, pB.ptr, n, 0.0, pC.ptr, n, b,
+                                  np.float32)
+    one32, zero32 = np.array([1.0], np.float32), np.array([0.0], np.float32)
+
+    def singles32():
+        for i in range(b):
+            L.hcblasSgemm(h, 0, 0, n, n, n, one32.ctypes.data, dA.ptr + 4 * i * n * n, n,
+                          dB.ptr + 4 * i * n * n, n, zero32.ctypes.data, dC.ptr + 4 * i * n * n, n)
+    hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
+    ms_plain = timed(fs)
+    path_plain = hb.hcblasGetLastPath(h)
+    ms_plain_single = timed(singles32)
+    hb.hcblasSetMathMode(h, MATH_SPLIT, 6)
+    ms_split = timed(fs)
+    path_split = hb.hcblasGetLastPath(h)
+    ms_split_p = timed(fsp)
+    path_split_p = hb.hcblasGetLastPath(h)
+    hb.hcblasSetMathMode(h, MATH_NATIVE, 0)
+    out["sgemm_batch_512x128^3"] = {
+        "plain_strided": {"path": path_plain, "ms": round(ms_plain, 4),
+                          "tflops": round(2 * b * n ** 3 / ms_plain / 1e9, 2)},
+        "plain_per_problem_calls_ms": round(ms_plain_single, 4),
+        "split_bf16x6_strided": {"path": path_split, "ms": round(ms_split, 4),
+                                 "tflops": round(2 * b * n ** 3 / ms_split / 1e9, 2)},
+        "split_bf16x6_ptr_array": {"path": path_split_p, "ms": round(ms_split_p, 4),
+                                   "tflops": round(2 * b * n ** 3 / ms_split_p / 1e9, 2)},
+        "speedup_split_strided_vs_per_problem_plain": round(ms_plain_single / ms_split, 2)}
+    del dA, dB, dC, pA, pB, pC
     # C4b: grouped 4096 problems, M, N, K log-uniform in [16, 1024], seed 3, mixed N/T
     import bench_cases as profile_cases
     call, keep = profile_cases.CASES["hgemm_grouped_4096"](h)

@@ -815,6 +815,116 @@ int hgemm_strided_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *st
   return rc;
 }
 
+/* Pointer-array HGEMM batch on the grouped tensor-core kernel: a kernel
+ * builds the problem table on the device (the template entry's tensor maps
+ * with their global addresses replaced from the device-resident pointer
+ * arrays), the grouped kernel walks every problem's tiles, and a CUDA-core
+ * pass computes the entries whose A or B TMA cannot address (flagged by the
+ * builder; that pass launches whether or not any is flagged, since the host
+ * cannot see the flags without waiting). */
+int hgemm_ptr_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *stream,
+                      const char **path) {
+  if (!a->a_array || a->batch < 1 || a->batch > (1 << 24) || a->m > 0x7fffffff ||
+      a->n > 0x7fffffff || a->k > 0x7fffffff || a->op_a == HCBK_OP_C || a->op_b == HCBK_OP_C)
+    return HCBK_ERR_ARGS;
+  if ((a->lda & 7) || (a->ldb & 7)) return HCBK_ERR_ALIGN; /* TMA strides: 16 bytes */
+  HcblasGroupedPlan &gp = st->grouped_ptr;
+  const int count = (int)a->batch;
+  const size_t ent_bytes = sizeof(hcbk_grouped_entry) * (size_t)count;
+  const size_t ts_off = (ent_bytes + 255) & ~size_t(255);
+  const size_t skip_off = (ts_off + sizeof(int32_t) * ((size_t)count + 1) + 255) & ~size_t(255);
+  const size_t bytes = skip_off + sizeof(int32_t) * (size_t)count;
+  if (!grouped_ensure_table(gp, bytes, stream)) return HCBK_ERR_NOMEM;
+  char *tb = static_cast<char *>(gp.table);
+  /* the template: this batch's shape and strides, with the table itself as
+   * a stand-in base address (replaced for every entry on the device) */
+  hcbk_grouped_entry tmpl;
+  int rc = hcbk_grouped_encode(&tmpl, a->op_a, a->op_b, a->m, a->n, a->k, tb, a->lda, tb,
+                               a->ldb, tb, a->ldc);
+  if (rc) return rc;
+  int *err = device_error_flag(st);
+  if (!err) return HCBK_ERR_NOMEM;
+  auto *table = reinterpret_cast<hcbk_grouped_entry *>(tb);
+  auto *ts = reinterpret_cast<int32_t *>(tb + ts_off);
+  auto *skip = reinterpret_cast<int32_t *>(tb + skip_off);
+  rc = timed_launch(st, stream, "tc.h.grouped.table", [&] {
+    return hcbk_grouped_ptr_table(&tmpl, table, ts, skip, a->a_array, a->b_array, a->c_array,
+                                  a->a_off * 2, a->b_off * 2, a->c_off * 2, a->stride_a * 2,
+                                  a->stride_b * 2, a->stride_c * 2, count, stream);
+  });
+  if (rc) return rc;
+  hcbk_grouped_args g;
+  g.table = table;
+  g.tile_start = ts;
+  g.count = count;
+  g.total_tiles = hcbk_grouped_tiles(&tmpl) * count;
+  g.alpha = (float)a->alpha_re;
+  g.beta = (float)a->beta_re;
+  g.device_maps = 1;
+  if ((int64_t)hcbk_grouped_tiles(&tmpl) * count > 0x7fffffff) return HCBK_ERR_ARGS;
+  rc = timed_launch(st, stream, "tc.h.grouped.ptr",
+                    [&] { return hcbk_hgemm_grouped_tc(&g, err, stream); });
+  if (rc) return rc;
+  /* the entries the table builder flagged, on the CUDA cores */
+  hcbk_gemm_args f = *a;
+  f.batch_select = skip;
+  hcbk_simt_cfg cfg;
+  cfg.variant = 1;
+  rc = timed_launch(st, stream, "simt.h.flagged", [&] { return hcbk_gemm_simt(&f, cfg, stream); });
+  if (rc) return rc;
+  *path = "tc.h.grouped.ptr";
+  return HCBK_OK;
+}
+
+/* split-BF16 SGEMM batch (strided or pointer-array) on the grouped
+ * tensor-core path: one pack launch and one GEMM launch for the batch */
+int sgemm_split_batched(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *stream,
+                        const char **path) {
+  if (a->batch < 2 || a->batch > 0x7fffffff || a->m > 0x7fffffff || a->n > 0x7fffffff ||
+      a->k > 0x7fffffff || a->lda > 0x7fffffff || a->ldb > 0x7fffffff || a->ldc > 0x7fffffff)
+    return HCBK_ERR_ARGS;
+  std::vector<hcblasGemmProblem> probs((size_t)a->batch);
+  const bool ptr = a->a_array != nullptr;
+  const float *A = static_cast<const float *>(a->a) + a->a_off;
+  const float *B = static_cast<const float *>(a->b) + a->b_off;
+  float *C = static_cast<float *>(a->c) + a->c_off;
+  for (int64_t i = 0; i < a->batch; ++i) {
+    hcblasGemmProblem &p = probs[(size_t)i];
+    p.transa = a->op_a == HCBK_OP_N ? HCBLAS_OP_N : HCBLAS_OP_T;
+    p.transb = a->op_b == HCBK_OP_N ? HCBLAS_OP_N : HCBLAS_OP_T;
+    p.m = (int)a->m;
+    p.n = (int)a->n;
+    p.k = (int)a->k;
+    p.lda = (int)a->lda;
+    p.ldb = (int)a->ldb;
+    p.ldc = (int)a->ldc;
+    if (ptr) { /* placeholders: the device arrays supply the pointers */
+      p.A = p.B = p.C = reinterpret_cast<void *>(uintptr_t(256));
+    } else {
+      p.A = A + i * a->stride_a;
+      p.B = B + i * a->stride_b;
+      p.C = C + i * a->stride_c;
+    }
+  }
+  PtrBatch pb;
+  if (ptr) {
+    pb.a = a->a_array;
+    pb.b = a->b_array;
+    pb.c = a->c_array;
+    pb.a_off = a->a_off;
+    pb.b_off = a->b_off;
+    pb.c_off = a->c_off;
+    pb.sa = a->stride_a;
+    pb.sb = a->stride_b;
+    pb.sc = a->stride_c;
+  }
+  const int rc = grouped_sgemm_split(st, stream, ColMajor, (int)a->batch, probs.data(),
+                                     (float)a->alpha_re, (float)a->beta_re, terms,
+                                     ptr ? &pb : nullptr);
+  *path = st->last_path;
+  return rc;
+}
+
 /* Does the handle's math mode give this dtype an emulated path? */
 bool emulated_mode(const HcblasB200State *st, int dtype) {
   switch (st->math_mode) {
@@ -827,6 +937,18 @@ bool emulated_mode(const HcblasB200State *st, int dtype) {
 }
 
 int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+  if (a->dtype == HCBK_S && st->math_mode == 1 /* HCBLAS_MATH_SPLIT_BF16 */ && a->batch > 1) {
+    /* strided and pointer-array batches: the grouped split-BF16 kernel */
+    const int terms = plan_emulation(1, st->math_param, st->accuracy_bits, HCBK_S, a->k, nullptr);
+    int rc = sgemm_split_batched(st, a, terms, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] split-bf16 batch path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_H && a->a_array) {
+    int rc = hgemm_ptr_grouped(st, a, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] pointer-array hgemm grouped path declined (%d)\n", rc);
+  }
   if (a->batch > 1 && !a->a_array && emulated_mode(st, a->dtype)) {
     /* strided batch under an emulated math mode: one emulated call per
      * element, in order on the stream (they share the workspace) */

@@ -78,9 +78,26 @@ int grouped_simt(HcblasB200State *st, void *stream, int dtype, hcblasOrder order
                  const hcblasGemmProblem *probs, double alpha_re, double alpha_im,
                  double beta_re, double beta_im);
 
-/* Grouped FP32 GEMM on the split-BF16 tensor-core path (terms 3 or 6). */
+/* Device-resident pointer arrays of a uniform batch: matrix i of X is
+ * x[i] + x_off + i * x_stride (elements). */
+struct PtrBatch {
+  const void *const *a;
+  const void *const *b;
+  void *const *c;
+  int64_t a_off, b_off, c_off;
+  int64_t sa, sb, sc;
+};
+
+/* Grouped FP32 GEMM on the split-BF16 tensor-core path (terms 3 or 6).
+ * With `ptrs`, the problems' A, B, C pointers are placeholders and the
+ * operands come from the device-resident arrays (patched on the device). */
 int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, int count,
-                        const hcblasGemmProblem *probs, float alpha, float beta, int terms);
+                        const hcblasGemmProblem *probs, float alpha, float beta, int terms,
+                        const PtrBatch *ptrs = nullptr);
+
+/* Shared helpers of the grouped paths (grouped.cpp): a plan's device table
+ * of at least `bytes` (grown after the stream's queued work) */
+bool grouped_ensure_table(HcblasGroupedPlan &gp, size_t bytes, void *stream);
 
 }  // namespace hcblas_b200
 

@@ -105,6 +105,10 @@ bool ensure_staging(HcblasGroupedPlan &gp, size_t bytes) {
 
 }  // namespace
 
+bool grouped_ensure_table(HcblasGroupedPlan &gp, size_t bytes, void *stream) {
+  return ensure_table(gp, bytes, stream);
+}
+
 /* Build (or reuse) the plan and run every problem; HCBK_* code. */
 int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,
                   const hcblasGemmProblem *probs, float alpha, float beta) {
@@ -155,9 +159,9 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
       else if (rc == HCBK_ERR_ALIGN || rc == HCBK_ERR_ARGS) fallback.push_back(i);
       else return rc;
     }
-    auto work = [&](int i) {
+    auto work = [&](int i) { /* tensor work of a problem's padded tiles */
       const hcbk_grouped_entry &e = ent[i];
-      return (int64_t)e.tiles_m * ((e.n + 127) / 128) * ((e.k + 63) / 64);
+      return (int64_t)hcbk_grouped_tiles(&e) * e.bn * ((e.k + 63) / 64);
     };
     std::stable_sort(ok_idx.begin(), ok_idx.end(),
                      [&](int x, int y) { return work(x) > work(y); });
@@ -175,7 +179,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
         const hcbk_grouped_entry &e = ent[ok_idx[j]];
         std::memcpy(&dst[j], &e, sizeof(e));
         ts[j] = (int32_t)total;
-        total += (int64_t)e.tiles_m * ((e.n + 127) / 128);
+        total += (int64_t)hcbk_grouped_tiles(&e);
         if (total > 0x7fffffff) return HCBK_ERR_ARGS;
       }
       ts[nt] = (int32_t)total;
@@ -210,6 +214,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     g.total_tiles = gp.total_tiles;
     g.alpha = alpha;
     g.beta = beta;
+    g.device_maps = 0;
     int rc = timed_launch(st, stream, "tc.h.grouped",
                           [&] { return hcbk_hgemm_grouped_tc(&g, err, stream); });
     if (rc) return rc;
@@ -246,7 +251,8 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
  * table whose 3-D maps read it; each call packs the current operands (one
  * launch) and runs the grouped tensor-core kernel (one launch). */
 int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, int count,
-                        const hcblasGemmProblem *probs, float alpha, float beta, int terms) {
+                        const hcblasGemmProblem *probs, float alpha, float beta, int terms,
+                        const PtrBatch *ptrs) {
   if (alpha == 0.0f) { /* C_i := beta*C_i, A and B not referenced (CBLAS) */
     for (int i = 0; i < count; ++i) {
       const Canon c = canonical(probs[i], order);
@@ -414,7 +420,17 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;
   char *tb = static_cast<char *>(gp.table);
-  int rc = timed_launch(st, stream, "pack.split_bf16.grouped", [&] {
+  int rc = HCBK_OK;
+  if (ptrs) { /* the batch's operands and C from its device pointer arrays */
+    rc = timed_launch(st, stream, "pack.ptr_patch", [&] {
+      return hcbk_grouped_split_patch(reinterpret_cast<hcbk_gpack_job *>(tb + gp.pack_offset),
+                                      reinterpret_cast<hcbk_grouped_entry *>(tb), ptrs->a,
+                                      ptrs->b, ptrs->c, ptrs->a_off, ptrs->b_off, ptrs->c_off,
+                                      ptrs->sa, ptrs->sb, ptrs->sc, count, stream);
+    });
+    if (rc) return rc;
+  }
+  rc = timed_launch(st, stream, "pack.split_bf16.grouped", [&] {
     return hcbk_grouped_pack(reinterpret_cast<const hcbk_gpack_job *>(tb + gp.pack_offset),
                              reinterpret_cast<const int32_t *>(tb + gp.pack_ts_offset),
                              gp.pack_count, gp.pack_tiles, nplanes, stream);
@@ -427,6 +443,7 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
   g.total_tiles = gp.total_tiles;
   g.alpha = alpha;
   g.beta = beta;
+  g.device_maps = 0;
   const char *path = terms == 6 ? "tc.s.grouped_split_bf16x6" : "tc.s.grouped_split_bf16x3";
   rc = timed_launch(st, stream, path,
                     [&] { return hcbk_sgemm_grouped_split_tc(&g, terms, err, stream); });

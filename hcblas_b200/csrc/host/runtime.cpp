@@ -270,7 +270,8 @@ Hcblaslibrary::~Hcblaslibrary() {
     }
     cudaStreamSynchronize(static_cast<cudaStream_t>(currentAcclView.stream));
     hcblas_b200::clear_graph_cache(impl);
-    for (HcblasGroupedPlan *pp : {&impl->grouped, &impl->grouped_split, &impl->grouped_simt}) {
+    for (HcblasGroupedPlan *pp :
+         {&impl->grouped, &impl->grouped_split, &impl->grouped_simt, &impl->grouped_ptr}) {
       HcblasGroupedPlan &gp = *pp;
       if (gp.upload_done) {
         cudaEventSynchronize(static_cast<cudaEvent_t>(gp.upload_done));

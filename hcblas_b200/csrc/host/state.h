@@ -88,6 +88,7 @@ struct HcblasB200State {
   HcblasGroupedPlan grouped;
   HcblasGroupedPlan grouped_split; /* hcblasSgemmGrouped (split-BF16) */
   HcblasGroupedPlan grouped_simt;  /* hcblas{D,C,Z}gemmGrouped (CUDA cores) */
+  HcblasGroupedPlan grouped_ptr;   /* pointer-array HGEMM batches (device-built table) */
   /* CUDA-graph replay of repeated identical calls (off by default) */
   int graphs = 0;
   /* time candidate tile configurations per size bucket (off by default) */

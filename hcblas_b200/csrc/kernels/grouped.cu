@@ -39,9 +39,13 @@ using namespace hcbk::tc;
 constexpr int BM = 128, BN = 128, BK = 64; /* BK f16 = one 128-byte swizzle atom */
 constexpr int STAGES = 6;
 constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128;
-constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + 256 + 1024;
+constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES; /* stage slot sized for 128-wide tiles */
+constexpr uint32_t OUT_BOX = 32 * 32 * 2;           /* one f16 32 x 32 C box */
+constexpr uint32_t OUT_OFF = STAGES * STAGE_BYTES;  /* 4 epilogue warps x 2 boxes */
+constexpr uint32_t BAR_OFF = OUT_OFF + 8 * OUT_BOX;
+constexpr uint32_t SMEM_BYTES = BAR_OFF + 256 + 1024;
 constexpr uint32_t TMEM_COLS = 2 * BN;
+static_assert(SMEM_BYTES <= 232448, "shared memory");
 
 struct Params {
   const hcbk_grouped_entry *table;
@@ -50,6 +54,7 @@ struct Params {
   int total_tiles;
   float alpha, beta;
   int beta_nonzero;
+  int device_maps; /* the table's maps were patched on the device: acquire them */
   int *err;
 };
 
@@ -77,15 +82,26 @@ __device__ __forceinline__ TileRef tile_ref(const Params &p, int t) {
   return TileRef{e, lt % tiles_m, lt / tiles_m};
 }
 
+/*
+ * Per problem the tile is 128 x bn with bn = 64 or 128 (the entry's choice:
+ * the width that pads N least), so narrow problems do not spend tensor work
+ * on padding.  The epilogue stages each 32 x 32 block of C in shared memory
+ * and writes it with one TMA tensor store through the problem's C map (C
+ * read the same way when beta != 0); a C that TMA cannot address (base not
+ * 16-byte aligned, ldc not a multiple of 8) is written by plain stores.  An
+ * entry flagged `skip` (operands TMA cannot address, found by the
+ * device-side table builder) is passed over by every role alike.
+ */
 __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_constant__ Params p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + BAR_OFF);
   uint64_t *empty = full + STAGES;
   uint64_t *tfull = empty + STAGES;
   uint64_t *tempty = tfull + 2;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+  uint64_t *obar = tempty + 2; /* C loads: two per epilogue warp */
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(obar + 8);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -99,6 +115,7 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4);
     }
+    for (int b = 0; b < 8; ++b) mbar_init(&obar[b], 1);
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -118,17 +135,24 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       bool ok = true;
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
         const TileRef r = tile_ref(p, t);
+        if (__ldg(&r.e->skip)) continue;
         const CUtensorMap *ma = reinterpret_cast<const CUtensorMap *>(r.e->map_a);
         const CUtensorMap *mb = reinterpret_cast<const CUtensorMap *>(r.e->map_b);
+        if (p.device_maps) {
+          tensormap_acquire(ma);
+          tensormap_acquire(mb);
+        }
         const int k = __ldg(&r.e->k);
+        const int bn = __ldg(&r.e->bn);
         const int a_mn = __ldg(&r.e->a_mn), b_mn = __ldg(&r.e->b_mn);
         const int kblocks = (k + BK - 1) / BK;
+        const uint32_t bytes = A_BYTES + (uint32_t)bn * 128u;
         for (int kb = 0; kb < kblocks; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
             ok = false;
             break;
           }
-          mbar_expect_tx(&full[s], STAGE_BYTES);
+          mbar_expect_tx(&full[s], bytes);
           uint8_t *st = smem + s * STAGE_BYTES;
           const int k0 = kb * BK;
           if (!a_mn) {
@@ -139,10 +163,10 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
           }
           uint8_t *sb = st + A_BYTES;
           if (!b_mn) {
-            tma_load_2d(sb, mb, &full[s], k0, r.tn * BN);
+            tma_load_2d(sb, mb, &full[s], k0, r.tn * bn); /* box {64, bn} */
           } else {
-            tma_load_2d(sb, mb, &full[s], r.tn * BN, k0);
-            tma_load_2d(sb + BK * 128, mb, &full[s], r.tn * BN + 64, k0);
+            for (int j = 0; j < bn; j += 64)
+              tma_load_2d(sb + (j / 64) * (BK * 128), mb, &full[s], r.tn * bn + j, k0);
           }
           if (++s == STAGES) {
             s = 0;
@@ -156,18 +180,21 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
-      int ci = 0;
+      int ci = 0; /* tiles computed by this CTA: selects the TMEM buffer */
       bool ok = true;
-      for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x, ++ci) {
+      for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
         const TileRef r = tile_ref(p, t);
+        if (__ldg(&r.e->skip)) continue;
         const int k = __ldg(&r.e->k);
+        const int bn = __ldg(&r.e->bn);
         const bool a_mn = __ldg(&r.e->a_mn) != 0, b_mn = __ldg(&r.e->b_mn) != 0;
         const int kblocks = (k + BK - 1) / BK;
-        const uint32_t idesc = make_idesc(1, 0, a_mn, b_mn, BM, BN);
+        const uint32_t idesc = make_idesc(1, 0, a_mn, b_mn, BM, (uint32_t)bn);
         const uint32_t a_lbo = a_mn ? BK * 128 : 16, b_lbo = b_mn ? BK * 128 : 16;
         const uint32_t a_kstep = a_mn ? 16 * 128 : 32, b_kstep = b_mn ? 16 * 128 : 32;
         const int b = ci & 1;
         const uint32_t tph = (ci >> 1) & 1;
+        ++ci;
         if (!mbar_wait(&tempty[b], tph ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) break;
         tc_fence_after();
         const uint32_t dbase = tmem_base + b * BN;
@@ -197,39 +224,89 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
   } else {
     /* ------------------------------------------------ epilogue -- */
     const int q = warp & 3; /* TMEM lane quadrant */
+    __half *boxes = reinterpret_cast<__half *>(smem + OUT_OFF) + q * 2 * (32 * 32);
+    uint64_t *wbar = obar + 2 * q;
+    uint32_t lphase = 0; /* bit x: parity of box x's next C load */
+    uint32_t pend = 0;   /* bit x: a C load into box x did not complete in time */
     int ci = 0;
-    for (int t = blockIdx.x; t < p.total_tiles; t += gridDim.x, ++ci) {
+    for (int t = blockIdx.x; t < p.total_tiles; t += gridDim.x) {
       const TileRef r = tile_ref(p, t);
-      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n);
+      if (__ldg(&r.e->skip)) continue;
+      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n), bn = __ldg(&r.e->bn);
+      const bool c_tma = __ldg(&r.e->c_tma) != 0;
+      const CUtensorMap *mc = reinterpret_cast<const CUtensorMap *>(r.e->map_c);
       const long long ldc = __ldg(&r.e->ldc);
       __half *C = static_cast<__half *>(r.e->c);
       const int b = ci & 1;
       const uint32_t tph = (ci >> 1) & 1;
+      ++ci;
       if (!mbar_wait(&tfull[b], tph, p.err, ERR_TIMEOUT_EPILOGUE)) break;
       tc_fence_after();
-      const int m = r.tm * BM + q * 32 + lane;
-      const int n0 = r.tn * BN;
+      if (c_tma && p.device_maps && lane == 0) tensormap_acquire(mc);
+      const int m0 = r.tm * BM + q * 32;
+      const int m = m0 + lane;
+      const int n0 = r.tn * bn;
       const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + b * BN;
+      bool wait_ok = true;
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 32) {
+      for (int c = 0; c < bn; c += 32) {
         uint32_t v[32];
         tmem_ld_32x32b_x32(tbase + c, v);
-        tmem_ld_wait();
-        const int nvalid = pn - (n0 + c);
-        if (m < pm && nvalid > 0) {
-          __half *cp = C + (long long)m + (long long)(n0 + c) * ldc;
-          float cv[32];
+        if (c_tma) {
+          const int x = (c >> 5) & 1;
+          __half *box = boxes + x * (32 * 32); /* column-major 32 x 32, as C */
+          if (lane == 0) {
+            bulk_wait_read<1>(); /* the store issued from this box two groups ago has read it */
+            if (p.beta_nonzero) {
+              mbar_expect_tx(&wbar[x], OUT_BOX);
+              tma_load_2d(box, mc, &wbar[x], m0, n0 + c);
+            }
+          }
+          __syncwarp();
+          tmem_ld_wait();
           if (p.beta_nonzero) {
+            /* the C box has landed (out-of-range parts read as zeros) */
+            if (!__all_sync(0xffffffffu, mbar_wait(&wbar[x], (lphase >> x) & 1u, p.err,
+                                                   ERR_TIMEOUT_EPILOGUE))) {
+              pend |= 1u << x;
+              wait_ok = false;
+              break;
+            }
+            lphase ^= 1u << x;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const float cv = __half2float(box[j * 32 + lane]);
+              box[j * 32 + lane] = __float2half_rn(fmaf(p.beta, cv, p.alpha * __uint_as_float(v[j])));
+            }
+          } else {
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-              cv[j] = (j < nvalid) ? __half2float(cp[(long long)j * ldc]) : 0.f;
+              box[j * 32 + lane] = __float2half_rn(p.alpha * __uint_as_float(v[j]));
           }
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_2d(mc, box, m0, n0 + c); /* rows >= m, columns >= n are dropped */
+            bulk_commit();
+          }
+        } else {
+          tmem_ld_wait();
+          const int nvalid = pn - (n0 + c);
+          if (m < pm && nvalid > 0) {
+            __half *cp = C + (long long)m + (long long)(n0 + c) * ldc;
+            float cv[32];
+            if (p.beta_nonzero) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            if (j < nvalid) {
-              float o = p.alpha * __uint_as_float(v[j]);
-              if (p.beta_nonzero) o = fmaf(p.beta, cv[j], o);
-              cp[(long long)j * ldc] = __float2half_rn(o);
+              for (int j = 0; j < 32; ++j)
+                cv[j] = (j < nvalid) ? __half2float(cp[(long long)j * ldc]) : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              if (j < nvalid) {
+                float o = p.alpha * __uint_as_float(v[j]);
+                if (p.beta_nonzero) o = fmaf(p.beta, cv[j], o);
+                cp[(long long)j * ldc] = __float2half_rn(o);
+              }
             }
           }
         }
@@ -237,6 +314,16 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty[b]);
+      if (!wait_ok) break;
+    }
+    if (lane == 0) {
+      /* a C load still in flight (only after a failed wait): a bounded time
+       * to land before the CTA's shared memory is released */
+      for (int x = 0; x < 2; ++x)
+        if ((pend >> x) & 1u)
+          for (int it = 0; it < (1 << 22) && !mbar_try_wait(&wbar[x], (lphase >> x) & 1u); ++it) {
+          }
+      bulk_wait_all(); /* this warp's tensor stores have completed */
     }
   }
 
@@ -247,6 +334,58 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
     tc_fence_after();
     tmem_dealloc(tmem_base, TMEM_COLS);
   }
+}
+
+/* Device-side table of a pointer-array batch (uniform problems): entry i is
+ * the template with the global addresses of its A, B (and C) maps replaced
+ * by a_arr[i] + a_off + i * a_stride (likewise B, C; byte offsets); an entry
+ * whose A or B is not 16-byte aligned is flagged `skip` (the batch's
+ * CUDA-core pass computes it), and one whose C is not is written by plain
+ * stores.  tile_start[i] = i * tiles. */
+struct PtrTableArgs {
+  uint4 tmpl[sizeof(hcbk_grouped_entry) / 16]; /* the template entry's bytes */
+  int tmpl_c_tma;
+  hcbk_grouped_entry *table;
+  int32_t *tile_start;
+  int32_t *skip_out; /* per entry, for the CUDA-core pass (1 = compute there) */
+  const void *const *a_arr;
+  const void *const *b_arr;
+  void *const *c_arr;
+  int64_t a_off_bytes, b_off_bytes, c_off_bytes;
+  int64_t a_stride_bytes, b_stride_bytes, c_stride_bytes;
+  int count;
+  int tiles;
+};
+
+__global__ void __launch_bounds__(128) grouped_ptr_table_kernel(const __grid_constant__ PtrTableArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > a.count) return;
+  a.tile_start[i] = i * a.tiles;
+  if (i == a.count) return;
+  hcbk_grouped_entry *e = a.table + i;
+  const uint4 *src = a.tmpl;
+  uint4 *dst = reinterpret_cast<uint4 *>(e);
+#pragma unroll 4
+  for (int j = 0; j < (int)(sizeof(hcbk_grouped_entry) / 16); ++j) dst[j] = src[j];
+  const char *pa = static_cast<const char *>(a.a_arr[i]);
+  const char *pb = static_cast<const char *>(a.b_arr[i]);
+  char *pc = static_cast<char *>(a.c_arr[i]);
+  pa = pa ? pa + a.a_off_bytes + (int64_t)i * a.a_stride_bytes : nullptr;
+  pb = pb ? pb + a.b_off_bytes + (int64_t)i * a.b_stride_bytes : nullptr;
+  pc = pc ? pc + a.c_off_bytes + (int64_t)i * a.c_stride_bytes : nullptr;
+  const bool ok = pa && pb && pc && ((reinterpret_cast<uintptr_t>(pa) & 15) == 0) &&
+                  ((reinterpret_cast<uintptr_t>(pb) & 15) == 0);
+  const bool c_ok = ok && a.tmpl_c_tma && ((reinterpret_cast<uintptr_t>(pc) & 15) == 0);
+  e->c = pc;
+  e->skip = ok ? 0 : 1;
+  e->c_tma = c_ok ? 1 : 0;
+  a.skip_out[i] = ok ? 0 : 1;
+  if (ok) {
+    tensormap_replace_address(e->map_a, pa);
+    tensormap_replace_address(e->map_b, pb);
+    if (c_ok) tensormap_replace_address(e->map_c, pc);
+  }
+  tensormap_release();
 }
 
 /* ------------------------------------------------------------------------
@@ -578,6 +717,21 @@ __global__ void __launch_bounds__(256) grouped_pack_kernel(const hcbk_gpack_job 
   }
 }
 
+/* Pointer-array batch on the grouped split-BF16 path: the plan's pack jobs
+ * (2i: op(A) of problem i, 2i + 1: op(B)) and GEMM entries (i) take their
+ * source and C pointers from the device-resident arrays, matrix i being
+ * X[i] + x_off + i * x_stride (elements). */
+__global__ void __launch_bounds__(128) grouped_split_patch_kernel(
+    hcbk_gpack_job *jobs, hcbk_grouped_entry *table, const float *const *a_arr,
+    const float *const *b_arr, float *const *c_arr, int64_t a_off, int64_t b_off, int64_t c_off,
+    int64_t a_stride, int64_t b_stride, int64_t c_stride, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  jobs[2 * i].src = a_arr[i] + a_off + (int64_t)i * a_stride;
+  jobs[2 * i + 1].src = b_arr[i] + b_off + (int64_t)i * b_stride;
+  table[i].c = c_arr[i] + c_off + (int64_t)i * c_stride;
+}
+
 }  // namespace grouped
 }  // namespace hcbk
 
@@ -587,14 +741,19 @@ extern "C" int hcbk_grouped_encode(hcbk_grouped_entry *e, int op_a, int op_b, in
   if (m <= 0 || n <= 0 || k <= 0 || m > 0x7fffffff || n > 0x7fffffff || k > 0x7fffffff)
     return HCBK_ERR_ARGS;
   memset(e, 0, sizeof(*e));
+  /* the tile width that pads N least (ties: the wider) */
+  const int64_t w64 = (n + 63) / 64 * 64, w128 = (n + 127) / 128 * 128;
+  e->bn = w64 < w128 ? 64 : 128;
   e->a_mn = op_a == HCBK_OP_N; /* op(A) = A: column-major M x K, M contiguous */
   e->b_mn = op_b != HCBK_OP_N; /* op(B) = B^T: N contiguous */
   int rc = e->a_mn ? hcbk_encode_tma_2d(e->map_a, 0, a, m, k, lda, 64, 64)
                    : hcbk_encode_tma_2d(e->map_a, 0, a, k, m, lda, 64, 128);
   if (rc) return rc;
   rc = e->b_mn ? hcbk_encode_tma_2d(e->map_b, 0, b, n, k, ldb, 64, 64)
-               : hcbk_encode_tma_2d(e->map_b, 0, b, k, n, ldb, 64, 128);
+               : hcbk_encode_tma_2d(e->map_b, 0, b, k, n, ldb, 64, (uint32_t)e->bn);
   if (rc) return rc;
+  /* C by tensor stores when TMA can address it */
+  e->c_tma = hcbk_encode_out_2d(e->map_c, c, m, n, ldc) == HCBK_OK ? 1 : 0;
   e->c = c;
   e->ldc = ldc;
   e->m = (int32_t)m;
@@ -602,6 +761,45 @@ extern "C" int hcbk_grouped_encode(hcbk_grouped_entry *e, int op_a, int op_b, in
   e->k = (int32_t)k;
   e->tiles_m = (int32_t)((m + 127) / 128);
   return HCBK_OK;
+}
+
+extern "C" int hcbk_grouped_tiles(const hcbk_grouped_entry *e) {
+  return e->tiles_m * (int)((e->n + e->bn - 1) / e->bn);
+}
+
+extern "C" int hcbk_grouped_ptr_table(const hcbk_grouped_entry *tmpl, hcbk_grouped_entry *table,
+                                      int32_t *tile_start, int32_t *skip,
+                                      const void *const *a_arr, const void *const *b_arr,
+                                      void *const *c_arr, int64_t a_off_bytes,
+                                      int64_t b_off_bytes, int64_t c_off_bytes,
+                                      int64_t a_stride_bytes, int64_t b_stride_bytes,
+                                      int64_t c_stride_bytes, int count, void *stream) {
+  using namespace hcbk::grouped;
+  if (count <= 0 || !a_arr || !b_arr || !c_arr ||
+      (reinterpret_cast<uintptr_t>(table) & 127))
+    return HCBK_ERR_ARGS;
+  static_assert(sizeof(hcbk_grouped_entry) % 16 == 0, "entry size");
+  PtrTableArgs a;
+  memcpy(a.tmpl, tmpl, sizeof(hcbk_grouped_entry));
+  a.tmpl_c_tma = tmpl->c_tma;
+  a.table = table;
+  a.tile_start = tile_start;
+  a.skip_out = skip;
+  a.a_arr = a_arr;
+  a.b_arr = b_arr;
+  a.c_arr = c_arr;
+  a.a_off_bytes = a_off_bytes;
+  a.b_off_bytes = b_off_bytes;
+  a.c_off_bytes = c_off_bytes;
+  a.a_stride_bytes = a_stride_bytes;
+  a.b_stride_bytes = b_stride_bytes;
+  a.c_stride_bytes = c_stride_bytes;
+  a.count = count;
+  a.tiles = hcbk_grouped_tiles(tmpl);
+  const int threads = 128;
+  const int blocks = (count + 1 + threads - 1) / threads;
+  grouped_ptr_table_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
 extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream) {
@@ -624,6 +822,7 @@ extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void 
   p.alpha = g->alpha;
   p.beta = g->beta;
   p.beta_nonzero = g->beta != 0.0f;
+  p.device_maps = g->device_maps;
   p.err = err;
   int grid = hcbk_sm_count();
   if (g->total_tiles < grid) grid = g->total_tiles;
@@ -664,6 +863,7 @@ int launch_grouped_split(const hcbk_grouped_args *g, int *err, void *stream) {
   p.alpha = g->alpha;
   p.beta = g->beta;
   p.beta_nonzero = g->beta != 0.0f;
+  p.device_maps = 0;
   p.err = err;
   int grid = hcbk_sm_count();
   if (g->total_tiles < grid) grid = g->total_tiles;
@@ -679,4 +879,20 @@ extern "C" int hcbk_sgemm_grouped_split_tc(const hcbk_grouped_args *g, int terms
   if (terms == 6) return launch_grouped_split<hcbk::tc::RecipeBf16x6, SplitCfg6>(g, err, stream);
   if (terms == 3) return launch_grouped_split<hcbk::tc::RecipeBf16x3, SplitCfg3>(g, err, stream);
   return HCBK_ERR_ARGS;
+}
+
+extern "C" int hcbk_grouped_split_patch(hcbk_gpack_job *jobs, hcbk_grouped_entry *table,
+                                        const void *const *a_arr, const void *const *b_arr,
+                                        void *const *c_arr, int64_t a_off, int64_t b_off,
+                                        int64_t c_off, int64_t a_stride, int64_t b_stride,
+                                        int64_t c_stride, int count, void *stream) {
+  using namespace hcbk::grouped;
+  if (count <= 0 || !a_arr || !b_arr || !c_arr) return HCBK_ERR_ARGS;
+  const int threads = 128;
+  grouped_split_patch_kernel<<<(count + threads - 1) / threads, threads, 0,
+                               static_cast<cudaStream_t>(stream)>>>(
+      jobs, table, reinterpret_cast<const float *const *>(a_arr),
+      reinterpret_cast<const float *const *>(b_arr), reinterpret_cast<float *const *>(c_arr),
+      a_off, b_off, c_off, a_stride, b_stride, c_stride, count);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -56,6 +56,10 @@ typedef struct hcbk_gemm_args {
   const void *const *b_array;
   void *const *c_array;
   int64_t batch;
+  /* device flags or NULL: batch entry i is computed only where
+   * batch_select[i] != 0 (the CUDA-core pass of a batch whose tensor-core
+   * pass skipped entries it could not address) */
+  const int32_t *batch_select;
   double alpha_re, alpha_im;
   double beta_re, beta_im;
 } hcbk_gemm_args;
@@ -428,14 +432,18 @@ int hcbk_ger(const hcbk_ger_args *g, void *stream);
  * device memory: TMA tensor maps of op(A) and op(B) (encoded on the host by
  * hcbk_grouped_encode), the C block and the problem shape.  128-byte maps,
  * 64-byte aligned entries. */
-typedef struct alignas(64) hcbk_grouped_entry {
+typedef struct alignas(128) hcbk_grouped_entry {
   unsigned char map_a[128];
   unsigned char map_b[128];
+  unsigned char map_c[128]; /* f16 C {m, n}, box 32 x 32 (valid when c_tma) */
   void *c;
   int64_t ldc;
   int32_t m, n, k;
   int32_t a_mn, b_mn; /* operand is MN-major in memory */
   int32_t tiles_m;
+  int32_t bn;    /* tile columns of this problem: 64 or 128 */
+  int32_t c_tma; /* C is written (and read) by TMA through map_c */
+  int32_t skip;  /* set by the device-side table builder: computed elsewhere */
 } hcbk_grouped_entry;
 
 /* 2-D tensor map (128 bytes at `map`, 64-byte aligned) over 16-bit data
@@ -452,15 +460,38 @@ int hcbk_grouped_encode(hcbk_grouped_entry *e, int op_a, int op_b, int64_t m, in
                         int64_t k, const void *a, int64_t lda, const void *b, int64_t ldb,
                         void *c, int64_t ldc);
 
-/* Persistent grouped HGEMM: 128 x 128 tiles of every problem, enumerated by
- * tile_start[] (count + 1 ascending prefix sums of each problem's tile
- * count), C = alpha * op(A) op(B) + beta * C with f32 accumulation. */
+/* 2-D map over a column-major f16 C {rows, cols} with column pitch ld
+ * elements, box {32, 32}, no swizzle (the grouped epilogue's tensor stores);
+ * HCBK_ERR_ALIGN when TMA cannot address C. */
+int hcbk_encode_out_2d(void *map, void *base, uint64_t rows, uint64_t cols, uint64_t ld);
+
+/* tiles of an encoded problem: tiles_m * ceil(n / bn) */
+int hcbk_grouped_tiles(const hcbk_grouped_entry *e);
+
+/* Device-side table of a uniform pointer-array batch: entry i is *tmpl with
+ * the addresses of its maps replaced by a_arr[i] + a_off_bytes +
+ * i * a_stride_bytes etc. (on the
+ * GPU, by tensormap.replace), skip[i] = 1 where A or B is not 16-byte
+ * aligned, tile_start[i] = i * tiles (count + 1 entries).  table must be
+ * 128-byte aligned. */
+int hcbk_grouped_ptr_table(const hcbk_grouped_entry *tmpl, hcbk_grouped_entry *table,
+                           int32_t *tile_start, int32_t *skip, const void *const *a_arr,
+                           const void *const *b_arr, void *const *c_arr, int64_t a_off_bytes,
+                           int64_t b_off_bytes, int64_t c_off_bytes, int64_t a_stride_bytes,
+                           int64_t b_stride_bytes, int64_t c_stride_bytes, int count,
+                           void *stream);
+
+/* Persistent grouped HGEMM: 128 x bn tiles (bn per problem) of every problem,
+ * enumerated by tile_start[] (count + 1 ascending prefix sums of each
+ * problem's tile count), C = alpha * op(A) op(B) + beta * C with f32
+ * accumulation. */
 typedef struct hcbk_grouped_args {
   const hcbk_grouped_entry *table; /* device */
   const int32_t *tile_start;        /* device, count + 1 entries */
   int32_t count;
   int32_t total_tiles;
   float alpha, beta;
+  int32_t device_maps; /* the table's maps were patched on the device */
 } hcbk_grouped_args;
 int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
 
@@ -509,6 +540,15 @@ typedef struct hcbk_gpack_job {
   int32_t tiles_r;
   int32_t pad_;
 } hcbk_gpack_job;
+
+/* Pointer-array batches on the grouped split-BF16 path: job 2i / 2i + 1 and
+ * entry i take a_arr[i] + a_off + i * a_stride (f32 elements; B, C alike)
+ * as their source / C pointers, on the device. */
+int hcbk_grouped_split_patch(hcbk_gpack_job *jobs, hcbk_grouped_entry *table,
+                             const void *const *a_arr, const void *const *b_arr,
+                             void *const *c_arr, int64_t a_off, int64_t b_off, int64_t c_off,
+                             int64_t a_stride, int64_t b_stride, int64_t c_stride, int count,
+                             void *stream);
 
 /* Split every job's operand in one launch: 32 x 64 tiles enumerated by
  * tile_start[] (count + 1 ascending prefix sums, device). */

@@ -149,6 +149,7 @@ template <typename T, typename Acc> struct SimtParams {
   const T *const *b_arr;
   T *const *c_arr;
   int64_t batch;
+  const int32_t *sel; /* batch entries to compute (NULL: all) */
   Acc alpha, beta;
   int beta_nonzero;
 };
@@ -402,6 +403,7 @@ simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
   const int64_t n0 = tile_n * BN;
 
   for (int64_t bidx = blockIdx.y; bidx < p.batch; bidx += gridDim.y) {
+    if (p.sel && p.sel[bidx] == 0) continue; /* uniform across the block */
     TileJob<T> j;
     j.m = p.m;
     j.n = p.n;
@@ -495,6 +497,7 @@ int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
   p.b_arr = reinterpret_cast<const T *const *>(a->b_array);
   p.c_arr = reinterpret_cast<T *const *>(a->c_array);
   p.batch = a->batch;
+  p.sel = a->batch_select;
   p.alpha = HostScalar<Acc>::make(a->alpha_re, a->alpha_im);
   p.beta = HostScalar<Acc>::make(a->beta_re, a->beta_im);
   p.beta_nonzero = (a->beta_re != 0.0 || a->beta_im != 0.0);

@@ -240,6 +240,28 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void 
       : "memory");
 }
 
+/* Tensor maps patched on the device (problem tables built by a kernel
+ * from device-resident pointer arrays): the global address of a 128-byte
+ * aligned map in global memory is replaced in place, the patching thread
+ * releases its generic-proxy writes to the tensor-map proxy, and a kernel
+ * that then loads or stores through the map acquires it first. */
+__device__ __forceinline__ void tensormap_replace_address(void *map, const void *addr) {
+  asm volatile("tensormap.replace.tile.global_address.global.b1024.b64 [%0], %1;" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "l"(reinterpret_cast<uint64_t>(addr))
+               : "memory");
+}
+
+__device__ __forceinline__ void tensormap_release() {
+  asm volatile("fence.proxy.tensormap::generic.release.gpu;" ::: "memory");
+}
+
+__device__ __forceinline__ void tensormap_acquire(const void *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                   reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 /* make this thread's generic-proxy shared-memory writes visible to the
  * async proxy (bulk / tensor copies) */
 __device__ __forceinline__ void fence_proxy_async_smem() {

@@ -1158,6 +1158,12 @@ static int make_map_out(CUtensorMap *map, CUtensorMapDataType dt, uint32_t esz, 
   return r == CUDA_SUCCESS ? HCBK_OK : HCBK_ERR_ALIGN;
 }
 
+extern "C" int hcbk_encode_out_2d(void *map, void *base, uint64_t rows, uint64_t cols,
+                                  uint64_t ld) {
+  return make_map_out(static_cast<CUtensorMap *>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base,
+                      rows, cols, ld);
+}
+
 /* f16 operands straight from the caller's matrices (column-major canonical). */
 static int hgemm_tc_impl(const hcbk_gemm_args *a, int bn, int pair, int *err, void *stream,
                          int inject_skip_load) {
