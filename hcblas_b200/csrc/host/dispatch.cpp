@@ -33,6 +33,18 @@ bool aligned16(const void *p, int64_t off, int esz) {
 }
 
 int simt(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char **path) {
+  if (a->dtype == HCBK_D && st->dgemm_dmma) {
+    /* native FP64 on the DMMA path (mma.sync .f64) */
+    *path = "dmma.d.128x128";
+    int rc = timed_launch(st, stream, *path, [&] { return hcbk_dgemm_dmma(a, stream); });
+    if (rc != HCBK_ERR_ARGS) return rc;
+  }
+  if (a->dtype == HCBK_Z && st->dgemm_dmma) {
+    /* native complex FP64: four real DMMA products per fragment set */
+    *path = "dmma.z.128x64";
+    int rc = timed_launch(st, stream, *path, [&] { return hcbk_zgemm_zmma(a, stream); });
+    if (rc != HCBK_ERR_ARGS) return rc;
+  }
   const int sms = hcbk_sm_count();
   const int64_t big = (a->dtype == HCBK_C || a->dtype == HCBK_Z) ? 64 : 128;
   hcbk_simt_cfg cfg;

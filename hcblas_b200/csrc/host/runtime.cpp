@@ -487,6 +487,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->crt_i8 = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "dgemm_dmma") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->dgemm_dmma = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   if (std::strcmp(name, "workspace_mb") == 0) {
     if (value < 0) return HCBLAS_STATUS_INVALID_VALUE;
     handle->impl->workspace_limit = (size_t)value << 20;

@@ -1,0 +1,530 @@
+/*
+ * dmma_gemm.cu -- native FP64 DGEMM on the FP64 tensor path of sm_100a
+ * (warp-level mma.sync .f64, m16n8k4), the plain DGEMM of this library
+ * (reference: lib/src/blas/dgemm/dgemm_*kernels*.cpp, one HCC tile kernel per
+ * layout and size bucket).
+ *
+ * Why the tensor path for FP64: B200's FP64 rate is the same on the CUDA
+ * cores and through DMMA, but one m16n8k4 instruction does 512 multiply-adds
+ * from 3 operand registers per lane where the CUDA-core form needs 16 DFMA
+ * instructions and 32 register reads; the shared-memory traffic per flop
+ * drops 4x, which leaves issue slots for loads and lets one CTA per SM keep
+ * the FP64 pipe busy.
+ *
+ * Design: 128 x 128 CTA tiles, 256 threads = 8 warps as 2 (M) x 4 (N), each
+ * warp a 64 x 32 block = 4 x 4 m16n8 accumulators (64 doubles per lane).
+ * K advances in slabs of 16 through two shared-memory buffers laid out
+ * [k][mn] (row pitch 132 doubles: the 16 lanes of a half-warp reading A or B
+ * fragments hit 16 distinct bank pairs); the next slab is fetched into
+ * registers with 16-byte loads while the current one is multiplied, whatever
+ * the transposes (each operand is read along its contiguous dimension).
+ * Out-of-range rows, columns and k are zero-filled, so any shape, leading
+ * dimension, offset and alignment runs here; batches (strided or pointer
+ * arrays) take blockIdx.y.  Epilogue: alpha * acc + beta * C in registers,
+ * beta == 0 never reads C.
+ *
+ * Fragment layout of mma.sync.aligned.m16n8k4.row.col.f64 (PTX ISA, "matrix
+ * fragments for mma.m16n8k4 .f64"): lane = 4 g + t; A (16 x 4, row):
+ * a0 = A[g][t], a1 = A[g + 8][t]; B (4 x 8, col): b0 = B[t][g];
+ * C (16 x 8): c0, c1 = C[g][2t], C[g][2t + 1]; c2, c3 = C[g + 8][2t],
+ * C[g + 8][2t + 1].
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hcbk.h"
+
+namespace hcbk {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16;
+constexpr int NT = 256;
+constexpr int LDS = BM + 4; /* doubles per smem row (both operands) */
+constexpr int WM = 64, WN = 32; /* warp tile */
+constexpr int MT = WM / 16, NTL = WN / 8; /* m16 x n8 accumulators per warp */
+
+struct DmmaParams {
+  int64_t m, n, k;
+  const double *a;
+  int64_t lda, sa, a_off;
+  const double *b;
+  int64_t ldb, sb, b_off;
+  double *c;
+  int64_t ldc, sc, c_off;
+  const double *const *a_arr;
+  const double *const *b_arr;
+  double *const *c_arr;
+  const int32_t *sel;
+  int64_t batch;
+  double alpha, beta;
+  int beta_nonzero;
+};
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
+      "{%0, %1, %2, %3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+struct alignas(16) D2 {
+  double v[2];
+};
+
+/*
+ * OP_A / OP_B: 0 = N, 1 = T (column-major canonical; FP64 has no conjugate).
+ *   op(A) MN-contiguous iff OP_A == N;  op(B) K-contiguous iff OP_B == N.
+ */
+template <int OP_A, int OP_B>
+__global__ void __launch_bounds__(NT, 1) dmma_gemm_kernel(const DmmaParams p) {
+  constexpr bool A_MN = (OP_A == HCBK_OP_N);
+  constexpr bool B_MN = (OP_B != HCBK_OP_N);
+  /* 16-byte vectors (2 doubles) per thread and slab: 128 x 16 / 2 / 256 = 4 */
+  constexpr int VA = (BM * BK) / (2 * NT);
+  constexpr int VB = (BN * BK) / (2 * NT);
+  extern __shared__ __align__(16) double dmma_smem[];
+  auto As = reinterpret_cast<double (*)[BK][LDS]>(dmma_smem);              /* [2][BK][LDS] */
+  auto Bs = reinterpret_cast<double (*)[BK][LDS]>(dmma_smem + 2 * BK * LDS); /* [2][BK][LDS] */
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * WM, wn = (warp >> 1) * WN;
+
+  /* tile rasterisation: bands of 8 M-tiles for L2 reuse of B panels */
+  const int64_t tiles_m = (p.m + BM - 1) / BM;
+  const int64_t tiles_n = (p.n + BN - 1) / BN;
+  const int64_t lin = blockIdx.x;
+  constexpr int64_t BAND = 8;
+  const int64_t per_band = BAND * tiles_n;
+  const int64_t band = lin / per_band;
+  const int64_t first_m = band * BAND;
+  const int64_t band_h = (tiles_m - first_m) < BAND ? (tiles_m - first_m) : BAND;
+  const int64_t in_band = lin - band * per_band;
+  const int64_t m0 = (first_m + in_band % band_h) * BM;
+  const int64_t n0 = (in_band / band_h) * BN;
+
+  for (int64_t bidx = blockIdx.y; bidx < p.batch; bidx += gridDim.y) {
+    if (p.sel && p.sel[bidx] == 0) continue; /* uniform across the block */
+    const double *A = (p.a_arr ? p.a_arr[bidx] : p.a) + p.a_off + bidx * p.sa;
+    const double *B = (p.b_arr ? p.b_arr[bidx] : p.b) + p.b_off + bidx * p.sb;
+    double *C = (p.c_arr ? p.c_arr[bidx] : p.c) + p.c_off + bidx * p.sc;
+    const bool vec_a = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((p.lda & 1) == 0);
+    const bool vec_b = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && ((p.ldb & 1) == 0);
+
+    D2 ra[VA], rb[VB];
+    auto fetch = [&](int64_t k0) {
+#pragma unroll
+      for (int v = 0; v < VA; ++v) {
+        const int idx = tid + v * NT;
+        if (A_MN) { /* 64 vectors along m per k row */
+          const int64_t mn = m0 + (int64_t)(idx % (BM / 2)) * 2, kk = k0 + idx / (BM / 2);
+          const double *src = A + mn + kk * p.lda;
+          if (kk < p.k && mn + 2 <= p.m && vec_a) {
+            ra[v] = *reinterpret_cast<const D2 *>(src);
+          } else {
+            ra[v].v[0] = (kk < p.k && mn < p.m) ? src[0] : 0.0;
+            ra[v].v[1] = (kk < p.k && mn + 1 < p.m) ? src[1] : 0.0;
+          }
+        } else { /* 8 vectors along k per m row */
+          const int64_t mn = m0 + idx / (BK / 2), kk = k0 + (int64_t)(idx % (BK / 2)) * 2;
+          const double *src = A + kk + mn * p.lda;
+          if (mn < p.m && kk + 2 <= p.k && vec_a) {
+            ra[v] = *reinterpret_cast<const D2 *>(src);
+          } else {
+            ra[v].v[0] = (mn < p.m && kk < p.k) ? src[0] : 0.0;
+            ra[v].v[1] = (mn < p.m && kk + 1 < p.k) ? src[1] : 0.0;
+          }
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VB; ++v) {
+        const int idx = tid + v * NT;
+        if (B_MN) {
+          const int64_t mn = n0 + (int64_t)(idx % (BN / 2)) * 2, kk = k0 + idx / (BN / 2);
+          const double *src = B + mn + kk * p.ldb;
+          if (kk < p.k && mn + 2 <= p.n && vec_b) {
+            rb[v] = *reinterpret_cast<const D2 *>(src);
+          } else {
+            rb[v].v[0] = (kk < p.k && mn < p.n) ? src[0] : 0.0;
+            rb[v].v[1] = (kk < p.k && mn + 1 < p.n) ? src[1] : 0.0;
+          }
+        } else {
+          const int64_t mn = n0 + idx / (BK / 2), kk = k0 + (int64_t)(idx % (BK / 2)) * 2;
+          const double *src = B + kk + mn * p.ldb;
+          if (mn < p.n && kk + 2 <= p.k && vec_b) {
+            rb[v] = *reinterpret_cast<const D2 *>(src);
+          } else {
+            rb[v].v[0] = (mn < p.n && kk < p.k) ? src[0] : 0.0;
+            rb[v].v[1] = (mn < p.n && kk + 1 < p.k) ? src[1] : 0.0;
+          }
+        }
+      }
+    };
+    auto stash = [&](int s) {
+#pragma unroll
+      for (int v = 0; v < VA; ++v) {
+        const int idx = tid + v * NT;
+        if (A_MN) {
+          const int mn = (idx % (BM / 2)) * 2, kk = idx / (BM / 2);
+          *reinterpret_cast<D2 *>(&As[s][kk][mn]) = ra[v];
+        } else {
+          const int mn = idx / (BK / 2), kk = (idx % (BK / 2)) * 2;
+          As[s][kk][mn] = ra[v].v[0];
+          As[s][kk + 1][mn] = ra[v].v[1];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VB; ++v) {
+        const int idx = tid + v * NT;
+        if (B_MN) {
+          const int mn = (idx % (BN / 2)) * 2, kk = idx / (BN / 2);
+          *reinterpret_cast<D2 *>(&Bs[s][kk][mn]) = rb[v];
+        } else {
+          const int mn = idx / (BK / 2), kk = (idx % (BK / 2)) * 2;
+          Bs[s][kk][mn] = rb[v].v[0];
+          Bs[s][kk + 1][mn] = rb[v].v[1];
+        }
+      }
+    };
+
+    double acc[MT][NTL][4];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+    const int64_t ktiles = (p.k + BK - 1) / BK;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    for (int64_t kt = 0; kt < ktiles; ++kt) {
+      const int s = (int)(kt & 1);
+      if (kt + 1 < ktiles) fetch((kt + 1) * BK);
+#pragma unroll
+      for (int k4 = 0; k4 < BK; k4 += 4) {
+        double af[MT][2], bf[NTL];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) {
+          af[i][0] = As[s][k4 + t][wm + 16 * i + g];
+          af[i][1] = As[s][k4 + t][wm + 16 * i + g + 8];
+        }
+#pragma unroll
+        for (int j = 0; j < NTL; ++j) bf[j] = Bs[s][k4 + t][wn + 8 * j + g];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NTL; ++j) dmma(acc[i][j], af[i][0], af[i][1], bf[j]);
+      }
+      if (kt + 1 < ktiles) stash(s ^ 1);
+      __syncthreads();
+    }
+
+    /* epilogue: c0, c1 at (g, 2t), (g, 2t + 1); c2, c3 at row g + 8 */
+    const bool rd = p.beta_nonzero != 0;
+#pragma unroll
+    for (int i = 0; i < MT; ++i) {
+#pragma unroll
+      for (int j = 0; j < NTL; ++j) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int64_t row = m0 + wm + 16 * i + g + (e >> 1) * 8;
+          const int64_t col = n0 + wn + 8 * j + 2 * t + (e & 1);
+          if (row < p.m && col < p.n) {
+            double *dst = C + row + col * p.ldc;
+            const double o = p.alpha * acc[i][j][e];
+            *dst = rd ? fma(p.beta, *dst, o) : o;
+          }
+        }
+      }
+    }
+    if (p.batch > 1) __syncthreads(); /* the shared buffers are reused by the next entry */
+  }
+}
+
+/*
+ * Native ZGEMM on the same FP64 tensor path: the complex product is four
+ * real products per fragment set, Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br
+ * (the 4M form, exact in the order of its FMAs as the CUDA-core kernel's),
+ * with the operands split into real and imaginary shared-memory planes when
+ * a slab is stored (conjugation applied there).  128 x 64 CTA tiles, 8 warps
+ * as 4 (M) x 2 (N), warp tiles 32 x 32 = 2 x 4 m16n8 accumulator pairs;
+ * K slabs of 8 complex elements, one 16-byte load per element.
+ */
+constexpr int ZBM = 128, ZBN = 64, ZBK = 8;
+constexpr int ZLDA = ZBM + 4, ZLDB = ZBN + 4;
+constexpr int ZWM = 32, ZWN = 32, ZMT = ZWM / 16, ZNT = ZWN / 8;
+
+struct ZmmaParams {
+  int64_t m, n, k;
+  const double2 *a;
+  int64_t lda, sa, a_off;
+  const double2 *b;
+  int64_t ldb, sb, b_off;
+  double2 *c;
+  int64_t ldc, sc, c_off;
+  const double2 *const *a_arr;
+  const double2 *const *b_arr;
+  double2 *const *c_arr;
+  const int32_t *sel;
+  int64_t batch;
+  double2 alpha, beta;
+  int beta_nonzero;
+};
+
+template <int OP_A, int OP_B>
+__global__ void __launch_bounds__(NT, 1) zmma_gemm_kernel(const ZmmaParams p) {
+  constexpr bool A_MN = (OP_A == HCBK_OP_N);
+  constexpr bool B_MN = (OP_B != HCBK_OP_N);
+  constexpr bool CJ_A = (OP_A == HCBK_OP_C);
+  constexpr bool CJ_B = (OP_B == HCBK_OP_C);
+  constexpr int VA = (ZBM * ZBK) / NT; /* complex elements per thread and slab: 4 */
+  constexpr int VB = (ZBN * ZBK) / NT; /* 2 */
+  extern __shared__ __align__(16) double zmma_smem[];
+  /* [2 buffers][re, im][ZBK][ld] */
+  auto As = reinterpret_cast<double (*)[2][ZBK][ZLDA]>(zmma_smem);
+  auto Bs = reinterpret_cast<double (*)[2][ZBK][ZLDB]>(zmma_smem + 2 * 2 * ZBK * ZLDA);
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * ZWM, wn = (warp >> 2) * ZWN;
+
+  const int64_t tiles_m = (p.m + ZBM - 1) / ZBM;
+  const int64_t tiles_n = (p.n + ZBN - 1) / ZBN;
+  const int64_t lin = blockIdx.x;
+  constexpr int64_t BAND = 8;
+  const int64_t per_band = BAND * tiles_n;
+  const int64_t band = lin / per_band;
+  const int64_t first_m = band * BAND;
+  const int64_t band_h = (tiles_m - first_m) < BAND ? (tiles_m - first_m) : BAND;
+  const int64_t in_band = lin - band * per_band;
+  const int64_t m0 = (first_m + in_band % band_h) * ZBM;
+  const int64_t n0 = (in_band / band_h) * ZBN;
+
+  for (int64_t bidx = blockIdx.y; bidx < p.batch; bidx += gridDim.y) {
+    if (p.sel && p.sel[bidx] == 0) continue; /* uniform across the block */
+    const double2 *A = (p.a_arr ? p.a_arr[bidx] : p.a) + p.a_off + bidx * p.sa;
+    const double2 *B = (p.b_arr ? p.b_arr[bidx] : p.b) + p.b_off + bidx * p.sb;
+    double2 *C = (p.c_arr ? p.c_arr[bidx] : p.c) + p.c_off + bidx * p.sc;
+
+    double2 ra[VA], rb[VB];
+    auto fetch = [&](int64_t k0) {
+#pragma unroll
+      for (int v = 0; v < VA; ++v) {
+        const int idx = tid + v * NT;
+        const int64_t mn = m0 + (A_MN ? idx % ZBM : idx / ZBK);
+        const int64_t kk = k0 + (A_MN ? idx / ZBM : idx % ZBK);
+        ra[v] = (mn < p.m && kk < p.k) ? (A_MN ? A[mn + kk * p.lda] : A[kk + mn * p.lda])
+                                       : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int v = 0; v < VB; ++v) {
+        const int idx = tid + v * NT;
+        const int64_t mn = n0 + (B_MN ? idx % ZBN : idx / ZBK);
+        const int64_t kk = k0 + (B_MN ? idx / ZBN : idx % ZBK);
+        rb[v] = (mn < p.n && kk < p.k) ? (B_MN ? B[mn + kk * p.ldb] : B[kk + mn * p.ldb])
+                                       : make_double2(0.0, 0.0);
+      }
+    };
+    auto stash = [&](int s) {
+#pragma unroll
+      for (int v = 0; v < VA; ++v) {
+        const int idx = tid + v * NT;
+        const int mn = A_MN ? idx % ZBM : idx / ZBK, kk = A_MN ? idx / ZBM : idx % ZBK;
+        As[s][0][kk][mn] = ra[v].x;
+        As[s][1][kk][mn] = CJ_A ? -ra[v].y : ra[v].y;
+      }
+#pragma unroll
+      for (int v = 0; v < VB; ++v) {
+        const int idx = tid + v * NT;
+        const int mn = B_MN ? idx % ZBN : idx / ZBK, kk = B_MN ? idx / ZBN : idx % ZBK;
+        Bs[s][0][kk][mn] = rb[v].x;
+        Bs[s][1][kk][mn] = CJ_B ? -rb[v].y : rb[v].y;
+      }
+    };
+
+    double cr[ZMT][ZNT][4], ci[ZMT][ZNT][4];
+#pragma unroll
+    for (int i = 0; i < ZMT; ++i)
+#pragma unroll
+      for (int j = 0; j < ZNT; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) cr[i][j][e] = ci[i][j][e] = 0.0;
+
+    const int64_t ktiles = (p.k + ZBK - 1) / ZBK;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    for (int64_t kt = 0; kt < ktiles; ++kt) {
+      const int s = (int)(kt & 1);
+      if (kt + 1 < ktiles) fetch((kt + 1) * ZBK);
+#pragma unroll
+      for (int k4 = 0; k4 < ZBK; k4 += 4) {
+        double ar[ZMT][2], ai[ZMT][2], br[ZNT], bi[ZNT];
+#pragma unroll
+        for (int i = 0; i < ZMT; ++i) {
+          ar[i][0] = As[s][0][k4 + t][wm + 16 * i + g];
+          ar[i][1] = As[s][0][k4 + t][wm + 16 * i + g + 8];
+          ai[i][0] = As[s][1][k4 + t][wm + 16 * i + g];
+          ai[i][1] = As[s][1][k4 + t][wm + 16 * i + g + 8];
+        }
+#pragma unroll
+        for (int j = 0; j < ZNT; ++j) {
+          br[j] = Bs[s][0][k4 + t][wn + 8 * j + g];
+          bi[j] = Bs[s][1][k4 + t][wn + 8 * j + g];
+        }
+#pragma unroll
+        for (int i = 0; i < ZMT; ++i)
+#pragma unroll
+          for (int j = 0; j < ZNT; ++j) {
+            dmma(cr[i][j], ar[i][0], ar[i][1], br[j]);
+            dmma(cr[i][j], -ai[i][0], -ai[i][1], bi[j]);
+            dmma(ci[i][j], ar[i][0], ar[i][1], bi[j]);
+            dmma(ci[i][j], ai[i][0], ai[i][1], br[j]);
+          }
+      }
+      if (kt + 1 < ktiles) stash(s ^ 1);
+      __syncthreads();
+    }
+
+    const bool rd = p.beta_nonzero != 0;
+#pragma unroll
+    for (int i = 0; i < ZMT; ++i) {
+#pragma unroll
+      for (int j = 0; j < ZNT; ++j) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int64_t row = m0 + wm + 16 * i + g + (e >> 1) * 8;
+          const int64_t col = n0 + wn + 8 * j + 2 * t + (e & 1);
+          if (row < p.m && col < p.n) {
+            double2 *dst = C + row + col * p.ldc;
+            const double re = cr[i][j][e], im = ci[i][j][e];
+            double2 o;
+            o.x = p.alpha.x * re - p.alpha.y * im;
+            o.y = p.alpha.x * im + p.alpha.y * re;
+            if (rd) {
+              const double2 cv = *dst;
+              o.x += p.beta.x * cv.x - p.beta.y * cv.y;
+              o.y += p.beta.x * cv.y + p.beta.y * cv.x;
+            }
+            *dst = o;
+          }
+        }
+      }
+    }
+    if (p.batch > 1) __syncthreads(); /* the shared buffers are reused by the next entry */
+  }
+}
+
+}  // namespace
+}  // namespace hcbk
+
+using namespace hcbk;
+
+extern "C" int hcbk_dgemm_dmma(const hcbk_gemm_args *a, void *stream) {
+  if (a->dtype != HCBK_D || a->m <= 0 || a->n <= 0 || a->k <= 0 || a->batch <= 0 ||
+      a->op_a == HCBK_OP_C || a->op_b == HCBK_OP_C)
+    return HCBK_ERR_ARGS;
+  DmmaParams p;
+  p.m = a->m;
+  p.n = a->n;
+  p.k = a->k;
+  p.a = static_cast<const double *>(a->a);
+  p.lda = a->lda;
+  p.sa = a->stride_a;
+  p.a_off = a->a_off;
+  p.b = static_cast<const double *>(a->b);
+  p.ldb = a->ldb;
+  p.sb = a->stride_b;
+  p.b_off = a->b_off;
+  p.c = static_cast<double *>(a->c);
+  p.ldc = a->ldc;
+  p.sc = a->stride_c;
+  p.c_off = a->c_off;
+  p.a_arr = reinterpret_cast<const double *const *>(a->a_array);
+  p.b_arr = reinterpret_cast<const double *const *>(a->b_array);
+  p.c_arr = reinterpret_cast<double *const *>(a->c_array);
+  p.sel = a->batch_select;
+  p.batch = a->batch;
+  p.alpha = a->alpha_re;
+  p.beta = a->beta_re;
+  p.beta_nonzero = a->beta_re != 0.0;
+  const int64_t tiles = ((a->m + BM - 1) / BM) * ((a->n + BN - 1) / BN);
+  if (tiles > 0x7fffffffLL) return HCBK_ERR_ARGS;
+  dim3 grid((unsigned)tiles, (unsigned)(a->batch < 65535 ? a->batch : 65535), 1);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  constexpr int smem = 4 * BK * LDS * (int)sizeof(double); /* two buffers of A and of B */
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HCBK_ERR_LAUNCH;
+  auto kern = (a->op_a == HCBK_OP_N && a->op_b == HCBK_OP_N) ? dmma_gemm_kernel<0, 0>
+              : (a->op_a == HCBK_OP_N)                        ? dmma_gemm_kernel<0, 1>
+              : (a->op_b == HCBK_OP_N)                        ? dmma_gemm_kernel<1, 0>
+                                                              : dmma_gemm_kernel<1, 1>;
+  if (!attr_set[dev]) {
+    for (auto k : {dmma_gemm_kernel<0, 0>, dmma_gemm_kernel<0, 1>, dmma_gemm_kernel<1, 0>,
+                   dmma_gemm_kernel<1, 1>})
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+          cudaSuccess)
+        return HCBK_ERR_LAUNCH;
+    attr_set[dev] = true;
+  }
+  kern<<<grid, NT, smem, st>>>(p);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+extern "C" int hcbk_zgemm_zmma(const hcbk_gemm_args *a, void *stream) {
+  if (a->dtype != HCBK_Z || a->m <= 0 || a->n <= 0 || a->k <= 0 || a->batch <= 0)
+    return HCBK_ERR_ARGS;
+  ZmmaParams p;
+  p.m = a->m;
+  p.n = a->n;
+  p.k = a->k;
+  p.a = static_cast<const double2 *>(a->a);
+  p.lda = a->lda;
+  p.sa = a->stride_a;
+  p.a_off = a->a_off;
+  p.b = static_cast<const double2 *>(a->b);
+  p.ldb = a->ldb;
+  p.sb = a->stride_b;
+  p.b_off = a->b_off;
+  p.c = static_cast<double2 *>(a->c);
+  p.ldc = a->ldc;
+  p.sc = a->stride_c;
+  p.c_off = a->c_off;
+  p.a_arr = reinterpret_cast<const double2 *const *>(a->a_array);
+  p.b_arr = reinterpret_cast<const double2 *const *>(a->b_array);
+  p.c_arr = reinterpret_cast<double2 *const *>(a->c_array);
+  p.sel = a->batch_select;
+  p.batch = a->batch;
+  p.alpha = make_double2(a->alpha_re, a->alpha_im);
+  p.beta = make_double2(a->beta_re, a->beta_im);
+  p.beta_nonzero = a->beta_re != 0.0 || a->beta_im != 0.0;
+  const int64_t tiles = ((a->m + ZBM - 1) / ZBM) * ((a->n + ZBN - 1) / ZBN);
+  if (tiles > 0x7fffffffLL) return HCBK_ERR_ARGS;
+  dim3 grid((unsigned)tiles, (unsigned)(a->batch < 65535 ? a->batch : 65535), 1);
+  constexpr int smem = 2 * 2 * ZBK * (ZLDA + ZLDB) * (int)sizeof(double);
+  using K = void (*)(const ZmmaParams);
+  static const K table[3][3] = {
+      {zmma_gemm_kernel<0, 0>, zmma_gemm_kernel<0, 1>, zmma_gemm_kernel<0, 2>},
+      {zmma_gemm_kernel<1, 0>, zmma_gemm_kernel<1, 1>, zmma_gemm_kernel<1, 2>},
+      {zmma_gemm_kernel<2, 0>, zmma_gemm_kernel<2, 1>, zmma_gemm_kernel<2, 2>}};
+  if (a->op_a < 0 || a->op_a > 2 || a->op_b < 0 || a->op_b > 2) return HCBK_ERR_ARGS;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HCBK_ERR_LAUNCH;
+  if (!attr_set[dev]) {
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y)
+        if (cudaFuncSetAttribute(table[x][y], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem) != cudaSuccess)
+          return HCBK_ERR_LAUNCH;
+    attr_set[dev] = true;
+  }
+  table[a->op_a][a->op_b]<<<grid, NT, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}

@@ -73,6 +73,16 @@ typedef struct hcbk_simt_cfg {
  * accumulation.  Any op, ld, offset, alignment, batch. */
 int hcbk_gemm_simt(const hcbk_gemm_args *args, hcbk_simt_cfg cfg, void *stream);
 
+/* Native FP64 GEMM on the FP64 tensor path (mma.sync .f64 m16n8k4, 128 x 128
+ * CTA tiles).  Any ld, offset, alignment, batch (strided or pointer arrays,
+ * batch_select honoured); HCBK_ERR_ARGS for other dtypes. */
+int hcbk_dgemm_dmma(const hcbk_gemm_args *args, void *stream);
+
+/* Native complex FP64 GEMM on the same path: Re += Ar Br - Ai Bi,
+ * Im += Ar Bi + Ai Br as four real DMMA products (128 x 64 CTA tiles); any
+ * op (N, T, C), ld, offset, alignment, batch; HCBK_ERR_ARGS for other dtypes. */
+int hcbk_zgemm_zmma(const hcbk_gemm_args *args, void *stream);
+
 /* C := beta * C (beta == 0 writes zeros without reading C): the alpha == 0
  * path.  Any dtype, ld, offset, batch. */
 int hcbk_scale_c(const hcbk_gemm_args *args, void *stream);

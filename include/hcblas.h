@@ -486,6 +486,10 @@ hcblasStatus_t hcblasPlanEmulation(int mode, int param, int bits, int dtype, lon
  *                       0 binary16 residue planes on the f16 tensor cores,
  *                       sums reduced mod p every 1024 K.  Both give
  *                       bit-identical results.
+ *   "dgemm_dmma"        native DGEMM and ZGEMM (HCBLAS_MATH_NATIVE): 1
+ *                       (default) on the FP64 tensor path (warp-level
+ *                       mma.sync .f64; ZGEMM as four real products), 0 on the
+ *                       CUDA cores (DFMA); both accumulate in binary64.
  *   "workspace_mb"      upper limit of the handle's device workspace in MiB
  *                       (0, the default: none).  A call whose path needs more
  *                       returns HCBLAS_STATUS_EXECUTION_FAILED without

@@ -422,3 +422,105 @@ def test_set_get_matrix_async_on_a_stream(handle):
     assert hb.hcblasSetMatrixAsync(handle, rows, -1, 8, A.ctypes.data, lda, dB, ldb,
                                    s.cuda_stream) == hb.HCBLAS_STATUS_INVALID_VALUE
     hb.am_free(dB)
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_dgemm_dmma_matches_fma_path(handle, ta, tb):
+    """Native DGEMM: the FP64 tensor path (mma.sync .f64, the default) and
+    the CUDA-core DFMA path (tuning knob "dgemm_dmma" = 0) both stay within
+    gamma_{K+2}(f64) of the double-double oracle on ragged shapes with
+    padded leading dimensions and offsets; integer data gives exact results
+    on both."""
+    rng = np.random.default_rng(70 + 2 * ta + tb)
+    M, N, K = 301, 259, 517
+    lda = (M if ta == 0 else K) + 3
+    ldb = (K if tb == 0 else N) + 5
+    ldc = M + 1
+    A = rng.standard_normal(lda * (K if ta == 0 else M) + 7)
+    B = rng.standard_normal(ldb * (N if tb == 0 else K) + 7)
+    C = rng.standard_normal(ldc * N + 7)
+    outs = {}
+    for dmma in (1, 0):
+        assert hb.set_tuning(handle, "dgemm_dmma", dmma) == 0
+        try:
+            dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+            s = hb.lib_gemm(handle, O.COL, "nt"[ta], "nt"[tb], M, N, K, 1.25, dA, lda, dB, ldb,
+                            -0.5, dC, ldc, 3, 5, 7)
+            assert s == 0
+            outs[hb.hcblasGetLastPath(handle)] = dC.download()
+        finally:
+            hb.set_tuning(handle, "dgemm_dmma", 1)
+    assert set(outs) == {"dmma.d.128x128", "simt.d.64x64"} or \
+        set(outs) == {"dmma.d.128x128", "simt.d.128x128"}, set(outs)
+    _, ref = O.gemm(O.COL, ta, tb, M, N, K, 1.25, A, lda, B, ldb, -0.5, C, ldc, 3, 5, 7)
+    Ad = np.abs(op_dense(A, O.COL, ta, M, K, lda, 3))
+    Bd = np.abs(op_dense(B, O.COL, tb, K, N, ldb, 5))
+    Cd = np.abs(O.view_c(C, O.COL, M, N, ldc, 7))
+    bound = gamma("d", K) * np.linalg.norm(1.25 * (Ad @ Bd) + 0.5 * Cd)
+    for path, got in outs.items():
+        assert np.linalg.norm(O.view_c(got, O.COL, M, N, ldc, 7) - ref) <= bound, path
+        # outside the M x N window (ld padding, the offset) nothing changed
+        assert np.array_equal(got[:7], C[:7]), path
+    # integer data: exact on both paths
+    Ai = rng.integers(-50, 51, A.size).astype(np.float64)
+    Bi = rng.integers(-50, 51, B.size).astype(np.float64)
+    Ci = rng.integers(-50, 51, C.size).astype(np.float64)
+    exp, _ = O.gemm(O.COL, ta, tb, M, N, K, 2.0, Ai, lda, Bi, ldb, 1.0, Ci, ldc, 3, 5, 7,
+                    want_ref=False)
+    for dmma in (1, 0):
+        assert hb.set_tuning(handle, "dgemm_dmma", dmma) == 0
+        try:
+            dA, dB, dC = (hb.DeviceArray(handle, X) for X in (Ai, Bi, Ci))
+            assert hb.lib_gemm(handle, O.COL, "nt"[ta], "nt"[tb], M, N, K, 2.0, dA, lda, dB,
+                               ldb, 1.0, dC, ldc, 3, 5, 7) == 0
+            assert np.array_equal(dC.download(), exp), dmma
+        finally:
+            hb.set_tuning(handle, "dgemm_dmma", 1)
+
+
+@pytest.mark.parametrize("ta,tb", [(2, 0), (0, 2), (1, 2), (2, 1)])
+def test_zgemm_dmma_matches_fma_path(handle, ta, tb):
+    """Native ZGEMM on the FP64 tensor path (four real DMMA products per
+    fragment set) against the CUDA-core path and the double-double oracle,
+    conjugate transposes included; integer data exact on both."""
+    rng = np.random.default_rng(80 + 3 * ta + tb)
+    M, N, K = 200, 150, 333
+    lda = (M if ta == 0 else K) + 2
+    ldb = (K if tb == 0 else N) + 1
+    ldc = M + 3
+    mk = lambda n: (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    A, B, C = mk(lda * (K if ta == 0 else M) + 4), mk(ldb * (N if tb == 0 else K) + 4), \
+        mk(ldc * N + 4)
+    alpha, beta = (0.75 - 0.5j), (0.25 + 1j)
+    outs = {}
+    for dmma in (1, 0):
+        assert hb.set_tuning(handle, "dgemm_dmma", dmma) == 0
+        try:
+            dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
+            assert hb.lib_gemm(handle, O.COL, "ntc"[ta], "ntc"[tb], M, N, K, alpha, dA, lda, dB,
+                               ldb, beta, dC, ldc, 1, 2, 3) == 0
+            outs[hb.hcblasGetLastPath(handle)] = dC.download()
+        finally:
+            hb.set_tuning(handle, "dgemm_dmma", 1)
+    assert "dmma.z.128x64" in outs and any(k.startswith("simt.z") for k in outs), set(outs)
+    _, ref = O.gemm(O.COL, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, 1, 2, 3)
+    Ad = np.abs(op_dense(A, O.COL, ta, M, K, lda, 1))
+    Bd = np.abs(op_dense(B, O.COL, tb, K, N, ldb, 2))
+    Cd = np.abs(O.view_c(C, O.COL, M, N, ldc, 3))
+    bound = gamma("z", K) * np.linalg.norm(abs(alpha) * (Ad @ Bd) + abs(beta) * Cd)
+    for path, got in outs.items():
+        assert np.linalg.norm(O.view_c(got, O.COL, M, N, ldc, 3) - ref) <= bound, path
+        assert np.array_equal(got[:3], C[:3]), path
+    ints = lambda n: (rng.integers(-30, 31, n) + 1j * rng.integers(-30, 31, n)).astype(np.complex128)
+    Ai, Bi, Ci = ints(A.size), ints(B.size), ints(C.size)
+    exp, _ = O.gemm(O.COL, ta, tb, M, N, K, (2 - 1j), Ai, lda, Bi, ldb, (1 + 1j), Ci, ldc, 1, 2,
+                    3, want_ref=False)
+    for dmma in (1, 0):
+        assert hb.set_tuning(handle, "dgemm_dmma", dmma) == 0
+        try:
+            dA, dB, dC = (hb.DeviceArray(handle, X) for X in (Ai, Bi, Ci))
+            assert hb.lib_gemm(handle, O.COL, "ntc"[ta], "ntc"[tb], M, N, K, (2 - 1j), dA, lda,
+                               dB, ldb, (1 + 1j), dC, ldc, 1, 2, 3) == 0
+            assert np.array_equal(dC.download(), exp), dmma
+        finally:
+            hb.set_tuning(handle, "dgemm_dmma", 1)

@@ -480,7 +480,7 @@ def test_zgemm_crt_vs_native_accuracy(handle):
             O.view_c(dC.download(), O.COL, M, N, M), ref)
     hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
     print("zgemm native vs crt:", errs)
-    native = [v for k, v in errs.items() if k.startswith("simt")][0]
+    native = [v for k, v in errs.items() if k.startswith(("simt", "dmma"))][0]
     crt = [v for k, v in errs.items() if k.startswith("tc.zcrt")][0]
     assert crt <= native
 
