@@ -1141,12 +1141,17 @@ extern "C" int hcbk_encode_tma_2d(void *map, int bf16, const void *base, uint64_
 /* 2-D map over a column-major C {rows, cols} of esz-byte elements, column
  * pitch ld elements; box {32, 32}, no swizzle.  HCBK_ERR_ALIGN when C is not
  * TMA-addressable (base not 16-byte aligned, pitch not a multiple of 16
- * bytes). */
+ * bytes) or when a column is not a whole number of 16-byte chunks: measured
+ * on B200, a tensor store whose box crosses the end of the rows writes the
+ * rest of the 16-byte chunk holding the last row, which would overwrite the
+ * leading-dimension padding below row `rows` (C outside the M x N window
+ * must stay untouched). */
 static int make_map_out(CUtensorMap *map, CUtensorMapDataType dt, uint32_t esz, void *base,
                         uint64_t rows, uint64_t cols, uint64_t ld) {
   auto fn = encode_fn();
   if (!fn) return HCBK_ERR_DRIVER;
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * esz) & 15) || rows == 0 || cols == 0)
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * esz) & 15) || ((rows * esz) & 15) ||
+      rows == 0 || cols == 0)
     return HCBK_ERR_ALIGN;
   cuuint64_t dims[2] = {rows, cols};
   cuuint64_t strides[1] = {ld * esz};

@@ -487,7 +487,7 @@ def test_zgemm_crt_vs_native_accuracy(handle):
 
 @pytest.mark.parametrize("kind,mode,param,prefix", [("d", hb.HCBLAS_MATH_OZAKI_CRT, 0, "tc.crt_m"),
                                                     ("z", hb.HCBLAS_MATH_OZAKI_CRT, 0, "tc.zcrt3m_m"),
-                                                    ("s", hb.HCBLAS_MATH_SPLIT_BF16, 6, "tc.split_bf16x6"),
+                                                    ("s", hb.HCBLAS_MATH_SPLIT_BF16, 6, "tc.s.grouped_split_bf16x6"),
                                                     ("c", hb.HCBLAS_MATH_SPLIT_BF16, 6, "tc.csplit3m_bf16x6")])
 def test_strided_batch_uses_emulated_mode(handle, kind, mode, param, prefix):
     """A strided batch under an emulated math mode runs every element on the
