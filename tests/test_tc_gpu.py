@@ -213,28 +213,31 @@ def test_tc_epilogue_keeps_ld_padding(handle, kind, M, ldc):
     rng = np.random.default_rng(M + ldc)
     N, K = 70, 96
     dt = np.float16 if kind == "h" else np.float32
-    A = rng.uniform(-1, 1, M * K).astype(dt)
+    lda = -(-M // 8) * 8  # a leading dimension TMA can address
+    A = rng.uniform(-1, 1, lda * K).astype(dt)
     B = rng.uniform(-1, 1, K * N).astype(dt)
     C = rng.uniform(-1, 1, ldc * N).astype(dt)
     mode = hb.HCBLAS_MATH_NATIVE if kind == "h" else hb.HCBLAS_MATH_SPLIT_BF16
     assert hb.hcblasSetMathMode(handle, mode, 6 if kind == "s" else 0) == 0
     try:
         dA, dB, dC = (hb.DeviceArray(handle, X) for X in (A, B, C))
-        assert hb.lib_gemm(handle, O.COL, "n", "n", M, N, K, 1.0, dA, M, dB, K, 0.5, dC, ldc) == 0
+        assert hb.lib_gemm(handle, O.COL, "n", "n", M, N, K, 1.0, dA, lda, dB, K, 0.5, dC,
+                           ldc) == 0
         assert hb.device_error(handle) == 0
         assert hb.hcblasGetLastPath(handle).startswith("tc."), hb.hcblasGetLastPath(handle)
         got = dC.download()
     finally:
         hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
     assert np.array_equal(got.reshape(N, ldc)[:, M:], C.reshape(N, ldc)[:, M:])
-    _, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A, M, B, K, 0.5, C, ldc)
+    _, ref = O.gemm(O.COL, 0, 0, M, N, K, 1.0, A, lda, B, K, 0.5, C, ldc)
     tol = 2e-3 if kind == "h" else 1e-5
     assert O.normwise_rel_error(O.view_c(got, O.COL, M, N, ldc).astype(np.float64), ref) < tol
     if kind == "h":  # the grouped kernel on the same problem
         dC.upload(C)
-        p = hb.GemmProblem(0, 0, M, N, K, dA.ptr, M if M % 8 == 0 else -(-M // 8) * 8, dB.ptr, K,
-                           dC.ptr, ldc)
-        if M % 8 == 0:
-            assert hb.hgemm_grouped(handle, [p], 1.0, 0.5) == 0
-            got = dC.download()
-            assert np.array_equal(got.reshape(N, ldc)[:, M:], C.reshape(N, ldc)[:, M:])
+        p = hb.GemmProblem(0, 0, M, N, K, dA.ptr, lda, dB.ptr, K, dC.ptr, ldc)
+        assert hb.hgemm_grouped(handle, [p], 1.0, 0.5) == 0
+        assert hb.hcblasGetLastPath(handle) == "tc.h.grouped"
+        got = dC.download()
+        assert np.array_equal(got.reshape(N, ldc)[:, M:], C.reshape(N, ldc)[:, M:])
+        assert O.normwise_rel_error(O.view_c(got, O.COL, M, N, ldc).astype(np.float64),
+                                    ref) < tol
