@@ -741,9 +741,10 @@ extern "C" int hcbk_grouped_encode(hcbk_grouped_entry *e, int op_a, int op_b, in
   if (m <= 0 || n <= 0 || k <= 0 || m > 0x7fffffff || n > 0x7fffffff || k > 0x7fffffff)
     return HCBK_ERR_ARGS;
   memset(e, 0, sizeof(*e));
-  /* the tile width that pads N least (ties: the wider) */
-  const int64_t w64 = (n + 63) / 64 * 64, w128 = (n + 127) / 128 * 128;
-  e->bn = w64 < w128 ? 64 : 128;
+  /* 64-wide tiles for problems no wider than 64 (half the tensor work of a
+   * 128-wide tile for the same one tile); wider problems keep 128-wide tiles,
+   * since more, narrower tiles re-read A once per tile column */
+  e->bn = n <= 64 ? 64 : 128;
   e->a_mn = op_a == HCBK_OP_N; /* op(A) = A: column-major M x K, M contiguous */
   e->b_mn = op_b != HCBK_OP_N; /* op(B) = B^T: N contiguous */
   int rc = e->a_mn ? hcbk_encode_tma_2d(e->map_a, 0, a, m, k, lda, 64, 64)
