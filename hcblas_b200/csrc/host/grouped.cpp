@@ -166,21 +166,30 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     std::stable_sort(ok_idx.begin(), ok_idx.end(),
                      [&](int x, int y) { return work(x) > work(y); });
     const int nt = (int)ok_idx.size();
+    if (nt >= (1 << 24)) return HCBK_ERR_ARGS;
+    int64_t total = 0;
+    for (int j = 0; j < nt; ++j) {
+      total += (int64_t)hcbk_grouped_tiles(&ent[ok_idx[j]]);
+      if (total > 0x7fffffff) return HCBK_ERR_ARGS;
+    }
+    /* table: entries | tile prefix sums | per-tile descriptors */
     const size_t ent_bytes = sizeof(hcbk_grouped_entry) * (size_t)nt;
     const size_t ts_off = (ent_bytes + 255) & ~size_t(255);
-    const size_t bytes = ts_off + sizeof(int32_t) * ((size_t)nt + 1);
-    int64_t total = 0;
+    const size_t td_off = (ts_off + sizeof(int32_t) * ((size_t)nt + 1) + 255) & ~size_t(255);
+    const size_t bytes = td_off + 4 * sizeof(int32_t) * (size_t)total;
+    total = 0;
     if (nt > 0) {
       if (!ensure_table(gp, bytes, stream) || !ensure_staging(gp, bytes)) return HCBK_ERR_NOMEM;
       unsigned char *stg = static_cast<unsigned char *>(gp.staging);
       auto *dst = reinterpret_cast<hcbk_grouped_entry *>(stg);
       auto *ts = reinterpret_cast<int32_t *>(stg + ts_off);
+      auto *td = reinterpret_cast<int32_t *>(stg + td_off);
       for (int j = 0; j < nt; ++j) {
         const hcbk_grouped_entry &e = ent[ok_idx[j]];
         std::memcpy(&dst[j], &e, sizeof(e));
         ts[j] = (int32_t)total;
+        hcbk_grouped_fill_tiles(&e, j, td + 4 * total);
         total += (int64_t)hcbk_grouped_tiles(&e);
-        if (total > 0x7fffffff) return HCBK_ERR_ARGS;
       }
       ts[nt] = (int32_t)total;
       if (cudaMemcpyAsync(gp.table, stg, bytes, cudaMemcpyHostToDevice,
@@ -199,6 +208,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     gp.count = nt;
     gp.total_tiles = (int)total;
     gp.tile_start_offset = ts_off;
+    gp.tile_desc_offset = td_off;
     gp.fallback = fallback;
     gp.key = key;
   }
@@ -215,6 +225,10 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     g.alpha = alpha;
     g.beta = beta;
     g.device_maps = 0;
+    g.tile_desc =
+        reinterpret_cast<const int32_t *>(static_cast<char *>(gp.table) + gp.tile_desc_offset);
+    g.uniform_tiles = 0;
+    g.u_tiles_m = g.u_k = g.u_flags = 0;
     int rc = timed_launch(st, stream, "tc.h.grouped",
                           [&] { return hcbk_hgemm_grouped_tc(&g, err, stream); });
     if (rc) return rc;
@@ -340,6 +354,7 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
       e.n = (int32_t)c.n;
       e.k = (int32_t)c.k;
       e.tiles_m = (int32_t)((c.m + 127) / 128);
+      e.bn = 128; /* the split kernel's tile: 128 x 128 over K-major planes */
       /* op(A) rows m: column-major A is M-contiguous for N, K-contiguous for T;
        * op(B) rows n: B is K-contiguous for N, N-contiguous for T */
       for (int side = 0; side < 2; ++side) {
@@ -364,26 +379,34 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
     };
     std::stable_sort(order_idx.begin(), order_idx.end(),
                      [&](int x, int y) { return work(x) > work(y); });
-    /* table: entries | tile prefix | pack jobs | pack tile prefix */
+    if (count >= (1 << 24)) return HCBK_ERR_ARGS;
+    int64_t total_est = 0;
+    for (int i = 0; i < count; ++i) {
+      total_est += (int64_t)hcbk_grouped_tiles(&ent[i]);
+      if (total_est > 0x7fffffff) return HCBK_ERR_ARGS;
+    }
+    /* table: entries | tile prefix | pack jobs | pack tile prefix | tile descriptors */
     const size_t ent_bytes = sizeof(hcbk_grouped_entry) * (size_t)count;
     const size_t ts_off = (ent_bytes + 255) & ~size_t(255);
     const size_t job_off = (ts_off + sizeof(int32_t) * ((size_t)count + 1) + 255) & ~size_t(255);
     const size_t njobs = (size_t)count * 2;
     const size_t jts_off = (job_off + sizeof(hcbk_gpack_job) * njobs + 255) & ~size_t(255);
-    const size_t bytes = jts_off + sizeof(int32_t) * (njobs + 1);
+    const size_t td_off = (jts_off + sizeof(int32_t) * (njobs + 1) + 255) & ~size_t(255);
+    const size_t bytes = td_off + 4 * sizeof(int32_t) * (size_t)total_est;
     if (!ensure_table(gp, bytes, stream) || !ensure_staging(gp, bytes)) return HCBK_ERR_NOMEM;
     unsigned char *stg = static_cast<unsigned char *>(gp.staging);
     auto *dst = reinterpret_cast<hcbk_grouped_entry *>(stg);
     auto *ts = reinterpret_cast<int32_t *>(stg + ts_off);
     auto *jdst = reinterpret_cast<hcbk_gpack_job *>(stg + job_off);
     auto *jts = reinterpret_cast<int32_t *>(stg + jts_off);
+    auto *td = reinterpret_cast<int32_t *>(stg + td_off);
     int64_t total = 0;
     for (int x = 0; x < count; ++x) {
       const hcbk_grouped_entry &e = ent[order_idx[x]];
       std::memcpy(&dst[x], &e, sizeof(e));
       ts[x] = (int32_t)total;
-      total += (int64_t)e.tiles_m * ((e.n + 127) / 128);
-      if (total > 0x7fffffff) return HCBK_ERR_ARGS;
+      hcbk_grouped_fill_tiles(&e, x, td + 4 * total);
+      total += (int64_t)hcbk_grouped_tiles(&e);
     }
     ts[count] = (int32_t)total;
     int64_t ptotal = 0;
@@ -413,6 +436,7 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
     gp.pack_tiles = (int)ptotal;
     gp.pack_offset = job_off;
     gp.pack_ts_offset = jts_off;
+    gp.tile_desc_offset = td_off;
     gp.fallback.clear();
     gp.key = key;
   }
@@ -444,6 +468,9 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
   g.alpha = alpha;
   g.beta = beta;
   g.device_maps = 0;
+  g.tile_desc = reinterpret_cast<const int32_t *>(tb + gp.tile_desc_offset);
+  g.uniform_tiles = 0;
+  g.u_tiles_m = g.u_k = g.u_flags = 0;
   const char *path = terms == 6 ? "tc.s.grouped_split_bf16x6" : "tc.s.grouped_split_bf16x3";
   rc = timed_launch(st, stream, path,
                     [&] { return hcbk_sgemm_grouped_split_tc(&g, terms, err, stream); });

@@ -36,6 +36,7 @@ struct HcblasGroupedPlan {
   int count = 0;       /* problems in the device table */
   int total_tiles = 0;
   size_t tile_start_offset = 0;
+  size_t tile_desc_offset = 0; /* per-tile descriptors (hcbk_grouped_fill_tiles) */
   std::vector<int> fallback; /* problems the table cannot hold (TMA alignment) */
   /* split-BF16 SGEMM plans only: the bf16 planes of every problem (device),
    * and the pack jobs' place in the table */

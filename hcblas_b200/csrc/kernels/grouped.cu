@@ -50,8 +50,12 @@ static_assert(SMEM_BYTES <= 232448, "shared memory");
 struct Params {
   const hcbk_grouped_entry *table;
   const int32_t *tile_start;
+  const int4 *tile_desc; /* per tile: problem | flags << 24, tm, tn, k (host tables) */
   int count;
   int total_tiles;
+  /* uniform batches (device-built tables): every problem has uniform_tiles
+   * tiles of this shape; per-problem c_tma / skip come from the entries */
+  int uniform_tiles, u_tiles_m, u_k, u_flags;
   float alpha, beta;
   int beta_nonzero;
   int device_maps; /* the table's maps were patched on the device: acquire them */
@@ -72,14 +76,23 @@ __device__ __forceinline__ int find_problem(const int32_t *ts, int count, int t)
 struct TileRef {
   const hcbk_grouped_entry *e;
   int tm, tn;
+  int k;
+  int flags; /* HCBK_GT_* */
 };
 
+/* One 16-byte load per tile (host tables) or arithmetic (uniform batches):
+ * a binary search over the tile prefix sums costs a dozen dependent global
+ * loads per tile and role, which dominated small tiles. */
 __device__ __forceinline__ TileRef tile_ref(const Params &p, int t) {
-  const int g = find_problem(p.tile_start, p.count, t);
-  const hcbk_grouped_entry *e = p.table + g;
-  const int lt = t - __ldg(p.tile_start + g);
-  const int tiles_m = __ldg(&e->tiles_m);
-  return TileRef{e, lt % tiles_m, lt / tiles_m};
+  if (p.uniform_tiles > 0) {
+    const int g = t / p.uniform_tiles, lt = t - g * p.uniform_tiles;
+    const hcbk_grouped_entry *e = p.table + g;
+    const int flags = p.u_flags | (__ldg(&e->c_tma) ? HCBK_GT_CTMA : 0) |
+                      (__ldg(&e->skip) ? HCBK_GT_SKIP : 0);
+    return TileRef{e, lt % p.u_tiles_m, lt / p.u_tiles_m, p.u_k, flags};
+  }
+  const int4 d = __ldg(p.tile_desc + t);
+  return TileRef{p.table + (d.x & 0xffffff), d.y, d.z, d.w, (int)((unsigned)d.x >> 24)};
 }
 
 /*
@@ -135,16 +148,16 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       bool ok = true;
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
         const TileRef r = tile_ref(p, t);
-        if (__ldg(&r.e->skip)) continue;
+        if (r.flags & HCBK_GT_SKIP) continue;
         const CUtensorMap *ma = reinterpret_cast<const CUtensorMap *>(r.e->map_a);
         const CUtensorMap *mb = reinterpret_cast<const CUtensorMap *>(r.e->map_b);
         if (p.device_maps) {
           tensormap_acquire(ma);
           tensormap_acquire(mb);
         }
-        const int k = __ldg(&r.e->k);
-        const int bn = __ldg(&r.e->bn);
-        const int a_mn = __ldg(&r.e->a_mn), b_mn = __ldg(&r.e->b_mn);
+        const int k = r.k;
+        const int bn = (r.flags & HCBK_GT_BN64) ? 64 : 128;
+        const int a_mn = r.flags & HCBK_GT_AMN, b_mn = r.flags & HCBK_GT_BMN;
         const int kblocks = (k + BK - 1) / BK;
         const uint32_t bytes = A_BYTES + (uint32_t)bn * 128u;
         for (int kb = 0; kb < kblocks; ++kb) {
@@ -184,10 +197,10 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       bool ok = true;
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
         const TileRef r = tile_ref(p, t);
-        if (__ldg(&r.e->skip)) continue;
-        const int k = __ldg(&r.e->k);
-        const int bn = __ldg(&r.e->bn);
-        const bool a_mn = __ldg(&r.e->a_mn) != 0, b_mn = __ldg(&r.e->b_mn) != 0;
+        if (r.flags & HCBK_GT_SKIP) continue;
+        const int k = r.k;
+        const int bn = (r.flags & HCBK_GT_BN64) ? 64 : 128;
+        const bool a_mn = (r.flags & HCBK_GT_AMN) != 0, b_mn = (r.flags & HCBK_GT_BMN) != 0;
         const int kblocks = (k + BK - 1) / BK;
         const uint32_t idesc = make_idesc(1, 0, a_mn, b_mn, BM, (uint32_t)bn);
         const uint32_t a_lbo = a_mn ? BK * 128 : 16, b_lbo = b_mn ? BK * 128 : 16;
@@ -231,9 +244,10 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
     int ci = 0;
     for (int t = blockIdx.x; t < p.total_tiles; t += gridDim.x) {
       const TileRef r = tile_ref(p, t);
-      if (__ldg(&r.e->skip)) continue;
-      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n), bn = __ldg(&r.e->bn);
-      const bool c_tma = __ldg(&r.e->c_tma) != 0;
+      if (r.flags & HCBK_GT_SKIP) continue;
+      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n);
+      const int bn = (r.flags & HCBK_GT_BN64) ? 64 : 128;
+      const bool c_tma = (r.flags & HCBK_GT_CTMA) != 0;
       const CUtensorMap *mc = reinterpret_cast<const CUtensorMap *>(r.e->map_c);
       const long long ldc = __ldg(&r.e->ldc);
       __half *C = static_cast<__half *>(r.e->c);
@@ -460,7 +474,7 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
         const TileRef r = tile_ref(p, t);
         const CUtensorMap *ma = reinterpret_cast<const CUtensorMap *>(r.e->map_a);
         const CUtensorMap *mb = reinterpret_cast<const CUtensorMap *>(r.e->map_b);
-        const int kblocks = (__ldg(&r.e->k) + BK - 1) / BK;
+        const int kblocks = (r.k + BK - 1) / BK;
         for (int kb = 0; kb < kblocks; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, p.err, ERR_TIMEOUT_PRODUCER)) {
             ok = false;
@@ -492,7 +506,7 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
       bool ok = true;
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
         const TileRef r = tile_ref(p, t);
-        const int kblocks = (__ldg(&r.e->k) + BK - 1) / BK;
+        const int kblocks = (r.k + BK - 1) / BK;
         for (int kb = 0; ok && kb < kblocks; ++kb, ++ci) {
           const int b = ci & 1;
           if (!mbar_wait(&tempty[b], ((ci >> 1) & 1) ^ 1u, p.err, ERR_TIMEOUT_MMA_TMEM)) {
@@ -535,7 +549,7 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
     for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
       const TileRef r = tile_ref(p, t);
       const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n);
-      const int kblocks = (__ldg(&r.e->k) + BK - 1) / BK;
+      const int kblocks = (r.k + BK - 1) / BK;
       float acc[BN];
 #pragma unroll
       for (int j = 0; j < BN; ++j) acc[j] = 0.f;
@@ -768,6 +782,24 @@ extern "C" int hcbk_grouped_tiles(const hcbk_grouped_entry *e) {
   return e->tiles_m * (int)((e->n + e->bn - 1) / e->bn);
 }
 
+extern "C" int hcbk_grouped_tile_flags(const hcbk_grouped_entry *e) {
+  return (e->bn == 64 ? HCBK_GT_BN64 : 0) | (e->a_mn ? HCBK_GT_AMN : 0) |
+         (e->b_mn ? HCBK_GT_BMN : 0) | (e->c_tma ? HCBK_GT_CTMA : 0) |
+         (e->skip ? HCBK_GT_SKIP : 0);
+}
+
+extern "C" void hcbk_grouped_fill_tiles(const hcbk_grouped_entry *e, int problem, int32_t *desc) {
+  const int tiles = hcbk_grouped_tiles(e);
+  const int flags = hcbk_grouped_tile_flags(e);
+  for (int lt = 0; lt < tiles; ++lt) {
+    int32_t *d = desc + 4 * lt;
+    d[0] = (int32_t)((unsigned)problem | ((unsigned)flags << 24));
+    d[1] = lt % e->tiles_m;
+    d[2] = lt / e->tiles_m;
+    d[3] = e->k;
+  }
+}
+
 extern "C" int hcbk_grouped_ptr_table(const hcbk_grouped_entry *tmpl, hcbk_grouped_entry *table,
                                       int32_t *tile_start, int32_t *skip,
                                       const void *const *a_arr, const void *const *b_arr,
@@ -818,8 +850,13 @@ extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void 
   Params p;
   p.table = g->table;
   p.tile_start = g->tile_start;
+  p.tile_desc = reinterpret_cast<const int4 *>(g->tile_desc);
   p.count = g->count;
   p.total_tiles = g->total_tiles;
+  p.uniform_tiles = g->uniform_tiles;
+  p.u_tiles_m = g->u_tiles_m;
+  p.u_k = g->u_k;
+  p.u_flags = g->u_flags;
   p.alpha = g->alpha;
   p.beta = g->beta;
   p.beta_nonzero = g->beta != 0.0f;
@@ -859,8 +896,11 @@ int launch_grouped_split(const hcbk_grouped_args *g, int *err, void *stream) {
   Params p;
   p.table = g->table;
   p.tile_start = g->tile_start;
+  p.tile_desc = reinterpret_cast<const int4 *>(g->tile_desc);
   p.count = g->count;
   p.total_tiles = g->total_tiles;
+  p.uniform_tiles = 0;
+  p.u_tiles_m = p.u_k = p.u_flags = 0;
   p.alpha = g->alpha;
   p.beta = g->beta;
   p.beta_nonzero = g->beta != 0.0f;

@@ -478,6 +478,19 @@ int hcbk_encode_out_2d(void *map, void *base, uint64_t rows, uint64_t cols, uint
 /* tiles of an encoded problem: tiles_m * ceil(n / bn) */
 int hcbk_grouped_tiles(const hcbk_grouped_entry *e);
 
+/* Per-tile descriptors of the grouped kernels (host tables): four int32 per
+ * tile {problem | flags << 24, tile row, tile column, k}; problem < 2^24. */
+enum {
+  HCBK_GT_BN64 = 1, /* 64-wide tiles */
+  HCBK_GT_AMN = 2,  /* op(A) MN-major */
+  HCBK_GT_BMN = 4,  /* op(B) MN-major */
+  HCBK_GT_CTMA = 8, /* C through tensor stores */
+  HCBK_GT_SKIP = 16 /* not computed by the grouped kernel */
+};
+int hcbk_grouped_tile_flags(const hcbk_grouped_entry *e);
+/* the descriptors of every tile of problem `problem` (entry e) into desc */
+void hcbk_grouped_fill_tiles(const hcbk_grouped_entry *e, int problem, int32_t *desc);
+
 /* Device-side table of a uniform pointer-array batch: entry i is *tmpl with
  * the addresses of its maps replaced by a_arr[i] + a_off_bytes +
  * i * a_stride_bytes etc. (on the
@@ -502,6 +515,9 @@ typedef struct hcbk_grouped_args {
   int32_t total_tiles;
   float alpha, beta;
   int32_t device_maps; /* the table's maps were patched on the device */
+  const int32_t *tile_desc; /* device, 4 int32 per tile (host tables), or NULL with: */
+  int32_t uniform_tiles;    /* > 0: every problem has this many tiles, of shape: */
+  int32_t u_tiles_m, u_k, u_flags;
 } hcbk_grouped_args;
 int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
 
