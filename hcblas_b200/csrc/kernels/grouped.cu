@@ -95,6 +95,24 @@ __device__ __forceinline__ TileRef tile_ref(const Params &p, int t) {
   return TileRef{p.table + (d.x & 0xffffff), d.y, d.z, d.w, (int)((unsigned)d.x >> 24)};
 }
 
+/* what the epilogue needs of a tile: its descriptor and the problem's C */
+struct EpiRef {
+  TileRef r;
+  int m, n;
+  long long ldc;
+  void *c;
+};
+
+__device__ __forceinline__ EpiRef epi_ref(const Params &p, int t) {
+  EpiRef x;
+  x.r = tile_ref(p, t);
+  x.m = __ldg(&x.r.e->m);
+  x.n = __ldg(&x.r.e->n);
+  x.ldc = __ldg(&x.r.e->ldc);
+  x.c = x.r.e->c;
+  return x;
+}
+
 /*
  * Per problem the tile is 128 x bn with bn = 64 or 128 (the entry's choice:
  * the width that pads N least), so narrow problems do not spend tensor work
@@ -146,8 +164,11 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
+      /* the next tile's descriptor is loaded while this tile's loads go out */
+      TileRef nr = blockIdx.x < p.total_tiles ? tile_ref(p, blockIdx.x) : TileRef{};
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
-        const TileRef r = tile_ref(p, t);
+        const TileRef r = nr;
+        if (t + (int)gridDim.x < p.total_tiles) nr = tile_ref(p, t + gridDim.x);
         if (r.flags & HCBK_GT_SKIP) continue;
         const CUtensorMap *ma = reinterpret_cast<const CUtensorMap *>(r.e->map_a);
         const CUtensorMap *mb = reinterpret_cast<const CUtensorMap *>(r.e->map_b);
@@ -195,8 +216,10 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
       uint32_t ph = 0;
       int ci = 0; /* tiles computed by this CTA: selects the TMEM buffer */
       bool ok = true;
+      TileRef nr = blockIdx.x < p.total_tiles ? tile_ref(p, blockIdx.x) : TileRef{};
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
-        const TileRef r = tile_ref(p, t);
+        const TileRef r = nr;
+        if (t + (int)gridDim.x < p.total_tiles) nr = tile_ref(p, t + gridDim.x);
         if (r.flags & HCBK_GT_SKIP) continue;
         const int k = r.k;
         const int bn = (r.flags & HCBK_GT_BN64) ? 64 : 128;
@@ -242,15 +265,20 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
     uint32_t lphase = 0; /* bit x: parity of box x's next C load */
     uint32_t pend = 0;   /* bit x: a C load into box x did not complete in time */
     int ci = 0;
+    /* the next tile's descriptor and C geometry are loaded while this tile
+     * waits for its accumulator */
+    EpiRef nx = blockIdx.x < p.total_tiles ? epi_ref(p, blockIdx.x) : EpiRef{};
     for (int t = blockIdx.x; t < p.total_tiles; t += gridDim.x) {
-      const TileRef r = tile_ref(p, t);
+      const EpiRef x0 = nx;
+      if (t + (int)gridDim.x < p.total_tiles) nx = epi_ref(p, t + gridDim.x);
+      const TileRef &r = x0.r;
       if (r.flags & HCBK_GT_SKIP) continue;
-      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n);
+      const int pm = x0.m, pn = x0.n;
       const int bn = (r.flags & HCBK_GT_BN64) ? 64 : 128;
       const bool c_tma = (r.flags & HCBK_GT_CTMA) != 0;
       const CUtensorMap *mc = reinterpret_cast<const CUtensorMap *>(r.e->map_c);
-      const long long ldc = __ldg(&r.e->ldc);
-      __half *C = static_cast<__half *>(r.e->c);
+      const long long ldc = x0.ldc;
+      __half *C = static_cast<__half *>(x0.c);
       const int b = ci & 1;
       const uint32_t tph = (ci >> 1) & 1;
       ++ci;
@@ -470,8 +498,10 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
+      TileRef nr = blockIdx.x < p.total_tiles ? tile_ref(p, blockIdx.x) : TileRef{};
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
-        const TileRef r = tile_ref(p, t);
+        const TileRef r = nr;
+        if (t + (int)gridDim.x < p.total_tiles) nr = tile_ref(p, t + gridDim.x);
         const CUtensorMap *ma = reinterpret_cast<const CUtensorMap *>(r.e->map_a);
         const CUtensorMap *mb = reinterpret_cast<const CUtensorMap *>(r.e->map_b);
         const int kblocks = (r.k + BK - 1) / BK;
@@ -504,8 +534,10 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
       uint32_t ph = 0;
       int ci = 0; /* 64-K slabs so far: selects the TMEM buffer */
       bool ok = true;
+      TileRef nr = blockIdx.x < p.total_tiles ? tile_ref(p, blockIdx.x) : TileRef{};
       for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
-        const TileRef r = tile_ref(p, t);
+        const TileRef r = nr;
+        if (t + (int)gridDim.x < p.total_tiles) nr = tile_ref(p, t + gridDim.x);
         const int kblocks = (r.k + BK - 1) / BK;
         for (int kb = 0; ok && kb < kblocks; ++kb, ++ci) {
           const int b = ci & 1;
@@ -546,9 +578,12 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
     const int q = warp & 3; /* TMEM lane quadrant */
     int ci = 0;
     bool ok = true;
+    EpiRef nx = blockIdx.x < p.total_tiles ? epi_ref(p, blockIdx.x) : EpiRef{};
     for (int t = blockIdx.x; ok && t < p.total_tiles; t += gridDim.x) {
-      const TileRef r = tile_ref(p, t);
-      const int pm = __ldg(&r.e->m), pn = __ldg(&r.e->n);
+      const EpiRef x0 = nx;
+      if (t + (int)gridDim.x < p.total_tiles) nx = epi_ref(p, t + gridDim.x);
+      const TileRef &r = x0.r;
+      const int pm = x0.m, pn = x0.n;
       const int kblocks = (r.k + BK - 1) / BK;
       float acc[BN];
 #pragma unroll
@@ -588,8 +623,8 @@ __global__ void __launch_bounds__(192, 1) grouped_split_kernel(const __grid_cons
       const int m = r.tm * BM + q * 32 + lane;
       const int n0 = r.tn * BN;
       if (m < pm) {
-        const long long ldc = __ldg(&r.e->ldc);
-        float *C = static_cast<float *>(r.e->c) + (long long)m + (long long)n0 * ldc;
+        const long long ldc = x0.ldc;
+        float *C = static_cast<float *>(x0.c) + (long long)m + (long long)n0 * ldc;
 #pragma unroll
         for (int c = 0; c < BN; c += 32) {
           const int nvalid = pn - (n0 + c);
