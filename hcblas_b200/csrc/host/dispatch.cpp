@@ -878,6 +878,7 @@ int hgemm_ptr_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *stream
   g.u_tiles_m = tmpl.tiles_m;
   g.u_k = tmpl.k;
   g.u_flags = hcbk_grouped_tile_flags(&tmpl) & (HCBK_GT_BN64 | HCBK_GT_AMN | HCBK_GT_BMN);
+  g.ctas_per_sm = st->grouped_ctas;
   if ((int64_t)hcbk_grouped_tiles(&tmpl) * count > 0x7fffffff) return HCBK_ERR_ARGS;
   rc = timed_launch(st, stream, "tc.h.grouped.ptr",
                     [&] { return hcbk_hgemm_grouped_tc(&g, err, stream); });

@@ -229,6 +229,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
         reinterpret_cast<const int32_t *>(static_cast<char *>(gp.table) + gp.tile_desc_offset);
     g.uniform_tiles = 0;
     g.u_tiles_m = g.u_k = g.u_flags = 0;
+    g.ctas_per_sm = st->grouped_ctas;
     int rc = timed_launch(st, stream, "tc.h.grouped",
                           [&] { return hcbk_hgemm_grouped_tc(&g, err, stream); });
     if (rc) return rc;
@@ -471,6 +472,7 @@ int grouped_sgemm_split(HcblasB200State *st, void *stream, hcblasOrder order, in
   g.tile_desc = reinterpret_cast<const int32_t *>(tb + gp.tile_desc_offset);
   g.uniform_tiles = 0;
   g.u_tiles_m = g.u_k = g.u_flags = 0;
+  g.ctas_per_sm = 1;
   const char *path = terms == 6 ? "tc.s.grouped_split_bf16x6" : "tc.s.grouped_split_bf16x3";
   rc = timed_launch(st, stream, path,
                     [&] { return hcbk_sgemm_grouped_split_tc(&g, terms, err, stream); });

@@ -487,6 +487,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->crt_i8 = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "grouped_ctas") == 0) {
+    if (value != 1 && value != 2) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->grouped_ctas = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   if (std::strcmp(name, "dgemm_dmma") == 0) {
     if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
     handle->impl->dgemm_dmma = value;

@@ -37,15 +37,25 @@ namespace grouped {
 using namespace hcbk::tc;
 
 constexpr int BM = 128, BN = 128, BK = 64; /* BK f16 = one 128-byte swizzle atom */
-constexpr int STAGES = 6;
 constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128;
 constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES; /* stage slot sized for 128-wide tiles */
 constexpr uint32_t OUT_BOX = 32 * 32 * 2;           /* one f16 32 x 32 C box */
-constexpr uint32_t OUT_OFF = STAGES * STAGE_BYTES;  /* 4 epilogue warps x 2 boxes */
-constexpr uint32_t BAR_OFF = OUT_OFF + 8 * OUT_BOX;
-constexpr uint32_t SMEM_BYTES = BAR_OFF + 256 + 1024;
 constexpr uint32_t TMEM_COLS = 2 * BN;
-static_assert(SMEM_BYTES <= 232448, "shared memory");
+
+/* Shared-memory layout of the grouped HGEMM for a ring of STG stages: the
+ * stages, the epilogue's C boxes (4 warps x 2), the barriers.  MINB CTAs per
+ * SM: one CTA with a 6-stage ring, or two with 3 stages each, whose tile
+ * pipelines then hide each other's per-tile latencies. */
+template <int STG, int MINB>
+struct GCfg {
+  static constexpr int STAGES = STG;
+  static constexpr int NBOX = MINB == 1 ? 2 : 1; /* C boxes per epilogue warp */
+  static constexpr uint32_t OUT_OFF = STG * STAGE_BYTES;
+  static constexpr uint32_t BAR_OFF = OUT_OFF + 4 * NBOX * OUT_BOX;
+  static constexpr uint32_t SMEM_BYTES = BAR_OFF + 256 + 1024;
+  static_assert(SMEM_BYTES * MINB + 1024 * MINB <= 233472, "shared memory per SM");
+  static_assert(TMEM_COLS * MINB <= 512, "TMEM per SM");
+};
 
 struct Params {
   const hcbk_grouped_entry *table;
@@ -123,7 +133,12 @@ __device__ __forceinline__ EpiRef epi_ref(const Params &p, int t) {
  * entry flagged `skip` (operands TMA cannot address, found by the
  * device-side table builder) is passed over by every role alike.
  */
-__global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_constant__ Params p) {
+template <int STG, int MINB>
+__global__ void __launch_bounds__(192, MINB) grouped_hgemm_kernel(const __grid_constant__ Params p) {
+  using Cfg = GCfg<STG, MINB>;
+  constexpr int STAGES = Cfg::STAGES;
+  constexpr int NBOX = Cfg::NBOX;
+  constexpr uint32_t OUT_OFF = Cfg::OUT_OFF, BAR_OFF = Cfg::BAR_OFF;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -260,7 +275,7 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
   } else {
     /* ------------------------------------------------ epilogue -- */
     const int q = warp & 3; /* TMEM lane quadrant */
-    __half *boxes = reinterpret_cast<__half *>(smem + OUT_OFF) + q * 2 * (32 * 32);
+    __half *boxes = reinterpret_cast<__half *>(smem + OUT_OFF) + q * NBOX * (32 * 32);
     uint64_t *wbar = obar + 2 * q;
     uint32_t lphase = 0; /* bit x: parity of box x's next C load */
     uint32_t pend = 0;   /* bit x: a C load into box x did not complete in time */
@@ -295,10 +310,11 @@ __global__ void __launch_bounds__(192, 1) grouped_hgemm_kernel(const __grid_cons
         uint32_t v[32];
         tmem_ld_32x32b_x32(tbase + c, v);
         if (c_tma) {
-          const int x = (c >> 5) & 1;
+          const int x = NBOX == 2 ? (c >> 5) & 1 : 0;
           __half *box = boxes + x * (32 * 32); /* column-major 32 x 32, as C */
           if (lane == 0) {
-            bulk_wait_read<1>(); /* the store issued from this box two groups ago has read it */
+            /* the store issued from this box (NBOX groups ago) has read it */
+            bulk_wait_read<NBOX - 1>();
             if (p.beta_nonzero) {
               mbar_expect_tx(&wbar[x], OUT_BOX);
               tma_load_2d(box, mc, &wbar[x], m0, n0 + c);
@@ -870,15 +886,18 @@ extern "C" int hcbk_grouped_ptr_table(const hcbk_grouped_entry *tmpl, hcbk_group
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
-extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream) {
+namespace {
+template <int STG, int MINB>
+int launch_grouped_h(const hcbk_grouped_args *g, int *err, void *stream) {
   using namespace hcbk::grouped;
-  if (g->count <= 0 || g->total_tiles <= 0) return HCBK_ERR_ARGS;
+  using Cfg = GCfg<STG, MINB>;
+  auto kern = grouped_hgemm_kernel<STG, MINB>;
   static bool attr_set[64] = {false};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HCBK_ERR_LAUNCH;
   if (!attr_set[dev]) {
-    if (cudaFuncSetAttribute(grouped_hgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SMEM_BYTES) != cudaSuccess)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Cfg::SMEM_BYTES) != cudaSuccess)
       return HCBK_ERR_LAUNCH;
     attr_set[dev] = true;
   }
@@ -897,10 +916,17 @@ extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void 
   p.beta_nonzero = g->beta != 0.0f;
   p.device_maps = g->device_maps;
   p.err = err;
-  int grid = hcbk_sm_count();
+  int grid = hcbk_sm_count() * MINB;
   if (g->total_tiles < grid) grid = g->total_tiles;
-  grouped_hgemm_kernel<<<grid, 192, SMEM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
+  kern<<<grid, 192, Cfg::SMEM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+}  // namespace
+
+extern "C" int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream) {
+  if (g->count <= 0 || g->total_tiles <= 0) return HCBK_ERR_ARGS;
+  if (g->ctas_per_sm == 2) return launch_grouped_h<3, 2>(g, err, stream);
+  return launch_grouped_h<6, 1>(g, err, stream);
 }
 
 extern "C" int hcbk_grouped_pack(const hcbk_gpack_job *jobs, const int32_t *tile_start,

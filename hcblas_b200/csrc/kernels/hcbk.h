@@ -518,6 +518,7 @@ typedef struct hcbk_grouped_args {
   const int32_t *tile_desc; /* device, 4 int32 per tile (host tables), or NULL with: */
   int32_t uniform_tiles;    /* > 0: every problem has this many tiles, of shape: */
   int32_t u_tiles_m, u_k, u_flags;
+  int32_t ctas_per_sm; /* f16 kernel: 1 (6-stage ring) or 2 (3 stages each) */
 } hcbk_grouped_args;
 int hcbk_hgemm_grouped_tc(const hcbk_grouped_args *g, int *err, void *stream);
 

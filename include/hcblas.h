@@ -486,6 +486,9 @@ hcblasStatus_t hcblasPlanEmulation(int mode, int param, int bits, int dtype, lon
  *                       0 binary16 residue planes on the f16 tensor cores,
  *                       sums reduced mod p every 1024 K.  Both give
  *                       bit-identical results.
+ *   "grouped_ctas"      grouped / batched HGEMM kernel: 2 (default) CTAs per SM
+ *                       with 3-stage rings, whose per-tile latencies overlap,
+ *                       or 1 CTA per SM with a 6-stage ring.
  *   "dgemm_dmma"        native DGEMM and ZGEMM (HCBLAS_MATH_NATIVE): 1
  *                       (default) on the FP64 tensor path (warp-level
  *                       mma.sync .f64; ZGEMM as four real products), 0 on the

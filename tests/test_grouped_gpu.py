@@ -231,3 +231,18 @@ def test_sgemm_grouped_alpha_zero_and_status(handle):
     assert hb.sgemm_grouped(handle, probs + bad, 1.0, 0.0) == hb.HCBLAS_STATUS_INVALID_VALUE
     L = hb.lib()
     assert L.hcblasSgemmGrouped(None, 1, None, None, None) == hb.HCBLAS_STATUS_NOT_INITIALIZED
+
+
+@pytest.mark.parametrize("ctas", [1, 2])
+def test_grouped_kernel_configurations(handle, ctas):
+    """Both shapes of the grouped kernel (one CTA per SM with a 6-stage ring,
+    two with 3 stages each) give results within the bound, beta != 0."""
+    rng = np.random.default_rng(40 + ctas)
+    probs, host, dev = make_problems(handle, rng, 40)
+    assert hb.set_tuning(handle, "grouped_ctas", ctas) == 0
+    try:
+        assert hb.hgemm_grouped(handle, probs, 0.75, -1.5) == 0
+        assert hb.device_error(handle) == 0
+    finally:
+        hb.set_tuning(handle, "grouped_ctas", 2)
+    check(host, dev, 0.75, -1.5)
