@@ -208,16 +208,39 @@ __device__ __forceinline__ uint32_t residue2_s8(const Limbs2 &L, const ModPair &
 
 /* K-contiguous source: 8 consecutive k per thread, 16-byte (binary16) or
  * 8-byte (int8) plane stores */
+/* grid-stride walk over the (row, chunk) cells of a rows x chunks grid, the
+ * row and chunk kept by additions instead of a 64-bit division per step */
+struct GridWalk {
+  int64_t idx, r, c, dr, dc, chunks, stride;
+  __device__ __forceinline__ explicit GridWalk(int64_t chunks_) {
+    stride = (int64_t)gridDim.x * blockDim.x;
+    idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    chunks = chunks_;
+    r = idx / chunks;
+    c = idx % chunks;
+    dr = stride / chunks;
+    dc = stride % chunks;
+  }
+  __device__ __forceinline__ void next() {
+    idx += stride;
+    r += dr;
+    c += dc;
+    if (c >= chunks) {
+      c -= chunks;
+      ++r;
+    }
+  }
+};
+
 template <bool I8>
 __global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
   struct alignas(16) H8 { __half2 v[4]; };
   constexpr int ESZ = I8 ? 1 : 2;
   const int64_t kq = (a.kdim + 7) / 8;
   const int64_t total = a.rows * kq;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = idx / kq;
-    const int64_t k0 = (idx % kq) * 8;
+  for (GridWalk g(kq); g.idx < total; g.next()) {
+    const int64_t r = g.r;
+    const int64_t k0 = g.c * 8;
     const int e = a.exps[r];
     const double f = a.frac ? a.frac[r] : 1.0;
     Limbs2 L2[4];
@@ -431,6 +454,33 @@ constexpr int ZCMB_STAGES = 3;
 __device__ __forceinline__ int lo8(uint32_t w) { return (int)(w << 24) >> 24; }
 __device__ __forceinline__ int hi8(uint32_t w) { return (int)(w << 16) >> 24; }
 
+/* Walk over a block's tiles first, first + stride, ... of a grid of
+ * row_tiles x columns tiles (column-major tile order), keeping the tile's
+ * row tile and column by additions: no 64-bit division per tile.  Also
+ * tracks the ring stage and its phase.  Row tiles and the stride are below
+ * 2^31; the walk ends once the column reaches the column count. */
+template <int STAGES>
+struct TileWalk {
+  int64_t col, dcol;
+  int rt, drt, row_tiles, s;
+  uint32_t ph;
+  __device__ __forceinline__ TileWalk(int first, int stride, int row_tiles_)
+      : col(first / row_tiles_), dcol(stride / row_tiles_), rt(first % row_tiles_),
+        drt(stride % row_tiles_), row_tiles(row_tiles_), s(0), ph(0) {}
+  __device__ __forceinline__ void next() {
+    rt += drt;
+    col += dcol;
+    if (rt >= row_tiles) {
+      rt -= row_tiles;
+      ++col;
+    }
+    if (++s == STAGES) {
+      s = 0;
+      ph ^= 1u;
+    }
+  }
+};
+
 /* Producer of a warp-specialised combine (one thread): tile j of this block
  * (ROWS rows of one column, every residue plane) goes to stage j % STAGES by
  * 1-D bulk copies once the consumers have released the stage's previous
@@ -439,22 +489,22 @@ __device__ __forceinline__ int hi8(uint32_t w) { return (int)(w << 16) >> 24; }
  * shared memory after the block has left. */
 template <int STAGES, int ROWS>
 __device__ __forceinline__ void ws_produce(const int8_t *res, int64_t res_plane, int64_t ldr,
-                                           int nplanes, int64_t row_tiles, int64_t ntiles,
+                                           int nplanes, int64_t row_tiles, int64_t ncols,
                                            int8_t *buf, uint64_t *full, uint64_t *empty,
                                            int *err) {
   using namespace hcbk::tc;
   const size_t stage_elems = (size_t)nplanes * ROWS;
   int64_t j = 0;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
-    const int s = (int)(j % STAGES);
-    if (j >= STAGES &&
-        !mbar_wait(&empty[s], (uint32_t)((j / STAGES) - 1) & 1u, err, ERR_TIMEOUT_COMBINE))
-      break;
-    const int64_t r0 = (t % row_tiles) * ROWS, col = t / row_tiles;
+  TileWalk<STAGES> w((int)blockIdx.x, (int)gridDim.x, (int)row_tiles);
+  for (; w.col < ncols; w.next(), ++j) {
+    const int s = w.s;
+    /* the stage's previous tile was taken in the phase before this one */
+    if (j >= STAGES && !mbar_wait(&empty[s], w.ph ^ 1u, err, ERR_TIMEOUT_COMBINE)) break;
+    const int64_t r0 = w.rt * ROWS;
     const int64_t rows = ldr - r0 < ROWS ? ldr - r0 : ROWS;
     const uint32_t bytes = (uint32_t)rows; /* ldr, r0 multiples of 16 */
     mbar_expect_tx(&full[s], bytes * (uint32_t)nplanes);
-    const int8_t *src = res + col * ldr + r0;
+    const int8_t *src = res + w.col * ldr + r0;
     int8_t *dst = buf + s * stage_elems;
     for (int p = 0; p < nplanes; ++p)
       bulk_load_1d(dst + p * ROWS, src + p * res_plane, bytes, &full[s]);
@@ -480,7 +530,7 @@ constexpr int CMB_CONSUMERS = CMB_THREADS / 32;
 constexpr int CMB_BLOCK = CMB_THREADS + 32;
 
 template <int NC>
-__global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_constant__ CombArgs a) {
+__global__ void __launch_bounds__(CMB_BLOCK, 5) crt_combine_kernel(const __grid_constant__ CombArgs a) {
   using namespace hcbk::tc;
   extern __shared__ __align__(128) unsigned char cmb_smem[];
   __shared__ __align__(8) uint64_t full[CMB_STAGES], empty[CMB_STAGES];
@@ -492,7 +542,6 @@ __global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_
   const int nmod = a.nmod;
   int8_t *buf = reinterpret_cast<int8_t *>(cmb_smem);
   const int64_t row_tiles = (a.m + CMB_ROWS - 1) / CMB_ROWS;
-  const int64_t ntiles = row_tiles * a.n;
   const int64_t first = blockIdx.x, stride = gridDim.x;
   const size_t stage_elems = (size_t)nmod * CMB_ROWS;
   if (tid == 0) {
@@ -506,20 +555,17 @@ __global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_
 
   if (warp == CMB_CONSUMERS) { /* producer */
     if (lane == 0)
-      ws_produce<CMB_STAGES, CMB_ROWS>(a.res, a.res_plane, a.ldr, nmod, row_tiles, ntiles, buf,
+      ws_produce<CMB_STAGES, CMB_ROWS>(a.res, a.res_plane, a.ldr, nmod, row_tiles, a.n, buf,
                                        full, empty, a.err);
     return;
   }
 
   /* ------------------------------------------------ consumers -- */
-  int64_t j = 0;
-  for (int64_t t = first; t < ntiles; t += stride, ++j) {
-    const int s = (int)(j % CMB_STAGES);
-    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)(j / CMB_STAGES) & 1u, a.err,
-                                           ERR_TIMEOUT_COMBINE)))
-      break;
+  for (TileWalk<CMB_STAGES> w((int)first, (int)stride, (int)row_tiles); w.col < a.n; w.next()) {
+    const int s = w.s;
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], w.ph, a.err, ERR_TIMEOUT_COMBINE))) break;
     const int8_t *R = buf + s * stage_elems;
-    const int64_t row = (t % row_tiles) * CMB_ROWS + CMB_RPT * tid, col = t / row_tiles;
+    const int64_t row = w.rt * CMB_ROWS + CMB_RPT * tid, col = w.col;
     if (row < a.m) {
       CrtAcc<NC> acc[CMB_RPT];
 #pragma unroll
@@ -743,10 +789,9 @@ __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
   constexpr int ESZ = I8 ? 1 : 2;
   const int64_t kq = (a.kdim + 3) / 4;
   const int64_t total = a.rows * kq;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = idx / kq;
-    const int64_t k0 = (idx % kq) * 4;
+  for (GridWalk g(kq); g.idx < total; g.next()) {
+    const int64_t r = g.r;
+    const int64_t k0 = g.c * 4;
     const int e = row_exp(a.exps, a.exp_pair, r);
     const double f = a.frac ? a.frac[r] : 1.0;
     Limbs2 lr[2], li[2]; /* element pairs (0, 1), (2, 3); im carries the conj sign */
@@ -918,7 +963,6 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
   const int nmod = a.g.nmod;
   int8_t *buf = reinterpret_cast<int8_t *>(cmb_smem);
   const int64_t row_tiles = (a.g.m + ZCMB_ROWS - 1) / ZCMB_ROWS;
-  const int64_t ntiles = row_tiles * a.g.n;
   const size_t stage_elems = (size_t)3 * nmod * ZCMB_ROWS;
   if (tid == 0) {
     for (int s = 0; s < ZCMB_STAGES; ++s) {
@@ -931,17 +975,15 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
   if (warp == ZCMB_CONSUMERS) { /* producer */
     if (lane == 0)
       ws_produce<ZCMB_STAGES, ZCMB_ROWS>(a.g.res, a.g.res_plane, a.g.ldr, 3 * nmod, row_tiles,
-                                         ntiles, buf, full, empty, a.g.err);
+                                         a.g.n, buf, full, empty, a.g.err);
     return;
   }
-  int64_t j = 0;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
-    const int s = (int)(j % ZCMB_STAGES);
-    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)(j / ZCMB_STAGES) & 1u, a.g.err,
-                                           ERR_TIMEOUT_COMBINE)))
-      break;
+  for (TileWalk<ZCMB_STAGES> w((int)blockIdx.x, (int)gridDim.x, (int)row_tiles); w.col < a.g.n;
+       w.next()) {
+    const int s = w.s;
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], w.ph, a.g.err, ERR_TIMEOUT_COMBINE))) break;
     const int8_t *R = buf + s * stage_elems;
-    const int64_t row = (t % row_tiles) * ZCMB_ROWS + tid, col = t / row_tiles;
+    const int64_t row = w.rt * ZCMB_ROWS + tid, col = w.col;
     CrtAcc<NC> acc_re, acc_im;
     if (row < a.g.m) {
 #pragma unroll

@@ -381,8 +381,8 @@ __device__ __forceinline__ void simt_tile(const TileJob<T> &p, typename AccOf<T>
   }
 }
 
-template <typename T, int BM, int BN, int BK, int TM, int TN, int OP_A, int OP_B>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+template <typename T, int BM, int BN, int BK, int TM, int TN, int OP_A, int OP_B, int MINB>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB)
 simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
   using Acc = typename AccOf<T>::type;
   __shared__ __align__(16) SimtSmem<Acc, BM, BN, BK> sm;
@@ -485,7 +485,10 @@ simt_grouped_kernel(const hcbk_simt_entry *table, const int32_t *tile_start, int
 
 /* ------------------------------------------------------------ launchers -- */
 
-template <typename T, int BM, int BN, int BK, int TM, int TN>
+/* MINB: CTAs per SM the register allocation must allow (2 for the FP32
+ * 128 x 128 tile: sixteen warps per SM hide the global-load latency of each
+ * K-slab better than eight) */
+template <typename T, int BM, int BN, int BK, int TM, int TN, int MINB = 1>
 int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
   using Acc = typename AccOf<T>::type;
   SimtParams<T, Acc> p;
@@ -507,7 +510,7 @@ int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
   dim3 block((BM / TM) * (BN / TN));
 #define HCBK_SIMT_CASE(OA, OB)                                                    \
   if (a->op_a == OA && a->op_b == OB) {                                           \
-    simt_gemm_kernel<T, BM, BN, BK, TM, TN, OA, OB><<<grid, block, 0, st>>>(p);  \
+    simt_gemm_kernel<T, BM, BN, BK, TM, TN, OA, OB, MINB><<<grid, block, 0, st>>>(p); \
     return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;         \
   }
   HCBK_SIMT_CASE(0, 0) HCBK_SIMT_CASE(0, 1) HCBK_SIMT_CASE(1, 0) HCBK_SIMT_CASE(1, 1)
@@ -573,7 +576,7 @@ extern "C" int hcbk_gemm_simt(const hcbk_gemm_args *a, hcbk_simt_cfg cfg, void *
   switch (a->dtype) {
     case HCBK_S:
       return small ? launch_cfg<float, 64, 64, 16, 4, 4>(a, st)
-                   : launch_cfg<float, 128, 128, 8, 8, 8>(a, st);
+                   : launch_cfg<float, 128, 128, 16, 8, 8, 2>(a, st);
     case HCBK_D:
       return small ? launch_cfg<double, 64, 64, 8, 4, 4>(a, st)
                    : launch_cfg<double, 128, 128, 8, 8, 8>(a, st);
