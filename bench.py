@@ -334,6 +334,43 @@ def measure_int8_peak(torch, n=8192, reps=10):
         return None
 
 
+def measure_native_peaks(hb, torch, n=8192, reps=5):
+    """Rates the native (non-emulated) kernels are stated against, measured
+    in this run: the library's issue-rate probes of the pipes they run on
+    (FP32 FMA, FP64 FMA, FP64 mma.sync; hcbk_peak_probe) and the vendor
+    library's plain GEMMs (cuBLAS DGEMM and SGEMM, TF32 off, through
+    torch.mm, n^3, best of `reps`) -- library code, never on this library's
+    paths."""
+    out = {}
+    for key, kind in (("fp32_fma_probe", 0), ("fp64_fma_probe", 1), ("fp64_mma_probe", 2)):
+        v = hb.peak_probe(kind)
+        out[key] = round(v, 2) if v else None
+    try:
+        torch.backends.cuda.matmul.allow_tf32 = False
+        g = torch.Generator(device="cuda").manual_seed(12)
+        for key, dt in (("cublas_dgemm_8192", torch.float64), ("cublas_sgemm_8192", torch.float32)):
+            a = torch.randn(n, n, device="cuda", dtype=dt, generator=g)
+            b = torch.randn(n, n, device="cuda", dtype=dt, generator=g)
+            torch.mm(a, b)
+            torch.cuda.synchronize()
+            best = None
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.mm(a, b)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            out[key] = round(2.0 * n ** 3 / (best * 1e-3) / 1e12, 2)
+            del a, b
+        torch.cuda.empty_cache()
+    except Exception:
+        out.setdefault("cublas_dgemm_8192", None)
+        out.setdefault("cublas_sgemm_8192", None)
+    return out
+
+
 def oracle_err(O, Cg, A, lda, ta, B, ldb, tb, m, k, cols, ncol_total, beta=0.0, C0=None):
     """normwise error of the (m x ncol_total) column-major result Cg on the
     sampled columns against the double-double oracle (alpha = 1; beta * C0
@@ -487,6 +524,7 @@ def main():
     # 10 at 8192^3, as MEASURED_PEAKS.json measures bf16); twice the measured
     # bf16 rate if that measurement is unavailable
     int8_peak = measure_int8_peak(torch) if dom == "tc.crt_modgemm" else None
+    native_peaks = measure_native_peaks(hb, torch)
     if dom == "tc.crt_modgemm":
         peak = round(int8_peak, 1) if int8_peak else 2.0 * peaks.get("bf16_tflops")
     else:
@@ -618,7 +656,14 @@ def main():
                        "ms_per_step_eager_profiled": round(ms_eager, 4)},
             "native": {"path": native_path, "tflops": round(native_tflops, 3),
                        "ms_per_step": round(native_ms, 4), "normwise_err": err_native,
-                       "speedup_emulated_vs_native": round(value / world / native_tflops, 3)},
+                       "speedup_emulated_vs_native": round(value / world / native_tflops, 3),
+                       "reference_rates_tflops": native_peaks,
+                       "frac_of_fp64_mma_probe": (
+                           round(native_tflops / native_peaks["fp64_mma_probe"], 4)
+                           if native_peaks.get("fp64_mma_probe") else None),
+                       "frac_of_cublas_dgemm_8192": (
+                           round(native_tflops / native_peaks["cublas_dgemm_8192"], 4)
+                           if native_peaks.get("cublas_dgemm_8192") else None)},
             "e2e": {"value": round(e2e, 3), "unit": "TFLOPS",
                     "h2d_bytes_per_step": 8 * (M * K + N * K),
                     "d2h_bytes_per_step": 8 * M * N, "ms_per_step": round(e2e_ms, 3),
@@ -681,7 +726,10 @@ def summarize(line):
     JSON line: native vs emulated at 4096^3 and 8192^3 (DGEMM), split-BF16 vs
     plain SGEMM (8192^3 and 8192 x 8192 x 256), grouped vs per-problem
     calls, complex at 2048^3; each with the errors behind it."""
+    rates = line["native"].get("reference_rates_tflops") or {}
     out = {"dgemm_4096": {"native_tflops": line["native"]["tflops"],
+                          "native_frac_of_fp64_mma_probe": line["native"].get("frac_of_fp64_mma_probe"),
+                          "native_frac_of_cublas_dgemm": line["native"].get("frac_of_cublas_dgemm_8192"),
                           "native_err": line["accuracy"]["native_normwise_err"],
                           "crt_tflops": line["value"],
                           "crt_err": line["accuracy"]["normwise_err_vs_double_double_oracle"],
@@ -708,7 +756,14 @@ def summarize(line):
                        ("sgemm_colmajor_TN_8192x8192x256_beta1", "sgemm_8192x8192x256")):
         s3 = sec.get(key)
         if s3:
-            out[short] = {"plain_tflops": pick(s3, "plain", "tflops"),
+            pt = pick(s3, "plain", "tflops")
+            out[short] = {"plain_tflops": pt,
+                          "plain_frac_of_fp32_fma_probe": (
+                              round(pt / rates["fp32_fma_probe"], 4)
+                              if pt and rates.get("fp32_fma_probe") else None),
+                          "plain_frac_of_cublas_sgemm": (
+                              round(pt / rates["cublas_sgemm_8192"], 4)
+                              if pt and rates.get("cublas_sgemm_8192") else None),
                           "plain_err": pick(s3, "plain", "normwise_err"),
                           "split6_tflops": pick(s3, "split_bf16x6", "tflops"),
                           "split6_err": pick(s3, "split_bf16x6", "normwise_err"),

@@ -210,6 +210,19 @@ def lib():
 
 # ------------------------------------------------------------------ handle --
 
+
+def peak_probe(kind, iters=0):
+    """TFLOP/s of one arithmetic pipe measured by the library's issue-rate
+    probe: kind 0 = FP32 FMA (f32x2), 1 = FP64 FMA, 2 = FP64 mma.sync
+    m16n8k4 (the pipes the native SGEMM, the FP64 SIMT kernel and the DMMA
+    DGEMM run on); iters per chain, 0 for the default.  None on failure."""
+    L = lib()
+    f = L.hcbk_peak_probe
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    f.restype = ctypes.c_int
+    out = ctypes.c_double(0.0)
+    return out.value if f(int(kind), int(iters), ctypes.byref(out)) == 0 else None
+
 def hcblasCreate(device: int = 0, stream: int | None = None):
     """Returns ``(status, handle)``; the handle is a raw pointer (int)."""
     h = ctypes.c_void_p()

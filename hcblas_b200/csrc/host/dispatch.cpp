@@ -49,12 +49,20 @@ int simt(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const char 
   const int64_t big = (a->dtype == HCBK_C || a->dtype == HCBK_Z) ? 64 : 128;
   hcbk_simt_cfg cfg;
   cfg.variant = (tiles_of(a->m, a->n, big, big) * a->batch >= sms) ? 0 : 1;
-  if (st->autotune && a->beta_re == 0.0 && a->beta_im == 0.0) /* re-running is harmless */
-    cfg.variant = tune_choice(st, stream, tune_key("simt", a), 2, [&](int i) {
-      hcbk_simt_cfg c;
-      c.variant = i;
-      return hcbk_gemm_simt(a, c, stream);
-    }, cfg.variant);
+  const bool zero_beta = a->beta_re == 0.0 && a->beta_im == 0.0;
+  if (st->autotune) {
+    /* beta == 0: the candidates write C, which the final launch rewrites;
+     * otherwise they write a scratch matrix of C's shape */
+    TuneTarget tt(a, stream);
+    if (zero_beta || tt.usable())
+      cfg.variant = tune_choice(st, stream, tune_key("simt", a), 2, [&](int i) {
+        const hcbk_gemm_args *t = zero_beta ? a : tt.args();
+        if (!t) return (int)HCBK_ERR_NOMEM;
+        hcbk_simt_cfg c;
+        c.variant = i;
+        return hcbk_gemm_simt(t, c, stream);
+      }, cfg.variant);
+  }
   static const char *names[5][2] = {
       {"simt.s.128x128", "simt.s.64x64"}, {"simt.d.128x128", "simt.d.64x64"},
       {"simt.c.64x64", "simt.c.64x64"},   {"simt.z.64x64", "simt.z.64x64"},
@@ -92,11 +100,15 @@ int hgemm_tc(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, const c
   }
   int pair = use_pair(st, a->m, a->n, 256) ? 1 : 0;
   int bn = pair || tiles_of(a->m, a->n, 128, 256) >= hcbk_sm_count() ? 256 : 128;
-  if (st->autotune && st->tc_pair == 1 && a->beta_re == 0.0) {
-    /* candidates: 128x128, 128x256, 256x256 over a CTA pair */
+  if (st->autotune && st->tc_pair == 1) {
+    /* candidates: 128x128, 128x256, 256x256 over a CTA pair; with beta != 0
+     * they write a scratch matrix of C's shape */
     static const int cbn[3] = {128, 256, 256}, cpair[3] = {0, 0, 1};
+    TuneTarget tt(a, stream);
     const int c = tune_choice(st, stream, tune_key("hgemm_tc", a), 3, [&](int i) {
-      return hcbk_hgemm_tc(a, cbn[i], cpair[i], err, stream);
+      const hcbk_gemm_args *t = tt.args();
+      if (!t) return (int)HCBK_ERR_NOMEM;
+      return hcbk_hgemm_tc(t, cbn[i], cpair[i], err, stream);
     }, pair ? 2 : bn == 256 ? 1 : 0);
     bn = cbn[c];
     pair = cpair[c];
@@ -165,6 +177,20 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   g.ldc = a->ldc;
   g.alpha = a->alpha_re;
   g.beta = a->beta_re;
+  if (st->autotune && st->tc_pair == 1) {
+    /* 128 x 128 tiles or 256 x 128 over a CTA pair: the same sums in the
+     * same order, so the choice never changes a result (the promotion
+     * interval, which does, stays the knob's) */
+    TuneTarget tt(a, stream);
+    g.pair = tune_choice(st, stream, tune_key(terms == 6 ? "split6" : "split3", a), 2, [&](int i) {
+      const hcbk_gemm_args *t = tt.args();
+      if (!t) return (int)HCBK_ERR_NOMEM;
+      hcbk_split_gemm gi = g;
+      gi.pair = i;
+      gi.c = static_cast<float *>(t->c) + t->c_off;
+      return hcbk_sgemm_split_tc(&gi, err, stream);
+    }, 0);
+  }
   static const char *names[2][2][2] = {
       {{"tc.split_bf16x3.128x128.p1", "tc.split_bf16x3.128x128.p4"},
        {"tc.split_bf16x3.256x128.pair.p1", "tc.split_bf16x3.256x128.pair.p4"}},
@@ -363,6 +389,18 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
     g.d_plane = ldd * a->n;
     g.pair = st->tc_pair == 2 ||
              (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * s >= hcbk_sm_count() / 2);
+    if (st->autotune && st->tc_pair == 1) {
+      /* the slice products land in workspace planes: re-running is harmless */
+      g.k0 = 0;
+      g.k = a->k < kmax ? a->k : kmax;
+      g.pair = tune_choice(st, stream, tune_key(f32 ? "sozaki_groups" : "ozaki_groups", a), 2,
+                           [&](int i) {
+                             hcbk_ozaki_groups gi = g;
+                             gi.pair = i;
+                             return hcbk_ozaki_groups_tc(&gi, err, stream);
+                           },
+                           g.pair);
+    }
     hcbk_ozaki_groups_combine_args cb;
     cb.m = a->m;
     cb.n = a->n;

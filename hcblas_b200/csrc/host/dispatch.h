@@ -49,8 +49,35 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
  * returns an HCBK_* code -- measured once per key while the handle's
  * "autotune" knob is on (else `fallback`). */
 std::string tune_key(const char *family, const hcbk_gemm_args *a);
+/* the same key for a family whose bucket is described by `shape` */
+std::string tune_key_shape(const char *family, const char *shape);
 int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int ncand,
                 const std::function<int(int)> &run, int fallback);
+
+/* Output of the candidates while a call whose C must not be rewritten
+ * (beta != 0) is tuned: the call's arguments with C moved to a scratch
+ * matrix of the same shape, leading dimension and 256-byte phase, allocated
+ * stream-ordered on first use (only when the bucket is actually tuned) and
+ * released by the destructor.  For beta == 0 the candidates write C itself,
+ * which the final launch overwrites.  Single problems only (batch 1, no
+ * pointer arrays); args() is nullptr when the scratch cannot be had. */
+class TuneTarget {
+ public:
+  TuneTarget(const hcbk_gemm_args *a, void *stream);
+  ~TuneTarget();
+  TuneTarget(const TuneTarget &) = delete;
+  TuneTarget &operator=(const TuneTarget &) = delete;
+  const hcbk_gemm_args *args();
+  /* whether tuning is offered for this call at all */
+  bool usable() const { return usable_; }
+
+ private:
+  hcbk_gemm_args t_;
+  const hcbk_gemm_args *a_;
+  void *stream_;
+  void *scratch_ = nullptr;
+  bool usable_ = false, failed_ = false;
+};
 
 /* CRT plan of a real row of length k (dispatch.cpp): the moduli count, the
  * shift below 53 bits of the norm-scaled integers and whether rows are

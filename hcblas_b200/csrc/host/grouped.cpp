@@ -167,9 +167,10 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
                      [&](int x, int y) { return work(x) > work(y); });
     const int nt = (int)ok_idx.size();
     if (nt >= (1 << 24)) return HCBK_ERR_ARGS;
-    int64_t total = 0;
+    int64_t total = 0, all_work = 0;
     for (int j = 0; j < nt; ++j) {
       total += (int64_t)hcbk_grouped_tiles(&ent[ok_idx[j]]);
+      all_work += work(ok_idx[j]);
       if (total > 0x7fffffff) return HCBK_ERR_ARGS;
     }
     /* table: entries | tile prefix sums | per-tile descriptors */
@@ -210,6 +211,8 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     gp.tile_start_offset = ts_off;
     gp.tile_desc_offset = td_off;
     gp.fallback = fallback;
+    gp.work = all_work;
+    gp.tuned_ctas = 0;
     gp.key = key;
   }
 
@@ -230,6 +233,29 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     g.uniform_tiles = 0;
     g.u_tiles_m = g.u_k = g.u_flags = 0;
     g.ctas_per_sm = st->grouped_ctas;
+    if (st->autotune) {
+      /* one or two CTAs per SM, per bucket of problem count, tiles and
+       * tensor work; tuned on a beta == 0 call, where every candidate
+       * writes what the final launch rewrites, then kept with the plan */
+      if (!gp.tuned_ctas && beta == 0.0f) {
+        auto lg = [](int64_t v) {
+          int r = 0;
+          while (((int64_t)1 << r) < v && r < 62) ++r;
+          return r;
+        };
+        char shape[96];
+        std::snprintf(shape, sizeof(shape), "count%d|tiles%d|work%d", lg(gp.count),
+                      lg(gp.total_tiles), lg(gp.work));
+        gp.tuned_ctas = 1 + tune_choice(st, stream, tune_key_shape("grouped_h", shape), 2,
+                                        [&](int i) {
+                                          hcbk_grouped_args gi = g;
+                                          gi.ctas_per_sm = 1 + i;
+                                          return hcbk_hgemm_grouped_tc(&gi, err, stream);
+                                        },
+                                        st->grouped_ctas - 1);
+      }
+      if (gp.tuned_ctas) g.ctas_per_sm = gp.tuned_ctas;
+    }
     int rc = timed_launch(st, stream, "tc.h.grouped",
                           [&] { return hcbk_hgemm_grouped_tc(&g, err, stream); });
     if (rc) return rc;

@@ -38,6 +38,8 @@ struct HcblasGroupedPlan {
   size_t tile_start_offset = 0;
   size_t tile_desc_offset = 0; /* per-tile descriptors (hcbk_grouped_fill_tiles) */
   std::vector<int> fallback; /* problems the table cannot hold (TMA alignment) */
+  int64_t work = 0;          /* padded tensor work of the table (bucket of the tuner) */
+  int tuned_ctas = 0;        /* CTAs per SM chosen by the autotuner; 0 = not tuned */
   /* split-BF16 SGEMM plans only: the bf16 planes of every problem (device),
    * and the pack jobs' place in the table */
   void *planes = nullptr;

@@ -13,8 +13,9 @@
  * processes start tuned.  Candidates run through the kernels' own C entry
  * points (not counted, not profiled) bracketed by CUDA events on the call's
  * stream; nothing is tuned while the stream is being captured into a graph.
- * Callers only offer tuning when re-running the kernel is harmless (outputs
- * that the final run overwrites completely).
+ * Candidates write either outputs that the final run overwrites completely
+ * (beta == 0, workspace planes) or, for beta != 0, a scratch copy of C's
+ * shape (TuneTarget), so tuning never changes a result.
  */
 #include <cuda_runtime.h>
 
@@ -92,6 +93,55 @@ std::string tune_key(const char *family, const hcbk_gemm_args *a) {
   return buf;
 }
 
+std::string tune_key_shape(const char *family, const char *shape) {
+  hcbk_gemm_args none;
+  std::memset(&none, 0, sizeof(none));
+  std::string k = tune_key(family, &none);
+  const size_t cut = k.find("|dt");
+  return (cut == std::string::npos ? k : k.substr(0, cut)) + "|" + shape;
+}
+
+namespace {
+size_t elem_bytes(int dtype) {
+  switch (dtype) {
+    case HCBK_S: return 4;
+    case HCBK_D: return 8;
+    case HCBK_C: return 8;
+    case HCBK_Z: return 16;
+    default: return 2;
+  }
+}
+}  // namespace
+
+TuneTarget::TuneTarget(const hcbk_gemm_args *a, void *stream) : t_(*a), a_(a), stream_(stream) {
+  usable_ = a->batch == 1 && !a->a_array && a->m > 0 && a->n > 0 && a->ldc >= a->m;
+}
+
+const hcbk_gemm_args *TuneTarget::args() {
+  if (!usable_ || failed_) return nullptr;
+  if (a_->beta_re == 0.0 && a_->beta_im == 0.0) return a_;
+  if (!scratch_) {
+    const size_t esz = elem_bytes(a_->dtype);
+    const int64_t phase = a_->c_off % (int64_t)(256 / esz); /* same 256-byte alignment phase */
+    const size_t bytes = ((size_t)a_->ldc * (size_t)(a_->n - 1) + (size_t)a_->m + phase) * esz;
+    if (cudaMallocAsync(&scratch_, bytes, static_cast<cudaStream_t>(stream_)) != cudaSuccess) {
+      cudaGetLastError();
+      scratch_ = nullptr;
+      failed_ = true;
+      return nullptr;
+    }
+    /* finite contents: beta * C reads them */
+    cudaMemsetAsync(scratch_, 0, bytes, static_cast<cudaStream_t>(stream_));
+    t_.c = scratch_;
+    t_.c_off = phase;
+  }
+  return &t_;
+}
+
+TuneTarget::~TuneTarget() {
+  if (scratch_) cudaFreeAsync(scratch_, static_cast<cudaStream_t>(stream_));
+}
+
 int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int ncand,
                 const std::function<int(int)> &run, int fallback) {
   if (!st->autotune) return fallback;
@@ -116,6 +166,7 @@ int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int n
   }
   int best = fallback;
   float best_ms = 1e30f;
+  bool timed_any = false;
   for (int i = 0; i < ncand; ++i) {
     if (run(i) != HCBK_OK) { /* candidate not applicable to this call */
       cudaGetLastError();
@@ -131,6 +182,7 @@ int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int n
       cudaGetLastError();
       continue;
     }
+    timed_any = true;
     if (ms < best_ms) {
       best_ms = ms;
       best = i;
@@ -138,6 +190,7 @@ int tune_choice(HcblasB200State *st, void *stream, const std::string &key, int n
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (!timed_any) return fallback; /* nothing ran: decide again on a later call */
   if (log_enabled())
     std::fprintf(stderr, "[hcblas] autotune %s -> %d (%.4f ms)\n", key.c_str(), best, best_ms);
   std::lock_guard<std::mutex> lock(g_tune_mutex);

@@ -90,6 +90,11 @@ int hcbk_scale_c(const hcbk_gemm_args *args, void *stream);
 /* Number of SMs of the current device (cached per device). */
 int hcbk_sm_count(void);
 
+/* Issue-rate probe of one arithmetic pipe (peak.cu): kind 0 = FP32 FMA
+ * (f32x2), 1 = FP64 FMA, 2 = FP64 mma.sync m16n8k4; iters per chain, 0 for
+ * the default.  Writes TFLOP/s. */
+int hcbk_peak_probe(int kind, int iters, double *tflops);
+
 /* ------------------------------------------------ tensor-core paths -- */
 
 /* HGEMM on tcgen05: f16 operands read by TMA directly from the caller's

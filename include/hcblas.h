@@ -463,13 +463,20 @@ hcblasStatus_t hcblasPlanEmulation(int mode, int param, int bits, int dtype, lon
  *                       accumulator (1 or 4; default 1).
  *   "autotune"          1: the first call in each size bucket (kernel family,
  *                       type, transposes, ceil(log2) of M, N, K) times every
- *                       candidate tile configuration (SIMT tile; HGEMM
- *                       128x128 / 128x256 / CTA-pair 256x256; CRT modular
- *                       GEMM the same three) and keeps the fastest, for this
+ *                       candidate configuration (SIMT tile; HGEMM 128x128 /
+ *                       128x256 / CTA-pair 256x256; CRT modular GEMM the
+ *                       same three; split-BF16 and Ozaki-I slice-group GEMMs
+ *                       with or without CTA pairs; the grouped f16 kernel at
+ *                       one or two CTAs per SM, bucketed by problem count,
+ *                       tiles and work) and keeps the fastest, for this
  *                       process and, when HCBLAS_AUTOTUNE_CACHE names a file,
- *                       for later ones; only offered where re-running the
- *                       kernel is harmless (beta == 0, or the CRT residues);
- *                       0 (default): size heuristics.
+ *                       for later ones.  Only tiling and placement are
+ *                       tuned, never the arithmetic (promotion interval,
+ *                       slice and moduli counts stay as set).  With beta != 0 the
+ *                       candidates write a scratch matrix of C's shape
+ *                       (allocated stream-ordered while tuning), so C is
+ *                       updated once; grouped calls are tuned on a beta == 0
+ *                       call; 0 (default): size heuristics.
  *   "graphs"            1: a call identical to an earlier one (same
  *                       arguments, pointers, math mode and knobs, same
  *                       non-default stream) replays a CUDA graph captured
