@@ -892,6 +892,7 @@ int hgemm_ptr_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *stream
   int rc = hcbk_grouped_encode(&tmpl, a->op_a, a->op_b, a->m, a->n, a->k, tb, a->lda, tb,
                                a->ldb, tb, a->ldc);
   if (rc) return rc;
+  if (!st->grouped_c_tma) tmpl.c_tma = 0; /* direct stores */
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;
   auto *table = reinterpret_cast<hcbk_grouped_entry *>(tb);

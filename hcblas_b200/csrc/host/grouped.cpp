@@ -134,8 +134,9 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
   HcblasGroupedPlan &gp = st->grouped;
   int dev = 0;
   cudaGetDevice(&dev);
-  std::vector<unsigned char> key(sizeof(hcblasGemmProblem) * (size_t)count + 2);
+  std::vector<unsigned char> key(sizeof(hcblasGemmProblem) * (size_t)count + 3);
   std::memcpy(key.data(), probs, sizeof(hcblasGemmProblem) * (size_t)count);
+  key[key.size() - 3] = static_cast<unsigned char>(st->grouped_c_tma);
   key[key.size() - 2] = static_cast<unsigned char>(order);
   key[key.size() - 1] = static_cast<unsigned char>(dev);
   const bool reuse = gp.table && gp.table_device == dev && key == gp.key;
@@ -155,6 +156,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
       const Canon c = canonical(probs[i], order);
       int rc = hcbk_grouped_encode(&ent[i], c.op_a, c.op_b, c.m, c.n, c.k, c.a, c.lda, c.b,
                                    c.ldb, c.c, c.ldc);
+      if (rc == HCBK_OK && !st->grouped_c_tma) ent[i].c_tma = 0; /* direct stores */
       if (rc == HCBK_OK) ok_idx.push_back(i);
       else if (rc == HCBK_ERR_ALIGN || rc == HCBK_ERR_ARGS) fallback.push_back(i);
       else return rc;

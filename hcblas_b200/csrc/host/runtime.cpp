@@ -492,6 +492,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
     handle->impl->grouped_ctas = value;
     return HCBLAS_STATUS_SUCCESS;
   }
+  if (std::strcmp(name, "grouped_c_tma") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->grouped_c_tma = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
   if (std::strcmp(name, "dgemm_dmma") == 0) {
     if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
     handle->impl->dgemm_dmma = value;

@@ -67,6 +67,7 @@ struct HcblasB200State {
   int tc_pair = 1; /* CTA-pair (cta_group::2) tensor-core kernels: 0 never, 1 auto, 2 always */
   int crt_i8 = 1;  /* CRT DGEMM modular GEMMs: 1 int8 residues on kind::i8, 0 binary16 */
   int grouped_ctas = 2; /* grouped f16 kernel: CTAs per SM (1: 6-stage ring, 2: 3 stages each) */
+  int grouped_c_tma = 1; /* grouped f16 kernel: C through TMA boxes where C allows (0: stores) */
   int dgemm_dmma = 1; /* native D/Z GEMM: 1 FP64 tensor path (mma.sync .f64), 0 CUDA-core FMA */
   int ozaki_default_slices = 7; /* Ozaki slices when the mode's param is 0 */
   /* requested accuracy of the emulated modes in bits (hcblasSetAccuracyTarget;

@@ -233,16 +233,19 @@ def test_sgemm_grouped_alpha_zero_and_status(handle):
     assert L.hcblasSgemmGrouped(None, 1, None, None, None) == hb.HCBLAS_STATUS_NOT_INITIALIZED
 
 
-@pytest.mark.parametrize("ctas", [1, 2])
-def test_grouped_kernel_configurations(handle, ctas):
+@pytest.mark.parametrize("ctas,c_tma", [(1, 1), (2, 1), (1, 0), (2, 0)])
+def test_grouped_kernel_configurations(handle, ctas, c_tma):
     """Both shapes of the grouped kernel (one CTA per SM with a 6-stage ring,
-    two with 3 stages each) give results within the bound, beta != 0."""
-    rng = np.random.default_rng(40 + ctas)
+    two with 3 stages each), with C written through TMA boxes or by direct
+    stores, give results within the bound, beta != 0, ld padding untouched."""
+    rng = np.random.default_rng(40 + ctas + 2 * c_tma)
     probs, host, dev = make_problems(handle, rng, 40)
     assert hb.set_tuning(handle, "grouped_ctas", ctas) == 0
+    assert hb.set_tuning(handle, "grouped_c_tma", c_tma) == 0
     try:
         assert hb.hgemm_grouped(handle, probs, 0.75, -1.5) == 0
         assert hb.device_error(handle) == 0
     finally:
         hb.set_tuning(handle, "grouped_ctas", 2)
+        hb.set_tuning(handle, "grouped_c_tma", 1)
     check(host, dev, 0.75, -1.5)
