@@ -784,9 +784,21 @@ __device__ __forceinline__ ZRes3 zresidue(const Limbs &lr, const Limbs &li, cons
  * registers), residues of element pairs by packed f32x2 arithmetic with the
  * moduli constants as constant-bank operands, 8-byte (binary16) or 4-byte
  * (int8) stores per plane */
+/* moduli loop of the complex residue kernels: constants staged in shared
+ * memory and the loop unrolled ZRES_UNROLL deep, which keeps the kernel's
+ * code within the instruction cache (fully unrolled over 20 moduli with three
+ * plane sets it was not, and warps stalled on instruction fetch) */
+constexpr int ZRES_UNROLL = 2;
+
 template <bool I8>
 __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
   constexpr int ESZ = I8 ? 1 : 2;
+  __shared__ ModPair smp[HCBK_CRT_MAX_MODULI];
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) smp[i] = a.mp[i];
+  }
+  __syncthreads();
   const int64_t kq = (a.kdim + 3) / 4;
   const int64_t total = a.rows * kq;
   for (GridWalk g(kq); g.idx < total; g.next()) {
@@ -810,10 +822,9 @@ __global__ void __launch_bounds__(256, 3) zcrt_res_kcontig(ZResArgs a) {
     char *d0 = a.planes + (r * a.ld_dst + k0) * (int64_t)ESZ;
     const bool vec = nk == 4 && (reinterpret_cast<uintptr_t>(d0) & (4 * ESZ - 1)) == 0 &&
                      (a.plane_stride & (4 * ESZ - 1)) == 0;
-#pragma unroll
-    for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
-      if (i >= a.nmod) break;
-      const ModPair m = a.mp[i];
+#pragma unroll ZRES_UNROLL
+    for (int i = 0; i < a.nmod; ++i) {
+      const ModPair m = smp[i];
       if constexpr (I8) {
         uint32_t w[3][2];
 #pragma unroll

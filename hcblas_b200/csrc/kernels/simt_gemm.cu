@@ -253,8 +253,92 @@ __device__ __forceinline__ void simt_tile(const TileJob<T> &p, typename AccOf<T>
   Vec<T, VW> ra[VA];
   Vec<T, VW> rb[VB];
 
-  /* fetch the K-slab starting at k0 into registers (zero-filled) */
-  auto fetch = [&](int64_t k0) {
+  /* Per-thread load positions inside a K-slab: vector v of A covers
+   * (mn, kk) = (a_mn(v) .. + VW, a_kk(v)) for MN-contiguous A, or
+   * (a_mn(v), a_kk(v) .. + VW) for K-contiguous A (likewise B).  The source
+   * pointers advance by one slab per fetch; bounds are checked against the
+   * tile's remaining rows and the slab's remaining K as 32-bit values. */
+  auto a_mn = [&](int v) {
+    const int idx = tid + v * NT;
+    return A_MN ? (idx % (BM / VW)) * VW : idx / (BK / VW);
+  };
+  auto a_kk = [&](int v) {
+    const int idx = tid + v * NT;
+    return A_MN ? idx / (BM / VW) : (idx % (BK / VW)) * VW;
+  };
+  auto b_mn = [&](int v) {
+    const int idx = tid + v * NT;
+    return B_MN ? (idx % (BN / VW)) * VW : idx / (BK / VW);
+  };
+  auto b_kk = [&](int v) {
+    const int idx = tid + v * NT;
+    return B_MN ? idx / (BN / VW) : (idx % (BK / VW)) * VW;
+  };
+  const int rem_m = (int)((p.m - m0) < BM ? (p.m - m0) : BM);
+  const int rem_n = (int)((p.n - n0) < BN ? (p.n - n0) : BN);
+  const T *pa[VA];
+  const T *pb[VB];
+#pragma unroll
+  for (int v = 0; v < VA; ++v)
+    pa[v] = A_MN ? A + m0 + a_mn(v) + (int64_t)a_kk(v) * p.lda
+                 : A + a_kk(v) + (m0 + a_mn(v)) * p.lda;
+#pragma unroll
+  for (int v = 0; v < VB; ++v)
+    pb[v] = B_MN ? B + n0 + b_mn(v) + (int64_t)b_kk(v) * p.ldb
+                 : B + b_kk(v) + (n0 + b_mn(v)) * p.ldb;
+  const int64_t a_step = A_MN ? (int64_t)BK * p.lda : BK;
+  const int64_t b_step = B_MN ? (int64_t)BK * p.ldb : BK;
+
+  /* fetch the next K-slab (starting at k0) into registers, zero-filled */
+  auto fetch_ptr = [&](int64_t k0) {
+    const int rem_k = (int)((p.k - k0) < BK ? (p.k - k0) : BK);
+#pragma unroll
+    for (int v = 0; v < VA; ++v) {
+      const T *src = pa[v];
+      const int mn = a_mn(v), kk = a_kk(v);
+      if (A_MN) {
+        if (kk < rem_k && mn + VW <= rem_m && vec_a) {
+          ra[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e) ra[v].v[e] = (kk < rem_k && mn + e < rem_m) ? src[e] : T();
+        }
+      } else {
+        if (mn < rem_m && kk + VW <= rem_k && vec_a) {
+          ra[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e) ra[v].v[e] = (mn < rem_m && kk + e < rem_k) ? src[e] : T();
+        }
+      }
+      pa[v] += a_step;
+    }
+#pragma unroll
+    for (int v = 0; v < VB; ++v) {
+      const T *src = pb[v];
+      const int mn = b_mn(v), kk = b_kk(v);
+      if (B_MN) {
+        if (kk < rem_k && mn + VW <= rem_n && vec_b) {
+          rb[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e) rb[v].v[e] = (kk < rem_k && mn + e < rem_n) ? src[e] : T();
+        }
+      } else {
+        if (mn < rem_n && kk + VW <= rem_k && vec_b) {
+          rb[v] = *reinterpret_cast<const Vec<T, VW> *>(src);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e) rb[v].v[e] = (mn < rem_n && kk + e < rem_k) ? src[e] : T();
+        }
+      }
+      pb[v] += b_step;
+    }
+  };
+
+  /* the same K-slab fetch with positions recomputed from k0 (complex types:
+   * measured faster than the advancing pointers at their 64 x 64 tiles) */
+  auto fetch_idx = [&](int64_t k0) {
 #pragma unroll
     for (int v = 0; v < VA; ++v) {
       const int idx = tid + v * NT;
@@ -317,6 +401,13 @@ __device__ __forceinline__ void simt_tile(const TileJob<T> &p, typename AccOf<T>
         }
       }
     }
+  };
+
+  auto fetch = [&](int64_t k0) {
+    if constexpr (IsComplex<T>::value)
+      fetch_idx(k0);
+    else
+      fetch_ptr(k0);
   };
 
   /* registers -> shared buffer s, as [k][mn] in the compute type */
