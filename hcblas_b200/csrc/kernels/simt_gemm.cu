@@ -488,18 +488,43 @@ __device__ __forceinline__ void simt_tile(const TileJob<T> &p, typename AccOf<T>
     __syncthreads();
   }
 
-  /* ---- epilogue: C = alpha * acc + beta * C ---- */
+  /* ---- epilogue: C = alpha * acc + beta * C ----
+   * Each thread's GSA consecutive rows of a column are one contiguous run of
+   * C (16 bytes in the compute type; the 16 lanes of a warp row cover 16 such
+   * runs back to back), so a whole run is read and written as one vector
+   * when it lies inside C and is aligned, element by element otherwise. */
+  constexpr int RUN_BYTES = GSA * (int)sizeof(T);
+  constexpr bool RUN_VEC = RUN_BYTES == 8 || RUN_BYTES == 16;
 #pragma unroll
   for (int j = 0; j < TN; ++j) {
     const int64_t col = n0 + (j / GSB) * (BN / GB) + ty * GSB + (j % GSB);
     if (col >= p.n) continue;
 #pragma unroll
-    for (int i = 0; i < TM; ++i) {
-      const int64_t row = m0 + (i / GSA) * (BM / GA) + tx * GSA + (i % GSA);
-      if (row < p.m) {
-        T *dst = p.C + row + col * p.ldc;
-        Acc cv = rd ? c_load(dst) : zero_of<Acc>();
-        c_store(dst, axpby(alpha, acc[i][j], beta, cv, rd));
+    for (int g = 0; g < GA; ++g) {
+      const int64_t row0 = m0 + g * (BM / GA) + tx * GSA;
+      T *dst0 = p.C + row0 + col * p.ldc;
+      if constexpr (RUN_VEC) {
+        if (row0 + GSA <= p.m && (reinterpret_cast<uintptr_t>(dst0) & (RUN_BYTES - 1)) == 0) {
+          struct alignas(RUN_BYTES) Run { T v[GSA]; };
+          Run cr;
+          if (rd) cr = *reinterpret_cast<const Run *>(dst0);
+          Run out;
+#pragma unroll
+          for (int e = 0; e < GSA; ++e) {
+            const Acc cv = rd ? c_load(&cr.v[e]) : zero_of<Acc>();
+            c_store(&out.v[e], axpby(alpha, acc[g * GSA + e][j], beta, cv, rd));
+          }
+          *reinterpret_cast<Run *>(dst0) = out;
+          continue;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < GSA; ++e) {
+        if (row0 + e < p.m) {
+          T *dst = dst0 + e;
+          const Acc cv = rd ? c_load(dst) : zero_of<Acc>();
+          c_store(dst, axpby(alpha, acc[g * GSA + e][j], beta, cv, rd));
+        }
       }
     }
   }
