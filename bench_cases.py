@@ -65,10 +65,11 @@ def _complex(h, dtype, op_a, op_b, m, n, k, mode=0, param=0, seed=4):
     return call, (dA, dB, dC)
 
 
-def _grouped(h, count=4096, seed=3, dtype=np.float16):
+def _grouped(h, count=4096, seed=3, dtype=np.float16, pad_c=False):
     """Uneven grouped GEMM: M, N, K log-uniform integers in [16, 1024], mixed
-    N/T; f16 (hcblasHgemmGrouped, leading dimensions padded to 8 elements for
-    TMA) or f32 (hcblasSgemmGrouped on the split-BF16 path, unpadded)."""
+    N/T; f16 (hcblasHgemmGrouped, the leading dimensions of A and B padded to
+    8 elements for TMA; C's too when pad_c) or f32 (hcblasSgemmGrouped on the
+    split-BF16 path, unpadded)."""
     rng = np.random.default_rng(seed)
     lu = lambda: int(np.exp(rng.uniform(np.log(16), np.log(1025))))
     probs, keep = [], []
@@ -81,9 +82,10 @@ def _grouped(h, count=4096, seed=3, dtype=np.float16):
         A = rng.uniform(-1, 1, lda * (k if ta == 0 else m)).astype(dtype)
         B = rng.uniform(-1, 1, ldb * (n if tb == 0 else k)).astype(dtype)
         dA, dB = _dev(h, A), _dev(h, B)
-        dC = hb.DeviceArray(h, nbytes=esz * m * n, dtype=dtype)
+        ldc = r8(m) if pad_c else m
+        dC = hb.DeviceArray(h, nbytes=esz * ldc * n, dtype=dtype)
         keep += [dA, dB, dC]
-        probs.append(hb.GemmProblem(ta, tb, m, n, k, dA.ptr, lda, dB.ptr, ldb, dC.ptr, m))
+        probs.append(hb.GemmProblem(ta, tb, m, n, k, dA.ptr, lda, dB.ptr, ldb, dC.ptr, ldc))
     arr = (hb.GemmProblem * count)(*probs)
     if esz == 2:
         one = np.array([1.0], np.float16).view(np.uint16)
@@ -184,6 +186,7 @@ CASES = {
     "zgemm_native_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048),
     "zgemm_crt3m_cn_2048": lambda h: _complex(h, np.complex128, C_, N_, 2048, 2048, 2048, 4, 0),
     "hgemm_grouped_4096": _grouped,
+    "hgemm_grouped_4096_ldc8": lambda h: _grouped(h, pad_c=True),
     "sgemm_grouped_4096": lambda h: _grouped(h, dtype=np.float32),
     "hgemm_strided_512x128": _strided,
     "sgemv_n_16384": lambda h: _gemv(h, np.float32, 0, 16384, 16384),
