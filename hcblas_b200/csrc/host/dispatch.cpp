@@ -329,7 +329,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   char *pb_base = pa_base + s * a_pl;
   int32_t *dsum = reinterpret_cast<int32_t *>(pb_base + s * b_pl);
 
-  hcbk_ozaki_prep pa;
+  hcbk_ozaki_prep pa{};
   pa.src = f32 ? nullptr : static_cast<const double *>(a->a) + a->a_off;
   pa.src_f32 = f32 ? static_cast<const float *>(a->a) + a->a_off : nullptr;
   pa.ld = a->lda;
@@ -342,7 +342,7 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
   pa.plane_stride = (int64_t)a_pl;
   pa.ld_dst = kp;
   pa.f16 = f16 ? 1 : 0;
-  hcbk_ozaki_prep pb;
+  hcbk_ozaki_prep pb{};
   pb.src = f32 ? nullptr : static_cast<const double *>(a->b) + a->b_off;
   pb.src_f32 = f32 ? static_cast<const float *>(a->b) + a->b_off : nullptr;
   pb.ld = a->ldb;
@@ -455,13 +455,12 @@ int dgemm_ozaki(HcblasB200State *st, const hcbk_gemm_args *a_in, int s, bool f16
 /* CRT (Ozaki scheme II) DGEMM: exponents, residue planes of the scaled
  * integer operands, one modular tensor-core GEMM launch over every modulus,
  * CRT reconstruction (weighted residue sum mod M) with the alpha/beta
- * epilogue. */
-int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
-              const char **path) {
-  if (a->batch != 1 || a->a_array) return HCBK_ERR_ARGS;
-  int nmod = 0, shift = 0;
-  bool norm = false;
-  if (!crt_plan_rows(a->k, want, &nmod, &shift, &norm)) return HCBK_ERR_ARGS;
+ * epilogue.  A strided batch runs as one pass of each kernel over `nb`
+ * elements starting at element e0 (element e's planes after element e-1's;
+ * its modulus-i GEMM is plane e * nmod + i of the modular GEMM). */
+static int dgemm_crt_elements(HcblasB200State *st, const hcbk_gemm_args *a, int nmod, int shift,
+                              bool norm, int64_t e0, int64_t nb, void *stream,
+                              const char **path) {
   const int beta_bits = 53;
   const int *mods = hcbk_crt_moduli(nullptr);
   /* int8 residues on kind::i8 (INT32 sums exact over all of K) unless K is
@@ -475,17 +474,17 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
    * combine's bulk copies */
   const int64_t ldt = (a->m + 15) & ~int64_t(15);
   const size_t t_pl = up1k((size_t)ldt * a->n);
-  const size_t ea_bytes = up1k(sizeof(int) * a->m), eb_bytes = up1k(sizeof(int) * a->n);
+  const size_t ea_bytes = up1k(sizeof(int) * a->m * nb), eb_bytes = up1k(sizeof(int) * a->n * nb);
   const bool a_k = a->op_a != HCBK_OP_N, b_k = a->op_b == HCBK_OP_N;
   /* per row: the fraction and its reciprocal */
-  const size_t fa_bytes = norm ? up1k(2 * sizeof(double) * a->m) : 0;
-  const size_t fb_bytes = norm ? up1k(2 * sizeof(double) * a->n) : 0;
+  const size_t fa_bytes = norm ? up1k(2 * sizeof(double) * a->m * nb) : 0;
+  const size_t fb_bytes = norm ? up1k(2 * sizeof(double) * a->n * nb) : 0;
   const size_t wa_bytes =
-      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a->m, a->k, a_k)) : 0;
+      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace_batch(a->m, a->k, a_k, nb)) : 0;
   const size_t wb_bytes =
-      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace(a->n, a->k, b_k)) : 0;
+      norm ? up1k((size_t)hcbk_crt_row_exponents_workspace_batch(a->n, a->k, b_k, nb)) : 0;
   const size_t total = ea_bytes + eb_bytes + fa_bytes + fb_bytes + wa_bytes + wb_bytes +
-                       nmod * (a_pl + b_pl + t_pl);
+                       (size_t)nb * nmod * (a_pl + b_pl + t_pl);
   char *ws = static_cast<char *>(ensure_workspace(st, total, stream));
   int *err = device_error_flag(st);
   if (!ws || !err) return HCBK_ERR_NOMEM;
@@ -493,27 +492,30 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   int *exp_b = reinterpret_cast<int *>(ws + ea_bytes);
   double *frac_a = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes) : nullptr;
   double *frac_b = norm ? reinterpret_cast<double *>(ws + ea_bytes + eb_bytes + fa_bytes) : nullptr;
-  double *inv_a = norm ? frac_a + a->m : nullptr;
-  double *inv_b = norm ? frac_b + a->n : nullptr;
+  double *inv_a = norm ? frac_a + a->m * nb : nullptr;
+  double *inv_b = norm ? frac_b + a->n * nb : nullptr;
   char *wa = ws + ea_bytes + eb_bytes + fa_bytes + fb_bytes, *wb = wa + wa_bytes;
   char *pa_base = wb + wb_bytes;
-  char *pb_base = pa_base + nmod * a_pl;
-  char *t_base = pb_base + nmod * b_pl;
+  char *pb_base = pa_base + nb * nmod * a_pl;
+  char *t_base = pb_base + nb * nmod * b_pl;
 
   hcbk_ozaki_prep ea;
   std::memset(&ea, 0, sizeof(ea));
-  ea.src = static_cast<const double *>(a->a) + a->a_off;
+  ea.src = static_cast<const double *>(a->a) + a->a_off + e0 * a->stride_a;
   ea.ld = a->lda;
   ea.k_contig = a->op_a != HCBK_OP_N;
   ea.rows = a->m;
   ea.kdim = a->k;
   ea.exps = exp_a;
+  ea.batch = nb;
+  ea.src_bstride = a->stride_a;
   hcbk_ozaki_prep eb = ea;
-  eb.src = static_cast<const double *>(a->b) + a->b_off;
+  eb.src = static_cast<const double *>(a->b) + a->b_off + e0 * a->stride_b;
   eb.ld = a->ldb;
   eb.k_contig = a->op_b == HCBK_OP_N;
   eb.rows = a->n;
   eb.exps = exp_b;
+  eb.src_bstride = a->stride_b;
   /* row exponents: the row maximum's; when the moduli are too few for the
    * worst case, exponent and 8-bit fraction from the row norm instead */
   auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes) {
@@ -526,7 +528,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   if (!rc) rc = exps(eb, frac_b, inv_b, wb, wb_bytes);
   if (rc) return rc;
 
-  hcbk_crt_prep ra;
+  hcbk_crt_prep ra{};
   ra.src = ea.src;
   ra.ld = ea.ld;
   ra.k_contig = ea.k_contig;
@@ -540,6 +542,9 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   ra.plane_stride = (int64_t)a_pl;
   ra.ld_dst = kp;
   ra.i8 = i8 ? 1 : 0;
+  ra.batch = nb;
+  ra.src_bstride = a->stride_a;
+  ra.planes_bstride = (int64_t)(nmod * a_pl);
   hcbk_crt_prep rb = ra;
   rb.src = eb.src;
   rb.ld = eb.ld;
@@ -549,16 +554,24 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   rb.frac = frac_b;
   rb.planes = pb_base;
   rb.plane_stride = (int64_t)b_pl;
+  rb.src_bstride = a->stride_b;
+  rb.planes_bstride = (int64_t)(nmod * b_pl);
   rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&ra, stream); });
   if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
   if (rc) return rc;
 
-  /* every modulus in one persistent launch: the tile walk covers nmod
-   * planes, so the tile-count thresholds count all of them */
+  /* every modulus of every element in one persistent launch: the tile walk
+   * covers nb * nmod planes, so the tile-count thresholds count all of them */
+  const int64_t planes = nmod * nb;
+  /* 256-row CTA-pair and 256-column tiles only where the GEMM is larger than
+   * the 128-row / 128-column tile (a batch of small GEMMs would otherwise pad
+   * every plane's tile) */
   int pair = st->tc_pair == 2 ||
-             (st->tc_pair == 1 && tiles_of(a->m, a->n, 256, 256) * nmod >= hcbk_sm_count() / 2);
-  int bn = pair || tiles_of(a->m, a->n, 128, 256) * nmod >= hcbk_sm_count() ? 256 : 128;
-  hcbk_crt_gemm g;
+             (st->tc_pair == 1 && a->m > 128 && a->n > 128 &&
+              tiles_of(a->m, a->n, 256, 256) * planes >= hcbk_sm_count() / 2);
+  int bn = pair || (a->n > 128 && tiles_of(a->m, a->n, 128, 256) * planes >= hcbk_sm_count())
+               ? 256 : 128;
+  hcbk_crt_gemm g{};
   g.m = a->m;
   g.n = a->n;
   g.k = a->k;
@@ -576,6 +589,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   g.pair = pair;
   g.bn = bn;
   g.i8 = i8 ? 1 : 0;
+  g.batch = nb;
   if (st->autotune && st->tc_pair == 1) {
     /* every candidate writes the same exact residues: tuning in place is safe */
     static const int cbn[3] = {128, 256, 256}, cpair[3] = {0, 0, 1};
@@ -591,7 +605,7 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   rc = timed_launch(st, stream, "tc.crt_modgemm", [&] { return hcbk_crt_gemm_tc(&g, err, stream); });
   if (rc) return rc;
 
-  hcbk_crt_combine_args cb;
+  hcbk_crt_combine_args cb{};
   cb.m = a->m;
   cb.n = a->n;
   cb.nmod = nmod;
@@ -603,17 +617,70 @@ int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   cb.inv_a = inv_a;
   cb.inv_b = inv_b;
   cb.shift = 2 * beta_bits;
-  cb.c = static_cast<double *>(a->c) + a->c_off;
+  cb.c = static_cast<double *>(a->c) + a->c_off + e0 * a->stride_c;
   cb.ldc = a->ldc;
   cb.alpha = a->alpha_re;
   cb.beta = a->beta_re;
   cb.err = err;
-  static const char *names[HCBK_CRT_MAX_MODULI + 1] = {
-      "", "", "", "", "", "", "", "", "tc.crt_m8", "tc.crt_m9", "tc.crt_m10", "tc.crt_m11",
-      "tc.crt_m12", "tc.crt_m13", "tc.crt_m14", "tc.crt_m15", "tc.crt_m16", "tc.crt_m17",
-      "tc.crt_m18", "tc.crt_m19", "tc.crt_m20"};
-  *path = names[nmod];
+  cb.batch = nb;
+  cb.res_bstride = (int64_t)(nmod * t_pl);
+  cb.c_bstride = a->stride_c;
+  static const char *names[2][HCBK_CRT_MAX_MODULI + 1] = {
+      {"", "", "", "", "", "", "", "", "tc.crt_m8", "tc.crt_m9", "tc.crt_m10", "tc.crt_m11",
+       "tc.crt_m12", "tc.crt_m13", "tc.crt_m14", "tc.crt_m15", "tc.crt_m16", "tc.crt_m17",
+       "tc.crt_m18", "tc.crt_m19", "tc.crt_m20"},
+      {"", "", "", "", "", "", "", "", "tc.crt_m8.batched", "tc.crt_m9.batched",
+       "tc.crt_m10.batched", "tc.crt_m11.batched", "tc.crt_m12.batched", "tc.crt_m13.batched",
+       "tc.crt_m14.batched", "tc.crt_m15.batched", "tc.crt_m16.batched", "tc.crt_m17.batched",
+       "tc.crt_m18.batched", "tc.crt_m19.batched", "tc.crt_m20.batched"}};
+  *path = names[a->batch > 1 ? 1 : 0][nmod];
   return timed_launch(st, stream, "crt.combine", [&] { return hcbk_crt_combine(&cb, stream); });
+}
+
+/* Workspace bytes per element of a CRT DGEMM (planes, exponents, scales and
+ * partial sums), to size the element chunks of a batch. */
+static size_t crt_bytes_per_element(const hcbk_gemm_args *a, int nmod, bool norm, bool i8) {
+  const int64_t kp = (a->k + 15) & ~int64_t(15);
+  const int64_t ldt = (a->m + 15) & ~int64_t(15);
+  const int esz = i8 ? 1 : 2;
+  auto up1k = [](size_t v) { return (v + 1023) & ~size_t(1023); };
+  size_t b = (size_t)nmod * (up1k((size_t)a->m * kp * esz) + up1k((size_t)a->n * kp * esz) +
+                             up1k((size_t)ldt * a->n));
+  b += sizeof(int) * (size_t)(a->m + a->n);
+  if (norm) {
+    b += 2 * sizeof(double) * (size_t)(a->m + a->n);
+    b += (size_t)hcbk_crt_row_exponents_workspace(a->m, a->k, a->op_a != HCBK_OP_N) +
+         (size_t)hcbk_crt_row_exponents_workspace(a->n, a->k, a->op_b == HCBK_OP_N);
+  }
+  return b;
+}
+
+int dgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stream,
+              const char **path) {
+  if (a->a_array || a->batch < 1) return HCBK_ERR_ARGS;
+  int nmod = 0, shift = 0;
+  bool norm = false;
+  if (!crt_plan_rows(a->k, want, &nmod, &shift, &norm)) return HCBK_ERR_ARGS;
+  if (a->batch == 1) return dgemm_crt_elements(st, a, nmod, shift, norm, 0, 1, stream, path);
+  /* a strided batch: the full-width plan's row exponents take one operand
+   * at a time (declined here: the caller runs element by element) */
+  if (!norm) return HCBK_ERR_ARGS;
+  /* elements per pass: the workspace of a pass stays within 2 GiB (or the
+   * handle's limit) and the grids' batch dimension within 65535 */
+  const bool i8 = st->crt_i8 && a->k <= HCBK_CRT_I8_MAX_K;
+  const size_t per = crt_bytes_per_element(a, nmod, norm, i8) + 8192;
+  size_t budget = (size_t)2 << 30;
+  if (st->workspace_limit && st->workspace_limit < budget) budget = st->workspace_limit;
+  int64_t chunk = (int64_t)(budget / per);
+  if (chunk < 1) chunk = 1;
+  if (chunk > 65535) chunk = 65535;
+  for (int64_t e0 = 0; e0 < a->batch; e0 += chunk) {
+    const int64_t nb = a->batch - e0 < chunk ? a->batch - e0 : chunk;
+    const int rc = dgemm_crt_elements(st, a, nmod, shift, norm, e0, nb, stream, path);
+    /* after the first pass, C of earlier elements is written: no fallback */
+    if (rc) return e0 > 0 && (rc == HCBK_ERR_ARGS || rc == HCBK_ERR_ALIGN) ? HCBK_ERR_LAUNCH : rc;
+  }
+  return HCBK_OK;
 }
 
 /* ZGEMM on the CRT path: 3M in modular arithmetic (exact), so one complex
@@ -739,7 +806,7 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   const int bn = pair || tiles_of(a->m, a->n, 128, 256) * nmod >= hcbk_sm_count() ? 256 : 128;
   /* one launch per 3M product (all moduli in each) */
   for (int set = 0; set < 3 && !rc; ++set) {
-    hcbk_crt_gemm g;
+    hcbk_crt_gemm g{};
     g.m = a->m;
     g.n = a->n;
     g.k = a->k;
@@ -1005,6 +1072,15 @@ int dispatch_gemm(HcblasB200State *st, const hcbk_gemm_args *a, void *stream, co
     int rc = hgemm_ptr_grouped(st, a, stream, path);
     if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
     if (log_enabled()) std::fprintf(stderr, "[hcblas] pointer-array hgemm grouped path declined (%d)\n", rc);
+  }
+  if (a->dtype == HCBK_D && st->math_mode == 4 /* HCBLAS_MATH_OZAKI_CRT */ && a->batch > 1 &&
+      !a->a_array) {
+    /* strided CRT DGEMM batch: each pass of the CRT pipeline over a chunk of
+     * elements (the norm-scaled plans; the full-width plan runs per element) */
+    const int want = plan_emulation(4, st->math_param, st->accuracy_bits, HCBK_D, a->k, nullptr);
+    int rc = dgemm_crt(st, a, want, stream, path);
+    if (rc != HCBK_ERR_ALIGN && rc != HCBK_ERR_ARGS) return rc;
+    if (log_enabled()) std::fprintf(stderr, "[hcblas] batched crt path declined (%d)\n", rc);
   }
   if (a->batch > 1 && !a->a_array && emulated_mode(st, a->dtype)) {
     /* strided batch under an emulated math mode: one emulated call per

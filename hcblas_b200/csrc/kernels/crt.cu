@@ -82,6 +82,9 @@ struct ResArgs {
   char *planes;
   int64_t plane_stride; /* bytes */
   int64_t ld_dst;       /* elements */
+  /* strided batch: element e's source at src + e * src_bstride, its exps /
+   * frac at + e * rows, its planes at planes + e * planes_bstride */
+  int64_t batch, src_bstride, planes_bstride;
 };
 
 /* 14-bit limbs of the scaled integer y = rint(x 2^(beta - e)), |y| <= 2^53:
@@ -237,26 +240,28 @@ __global__ void __launch_bounds__(256, 3) crt_res_kcontig(ResArgs a) {
   struct alignas(16) H8 { __half2 v[4]; };
   constexpr int ESZ = I8 ? 1 : 2;
   const int64_t kq = (a.kdim + 7) / 8;
-  const int64_t total = a.rows * kq;
+  const int64_t total = a.rows * kq * a.batch; /* rows of every batch element in turn */
   for (GridWalk g(kq); g.idx < total; g.next()) {
-    const int64_t r = g.r;
+    const int64_t b = g.r / a.rows, r = g.r - b * a.rows;
+    const double *src = a.src + b * a.src_bstride;
+    char *planes = a.planes + b * a.planes_bstride;
     const int64_t k0 = g.c * 8;
-    const int e = a.exps[r];
-    const double f = a.frac ? a.frac[r] : 1.0;
+    const int e = a.exps[g.r];
+    const double f = a.frac ? a.frac[g.r] : 1.0;
     Limbs2 L2[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const Limbs x0 = limbs_of(
-          f * ((k0 + 2 * j < a.kdim) ? a.src[r * a.ld + k0 + 2 * j] : 0.0), e, a.beta);
+          f * ((k0 + 2 * j < a.kdim) ? src[r * a.ld + k0 + 2 * j] : 0.0), e, a.beta);
       const Limbs x1 = limbs_of(
-          f * ((k0 + 2 * j + 1 < a.kdim) ? a.src[r * a.ld + k0 + 2 * j + 1] : 0.0), e, a.beta);
+          f * ((k0 + 2 * j + 1 < a.kdim) ? src[r * a.ld + k0 + 2 * j + 1] : 0.0), e, a.beta);
       L2[j] = pair_limbs(x0, x1);
     }
 #pragma unroll
     for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank operands, no indexed loads */
       if (i >= a.nmod) break;
       const ModPair m = a.mp[i];
-      char *d = a.planes + i * a.plane_stride + (r * a.ld_dst + k0) * ESZ;
+      char *d = planes + i * a.plane_stride + (r * a.ld_dst + k0) * ESZ;
       const bool whole = k0 + 8 <= a.kdim && (reinterpret_cast<uintptr_t>(d) & (8 * ESZ - 1)) == 0;
       if constexpr (I8) {
         uint2 out;
@@ -296,20 +301,22 @@ __global__ void __launch_bounds__(256) crt_res_rcontig(ResArgs a) {
   __shared__ double tile[KT][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
   const int64_t k0 = (int64_t)blockIdx.y * KT;
+  const int64_t b = blockIdx.z; /* batch element */
+  const double *src = a.src + b * a.src_bstride;
   const int tx = threadIdx.x, ty = threadIdx.y; /* 32 x 8 */
 #pragma unroll
   for (int i = 0; i < KT / 8; ++i) {
     const int kl = ty + 8 * i;
     const int64_t r = r0 + tx, k = k0 + kl;
-    tile[kl][tx] = (r < a.rows && k < a.kdim) ? a.src[r + k * a.ld] : 0.0;
+    tile[kl][tx] = (r < a.rows && k < a.kdim) ? src[r + k * a.ld] : 0.0;
   }
   __syncthreads();
   const int t = ty * 32 + tx;
   const int rl = t >> 3, kq = (t & 7) * KPT;
   const int64_t r = r0 + rl, k = k0 + kq;
   if (r >= a.rows || k >= a.kdim) return;
-  const int e = a.exps[r];
-  const double f = a.frac ? a.frac[r] : 1.0;
+  const int e = a.exps[b * a.rows + r];
+  const double f = a.frac ? a.frac[b * a.rows + r] : 1.0;
   Limbs2 L2[NP];
 #pragma unroll
   for (int j = 0; j < NP; ++j)
@@ -317,7 +324,7 @@ __global__ void __launch_bounds__(256) crt_res_rcontig(ResArgs a) {
                        limbs_of(f * tile[kq + 2 * j + 1][rl], e, a.beta));
   const int64_t left = a.kdim - k;
   const int nk = left < KPT ? (int)left : KPT;
-  char *d0 = a.planes + (r * a.ld_dst + k) * (int64_t)ESZ;
+  char *d0 = a.planes + b * a.planes_bstride + (r * a.ld_dst + k) * (int64_t)ESZ;
   const bool vec = nk == KPT && (reinterpret_cast<uintptr_t>(d0) & 7) == 0 &&
                    (a.plane_stride & 7) == 0;
 #pragma unroll
@@ -381,6 +388,9 @@ struct CombArgs {
   double alpha, beta;
   int beta_nonzero;
   int *err; /* device error flag (pipeline wait timed out) */
+  /* strided batch: element e's residue planes at res + e * res_bstride,
+   * exp_a / inv_a at + e * m, exp_b / inv_b at + e * n, C at c + e * c_bstride */
+  int64_t batch, res_bstride, c_bstride;
 };
 
 /* small integer to binary64 without the conversion unit: the bit pattern
@@ -482,7 +492,8 @@ struct TileWalk {
 };
 
 /* Producer of a warp-specialised combine (one thread): tile j of this block
- * (ROWS rows of one column, every residue plane) goes to stage j % STAGES by
+ * (ROWS rows of one column, every residue plane; the columns of a batch's
+ * elements one after the other, ncols in all) goes to stage j % STAGES by
  * 1-D bulk copies once the consumers have released the stage's previous
  * tile; before returning it lets the last copies land (immediately when the
  * consumers took them; bounded when a wait failed), so that no copy writes
@@ -490,6 +501,7 @@ struct TileWalk {
 template <int STAGES, int ROWS>
 __device__ __forceinline__ void ws_produce(const int8_t *res, int64_t res_plane, int64_t ldr,
                                            int nplanes, int64_t row_tiles, int64_t ncols,
+                                           int64_t cols_per, int64_t res_bstride,
                                            int8_t *buf, uint64_t *full, uint64_t *empty,
                                            int *err) {
   using namespace hcbk::tc;
@@ -504,7 +516,9 @@ __device__ __forceinline__ void ws_produce(const int8_t *res, int64_t res_plane,
     const int64_t rows = ldr - r0 < ROWS ? ldr - r0 : ROWS;
     const uint32_t bytes = (uint32_t)rows; /* ldr, r0 multiples of 16 */
     mbar_expect_tx(&full[s], bytes * (uint32_t)nplanes);
-    const int8_t *src = res + w.col * ldr + r0;
+    /* column w.col of the batch: element e's column c */
+    const int64_t e = w.col / cols_per, c = w.col - e * cols_per;
+    const int8_t *src = res + e * res_bstride + c * ldr + r0;
     int8_t *dst = buf + s * stage_elems;
     for (int p = 0; p < nplanes; ++p)
       bulk_load_1d(dst + p * ROWS, src + p * res_plane, bytes, &full[s]);
@@ -555,17 +569,20 @@ __global__ void __launch_bounds__(CMB_BLOCK, 5) crt_combine_kernel(const __grid_
 
   if (warp == CMB_CONSUMERS) { /* producer */
     if (lane == 0)
-      ws_produce<CMB_STAGES, CMB_ROWS>(a.res, a.res_plane, a.ldr, nmod, row_tiles, a.n, buf,
-                                       full, empty, a.err);
+      ws_produce<CMB_STAGES, CMB_ROWS>(a.res, a.res_plane, a.ldr, nmod, row_tiles,
+                                       a.n * a.batch, a.n, a.res_bstride, buf, full, empty,
+                                       a.err);
     return;
   }
 
   /* ------------------------------------------------ consumers -- */
-  for (TileWalk<CMB_STAGES> w((int)first, (int)stride, (int)row_tiles); w.col < a.n; w.next()) {
+  const int64_t ncols = a.n * a.batch; /* the columns of every batch element in turn */
+  for (TileWalk<CMB_STAGES> w((int)first, (int)stride, (int)row_tiles); w.col < ncols; w.next()) {
     const int s = w.s;
     if (!__all_sync(0xffffffffu, mbar_wait(&full[s], w.ph, a.err, ERR_TIMEOUT_COMBINE))) break;
     const int8_t *R = buf + s * stage_elems;
-    const int64_t row = w.rt * CMB_ROWS + CMB_RPT * tid, col = w.col;
+    const int64_t be = w.col / a.n; /* batch element */
+    const int64_t row = w.rt * CMB_ROWS + CMB_RPT * tid, col = w.col - be * a.n;
     if (row < a.m) {
       CrtAcc<NC> acc[CMB_RPT];
 #pragma unroll
@@ -581,14 +598,15 @@ __global__ void __launch_bounds__(CMB_BLOCK, 5) crt_combine_kernel(const __grid_
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]); /* the stage's residues are in registers */
-      const int eb = a.exp_b[col];
-      const double ib = a.inv_b ? a.inv_b[col] : 1.0;
-      double *dst = a.c + row + col * a.ldc;
+      const int eb = a.exp_b[be * a.n + col];
+      const double ib = a.inv_b ? a.inv_b[be * a.n + col] : 1.0;
+      double *dst = a.c + be * a.c_bstride + row + col * a.ldc;
+      const int64_t ra = be * a.m + row;
 #pragma unroll
       for (int u = 0; u < CMB_RPT; ++u) {
         if (row + u >= a.m) break;
-        double v = acc[u].finish(a, a.exp_a[row + u], eb);
-        if (a.inv_a) v *= a.inv_a[row + u] * ib;
+        double v = acc[u].finish(a, a.exp_a[ra + u], eb);
+        if (a.inv_a) v *= a.inv_a[ra + u] * ib;
         double o = a.alpha * v;
         if (a.beta_nonzero) o = fma(a.beta, dst[u], o);
         dst[u] = o;
@@ -986,7 +1004,7 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
   if (warp == ZCMB_CONSUMERS) { /* producer */
     if (lane == 0)
       ws_produce<ZCMB_STAGES, ZCMB_ROWS>(a.g.res, a.g.res_plane, a.g.ldr, 3 * nmod, row_tiles,
-                                         a.g.n, buf, full, empty, a.g.err);
+                                         a.g.n, a.g.n, 0, buf, full, empty, a.g.err);
     return;
   }
   for (TileWalk<ZCMB_STAGES> w((int)blockIdx.x, (int)gridDim.x, (int)row_tiles); w.col < a.g.n;
@@ -1089,8 +1107,11 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
   a.planes = static_cast<char *>(in->planes);
   a.plane_stride = in->plane_stride;
   a.ld_dst = in->ld_dst;
+  a.batch = in->batch > 1 ? in->batch : 1;
+  a.src_bstride = a.batch > 1 ? in->src_bstride : 0;
+  a.planes_bstride = a.batch > 1 ? in->planes_bstride : 0;
   if (in->k_contig) {
-    const int64_t total = a.rows * ((a.kdim + 7) / 8);
+    const int64_t total = a.rows * ((a.kdim + 7) / 8) * a.batch;
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (blocks > cap) blocks = cap;
@@ -1101,11 +1122,12 @@ extern "C" int hcbk_crt_residues(const hcbk_crt_prep *in, void *stream) {
   } else {
     const int64_t kt = in->i8 ? 64 : 32; /* k per tile (crt_res_rcontig's KT) */
     const int64_t gx = (a.rows + 31) / 32, gy = (a.kdim + kt - 1) / kt;
-    if (gy > 65535) return HCBK_ERR_ARGS;
+    if (gy > 65535 || a.batch > 65535) return HCBK_ERR_ARGS;
+    const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)a.batch);
     if (in->i8)
-      crt_res_rcontig<true><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+      crt_res_rcontig<true><<<grid, dim3(32, 8), 0, st>>>(a);
     else
-      crt_res_rcontig<false><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(a);
+      crt_res_rcontig<false><<<grid, dim3(32, 8), 0, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
@@ -1134,7 +1156,12 @@ extern "C" int hcbk_crt_combine(const hcbk_crt_combine_args *in, void *stream) {
   a.beta = in->beta;
   a.beta_nonzero = in->beta != 0.0;
   a.err = in->err;
-  const int64_t ntiles = (a.m + CMB_ROWS - 1) / CMB_ROWS * a.n;
+  a.batch = in->batch > 1 ? in->batch : 1;
+  a.res_bstride = a.batch > 1 ? in->res_bstride : 0;
+  a.c_bstride = a.batch > 1 ? in->c_bstride : 0;
+  if (a.res_bstride & 15) return HCBK_ERR_ARGS; /* bulk copies start on 16 bytes */
+  const int64_t ntiles = (a.m + CMB_ROWS - 1) / CMB_ROWS * a.n * a.batch;
+  if (ntiles > 0x7fffffff) return HCBK_ERR_ARGS;
   const size_t smem = (size_t)CMB_STAGES * a.nmod * CMB_ROWS * sizeof(int8_t);
   int64_t grid = 0;
   int rc;
@@ -1219,6 +1246,8 @@ extern "C" int hcbk_zcrt_combine(const hcbk_zcrt_combine_args *in, void *stream)
   a.g.beta = 0.0;
   a.g.beta_nonzero = in->beta_re != 0.0 || in->beta_im != 0.0;
   a.g.err = in->err;
+  a.g.batch = 1; /* the complex combine takes one GEMM */
+  a.g.res_bstride = a.g.c_bstride = 0;
   a.exp_a_pair = in->exp_a_pair;
   a.exp_b_pair = in->exp_b_pair;
   a.c = static_cast<double2 *>(in->c);

@@ -201,6 +201,10 @@ typedef struct hcbk_ozaki_prep {
   int64_t ld_dst;       /* elements between rows */
   int f16;              /* 0: int8 slices of 7 bits; 1: binary16 slices of 8 bits */
   const float *src_f32; /* exponents and slices only: an FP32 source instead of src */
+  /* hcbk_crt_row_scales only: a strided batch of operands (0 or 1: one);
+   * element e's source at src + e * src_bstride, its exps / frac / inv at
+   * + e * rows (the other functions take one operand) */
+  int64_t batch, src_bstride;
 } hcbk_ozaki_prep;
 int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
 
@@ -213,6 +217,9 @@ int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream);
  * scale (the real and imaginary rows of a complex operand's real view);
  * exps / frac / inv then hold rows / 2 entries. */
 int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, int k_contig);
+/* the same for a batch of `batch` operands of rows x kdim */
+int64_t hcbk_crt_row_exponents_workspace_batch(int64_t rows, int64_t kdim, int k_contig,
+                                               int64_t batch);
 int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, int pair_rows, double *frac,
                         double *inv, void *work, int64_t work_bytes, void *stream);
 int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream);
@@ -304,6 +311,10 @@ typedef struct hcbk_crt_prep {
   int64_t plane_stride; /* bytes */
   int64_t ld_dst;       /* elements */
   int i8;               /* 1: int8 planes (hcbk_crt_gemm's i8 path), 0: binary16 */
+  /* a strided batch of operands (batch 0 or 1: one): element e's source at
+   * src + e * src_bstride, its exps / frac at + e * rows, its nmod planes at
+   * planes + e * planes_bstride bytes */
+  int64_t batch, src_bstride, planes_bstride;
 } hcbk_crt_prep;
 int hcbk_crt_residues(const hcbk_crt_prep *a, void *stream);
 
@@ -329,6 +340,8 @@ typedef struct hcbk_crt_gemm {
   int bn;   /* tile columns: 128 or 256 */
   int pair; /* 1: CTA pairs, 256 x 256 tiles (bn = 256) */
   int i8;   /* 1: int8 residue planes on kind::i8 */
+  int64_t batch; /* GEMMs in the launch (0 or 1: one); element e's modulus-i
+                    planes are plane e * nmod + i of A, B and T */
 } hcbk_crt_gemm;
 int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream);
 
@@ -352,6 +365,10 @@ typedef struct hcbk_crt_combine_args {
   int64_t ldc;
   double alpha, beta;
   int *err; /* device error flag: set when the pipeline's wait times out */
+  /* a strided batch (batch 0 or 1: one): element e's residue planes at
+   * res + e * res_bstride bytes, its exp_a / inv_a at + e * m, exp_b / inv_b
+   * at + e * n, its C at c + e * c_bstride */
+  int64_t batch, res_bstride, c_bstride;
 } hcbk_crt_combine_args;
 int hcbk_crt_combine(const hcbk_crt_combine_args *a, void *stream);
 

@@ -369,12 +369,15 @@ __device__ __forceinline__ void row_scale(int emax, int acc_e, double s, int nb,
  * row allows) */
 template <int VEC>
 __global__ void crt_rowexp_kcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
-                                   int nb, int *exps, double *frac, double *inv) {
+                                   int nb, int *exps, double *frac, double *inv,
+                                   int64_t rows_per, int64_t bstride) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = warp; r < rows; r += nwarps) {
-    const double *row = src + r * ld;
+    /* rows of a batch: element r / rows_per, its row r % rows_per */
+    const int64_t e = r / rows_per;
+    const double *row = src + e * bstride + (r - e * rows_per) * ld;
     unsigned long long m = 0;
     NormAcc acc;
     na_init(acc);
@@ -433,9 +436,14 @@ __global__ void crt_rowexp_kcontig(const double *src, int64_t ld, int64_t rows, 
  * maximum's bit pattern and its running sum (exponent, sum) */
 template <int VEC>
 __global__ void crt_rowexp_rcontig(const double *src, int64_t ld, int64_t rows, int64_t kdim,
-                                   int64_t kchunk, unsigned long long *pm, int *pe, double *ps) {
+                                   int64_t kchunk, unsigned long long *pm, int *pe, double *ps,
+                                   int64_t bstride) {
   const int64_t r = VEC * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
   if (r >= rows) return;
+  /* element blockIdx.z of a batch: its source, and its rows' partials after
+   * those of the elements before it */
+  src += (int64_t)blockIdx.z * bstride;
+  const int64_t rbase = (int64_t)blockIdx.z * rows;
   const int64_t k0 = (int64_t)blockIdx.y * kchunk;
   const int64_t k1 = (k0 + kchunk < kdim) ? k0 + kchunk : kdim;
   unsigned long long m[VEC];
@@ -477,7 +485,7 @@ __global__ void crt_rowexp_rcontig(const double *src, int64_t ld, int64_t rows, 
   }
 #pragma unroll
   for (int u = 0; u < VEC; ++u) { /* partials stored [row][chunk] for the finish */
-    const int64_t o = (r + u) * gridDim.y + blockIdx.y;
+    const int64_t o = (rbase + r + u) * gridDim.y + blockIdx.y;
     pm[o] = m[u];
     pe[o] = acc[u].e;
     ps[o] = acc[u].s;
@@ -590,7 +598,7 @@ static void rowexp_split(int64_t rows, int64_t kdim, int64_t *ky, int64_t *kchun
 
 extern "C" int hcbk_ozaki_exponents(const hcbk_ozaki_prep *a, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (a->rows <= 0 || a->kdim <= 0) return HCBK_ERR_ARGS;
+  if (a->rows <= 0 || a->kdim <= 0 || a->batch > 1) return HCBK_ERR_ARGS;
   if (a->src_f32) { /* FP32 source: element loads, widened in registers */
     if (a->k_contig) {
       int64_t blocks = (a->rows * 32 + 255) / 256;
@@ -655,7 +663,7 @@ extern "C" int hcbk_ozaki_groups_combine(const hcbk_ozaki_groups_combine_args *a
 
 extern "C" int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (a->rows <= 0 || a->kdim <= 0) return HCBK_ERR_ARGS;
+  if (a->rows <= 0 || a->kdim <= 0 || a->batch > 1) return HCBK_ERR_ARGS;
   switch (a->slices) {
     case 3: return launch_slice_any<3>(a, st);
     case 4: return launch_slice_any<4>(a, st);
@@ -667,11 +675,17 @@ extern "C" int hcbk_ozaki_slice(const hcbk_ozaki_prep *a, void *stream) {
   }
 }
 
-extern "C" int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, int k_contig) {
-  if (k_contig || rows <= 0 || kdim <= 0) return 0;
+extern "C" int64_t hcbk_crt_row_exponents_workspace_batch(int64_t rows, int64_t kdim,
+                                                           int k_contig, int64_t batch) {
+  if (k_contig || rows <= 0 || kdim <= 0 || batch <= 0) return 0;
   int64_t ky, kc;
   rowexp_split(rows, kdim, &ky, &kc);
-  return ky * rows * (int64_t)(sizeof(unsigned long long) + sizeof(double) + sizeof(int)) + 256;
+  return ky * rows * batch * (int64_t)(sizeof(unsigned long long) + sizeof(double) + sizeof(int)) +
+         256;
+}
+
+extern "C" int64_t hcbk_crt_row_exponents_workspace(int64_t rows, int64_t kdim, int k_contig) {
+  return hcbk_crt_row_exponents_workspace_batch(rows, kdim, k_contig, 1);
 }
 
 extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, int pair_rows, double *frac,
@@ -679,39 +693,48 @@ extern "C" int hcbk_crt_row_scales(const hcbk_ozaki_prep *a, int nb, int pair_ro
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a->rows <= 0 || a->kdim <= 0 || !frac || !inv) return HCBK_ERR_ARGS;
   if (pair_rows && (a->k_contig || (a->rows & 1))) return HCBK_ERR_ARGS;
-  const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0;
+  /* a batch: every element's rows in turn (exps / frac / inv of element e
+   * at + e * rows); one element when batch is 0 or 1 */
+  const int64_t batch = a->batch > 1 ? a->batch : 1;
+  const int64_t bstride = batch > 1 ? a->src_bstride : 0;
+  if (batch > 65535 && !a->k_contig) return HCBK_ERR_ARGS;
+  const int64_t all_rows = a->rows * batch;
+  const bool al16 = (reinterpret_cast<uintptr_t>(a->src) & 15) == 0 && (a->ld & 1) == 0 &&
+                    (bstride & 1) == 0;
   if (a->k_contig) {
-    int64_t blocks = (a->rows * 32 + 255) / 256;
+    int64_t blocks = (all_rows * 32 + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (blocks > cap) blocks = cap;
     if (al16 && (a->kdim & 1) == 0)
-      crt_rowexp_kcontig<2><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, nb,
-                                                              a->exps, frac, inv);
+      crt_rowexp_kcontig<2><<<(unsigned)blocks, 256, 0, st>>>(
+          a->src, a->ld, all_rows, a->kdim, nb, a->exps, frac, inv, a->rows, bstride);
     else
-      crt_rowexp_kcontig<1><<<(unsigned)blocks, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, nb,
-                                                              a->exps, frac, inv);
+      crt_rowexp_kcontig<1><<<(unsigned)blocks, 256, 0, st>>>(
+          a->src, a->ld, all_rows, a->kdim, nb, a->exps, frac, inv, a->rows, bstride);
   } else {
     int64_t ky, kc;
     rowexp_split(a->rows, a->kdim, &ky, &kc);
     if (ky > 65535 || !work ||
-        work_bytes < hcbk_crt_row_exponents_workspace(a->rows, a->kdim, 0))
+        work_bytes < hcbk_crt_row_exponents_workspace_batch(a->rows, a->kdim, 0, batch))
       return HCBK_ERR_ARGS;
     unsigned long long *pm = static_cast<unsigned long long *>(work);
-    double *ps = reinterpret_cast<double *>(pm + ky * a->rows);
-    int *pe = reinterpret_cast<int *>(ps + ky * a->rows);
+    double *ps = reinterpret_cast<double *>(pm + ky * all_rows);
+    int *pe = reinterpret_cast<int *>(ps + ky * all_rows);
     const int vec = (al16 && (a->rows & 1) == 0) ? 2 : 1;
-    const dim3 grid((unsigned)((a->rows / vec + 255) / 256), (unsigned)ky);
+    const dim3 grid((unsigned)((a->rows / vec + 255) / 256), (unsigned)ky, (unsigned)batch);
     if (vec == 2)
-      crt_rowexp_rcontig<2><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kc, pm, pe, ps);
+      crt_rowexp_rcontig<2><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kc, pm, pe, ps,
+                                                   bstride);
     else
-      crt_rowexp_rcontig<1><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kc, pm, pe, ps);
-    int64_t fb = (a->rows * 32 + 255) / 256;
+      crt_rowexp_rcontig<1><<<grid, 256, 0, st>>>(a->src, a->ld, a->rows, a->kdim, kc, pm, pe, ps,
+                                                   bstride);
+    int64_t fb = (all_rows * 32 + 255) / 256;
     const int64_t cap = (int64_t)hcbk_sm_count() * 16;
     if (fb > cap) fb = cap;
-    /* partials sit [row][chunk]: two consecutive rows merged are one row of
-     * twice the chunks */
+    /* partials sit [row][chunk], element after element: two consecutive
+     * rows merged are one row of twice the chunks */
     const int g = pair_rows ? 2 : 1;
-    crt_rowexp_finish<<<(unsigned)fb, 256, 0, st>>>(pm, pe, ps, a->rows / g, (int)ky * g, nb,
+    crt_rowexp_finish<<<(unsigned)fb, 256, 0, st>>>(pm, pe, ps, all_rows / g, (int)ky * g, nb,
                                                      a->exps, frac, inv);
   }
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;

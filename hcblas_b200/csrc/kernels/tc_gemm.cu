@@ -68,14 +68,22 @@ struct TcParams {
    * on that stage runs out (accepted only for one tile of one K block with
    * beta == 0, where nothing else is in flight) */
   int inject_skip_load;
-  /* modular (CRT) epilogue: output plane i is reduced modulo mod_tab[i];
-   * planes of A, B (3-D tensor maps) and C (c_plane_stride elements apart)
-   * are batched into one launch */
+  /* modular (CRT) epilogue: output plane i is reduced modulo
+   * mod_tab[i % mod_period] (mod_period = moduli per GEMM; a batch of GEMMs
+   * lays its elements' planes one after the other); planes of A, B (3-D
+   * tensor maps) and C (c_plane_stride elements apart) are batched into one
+   * launch */
   int nplanes;
+  int mod_period;
   long long c_plane_stride;
   int mod_tab[HCBK_CRT_MAX_MODULI];
   float inv_mod_tab[HCBK_CRT_MAX_MODULI];
 };
+
+/* the modulus slot of a plane of a (batched) modular GEMM */
+__device__ __forceinline__ int mod_slot(const TcParams &p, int plane) {
+  return plane < p.mod_period ? plane : plane % p.mod_period;
+}
 
 /* ---------------------------------------------------------- recipes -- */
 
@@ -338,8 +346,9 @@ struct EpiModP {
   /* reduce this warp's 32 lanes x BN columns of one buffer in place */
   template <int BN>
   static __device__ __forceinline__ void rmw(const TcParams &p, uint32_t tbase, int plane) {
-    const float pf = static_cast<float>(p.mod_tab[plane]);
-    const float inv = p.inv_mod_tab[plane];
+    const int slot = mod_slot(p, plane);
+    const float pf = static_cast<float>(p.mod_tab[slot]);
+    const float inv = p.inv_mod_tab[slot];
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
       uint32_t r[32];
@@ -368,9 +377,10 @@ struct EpiModP {
   static __device__ __forceinline__ void final_store(const TcParams &p, uint32_t ta, uint8_t *out,
                                                      int m0, int n0, int plane) {
     const int lane = threadIdx.x & 31;
-    const int mod = p.mod_tab[plane];
+    const int slot = mod_slot(p, plane);
+    const int mod = p.mod_tab[slot];
     const float pf = static_cast<float>(mod);
-    const float inv = p.inv_mod_tab[plane];
+    const float inv = p.inv_mod_tab[slot];
     const float hp = static_cast<float>((mod - 1) >> 1);
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
@@ -508,9 +518,10 @@ struct EpiModPi8 {
                                                      int m0, int n0, int plane) {
     static_assert(BN % 64 == 0, "64 columns per TMEM wait");
     const int lane = threadIdx.x & 31;
-    const int mod = p.mod_tab[plane];
+    const int slot = mod_slot(p, plane);
+    const int mod = p.mod_tab[slot];
     const float pf = static_cast<float>(mod);
-    const float inv = p.inv_mod_tab[plane];
+    const float inv = p.inv_mod_tab[slot];
     int c16 = (1 << 16) % mod; /* 2^16 mod p, symmetric */
     if (c16 > (mod - 1) / 2) c16 -= mod;
 #pragma unroll 1
@@ -1412,17 +1423,26 @@ extern "C" int hcbk_crt_gemm_tc(const hcbk_crt_gemm *g, int *err, void *stream) 
   p.m = (int)g->m;
   p.n = (int)g->n;
   p.k = (int)g->k;
+  /* a batch of GEMMs: element e's modulus-i planes are plane e * nmod + i
+   * of A, B and T */
+  const int64_t batch = g->batch > 1 ? g->batch : 1;
+  const int64_t planes = batch * g->nmod;
+  const int64_t tiles_m = (g->m + 127) / 128, tiles_n = (g->n + g->bn - 1) / g->bn;
+  if (planes > 0x7fffffff || tiles_m * tiles_n * planes > 0x7fffffff) return HCBK_ERR_ARGS;
   auto planes_map = g->i8 ? make_map_planes_s8 : make_map_planes_f16;
-  int rc = planes_map(&p.ta[0], g->a_planes, g->k, g->m, g->nmod, g->ld_a, g->a_plane_stride, BM);
+  int rc = planes_map(&p.ta[0], g->a_planes, g->k, g->m, (int)planes, g->ld_a, g->a_plane_stride,
+                      BM);
   if (rc) return rc;
   const uint32_t b_rows = g->pair ? g->bn / 2 : g->bn; /* B rows per CTA */
-  rc = planes_map(&p.tb[0], g->b_planes, g->k, g->n, g->nmod, g->ld_b, g->b_plane_stride, b_rows);
+  rc = planes_map(&p.tb[0], g->b_planes, g->k, g->n, (int)planes, g->ld_b, g->b_plane_stride,
+                  b_rows);
   if (rc) return rc;
   p.c = g->t;
   p.ldc = g->ldt;
-  p.nplanes = g->nmod;
+  p.nplanes = (int)planes;
+  p.mod_period = g->nmod;
   p.c_plane_stride = g->t_plane_stride;
-  rc = make_map_out_i8(&p.tc, g->t, g->m, g->n, g->nmod, g->ldt, g->t_plane_stride);
+  rc = make_map_out_i8(&p.tc, g->t, g->m, g->n, (int)planes, g->ldt, g->t_plane_stride);
   if (rc) return rc;
   for (int i = 0; i < g->nmod; ++i) {
     p.mod_tab[i] = g->moduli[i];
