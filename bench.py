@@ -773,6 +773,13 @@ def summarize(line):
     if c4a:
         out["batch_f16_ptr_512x128"] = {"ms": c4a.get("ms"), "tflops": c4a.get("tflops"),
                                         "speedup_vs_per_problem": c4a.get("speedup_vs_per_problem")}
+    cb = sec.get("dgemm_crt_strided_batch_128x256^3")
+    if cb:
+        out["dgemm_crt_batch_128x256"] = {
+            "batched_ms": pick(cb, "crt_m14_batched", "ms"),
+            "per_element_ms": cb.get("crt_m14_per_element_calls_ms"),
+            "speedup_vs_per_element": cb.get("speedup_batched_vs_per_element"),
+            "native_ms": pick(cb, "native", "ms")}
     for key, short in (("hgemm_grouped_4096_uneven", "grouped_f16"),
                        ("sgemm_grouped_4096_uneven_split_bf16x6", "grouped_f32_split")):
         gq = sec.get(key)
@@ -1000,6 +1007,42 @@ def run_secondary_small(hb, h, stream, torch, O, timed):
                                    "tflops": round(2 * b * n ** 3 / ms_split_p / 1e9, 2)},
         "speedup_split_strided_vs_per_problem_plain": round(ms_plain_single / ms_split, 2)}
     del dA, dB, dC, pA, pB, pC
+    # a strided batch of CRT DGEMMs (128 x 256^3, 14 moduli) in one pass per
+    # kernel, beside the native batch and one CRT call per element
+    nd, bd = 256, 128
+    rngd = np.random.default_rng(12)
+    dA = hb.DeviceArray(h, rngd.standard_normal(nd * nd * bd))
+    dB = hb.DeviceArray(h, rngd.standard_normal(nd * nd * bd))
+    dC = hb.DeviceArray(h, np.zeros(nd * nd * bd))
+    one_d, zero_d = np.array([1.0]), np.array([0.0])
+    Ld = hb.lib()
+
+    def dbatch():
+        assert hb.gemm_strided_batched(h, 0, 1, nd, nd, nd, 1.0, dA, nd, nd * nd, dB, nd, nd * nd,
+                                       0.0, dC, nd, nd * nd, bd) == 0
+
+    def dper_element():
+        for i in range(bd):
+            o = 8 * i * nd * nd
+            Ld.hcblasDgemm(h, 0, 1, nd, nd, nd, one_d.ctypes.data, dA.ptr + o, nd, dB.ptr + o, nd,
+                           zero_d.ctypes.data, dC.ptr + o, nd)
+    flop_d = 2.0 * nd ** 3 * bd
+    ms_dn = timed(dbatch)
+    path_dn = hb.hcblasGetLastPath(h)
+    hb.hcblasSetMathMode(h, MATH_CRT, 14)
+    try:
+        ms_dc = timed(dbatch)
+        path_dc = hb.hcblasGetLastPath(h)
+        ms_de = timed(dper_element)
+    finally:
+        hb.hcblasSetMathMode(h, 0, 0)
+    out["dgemm_crt_strided_batch_128x256^3"] = {
+        "native": {"path": path_dn, "ms": round(ms_dn, 4), "tflops": round(flop_d / ms_dn / 1e9, 2)},
+        "crt_m14_batched": {"path": path_dc, "ms": round(ms_dc, 4),
+                            "tflops": round(flop_d / ms_dc / 1e9, 2)},
+        "crt_m14_per_element_calls_ms": round(ms_de, 4),
+        "speedup_batched_vs_per_element": round(ms_de / ms_dc, 2)}
+    del dA, dB, dC
     # C4b: grouped 4096 problems, M, N, K log-uniform in [16, 1024], seed 3, mixed N/T
     import bench_cases as profile_cases
     call, keep = profile_cases.CASES["hgemm_grouped_4096"](h)

@@ -207,7 +207,11 @@ hcblasStatus_t hcblasHgemmBatched(hcblasHandle_t handle, hcblasOperation_t trans
 /* Extension: strided batched GEMM, X_i = X + i * strideX (elements).  The
  * reference's closest form is its row-major batch kernel addressing
  * `A_batchOffset * elt` (sgemm_array_kernels_rMajor_batch.cpp:67), which its
- * wrapper never reaches (sgemm_array_wrapper.cpp:113-151). */
+ * wrapper never reaches (sgemm_array_wrapper.cpp:113-151).  Under an
+ * emulated math mode every element runs on that mode's path: split-BF16
+ * SGEMM batches on the grouped kernel, CRT DGEMM batches with a norm-scaled
+ * plan (a moduli count below the full width, or an accuracy target) as one
+ * pass of each CRT kernel over the batch, the others element by element. */
 hcblasStatus_t hcblasSgemmStridedBatched(hcblasHandle_t handle, hcblasOperation_t transa,
                                          hcblasOperation_t transb, int m, int n, int k,
                                          const float *alpha, const float *A, int lda,
