@@ -82,7 +82,7 @@ struct TcParams {
 
 /* the modulus slot of a plane of a (batched) modular GEMM */
 __device__ __forceinline__ int mod_slot(const TcParams &p, int plane) {
-  return plane < p.mod_period ? plane : plane % p.mod_period;
+  return (p.mod_period <= 0 || plane < p.mod_period) ? plane : plane % p.mod_period;
 }
 
 /* ---------------------------------------------------------- recipes -- */
