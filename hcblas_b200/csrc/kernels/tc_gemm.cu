@@ -239,6 +239,22 @@ template <typename OutT> struct EpiAlphaBeta {
     }
   }
 
+  /* Configurations without output staging read C with plain loads in the
+   * tile's final store, one 32-column group at a time, each group a full
+   * DRAM latency.  At the start of a tile (its MMAs still running) every
+   * epilogue thread asks L2 for its row of the tile's C, so that those loads
+   * hit L2 instead. */
+  static constexpr bool L2_PREFETCH_C = true;
+  template <int BN>
+  static __device__ __forceinline__ void prefetch_c_l2(const TcParams &p, int m, int n0) {
+    if (!p.beta_nonzero || m >= p.m) return;
+    const OutT *C = static_cast<const OutT *>(p.c) + (long long)m + (long long)n0 * p.ldc;
+    const int nvalid = p.n - n0 < BN ? p.n - n0 : BN;
+#pragma unroll 4
+    for (int j = 0; j < nvalid; ++j)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (long long)j * p.ldc));
+  }
+
   /* C[m, n0 .. n0+31] = alpha * v + beta * C: all C loads are issued before
    * the first store, so they overlap instead of serialising behind stores
    * that might alias them. */
@@ -472,6 +488,12 @@ template <class E> struct EpiWarps<E, std::void_t<decltype(E::EPI_WARPS)>> {
   static constexpr int value = E::EPI_WARPS;
 };
 template <class E> struct CatK<E, std::void_t<decltype(E::CAT_K)>> : std::bool_constant<E::CAT_K> {};
+/* epilogues whose final store reads C with plain loads and can ask L2 for
+ * it ahead of time (L2_PREFETCH_C, default none) */
+template <class E, class = void> struct EpiL2Prefetch : std::false_type {};
+template <class E>
+struct EpiL2Prefetch<E, std::void_t<decltype(E::L2_PREFETCH_C)>>
+    : std::bool_constant<E::L2_PREFETCH_C> {};
 
 /* Modular epilogue of the int8 path: the INT32 accumulator holds the
  * exact sum over all of K (|s| <= K 127^2 <= 2114125824 for K <= 131072),
@@ -964,6 +986,8 @@ __global__ void __launch_bounds__(64 + 32 * EpiWarps<EPI>::value, 1)
       const int tm = tc_.m, tn = tc_.n;
       const int m = (tm * CG + (int)rank) * BM + q * 32 + lane;
       if constexpr (Cfg::OUT_BYTES > 0) EPI::template prefetch_c<BN>(p, m - lane, tn * BN, ostage);
+      else if constexpr (EpiL2Prefetch<EPI>::value && !EPI::PLANE_BATCH)
+        EPI::template prefetch_c_l2<BN>(p, m, tn * BN);
       if constexpr (PROMOTE_KB == 0) {
         const int b = ci % NBUF;
         const uint32_t tph = (ci / NBUF) & 1;
