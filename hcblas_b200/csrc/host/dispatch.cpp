@@ -518,15 +518,13 @@ static int dgemm_crt_elements(HcblasB200State *st, const hcbk_gemm_args *a, int 
   eb.src_bstride = a->stride_b;
   /* row exponents: the row maximum's; when the moduli are too few for the
    * worst case, exponent and 8-bit fraction from the row norm instead */
-  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes) {
-    return timed_launch(st, stream, "ozaki.exponents", [&] {
-      return norm ? hcbk_crt_row_scales(&p, 53 - shift, 0, frac, inv, w, (int64_t)wbytes, stream)
-                  : hcbk_ozaki_exponents(&p, stream);
+  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes,
+                  void *s) {
+    return timed_launch(st, s, "ozaki.exponents", [&] {
+      return norm ? hcbk_crt_row_scales(&p, 53 - shift, 0, frac, inv, w, (int64_t)wbytes, s)
+                  : hcbk_ozaki_exponents(&p, s);
     }, p.k_contig ? 1 : 2);
   };
-  int rc = exps(ea, frac_a, inv_a, wa, wa_bytes);
-  if (!rc) rc = exps(eb, frac_b, inv_b, wb, wb_bytes);
-  if (rc) return rc;
 
   hcbk_crt_prep ra{};
   ra.src = ea.src;
@@ -556,8 +554,20 @@ static int dgemm_crt_elements(HcblasB200State *st, const hcbk_gemm_args *a, int 
   rb.plane_stride = (int64_t)b_pl;
   rb.src_bstride = a->stride_b;
   rb.planes_bstride = (int64_t)(nmod * b_pl);
-  rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&ra, stream); });
-  if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&rb, stream); });
+  /* the two operands' passes are independent: op(B)'s go to the handle's
+   * second stream, so that its memory-bound row-scale pass overlaps op(A)'s
+   * and the residue passes fill each other's tails */
+  void *aux = aux_fork(st, stream);
+  void *sb = aux ? aux : stream;
+  int rc = exps(ea, frac_a, inv_a, wa, wa_bytes, stream);
+  int rcb = exps(eb, frac_b, inv_b, wb, wb_bytes, sb);
+  if (!rc) rc = timed_launch(st, stream, "crt.residues", [&] { return hcbk_crt_residues(&ra, stream); });
+  if (!rcb) rcb = timed_launch(st, sb, "crt.residues", [&] { return hcbk_crt_residues(&rb, sb); });
+  if (aux) {
+    const int rcj = aux_join(st, stream);
+    if (!rcb) rcb = rcj;
+  }
+  if (!rc) rc = rcb;
   if (rc) return rc;
 
   /* every modulus of every element in one persistent launch: the tile walk
@@ -758,16 +768,14 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   eb.rows = b_k ? a->n : 2 * a->n;
   eb.kdim = b_k ? 2 * a->k : a->k;
   eb.exps = exp_b;
-  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes) {
-    return timed_launch(st, stream, "ozaki.exponents", [&] {
+  auto exps = [&](const hcbk_ozaki_prep &p, double *frac, double *inv, char *w, size_t wbytes,
+                  void *s) {
+    return timed_launch(st, s, "ozaki.exponents", [&] {
       return norm ? hcbk_crt_row_scales(&p, 53 - shift, p.k_contig ? 0 : 1, frac, inv, w,
-                                        (int64_t)wbytes, stream)
-                  : hcbk_ozaki_exponents(&p, stream);
+                                        (int64_t)wbytes, s)
+                  : hcbk_ozaki_exponents(&p, s);
     }, p.k_contig ? 1 : 2);
   };
-  int rc = exps(ea, frac_a, inv_a, wa, wa_bytes);
-  if (!rc) rc = exps(eb, frac_b, inv_b, wb, wb_bytes);
-  if (rc) return rc;
 
   hcbk_zcrt_prep ra;
   std::memset(&ra, 0, sizeof(ra));
@@ -797,8 +805,18 @@ int zgemm_crt(HcblasB200State *st, const hcbk_gemm_args *a, int want, void *stre
   rb.frac = frac_b;
   rb.planes = pb_base;
   rb.plane_stride = (int64_t)b_pl;
-  rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&ra, stream); });
-  if (!rc) rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&rb, stream); });
+  /* op(B)'s passes on the handle's second stream, as in dgemm_crt */
+  void *aux = aux_fork(st, stream);
+  void *sb = aux ? aux : stream;
+  int rc = exps(ea, frac_a, inv_a, wa, wa_bytes, stream);
+  int rcb = exps(eb, frac_b, inv_b, wb, wb_bytes, sb);
+  if (!rc) rc = timed_launch(st, stream, "crt.zresidues", [&] { return hcbk_zcrt_residues(&ra, stream); });
+  if (!rcb) rcb = timed_launch(st, sb, "crt.zresidues", [&] { return hcbk_zcrt_residues(&rb, sb); });
+  if (aux) {
+    const int rcj = aux_join(st, stream);
+    if (!rcb) rcb = rcj;
+  }
+  if (!rc) rc = rcb;
   if (rc) return rc;
 
   const int pair = st->tc_pair == 2 ||

@@ -48,9 +48,10 @@ int dispatch_with_graph(HcblasB200State *st, const hcbk_gemm_args *a, void *stre
                         const char **path) {
   int dev = 0;
   cudaGetDevice(&dev);
-  const int knobs[9] = {st->math_mode, st->math_param,  st->split_promote_kb,
-                        st->tc_pair,   dev,             (int)st->workspace_epoch,
-                        st->crt_i8,    st->grouped_ctas, st->grouped_c_tma};
+  const int knobs[10] = {st->math_mode, st->math_param,  st->split_promote_kb,
+                         st->tc_pair,   dev,             (int)st->workspace_epoch,
+                         st->crt_i8,    st->grouped_ctas, st->grouped_c_tma,
+                         st->use_aux};
   std::vector<unsigned char> key(sizeof(*a) + sizeof(knobs) + sizeof(stream));
   std::memcpy(key.data(), a, sizeof(*a));
   std::memcpy(key.data() + sizeof(*a), knobs, sizeof(knobs));

@@ -169,6 +169,51 @@ void prof_record(void *ev, void *stream) {
   cudaEventRecord(static_cast<cudaEvent_t>(ev), static_cast<cudaStream_t>(stream));
 }
 
+void *aux_fork(HcblasB200State *st, void *stream) {
+  if (!st->use_aux) return nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (st->aux_stream && st->aux_device != dev) return nullptr; /* created for another device */
+  if (!st->aux_stream) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t f = nullptr, j = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      if (s) cudaStreamDestroy(s);
+      if (f) cudaEventDestroy(f);
+      return nullptr;
+    }
+    st->aux_stream = s;
+    st->aux_fork = f;
+    st->aux_join = j;
+    st->aux_device = dev;
+  }
+  if (cudaEventRecord(static_cast<cudaEvent_t>(st->aux_fork), static_cast<cudaStream_t>(stream)) !=
+          cudaSuccess ||
+      cudaStreamWaitEvent(static_cast<cudaStream_t>(st->aux_stream),
+                          static_cast<cudaEvent_t>(st->aux_fork), 0) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return st->aux_stream;
+}
+
+int aux_join(HcblasB200State *st, void *stream) {
+  if (cudaEventRecord(static_cast<cudaEvent_t>(st->aux_join),
+                      static_cast<cudaStream_t>(st->aux_stream)) != cudaSuccess ||
+      cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t>(st->aux_join),
+                          0) != cudaSuccess) {
+    cudaGetLastError();
+    return HCBK_ERR_LAUNCH;
+  }
+  return HCBK_OK;
+}
+
 bool log_enabled() {
   static int v = -1;
   if (v < 0) {
@@ -259,6 +304,13 @@ Hcblaslibrary::~Hcblaslibrary() {
       if (cudaStreamSynchronize(ws) != cudaSuccess) cudaGetLastError();
     }
     if (impl->workspace_event) cudaEventDestroy(static_cast<cudaEvent_t>(impl->workspace_event));
+    if (impl->aux_stream) {
+      DeviceGuard g(impl->aux_device);
+      cudaStreamSynchronize(static_cast<cudaStream_t>(impl->aux_stream));
+      cudaStreamDestroy(static_cast<cudaStream_t>(impl->aux_stream));
+      cudaEventDestroy(static_cast<cudaEvent_t>(impl->aux_fork));
+      cudaEventDestroy(static_cast<cudaEvent_t>(impl->aux_join));
+    }
     for (auto &r : impl->prof) {
       cudaEventDestroy(static_cast<cudaEvent_t>(r.ev0));
       cudaEventDestroy(static_cast<cudaEvent_t>(r.ev1));
@@ -495,6 +547,11 @@ extern "C" hcblasStatus_t hcblasSetTuningParam(hcblasHandle_t handle, const char
   if (std::strcmp(name, "grouped_c_tma") == 0) {
     if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
     handle->impl->grouped_c_tma = value;
+    return HCBLAS_STATUS_SUCCESS;
+  }
+  if (std::strcmp(name, "aux_stream") == 0) {
+    if (value != 0 && value != 1) return HCBLAS_STATUS_INVALID_VALUE;
+    handle->impl->use_aux = value;
     return HCBLAS_STATUS_SUCCESS;
   }
   if (std::strcmp(name, "dgemm_dmma") == 0) {

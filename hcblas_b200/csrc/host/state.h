@@ -87,6 +87,13 @@ struct HcblasB200State {
   int dev_err_device = -1;
   unsigned long long wait_limit_ns = 0; /* tuning knob "wait_timeout_us" (0 = 2 s) */
   int inject_timeout = 0; /* tuning knob "inject_timeout": arms the next HGEMM call */
+  /* a second stream of the handle's device for independent passes within one
+   * call (forked from and joined back into the call's stream by events);
+   * tuning knob "aux_stream" (1 = use it) */
+  int use_aux = 1;
+  void *aux_stream = nullptr;
+  int aux_device = -1;
+  void *aux_fork = nullptr, *aux_join = nullptr;
   /* per-kernel CUDA-event timing (hcblasSetProfiling) */
   bool profiling = false;
   std::vector<HcblasProfRec> prof;
@@ -110,6 +117,13 @@ void count_launch(int n = 1);
 long long launch_count();
 void *prof_event(HcblasB200State *st);
 void prof_record(void *ev, void *stream);
+
+/* Fork the handle's second stream off `stream` (it waits for everything
+ * queued on `stream` so far) and return it, or nullptr when the knob is off
+ * or the stream cannot be had (the caller then stays on `stream`). */
+void *aux_fork(HcblasB200State *st, void *stream);
+/* Make `stream` wait for everything queued on the second stream. */
+int aux_join(HcblasB200State *st, void *stream);
 
 /* Run `fn` (one library call, returning an HCBK_* code, that launches
  * `kernels` kernels); when profiling is on, bracket it with CUDA events on

@@ -504,6 +504,13 @@ hcblasStatus_t hcblasPlanEmulation(int mode, int param, int bits, int dtype, lon
  *                       through shared-memory boxes and TMA stores where C's
  *                       shape allows, 0 by direct stores from registers
  *                       (within 1 % of each other on 4096 uneven problems).
+ *   "aux_stream"        1 (default): independent passes of one call (the
+ *                       CRT DGEMM's and ZGEMM's row-scale and residue
+ *                       passes of op(B))
+ *                       run on a second stream of the handle, forked from
+ *                       and joined back into the call's stream with events
+ *                       (also inside a captured CUDA graph); 0 keeps every
+ *                       launch on the call's stream.  Results are identical.
  *   "dgemm_dmma"        native DGEMM and ZGEMM (HCBLAS_MATH_NATIVE): 1
  *                       (default) on the FP64 tensor path (warp-level
  *                       mma.sync .f64; ZGEMM as four real products), 0 on the

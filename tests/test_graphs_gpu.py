@@ -74,3 +74,37 @@ def test_workspace_growth_drops_graphs(stream_handle):
         _, ref = O.gemm(O.COL, 0, 1, M, N, K, 1.0, A, M, B, N, 0.0, np.zeros(M * N), M)
         assert O.normwise_rel_error(O.view_c(dC.download(), O.COL, M, N, M), ref) < 1e-14, shape
     assert hb.device_error(h) == 0
+
+
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_crt_second_stream_matches_one_stream(built_lib, graphs):
+    """The CRT DGEMM's op(B) passes on the handle's second stream (the
+    "aux_stream" knob, forked and joined by events, also inside a captured
+    graph) give the same words as every launch on the call's stream, on a
+    user stream and on the legacy default stream."""
+    rng = np.random.default_rng(19)
+    M, N, K = 520, 300, 700
+    A, B = rng.standard_normal(M * K), rng.standard_normal(N * K)
+    out = {}
+    for name, st in (("user", torch.cuda.Stream()), ("legacy", None)):
+        s, h = hb.hcblasCreate(0, st.cuda_stream if st is not None else None)
+        assert s == 0
+        try:
+            assert hb.set_tuning(h, "graphs", graphs if st is not None else 0) == 0
+            assert hb.hcblasSetMathMode(h, hb.HCBLAS_MATH_OZAKI_CRT, 14) == 0
+            dA, dB = hb.DeviceArray(h, A), hb.DeviceArray(h, B)
+            for aux in (1, 0, 1):
+                assert hb.set_tuning(h, "aux_stream", aux) == 0
+                dC = hb.DeviceArray(h, nbytes=8 * M * N, dtype=np.float64)
+                for _ in range(2):  # eager (+ capture), then replay when graphs are on
+                    assert dgemm(h, dA, dB, dC, M, N, K) == 0
+                torch.cuda.synchronize()
+                assert hb.device_error(h) == 0
+                out[(name, aux, len(out))] = dC.download()
+        finally:
+            hb.hcblasDestroy(h)
+    ref = next(iter(out.values()))
+    for k, v in out.items():
+        assert np.array_equal(v, ref), k
+    _, oracle = O.gemm(O.COL, 0, 1, M, N, K, 1.0, A, M, B, N, 0.0, np.zeros(M * N), M)
+    assert O.normwise_rel_error(O.view_c(ref, O.COL, M, N, M), oracle) < 1e-14
