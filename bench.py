@@ -805,16 +805,23 @@ def run_secondary(hb, L, h, stream, torch, O, n=8192, reps=3):
     cols = np.random.default_rng(6).choice(n, 4, replace=False)
 
     def timed(fn):
+        """Mean of back-to-back calls after a warm-up call: at least `reps`,
+        and as many as about 30 ms of calls (up to 50) for short ones."""
         fn()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(reps):
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        n_reps = int(min(50, max(reps, 30.0 / max(e0.elapsed_time(e1), 1e-3))))
+        e0.record(stream)
+        for _ in range(n_reps):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+        return e0.elapsed_time(e1) / n_reps
 
     # Ozaki-I INT8 slices at 5 / 6 / 7 on the headline workload (DGEMM
     # column-major NT 4096^3, N(0,1) seed 1), with native FP64 beside them

@@ -152,11 +152,10 @@ int sgemm_split(HcblasB200State *st, const hcbk_gemm_args *a, int terms, void *s
   char *bws = ws + nplanes * a_bytes;
   for (int i = 0; i < 3; ++i) pb.planes[i] = i < nplanes ? bws + i * b_bytes : nullptr;
 
+  /* both operands in one launch when both are K-contiguous */
   int rc = timed_launch(st, stream, "pack.split_bf16",
-                        [&] { return hcbk_pack_split_bf16(&pa, stream); });
-  if (rc) return rc;
-  rc = timed_launch(st, stream, "pack.split_bf16",
-                    [&] { return hcbk_pack_split_bf16(&pb, stream); });
+                        [&] { return hcbk_pack_split_bf16_pair(&pa, &pb, stream); },
+                        pa.k_contig && pb.k_contig ? 1 : 2);
   if (rc) return rc;
 
   hcbk_split_gemm g;

@@ -12,16 +12,19 @@
  * the FP64 pipe busy.
  *
  * Design: 128 x 128 CTA tiles, 256 threads = 8 warps as 2 (M) x 4 (N), each
- * warp a 64 x 32 block = 4 x 4 m16n8 accumulators (64 doubles per lane).
- * K advances in slabs of 16 through two shared-memory buffers laid out
- * [k][mn] (row pitch 132 doubles: the 16 lanes of a half-warp reading A or B
- * fragments hit 16 distinct bank pairs); the next slab is fetched into
- * registers with 16-byte loads while the current one is multiplied, whatever
- * the transposes (each operand is read along its contiguous dimension).
- * Out-of-range rows, columns and k are zero-filled, so any shape, leading
- * dimension, offset and alignment runs here; batches (strided or pointer
- * arrays) take blockIdx.y.  Epilogue: alpha * acc + beta * C in registers,
- * beta == 0 never reads C.
+ * warp a 64 x 32 block = 4 x 4 m16n8 accumulators (64 doubles per lane),
+ * multiplied with m16n8k16 DMMAs (one instruction per 16 K where m16n8k4
+ * needs four).  K advances in slabs of 32 through a 3-stage ring of
+ * shared-memory stages filled by cp.async (16-byte copies where the operand
+ * is 16-byte aligned with an even leading dimension, 8-byte copies
+ * otherwise; zero fill outside the matrix): an MN-contiguous operand is
+ * kept as [k][mn] (row pitch 132 doubles), a K-contiguous one as [mn][k]
+ * (row pitch 36), so that each is copied along its contiguous dimension
+ * and the 16 lanes of a half-warp reading a fragment hit 16 distinct bank
+ * pairs in either layout.  Any shape, leading dimension, offset and
+ * alignment runs here; batches (strided or pointer arrays) take
+ * blockIdx.y.  Epilogue: alpha * acc + beta * C in registers, beta == 0
+ * never reads C.
  *
  * Fragment layout of mma.sync.aligned.m16n8k4.row.col.f64 (PTX ISA, "matrix
  * fragments for mma.m16n8k4 .f64"): lane = 4 g + t; A (16 x 4, row):
@@ -37,9 +40,14 @@
 namespace hcbk {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16;
+constexpr int BM = 128, BN = 128, BK = 32;
 constexpr int NT = 256;
-constexpr int LDS = BM + 4; /* doubles per smem row (both operands) */
+constexpr int LDS = BM + 4; /* doubles per [k][mn] row: a half-warp's fragment loads hit 16 banks */
+constexpr int LDK = BK + 4; /* doubles per [mn][k] row: the same for the K-contiguous layout */
+/* doubles per operand and stage (the larger of the two layouts) */
+constexpr int OPD = BK * LDS > BM * LDK ? BK * LDS : BM * LDK;
+constexpr int DSTAGES = 3; /* cp.async ring depth */
+constexpr int DNT = 256;        /* DGEMM: 8 warps as 2 (M) x 4 (N) */
 constexpr int WM = 64, WN = 32; /* warp tile */
 constexpr int MT = WM / 16, NTL = WN / 8; /* m16 x n8 accumulators per warp */
 
@@ -68,24 +76,95 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+/* m16n8k16: a[2i] = A[g][t + 4i], a[2i + 1] = A[g + 8][t + 4i], b[i] = B[t + 4i][g]
+ * (the m16n8k4 fragments of the four K quarters side by side; checked lane
+ * by lane against a CPU product on B200) */
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, "
+      "{%4, %5, %6, %7, %8, %9, %10, %11}, {%12, %13, %14, %15}, {%0, %1, %2, %3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 struct alignas(16) D2 {
   double v[2];
 };
 
+/* shared-memory address of a generic pointer */
+__device__ __forceinline__ uint32_t sptr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+/* asynchronous global -> shared copies; `bytes` of the source are read and
+ * the rest of the destination is zero-filled (bytes = 0: nothing is read) */
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sptr(dst)), "l"(src),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sptr(dst)), "l"(src),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+/* one operand's K slab of a stage: an MN-contiguous operand as [k][mn]
+ * (pitch LDS), a K-contiguous one as [mn][k] (pitch LDK); either is copied
+ * along its contiguous dimension, two doubles per copy (16-byte copies when
+ * the operand allows, else two 8-byte ones), zero outside the matrix */
+template <bool MN>
+__device__ __forceinline__ void load_slab(double *dst, const double *X, int64_t ld, int64_t rows,
+                                          int64_t K, int64_t r0, int64_t k0, bool vec, int tid) {
+#pragma unroll
+  for (int v = 0; v < (BM * BK) / (2 * DNT); ++v) {
+    const int idx = tid + v * DNT;
+    int64_t grow, gk;
+    int off, nvalid;
+    const double *src;
+    if (MN) { /* 16 k rows of 64 pairs */
+      const int mn = (idx % (BM / 2)) * 2, kk = idx / (BM / 2);
+      grow = r0 + mn;
+      gk = k0 + kk;
+      src = X + grow + gk * ld;
+      off = kk * LDS + mn;
+      const int64_t left = rows - grow;
+      nvalid = gk < K ? (left >= 2 ? 2 : left > 0 ? (int)left : 0) : 0;
+    } else { /* 128 rows of 8 pairs */
+      const int mn = idx / (BK / 2), kk = (idx % (BK / 2)) * 2;
+      grow = r0 + mn;
+      gk = k0 + kk;
+      src = X + gk + grow * ld;
+      off = mn * LDK + kk;
+      const int64_t left = K - gk;
+      nvalid = grow < rows ? (left >= 2 ? 2 : left > 0 ? (int)left : 0) : 0;
+    }
+    if (vec) {
+      cp_async16(dst + off, nvalid ? src : X, nvalid * 8);
+    } else {
+      cp_async8(dst + off, nvalid >= 1 ? src : X, nvalid >= 1 ? 8 : 0);
+      cp_async8(dst + off + 1, nvalid >= 2 ? src + 1 : X, nvalid >= 2 ? 8 : 0);
+    }
+  }
+}
+
 /*
  * OP_A / OP_B: 0 = N, 1 = T (column-major canonical; FP64 has no conjugate).
  *   op(A) MN-contiguous iff OP_A == N;  op(B) K-contiguous iff OP_B == N.
+ * K slabs of 16 go through a DSTAGES-deep ring of shared-memory stages
+ * filled by cp.async: while one slab is multiplied, the next DSTAGES - 1
+ * are in flight, and one barrier per slab both publishes the landed slab
+ * and frees the stage that the next copies overwrite.
  */
 template <int OP_A, int OP_B>
-__global__ void __launch_bounds__(NT, 1) dmma_gemm_kernel(const DmmaParams p) {
+__global__ void __launch_bounds__(DNT, 1) dmma_gemm_kernel(const DmmaParams p) {
   constexpr bool A_MN = (OP_A == HCBK_OP_N);
   constexpr bool B_MN = (OP_B != HCBK_OP_N);
-  /* 16-byte vectors (2 doubles) per thread and slab: 128 x 16 / 2 / 256 = 4 */
-  constexpr int VA = (BM * BK) / (2 * NT);
-  constexpr int VB = (BN * BK) / (2 * NT);
   extern __shared__ __align__(16) double dmma_smem[];
-  auto As = reinterpret_cast<double (*)[BK][LDS]>(dmma_smem);              /* [2][BK][LDS] */
-  auto Bs = reinterpret_cast<double (*)[BK][LDS]>(dmma_smem + 2 * BK * LDS); /* [2][BK][LDS] */
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -112,81 +191,12 @@ __global__ void __launch_bounds__(NT, 1) dmma_gemm_kernel(const DmmaParams p) {
     double *C = (p.c_arr ? p.c_arr[bidx] : p.c) + p.c_off + bidx * p.sc;
     const bool vec_a = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((p.lda & 1) == 0);
     const bool vec_b = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && ((p.ldb & 1) == 0);
+    const int64_t ktiles = (p.k + BK - 1) / BK;
 
-    D2 ra[VA], rb[VB];
-    auto fetch = [&](int64_t k0) {
-#pragma unroll
-      for (int v = 0; v < VA; ++v) {
-        const int idx = tid + v * NT;
-        if (A_MN) { /* 64 vectors along m per k row */
-          const int64_t mn = m0 + (int64_t)(idx % (BM / 2)) * 2, kk = k0 + idx / (BM / 2);
-          const double *src = A + mn + kk * p.lda;
-          if (kk < p.k && mn + 2 <= p.m && vec_a) {
-            ra[v] = *reinterpret_cast<const D2 *>(src);
-          } else {
-            ra[v].v[0] = (kk < p.k && mn < p.m) ? src[0] : 0.0;
-            ra[v].v[1] = (kk < p.k && mn + 1 < p.m) ? src[1] : 0.0;
-          }
-        } else { /* 8 vectors along k per m row */
-          const int64_t mn = m0 + idx / (BK / 2), kk = k0 + (int64_t)(idx % (BK / 2)) * 2;
-          const double *src = A + kk + mn * p.lda;
-          if (mn < p.m && kk + 2 <= p.k && vec_a) {
-            ra[v] = *reinterpret_cast<const D2 *>(src);
-          } else {
-            ra[v].v[0] = (mn < p.m && kk < p.k) ? src[0] : 0.0;
-            ra[v].v[1] = (mn < p.m && kk + 1 < p.k) ? src[1] : 0.0;
-          }
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < VB; ++v) {
-        const int idx = tid + v * NT;
-        if (B_MN) {
-          const int64_t mn = n0 + (int64_t)(idx % (BN / 2)) * 2, kk = k0 + idx / (BN / 2);
-          const double *src = B + mn + kk * p.ldb;
-          if (kk < p.k && mn + 2 <= p.n && vec_b) {
-            rb[v] = *reinterpret_cast<const D2 *>(src);
-          } else {
-            rb[v].v[0] = (kk < p.k && mn < p.n) ? src[0] : 0.0;
-            rb[v].v[1] = (kk < p.k && mn + 1 < p.n) ? src[1] : 0.0;
-          }
-        } else {
-          const int64_t mn = n0 + idx / (BK / 2), kk = k0 + (int64_t)(idx % (BK / 2)) * 2;
-          const double *src = B + kk + mn * p.ldb;
-          if (mn < p.n && kk + 2 <= p.k && vec_b) {
-            rb[v] = *reinterpret_cast<const D2 *>(src);
-          } else {
-            rb[v].v[0] = (mn < p.n && kk < p.k) ? src[0] : 0.0;
-            rb[v].v[1] = (mn < p.n && kk + 1 < p.k) ? src[1] : 0.0;
-          }
-        }
-      }
-    };
-    auto stash = [&](int s) {
-#pragma unroll
-      for (int v = 0; v < VA; ++v) {
-        const int idx = tid + v * NT;
-        if (A_MN) {
-          const int mn = (idx % (BM / 2)) * 2, kk = idx / (BM / 2);
-          *reinterpret_cast<D2 *>(&As[s][kk][mn]) = ra[v];
-        } else {
-          const int mn = idx / (BK / 2), kk = (idx % (BK / 2)) * 2;
-          As[s][kk][mn] = ra[v].v[0];
-          As[s][kk + 1][mn] = ra[v].v[1];
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < VB; ++v) {
-        const int idx = tid + v * NT;
-        if (B_MN) {
-          const int mn = (idx % (BN / 2)) * 2, kk = idx / (BN / 2);
-          *reinterpret_cast<D2 *>(&Bs[s][kk][mn]) = rb[v];
-        } else {
-          const int mn = idx / (BK / 2), kk = (idx % (BK / 2)) * 2;
-          Bs[s][kk][mn] = rb[v].v[0];
-          Bs[s][kk + 1][mn] = rb[v].v[1];
-        }
-      }
+    auto load_stage = [&](int slot, int64_t kt) {
+      double *sa = dmma_smem + slot * 2 * OPD, *sb = sa + OPD;
+      load_slab<A_MN>(sa, A, p.lda, p.m, p.k, m0, kt * BK, vec_a, tid);
+      load_slab<B_MN>(sb, B, p.ldb, p.n, p.k, n0, kt * BK, vec_b, tid);
     };
 
     double acc[MT][NTL][4];
@@ -197,31 +207,45 @@ __global__ void __launch_bounds__(NT, 1) dmma_gemm_kernel(const DmmaParams p) {
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-    const int64_t ktiles = (p.k + BK - 1) / BK;
-    fetch(0);
-    stash(0);
-    __syncthreads();
-    for (int64_t kt = 0; kt < ktiles; ++kt) {
-      const int s = (int)(kt & 1);
-      if (kt + 1 < ktiles) fetch((kt + 1) * BK);
 #pragma unroll
-      for (int k4 = 0; k4 < BK; k4 += 4) {
-        double af[MT][2], bf[NTL];
+    for (int s = 0; s < DSTAGES - 1; ++s) {
+      if (s < ktiles) load_stage(s, s);
+      cp_async_commit();
+    }
+    for (int64_t kt = 0; kt < ktiles; ++kt) {
+      cp_async_wait<DSTAGES - 2>(); /* this thread's copies of slab kt have landed */
+      __syncthreads();              /* everyone's; and slab kt - 1 is no longer read */
+      if (kt + DSTAGES - 1 < ktiles) load_stage((int)((kt + DSTAGES - 1) % DSTAGES), kt + DSTAGES - 1);
+      cp_async_commit();
+      const double *As = dmma_smem + (int)(kt % DSTAGES) * 2 * OPD, *Bs = As + OPD;
+#pragma unroll
+      for (int k16 = 0; k16 < BK; k16 += 16) {
+        double af[MT][8];
 #pragma unroll
         for (int i = 0; i < MT; ++i) {
-          af[i][0] = As[s][k4 + t][wm + 16 * i + g];
-          af[i][1] = As[s][k4 + t][wm + 16 * i + g + 8];
+          const int r = wm + 16 * i + g;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int kk = k16 + t + 4 * q;
+            af[i][2 * q] = A_MN ? As[kk * LDS + r] : As[r * LDK + kk];
+            af[i][2 * q + 1] = A_MN ? As[kk * LDS + r + 8] : As[(r + 8) * LDK + kk];
+          }
         }
 #pragma unroll
-        for (int j = 0; j < NTL; ++j) bf[j] = Bs[s][k4 + t][wn + 8 * j + g];
+        for (int j = 0; j < NTL; ++j) {
+          const int c = wn + 8 * j + g;
+          double bf[4];
 #pragma unroll
-        for (int i = 0; i < MT; ++i)
+          for (int q = 0; q < 4; ++q) {
+            const int kk = k16 + t + 4 * q;
+            bf[q] = B_MN ? Bs[kk * LDS + c] : Bs[c * LDK + kk];
+          }
 #pragma unroll
-          for (int j = 0; j < NTL; ++j) dmma(acc[i][j], af[i][0], af[i][1], bf[j]);
+          for (int i = 0; i < MT; ++i) dmma16(acc[i][j], af[i], bf);
+        }
       }
-      if (kt + 1 < ktiles) stash(s ^ 1);
-      __syncthreads();
     }
+    cp_async_wait<0>(); /* only empty groups remain */
 
     /* epilogue: c0, c1 at (g, 2t), (g, 2t + 1); c2, c3 at row g + 8 */
     const bool rd = p.beta_nonzero != 0;
@@ -241,7 +265,7 @@ __global__ void __launch_bounds__(NT, 1) dmma_gemm_kernel(const DmmaParams p) {
         }
       }
     }
-    if (p.batch > 1) __syncthreads(); /* the shared buffers are reused by the next entry */
+    if (p.batch > 1) __syncthreads(); /* the stages are reused by the next entry */
   }
 }
 
@@ -457,7 +481,7 @@ extern "C" int hcbk_dgemm_dmma(const hcbk_gemm_args *a, void *stream) {
   if (tiles > 0x7fffffffLL) return HCBK_ERR_ARGS;
   dim3 grid((unsigned)tiles, (unsigned)(a->batch < 65535 ? a->batch : 65535), 1);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  constexpr int smem = 4 * BK * LDS * (int)sizeof(double); /* two buffers of A and of B */
+  constexpr int smem = DSTAGES * 2 * OPD * (int)sizeof(double); /* the ring of A and B slabs */
   static bool attr_set[64] = {false};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HCBK_ERR_LAUNCH;
@@ -473,7 +497,7 @@ extern "C" int hcbk_dgemm_dmma(const hcbk_gemm_args *a, void *stream) {
         return HCBK_ERR_LAUNCH;
     attr_set[dev] = true;
   }
-  kern<<<grid, NT, smem, st>>>(p);
+  kern<<<grid, DNT, smem, st>>>(p);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 

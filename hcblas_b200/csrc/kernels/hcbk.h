@@ -147,6 +147,9 @@ typedef struct hcbk_pack_args {
   int64_t ld_dst;
 } hcbk_pack_args;
 int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream);
+/* both operands of a split-BF16 GEMM: one launch when both are K-contiguous,
+ * else one per operand */
+int hcbk_pack_split_bf16_pair(const hcbk_pack_args *a, const hcbk_pack_args *b, void *stream);
 
 /* CGEMM 3M on the split-BF16 path: split one complex f32 operand (float2
  * storage, `ld` in complex elements; element (r, k) at src[k + r*ld] if

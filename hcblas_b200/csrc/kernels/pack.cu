@@ -20,43 +20,61 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include "hcbk.h"
 #include "split_bf16.cuh"
 
 namespace {
 
-/* source K-contiguous: element (r, k) at src[k + r*ld]; 4 k per thread */
-__global__ void pack_kcontig(hcbk_pack_args a) {
-  const int64_t kq = (a.kdim + 3) / 4;
-  const int64_t total = a.rows * kq;
-  const bool vec = ((reinterpret_cast<uintptr_t>(a.src) & 15) == 0) && ((a.ld & 3) == 0);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+/* K-contiguous sources of one or two operands in one launch: element
+ * (r, k) of operand j at a[j].src[k + r*ld]; each thread splits 8
+ * consecutive k of one row (two 16-byte loads where the source allows) and
+ * writes 16 bytes to every plane where the planes' row pitch is a multiple of
+ * 8 elements (the row's padding past K then receives zeros). */
+struct PackPair {
+  hcbk_pack_args a[2];
+  int64_t kq[2];    /* 8-element groups per row */
+  int64_t units0;   /* rows * kq of operand 0 */
+  int64_t total;    /* all groups */
+  int vec_src[2], vec_dst[2];
+};
+
+__global__ void pack_kcontig(const __grid_constant__ PackPair pp) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pp.total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = i / kq;
-    const int64_t k0 = (i % kq) * 4;
+    const int which = i >= pp.units0 ? 1 : 0;
+    const hcbk_pack_args &a = pp.a[which];
+    const int64_t idx = i - (which ? pp.units0 : 0);
+    const int64_t kq = pp.kq[which];
+    const int64_t r = idx / kq;
+    const int64_t k0 = (idx - r * kq) * 8;
     const float *s = a.src + r * a.ld + k0;
-    float v[4];
-    if (vec && k0 + 4 <= a.kdim) {
-      const float4 f = *reinterpret_cast<const float4 *>(s);
-      v[0] = f.x;
-      v[1] = f.y;
-      v[2] = f.z;
-      v[3] = f.w;
+    float v[8];
+    if (pp.vec_src[which] && k0 + 8 <= a.kdim) {
+      const float4 f0 = *reinterpret_cast<const float4 *>(s);
+      const float4 f1 = *reinterpret_cast<const float4 *>(s + 4);
+      v[0] = f0.x; v[1] = f0.y; v[2] = f0.z; v[3] = f0.w;
+      v[4] = f1.x; v[5] = f1.y; v[6] = f1.z; v[7] = f1.w;
     } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) v[e] = (k0 + e < a.kdim) ? s[e] : 0.f;
+      for (int e = 0; e < 8; ++e) v[e] = (k0 + e < a.kdim) ? s[e] : 0.f;
     }
-    __nv_bfloat16 t[4][3];
+    uint32_t w[4][3];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) split_terms(v[e], t[e]);
-    #pragma unroll
-      for (int p = 0; p < 3; ++p) {
-        if (p >= a.nplanes) break;
+    for (int j = 0; j < 4; ++j) split_terms2(v[2 * j], v[2 * j + 1], w[j]);
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      if (p >= a.nplanes) break;
       __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(a.planes[p]) + r * a.ld_dst + k0;
+      if (pp.vec_dst[which]) {
+        *reinterpret_cast<uint4 *>(d) = make_uint4(w[0][p], w[1][p], w[2][p], w[3][p]);
+      } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (k0 + e < a.kdim) d[e] = t[e][p];
+        for (int e = 0; e < 8; ++e)
+          if (k0 + e < a.kdim)
+            d[e] = __ushort_as_bfloat16(static_cast<unsigned short>(w[e >> 1][p] >> (16 * (e & 1))));
+      }
     }
   }
 }
@@ -214,19 +232,59 @@ extern "C" int hcbk_c3m_combine(const hcbk_c3m_combine_args *a, void *stream) {
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }
 
-extern "C" int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream) {
-  if (a->rows <= 0 || a->kdim <= 0 || a->nplanes < 1 || a->nplanes > 3) return HCBK_ERR_ARGS;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (a->k_contig) {
-    const int64_t total = a->rows * ((a->kdim + 3) / 4);
-    int64_t blocks = (total + 255) / 256;
-    const int64_t cap = (int64_t)hcbk_sm_count() * 16;
-    if (blocks > cap) blocks = cap;
-    pack_kcontig<<<(unsigned)blocks, 256, 0, st>>>(*a);
-  } else {
-    const int64_t gx = (a->rows + 31) / 32, gy = (a->kdim + 31) / 32;
-    if (gy > 65535) return HCBK_ERR_ARGS;
-    pack_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(*a);
+namespace {
+bool pack_ok(const hcbk_pack_args *a) {
+  return a->rows > 0 && a->kdim > 0 && a->nplanes >= 1 && a->nplanes <= 3 && a->ld_dst >= a->kdim;
+}
+
+/* one launch over the K-contiguous operands among a[0 .. n-1] */
+int launch_kcontig(const hcbk_pack_args *const *a, int n, cudaStream_t st) {
+  PackPair pp;
+  memset(&pp, 0, sizeof(pp));
+  int64_t total = 0;
+  for (int j = 0; j < n; ++j) {
+    pp.a[j] = *a[j];
+    pp.kq[j] = (a[j]->kdim + 7) / 8;
+    pp.vec_src[j] = (reinterpret_cast<uintptr_t>(a[j]->src) & 15) == 0 && (a[j]->ld & 3) == 0;
+    int vd = (a[j]->ld_dst & 7) == 0;
+    for (int p = 0; p < a[j]->nplanes; ++p)
+      vd = vd && (reinterpret_cast<uintptr_t>(a[j]->planes[p]) & 15) == 0;
+    pp.vec_dst[j] = vd;
+    if (j == 0) pp.units0 = a[j]->rows * pp.kq[j];
+    total += a[j]->rows * pp.kq[j];
   }
+  pp.total = total;
+  int64_t blocks = (total + 255) / 256;
+  const int64_t cap = (int64_t)hcbk_sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  pack_kcontig<<<(unsigned)blocks, 256, 0, st>>>(pp);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+
+int launch_rcontig(const hcbk_pack_args *a, cudaStream_t st) {
+  const int64_t gx = (a->rows + 31) / 32, gy = (a->kdim + 31) / 32;
+  if (gy > 65535) return HCBK_ERR_ARGS;
+  pack_rcontig<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(*a);
+  return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
+}
+}  // namespace
+
+extern "C" int hcbk_pack_split_bf16(const hcbk_pack_args *a, void *stream) {
+  if (!pack_ok(a)) return HCBK_ERR_ARGS;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (a->k_contig) return launch_kcontig(&a, 1, st);
+  return launch_rcontig(a, st);
+}
+
+extern "C" int hcbk_pack_split_bf16_pair(const hcbk_pack_args *a, const hcbk_pack_args *b,
+                                         void *stream) {
+  if (!pack_ok(a) || !pack_ok(b)) return HCBK_ERR_ARGS;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (a->k_contig && b->k_contig) {
+    const hcbk_pack_args *both[2] = {a, b};
+    return launch_kcontig(both, 2, st);
+  }
+  int rc = a->k_contig ? launch_kcontig(&a, 1, st) : launch_rcontig(a, st);
+  if (rc) return rc;
+  return b->k_contig ? launch_kcontig(&b, 1, st) : launch_rcontig(b, st);
 }
