@@ -761,22 +761,26 @@ __global__ void __launch_bounds__(256) grouped_pack_kernel(const hcbk_gpack_job 
       nk0 = (lt / nj.tiles_r) * 64;
       pack_load(nj, nr0, nk0, v);
     }
-    /* this thread's k pair; the row's padding up to ld_dst (a multiple of
-     * 16: rows start on 32-byte sectors) is written too, as zeros, so that
-     * every sector is written whole and L2 never fetches one to merge */
-    const int k = k0 + 2 * tx;
+    /* this thread's row and 8 consecutive k: one 16-byte store per plane
+     * (ld_dst is a multiple of 16 and every plane 1 KiB aligned); the row's
+     * padding up to ld_dst is written too, as zeros, so that every sector is
+     * written whole and L2 never fetches one to merge */
+    {
+      const int u = ty * 32 + tx;
+      const int rl = u >> 3, kq = (u & 7) * 8;
+      const int r = r0 + rl, k = k0 + kq;
+      if (r < j.rows && k < j.ld_dst) {
+        uint32_t w[4][3];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int rl = ty + 8 * i, r = r0 + rl;
-      if (r >= j.rows || k >= j.ld_dst) continue;
-      __nv_bfloat16 a[3], b[3];
-      split_terms(tile[2 * tx][rl], a);
-      split_terms(tile[2 * tx + 1][rl], b);
-      __nv_bfloat16 *d = j.planes + (int64_t)r * j.ld_dst + k;
+        for (int e = 0; e < 4; ++e)
+          split_terms2(tile[kq + 2 * e][rl], tile[kq + 2 * e + 1][rl], w[e]);
+        __nv_bfloat16 *d = j.planes + (int64_t)r * j.ld_dst + k;
 #pragma unroll
-      for (int pl = 0; pl < 3; ++pl) {
-        if (pl >= nplanes) break;
-        *reinterpret_cast<__nv_bfloat162 *>(d + pl * j.pstride) = __halves2bfloat162(a[pl], b[pl]);
+        for (int pl = 0; pl < 3; ++pl) {
+          if (pl >= nplanes) break;
+          *reinterpret_cast<uint4 *>(d + pl * j.pstride) =
+              make_uint4(w[0][pl], w[1][pl], w[2][pl], w[3][pl]);
+        }
       }
     }
   }
