@@ -68,14 +68,6 @@ struct DmmaParams {
   int beta_nonzero;
 };
 
-__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
-      "{%0, %1, %2, %3};"
-      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-      : "d"(a0), "d"(a1), "d"(b0));
-}
-
 /* m16n8k16: a[2i] = A[g][t + 4i], a[2i + 1] = A[g + 8][t + 4i], b[i] = B[t + 4i][g]
  * (the m16n8k4 fragments of the four K quarters side by side; checked lane
  * by lane against a CPU product on B200) */
@@ -272,14 +264,22 @@ __global__ void __launch_bounds__(DNT, 1) dmma_gemm_kernel(const DmmaParams p) {
 /*
  * Native ZGEMM on the same FP64 tensor path: the complex product is four
  * real products per fragment set, Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br
- * (the 4M form, exact in the order of its FMAs as the CUDA-core kernel's),
- * with the operands split into real and imaginary shared-memory planes when
- * a slab is stored (conjugation applied there).  128 x 64 CTA tiles, 8 warps
- * as 4 (M) x 2 (N), warp tiles 32 x 32 = 2 x 4 m16n8 accumulator pairs;
- * K slabs of 8 complex elements, one 16-byte load per element.
+ * (the 4M form), on m16n8k16 DMMAs.  128 x 64 CTA tiles, 8 warps as 4 (M) x
+ * 2 (N), warp tiles 32 x 32 = 2 x 4 m16n8 accumulator pairs.  K advances in
+ * slabs of 16 complex elements through a 3-stage ring filled by cp.async,
+ * one 16-byte copy per element (two 8-byte ones for an operand that is only
+ * 8-byte aligned), complex values kept interleaved: an MN-contiguous operand
+ * as [k][mn] (pitch ZBM + 2 or ZBN + 2 elements), a K-contiguous one as
+ * [mn][k] (pitch 20), so that each quarter-warp's 16-byte fragment loads --
+ * real and imaginary part together -- hit 8 distinct bank groups.
+ * Conjugation is applied to the fragments.
  */
-constexpr int ZBM = 128, ZBN = 64, ZBK = 8;
-constexpr int ZLDA = ZBM + 4, ZLDB = ZBN + 4;
+constexpr int ZBM = 128, ZBN = 64, ZBK = 16;
+constexpr int ZSTAGES = 3;
+constexpr int ZLDA = ZBM + 2, ZLDB = ZBN + 2; /* [k][mn] pitches (complex elements) */
+constexpr int ZLDK = ZBK + 4;                 /* [mn][k] pitch */
+constexpr int ZOPA = ZBK * ZLDA > ZBM * ZLDK ? ZBK * ZLDA : ZBM * ZLDK; /* per stage */
+constexpr int ZOPB = ZBK * ZLDB > ZBN * ZLDK ? ZBK * ZLDB : ZBN * ZLDK;
 constexpr int ZWM = 32, ZWN = 32, ZMT = ZWM / 16, ZNT = ZWN / 8;
 
 struct ZmmaParams {
@@ -299,18 +299,47 @@ struct ZmmaParams {
   int beta_nonzero;
 };
 
+/* one operand's slab of complex elements into a stage (see load_slab) */
+template <bool MN, int ROWS>
+__device__ __forceinline__ void zload_slab(double2 *dst, const double2 *X, int64_t ld,
+                                           int64_t rows, int64_t K, int64_t r0, int64_t k0,
+                                           bool vec, int tid) {
+  constexpr int PITCH_MN = ROWS + 2;
+#pragma unroll
+  for (int v = 0; v < (ROWS * ZBK) / NT; ++v) {
+    const int idx = tid + v * NT;
+    int mn, kk, off;
+    if (MN) {
+      mn = idx % ROWS;
+      kk = idx / ROWS;
+      off = kk * PITCH_MN + mn;
+    } else {
+      mn = idx / ZBK;
+      kk = idx % ZBK;
+      off = mn * ZLDK + kk;
+    }
+    const int64_t grow = r0 + mn, gk = k0 + kk;
+    const bool ok = grow < rows && gk < K;
+    const double2 *src = ok ? (MN ? X + grow + gk * ld : X + gk + grow * ld) : X;
+    if (vec) {
+      cp_async16(dst + off, src, ok ? 16 : 0);
+    } else {
+      const double *s = reinterpret_cast<const double *>(src);
+      double *d = reinterpret_cast<double *>(dst + off);
+      cp_async8(d, s, ok ? 8 : 0);
+      cp_async8(d + 1, ok ? s + 1 : s, ok ? 8 : 0);
+    }
+  }
+}
+
 template <int OP_A, int OP_B>
 __global__ void __launch_bounds__(NT, 1) zmma_gemm_kernel(const ZmmaParams p) {
   constexpr bool A_MN = (OP_A == HCBK_OP_N);
   constexpr bool B_MN = (OP_B != HCBK_OP_N);
   constexpr bool CJ_A = (OP_A == HCBK_OP_C);
   constexpr bool CJ_B = (OP_B == HCBK_OP_C);
-  constexpr int VA = (ZBM * ZBK) / NT; /* complex elements per thread and slab: 4 */
-  constexpr int VB = (ZBN * ZBK) / NT; /* 2 */
   extern __shared__ __align__(16) double zmma_smem[];
-  /* [2 buffers][re, im][ZBK][ld] */
-  auto As = reinterpret_cast<double (*)[2][ZBK][ZLDA]>(zmma_smem);
-  auto Bs = reinterpret_cast<double (*)[2][ZBK][ZLDB]>(zmma_smem + 2 * 2 * ZBK * ZLDA);
+  double2 *zs = reinterpret_cast<double2 *>(zmma_smem);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -334,41 +363,14 @@ __global__ void __launch_bounds__(NT, 1) zmma_gemm_kernel(const ZmmaParams p) {
     const double2 *A = (p.a_arr ? p.a_arr[bidx] : p.a) + p.a_off + bidx * p.sa;
     const double2 *B = (p.b_arr ? p.b_arr[bidx] : p.b) + p.b_off + bidx * p.sb;
     double2 *C = (p.c_arr ? p.c_arr[bidx] : p.c) + p.c_off + bidx * p.sc;
+    const bool vec_a = (reinterpret_cast<uintptr_t>(A) & 15) == 0;
+    const bool vec_b = (reinterpret_cast<uintptr_t>(B) & 15) == 0;
+    const int64_t ktiles = (p.k + ZBK - 1) / ZBK;
 
-    double2 ra[VA], rb[VB];
-    auto fetch = [&](int64_t k0) {
-#pragma unroll
-      for (int v = 0; v < VA; ++v) {
-        const int idx = tid + v * NT;
-        const int64_t mn = m0 + (A_MN ? idx % ZBM : idx / ZBK);
-        const int64_t kk = k0 + (A_MN ? idx / ZBM : idx % ZBK);
-        ra[v] = (mn < p.m && kk < p.k) ? (A_MN ? A[mn + kk * p.lda] : A[kk + mn * p.lda])
-                                       : make_double2(0.0, 0.0);
-      }
-#pragma unroll
-      for (int v = 0; v < VB; ++v) {
-        const int idx = tid + v * NT;
-        const int64_t mn = n0 + (B_MN ? idx % ZBN : idx / ZBK);
-        const int64_t kk = k0 + (B_MN ? idx / ZBN : idx % ZBK);
-        rb[v] = (mn < p.n && kk < p.k) ? (B_MN ? B[mn + kk * p.ldb] : B[kk + mn * p.ldb])
-                                       : make_double2(0.0, 0.0);
-      }
-    };
-    auto stash = [&](int s) {
-#pragma unroll
-      for (int v = 0; v < VA; ++v) {
-        const int idx = tid + v * NT;
-        const int mn = A_MN ? idx % ZBM : idx / ZBK, kk = A_MN ? idx / ZBM : idx % ZBK;
-        As[s][0][kk][mn] = ra[v].x;
-        As[s][1][kk][mn] = CJ_A ? -ra[v].y : ra[v].y;
-      }
-#pragma unroll
-      for (int v = 0; v < VB; ++v) {
-        const int idx = tid + v * NT;
-        const int mn = B_MN ? idx % ZBN : idx / ZBK, kk = B_MN ? idx / ZBN : idx % ZBK;
-        Bs[s][0][kk][mn] = rb[v].x;
-        Bs[s][1][kk][mn] = CJ_B ? -rb[v].y : rb[v].y;
-      }
+    auto load_stage = [&](int slot, int64_t kt) {
+      double2 *sa = zs + slot * (ZOPA + ZOPB), *sb = sa + ZOPA;
+      zload_slab<A_MN, ZBM>(sa, A, p.lda, p.m, p.k, m0, kt * ZBK, vec_a, tid);
+      zload_slab<B_MN, ZBN>(sb, B, p.ldb, p.n, p.k, n0, kt * ZBK, vec_b, tid);
     };
 
     double cr[ZMT][ZNT][4], ci[ZMT][ZNT][4];
@@ -379,41 +381,55 @@ __global__ void __launch_bounds__(NT, 1) zmma_gemm_kernel(const ZmmaParams p) {
 #pragma unroll
         for (int e = 0; e < 4; ++e) cr[i][j][e] = ci[i][j][e] = 0.0;
 
-    const int64_t ktiles = (p.k + ZBK - 1) / ZBK;
-    fetch(0);
-    stash(0);
-    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < ZSTAGES - 1; ++s) {
+      if (s < ktiles) load_stage(s, s);
+      cp_async_commit();
+    }
     for (int64_t kt = 0; kt < ktiles; ++kt) {
-      const int s = (int)(kt & 1);
-      if (kt + 1 < ktiles) fetch((kt + 1) * ZBK);
+      cp_async_wait<ZSTAGES - 2>();
+      __syncthreads();
+      if (kt + ZSTAGES - 1 < ktiles)
+        load_stage((int)((kt + ZSTAGES - 1) % ZSTAGES), kt + ZSTAGES - 1);
+      cp_async_commit();
+      const double2 *As = zs + (int)(kt % ZSTAGES) * (ZOPA + ZOPB), *Bs = As + ZOPA;
 #pragma unroll
-      for (int k4 = 0; k4 < ZBK; k4 += 4) {
-        double ar[ZMT][2], ai[ZMT][2], br[ZNT], bi[ZNT];
+      for (int i = 0; i < ZMT; ++i) {
+        const int r = wm + 16 * i + g;
+        /* real parts, and the imaginary parts both ways round: ai for the
+         * imaginary accumulator, -ai for the real one */
+        double ar[8], ai[8], nai[8];
 #pragma unroll
-        for (int i = 0; i < ZMT; ++i) {
-          ar[i][0] = As[s][0][k4 + t][wm + 16 * i + g];
-          ar[i][1] = As[s][0][k4 + t][wm + 16 * i + g + 8];
-          ai[i][0] = As[s][1][k4 + t][wm + 16 * i + g];
-          ai[i][1] = As[s][1][k4 + t][wm + 16 * i + g + 8];
+        for (int q = 0; q < 4; ++q) {
+          const int kk = t + 4 * q;
+          const double2 x0 = A_MN ? As[kk * ZLDA + r] : As[r * ZLDK + kk];
+          const double2 x1 = A_MN ? As[kk * ZLDA + r + 8] : As[(r + 8) * ZLDK + kk];
+          ar[2 * q] = x0.x;
+          ar[2 * q + 1] = x1.x;
+          ai[2 * q] = CJ_A ? -x0.y : x0.y;
+          ai[2 * q + 1] = CJ_A ? -x1.y : x1.y;
+          nai[2 * q] = -ai[2 * q];
+          nai[2 * q + 1] = -ai[2 * q + 1];
         }
 #pragma unroll
         for (int j = 0; j < ZNT; ++j) {
-          br[j] = Bs[s][0][k4 + t][wn + 8 * j + g];
-          bi[j] = Bs[s][1][k4 + t][wn + 8 * j + g];
-        }
+          const int c = wn + 8 * j + g;
+          double br[4], bi[4];
 #pragma unroll
-        for (int i = 0; i < ZMT; ++i)
-#pragma unroll
-          for (int j = 0; j < ZNT; ++j) {
-            dmma(cr[i][j], ar[i][0], ar[i][1], br[j]);
-            dmma(cr[i][j], -ai[i][0], -ai[i][1], bi[j]);
-            dmma(ci[i][j], ar[i][0], ar[i][1], bi[j]);
-            dmma(ci[i][j], ai[i][0], ai[i][1], br[j]);
+          for (int q = 0; q < 4; ++q) {
+            const int kk = t + 4 * q;
+            const double2 y = B_MN ? Bs[kk * ZLDB + c] : Bs[c * ZLDK + kk];
+            br[q] = y.x;
+            bi[q] = CJ_B ? -y.y : y.y;
           }
+          dmma16(cr[i][j], ar, br);
+          dmma16(cr[i][j], nai, bi);
+          dmma16(ci[i][j], ar, bi);
+          dmma16(ci[i][j], ai, br);
+        }
       }
-      if (kt + 1 < ktiles) stash(s ^ 1);
-      __syncthreads();
     }
+    cp_async_wait<0>();
 
     const bool rd = p.beta_nonzero != 0;
 #pragma unroll
@@ -440,7 +456,7 @@ __global__ void __launch_bounds__(NT, 1) zmma_gemm_kernel(const ZmmaParams p) {
         }
       }
     }
-    if (p.batch > 1) __syncthreads(); /* the shared buffers are reused by the next entry */
+    if (p.batch > 1) __syncthreads(); /* the stages are reused by the next entry */
   }
 }
 
@@ -531,7 +547,7 @@ extern "C" int hcbk_zgemm_zmma(const hcbk_gemm_args *a, void *stream) {
   const int64_t tiles = ((a->m + ZBM - 1) / ZBM) * ((a->n + ZBN - 1) / ZBN);
   if (tiles > 0x7fffffffLL) return HCBK_ERR_ARGS;
   dim3 grid((unsigned)tiles, (unsigned)(a->batch < 65535 ? a->batch : 65535), 1);
-  constexpr int smem = 2 * 2 * ZBK * (ZLDA + ZLDB) * (int)sizeof(double);
+  constexpr int smem = ZSTAGES * (ZOPA + ZOPB) * (int)sizeof(double2); /* the ring */
   using K = void (*)(const ZmmaParams);
   static const K table[3][3] = {
       {zmma_gemm_kernel<0, 0>, zmma_gemm_kernel<0, 1>, zmma_gemm_kernel<0, 2>},
