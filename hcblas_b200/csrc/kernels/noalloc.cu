@@ -24,7 +24,8 @@
  * device, with that device current, asks the runtime for the array's device
  * address with cudaGetSymbolAddress and caches it together with the context
  * it belongs to; a call from another context (for example after
- * cudaDeviceReset) looks the address up again.
+ * cudaDeviceReset) looks the address up again.  That first call should come
+ * before any stream capture begins.
  *
  * Every call on a device shares the one array, and the array keeps the last
  * call's contents.  The pack kernel rewrites every plane element the GEMM

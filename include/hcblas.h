@@ -582,7 +582,8 @@ int hcblasGetProfile(hcblasHandle_t handle, char *buf, int cap);
  *
  * The first call in each CUDA context of a device looks up the array's
  * device address (cudaGetSymbolAddress, with that device current) and
- * caches it with the context.  All calls on a device share the array and it keeps the
+ * caches it with the context; make that first call before any stream
+ * capture begins.  All calls on a device share the array and it keeps the
  * last call's contents, so calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller. */
 #define HCBLAS_NOALLOC_SCRATCH_BYTES (64u << 20)
