@@ -134,6 +134,38 @@ def test_split_bf16_sgemm(handle, terms, ta, tb, pair_mode):
         hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
 
 
+def test_split_bf16_pack_paths_agree(handle):
+    """The K-contiguous pack (packed f32x2 Veltkamp splits where the values
+    allow, integer rounding elsewhere) and the MN-contiguous pack (integer
+    rounding throughout) must produce the same bf16 planes: the same matrix
+    stored both ways round (op N vs op T) gives bit-identical C, with zeros,
+    subnormals, values near 2^-100 and 2^110 and beyond mixed in."""
+    rng = np.random.default_rng(77)
+    M, N, K = 192, 160, 200
+    Ad = (rng.standard_normal((M, K)) * np.exp2(rng.integers(-30, 31, (M, K)))).astype(np.float32)
+    special = np.array([0.0, -0.0, 1e-40, -3e-39, 2.0 ** -100, -(2.0 ** -101), 2.0 ** 109,
+                        -(2.0 ** 110), 2.0 ** 115, 1.5 * 2.0 ** -99, 3.0, -7.0], np.float32)
+    idx = rng.choice(M * K, 600, replace=False)
+    Ad.reshape(-1)[idx] = special[rng.integers(0, special.size, idx.size)]
+    Bd = rng.standard_normal((K, N)).astype(np.float32)
+    A_n = np.asfortranarray(Ad).reshape(-1, order="F")    # column-major M x K, op N
+    A_t = np.asfortranarray(Ad.T).reshape(-1, order="F")  # column-major K x M, op T
+    B_n = np.asfortranarray(Bd).reshape(-1, order="F")
+    assert hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_SPLIT_BF16, 6) == 0
+    try:
+        outs = []
+        for A, ta, lda in ((A_n, "n", M), (A_t, "t", K)):
+            dA, dB = hb.DeviceArray(handle, A), hb.DeviceArray(handle, B_n)
+            dC = hb.DeviceArray(handle, np.zeros(M * N, np.float32))
+            assert hb.lib_gemm(handle, O.COL, ta, "n", M, N, K, 1.0, dA, lda, dB, K, 0.0, dC,
+                               M) == 0
+            assert hb.device_error(handle) == 0
+            outs.append(dC.download())
+    finally:
+        hb.hcblasSetMathMode(handle, hb.HCBLAS_MATH_NATIVE, 0)
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
 def test_split_bf16_accuracy_vs_plain(handle):
     """Report (and bound) the split-BF16 error next to plain FP32 at K = 2048,
     entries N(0,1) * 2^e, e ~ U{-8..8} per row of A / column of B."""
