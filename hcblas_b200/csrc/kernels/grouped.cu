@@ -695,21 +695,28 @@ __device__ __forceinline__ PackJob load_job(const hcbk_gpack_job *j) {
   return o;
 }
 
-/* this thread's eight source values of tile (r0, k0) */
+/* this thread's eight source values of tile (r0, k0); the addresses step
+ * by 8 rows (K-contiguous source) or 8 k (MN-contiguous) from one base */
 __device__ __forceinline__ void pack_load(const PackJob &j, int r0, int k0, float (&v)[8]) {
   const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t step = 8 * j.ld;
   if (j.k_contig) {
+    const int ka = k0 + tx, kb = k0 + tx + 32;
+    const bool oka = ka < j.kdim, okb = kb < j.kdim;
+    const float *p = j.src + (int64_t)(r0 + ty) * j.ld;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = r0 + ty + 8 * (i & 3), k = k0 + tx + 32 * (i >> 2);
-      v[i] = (r < j.rows && k < j.kdim) ? __ldg(j.src + (int64_t)r * j.ld + k) : 0.f;
+    for (int q = 0; q < 4; ++q, p += step) {
+      const bool rok = r0 + ty + 8 * q < j.rows;
+      v[q] = (rok && oka) ? __ldg(p + ka) : 0.f;
+      v[q + 4] = (rok && okb) ? __ldg(p + kb) : 0.f;
     }
   } else {
+    const int r = r0 + tx;
+    const bool rok = r < j.rows;
+    const float *p = j.src + r + (int64_t)(k0 + ty) * j.ld;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = r0 + tx, k = k0 + ty + 8 * i;
-      v[i] = (r < j.rows && k < j.kdim) ? __ldg(j.src + r + (int64_t)k * j.ld) : 0.f;
-    }
+    for (int i = 0; i < 8; ++i, p += step)
+      v[i] = (rok && k0 + ty + 8 * i < j.kdim) ? __ldg(p) : 0.f;
   }
 }
 
@@ -729,9 +736,9 @@ __global__ void __launch_bounds__(256) grouped_pack_kernel(const hcbk_gpack_job 
   const int t_end = (int)((int64_t)total * (blockIdx.x + 1) / gridDim.x);
   if (t_begin >= t_end) return;
   int g = find_problem(ts, count, t_begin);
-  int g_first = __ldg(ts + g), g_next = __ldg(ts + g + 1);
+  int g_next = __ldg(ts + g + 1);
   PackJob nj = load_job(jobs + g);
-  int lt = t_begin - g_first;
+  const int lt = t_begin - __ldg(ts + g); /* the one division: where the block starts */
   int nr0 = (lt % nj.tiles_r) * 32, nk0 = (lt / nj.tiles_r) * 64;
   float v[8];
   pack_load(nj, nr0, nk0, v);
@@ -748,17 +755,21 @@ __global__ void __launch_bounds__(256) grouped_pack_kernel(const hcbk_gpack_job 
     }
     __syncthreads();
     if (t + 1 < t_end) { /* start the next tile's loads */
-      if (t + 1 >= g_next) {
+      if (t + 1 >= g_next) { /* the next job's first tile */
         while (t + 1 >= g_next) {
           ++g;
           g_next = __ldg(ts + g + 1);
         }
-        g_first = __ldg(ts + g);
         nj = load_job(jobs + g);
+        nr0 = 0;
+        nk0 = 0;
+      } else { /* the job's next tile: row tiles first, then K */
+        nr0 += 32;
+        if (nr0 >= nj.tiles_r * 32) {
+          nr0 = 0;
+          nk0 += 64;
+        }
       }
-      lt = t + 1 - g_first;
-      nr0 = (lt % nj.tiles_r) * 32;
-      nk0 = (lt / nj.tiles_r) * 64;
       pack_load(nj, nr0, nk0, v);
     }
     /* this thread's row and 8 consecutive k: one 16-byte store per plane
