@@ -453,16 +453,13 @@ struct CrtAcc {
 
 /* real combine: 256 consumer threads x 2 consecutive rows (one 2-byte
  * load of two int8 residues per modulus); 3 stages of nmod / 2 KB */
-constexpr int CMB_THREADS = 256, CMB_RPT = 2, CMB_ROWS = CMB_THREADS * CMB_RPT;
+constexpr int CMB_THREADS = 256, CMB_RPT = 4, CMB_ROWS = CMB_THREADS * CMB_RPT;
 constexpr int CMB_STAGES = 3;
 /* complex combine: 256 consumer threads x 1 row (two accumulators a row
  * already); 3 stages of 0.75 nmod KB */
 constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 1, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
 constexpr int ZCMB_STAGES = 3;
 
-/* the two signed bytes of a 16-bit word */
-__device__ __forceinline__ int lo8(uint32_t w) { return (int)(w << 24) >> 24; }
-__device__ __forceinline__ int hi8(uint32_t w) { return (int)(w << 16) >> 24; }
 
 /* Walk over a block's tiles first, first + stride, ... of a grid of
  * row_tiles x columns tiles (column-major tile order), keeping the tile's
@@ -544,7 +541,7 @@ constexpr int CMB_CONSUMERS = CMB_THREADS / 32;
 constexpr int CMB_BLOCK = CMB_THREADS + 32;
 
 template <int NC>
-__global__ void __launch_bounds__(CMB_BLOCK, 5) crt_combine_kernel(const __grid_constant__ CombArgs a) {
+__global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_constant__ CombArgs a) {
   using namespace hcbk::tc;
   extern __shared__ __align__(128) unsigned char cmb_smem[];
   __shared__ __align__(8) uint64_t full[CMB_STAGES], empty[CMB_STAGES];
@@ -588,12 +585,13 @@ __global__ void __launch_bounds__(CMB_BLOCK, 5) crt_combine_kernel(const __grid_
 #pragma unroll
       for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights */
         if (i >= nmod) break;
-        const uint32_t q = *reinterpret_cast<const uint16_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
-        const double r0 = small_int_to_d(lo8(q)), r1 = small_int_to_d(hi8(q));
+        /* the four rows' residues of this modulus, each byte sign-extended */
+        const uint32_t q = *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
 #pragma unroll
-        for (int k = 0; k < NC; ++k) {
-          acc[0].S[k] = fma(r0, a.w[i][k], acc[0].S[k]);
-          acc[1].S[k] = fma(r1, a.w[i][k], acc[1].S[k]);
+        for (int u = 0; u < CMB_RPT; ++u) {
+          const double r = small_int_to_d((int)(q << (24 - 8 * u)) >> 24);
+#pragma unroll
+          for (int k = 0; k < NC; ++k) acc[u].S[k] = fma(r, a.w[i][k], acc[u].S[k]);
         }
       }
       __syncwarp();
