@@ -457,7 +457,7 @@ constexpr int CMB_THREADS = 256, CMB_RPT = 4, CMB_ROWS = CMB_THREADS * CMB_RPT;
 constexpr int CMB_STAGES = 3;
 /* complex combine: 256 consumer threads x 1 row (two accumulators a row
  * already); 3 stages of 0.75 nmod KB */
-constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 1, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
+constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 2, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
 constexpr int ZCMB_STAGES = 3;
 
 
@@ -1010,38 +1010,47 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
     const int s = w.s;
     if (!__all_sync(0xffffffffu, mbar_wait(&full[s], w.ph, a.g.err, ERR_TIMEOUT_COMBINE))) break;
     const int8_t *R = buf + s * stage_elems;
-    const int64_t row = w.rt * ZCMB_ROWS + tid, col = w.col;
-    CrtAcc<NC> acc_re, acc_im;
+    /* two consecutive rows per thread: twice the independent FMA chains */
+    const int64_t row = w.rt * ZCMB_ROWS + ZCMB_RPT * tid, col = w.col;
+    CrtAcc<NC> acc_re[ZCMB_RPT], acc_im[ZCMB_RPT];
     if (row < a.g.m) {
 #pragma unroll
       for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights and moduli */
         if (i >= nmod) break;
-        const float t1 = small_int_to_f(R[i * ZCMB_ROWS + tid]);
-        const float t2 = small_int_to_f(R[(nmod + i) * ZCMB_ROWS + tid]);
-        const float t3 = small_int_to_f(R[(2 * nmod + i) * ZCMB_ROWS + tid]);
         const float p = a.g.p[i], ip = a.g.inv_p[i], hp = a.g.hp[i];
-        const double re = small_int_to_d(small_f_to_int(sym_f(mod_f(t1 - t2, p, ip), p, hp)));
-        const double im = small_int_to_d(small_f_to_int(sym_f(mod_f(t3 - t1 - t2, p, ip), p, hp)));
 #pragma unroll
-        for (int k = 0; k < NC; ++k) {
-          acc_re.S[k] = fma(re, a.g.w[i][k], acc_re.S[k]);
-          acc_im.S[k] = fma(im, a.g.w[i][k], acc_im.S[k]);
+        for (int u = 0; u < ZCMB_RPT; ++u) {
+          const int o = ZCMB_RPT * tid + u;
+          const float t1 = small_int_to_f(R[i * ZCMB_ROWS + o]);
+          const float t2 = small_int_to_f(R[(nmod + i) * ZCMB_ROWS + o]);
+          const float t3 = small_int_to_f(R[(2 * nmod + i) * ZCMB_ROWS + o]);
+          const double re = small_int_to_d(small_f_to_int(sym_f(mod_f(t1 - t2, p, ip), p, hp)));
+          const double im =
+              small_int_to_d(small_f_to_int(sym_f(mod_f(t3 - t1 - t2, p, ip), p, hp)));
+#pragma unroll
+          for (int k = 0; k < NC; ++k) {
+            acc_re[u].S[k] = fma(re, a.g.w[i][k], acc_re[u].S[k]);
+            acc_im[u].S[k] = fma(im, a.g.w[i][k], acc_im[u].S[k]);
+          }
         }
       }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]); /* the stage's residues are in registers */
-    if (row < a.g.m) {
-      const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
-      const int ea = row_exp(a.g.exp_a, a.exp_a_pair, row);
-      double re = acc_re.finish(a.g, ea, eb);
-      double im = acc_im.finish(a.g, ea, eb);
+    const int eb = row_exp(a.g.exp_b, a.exp_b_pair, col);
+#pragma unroll
+    for (int u = 0; u < ZCMB_RPT; ++u) {
+      const int64_t r = row + u;
+      if (r >= a.g.m) break;
+      const int ea = row_exp(a.g.exp_a, a.exp_a_pair, r);
+      double re = acc_re[u].finish(a.g, ea, eb);
+      double im = acc_im[u].finish(a.g, ea, eb);
       if (a.g.inv_a) {
-        const double sc = a.g.inv_a[row] * a.g.inv_b[col];
+        const double sc = a.g.inv_a[r] * a.g.inv_b[col];
         re *= sc;
         im *= sc;
       }
-      double2 *dst = a.c + row + col * a.ldc;
+      double2 *dst = a.c + r + col * a.ldc;
       double2 o;
       o.x = a.alpha.x * re - a.alpha.y * im;
       o.y = a.alpha.x * im + a.alpha.y * re;
