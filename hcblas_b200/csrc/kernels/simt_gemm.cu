@@ -551,6 +551,15 @@ simt_gemm_kernel(SimtParams<T, typename AccOf<T>::type> p) {
   const int64_t m0 = tile_m * BM;
   const int64_t n0 = tile_n * BN;
 
+  if (p.sel) {
+    /* a selective pass (usually with nothing selected): the block's threads
+     * read its entries' flags together and the block leaves when none is set */
+    int any = 0;
+    for (int64_t b = blockIdx.y + (int64_t)threadIdx.x * gridDim.y; b < p.batch;
+         b += (int64_t)gridDim.y * blockDim.x)
+      any |= p.sel[b];
+    if (!__syncthreads_or(any)) return;
+  }
   for (int64_t bidx = blockIdx.y; bidx < p.batch; bidx += gridDim.y) {
     if (p.sel && p.sel[bidx] == 0) continue; /* uniform across the block */
     TileJob<T> j;
@@ -655,11 +664,27 @@ int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
   p.beta_nonzero = (a->beta_re != 0.0 || a->beta_im != 0.0);
   const int64_t tiles = ((a->m + BM - 1) / BM) * ((a->n + BN - 1) / BN);
   if (tiles > 0x7fffffffLL) return HCBK_ERR_ARGS;
-  dim3 grid((unsigned)tiles, (unsigned)(a->batch < 65535 ? a->batch : 65535), 1);
+  const int64_t gy = a->batch < 65535 ? a->batch : 65535;
   dim3 block((BM / TM) * (BN / TN));
+  /* a selective pass runs as one wave of blocks, each scanning its share of
+   * the flags at once (as many blocks as entries would queue in waves of
+   * blocks that mostly find nothing to do) */
+  auto grid_of = [&](auto kern) {
+    int per_sm = 0;
+    int64_t y = gy;
+    if (a->batch_select &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)block.x, 0) ==
+            cudaSuccess &&
+        per_sm > 0) {
+      const int64_t cap = ((int64_t)hcbk_sm_count() * per_sm + tiles - 1) / tiles;
+      if (y > cap) y = cap;
+    }
+    return dim3((unsigned)tiles, (unsigned)y, 1);
+  };
 #define HCBK_SIMT_CASE(OA, OB)                                                    \
   if (a->op_a == OA && a->op_b == OB) {                                           \
-    simt_gemm_kernel<T, BM, BN, BK, TM, TN, OA, OB, MINB><<<grid, block, 0, st>>>(p); \
+    auto kern = simt_gemm_kernel<T, BM, BN, BK, TM, TN, OA, OB, MINB>;           \
+    kern<<<grid_of(kern), block, 0, st>>>(p);                                     \
     return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;         \
   }
   HCBK_SIMT_CASE(0, 0) HCBK_SIMT_CASE(0, 1) HCBK_SIMT_CASE(1, 0) HCBK_SIMT_CASE(1, 1)
