@@ -971,12 +971,25 @@ int hgemm_ptr_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *stream
   if (!grouped_ensure_table(gp, bytes, stream)) return HCBK_ERR_NOMEM;
   char *tb = static_cast<char *>(gp.table);
   /* the template: this batch's shape and strides, with the table itself as
-   * a stand-in base address (replaced for every entry on the device) */
+   * a stand-in base address (replaced for every entry on the device); kept
+   * for the next call of the same shape */
+  const int64_t tkey[] = {a->op_a, a->op_b, a->m, a->n, a->k, a->lda, a->ldb, a->ldc,
+                          st->grouped_c_tma, (int64_t)reinterpret_cast<uintptr_t>(tb)};
   hcbk_grouped_entry tmpl;
-  int rc = hcbk_grouped_encode(&tmpl, a->op_a, a->op_b, a->m, a->n, a->k, tb, a->lda, tb,
-                               a->ldb, tb, a->ldc);
-  if (rc) return rc;
-  if (!st->grouped_c_tma) tmpl.c_tma = 0; /* direct stores */
+  if (gp.key.size() == sizeof(tkey) + sizeof(tmpl) &&
+      std::memcmp(gp.key.data(), tkey, sizeof(tkey)) == 0) {
+    std::memcpy(&tmpl, gp.key.data() + sizeof(tkey), sizeof(tmpl));
+  } else {
+    gp.key.clear();
+    const int rc = hcbk_grouped_encode(&tmpl, a->op_a, a->op_b, a->m, a->n, a->k, tb, a->lda,
+                                       tb, a->ldb, tb, a->ldc);
+    if (rc) return rc;
+    if (!st->grouped_c_tma) tmpl.c_tma = 0; /* direct stores */
+    gp.key.resize(sizeof(tkey) + sizeof(tmpl));
+    std::memcpy(gp.key.data(), tkey, sizeof(tkey));
+    std::memcpy(gp.key.data() + sizeof(tkey), &tmpl, sizeof(tmpl));
+  }
+  int rc = HCBK_OK;
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;
   auto *table = reinterpret_cast<hcbk_grouped_entry *>(tb);

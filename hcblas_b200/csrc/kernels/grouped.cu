@@ -416,15 +416,19 @@ struct PtrTableArgs {
 };
 
 __global__ void __launch_bounds__(128) grouped_ptr_table_kernel(const __grid_constant__ PtrTableArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  /* one warp per entry: the lanes copy the template together, lane 0 then
+   * patches the addresses */
+  const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (i > a.count) return;
-  a.tile_start[i] = i * a.tiles;
+  if (lane == 0) a.tile_start[i] = i * a.tiles;
   if (i == a.count) return;
   hcbk_grouped_entry *e = a.table + i;
-  const uint4 *src = a.tmpl;
   uint4 *dst = reinterpret_cast<uint4 *>(e);
-#pragma unroll 4
-  for (int j = 0; j < (int)(sizeof(hcbk_grouped_entry) / 16); ++j) dst[j] = src[j];
+  for (int j = lane; j < (int)(sizeof(hcbk_grouped_entry) / 16); j += 32) dst[j] = a.tmpl[j];
+  tensormap_release();
+  __syncwarp(); /* the copies are ordered before lane 0's patches */
+  if (lane != 0) return;
   const char *pa = static_cast<const char *>(a.a_arr[i]);
   const char *pb = static_cast<const char *>(a.b_arr[i]);
   char *pc = static_cast<char *>(a.c_arr[i]);
@@ -895,8 +899,8 @@ extern "C" int hcbk_grouped_ptr_table(const hcbk_grouped_entry *tmpl, hcbk_group
   a.c_stride_bytes = c_stride_bytes;
   a.count = count;
   a.tiles = hcbk_grouped_tiles(tmpl);
-  const int threads = 128;
-  const int blocks = (count + 1 + threads - 1) / threads;
+  const int threads = 128; /* four entries per block */
+  const int blocks = (count + 1 + 3) / 4;
   grouped_ptr_table_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(a);
   return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;
 }

@@ -643,6 +643,16 @@ simt_grouped_kernel(const hcbk_simt_entry *table, const int32_t *tile_start, int
 
 /* ------------------------------------------------------------ launchers -- */
 
+/* blocks of `kern` resident per SM (1 if the query fails) */
+template <class K> static int resident_blocks(K kern, int threads) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  return per_sm > 0 ? per_sm : 1;
+}
+
 /* MINB: CTAs per SM the register allocation must allow (2 for the FP32
  * 128 x 128 tile: sixteen warps per SM hide the global-load latency of each
  * K-slab better than eight) */
@@ -669,13 +679,9 @@ int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
   /* a selective pass runs as one wave of blocks, each scanning its share of
    * the flags at once (as many blocks as entries would queue in waves of
    * blocks that mostly find nothing to do) */
-  auto grid_of = [&](auto kern) {
-    int per_sm = 0;
+  auto grid_of = [&](int per_sm) {
     int64_t y = gy;
-    if (a->batch_select &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)block.x, 0) ==
-            cudaSuccess &&
-        per_sm > 0) {
+    if (a->batch_select) {
       const int64_t cap = ((int64_t)hcbk_sm_count() * per_sm + tiles - 1) / tiles;
       if (y > cap) y = cap;
     }
@@ -684,7 +690,12 @@ int launch_cfg(const hcbk_gemm_args *a, cudaStream_t st) {
 #define HCBK_SIMT_CASE(OA, OB)                                                    \
   if (a->op_a == OA && a->op_b == OB) {                                           \
     auto kern = simt_gemm_kernel<T, BM, BN, BK, TM, TN, OA, OB, MINB>;           \
-    kern<<<grid_of(kern), block, 0, st>>>(p);                                     \
+    int per_sm = 1;                                                               \
+    if (a->batch_select) {                                                        \
+      static const int resident = resident_blocks(kern, (int)block.x);           \
+      per_sm = resident;                                                          \
+    }                                                                             \
+    kern<<<grid_of(per_sm), block, 0, st>>>(p);                                   \
     return cudaGetLastError() == cudaSuccess ? HCBK_OK : HCBK_ERR_LAUNCH;         \
   }
   HCBK_SIMT_CASE(0, 0) HCBK_SIMT_CASE(0, 1) HCBK_SIMT_CASE(1, 0) HCBK_SIMT_CASE(1, 1)
