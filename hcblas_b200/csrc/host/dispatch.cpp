@@ -925,10 +925,27 @@ int hgemm_strided_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *st
   if ((a->lda & 7) || (a->ldb & 7) || (a->stride_a & 7) || (a->stride_b & 7) ||
       !aligned16(a->a, a->a_off, 2) || !aligned16(a->b, a->b_off, 2))
     return HCBK_ERR_ALIGN;
-  std::vector<hcblasGemmProblem> probs((size_t)a->batch);
   const uint16_t *A = static_cast<const uint16_t *>(a->a) + a->a_off; /* f16 storage */
   const uint16_t *B = static_cast<const uint16_t *>(a->b) + a->b_off;
   uint16_t *C = static_cast<uint16_t *>(a->c) + a->c_off;
+  /* the batch in a few words: a repeated call finds its table without
+   * spelling out every element */
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int64_t ck[] = {a->op_a, a->op_b, a->m, a->n, a->k, a->lda, a->ldb, a->ldc,
+                        a->stride_a, a->stride_b, a->stride_c, a->batch,
+                        (int64_t)reinterpret_cast<uintptr_t>(A),
+                        (int64_t)reinterpret_cast<uintptr_t>(B),
+                        (int64_t)reinterpret_cast<uintptr_t>(C), st->grouped_c_tma, dev};
+  const std::vector<unsigned char> compact(reinterpret_cast<const unsigned char *>(ck),
+                                           reinterpret_cast<const unsigned char *>(ck) + sizeof(ck));
+  if (a->alpha_re != 0.0 && grouped_hgemm_compact_match(st, compact)) {
+    const int rc = grouped_hgemm(st, stream, ColMajor, (int)a->batch, nullptr,
+                                 (float)a->alpha_re, (float)a->beta_re, &compact);
+    *path = st->last_path;
+    return rc;
+  }
+  std::vector<hcblasGemmProblem> probs((size_t)a->batch);
   for (int64_t i = 0; i < a->batch; ++i) {
     hcblasGemmProblem &p = probs[(size_t)i];
     p.transa = a->op_a == HCBK_OP_N ? HCBLAS_OP_N : HCBLAS_OP_T;
@@ -944,7 +961,7 @@ int hgemm_strided_grouped(HcblasB200State *st, const hcbk_gemm_args *a, void *st
     p.ldc = (int)a->ldc;
   }
   int rc = grouped_hgemm(st, stream, ColMajor, (int)a->batch, probs.data(), (float)a->alpha_re,
-                         (float)a->beta_re);
+                         (float)a->beta_re, &compact);
   *path = st->last_path;
   return rc;
 }

@@ -95,9 +95,18 @@ int plan_emulation(int mode, int param, int bits, int dtype, int64_t k, double *
 double emulation_model_bits(int mode, int dtype, int64_t k, int count);
 
 /* Grouped HGEMM over `count` problems (grouped.cpp): builds or reuses the
- * handle's device problem table and runs the persistent kernel. */
+ * handle's device problem table and runs the persistent kernel.  `compact`
+ * (optional) is a short key that determines every problem (a strided batch's
+ * shape, strides and base addresses): when it matches the one the table was
+ * built for, the table is reused without looking at `probs`, which may then
+ * be null (alpha != 0 only). */
 int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,
-                  const hcblasGemmProblem *probs, float alpha, float beta);
+                  const hcblasGemmProblem *probs, float alpha, float beta,
+                  const std::vector<unsigned char> *compact = nullptr);
+
+/* whether `compact` is the short key of the handle's current grouped HGEMM
+ * table (the caller may then pass no problems) */
+bool grouped_hgemm_compact_match(HcblasB200State *st, const std::vector<unsigned char> &compact);
 
 /* Grouped GEMM of S/D/C/Z problems on the CUDA cores (one persistent
  * launch); scalars as real and imaginary parts. */

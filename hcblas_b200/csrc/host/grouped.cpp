@@ -110,8 +110,19 @@ bool grouped_ensure_table(HcblasGroupedPlan &gp, size_t bytes, void *stream) {
 }
 
 /* Build (or reuse) the plan and run every problem; HCBK_* code. */
+bool grouped_hgemm_compact_match(HcblasB200State *st, const std::vector<unsigned char> &compact) {
+  const HcblasGroupedPlan &gp = st->grouped;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return gp.table && gp.table_device == dev && !gp.compact_key.empty() &&
+         gp.fallback.empty() && compact == gp.compact_key;
+}
+
 int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int count,
-                  const hcblasGemmProblem *probs, float alpha, float beta) {
+                  const hcblasGemmProblem *probs, float alpha, float beta,
+                  const std::vector<unsigned char> *compact) {
+  if (!probs && (alpha == 0.0f || !compact || !grouped_hgemm_compact_match(st, *compact)))
+    return HCBK_ERR_ARGS;
   if (alpha == 0.0f) { /* C_i := beta*C_i, A and B not referenced (CBLAS) */
     for (int i = 0; i < count; ++i) {
       const Canon c = canonical(probs[i], order);
@@ -134,12 +145,16 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
   HcblasGroupedPlan &gp = st->grouped;
   int dev = 0;
   cudaGetDevice(&dev);
-  std::vector<unsigned char> key(sizeof(hcblasGemmProblem) * (size_t)count + 3);
-  std::memcpy(key.data(), probs, sizeof(hcblasGemmProblem) * (size_t)count);
-  key[key.size() - 3] = static_cast<unsigned char>(st->grouped_c_tma);
-  key[key.size() - 2] = static_cast<unsigned char>(order);
-  key[key.size() - 1] = static_cast<unsigned char>(dev);
-  const bool reuse = gp.table && gp.table_device == dev && key == gp.key;
+  std::vector<unsigned char> key;
+  bool reuse = compact && grouped_hgemm_compact_match(st, *compact);
+  if (!reuse) {
+    key.resize(sizeof(hcblasGemmProblem) * (size_t)count + 3);
+    std::memcpy(key.data(), probs, sizeof(hcblasGemmProblem) * (size_t)count);
+    key[key.size() - 3] = static_cast<unsigned char>(st->grouped_c_tma);
+    key[key.size() - 2] = static_cast<unsigned char>(order);
+    key[key.size() - 1] = static_cast<unsigned char>(dev);
+    reuse = gp.table && gp.table_device == dev && key == gp.key;
+  }
 
   if (!reuse) {
     /* captured graphs of earlier grouped calls read this table: drop them */
@@ -148,6 +163,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
       clear_graph_cache(st);
     }
     gp.key.clear();
+    gp.compact_key.clear();
     std::vector<hcbk_grouped_entry> ent((size_t)count);
     std::vector<int> ok_idx;
     std::vector<int> fallback;
@@ -217,6 +233,7 @@ int grouped_hgemm(HcblasB200State *st, void *stream, hcblasOrder order, int coun
     gp.tuned_ctas = 0;
     gp.key = key;
   }
+  if (compact) gp.compact_key = *compact; /* the table built or matched holds these problems */
 
   int *err = device_error_flag(st);
   if (!err) return HCBK_ERR_NOMEM;

@@ -33,6 +33,7 @@ struct HcblasGroupedPlan {
   size_t staging_bytes = 0;
   void *upload_done = nullptr; /* cudaEvent_t recorded after the staging copy */
   std::vector<unsigned char> key;
+  std::vector<unsigned char> compact_key; /* strided batches: a short key equivalent to `key` */
   int count = 0;       /* problems in the device table */
   int total_tiles = 0;
   size_t tile_start_offset = 0;
