@@ -114,6 +114,23 @@ def _strided(h, batch=512, n=128, seed=5):
     return call, (dA, dB, dC)
 
 
+def _ptr_batch(h, batch=512, n=128, seed=5):
+    """The strided case's batch through hcblasHgemmBatched (device-resident
+    pointer arrays): table build, grouped launch, selective CUDA-core pass."""
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1, 1, n * n * batch).astype(np.float16)
+    B = rng.uniform(-1, 1, n * n * batch).astype(np.float16)
+    dA, dB = _dev(h, A), _dev(h, B)
+    dC = hb.DeviceArray(h, nbytes=2 * n * n * batch, dtype=np.float16)
+    ptrs = [_dev(h, np.array([d.ptr + 2 * i * n * n for i in range(batch)], dtype=np.uint64))
+            for d in (dA, dB, dC)]
+
+    def call():
+        assert hb.gemm_batched(h, 0, 0, n, n, n, 1.0, ptrs[0].ptr, n, ptrs[1].ptr, n, 0.0,
+                               ptrs[2].ptr, n, batch, np.float16) == 0
+    return call, (dA, dB, dC, ptrs)
+
+
 def _gemv(h, dtype, trans, m, n, seed=6):
     rng = np.random.default_rng(seed)
     A = rng.uniform(-1, 1, m * n).astype(dtype)
@@ -189,6 +206,7 @@ CASES = {
     "hgemm_grouped_4096_ldc8": lambda h: _grouped(h, pad_c=True),
     "sgemm_grouped_4096": lambda h: _grouped(h, dtype=np.float32),
     "hgemm_strided_512x128": _strided,
+    "hgemm_ptr_512x128": _ptr_batch,
     "sgemv_n_16384": lambda h: _gemv(h, np.float32, 0, 16384, 16384),
     "sgemv_t_16384": lambda h: _gemv(h, np.float32, 1, 16384, 16384),
     "dgemv_n_16384": lambda h: _gemv(h, np.float64, 0, 16384, 16384),

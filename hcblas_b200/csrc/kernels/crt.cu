@@ -399,6 +399,14 @@ __device__ __forceinline__ double small_int_to_d(int r) {
   return __hiloint2double(0x43300000, r ^ (int)0x80000000) - 4503601774854144.0;
 }
 
+/* byte u of four int8 residues whose sign bits were flipped (each byte
+ * r + 128, 0..255) as the binary64 value r: the byte, zero-extended by one
+ * byte permute, under the exponent of 2^52 gives 2^52 + 128 + r */
+__device__ __forceinline__ double biased_byte_to_d(uint32_t qb, int u) {
+  return __hiloint2double(0x43300000, (int)__byte_perm(qb, 0u, 0x4440u + (uint32_t)u)) -
+         4503599627370624.0;
+}
+
 template <int NC>
 struct CrtAcc {
   double S[NC];
@@ -585,11 +593,12 @@ __global__ void __launch_bounds__(CMB_BLOCK, 4) crt_combine_kernel(const __grid_
 #pragma unroll
       for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights */
         if (i >= nmod) break;
-        /* the four rows' residues of this modulus, each byte sign-extended */
-        const uint32_t q = *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid);
+        /* the four rows' residues of this modulus, sign bits flipped */
+        const uint32_t q =
+            *reinterpret_cast<const uint32_t *>(R + i * CMB_ROWS + CMB_RPT * tid) ^ 0x80808080u;
 #pragma unroll
         for (int u = 0; u < CMB_RPT; ++u) {
-          const double r = small_int_to_d((int)(q << (24 - 8 * u)) >> 24);
+          const double r = biased_byte_to_d(q, u);
 #pragma unroll
           for (int k = 0; k < NC; ++k) acc[u].S[k] = fma(r, a.w[i][k], acc[u].S[k]);
         }
