@@ -459,14 +459,15 @@ struct CrtAcc {
   }
 };
 
-/* real combine: 256 consumer threads x 2 consecutive rows (one 2-byte
- * load of two int8 residues per modulus); 3 stages of nmod / 2 KB */
+/* real combine: 256 consumer threads x 4 consecutive rows (one 4-byte
+ * load of four int8 residues per modulus); 3 stages of nmod KB */
 constexpr int CMB_THREADS = 256, CMB_RPT = 4, CMB_ROWS = CMB_THREADS * CMB_RPT;
 constexpr int CMB_STAGES = 3;
-/* complex combine: 256 consumer threads x 1 row (two accumulators a row
- * already); 3 stages of 0.75 nmod KB */
+/* complex combine: 256 consumer threads x 2 rows (two accumulators a
+ * row); 3 stages of 1.5 nmod KB */
 constexpr int ZCMB_THREADS = 256, ZCMB_RPT = 2, ZCMB_ROWS = ZCMB_THREADS * ZCMB_RPT;
 constexpr int ZCMB_STAGES = 3;
+static_assert(ZCMB_RPT == 2, "the complex combine loads two rows' residues as one 2-byte word");
 
 
 /* Walk over a block's tiles first, first + stride, ... of a grid of
@@ -974,9 +975,17 @@ struct ZCombArgs {
   double2 alpha, beta;
 };
 
-/* f32 holding a small integer (|x| < 2^22) to int without the conversion unit */
-__device__ __forceinline__ int small_f_to_int(float x) {
-  return __float_as_int(x + RND_F) - 0x4B400000;
+/* f32 holding a small integer (|x| < 2^22) to binary64 without the
+ * conversion unit: x + 1.5 * 2^23 has the bit pattern 0x4B400000 + x, which
+ * under the exponent of 2^52 gives 2^52 + 0x4B400000 + x */
+__device__ __forceinline__ double small_f_to_d(float x) {
+  return __hiloint2double(0x43300000, __float_as_int(x + RND_F)) - 4503600889856000.0;
+}
+
+/* byte u of two int8 residues whose sign bits were flipped (r + 128) as the
+ * f32 value 1.5 * 2^23 + 128 + r: the byte under the bit pattern of 1.5 * 2^23 */
+__device__ __forceinline__ float biased_byte_to_f(uint32_t qb, int u) {
+  return __int_as_float((int)__byte_perm(qb, 0x4B400000u, 0x7650u + (uint32_t)u));
 }
 
 /* residues stream through the two accumulators, one modulus at a time: the
@@ -1027,15 +1036,22 @@ __global__ void __launch_bounds__(ZCMB_BLOCK, 3) zcrt_combine_kernel(const __gri
       for (int i = 0; i < HCBK_CRT_MAX_MODULI; ++i) { /* constant-bank weights and moduli */
         if (i >= nmod) break;
         const float p = a.g.p[i], ip = a.g.inv_p[i], hp = a.g.hp[i];
+        /* the two rows' residues of each plane in one 2-byte load, sign bits
+         * flipped; as f32 each is c = B + r with B = 1.5 * 2^23 + 128, so
+         * differences of two are exact without removing B */
+        const int o = ZCMB_RPT * tid;
+        const uint32_t q1 = *reinterpret_cast<const uint16_t *>(R + i * ZCMB_ROWS + o) ^ 0x8080u;
+        const uint32_t q2 =
+            *reinterpret_cast<const uint16_t *>(R + (nmod + i) * ZCMB_ROWS + o) ^ 0x8080u;
+        const uint32_t q3 =
+            *reinterpret_cast<const uint16_t *>(R + (2 * nmod + i) * ZCMB_ROWS + o) ^ 0x8080u;
 #pragma unroll
         for (int u = 0; u < ZCMB_RPT; ++u) {
-          const int o = ZCMB_RPT * tid + u;
-          const float t1 = small_int_to_f(R[i * ZCMB_ROWS + o]);
-          const float t2 = small_int_to_f(R[(nmod + i) * ZCMB_ROWS + o]);
-          const float t3 = small_int_to_f(R[(2 * nmod + i) * ZCMB_ROWS + o]);
-          const double re = small_int_to_d(small_f_to_int(sym_f(mod_f(t1 - t2, p, ip), p, hp)));
-          const double im =
-              small_int_to_d(small_f_to_int(sym_f(mod_f(t3 - t1 - t2, p, ip), p, hp)));
+          const float c1 = biased_byte_to_f(q1, u), c2 = biased_byte_to_f(q2, u);
+          const float c3 = biased_byte_to_f(q3, u);
+          const float t2 = c2 - (RND_F + 128.0f);             /* r2 */
+          const double re = small_f_to_d(sym_f(mod_f(c1 - c2, p, ip), p, hp));
+          const double im = small_f_to_d(sym_f(mod_f((c3 - c1) - t2, p, ip), p, hp));
 #pragma unroll
           for (int k = 0; k < NC; ++k) {
             acc_re[u].S[k] = fma(re, a.g.w[i][k], acc_re[u].S[k]);
